@@ -1,0 +1,149 @@
+"""ctypes mirrors of the plain-C structs in include/dopamine_b200.h.
+
+These are the only types that cross the C ABI: a raw gmsh-like mesh, per-patch boundary
+configurations and the solver parameters (src/solver/mod_fv_solver.f90:solver_params_t).
+"""
+import ctypes as C
+
+import numpy as np
+
+# Boundary-condition ids (src/mod_parameters.f90:41-51)
+BC_INLET, BC_OUTLET, BC_WALL_NOSLIP, BC_WALL_MODEL, BC_SLIP, BC_PERIODIC = 1, 2, 3, 4, 5, 6
+BC_SYMMETRY, BC_FIXEDTEMP, BC_ZEROGRADIENT, BC_WALL_VELOCITY = 7, 8, 9, 10
+BC_BY_NAME = {
+    "inlet": BC_INLET, "outlet": BC_OUTLET, "noSlip": BC_WALL_NOSLIP, "wallModel": BC_WALL_MODEL,
+    "slip": BC_SLIP, "periodic": BC_PERIODIC, "symmetry": BC_SYMMETRY, "fixedTemp": BC_FIXEDTEMP,
+    "zeroGradient": BC_ZEROGRADIENT, "wallVelocity": BC_WALL_VELOCITY,
+}
+
+SCHEME_VANLEER_TVD, SCHEME_KOREN_TVD, SCHEME_CDS, SCHEME_KEP, SCHEME_QUICK = 1, 2, 3, 4, 5
+SCHEME_BY_NAME = {"VANLEER_TVD": 1, "KOREN_TVD": 2, "CDS": 3, "KEP": 4, "QUICK": 5}
+SGS_NONE, SGS_VREMAN, SGS_SMAGORINSKY, SGS_AMD = 0, 1, 2, 3
+WM_LOGLAW, WM_NONE = 0, 1
+FORM_FP64, FORM_MIXED = 0, 1
+
+EL_TET4, EL_HEX8, EL_PRISM6, EL_PYR5 = 4, 5, 6, 7
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+_lp = C.POINTER(C.c_int64)
+
+
+class RawMeshT(C.Structure):
+    _fields_ = [
+        ("n_nodes", C.c_int64), ("xyz", _dp), ("n_cells", C.c_int64), ("cell_type", _ip),
+        ("cell_off", _lp), ("cell_nodes", _ip), ("n_bfaces", C.c_int64), ("bface_off", _lp),
+        ("bface_nodes", _ip), ("bface_patch", _ip), ("n_patches", C.c_int),
+    ]
+
+
+class PatchCfgT(C.Structure):
+    _fields_ = [
+        ("bc_id", C.c_int), ("U_val", C.c_double * 3), ("p_val", C.c_double), ("T_val", C.c_double),
+        ("scalar_mode", C.c_int * 4), ("scalar_value", C.c_double * 4),
+    ]
+
+
+class ParamsT(C.Structure):
+    _fields_ = [
+        ("nu", C.c_double), ("dt", C.c_double), ("cfl_max", C.c_double), ("p_tol", C.c_double),
+        ("p_max_iter", C.c_int), ("scheme", C.c_int), ("sgs_model", C.c_int), ("wall_model", C.c_int),
+        ("n_nonortho_corr", C.c_int), ("rhie_chow_dual", C.c_int), ("nonortho_check", C.c_int),
+        ("use_rotational_projection", C.c_int), ("adapt_dt", C.c_int),
+        ("pressure_min_cos_theta", C.c_double), ("f_const", C.c_double * 3), ("g", C.c_double * 3),
+        ("boussinesq", C.c_int), ("beta", C.c_double), ("T_ref", C.c_double), ("alpha_T", C.c_double),
+        ("Pr_t", C.c_double), ("temperature_scheme", C.c_int), ("n_scalars", C.c_int),
+        ("scalar_scheme", C.c_int), ("scalar_diffusivity", C.c_double * 4), ("scalar_pr_t", C.c_double * 4),
+        ("c_amd", C.c_double), ("amd_wall_gradient", C.c_int), ("wall_model_height", C.c_double),
+        ("wall_model_filter_time", C.c_double), ("wall_model_filter_tf_fac", C.c_double), ("form", C.c_int),
+    ]
+
+
+class StatsT(C.Structure):
+    _fields_ = [
+        ("time", C.c_double), ("E", C.c_double), ("eps", C.c_double), ("Umax", C.c_double), ("Ub", C.c_double),
+        ("tauw_mean", C.c_double), ("nu_sgs_mean", C.c_double), ("max_abs_divU", C.c_double),
+        ("volavg_abs_divU", C.c_double), ("dt_used", C.c_double), ("p_solves", C.c_int), ("p_iters", C.c_int),
+        ("p_resid_max", C.c_double),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+def default_params(**kw):
+    """solver_params_t defaults with the numerics the regression inputs pin
+    (cell_projection='LS', rhie_chow_dual, rotational projection, least-squares gradients)."""
+    p = ParamsT()
+    p.nu = 1.0e-5
+    p.dt = 1.0e-3
+    p.cfl_max = 0.5
+    p.p_tol = 1.0e-10
+    p.p_max_iter = 1000
+    p.scheme = SCHEME_KEP
+    p.sgs_model = SGS_NONE
+    p.wall_model = WM_LOGLAW
+    p.n_nonortho_corr = 0
+    p.rhie_chow_dual = 1
+    p.nonortho_check = 0
+    p.use_rotational_projection = 1
+    p.adapt_dt = 0
+    p.pressure_min_cos_theta = 0.0
+    p.boussinesq = 0
+    p.beta = 3.4e-3
+    p.T_ref = 300.0
+    p.alpha_T = 1.4e-5
+    p.Pr_t = 0.85
+    p.temperature_scheme = SCHEME_VANLEER_TVD
+    p.n_scalars = 0
+    p.scalar_scheme = SCHEME_VANLEER_TVD
+    p.c_amd = 1.0 / 3.0
+    p.amd_wall_gradient = 1
+    p.form = FORM_FP64
+    for k, v in kw.items():
+        if k in ("f_const", "g"):
+            arr = getattr(p, k)
+            for i in range(3):
+                arr[i] = v[i]
+        else:
+            setattr(p, k, v)
+    return p
+
+
+def patch_cfgs(patches):
+    """patches: list of dicts {bc: name or id, U: (3,), p: float, T: float}."""
+    arr = (PatchCfgT * max(1, len(patches)))()
+    for i, pd in enumerate(patches):
+        bc = pd["bc"]
+        arr[i].bc_id = BC_BY_NAME[bc] if isinstance(bc, str) else int(bc)
+        for k, v in enumerate(pd.get("U", (0.0, 0.0, 0.0))):
+            arr[i].U_val[k] = v
+        arr[i].p_val = pd.get("p", 0.0)
+        arr[i].T_val = pd.get("T", 0.0)
+    return arr
+
+
+def _ptr(a, ctype):
+    return a.ctypes.data_as(C.POINTER(ctype))
+
+
+class RawMeshView:
+    """Keeps the numpy buffers of a RawMesh alive while its C struct is in use."""
+
+    def __init__(self, mesh):
+        self._keep = [
+            np.ascontiguousarray(mesh.xyz, dtype=np.float64),
+            np.ascontiguousarray(mesh.cell_type, dtype=np.int32),
+            np.ascontiguousarray(mesh.cell_off, dtype=np.int64),
+            np.ascontiguousarray(mesh.cell_nodes, dtype=np.int32),
+            np.ascontiguousarray(mesh.bface_off, dtype=np.int64),
+            np.ascontiguousarray(mesh.bface_nodes, dtype=np.int32),
+            np.ascontiguousarray(mesh.bface_patch, dtype=np.int32),
+        ]
+        xyz, ct, co, cn, bo, bn, bp = self._keep
+        self.struct = RawMeshT(
+            n_nodes=xyz.shape[0], xyz=_ptr(xyz, C.c_double), n_cells=ct.shape[0], cell_type=_ptr(ct, C.c_int),
+            cell_off=_ptr(co, C.c_int64), cell_nodes=_ptr(cn, C.c_int), n_bfaces=bp.shape[0],
+            bface_off=_ptr(bo, C.c_int64), bface_nodes=_ptr(bn, C.c_int), bface_patch=_ptr(bp, C.c_int),
+            n_patches=len(mesh.patch_names),
+        )

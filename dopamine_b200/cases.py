@@ -1,0 +1,283 @@
+"""Meshes, initial conditions and run configurations for the RK3W hot path.
+
+The reference reads gmsh / OpenFOAM files and sets initial fields in Fortran
+(src/mesh/mod_gmsh_reader.f90, src/init/mod_initconditions.f90).  This module produces the same
+inputs directly as arrays: a gmsh-like raw mesh (nodes, volume elements, tagged boundary
+elements) and cell-centred initial fields.  It is host set-up code, outside the timed step.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import abi
+
+
+@dataclass
+class RawMesh:
+    xyz: np.ndarray            # (n_nodes, 3) float64
+    cell_type: np.ndarray      # (n_cells,) int32 gmsh codes
+    cell_off: np.ndarray       # (n_cells+1,) int64
+    cell_nodes: np.ndarray     # int32, 0-based
+    bface_off: np.ndarray      # (n_bfaces+1,) int64
+    bface_nodes: np.ndarray    # int32
+    bface_patch: np.ndarray    # (n_bfaces,) int32
+    patch_names: list = field(default_factory=list)
+
+    @property
+    def n_cells(self):
+        return int(self.cell_type.shape[0])
+
+    def vertex_bounds(self):
+        return self.xyz.min(axis=0), self.xyz.max(axis=0)
+
+
+def structured_box(X, Y, Z, names=("x0", "xL", "y0", "yL", "z0", "zL")):
+    """Hex box from node coordinate arrays X, Y, Z of shape (nx+1, ny+1, nz+1).
+
+    Node, element and boundary-quad numbering follow tests/regression/mk_box_mesh.py:
+    node id i + (nx+1)(j + (ny+1) k), hexes in k, j, i order, boundary quads per surface in the
+    order x0, xL, y0, yL, z0, zL.
+    """
+    nx, ny, nz = (s - 1 for s in X.shape)
+    xyz = np.stack([X.transpose(2, 1, 0).ravel(), Y.transpose(2, 1, 0).ravel(), Z.transpose(2, 1, 0).ravel()], axis=1)
+
+    def nid(i, j, k):
+        return i + (nx + 1) * (j + (ny + 1) * k)
+
+    k, j, i = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    i, j, k = i.ravel(), j.ravel(), k.ravel()
+    hexes = np.stack([nid(i, j, k), nid(i + 1, j, k), nid(i + 1, j + 1, k), nid(i, j + 1, k),
+                      nid(i, j, k + 1), nid(i + 1, j, k + 1), nid(i + 1, j + 1, k + 1), nid(i, j + 1, k + 1)], axis=1)
+    quads = []
+    patch = []
+
+    def surf(s, a_n, b_n, fn):
+        b, a = np.meshgrid(np.arange(b_n), np.arange(a_n), indexing="ij")
+        # mk_box_mesh loops "for a in range(N): for b in range(N)" -> a slowest
+        a, b = a.T.ravel(), b.T.ravel()
+        quads.append(fn(a, b))
+        patch.append(np.full(a.shape[0], s, dtype=np.int32))
+
+    surf(0, ny, nz, lambda a, b: np.stack([nid(0, a, b), nid(0, a + 1, b), nid(0, a + 1, b + 1), nid(0, a, b + 1)], 1))
+    surf(1, ny, nz, lambda a, b: np.stack([nid(nx, a, b), nid(nx, a + 1, b), nid(nx, a + 1, b + 1), nid(nx, a, b + 1)], 1))
+    surf(2, nx, nz, lambda a, b: np.stack([nid(a, 0, b), nid(a + 1, 0, b), nid(a + 1, 0, b + 1), nid(a, 0, b + 1)], 1))
+    surf(3, nx, nz, lambda a, b: np.stack([nid(a, ny, b), nid(a + 1, ny, b), nid(a + 1, ny, b + 1), nid(a, ny, b + 1)], 1))
+    surf(4, nx, ny, lambda a, b: np.stack([nid(a, b, 0), nid(a + 1, b, 0), nid(a + 1, b + 1, 0), nid(a, b + 1, 0)], 1))
+    surf(5, nx, ny, lambda a, b: np.stack([nid(a, b, nz), nid(a + 1, b, nz), nid(a + 1, b + 1, nz), nid(a, b + 1, nz)], 1))
+    q = np.concatenate(quads).astype(np.int32)
+    nh = hexes.shape[0]
+    return RawMesh(
+        xyz=np.ascontiguousarray(xyz, dtype=np.float64),
+        cell_type=np.full(nh, abi.EL_HEX8, dtype=np.int32),
+        cell_off=np.arange(0, 8 * nh + 1, 8, dtype=np.int64),
+        cell_nodes=hexes.astype(np.int32).ravel(),
+        bface_off=np.arange(0, 4 * q.shape[0] + 1, 4, dtype=np.int64),
+        bface_nodes=q.ravel(),
+        bface_patch=np.concatenate(patch),
+        patch_names=list(names),
+    )
+
+
+def uniform_box(nx, ny, nz, lx, ly, lz, names=("x0", "xL", "y0", "yL", "z0", "zL")):
+    x = np.arange(nx + 1) * (lx / nx)
+    y = np.arange(ny + 1) * (ly / ny)
+    z = np.arange(nz + 1) * (lz / nz)
+    X, Y, Z = np.meshgrid(x, y, z, indexing="ij")
+    return structured_box(X, Y, Z, names)
+
+
+def skewed_unit_box(n, amp):
+    """Curvilinear unit box of tests/regression/mk_box_mesh.py (N, AMP): nodes displaced by
+    AMP sin(pi X) sin(2 pi Y) sin(pi Z) cyclically; coordinates rounded to 16 significant digits
+    as the %.16g gmsh file carries them."""
+    X = np.empty((n + 1, n + 1, n + 1))
+    Y = np.empty_like(X)
+    Z = np.empty_like(X)
+    s, pi = math.sin, math.pi
+    for k in range(n + 1):
+        for j in range(n + 1):
+            for i in range(n + 1):
+                a, b, c = i / n, j / n, k / n
+                X[i, j, k] = float(f"{a + amp * s(pi * a) * s(2 * pi * b) * s(pi * c):.16g}")
+                Y[i, j, k] = float(f"{b + amp * s(pi * b) * s(2 * pi * c) * s(pi * a):.16g}")
+                Z[i, j, k] = float(f"{c + amp * s(pi * c) * s(2 * pi * a) * s(pi * b):.16g}")
+    return structured_box(X, Y, Z)
+
+
+def channel_box(nx, ny, nz, lx, ly, lz, stretch):
+    """Channel with walls at y = -ly/2, +ly/2 and tanh wall-normal clustering:
+    y_j = (ly/2) tanh(stretch (2 j/ny - 1)) / tanh(stretch)."""
+    x = np.arange(nx + 1) * (lx / nx)
+    eta = 2.0 * np.arange(ny + 1) / ny - 1.0
+    y = 0.5 * ly * np.tanh(stretch * eta) / math.tanh(stretch)
+    z = np.arange(nz + 1) * (lz / nz)
+    X, Y, Z = np.meshgrid(x, y, z, indexing="ij")
+    return structured_box(X, Y, Z, names=("x0", "xL", "bottom_wall", "top_wall", "z0", "zL"))
+
+
+# ------------------------------------------------------------------------------------------
+# Initial conditions (src/init/mod_initconditions.f90)
+# ------------------------------------------------------------------------------------------
+def taylor_green(centroid, lo, hi, u0=1.0):
+    """initialize_taylor_green_ic (mod_initconditions.f90:276-334)."""
+    L = hi - lo
+    L = np.where(L <= 0.0, 1.0, L)
+    k = 2.0 * math.pi / L
+    xl = np.mod(centroid - lo, L)
+    U = np.zeros_like(centroid)
+    U[:, 0] = u0 * np.sin(k[0] * xl[:, 0]) * np.cos(k[1] * xl[:, 1]) * np.cos(k[2] * xl[:, 2])
+    U[:, 1] = -u0 * np.cos(k[0] * xl[:, 0]) * np.sin(k[1] * xl[:, 1]) * np.cos(k[2] * xl[:, 2])
+    return U
+
+
+def channel_parabolic(centroid, lo, hi, uref, wall_dir=1, stream_dir=0):
+    """initialize_channel_profile_ic 'parabolic' (mod_initconditions.f90:114-196)."""
+    H = max(hi[wall_dir] - lo[wall_dir], 1e-30)
+    zeta = np.clip((centroid[:, wall_dir] - lo[wall_dir]) / H, 0.0, 1.0)
+    U = np.zeros_like(centroid)
+    U[:, stream_dir] = 4.0 * uref * zeta * (1.0 - zeta)
+    return U
+
+
+def splitmix64_uniform(n, seed):
+    """Seeded uniform draws in [0,1) from SplitMix64 (reproducible on any platform; the
+    reference's gfortran random_number stream is not)."""
+    out = np.empty(n, dtype=np.float64)
+    mask = (1 << 64) - 1
+    x = seed & mask
+    for i in range(n):
+        x = (x + 0x9E3779B97F4A7C15) & mask
+        z = x
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & mask
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & mask
+        z ^= z >> 31
+        out[i] = (z >> 11) * (1.0 / (1 << 53))
+    return out
+
+
+def multiplicative_noise(U, frac, seed):
+    """add_random_velocity_noise (mod_initconditions.f90:200-250): U_k *= 1 + frac (2 r - 1),
+    r drawn per cell and component in the reference's loop order (cell outer, component inner)."""
+    r = _fast_uniform(U.size, seed).reshape(U.shape)
+    return U * (1.0 + frac * (2.0 * r - 1.0))
+
+
+def _fast_uniform(n, seed):
+    # vectorised SplitMix64 (identical stream to splitmix64_uniform)
+    idx = np.arange(1, n + 1, dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        x = np.uint64(seed) + idx * np.uint64(0x9E3779B97F4A7C15)
+        z = (x ^ (x >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z = z ^ (z >> np.uint64(31))
+    return (z >> np.uint64(11)).astype(np.float64) * (1.0 / (1 << 53))
+
+
+# ------------------------------------------------------------------------------------------
+# Run configurations
+# ------------------------------------------------------------------------------------------
+@dataclass
+class Case:
+    name: str
+    mesh: RawMesh
+    patches: list            # dicts for abi.patch_cfgs, in mesh patch order
+    params: dict             # keyword arguments of abi.default_params
+    ic: str                  # 'taylor_green' | 'uniform' | 'channel'
+    ic_uref: float = 1.0
+    noise: float = 0.0
+    noise_seed: int = 12345
+    n_steps: int = 20
+    stats_every: int = 1
+    description: str = ""
+
+    def make_params(self):
+        return abi.default_params(**self.params)
+
+    def initial_velocity(self, centroid):
+        lo, hi = self.mesh.vertex_bounds()
+        if self.ic == "taylor_green":
+            U = taylor_green(centroid, lo, hi, self.ic_uref)
+        elif self.ic == "uniform":
+            U = np.zeros_like(centroid)
+            U[:, 0] = self.ic_uref
+        elif self.ic == "channel":
+            U = channel_parabolic(centroid, lo, hi, self.ic_uref)
+        else:
+            raise ValueError(self.ic)
+        if self.noise > 0.0:
+            U = multiplicative_noise(U, self.noise, self.noise_seed)
+        return U
+
+
+def _periodic6():
+    return [{"bc": "periodic"} for _ in range(6)]
+
+
+def regression_case(name):
+    """The reference's regression cases whose meshes need no gmsh
+    (tests/regression/cases/<name>/case.input)."""
+    if name == "tgv":
+        L = 6.283185307179586
+        return Case(name, uniform_box(32, 32, 32, L, L, L), _periodic6(),
+                    dict(scheme=abi.SCHEME_QUICK, nu=6.25e-4, dt=1.0e-2, cfl_max=0.6, p_tol=1e-10, rhie_chow_dual=0),
+                    "taylor_green", 1.0, n_steps=20)
+    if name == "tgv_skew":
+        return Case(name, skewed_unit_box(16, 0.08), _periodic6(),
+                    dict(scheme=abi.SCHEME_KEP, nu=6.25e-4, dt=2.0e-2, cfl_max=0.6, p_tol=1e-10,
+                         n_nonortho_corr=3, rhie_chow_dual=1),
+                    "taylor_green", 1.0, n_steps=30)
+    if name == "tgv_skew_chk":
+        return Case(name, skewed_unit_box(16, 0.08), _periodic6(),
+                    dict(scheme=abi.SCHEME_KEP, nu=6.25e-4, dt=2.0e-2, cfl_max=0.6, p_tol=1e-10,
+                         n_nonortho_corr=5, nonortho_check=1, rhie_chow_dual=1),
+                    "taylor_green", 1.0, n_steps=30)
+    if name in ("pdrop", "hydro"):
+        fz = 0.0 if name == "pdrop" else -1.0
+        patches = [{"bc": "periodic"}] * 4 + [{"bc": "outlet", "p": 1.0}, {"bc": "outlet", "p": 0.0}]
+        return Case(name, skewed_unit_box(12, 0.04), patches,
+                    dict(scheme=abi.SCHEME_CDS, nu=1.0e-2, dt=2.0e-3, cfl_max=0.5, p_tol=1e-12,
+                         n_nonortho_corr=4, rhie_chow_dual=0, f_const=(0.0, 0.0, fz)),
+                    "uniform", 0.0, n_steps=20, stats_every=10)
+    if name == "hydrowall":
+        patches = [{"bc": "noSlip"}] * 6
+        return Case(name, skewed_unit_box(12, 0.04), patches,
+                    dict(scheme=abi.SCHEME_CDS, nu=1.0e-2, dt=2.0e-3, cfl_max=0.5, p_tol=1e-12,
+                         n_nonortho_corr=4, rhie_chow_dual=0, f_const=(0.0, 0.0, -1.0)),
+                    "uniform", 0.0, n_steps=20, stats_every=10)
+    raise KeyError(name)
+
+
+REGRESSION_CASES = ("tgv", "tgv_skew", "tgv_skew_chk", "pdrop", "hydro", "hydrowall")
+
+
+def tgv_config(n=32, n_steps=200, scheme=abi.SCHEME_CDS):
+    """Taylor-Green vortex, periodic [0,2pi]^3 hex box, nu=1/1600, no SGS, CDS, dt=0.01,
+    Jacobi-PCG to rtol 1e-10 (first configuration)."""
+    L = 2.0 * math.pi
+    return Case(f"tgv{n}", uniform_box(n, n, n, L, L, L), _periodic6(),
+                dict(scheme=scheme, nu=1.0 / 1600.0, dt=0.01, cfl_max=0.6, p_tol=1e-10),
+                "taylor_green", 1.0, n_steps=n_steps,
+                description=f"Taylor-Green vortex {n}^3 periodic hex box, CDS, nu=1/1600, dt=0.01")
+
+
+def channel_config(nx=96, ny=64, nz=64, n_steps=1000, retau=395.0, noise_seed=20261203):
+    """Turbulent channel 2pi x 2 x pi, tanh stretching 2.0 in y, walls at y=+-1 (log-law wall
+    model), periodic x and z, Vreman SGS, KEP advection, constant streamwise pressure gradient
+    u_tau^2/delta = 1 with u_tau = 1, nu = u_tau delta / Re_tau; laminar parabola with seeded
+    +-10% multiplicative noise (second configuration)."""
+    mesh = channel_box(nx, ny, nz, 2.0 * math.pi, 2.0, math.pi, 2.0)
+    patches = [{"bc": "periodic"}, {"bc": "periodic"}, {"bc": "wallModel"}, {"bc": "wallModel"},
+               {"bc": "periodic"}, {"bc": "periodic"}]
+    nu = 1.0 / retau
+    # bulk velocity of the log-law profile at Re_tau 395 is about 17.5 u_tau; dt keeps CFL ~0.3
+    ub = 17.5
+    dx = 2.0 * math.pi / nx
+    dt = 0.3 * dx / (1.5 * ub)
+    return Case(f"channel{nx}x{ny}x{nz}", mesh, patches,
+                dict(scheme=abi.SCHEME_KEP, sgs_model=abi.SGS_VREMAN, wall_model=abi.WM_LOGLAW,
+                     nu=nu, dt=dt, cfl_max=0.5, p_tol=1e-8, f_const=(1.0, 0.0, 0.0)),
+                "channel", 1.5 * ub, noise=0.10, noise_seed=noise_seed, n_steps=n_steps,
+                description=f"channel {nx}x{ny}x{nz} Re_tau={retau:g}, KEP, Vreman, log-law wall model")

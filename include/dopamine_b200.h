@@ -1,0 +1,225 @@
+/*
+ * dopamine_b200 — C ABI of the sm_100a RK3W fractional-step hot path.
+ *
+ * Two groups of entry points:
+ *
+ *  1. fvm_petsc_*  — the pressure-solve seam the reference already has.  Same symbol names,
+ *     argument order and meaning as src/solver/pressure_backend_petsc.c (declared for Fortran in
+ *     src/solver/mod_pressure_solver.f90:23-74), implemented here with a device-resident
+ *     Jacobi-preconditioned conjugate gradient instead of PETSc/hypre.  A Fortran host that links
+ *     this library instead of pressure_backend_petsc.c needs no source change.
+ *
+ *  2. dpm_*        — the explicit part of the time step plus the whole-step driver, mirroring the
+ *     FVSolver interface (src/solver/mod_fv_solver.f90:270-285: init, advance, project_once,
+ *     compute_dt, to_device, sync_host, state_is_finite) and the per-operator Fortran
+ *     subroutines, so that one operator at a time can be swapped.
+ *
+ * Conventions: plain C types only; all arrays are host pointers unless a name says "_dev";
+ * cell vectors use the reference's Fortran layout (U(3,n): component fastest; grad(3,3,n):
+ * grad(i,j,c) = dU_j/dx_i, i fastest).  Indices are 0-based in dpm_* calls; fvm_petsc_* keeps
+ * the reference's 1-based indices.  Every call returns 0 on success or a negative status;
+ * nothing throws and nothing calls exit().  One host thread per handle; calls are ordered on
+ * the handle's CUDA stream.
+ */
+#ifndef DOPAMINE_B200_H
+#define DOPAMINE_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------------------------------- */
+/* Status codes                                                                              */
+/* ---------------------------------------------------------------------------------------- */
+#define DPM_OK 0
+#define DPM_ERR_ARG (-1)
+#define DPM_ERR_CUDA (-2)
+#define DPM_ERR_MESH (-3)
+#define DPM_ERR_NOT_FINITE (-4)
+#define DPM_ERR_DT_COLLAPSE (-5)
+#define DPM_ERR_UNSUPPORTED (-6)
+/* Krylov failure after the fallback retry: -(1000 + reason), reason < 0 as in PETSc. */
+
+/* Advection schemes (src/mod_parameters.f90:54-60). */
+#define DPM_SCHEME_VANLEER_TVD 1
+#define DPM_SCHEME_KOREN_TVD 2
+#define DPM_SCHEME_CDS 3
+#define DPM_SCHEME_KEP 4
+#define DPM_SCHEME_QUICK 5
+
+/* SGS closures (src/solver/mod_fv_solver.f90:1258-1278). */
+#define DPM_SGS_NONE 0
+#define DPM_SGS_VREMAN 1
+#define DPM_SGS_SMAGORINSKY 2
+#define DPM_SGS_AMD 3
+
+/* Wall models (src/abl/mod_abl_types.f90 WM_*): log law (Reichardt) or none. */
+#define DPM_WM_LOGLAW 0
+#define DPM_WM_NONE 1
+
+/* Pressure-solve forms. */
+#define DPM_FORM_FP64 0     /* plain: FP64 Jacobi-PCG                                    */
+#define DPM_FORM_MIXED 1    /* FP32 inner PCG inside FP64 defect correction              */
+
+/* Raw mesh, as a gmsh v4 file holds it (src/mesh/mod_gmsh_reader.f90:build_mesh_from_gmsh). */
+typedef struct dpm_raw_mesh {
+  int64_t n_nodes;
+  const double* xyz;          /* [n_nodes][3]                                                */
+  int64_t n_cells;
+  const int* cell_type;       /* gmsh codes: 4 tet, 5 hex, 6 prism, 7 pyramid                */
+  const int64_t* cell_off;    /* [n_cells+1]                                                 */
+  const int* cell_nodes;      /* 0-based node ids, gmsh local ordering                       */
+  int64_t n_bfaces;
+  const int64_t* bface_off;   /* [n_bfaces+1]                                                */
+  const int* bface_nodes;
+  const int* bface_patch;     /* [n_bfaces] patch index 0..n_patches-1                       */
+  int n_patches;
+} dpm_raw_mesh_t;
+
+/* Per-patch boundary configuration (src/bc/mod_bc.f90:BCConfig). */
+typedef struct dpm_patch_cfg {
+  int bc_id;                  /* BC_* id (src/mod_parameters.f90:41-51)                      */
+  double U_val[3];            /* inlet / moving-wall velocity                                */
+  double p_val;               /* outlet pressure                                             */
+  double T_val;               /* fixed temperature                                           */
+  int scalar_mode[4];         /* per passive scalar: 0 zero-gradient, 1 Dirichlet            */
+  double scalar_value[4];
+} dpm_patch_cfg_t;
+
+/* Solver parameters (src/solver/mod_fv_solver.f90:solver_params_t), numerics pinned as the
+ * reference's regression inputs pin them. */
+typedef struct dpm_params {
+  double nu;                  /* molecular kinematic viscosity                               */
+  double dt;                  /* requested time step (clamped to the CFL limit)              */
+  double cfl_max;
+  double p_tol;               /* Poisson relative tolerance                                  */
+  int p_max_iter;
+  int scheme;                 /* DPM_SCHEME_* for momentum                                   */
+  int sgs_model;              /* DPM_SGS_*                                                   */
+  int wall_model;             /* DPM_WM_*                                                    */
+  int n_nonortho_corr;        /* Jasak correctors per stage (>= 1)                           */
+  int rhie_chow_dual;
+  int nonortho_check;
+  int use_rotational_projection;
+  int adapt_dt;
+  double pressure_min_cos_theta;
+  double f_const[3];          /* constant body force                                         */
+  double g[3];                /* gravity, Boussinesq only                                    */
+  int boussinesq;
+  double beta, T_ref, alpha_T, Pr_t;
+  int temperature_scheme;
+  int n_scalars;              /* passive scalars, <= 4                                       */
+  int scalar_scheme;
+  double scalar_diffusivity[4];
+  double scalar_pr_t[4];
+  double c_amd;
+  int amd_wall_gradient;
+  double wall_model_height, wall_model_filter_time, wall_model_filter_tf_fac;
+  int form;                   /* DPM_FORM_*                                                  */
+} dpm_params_t;
+
+/* Per-step integral statistics (src/stats/mod_stats.f90:compute_stats_sums and
+ * src/solver/mod_fv_solver.f90:solver_divergence_metrics). */
+typedef struct dpm_stats {
+  double time, E, eps, Umax, Ub, tauw_mean, nu_sgs_mean;
+  double max_abs_divU, volavg_abs_divU;
+  double dt_used;
+  int p_solves, p_iters;
+  double p_resid_max;
+} dpm_stats_t;
+
+/* ---------------------------------------------------------------------------------------- */
+/* 1. Pressure-solve seam (src/solver/pressure_backend_petsc.c)                              */
+/* ---------------------------------------------------------------------------------------- */
+/* src/solver/mod_pressure_solver.f90:25 — 1 when the backend can be used. */
+int fvm_petsc_backend_available(void);
+/* src/solver/mod_pressure_solver.f90:29 — creates the CUDA context and stream. */
+int fvm_petsc_backend_initialize(void);
+/* src/solver/mod_pressure_solver.f90:33 — releases the cached operator and device memory. */
+int fvm_petsc_backend_finalize(void);
+/* src/solver/mod_pressure_solver.f90:37 — "boomeramg" / "gamg" are accepted and mapped to the
+ * Jacobi PCG; "jacobi" / "pcg" select it explicitly. */
+void fvm_petsc_set_pressure_solver(const char* solver_name);
+/* src/solver/mod_pressure_solver.f90:42 — 1: rhs/solution may be device pointers. */
+int fvm_petsc_device_io_supported(void);
+/* src/solver/mod_pressure_solver.f90:47 */
+void fvm_petsc_set_io_on_device(int on);
+/* src/solver/mod_pressure_solver.f90:52 — PETSc option strings; "-pc_type jacobi",
+ * "-ksp_max_it N", "-ksp_rtol X" are honoured, others ignored. */
+void fvm_petsc_insert_option(const char* opt);
+/* src/solver/mod_device.f90:119-126 — device binding of the calling rank. */
+void fvm_petsc_set_device_local_rank(int local_rank);
+/* src/solver/pressure_backend_petsc.c:648-668 (Fortran interface mod_pressure_solver.f90:60-73).
+ * Solves A x = rhs, A = diag - sum_f coeff_f (off-diagonal), with conjugate gradients on the
+ * unpreconditioned residual norm, ||r|| <= max(rtol ||b||, atol), nonzero initial guess
+ * (solution on entry), constant null space when no Dirichlet rows exist.  Indices 1-based. */
+int fvm_petsc_solve_pressure(int n_cells_local, int n_cells_global, int n_faces,
+                             const int* local_to_global, const int* face_owner,
+                             const int* face_neighbor_local, const int* face_neighbor_global,
+                             const int* skip_face, const double* diagonal, const double* rhs,
+                             const double* face_coeff, int reference_cell, int max_iterations,
+                             double rtol, double atol, const int* dirichlet_rows,
+                             const double* dirichlet_values, int n_dirichlet_rows,
+                             double* solution, int* iteration_count, double* residual_norm);
+
+/* ---------------------------------------------------------------------------------------- */
+/* 2. Whole-step solver handle (src/solver/mod_fv_solver.f90 FVSolver)                       */
+/* ---------------------------------------------------------------------------------------- */
+typedef struct dpm_solver dpm_solver_t;
+
+/* Mesh set-up and solver_init (mod_fv_solver.f90:302-508): builds geometry, periodic pairs,
+ * LS stencils and the static projection operators on the host, uploads them to HBM. */
+int dpm_create(const dpm_raw_mesh_t* mesh, const dpm_patch_cfg_t* patches, const dpm_params_t* params,
+               int device, dpm_solver_t** out);
+int dpm_destroy(dpm_solver_t* s);
+int dpm_n_cells(const dpm_solver_t* s, int64_t* n_cells, int64_t* n_faces, int64_t* n_bnd_faces);
+/* solver_to_device (mod_fv_solver.f90:3286): U(3,nc), p(nc), T(nc) may be NULL. */
+int dpm_upload_state(dpm_solver_t* s, const double* U, const double* p, const double* T);
+/* solver_sync_host (mod_fv_solver.f90:3326): any output pointer may be NULL. */
+int dpm_download_state(dpm_solver_t* s, double* U, double* p, double* T, double* nu_sgs);
+/* Fields that only the projection produces: face flux (n_faces) and the cell pressure gradient. */
+int dpm_download_face_flux(dpm_solver_t* s, double* face_flux);
+/* solver_project_once (mod_fv_solver.f90:837-918). */
+int dpm_project_once(dpm_solver_t* s, double dt);
+/* solver_advance (mod_fv_solver.f90:920-958): CFL clamp of a fixed dt, RK3W, time += dt.
+ * Status DPM_ERR_DT_COLLAPSE mirrors solver_compute_dt's stop. */
+int dpm_advance(dpm_solver_t* s, double dt);
+/* n steps in one call, captured as a CUDA graph after the first; stats of the last step. */
+int dpm_advance_n(dpm_solver_t* s, double dt, int n_steps);
+int dpm_stats(dpm_solver_t* s, dpm_stats_t* out);
+/* solver_state_is_finite (mod_fv_solver.f90:3925-3945): *ok = 1 when U and p are finite. */
+int dpm_state_is_finite(dpm_solver_t* s, int* ok);
+/* solver_compute_dt (mod_fv_solver.f90:3872-3899). */
+int dpm_compute_dt(dpm_solver_t* s, double* dt);
+int dpm_get_time(const dpm_solver_t* s, double* time);
+int dpm_set_time(dpm_solver_t* s, double time);
+/* Device time of the last dpm_advance*/ /* in ms: total and Poisson part. */
+int dpm_last_timing(const dpm_solver_t* s, double* step_ms, double* poisson_ms);
+/* Kernel launch count since the handle was created (own kernels only). */
+int dpm_kernel_launches(const dpm_solver_t* s, int64_t* n);
+
+/* ---------------------------------------------------------------------------------------- */
+/* 3. Per-operator entry points: same arguments as the Fortran subroutines, operating on the */
+/*    handle's mesh.  Host arrays in, host arrays out, so a single operator can be compared   */
+/*    or swapped in.                                                                          */
+/* ---------------------------------------------------------------------------------------- */
+/* ls_gradient_vector (src/numerics/mod_gradient.f90:425): grad_U(3,3,nc) from U(3,nc), U_bnd(3,nbnd). */
+int dpm_ls_gradient_vector(dpm_solver_t* s, const double* U, const double* U_bnd, double* grad_U);
+/* advection_rhs_vector (src/numerics/mod_advection.f90:679) with face_flux(n_faces). */
+int dpm_advection_rhs_vector(dpm_solver_t* s, int scheme, const double* U, const double* U_bnd,
+                             const double* face_flux, const double* grad_U, double* rhs);
+/* viscous_rhs_vector (src/numerics/mod_viscous.f90:37). */
+int dpm_viscous_rhs_vector(dpm_solver_t* s, const double* U, double nu, const double* nu_sgs,
+                           const double* grad_U, const double* U_bnd, double* rhs);
+/* vreman_sgs_viscosity / smagorinsky_sgs / amd_sgs_viscosity (src/sgs/): nu_sgs(nc). */
+int dpm_sgs_viscosity(dpm_solver_t* s, int model, const double* U, const double* U_bnd,
+                      const double* grad_U, double dt_stab, double* nu_sgs);
+/* apply_wall_model_bc (src/sgs/mod_wall_model.f90:176): tau_w(3,nbnd). */
+int dpm_wall_model(dpm_solver_t* s, const double* U, double nu, double* tau_w);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DOPAMINE_B200_H */

@@ -1,0 +1,1894 @@
+// ORACLE — test infrastructure only.  A CPU restatement of the reference's RK3W fractional-step
+// time step (AkshayPatil1994/dopamine, Fortran) used as the parity checker for the sm_100a
+// product path and as the timed CPU baseline.  Nothing in the product links, imports or
+// executes this file.  Every routine cites the reference routine it follows; face loops run in
+// the reference's face order and accumulate in the same sequence, and the Poisson solve follows
+// PETSc's KSPCG (unpreconditioned residual norm, nonzero initial guess, constant null space,
+// Jacobi preconditioner) as configured in src/solver/pressure_backend_petsc.c:381-463.
+//
+// Pinning: checked against the reference's regression CSVs (tests/regression/reference/*.csv)
+// for the cases whose meshes can be regenerated without gmsh; see tests/test_oracle_golden.py.
+//
+// Mesh geometry, periodic pairing and LS stencils come from the shared host set-up
+// (dopamine_b200/csrc/host/mesh.cpp), the restatement of src/mesh/mod_mesh.f90 set-up.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../dopamine_b200/csrc/host/mesh.hpp"
+#include "../include/dopamine_b200.h"
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace orc {
+using namespace dpm;
+
+constexpr double KAPPA = 0.41;                  // src/mod_parameters.f90:14
+constexpr double BLOG = 5.2;                    // src/mod_parameters.f90:17
+constexpr double C_VREMAN = 0.025;              // src/mod_parameters.f90:20
+constexpr double NU_SGS_STAB_FRAC = 0.4;        // src/sgs/mod_vreman.f90:34
+constexpr double NONORTHO_SIN2_TOL = 1.0e-10;   // src/numerics/mod_nonortho.f90:7
+constexpr double NONORTHO_PHI_TOL = 1.0e-3;     // src/solver/mod_fv_solver.f90:116
+constexpr double AMD_ALPHA_SQ_MIN = 1.0e-20;    // src/sgs/mod_amd.f90:18
+constexpr double AMD_ROUNDOFF_FRAC = 1.0e-12;   // src/sgs/mod_amd.f90:22
+const double RK3W_ALPHA[3] = {8.0 / 15.0, 5.0 / 12.0, 3.0 / 4.0};   // src/mod_parameters.f90:64
+const double RK3W_BETA[3] = {0.0, -17.0 / 60.0, -5.0 / 12.0};
+const double RK3W_GAMMA[3] = {8.0 / 15.0, 2.0 / 15.0, 1.0 / 3.0};
+const double RK3W_C[3] = {0.0, 8.0 / 15.0, 2.0 / 3.0};
+
+inline double dot3(const double* a, const double* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+inline bool finite(double x) { return std::fabs(x) <= 1.79769313486231570e308; }
+inline bool is_wall(int bc) {
+  return bc == BC_WALL_NOSLIP || bc == BC_WALL_MODEL || bc == BC_WALL_VELOCITY || bc == BC_SLIP || bc == BC_SYMMETRY;
+}
+
+// src/numerics/mod_nonortho.f90:65-99
+void kfactor_limited(const double* sf, const double* d_on, double min_cos, double* k) {
+  double len = std::sqrt(d_on[0] * d_on[0] + d_on[1] * d_on[1] + d_on[2] * d_on[2]);
+  if (len < 1.0e-30) { k[0] = k[1] = k[2] = 0.0; return; }
+  double inv = 1.0 / len;
+  double sdd = dot3(sf, d_on) * inv;
+  double d_len = sdd * len;
+  double sf_sq = sf[0] * sf[0] + sf[1] * sf[1] + sf[2] * sf[2];
+  if (min_cos > 0.0) d_len = std::max(d_len, min_cos * std::sqrt(sf_sq) * len);
+  if (d_len > 1.0e-30) {
+    for (int i = 0; i < 3; ++i) k[i] = sf[i] - (sf_sq / d_len) * d_on[i];
+  } else {
+    for (int i = 0; i < 3; ++i) k[i] = sf[i] - (sdd * inv) * d_on[i];
+  }
+}
+
+// src/sgs/mod_wall_model.f90:50-64
+void reichardt_uplus(double yp, double c_buf, double& up, double& dup) {
+  const double A1 = 11.0, A2 = 0.33, A1I = 1.0 / A1;
+  double e1 = std::exp(-yp * A1I), e2 = std::exp(-A2 * yp);
+  up = std::log(1.0 + KAPPA * yp) / KAPPA + c_buf * (1.0 - e1 - yp * A1I * e2);
+  dup = 1.0 / (1.0 + KAPPA * yp) + c_buf * (A1I * e1 - A1I * e2 + yp * A1I * A2 * e2);
+}
+
+// src/sgs/mod_wall_model.f90:67-114
+void wall_stress_newton(double u_par, double y_w, double nu, double& u_tau, double& tau_mag, bool& capped) {
+  const double C_BUF = BLOG - std::log(KAPPA) / KAPPA;
+  capped = false;
+  if (u_par <= SMALL || y_w <= SMALL) { u_tau = 0.0; tau_mag = 0.0; return; }
+  u_tau = std::max(0.01 * u_par, std::sqrt(nu * u_par / (y_w + SMALL)));
+  double inv_nu = 1.0 / (nu + SMALL), ywn = y_w * inv_nu;
+  for (int it = 0; it < 50; ++it) {
+    double yp = u_tau * ywn, up, dup;
+    reichardt_uplus(yp, C_BUF, up, dup);
+    double f = u_par / (u_tau + SMALL) - up;
+    double df = -u_par / (u_tau * u_tau + SMALL) - dup * ywn;
+    double s = df >= 0.0 ? SMALL : -SMALL;
+    double un = u_tau - f / (df + s);
+    un = std::min(std::max(un, 0.1 * u_tau), 10.0 * u_tau);
+    if (std::fabs(un - u_tau) < 1.0e-8 * un) { u_tau = un; break; }
+    u_tau = un;
+  }
+  capped = (u_tau * ywn < 1.0);
+  tau_mag = u_tau * u_tau;
+}
+
+// src/sgs/mod_amd.f90:31-66
+double amd_point(const double* a, const double* G, double c_amd) {
+  // a, G column-major 3x3: a[i + 3j] = alpha(i+1, j+1)
+  double asq = 0.0;
+  for (int j = 0; j < 3; ++j)
+    for (int i = 0; i < 3; ++i) asq += a[i + 3 * j] * a[i + 3 * j];
+  double num = 0.0;
+  for (int n = 0; n < 3; ++n)
+    for (int mm = 0; mm < 3; ++mm) {
+      double beta = 0.0;
+      for (int j = 0; j < 3; ++j)
+        for (int i = 0; i < 3; ++i) beta += G[i + 3 * j] * a[i + 3 * mm] * a[j + 3 * n];
+      num -= beta * a[mm + 3 * n];
+    }
+  double trg = G[0] + G[4] + G[8];
+  if (asq > AMD_ALPHA_SQ_MIN && num > AMD_ROUNDOFF_FRAC * trg * asq * std::sqrt(asq)) return c_amd * num / asq;
+  return 0.0;
+}
+
+double det3(const double* A) {  // column-major
+  auto a = [&](int i, int j) { return A[(i - 1) + 3 * (j - 1)]; };
+  return a(1, 1) * (a(2, 2) * a(3, 3) - a(2, 3) * a(3, 2)) - a(1, 2) * (a(2, 1) * a(3, 3) - a(2, 3) * a(3, 1)) +
+         a(1, 3) * (a(2, 1) * a(3, 2) - a(2, 2) * a(3, 1));
+}
+
+struct Solver {
+  Mesh m;
+  dpm_params_t P{};
+  std::vector<dpm_patch_cfg_t> pc;
+  int64_t nc = 0, nf = 0, nfi = 0, nb = 0;
+  int nthreads = 1;
+
+  // primary fields (AoS, Fortran layout)
+  std::vector<double> U, p, p_old, T, nu_sgs, U_bnd, p_bnd, phi_prev, phi_prev_bnd, tau_w;
+  std::vector<double> grad_U, face_flux, U_face, inv_vol;
+  std::vector<double> H_U, H_U0, rhs_p, conv_U, visc_U, gp, gp_rc, gp_cell, p_tot, p_tot_bnd, phi_it, Tinv;
+  std::vector<uint8_t> built;
+  bool u_face_ready = false;
+  double time = 0.0;
+  int64_t step = 0;
+
+  // patch classification (mod_fv_solver.f90:build_patch_classification)
+  std::vector<int64_t> per_bf, nper_bf;
+  int64_t n_outlet = 0;
+  double V_min = 0, V_total = 0, p_atol_factor = 1.0e-15;
+  bool diag_interface = false;
+
+  // pressure-solver face list (mod_pressure_solver.f90:pressure_solver_init)
+  int64_t nfp = 0;
+  std::vector<int> ps_owner, ps_nb, ps_mesh;
+  std::vector<uint8_t> ps_skip;
+  std::vector<double> ps_coeff, ps_diag;
+  std::vector<int> dir_rows;
+  std::vector<double> dir_vals;
+  // CSR of the assembled matrix, columns sorted (as PETSc AIJ stores them)
+  std::vector<int64_t> A_off;
+  std::vector<int> A_col;
+  std::vector<double> A_val;
+
+  // non-orthogonal caches (mod_fv_solver.f90:detect_nonortho_skip, build_nonortho_cache)
+  bool skip_nonortho = false, skip_grad_p = false;
+  std::vector<double> k_int, k_bnd;
+  std::vector<uint8_t> act_int, act_bnd;
+
+  // SGS filter tensor and wall-model sampling
+  std::vector<double> Gf;
+  std::vector<double> y_w;
+  std::vector<int> sample_cell;
+  std::vector<double> u_par_filt;
+  bool filt_ready = false;
+
+  // last-step diagnostics
+  int last_solves = 0, last_iters = 0;
+  double last_resid = 0.0, last_dt = 0.0;
+
+  int bc_of_face(int64_t f) const { return m.patch[f] >= 0 ? pc[m.patch[f]].bc_id : BC_ZEROGRADIENT; }
+
+  // ------------------------------------------------------------------------------------------
+  int init(const dpm_raw_mesh_t* raw, const dpm_patch_cfg_t* patches, const dpm_params_t* prm, std::string* err) {
+    RawMesh r;
+    r.n_nodes = raw->n_nodes; r.xyz = raw->xyz; r.n_cells = raw->n_cells; r.cell_type = raw->cell_type;
+    r.cell_off = raw->cell_off; r.cell_nodes = raw->cell_nodes; r.n_bfaces = raw->n_bfaces;
+    r.bface_off = raw->bface_off; r.bface_nodes = raw->bface_nodes; r.bface_patch = raw->bface_patch;
+    r.n_patches = raw->n_patches;
+    std::vector<int> pbc(raw->n_patches);
+    for (int i = 0; i < raw->n_patches; ++i) pbc[i] = patches[i].bc_id;
+    int rc = build_mesh(r, pbc.data(), m, err);
+    if (rc) return rc;
+    P = *prm;
+    pc.assign(patches, patches + raw->n_patches);
+    nc = m.n_cells; nf = m.n_faces; nfi = m.n_int_faces; nb = m.n_bnd_faces;
+    U.assign(3 * nc, 0.0); p.assign(nc, 0.0); p_old.assign(nc, 0.0); T.assign(nc, P.T_ref);
+    nu_sgs.assign(nc, 0.0); U_bnd.assign(3 * nb, 0.0); p_bnd.assign(nb, 0.0);
+    phi_prev.assign(nc, 0.0); phi_prev_bnd.assign(nb, 0.0); tau_w.assign(3 * nb, 0.0);
+    grad_U.assign(9 * nc, 0.0); face_flux.assign(nf, 0.0); U_face.assign(nf, 0.0);
+    inv_vol.resize(nc);
+    for (int64_t c = 0; c < nc; ++c) inv_vol[c] = 1.0 / std::max(m.volume[c], SMALL);
+    H_U.assign(3 * nc, 0.0); H_U0.assign(3 * nc, 0.0); rhs_p.assign(nc, 0.0);
+    conv_U.assign(3 * nc, 0.0); visc_U.assign(3 * nc, 0.0); gp.assign(3 * nc, 0.0); gp_rc.assign(3 * nc, 0.0);
+    gp_cell.assign(3 * nc, 0.0); p_tot.assign(nc, 0.0); p_tot_bnd.assign(nb, 0.0); phi_it.assign(nc, 0.0);
+    built.assign(nf, 0);
+    Tinv.assign(9 * nc, 0.0);
+    for (int64_t c = 0; c < nc; ++c) Tinv[9 * c] = Tinv[9 * c + 4] = Tinv[9 * c + 8] = 1.0;
+    // build_patch_classification
+    for (int q = 0; q < m.n_patches; ++q)
+      for (int64_t f = 0; f < m.patch_nfaces[q]; ++f)
+        (pc[q].bc_id == BC_PERIODIC ? per_bf : nper_bf).push_back(m.patch_start[q] + f);
+    n_outlet = 0;
+    for (int q = 0; q < m.n_patches; ++q)
+      if (pc[q].bc_id == BC_OUTLET) n_outlet += m.patch_nfaces[q];
+    apply_velocity_bc(-1, false);
+    apply_pressure_bc(p.data(), -1, false, false);
+    // initialize_velocity_from_bc
+    double u0[3] = {0, 0, 0};
+    for (int q = 0; q < m.n_patches; ++q)
+      if (pc[q].bc_id == BC_INLET) { for (int k = 0; k < 3; ++k) u0[k] = pc[q].U_val[k]; break; }
+    for (int64_t c = 0; c < nc; ++c)
+      for (int k = 0; k < 3; ++k) U[3 * c + k] = u0[k];
+    pressure_solver_init();
+    V_min = 1e300; V_total = 0.0;
+    for (int64_t c = 0; c < nc; ++c) { V_min = std::min(V_min, m.volume[c]); V_total += m.volume[c]; }
+    p_atol_factor = 1.0e-15;
+    detect_nonortho_skip();
+    build_nonortho_cache();
+    build_reconstruct_operator();
+    diag_interface = false;
+    for (int64_t f = 0; f < nfi; ++f)
+      if (m.is_refine[f]) { diag_interface = true; break; }
+    build_filter_tensor();
+    return 0;
+  }
+
+  // src/solver/mod_pressure_solver.f90:100-452
+  void pressure_solver_init() {
+    int64_t n_per_edges = 0;
+    auto per_nb = [&](int64_t f_bnd) -> int {
+      int pb = m.periodic_pair[f_bnd];
+      return pb >= 0 ? m.owner[nfi + pb] : -1;
+    };
+    for (int q = 0; q < m.n_patches; ++q) {
+      if (pc[q].bc_id != BC_PERIODIC) continue;
+      for (int64_t fl = 0; fl < m.patch_nfaces[q]; ++fl) {
+        int64_t fb = m.patch_start[q] + fl;
+        int nbc = per_nb(fb);
+        int o = m.owner[nfi + fb];
+        if (nbc < 0 || o == nbc || o >= nbc) continue;
+        n_per_edges++;
+      }
+    }
+    nfp = nfi + n_per_edges;
+    ps_owner.assign(nfp, -1); ps_nb.assign(nfp, -1); ps_mesh.assign(nfp, -1);
+    ps_skip.assign(nfp, 0); ps_coeff.assign(nfp, 0.0); ps_diag.assign(nc, 0.0);
+    for (int64_t i = 0; i < nfi; ++i) { ps_owner[i] = m.owner[i]; ps_mesh[i] = (int)i; ps_nb[i] = m.neighbour[i]; }
+    int64_t idx = nfi;
+    for (int q = 0; q < m.n_patches; ++q) {
+      if (pc[q].bc_id != BC_PERIODIC) continue;
+      for (int64_t fl = 0; fl < m.patch_nfaces[q]; ++fl) {
+        int64_t fb = m.patch_start[q] + fl, fg = nfi + fb;
+        int nbc = per_nb(fb);
+        int o = m.owner[fg];
+        if (nbc < 0 || o == nbc || o >= nbc) continue;
+        ps_owner[idx] = o; ps_mesh[idx] = (int)fg; ps_nb[idx] = nbc;
+        int pbd = m.periodic_pair[fb];
+        double pair_dcf = m.periodic_pair_dcf[fb];
+        int64_t pf = pbd >= 0 ? nfi + pbd : -1;
+        if (pair_dcf <= SMALL && pf >= 0) pair_dcf = m.d_cf[pf];
+        if (pair_dcf <= SMALL) pair_dcf = m.d_cf[fg];
+        double d_per = m.d_cf[fg] + pair_dcf;
+        double area_f = m.area[fg];
+        if (pf >= 0) area_f = 0.5 * (area_f + m.area[pf]);
+        double coeff = area_f / (d_per + SMALL);
+        ps_coeff[idx] = coeff;
+        ps_diag[o] += coeff;
+        ps_diag[nbc] += coeff;
+        idx++;
+      }
+    }
+    double cos_floor = P.pressure_min_cos_theta;
+    for (int64_t i = 0; i < nfi; ++i) {
+      int o = m.owner[i], n = m.neighbour[i];
+      double d[3];
+      for (int k = 0; k < 3; ++k) d[k] = m.centroid[3 * n + k] - m.centroid[3 * o + k];
+      double d_ortho = dot3(d, &m.normal[3 * i]);
+      if (cos_floor > 0.0 && d_ortho < cos_floor * m.d_cf[i]) d_ortho = cos_floor * m.d_cf[i];
+      double coeff = d_ortho > SMALL ? m.area[i] / d_ortho : m.area[i] / (m.d_cf[i] + SMALL);
+      if (!finite(coeff) || coeff <= SMALL) { ps_skip[i] = 1; continue; }
+      ps_coeff[i] = coeff;
+      ps_diag[o] += coeff;
+      ps_diag[n] += coeff;
+    }
+    dir_rows.clear(); dir_vals.clear();
+    for (int q = 0; q < m.n_patches; ++q) {
+      if (pc[q].bc_id != BC_OUTLET) continue;
+      for (int64_t fl = 0; fl < m.patch_nfaces[q]; ++fl) {
+        int64_t fg = nfi + m.patch_start[q] + fl;
+        int o = m.owner[fg];
+        double d[3];
+        for (int k = 0; k < 3; ++k) d[k] = m.centre[3 * fg + k] - m.centroid[3 * o + k];
+        double dpb = std::fabs(dot3(d, &m.normal[3 * fg]));
+        if (dpb <= SMALL) dpb = m.d_cf[fg];
+        if (cos_floor > 0.0) dpb = std::max(dpb, cos_floor * m.d_cf[fg]);
+        if (dpb <= SMALL) continue;
+        double cb = m.area[fg] / dpb;
+        if (!finite(cb) || cb <= SMALL) continue;
+        ps_diag[o] += cb;
+        dir_rows.push_back(o);
+        dir_vals.push_back(cb * pc[q].p_val);
+      }
+    }
+    for (int64_t c = 0; c < nc; ++c)
+      if (!finite(ps_diag[c]) || ps_diag[c] <= SMALL) ps_diag[c] = 1.0;
+    // Assemble the AIJ matrix (pressure_backend_petsc.c:330-360): diag, -coeff off-diagonals.
+    std::vector<std::vector<std::pair<int, double>>> rows(nc);
+    for (int64_t c = 0; c < nc; ++c) rows[c].push_back({(int)c, ps_diag[c]});
+    for (int64_t i = 0; i < nfp; ++i) {
+      if (ps_skip[i] || ps_coeff[i] == 0.0) continue;
+      rows[ps_owner[i]].push_back({ps_nb[i], -ps_coeff[i]});
+      rows[ps_nb[i]].push_back({ps_owner[i], -ps_coeff[i]});
+    }
+    A_off.assign(nc + 1, 0);
+    A_col.clear(); A_val.clear();
+    for (int64_t c = 0; c < nc; ++c) {
+      auto& r = rows[c];
+      std::stable_sort(r.begin(), r.end(), [](auto& a, auto& b) { return a.first < b.first; });
+      for (size_t j = 0; j < r.size(); ++j) {
+        if (!A_col.empty() && (int64_t)A_col.size() > A_off[c] && A_col.back() == r[j].first) {
+          A_val.back() += r[j].second;  // ADD_VALUES on a repeated entry
+        } else {
+          A_col.push_back(r[j].first);
+          A_val.push_back(r[j].second);
+        }
+      }
+      A_off[c + 1] = (int64_t)A_col.size();
+    }
+  }
+
+  // src/solver/mod_fv_solver.f90:1864-1941
+  void detect_nonortho_skip() {
+    int64_t n_active = 0, n_gradbc = 0;
+    for (int64_t i = 0; i < nfp; ++i) {
+      if (ps_skip[i]) continue;
+      int o = ps_owner[i], n = ps_nb[i];
+      int64_t fm = ps_mesh[i];
+      double d[3], k[3];
+      for (int j = 0; j < 3; ++j) d[j] = m.centroid[3 * n + j] - m.centroid[3 * o + j];
+      kfactor_limited(&m.sf[3 * fm], d, P.pressure_min_cos_theta, k);
+      if (dot3(k, k) >= NONORTHO_SIN2_TOL * dot3(&m.sf[3 * fm], &m.sf[3 * fm])) n_active++;
+    }
+    for (int64_t fb : nper_bf) {
+      int64_t fg = nfi + fb;
+      if (bc_of_face(fg) != BC_OUTLET) continue;
+      int o = m.owner[fg];
+      double d[3], k[3];
+      for (int j = 0; j < 3; ++j) d[j] = m.centre[3 * fg + j] - m.centroid[3 * o + j];
+      kfactor_limited(&m.sf[3 * fg], d, P.pressure_min_cos_theta, k);
+      if (dot3(k, k) >= NONORTHO_SIN2_TOL * dot3(&m.sf[3 * fg], &m.sf[3 * fg])) n_active++;
+    }
+    for (int q = 0; q < m.n_patches; ++q) {
+      int b = pc[q].bc_id;
+      if (!(b == BC_OUTLET || b == BC_PERIODIC || b == BC_WALL_NOSLIP || b == BC_WALL_VELOCITY ||
+            b == BC_WALL_MODEL || b == BC_SLIP || b == BC_SYMMETRY))
+        n_gradbc++;
+    }
+    skip_nonortho = (n_active == 0);
+    skip_grad_p = skip_nonortho && (n_gradbc == 0);
+    if (P.n_nonortho_corr <= 0) P.n_nonortho_corr = skip_nonortho ? 1 : 2;
+  }
+
+  // src/solver/mod_fv_solver.f90:1943-1997
+  void build_nonortho_cache() {
+    k_int.assign(3 * nfp, 0.0); act_int.assign(nfp, 0);
+    k_bnd.assign(3 * nper_bf.size(), 0.0); act_bnd.assign(nper_bf.size(), 0);
+    if (skip_nonortho) return;
+    for (int64_t i = 0; i < nfp; ++i) {
+      if (ps_skip[i]) continue;
+      int o = ps_owner[i], n = ps_nb[i];
+      int64_t fm = ps_mesh[i];
+      double d[3], k[3];
+      for (int j = 0; j < 3; ++j) d[j] = m.centroid[3 * n + j] - m.centroid[3 * o + j];
+      kfactor_limited(&m.sf[3 * fm], d, P.pressure_min_cos_theta, k);
+      if (dot3(k, k) >= NONORTHO_SIN2_TOL * dot3(&m.sf[3 * fm], &m.sf[3 * fm])) {
+        for (int j = 0; j < 3; ++j) k_int[3 * i + j] = k[j];
+        act_int[i] = 1;
+      }
+    }
+    for (size_t ib = 0; ib < nper_bf.size(); ++ib) {
+      int64_t fg = nfi + nper_bf[ib];
+      if (bc_of_face(fg) != BC_OUTLET) continue;
+      int o = m.owner[fg];
+      double d[3], k[3];
+      for (int j = 0; j < 3; ++j) d[j] = m.centre[3 * fg + j] - m.centroid[3 * o + j];
+      kfactor_limited(&m.sf[3 * fg], d, P.pressure_min_cos_theta, k);
+      if (dot3(k, k) >= NONORTHO_SIN2_TOL * dot3(&m.sf[3 * fg], &m.sf[3 * fg])) {
+        for (int j = 0; j < 3; ++j) k_bnd[3 * ib + j] = k[j];
+        act_bnd[ib] = 1;
+      }
+    }
+  }
+
+  // src/solver/mod_fv_solver.f90:3410-3495 (T = sum |Sf| n n^T over closing faces, inverted)
+  void build_reconstruct_operator() {
+    std::vector<double> Tm(9 * nc, 0.0);
+    auto add = [&](int c, int64_t f) {
+      const double* n = &m.normal[3 * f];
+      for (int j = 0; j < 3; ++j)
+        for (int i = 0; i < 3; ++i) Tm[9 * c + i + 3 * j] += m.area[f] * n[i] * n[j];
+    };
+    for (int64_t i = 0; i < nfp; ++i) {
+      if (ps_skip[i]) continue;
+      add(ps_owner[i], ps_mesh[i]);
+      add(ps_nb[i], ps_mesh[i]);
+    }
+    for (int64_t fb : nper_bf) add(m.owner[nfi + fb], nfi + fb);
+    for (int64_t c = 0; c < nc; ++c) {
+      const double* A = &Tm[9 * c];
+      auto a = [&](int i, int j) { return A[(i - 1) + 3 * (j - 1)]; };
+      double c11 = a(2, 2) * a(3, 3) - a(2, 3) * a(3, 2);
+      double c12 = a(1, 3) * a(3, 2) - a(1, 2) * a(3, 3);
+      double c13 = a(1, 2) * a(2, 3) - a(1, 3) * a(2, 2);
+      double c22 = a(1, 1) * a(3, 3) - a(1, 3) * a(3, 1);
+      double c23 = a(1, 3) * a(2, 1) - a(1, 1) * a(2, 3);
+      double c33 = a(1, 1) * a(2, 2) - a(1, 2) * a(2, 1);
+      double det = a(1, 1) * c11 + a(1, 2) * (a(2, 3) * a(3, 1) - a(2, 1) * a(3, 3)) +
+                   a(1, 3) * (a(2, 1) * a(3, 2) - a(2, 2) * a(3, 1));
+      double tr = a(1, 1) + a(2, 2) + a(3, 3);
+      double* Ti = &Tinv[9 * c];
+      double mt = std::max(tr, SMALL);
+      if (std::fabs(det) <= 1.0e-12 * mt * mt * mt) {
+        for (int k = 0; k < 9; ++k) Ti[k] = 0.0;
+        Ti[0] = Ti[4] = Ti[8] = 3.0 / mt;
+        continue;
+      }
+      // Ti column-major: Ti[(i-1) + 3(j-1)] = Ainv(i,j)
+      Ti[0] = c11 / det; Ti[3] = c12 / det; Ti[6] = c13 / det;
+      Ti[1] = c12 / det; Ti[4] = c22 / det; Ti[7] = c23 / det;
+      Ti[2] = c13 / det; Ti[5] = c23 / det; Ti[8] = c33 / det;
+    }
+  }
+
+  // src/sgs/mod_vreman.f90:168-264 (build_filter_tensor + smooth_filter_tensor)
+  void build_filter_tensor() {
+    Gf.assign(9 * nc, 0.0);
+    for (int64_t c = 0; c < nc; ++c) {
+      double d2 = std::pow(m.volume[c], 2.0 / 3.0);
+      double g[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+      for (int64_t k = m.cell_face_off[c]; k < m.cell_face_off[c + 1]; ++k) {
+        int f = m.cell_faces[k];
+        double dx[3];
+        for (int j = 0; j < 3; ++j) dx[j] = m.centre[3 * (int64_t)f + j] - m.centroid[3 * c + j];
+        for (int n = 0; n < 3; ++n)
+          for (int mm = 0; mm < 3; ++mm) g[mm + 3 * n] += m.area[f] * dx[mm] * dx[n];
+      }
+      double det = det3(g);
+      double t = (g[0] + g[4] + g[8]) / 3.0;
+      double tr3 = t * t * t;
+      if (tr3 > 0.0 && det > 1.0e-12 * tr3) {
+        double s = std::pow(m.volume[c] * m.volume[c] / det, 1.0 / 3.0);
+        for (int j = 0; j < 9; ++j) Gf[9 * c + j] = s * g[j];
+      } else {
+        Gf[9 * c] = Gf[9 * c + 4] = Gf[9 * c + 8] = d2;
+      }
+    }
+    std::vector<double> gnb(9 * nc), ws(nc);
+    for (int pass = 0; pass < 2; ++pass) {
+      std::fill(gnb.begin(), gnb.end(), 0.0);
+      std::fill(ws.begin(), ws.end(), 0.0);
+      for (int64_t f = 0; f < nf; ++f) {
+        int o = m.owner[f], n = m.neighbour[f];
+        if (n < 0) continue;
+        double a = m.area[f];
+        for (int j = 0; j < 9; ++j) gnb[9 * o + j] += a * Gf[9 * n + j];
+        ws[o] += a;
+        for (int j = 0; j < 9; ++j) gnb[9 * n + j] += a * Gf[9 * o + j];
+        ws[n] += a;
+      }
+      for (int64_t c = 0; c < nc; ++c)
+        if (ws[c] > SMALL)
+          for (int j = 0; j < 9; ++j) Gf[9 * c + j] = 0.5 * Gf[9 * c + j] + 0.5 * gnb[9 * c + j] / ws[c];
+    }
+  }
+
+  // ---------------------------------------------------------------- boundary conditions
+  // src/bc/mod_bc.f90:196-380.  filt: -1 all faces, 0 non-periodic only, 1 periodic only.
+  void apply_velocity_bc(int filt, bool have_grad) {
+    for (int64_t fb = 0; fb < nb; ++fb) {
+      int64_t fg = nfi + fb;
+      int bc = bc_of_face(fg);
+      if (filt == 1 && bc != BC_PERIODIC) continue;
+      if (filt == 0 && bc == BC_PERIODIC) continue;
+      int o = m.owner[fg];
+      const double* n = &m.normal[3 * fg];
+      double u[3] = {U_bnd[3 * fb], U_bnd[3 * fb + 1], U_bnd[3 * fb + 2]};
+      switch (bc) {
+        case BC_INLET:
+          for (int k = 0; k < 3; ++k) u[k] = pc[m.patch[fg]].U_val[k];
+          break;
+        case BC_OUTLET:
+        case BC_ZEROGRADIENT: {
+          for (int k = 0; k < 3; ++k) u[k] = U[3 * o + k];
+          if (have_grad) {
+            double d[3];
+            for (int k = 0; k < 3; ++k) d[k] = m.centre[3 * fg + k] - m.centroid[3 * o + k];
+            for (int k = 0; k < 3; ++k)
+              u[k] = u[k] + grad_U[9 * o + 3 * k] * d[0] + grad_U[9 * o + 3 * k + 1] * d[1] + grad_U[9 * o + 3 * k + 2] * d[2];
+          }
+          break;
+        }
+        case BC_WALL_NOSLIP:
+        case BC_WALL_MODEL:
+          u[0] = u[1] = u[2] = 0.0;
+          break;
+        case BC_WALL_VELOCITY: {
+          for (int k = 0; k < 3; ++k) u[k] = pc[m.patch[fg]].U_val[k];
+          double un = u[0] * n[0] + u[1] * n[1] + u[2] * n[2];
+          for (int k = 0; k < 3; ++k) u[k] = u[k] - un * n[k];
+          break;
+        }
+        case BC_PERIODIC: {
+          for (int k = 0; k < 3; ++k) u[k] = U[3 * o + k];
+          int pnb = m.periodic_partner_cell(fb);
+          if (pnb >= 0 && pnb != o) {
+            double w = m.periodic_gc[fb];
+            for (int k = 0; k < 3; ++k) u[k] = w * u[k] + (1.0 - w) * U[3 * pnb + k];
+          }
+          break;
+        }
+        case BC_SLIP:
+        case BC_SYMMETRY: {
+          for (int k = 0; k < 3; ++k) u[k] = U[3 * o + k];
+          double un = u[0] * n[0] + u[1] * n[1] + u[2] * n[2];
+          for (int k = 0; k < 3; ++k) u[k] = u[k] - un * n[k];
+          break;
+        }
+        default:
+          break;
+      }
+      for (int k = 0; k < 3; ++k) U_bnd[3 * fb + k] = u[k];
+    }
+  }
+
+  // src/bc/mod_bc.f90:383-486.  pf: cell pressure-like field; writes p_bnd.
+  void apply_pressure_bc(const double* pf, int filt, bool have_grad, bool increment) {
+    double oscale = increment ? 0.0 : 1.0;
+    for (int64_t fb = 0; fb < nb; ++fb) {
+      int64_t fg = nfi + fb;
+      int bc = bc_of_face(fg);
+      if (filt == 1 && bc != BC_PERIODIC) continue;
+      if (filt == 0 && bc == BC_PERIODIC) continue;
+      int o = m.owner[fg];
+      switch (bc) {
+        case BC_OUTLET:
+          p_bnd[fb] = oscale * pc[m.patch[fg]].p_val;
+          break;
+        case BC_PERIODIC: {
+          int pnb = m.periodic_partner_cell(fb);
+          if (pnb >= 0 && pnb != o) p_bnd[fb] = m.periodic_gc[fb] * pf[o] + (1.0 - m.periodic_gc[fb]) * pf[pnb];
+          else p_bnd[fb] = pf[o];
+          break;
+        }
+        case BC_WALL_NOSLIP: case BC_WALL_VELOCITY: case BC_WALL_MODEL: case BC_SLIP: case BC_SYMMETRY:
+          p_bnd[fb] = pf[o] - 0.0;  // a_wall = 0: p_bnd = p_o - (a_wall.n) d_ortho
+          break;
+        default:
+          if (have_grad) {
+            double d[3];
+            for (int k = 0; k < 3; ++k) d[k] = m.centre[3 * fg + k] - m.centroid[3 * o + k];
+            p_bnd[fb] = pf[o] + gp[3 * o] * d[0] + gp[3 * o + 1] * d[1] + gp[3 * o + 2] * d[2];
+          } else {
+            p_bnd[fb] = pf[o];
+          }
+      }
+    }
+  }
+
+  void refresh_halos_and_bc() {  // src/solver/mod_fv_solver.f90:985-1001
+    apply_velocity_bc(0, true);
+    apply_pressure_bc(p.data(), 0, !skip_grad_p, false);
+    apply_velocity_bc(1, true);
+    apply_pressure_bc(p.data(), 1, !skip_grad_p, false);
+  }
+  void velocity_bc_refresh() {  // the apply_velocity_bc pair after each U update
+    apply_velocity_bc(0, true);
+    apply_velocity_bc(1, true);
+  }
+  void apply_pressure_bc_o2(bool incr) {  // src/solver/mod_fv_solver.f90:2324-2338
+    apply_pressure_bc(p.data(), 0, !skip_grad_p, incr);
+  }
+
+  // ---------------------------------------------------------------- gradients
+  // src/numerics/mod_gradient.f90:425-613 (CPU path)
+  void ls_gradient_vector(const double* Uc, const double* Ub, double* g) {
+#pragma omp parallel for schedule(static) num_threads(nthreads)
+    for (int64_t c = 0; c < nc; ++c) {
+      double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+      for (int64_t k = m.ls_off[c]; k < m.ls_off[c + 1]; ++k) {
+        int n = m.ls_cell[k];
+        double un[3];
+        if (n < 0) {
+          int f = m.ls_face[k];
+          int64_t bi = f >= 0 ? f - nfi : -1;
+          if (bi >= 0 && bi < nb) for (int j = 0; j < 3; ++j) un[j] = Ub[3 * bi + j];
+          else for (int j = 0; j < 3; ++j) un[j] = Uc[3 * c + j];
+        } else {
+          for (int j = 0; j < 3; ++j) un[j] = Uc[3 * (int64_t)n + j];
+        }
+        for (int j = 0; j < 3; ++j) {
+          double du = un[j] - Uc[3 * c + j];
+          for (int i = 0; i < 3; ++i) acc[i + 3 * j] += m.ls_w[3 * k + i] * du;
+        }
+      }
+      for (int j = 0; j < 9; ++j) g[9 * c + j] = acc[j];
+    }
+  }
+  // src/numerics/mod_gradient.f90:307-423 (CPU path)
+  void ls_gradient_scalar(const double* phi, const double* pb, double* g) {
+#pragma omp parallel for schedule(static) num_threads(nthreads)
+    for (int64_t c = 0; c < nc; ++c) {
+      double acc[3] = {0, 0, 0};
+      for (int64_t k = m.ls_off[c]; k < m.ls_off[c + 1]; ++k) {
+        int n = m.ls_cell[k];
+        double v;
+        if (n < 0) {
+          int f = m.ls_face[k];
+          int64_t bi = f >= 0 ? f - nfi : -1;
+          v = (bi >= 0 && bi < nb) ? pb[bi] : phi[c];
+        } else {
+          v = phi[n];
+        }
+        double d = v - phi[c];
+        for (int i = 0; i < 3; ++i) acc[i] += m.ls_w[3 * k + i] * d;
+      }
+      for (int i = 0; i < 3; ++i) g[3 * c + i] = acc[i];
+    }
+  }
+  void compute_all_gradients() { ls_gradient_vector(U.data(), U_bnd.data(), grad_U.data()); }
+  void compute_pressure_gradient() {
+    if (skip_grad_p) return;
+    ls_gradient_scalar(p.data(), p_bnd.data(), gp.data());
+  }
+
+  // ---------------------------------------------------------------- SGS
+  void sgs_viscosity(double dt_stab) {
+    if (P.sgs_model == DPM_SGS_NONE) { std::fill(nu_sgs.begin(), nu_sgs.end(), 0.0); return; }
+    if (P.sgs_model == DPM_SGS_VREMAN) {  // src/sgs/mod_vreman.f90:50-153
+#pragma omp parallel for schedule(static) num_threads(nthreads)
+      for (int64_t c = 0; c < nc; ++c) {
+        const double* a = &grad_U[9 * c];  // a[m + 3i] = alpha(m,i)
+        const double* G = &Gf[9 * c];
+        double beta[9];
+        for (int j = 0; j < 3; ++j)
+          for (int i = 0; i <= j; ++i) {
+            double s = 0.0;
+            for (int n = 0; n < 3; ++n)
+              for (int mm = 0; mm < 3; ++mm) s += G[mm + 3 * n] * a[mm + 3 * i] * a[n + 3 * j];
+            beta[i + 3 * j] = s;
+          }
+        double asq = a[0] * a[0] + a[3] * a[3] + a[6] * a[6] + a[1] * a[1] + a[4] * a[4] + a[7] * a[7] +
+                     a[2] * a[2] + a[5] * a[5] + a[8] * a[8];
+        double b11 = beta[0], b22 = beta[4], b33 = beta[8], b12 = beta[3], b13 = beta[6], b23 = beta[7];
+        double B = b11 * b22 - b12 * b12 + b11 * b33 - b13 * b13 + b22 * b33 - b23 * b23;
+        double nu_c = (asq > SMALL && B > 0.0) ? C_VREMAN * std::sqrt(B / asq) : 0.0;
+        double cap = NU_SGS_STAB_FRAC * std::pow(m.volume[c], 2.0 / 3.0) / std::max(dt_stab, SMALL);
+        nu_sgs[c] = std::min(nu_c, cap);
+      }
+      return;
+    }
+    if (P.sgs_model == DPM_SGS_SMAGORINSKY) {  // src/sgs/mod_vreman.f90:295-364
+#pragma omp parallel for schedule(static) num_threads(nthreads)
+      for (int64_t c = 0; c < nc; ++c) {
+        const double* g = &grad_U[9 * c];
+        double SS = 0.0;
+        for (int j = 0; j < 3; ++j)
+          for (int i = 0; i < 3; ++i) {
+            double s = 0.5 * (g[i + 3 * j] + g[j + 3 * i]);
+            SS += s * s;
+          }
+        double Sn = std::sqrt(2.0 * SS);
+        double delta = std::max(std::pow(std::max(det3(&Gf[9 * c]), 0.0), 1.0 / 6.0), SMALL);
+        double nu_c = (0.1 * delta) * (0.1 * delta) * Sn;
+        double cap = NU_SGS_STAB_FRAC * delta * delta / std::max(dt_stab, SMALL);
+        nu_sgs[c] = std::min(nu_c, cap);
+      }
+      return;
+    }
+    if (P.sgs_model == DPM_SGS_AMD) {  // src/sgs/mod_amd.f90:69-207
+      for (int64_t c = 0; c < nc; ++c) {
+        double nu_c = amd_point(&grad_U[9 * c], &Gf[9 * c], P.c_amd);
+        double cap = NU_SGS_STAB_FRAC * std::pow(m.volume[c], 2.0 / 3.0) / std::max(dt_stab, SMALL);
+        nu_sgs[c] = std::min(nu_c, cap);
+      }
+      if (P.amd_wall_gradient && nb > 0) {
+        for (int64_t fb = 0; fb < nb; ++fb) {
+          int64_t fg = nfi + fb;
+          if (bc_of_face(fg) != BC_WALL_MODEL) continue;
+          int o = m.owner[fg];
+          double nrm[3], d[3];
+          for (int k = 0; k < 3; ++k) { nrm[k] = -m.normal[3 * fg + k]; d[k] = m.centre[3 * fg + k] - m.centroid[3 * o + k]; }
+          double yw = std::fabs(dot3(d, nrm));
+          double un = dot3(&U[3 * o], nrm);
+          double ut[3];
+          for (int k = 0; k < 3; ++k) ut[k] = U[3 * o + k] - un * nrm[k];
+          double utm = std::sqrt(ut[0] * ut[0] + ut[1] * ut[1] + ut[2] * ut[2]);
+          if (utm <= 1.0e-14 || yw <= SMALL) continue;
+          double utau, taum;
+          bool cap;
+          wall_stress_newton(utm, yw, P.nu, utau, taum, cap);
+          double gw = utau / (KAPPA * yw);
+          double a[9];
+          for (int k = 0; k < 9; ++k) a[k] = grad_U[9 * o + k];
+          double dold[3], dt_[3];
+          for (int j = 0; j < 3; ++j) dold[j] = nrm[0] * a[0 + 3 * j] + nrm[1] * a[1 + 3 * j] + nrm[2] * a[2 + 3 * j];
+          double dn = dot3(dold, nrm);
+          for (int j = 0; j < 3; ++j) dt_[j] = gw * ut[j] / utm - (dold[j] - dn * nrm[j]);
+          for (int j = 0; j < 3; ++j)
+            for (int i = 0; i < 3; ++i) a[i + 3 * j] += nrm[i] * dt_[j];
+          double nu_c = amd_point(a, &Gf[9 * o], P.c_amd);
+          double cp = NU_SGS_STAB_FRAC * std::pow(m.volume[o], 2.0 / 3.0) / std::max(dt_stab, SMALL);
+          nu_sgs[o] = std::min(nu_c, cp);
+        }
+      }
+      return;
+    }
+  }
+
+  // ---------------------------------------------------------------- wall model
+  // src/sgs/mod_wall_model.f90:176-313
+  void wall_model(double dt_filter) {
+    if (y_w.empty()) {
+      y_w.assign(nb, 0.0);
+      sample_cell.assign(nb, -1);
+      u_par_filt.assign(3 * nb, 0.0);
+      for (int64_t fb = 0; fb < nb; ++fb) {
+        int64_t fg = nfi + fb;
+        if (bc_of_face(fg) != BC_WALL_MODEL) continue;
+        int o = m.owner[fg];
+        double d[3];
+        for (int k = 0; k < 3; ++k) d[k] = m.centroid[3 * o + k] - m.centre[3 * fg + k];
+        double nin[3] = {-m.normal[3 * fg], -m.normal[3 * fg + 1], -m.normal[3 * fg + 2]};
+        sample_cell[fb] = o;
+        y_w[fb] = std::fabs(dot3(d, nin)) + SMALL;
+      }
+    }
+    double t_use = P.wall_model_filter_time, tf = P.wall_model_filter_tf_fac;
+    bool adaptive = tf > SMALL;
+    bool do_filter = (t_use > SMALL || adaptive);
+    bool seed = !filt_ready;
+    double w_filt = (do_filter && !adaptive) ? dt_filter / (t_use + dt_filter) : 0.0;
+    for (int64_t fb = 0; fb < nb; ++fb) {
+      int64_t fg = nfi + fb;
+      if (bc_of_face(fg) != BC_WALL_MODEL) continue;
+      const double* n = &m.normal[3 * fg];
+      int cs = sample_cell[fb] >= 0 ? sample_cell[fb] : m.owner[fg];
+      double yw = y_w[fb];
+      double un = U[3 * cs] * n[0] + U[3 * cs + 1] * n[1] + U[3 * cs + 2] * n[2];
+      double u[3];
+      for (int k = 0; k < 3; ++k) u[k] = U[3 * cs + k] - un * n[k];
+      if (do_filter) {
+        double* uf = &u_par_filt[3 * fb];
+        if (seed) {
+          for (int k = 0; k < 3; ++k) uf[k] = u[k];
+        } else {
+          double e = w_filt;
+          if (adaptive) {
+            e = 0.0;
+            if (dt_filter > 0.0) {
+              double upm = std::sqrt(uf[0] * uf[0] + uf[1] * uf[1] + uf[2] * uf[2]), utp, tp;
+              bool cp;
+              wall_stress_newton(upm, yw, P.nu, utp, tp, cp);
+              e = 1.0;
+              if (utp > SMALL) e = std::min(1.0, dt_filter * KAPPA * utp / (tf * yw));
+            }
+          }
+          for (int k = 0; k < 3; ++k) uf[k] = uf[k] + e * (u[k] - uf[k]);
+        }
+        for (int k = 0; k < 3; ++k) u[k] = uf[k];
+      }
+      double um = std::sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+      double utau, tm;
+      bool cp;
+      wall_stress_newton(um, yw, P.nu, utau, tm, cp);
+      double sc = -tm / (um + SMALL);
+      for (int k = 0; k < 3; ++k) tau_w[3 * fb + k] = sc * u[k];
+    }
+    if (t_use > SMALL || adaptive) filt_ready = true;
+  }
+
+  // ---------------------------------------------------------------- advection
+  int periodic_nb(int64_t fb, int o) const {  // soa_resolve_periodic_nb_dev, single-rank
+    int n = m.periodic_partner_cell(fb);
+    if (n == o) n = -1;
+    return n;
+  }
+
+  // src/numerics/mod_advection.f90:1013-1197
+  void advection_kep(double* rhs) {
+    std::vector<double> div(nc, 0.0);
+    std::fill(rhs, rhs + 3 * nc, 0.0);
+    for (int64_t f = 0; f < nf; ++f) {
+      int o = m.owner[f], n = m.neighbour[f];
+      const double* sf = &m.sf[3 * f];
+      int64_t fb = 0;
+      int bc = -1, npr = -1;
+      double Uf[3], Fn;
+      if (n >= 0) {
+        for (int k = 0; k < 3; ++k) Uf[k] = m.gc[f] * U[3 * o + k] + (1.0 - m.gc[f]) * U[3 * n + k];
+        Fn = U_face[f];
+      } else {
+        fb = f - nfi;
+        bc = bc_of_face(f);
+        if (bc == BC_PERIODIC) npr = periodic_nb(fb, o);
+        if (bc == BC_PERIODIC && npr >= 0) {
+          double w = m.periodic_gc[fb];
+          for (int k = 0; k < 3; ++k) Uf[k] = w * U[3 * o + k] + (1.0 - w) * U[3 * npr + k];
+        } else {
+          for (int k = 0; k < 3; ++k) Uf[k] = U_bnd[3 * fb + k];
+        }
+        if (bc == BC_PERIODIC || bc == BC_OUTLET) Fn = U_face[f];
+        else if (is_wall(bc)) Fn = 0.0;
+        else Fn = dot3(Uf, sf);
+      }
+      div[o] += Fn;
+      if (n >= 0) div[n] -= Fn;
+      for (int k = 0; k < 3; ++k) {
+        double phi;
+        if (n >= 0) phi = 0.5 * (U[3 * o + k] + U[3 * n + k]);
+        else if (npr >= 0) phi = 0.5 * (U[3 * o + k] + U[3 * npr + k]);
+        else phi = Uf[k];
+        rhs[3 * o + k] -= Fn * phi * inv_vol[o];
+        if (n >= 0) rhs[3 * n + k] += Fn * phi * inv_vol[n];
+      }
+    }
+    for (int64_t c = 0; c < nc; ++c)
+      for (int k = 0; k < 3; ++k) rhs[3 * c + k] += 0.5 * U[3 * c + k] * div[c] * inv_vol[c];
+  }
+
+  // src/numerics/mod_advection.f90:1200-1392
+  void advection_cds(double* rhs) {
+    std::fill(rhs, rhs + 3 * nc, 0.0);
+    for (int64_t f = 0; f < nf; ++f) {
+      int o = m.owner[f], n = m.neighbour[f];
+      int64_t fb = 0;
+      int bc = -1, npr = -1;
+      double Fn;
+      if (n >= 0) {
+        Fn = U_face[f];
+      } else {
+        fb = f - nfi;
+        bc = bc_of_face(f);
+        if (bc == BC_PERIODIC || bc == BC_OUTLET) Fn = U_face[f];
+        else if (is_wall(bc)) Fn = 0.0;
+        else Fn = dot3(&U_bnd[3 * fb], &m.sf[3 * f]);
+      }
+      bool has_rec = n >= 0;
+      if (!has_rec && bc == BC_PERIODIC) {
+        npr = periodic_nb(fb, o);
+        has_rec = npr >= 0;
+      }
+      int ns = has_rec ? (n >= 0 ? n : npr) : -1;
+      for (int k = 0; k < 3; ++k) {
+        double phi;
+        if (has_rec) {
+          double gcv = f >= nfi ? m.periodic_gc[fb] : m.gc[f];
+          double plain = gcv * U[3 * o + k] + (1.0 - gcv) * U[3 * ns + k];
+          if (f < nfi) {
+            double gm[3], ph;
+            for (int i = 0; i < 3; ++i) gm[i] = gcv * grad_U[9 * o + 3 * k + i] + (1.0 - gcv) * grad_U[9 * (int64_t)ns + 3 * k + i];
+            ph = plain + dot3(gm, &m.eps[3 * f]);
+            double wb = refine_blend_weight(m.skew[f]);
+            if (wb < 1.0) ph = plain + wb * (ph - plain);
+            phi = ph;
+          } else {
+            phi = plain;
+          }
+        } else {
+          phi = U_bnd[3 * fb + k];
+        }
+        if (!finite(phi)) phi = 0.0;
+        rhs[3 * o + k] -= Fn * phi * inv_vol[o];
+        if (n >= 0) rhs[3 * n + k] += Fn * phi * inv_vol[n];
+      }
+    }
+  }
+
+  // Reconstruction context of face f for flux Fn (mod_advection.f90:2386-2498).
+  struct Ctx { int up, down; double x_up[3], x_down[3], x_face[3], up_shift[3], dir[3], s_face, s_down; };
+  bool recon_context(int64_t f, double Fn, Ctx& c) const {
+    c.up = c.down = -1;
+    for (int k = 0; k < 3; ++k) { c.x_up[k] = c.x_down[k] = c.up_shift[k] = c.dir[k] = 0.0; c.x_face[k] = m.centre[3 * f + k]; }
+    c.s_face = c.s_down = 0.0;
+    int o = m.owner[f], n = m.neighbour[f];
+    if (n >= 0) {
+      if (Fn >= 0.0) { c.up = o; c.down = n; } else { c.up = n; c.down = o; }
+      for (int k = 0; k < 3; ++k) { c.x_up[k] = m.centroid[3 * c.up + k]; c.x_down[k] = m.centroid[3 * c.down + k]; }
+    } else {
+      if (bc_of_face(f) != BC_PERIODIC) return false;
+      int64_t fb = f - nfi;
+      int pcell = periodic_nb(fb, o);
+      int pb = m.periodic_pair[fb];
+      int64_t pf = pb >= 0 ? nfi + pb : -1;
+      if (pcell < 0 && pf >= 0) pcell = m.owner[pf];
+      if (pcell < 0) return false;
+      double d_per;
+      if (pf >= 0) d_per = m.d_cf[f] + m.d_cf[pf];
+      else if (m.periodic_pair_dcf[fb] > SMALL) d_per = m.d_cf[f] + m.periodic_pair_dcf[fb];
+      else d_per = 2.0 * m.d_cf[f];
+      double shift[3];
+      for (int k = 0; k < 3; ++k) shift[k] = (m.centroid[3 * o + k] + d_per * m.normal[3 * f + k]) - m.centroid[3 * pcell + k];
+      if (Fn >= 0.0) {
+        c.up = o; c.down = pcell;
+        for (int k = 0; k < 3; ++k) { c.x_up[k] = m.centroid[3 * o + k]; c.x_down[k] = m.centroid[3 * pcell + k] + shift[k]; }
+      } else {
+        c.up = pcell; c.down = o;
+        for (int k = 0; k < 3; ++k) {
+          c.up_shift[k] = shift[k];
+          c.x_up[k] = m.centroid[3 * pcell + k] + c.up_shift[k];
+          c.x_down[k] = m.centroid[3 * o + k];
+        }
+      }
+    }
+    double dv[3], dn;
+    for (int k = 0; k < 3; ++k) dv[k] = c.x_face[k] - c.x_up[k];
+    dn = std::sqrt(dot3(dv, dv));
+    if (dn <= SMALL) {
+      for (int k = 0; k < 3; ++k) dv[k] = c.x_down[k] - c.x_up[k];
+      dn = std::sqrt(dot3(dv, dv));
+    }
+    if (dn <= SMALL) return false;
+    for (int k = 0; k < 3; ++k) c.dir[k] = dv[k] / dn;
+    double a[3], b[3];
+    for (int k = 0; k < 3; ++k) { a[k] = c.x_face[k] - c.x_up[k]; b[k] = c.x_down[k] - c.x_up[k]; }
+    c.s_face = dot3(a, c.dir);
+    c.s_down = dot3(b, c.dir);
+    if (c.s_face <= SMALL || c.s_down <= c.s_face) {
+      for (int k = 0; k < 3; ++k) dv[k] = c.x_down[k] - c.x_up[k];
+      dn = std::sqrt(dot3(dv, dv));
+      if (dn <= SMALL) return false;
+      for (int k = 0; k < 3; ++k) c.dir[k] = dv[k] / dn;
+      c.s_face = dot3(a, c.dir);
+      c.s_down = dot3(b, c.dir);
+    }
+    if (c.s_down <= SMALL) return false;
+    c.s_face = std::min(std::max(c.s_face, 0.0), c.s_down);
+    return true;
+  }
+
+  // mod_advection.f90:2501-2549
+  int far_upwind(const Ctx& c) const {
+    int far = -1;
+    if (c.up < 0 || c.up >= nc || c.down >= nc) return far;
+    double best_align = -1.0, best_perp2 = 1e308;
+    for (int64_t fi = m.cell_face_off[c.up]; fi < m.cell_face_off[c.up + 1]; ++fi) {
+      int fj = m.cell_faces[fi];
+      int n = m.owner[fj];
+      if (n == c.up) n = m.neighbour[fj];
+      if (n < 0) {
+        if (fj >= nfi && bc_of_face(fj) == BC_PERIODIC) n = periodic_nb(fj - nfi, c.up);
+      }
+      if (n == c.down || n < 0) continue;
+      double d[3];
+      for (int k = 0; k < 3; ++k) d[k] = m.centroid[3 * n + k] + c.up_shift[k] - c.x_up[k];
+      double s = dot3(d, c.dir);
+      if (s >= -1.0e-12) continue;
+      double dist2 = std::max(dot3(d, d), SMALL);
+      double align = -s / std::sqrt(dist2);
+      double perp2 = std::max(0.0, dist2 - s * s);
+      if (align > best_align + 1.0e-12 ||
+          (std::fabs(align - best_align) <= 1.0e-12 && perp2 < best_perp2 - 1.0e-12) ||
+          (std::fabs(align - best_align) <= 1.0e-12 && std::fabs(perp2 - best_perp2) <= 1.0e-12 && n < far)) {
+        best_align = align; best_perp2 = perp2; far = n;
+      }
+    }
+    return far;
+  }
+
+  static double clampv(double x, double lo, double hi) {
+    double l = std::min(lo, hi), h = std::max(lo, hi);
+    return std::min(std::max(x, l), h);
+  }
+
+  // mod_advection.f90:2632-2722 (3-component QUICK fit on the upwind cell's neighbours)
+  void quick3(const Ctx& c, double* phi_f) const {
+    bool have_grad = c.up < nc && c.down < nc;
+    double phU[3], phD[3], gup[3][3];
+    for (int k = 0; k < 3; ++k) {
+      phU[k] = U[3 * c.up + k];
+      phD[k] = U[3 * c.down + k];
+      for (int i = 0; i < 3; ++i) gup[k][i] = have_grad ? grad_U[9 * c.up + 3 * k + i] : 0.0;
+    }
+    auto axial = [&](double far, double up, const double* g, const double* dv, double s) {
+      double t[3];
+      for (int i = 0; i < 3; ++i) t[i] = dv[i] - s * c.dir[i];
+      return far - up - dot3(g, t);
+    };
+    double dv[3];
+    for (int i = 0; i < 3; ++i) dv[i] = c.x_down[i] - c.x_up[i];
+    double dist2 = std::max(dot3(dv, dv), SMALL);
+    double w = 1.0 / dist2;
+    double a11 = w * c.s_down * c.s_down, a12 = a11 * c.s_down, a22 = a12 * c.s_down, lin_den = a11;
+    int nfit = 1;
+    double b1[3], b2[3], ln[3];
+    for (int k = 0; k < 3; ++k) {
+      double dp = axial(phD[k], phU[k], gup[k], dv, c.s_down);
+      b1[k] = w * c.s_down * dp;
+      b2[k] = w * c.s_down * c.s_down * dp;
+      ln[k] = b1[k];
+    }
+    if (c.up < nc && c.down < nc) {
+      for (int64_t fi = m.cell_face_off[c.up]; fi < m.cell_face_off[c.up + 1]; ++fi) {
+        int fj = m.cell_faces[fi];
+        int n = m.owner[fj];
+        if (n == c.up) n = m.neighbour[fj];
+        if (n < 0 || n == c.down) continue;
+        double d[3];
+        for (int i = 0; i < 3; ++i) d[i] = m.centroid[3 * n + i] + c.up_shift[i] - c.x_up[i];
+        double s = dot3(d, c.dir);
+        if (s >= -1.0e-12) continue;
+        double d2 = std::max(dot3(d, d), SMALL);
+        if (s * s < 0.25 * d2) continue;
+        double al = std::min(1.0, -s / std::sqrt(d2));
+        double wt = (0.25 + al * al) / d2;
+        a11 += wt * s * s; a12 += wt * s * s * s; a22 += wt * s * s * s * s; lin_den += wt * s * s;
+        for (int k = 0; k < 3; ++k) {
+          double dp = axial(U[3 * n + k], phU[k], gup[k], d, s);
+          b1[k] += wt * s * dp; b2[k] += wt * s * s * dp; ln[k] += wt * s * dp;
+        }
+        nfit++;
+      }
+    }
+    double det = a11 * a22 - a12 * a12;
+    for (int k = 0; k < 3; ++k) {
+      double a1, a2;
+      if (nfit >= 2 && std::fabs(det) > SMALL) {
+        a1 = (b1[k] * a22 - b2[k] * a12) / det;
+        a2 = (-b1[k] * a12 + b2[k] * a11) / det;
+      } else if (lin_den > SMALL) {
+        a1 = ln[k] / lin_den; a2 = 0.0;
+      } else {
+        a1 = (phD[k] - phU[k]) / std::max(c.s_down, SMALL); a2 = 0.0;
+      }
+      double v = phU[k] + a1 * c.s_face + a2 * c.s_face * c.s_face;
+      phi_f[k] = clampv(v, std::min(phU[k], phD[k]), std::max(phU[k], phD[k]));
+    }
+  }
+
+  // mod_advection.f90:2725-2791
+  double tvd(int scheme, const double* phi, int stride, const Ctx& c, int far) const {
+    double pU = phi[stride * (int64_t)c.up], pD = phi[stride * (int64_t)c.down];
+    double sdn = (pD - pU) / std::max(c.s_down, SMALL), psi = 0.0;
+    if (far >= 0 && std::fabs(sdn) > SMALL) {
+      double xf[3];
+      for (int k = 0; k < 3; ++k) xf[k] = m.centroid[3 * far + k] + c.up_shift[k] - c.x_up[k];
+      double s_up = -dot3(xf, c.dir);
+      if (s_up <= SMALL) {
+        psi = 0.0;
+      } else {
+        double pUU = phi[stride * (int64_t)far];
+        double r = ((pU - pUU) / s_up) / sdn;
+        if (scheme == DPM_SCHEME_VANLEER_TVD) {
+          psi = (r + std::fabs(r)) / (1.0 + std::fabs(r));
+          psi = std::max(0.0, std::min(psi, 2.0));
+        } else {
+          psi = std::max(0.0, std::min(std::min(2.0 * r, (1.0 + 2.0 * r) / 3.0), 2.0));
+        }
+      }
+    }
+    return clampv(pU + psi * sdn * c.s_face, std::min(pU, pD), std::max(pU, pD));
+  }
+
+  // src/numerics/mod_advection.f90:1396-1635
+  void advection_recon(int scheme, double* rhs) {
+    std::fill(rhs, rhs + 3 * nc, 0.0);
+    for (int64_t f = 0; f < nf; ++f) {
+      int o = m.owner[f], n = m.neighbour[f];
+      int64_t fb = f >= nfi ? f - nfi : 0;
+      double Fn;
+      if (n >= 0) Fn = U_face[f];
+      else {
+        int bc = bc_of_face(f);
+        Fn = is_wall(bc) ? 0.0 : U_face[f];
+      }
+      Ctx c;
+      bool ok = recon_context(f, Fn, c);
+      int far = -1;
+      if (ok && scheme != DPM_SCHEME_QUICK) far = far_upwind(c);
+      if (!finite(Fn)) Fn = 0.0;
+      double pq[3] = {0, 0, 0};
+      if (ok && scheme == DPM_SCHEME_QUICK) quick3(c, pq);
+      for (int k = 0; k < 3; ++k) {
+        double phi;
+        if (ok) {
+          if (scheme == DPM_SCHEME_QUICK) phi = pq[k];
+          else phi = tvd(scheme, &U[k], 3, c, far);
+          if (!finite(phi)) phi = (Fn >= 0.0 || n < 0) ? U[3 * o + k] : U[3 * n + k];
+        } else {
+          phi = U_bnd[3 * fb + k];
+        }
+        if (!finite(phi)) phi = 0.0;
+        rhs[3 * o + k] -= Fn * phi * inv_vol[o];
+        if (n >= 0) rhs[3 * n + k] += Fn * phi * inv_vol[n];
+      }
+    }
+  }
+
+  void advection(double* rhs) {
+    if (P.scheme == DPM_SCHEME_KEP) advection_kep(rhs);
+    else if (P.scheme == DPM_SCHEME_CDS) advection_cds(rhs);
+    else advection_recon(P.scheme, rhs);
+  }
+
+  // ---------------------------------------------------------------- viscous
+  // src/numerics/mod_viscous.f90:37-282
+  static double ortho_weight(double sdd, double area) {
+    return area * std::max(0.0, std::min(1.0, sdd / (area + SMALL)));
+  }
+  void viscous(double* rhs) {
+    std::fill(rhs, rhs + 3 * nc, 0.0);
+    for (int64_t f = 0; f < nf; ++f) {
+      int o = m.owner[f], n = m.neighbour[f];
+      const double* sf = &m.sf[3 * f];
+      const double* nh = &m.normal[3 * f];
+      double st[3] = {0, 0, 0};
+      auto face_stress = [&](int nbc, double gcv, double nu_eff, const double* d_on, double dlen) {
+        double sdd = dot3(sf, d_on) / dlen;
+        double dperp[3];
+        for (int k = 0; k < 3; ++k) dperp[k] = sf[k] - (sdd / dlen) * d_on[k];
+        double wo = ortho_weight(sdd, m.area[f]);
+        double gf[9];
+        for (int j = 0; j < 9; ++j) gf[j] = gcv * grad_U[9 * o + j] + (1.0 - gcv) * grad_U[9 * (int64_t)nbc + j];
+        for (int k = 0; k < 3; ++k) {
+          // gf[i + 3k] = dU_k/dx_i ; gf(k,:) = dU_j/dx_k over j: gf[k + 3j]
+          double t1 = (U[3 * (int64_t)nbc + k] - U[3 * o + k]) * wo / dlen;
+          double t2 = gf[0 + 3 * k] * dperp[0] + gf[1 + 3 * k] * dperp[1] + gf[2 + 3 * k] * dperp[2];
+          double t3 = gf[k + 0] * sf[0] + gf[k + 3] * sf[1] + gf[k + 6] * sf[2];
+          st[k] = nu_eff * (t1 + t2 + t3);
+        }
+      };
+      if (n >= 0) {
+        double gcv = m.gc[f];
+        double nu_eff = P.nu + gcv * nu_sgs[o] + (1.0 - gcv) * nu_sgs[n];
+        double d[3];
+        for (int k = 0; k < 3; ++k) d[k] = m.centroid[3 * n + k] - m.centroid[3 * o + k];
+        double dl = std::sqrt(dot3(d, d)) + SMALL;
+        face_stress(n, gcv, nu_eff, d, dl);
+      } else {
+        int64_t fb = f - nfi;
+        int bc = bc_of_face(f);
+        if (bc == BC_PERIODIC) {
+          int npr = periodic_nb(fb, o);
+          int pb = m.periodic_pair[fb];
+          int64_t pf = pb >= 0 ? nfi + pb : -1;
+          if (npr >= 0) {
+            double dper, gcp;
+            if (pf >= 0) { dper = m.d_cf[f] + m.d_cf[pf]; gcp = m.d_cf[pf] / (dper + SMALL); }
+            else if (m.periodic_pair_dcf[fb] > SMALL) { dper = m.d_cf[f] + m.periodic_pair_dcf[fb]; gcp = m.periodic_pair_dcf[fb] / (dper + SMALL); }
+            else { dper = 2.0 * m.d_cf[f]; gcp = 0.5; }
+            double nu_eff = P.nu + gcp * nu_sgs[o] + (1.0 - gcp) * nu_sgs[npr];
+            double d[3] = {dper * nh[0], dper * nh[1], dper * nh[2]};
+            face_stress(npr, gcp, nu_eff, d, dper + SMALL);
+          } else {
+            double nu_eff = P.nu + nu_sgs[o];
+            for (int k = 0; k < 3; ++k) st[k] = nu_eff * ((U_bnd[3 * fb + k] - U[3 * o + k]) / (m.d_cf[f] + SMALL)) * m.area[f];
+          }
+        } else if (bc == BC_WALL_MODEL) {
+          // traction enters through add_wall_stress_to_rhs
+        } else {
+          double nu_eff = P.nu + nu_sgs[o];
+          double d[3];
+          for (int k = 0; k < 3; ++k) d[k] = m.centre[3 * f + k] - m.centroid[3 * o + k];
+          double dl = std::sqrt(dot3(d, d)) + SMALL;
+          double sdd = dot3(sf, d) / dl, dperp[3];
+          for (int k = 0; k < 3; ++k) dperp[k] = sf[k] - (sdd / dl) * d[k];
+          double wo = ortho_weight(sdd, m.area[f]);
+          const double* g = &grad_U[9 * o];
+          for (int k = 0; k < 3; ++k) {
+            double t1 = (U_bnd[3 * fb + k] - U[3 * o + k]) * wo / dl;
+            double t2 = g[0 + 3 * k] * dperp[0] + g[1 + 3 * k] * dperp[1] + g[2 + 3 * k] * dperp[2];
+            double t3 = g[k] * sf[0] + g[k + 3] * sf[1] + g[k + 6] * sf[2];
+            st[k] = nu_eff * (t1 + t2 + t3);
+          }
+        }
+      }
+      for (int k = 0; k < 3; ++k) rhs[3 * o + k] += st[k] * inv_vol[o];
+      if (n >= 0)
+        for (int k = 0; k < 3; ++k) rhs[3 * n + k] -= st[k] * inv_vol[n];
+    }
+  }
+
+  // src/solver/mod_fv_solver.f90:1617-1762 (momentum part)
+  void explicit_rhs() {
+    advection(conv_U.data());
+    viscous(visc_U.data());
+    const double* fbg = P.f_const;
+    for (int64_t c = 0; c < nc; ++c) {
+      for (int k = 0; k < 3; ++k) H_U[3 * c + k] = conv_U[3 * c + k] + visc_U[3 * c + k] + fbg[k];
+      if (P.boussinesq)
+        for (int k = 0; k < 3; ++k) H_U[3 * c + k] = H_U[3 * c + k] - P.beta * (T[c] - P.T_ref) * P.g[k];
+    }
+    // add_wall_stress_to_rhs (mod_fv_solver.f90:2238-2276)
+    for (int64_t fb = 0; fb < nb; ++fb) {
+      int64_t fg = nfi + fb;
+      if (bc_of_face(fg) != BC_WALL_MODEL) continue;
+      int o = m.owner[fg];
+      double w = m.area[fg] / m.volume[o];
+      for (int k = 0; k < 3; ++k) H_U[3 * o + k] = H_U[3 * o + k] + tau_w[3 * fb + k] * w;
+    }
+  }
+
+  // ---------------------------------------------------------------- projection
+  // src/solver/mod_fv_solver.f90:2389-2752
+  void face_fluxes_and_rhs(double dt, bool incr) {
+    if (!skip_grad_p) {
+      if (incr) {
+        for (int64_t c = 0; c < nc; ++c) p_tot[c] = phi_prev[c] + p[c];
+        for (int64_t b = 0; b < nb; ++b) p_tot_bnd[b] = phi_prev_bnd[b] + p_bnd[b];
+        ls_gradient_scalar(p_tot.data(), p_tot_bnd.data(), gp.data());
+      } else {
+        ls_gradient_scalar(p.data(), p_bnd.data(), gp.data());
+      }
+    }
+    std::fill(rhs_p.begin(), rhs_p.end(), 0.0);
+    std::fill(face_flux.begin(), face_flux.end(), 0.0);
+    std::fill(built.begin(), built.end(), 0);
+    for (int64_t i = 0; i < nfp; ++i) {
+      if (ps_skip[i]) continue;
+      int o = ps_owner[i], n = ps_nb[i];
+      int64_t fm = ps_mesh[i];
+      double gcf;
+      if (fm < nfi) {
+        gcf = m.gc[fm];
+      } else {
+        int64_t fb = fm - nfi;
+        double d_o = m.d_cf[fm], d_n = d_o;
+        if (m.periodic_pair_dcf[fb] > SMALL) d_n = m.periodic_pair_dcf[fb];
+        if (d_n <= SMALL && m.periodic_pair[fb] >= 0) d_n = m.d_cf[nfi + m.periodic_pair[fb]];
+        double d_t = d_o + d_n;
+        gcf = d_t > SMALL ? d_n / d_t : 0.5;
+      }
+      double d_on[3];
+      for (int k = 0; k < 3; ++k) d_on[k] = m.centroid[3 * n + k] - m.centroid[3 * o + k];
+      const double* sf = &m.sf[3 * fm];
+      double Uf[3], plain[3];
+      for (int k = 0; k < 3; ++k) plain[k] = gcf * U[3 * o + k] + (1.0 - gcf) * U[3 * n + k];
+      if (fm < nfi) {
+        double wb = refine_blend_weight(m.skew[fm]);
+        const double g = m.gc[fm];
+        for (int j = 0; j < 3; ++j) {
+          double ue = g * U[3 * o + j] + (1.0 - g) * U[3 * n + j];
+          double gm[3];
+          for (int i = 0; i < 3; ++i) gm[i] = g * grad_U[9 * o + 3 * j + i] + (1.0 - g) * grad_U[9 * (int64_t)n + 3 * j + i];
+          ue = ue + gm[0] * m.eps[3 * fm] + gm[1] * m.eps[3 * fm + 1] + gm[2] * m.eps[3 * fm + 2];
+          Uf[j] = plain[j] + wb * (ue - plain[j]);
+        }
+      } else {
+        for (int k = 0; k < 3; ++k) Uf[k] = plain[k];
+      }
+      double flux = Uf[0] * sf[0] + Uf[1] * sf[1] + Uf[2] * sf[2];
+      double krc[3] = {0, 0, 0};
+      if (!skip_nonortho && !P.rhie_chow_dual) {
+        double k[3];
+        kfactor_limited(sf, d_on, P.pressure_min_cos_theta, k);
+        if (dot3(k, k) >= NONORTHO_SIN2_TOL * dot3(sf, sf)) for (int j = 0; j < 3; ++j) krc[j] = k[j];
+      }
+      double gm[3], smk[3];
+      for (int j = 0; j < 3; ++j) { gm[j] = gcf * gp_rc[3 * o + j] + (1.0 - gcf) * gp_rc[3 * n + j]; smk[j] = sf[j] - krc[j]; }
+      double rc = dot3(gm, smk) - ps_coeff[i] * (phi_prev[n] - phi_prev[o]);
+      flux = flux + dt * rc;
+      face_flux[fm] = flux;
+      built[fm] = 1;
+      rhs_p[o] -= flux;
+      rhs_p[n] += flux;
+    }
+    for (int64_t fb : nper_bf) {
+      int64_t fg = nfi + fb;
+      int o = m.owner[fg];
+      int bc = bc_of_face(fg);
+      double flux = is_wall(bc) ? 0.0 : dot3(&U_bnd[3 * fb], &m.sf[3 * fg]);
+      face_flux[fg] = flux;
+      built[fg] = 1;
+      rhs_p[o] -= flux;
+    }
+    for (int64_t fb : per_bf) {
+      int64_t fg = nfi + fb;
+      if (built[fg]) continue;
+      int o = m.owner[fg];
+      int pb = m.periodic_pair[fb];
+      if (pb >= 0 && built[nfi + pb]) {
+        face_flux[fg] = -face_flux[nfi + pb];
+        built[fg] = 1;
+        continue;
+      }
+      int npr = pb >= 0 ? m.owner[nfi + pb] : -1;
+      if (npr >= 0) {
+        double s = 0;
+        for (int k = 0; k < 3; ++k) s += (U[3 * o + k] + U[3 * npr + k]) * m.sf[3 * fg + k];
+        face_flux[fg] = 0.5 * s;
+      } else {
+        face_flux[fg] = dot3(&U[3 * o], &m.sf[3 * fg]);
+      }
+      built[fg] = 1;
+    }
+    double rdt = 1.0 / std::max(dt, SMALL);
+    for (int64_t c = 0; c < nc; ++c) rhs_p[c] *= rdt;
+    if (!skip_nonortho) {
+      for (int64_t i = 0; i < nfp; ++i) {
+        if (ps_skip[i] || !act_int[i]) continue;
+        int o = ps_owner[i], n = ps_nb[i];
+        int64_t fm = ps_mesh[i];
+        double gw = fm >= nfi ? m.periodic_gc[fm - nfi] : m.gc[fm];
+        double cross = 0;
+        for (int j = 0; j < 3; ++j) cross += (gw * gp[3 * o + j] + (1.0 - gw) * gp[3 * n + j]) * k_int[3 * i + j];
+        rhs_p[o] += cross;
+        rhs_p[n] -= cross;
+      }
+      for (size_t ib = 0; ib < nper_bf.size(); ++ib) {
+        int64_t fg = nfi + nper_bf[ib];
+        if (bc_of_face(fg) != BC_OUTLET || !act_bnd[ib]) continue;
+        int o = m.owner[fg];
+        rhs_p[o] += dot3(&gp[3 * o], &k_bnd[3 * ib]);
+      }
+    }
+  }
+
+  // src/solver/mod_fv_solver.f90:2756-2902
+  void correct_face_fluxes(double dt, bool ptot) {
+    for (int64_t i = 0; i < nfp; ++i) {
+      if (ps_skip[i]) continue;
+      int o = ps_owner[i], n = ps_nb[i];
+      int64_t fm = ps_mesh[i];
+      face_flux[fm] = face_flux[fm] - dt * ps_coeff[i] * (p[n] - p[o]);
+      if (act_int[i]) {
+        double g = fm >= nfi ? m.periodic_gc[fm - nfi] : m.gc[fm];
+        double cross = 0;
+        for (int j = 0; j < 3; ++j) cross += (g * gp[3 * o + j] + (1.0 - g) * gp[3 * n + j]) * k_int[3 * i + j];
+        face_flux[fm] = face_flux[fm] - dt * cross;
+      }
+    }
+    for (size_t ib = 0; ib < nper_bf.size(); ++ib) {
+      int64_t fb = nper_bf[ib], fg = nfi + fb;
+      if (bc_of_face(fg) != BC_OUTLET) continue;
+      int o = m.owner[fg];
+      double d[3];
+      for (int k = 0; k < 3; ++k) d[k] = m.centre[3 * fg + k] - m.centroid[3 * o + k];
+      double dor = std::max(std::fabs(dot3(d, &m.normal[3 * fg])), SMALL);
+      double coeff = m.area[fg] / dor;
+      double pv = ptot ? pc[m.patch[fg]].p_val : 0.0;
+      face_flux[fg] = face_flux[fg] - dt * coeff * (pv - p[o]);
+      if (act_bnd[ib]) face_flux[fg] = face_flux[fg] - dt * dot3(&gp[3 * o], &k_bnd[3 * ib]);
+    }
+    for (int64_t fb : per_bf) {
+      int pb = m.periodic_pair[fb];
+      if (pb < 0) continue;
+      int os = m.owner[nfi + fb], op = m.owner[nfi + pb];
+      if (os == op) continue;
+      if (os > op) face_flux[nfi + fb] = -face_flux[nfi + pb];
+    }
+  }
+
+  // src/solver/mod_fv_solver.f90:2927-3151
+  void correct_velocity(double dt, bool with_cross, bool ptot) {
+    bool do_cross = with_cross && !skip_nonortho;
+    std::fill(gp_cell.begin(), gp_cell.end(), 0.0);
+    for (int64_t i = 0; i < nfp; ++i) {
+      if (ps_skip[i]) continue;
+      int o = ps_owner[i], n = ps_nb[i];
+      int64_t fm = ps_mesh[i];
+      double g = ps_coeff[i] * (p[n] - p[o]);
+      if (do_cross && act_int[i]) {
+        double gw = fm >= nfi ? m.periodic_gc[fm - nfi] : m.gc[fm];
+        double cross = 0;
+        for (int j = 0; j < 3; ++j) cross += (gw * gp[3 * o + j] + (1.0 - gw) * gp[3 * n + j]) * k_int[3 * i + j];
+        g = g + cross;
+      }
+      const double* nh = &m.normal[3 * fm];
+      for (int k = 0; k < 3; ++k) gp_cell[3 * o + k] = gp_cell[3 * o + k] + g * nh[k];
+      for (int k = 0; k < 3; ++k) gp_cell[3 * n + k] = gp_cell[3 * n + k] + g * nh[k];
+    }
+    for (size_t ib = 0; ib < nper_bf.size(); ++ib) {
+      int64_t fg = nfi + nper_bf[ib];
+      if (bc_of_face(fg) != BC_OUTLET) continue;
+      int o = m.owner[fg];
+      double d[3];
+      for (int k = 0; k < 3; ++k) d[k] = m.centre[3 * fg + k] - m.centroid[3 * o + k];
+      double dor = std::max(std::fabs(dot3(d, &m.normal[3 * fg])), SMALL);
+      double coeff = m.area[fg] / dor;
+      double g = coeff * ((ptot ? pc[m.patch[fg]].p_val : 0.0) - p[o]);
+      if (do_cross && act_bnd[ib]) g = g + dot3(&gp[3 * o], &k_bnd[3 * ib]);
+      for (int k = 0; k < 3; ++k) gp_cell[3 * o + k] = gp_cell[3 * o + k] + g * m.normal[3 * fg + k];
+    }
+    if (!do_cross) {
+      double bb = P.boussinesq ? P.beta : 0.0;
+      for (int64_t fb : nper_bf) {
+        int64_t fg = nfi + fb;
+        if (bc_of_face(fg) == BC_OUTLET) continue;
+        int o = m.owner[fg];
+        double d[3];
+        for (int k = 0; k < 3; ++k) d[k] = P.f_const[k] - bb * (T[o] - P.T_ref) * P.g[k];
+        const double* nh = &m.normal[3 * fg];
+        double fn = (d[0] * nh[0] + d[1] * nh[1] + d[2] * nh[2]) * m.area[fg];
+        for (int k = 0; k < 3; ++k) gp_cell[3 * o + k] = gp_cell[3 * o + k] + fn * nh[k];
+      }
+    }
+    for (int64_t c = 0; c < nc; ++c) {
+      const double* Ti = &Tinv[9 * c];
+      double* g = &gp_cell[3 * c];
+      double g1 = Ti[0] * g[0] + Ti[3] * g[1] + Ti[6] * g[2];
+      double g2 = Ti[1] * g[0] + Ti[4] * g[1] + Ti[7] * g[2];
+      double g3 = Ti[2] * g[0] + Ti[5] * g[1] + Ti[8] * g[2];
+      g[0] = g1; g[1] = g2; g[2] = g3;
+      U[3 * c] = U[3 * c] - dt * g1;
+      U[3 * c + 1] = U[3 * c + 1] - dt * g2;
+      U[3 * c + 2] = U[3 * c + 2] - dt * g3;
+    }
+  }
+
+  // src/solver/mod_fv_solver.f90:3610-3641
+  void anchor_pressure() {
+    if (n_outlet > 0) return;
+    double s = 0.0;
+    for (int64_t c = 0; c < nc; ++c) s += p[c] * m.volume[c];
+    double shift = V_total > 0.0 ? s / V_total : 0.0;
+    for (int64_t c = 0; c < nc; ++c) p[c] = p[c] - shift;
+  }
+
+  // ---------------------------------------------------------------- Poisson solve
+  void matvec(const double* x, double* y) const {
+#pragma omp parallel for schedule(static) num_threads(nthreads)
+    for (int64_t r = 0; r < nc; ++r) {
+      double s = 0.0;
+      for (int64_t k = A_off[r]; k < A_off[r + 1]; ++k) s += A_val[k] * x[A_col[k]];
+      y[r] = s;
+    }
+  }
+  double vdot(const double* a, const double* b) const {
+    double s = 0.0;
+#pragma omp parallel for schedule(static) reduction(+ : s) num_threads(nthreads)
+    for (int64_t i = 0; i < nc; ++i) s += a[i] * b[i];
+    return s;
+  }
+  void remove_mean(double* v) const {  // MatNullSpaceRemove with the constant vector
+    double s = 0.0;
+    for (int64_t i = 0; i < nc; ++i) s += v[i];
+    double mn = s / (double)nc;
+    for (int64_t i = 0; i < nc; ++i) v[i] -= mn;
+  }
+
+  // PETSc KSPSolve_CG with KSP_NORM_UNPRECONDITIONED and a Jacobi PC (x: guess in, solution
+  // out).  Returns the KSPConvergedReason; *its and *rnorm as KSPGetIterationNumber / true residual.
+  int cg(const double* b_in, double* x, double rtol, double atol, int maxit, bool guess_zero, int* its, double* resid) {
+    const bool nullsp = dir_rows.empty();
+    std::vector<double> b(b_in, b_in + nc), r(nc), z(nc), pv(nc), w(nc);
+    if (nullsp) remove_mean(b.data());
+    if (guess_zero) std::fill(x, x + nc, 0.0);
+    matvec(x, r.data());
+    for (int64_t i = 0; i < nc; ++i) r[i] = b[i] - r[i];
+    double dp = std::sqrt(vdot(r.data(), r.data()));
+    double rnorm0;
+    if (!guess_zero) {
+      double sn = std::sqrt(vdot(b.data(), b.data()));
+      rnorm0 = sn == 0.0 ? dp : sn;
+    } else {
+      rnorm0 = dp;
+    }
+    double ttol = std::max(rtol * rnorm0, atol);
+    const double divtol = 1.0e5;
+    int reason = 0;
+    *its = 0;
+    auto converged = [&](double rn) {
+      if (!finite(rn)) return -9;
+      if (rn <= ttol) return rn < atol ? 3 : 2;
+      if (rn >= divtol * rnorm0) return -4;
+      return 0;
+    };
+    reason = converged(dp);
+    if (!reason) {
+      auto pcapply = [&]() {
+        for (int64_t i = 0; i < nc; ++i) z[i] = r[i] / A_val_diag(i);
+        if (nullsp) remove_mean(z.data());
+      };
+      pcapply();
+      double beta = vdot(z.data(), r.data()), betaold = 0.0, dpi = 0.0, dpiold;
+      int i = 0;
+      do {
+        *its = i + 1;
+        if (beta == 0.0) { reason = 3; break; }
+        if (i > 0 && beta * betaold < 0.0) { reason = -8; break; }
+        if (i == 0) {
+          pv = z;
+        } else {
+          double bb = beta / betaold;
+          for (int64_t k = 0; k < nc; ++k) pv[k] = z[k] + bb * pv[k];
+        }
+        dpiold = dpi;
+        matvec(pv.data(), w.data());
+        dpi = vdot(pv.data(), w.data());
+        betaold = beta;
+        if (dpi == 0.0 || (i > 0 && ((dpi > 0) - (dpi < 0)) * ((dpiold > 0) - (dpiold < 0)) < 0)) {
+          reason = dpi == 0.0 ? 3 : -10;
+          break;
+        }
+        double a = beta / dpi;
+        for (int64_t k = 0; k < nc; ++k) { x[k] += a * pv[k]; r[k] -= a * w[k]; }
+        dp = std::sqrt(vdot(r.data(), r.data()));
+        reason = converged(dp);
+        if (reason) break;
+        pcapply();
+        beta = vdot(z.data(), r.data());
+        i++;
+      } while (i < maxit);
+      if (!reason && i >= maxit) reason = -3;
+    }
+    // true residual with the caller's right-hand side (KSPBuildResidual)
+    matvec(x, w.data());
+    double s = 0.0;
+    for (int64_t k = 0; k < nc; ++k) { double d = b_in[k] - w[k]; s += d * d; }
+    *resid = std::sqrt(s);
+    return reason;
+  }
+  double A_val_diag(int64_t r) const {
+    for (int64_t k = A_off[r]; k < A_off[r + 1]; ++k)
+      if (A_col[k] == r) return A_val[k];
+    return 1.0;
+  }
+
+  // src/solver/mod_pressure_solver.f90:638-806 + pressure_backend_petsc.c:648-1034
+  int pressure_solve(double tol, double atol, bool ptot, int* its_out, double* res_out) {
+    std::vector<double> rw(rhs_p), pw(p.begin(), p.end());
+    for (int64_t i = 0; i < nc; ++i) {
+      if (!finite(rw[i])) rw[i] = 0.0;
+      if (!finite(pw[i])) pw[i] = 0.0;
+    }
+    if (ptot)
+      for (size_t k = 0; k < dir_rows.size(); ++k) rw[dir_rows[k]] += dir_vals[k];
+    int maxit = std::max(P.p_max_iter, 2000);
+    int its;
+    double res;
+    int reason = cg(rw.data(), pw.data(), tol, atol, maxit, false, &its, &res);
+    if (reason < 0) {
+      reason = cg(rw.data(), pw.data(), tol, atol, 4 * maxit, true, &its, &res);
+      if (reason < 0 && !(reason == -3 && (res < tol * 1.0e4 || res < atol * 1.0e3))) return -(1000 + reason);
+    }
+    for (int64_t i = 0; i < nc; ++i) p[i] = pw[i];
+    *its_out = its;
+    *res_out = res;
+    return 0;
+  }
+
+  double atol_dynamic(double dt) const {
+    double u1 = 0.0, u2 = 0.0;
+    for (int64_t c = 0; c < nc; ++c) {
+      u1 += std::sqrt(U[3 * c] * U[3 * c] + U[3 * c + 1] * U[3 * c + 1] + U[3 * c + 2] * U[3 * c + 2]) * m.volume[c];
+      u2 += m.volume[c];
+    }
+    double us = u1 / std::max(u2, SMALL);
+    return std::max(1.0e-12 * std::max(us, 1.0) * V_min / dt, p_atol_factor);
+  }
+
+  // src/solver/mod_fv_solver.f90:837-918
+  int project_once(double dt) {
+    std::fill(rhs_p.begin(), rhs_p.end(), 0.0);
+    std::fill(phi_prev.begin(), phi_prev.end(), 0.0);
+    std::fill(phi_prev_bnd.begin(), phi_prev_bnd.end(), 0.0);
+    std::fill(gp_rc.begin(), gp_rc.end(), 0.0);
+    refresh_halos_and_bc();
+    face_fluxes_and_rhs(dt, false);
+    if (P.p_max_iter > 0) {
+      int its;
+      double res;
+      int rc = pressure_solve(P.p_tol, atol_dynamic(dt), true, &its, &res);
+      if (rc) return rc;
+    }
+    anchor_pressure();
+    correct_face_fluxes(dt, true);
+    U_face = face_flux;
+    u_face_ready = true;
+    apply_pressure_bc(p.data(), -1, false, false);
+    correct_velocity(dt, true, true);
+    apply_velocity_bc(-1, false);
+    if (P.use_rotational_projection) {
+      for (int64_t c = 0; c < nc; ++c) p[c] = p[c] + (P.nu + nu_sgs[c]) * rhs_p[c] * dt * inv_vol[c];
+      apply_pressure_bc(p.data(), -1, false, false);
+    }
+    p_old = p;
+    phi_prev = p;
+    phi_prev_bnd = p_bnd;
+    apply_pressure_bc(p.data(), -1, false, false);
+    compute_pressure_gradient();
+    return 0;
+  }
+
+  // src/solver/mod_fv_solver.f90:3718-3871
+  void cfl_rates(double& conv, double& diff) const {
+    std::vector<double> fs(nc, 0.0), ds(nc, 0.0);
+    for (int64_t f = 0; f < nf; ++f) {
+      int o = m.owner[f], n = m.neighbour[f];
+      const double* sf = &m.sf[3 * f];
+      double area = std::sqrt(sf[0] * sf[0] + sf[1] * sf[1] + sf[2] * sf[2]);
+      double uf = u_face_ready ? U_face[f] : dot3(&U[3 * o], sf);
+      fs[o] += std::fabs(uf);
+      if (n >= 0) fs[n] += std::fabs(uf);
+      double w = area / std::max(m.d_cf[f], SMALL);
+      if (n >= 0) {
+        double g = m.gc[f];
+        double ne = P.nu + g * std::max(0.0, nu_sgs[o]) + (1.0 - g) * std::max(0.0, nu_sgs[n]);
+        ds[o] += ne * w;
+        ds[n] += ne * w;
+      } else if (bc_of_face(f) != BC_WALL_MODEL) {
+        ds[o] += (P.nu + std::max(0.0, nu_sgs[o])) * w;
+      }
+    }
+    conv = 0.0; diff = 0.0;
+    for (int64_t c = 0; c < nc; ++c) {
+      conv = std::max(conv, fs[c] / (m.volume[c] + SMALL));
+      diff = std::max(diff, ds[c] / (m.volume[c] + SMALL));
+    }
+  }
+  int compute_dt(double& dt) const {
+    double cr, dr;
+    cfl_rates(cr, dr);
+    double dc = 1e308, dd = 1e308;
+    if (cr > SMALL) dc = P.cfl_max / cr;
+    if (dr > SMALL) dd = 1.0 / dr;
+    dt = std::min(dc, dd);
+    if (!(dt > 0.0)) dt = P.dt;
+    dt = std::min(dt, P.dt);
+    double dmin = 1.0e-6 * P.dt;
+    if (!(dt > 0.0)) dt = P.dt;
+    else if (dt < dmin) return DPM_ERR_DT_COLLAPSE;
+    return 0;
+  }
+
+  // src/solver/mod_fv_solver.f90:920-958 + advance_rk3w :1180-1614
+  int advance(double dt_in) {
+    double dt = dt_in;
+    if (!P.adapt_dt) {
+      double ds;
+      int rc = compute_dt(ds);
+      if (rc) return rc;
+      if (dt > ds) dt = ds;
+    }
+    last_dt = dt;
+    last_solves = 0; last_iters = 0; last_resid = 0.0;
+    std::fill(H_U.begin(), H_U.end(), 0.0);
+    std::fill(rhs_p.begin(), rhs_p.end(), 0.0);
+    std::fill(H_U0.begin(), H_U0.end(), 0.0);
+    double time_n = time;
+    for (int k = 0; k < 3; ++k) {
+      double gk_dt = RK3W_GAMMA[k] * dt;
+      time = time_n + RK3W_C[k] * dt;
+      refresh_halos_and_bc();
+      compute_all_gradients();
+      sgs_viscosity(gk_dt);
+      if (P.wall_model == DPM_WM_NONE) std::fill(tau_w.begin(), tau_w.end(), 0.0);
+      else wall_model(k == 0 ? dt : 0.0);
+      explicit_rhs();
+      double a_k = RK3W_ALPHA[k], b_k = RK3W_BETA[k];
+      for (int64_t c = 0; c < nc; ++c)
+        for (int j = 0; j < 3; ++j) U[3 * c + j] = U[3 * c + j] + dt * (a_k * H_U[3 * c + j] + b_k * H_U0[3 * c + j]);
+      velocity_bc_refresh();
+      p_old = p;
+      correct_velocity(gk_dt, false, true);
+      gp_rc = gp_cell;
+      velocity_bc_refresh();
+      compute_all_gradients();
+      phi_prev = p;
+      phi_prev_bnd = p_bnd;
+      // Poisson block with non-orthogonal correctors
+      double atol = atol_dynamic(gk_dt);
+      int n_max;
+      double stag;
+      if (diag_interface) { n_max = std::min(P.n_nonortho_corr, 8); stag = 0.99; }
+      else { n_max = std::min(P.n_nonortho_corr, 3); stag = 0.9; }
+      double dprev = 1e308, dphi_prev = 1e308;
+      if (P.nonortho_check) {
+        n_max = std::min(P.n_nonortho_corr, 8);
+        std::fill(phi_it.begin(), phi_it.end(), 0.0);
+      }
+      for (int jno = 1; jno <= n_max; ++jno) {
+        face_fluxes_and_rhs(gk_dt, jno > 1);
+        double dcur = 0.0;
+        for (int64_t c = 0; c < nc; ++c) dcur = std::max(dcur, std::fabs(rhs_p[c]));
+        if (jno == 1) std::fill(p.begin(), p.end(), 0.0);
+        int its;
+        double res;
+        int rc = pressure_solve(P.p_tol, atol, false, &its, &res);
+        if (rc) return rc;
+        last_solves++;
+        last_iters += its;
+        last_resid = std::max(last_resid, res);
+        apply_pressure_bc(p.data(), 0, !skip_grad_p, true);
+        apply_pressure_bc(p.data(), 1, false, false);
+        if (P.nonortho_check) {
+          double dd = 0.0, dpp = 0.0;
+          for (int64_t c = 0; c < nc; ++c) {
+            dd = std::max(dd, std::fabs(p[c] - phi_it[c]));
+            dpp = std::max(dpp, std::fabs(p[c]));
+            phi_it[c] = p[c];
+          }
+          if (jno > 1 && (dd < NONORTHO_PHI_TOL * dpp || dd > dphi_prev * stag)) break;
+          dphi_prev = dd;
+        } else if (jno > 1 && (dcur < atol || dcur > dprev * stag)) {
+          break;
+        }
+        dprev = dcur;
+      }
+      correct_face_fluxes(gk_dt, false);
+      U_face = face_flux;
+      u_face_ready = true;
+      correct_velocity(gk_dt, true, false);
+      velocity_bc_refresh();
+      if (P.use_rotational_projection) {
+        for (int64_t c = 0; c < nc; ++c) p[c] = p[c] + (P.nu + nu_sgs[c]) * rhs_p[c] * gk_dt * inv_vol[c];
+        apply_pressure_bc_o2(true);
+        apply_pressure_bc(p.data(), 1, false, false);
+      }
+      for (int64_t c = 0; c < nc; ++c) p[c] = p[c] + p_old[c];
+      anchor_pressure();
+      apply_pressure_bc_o2(false);
+      apply_pressure_bc(p.data(), 1, false, false);
+      compute_pressure_gradient();
+      H_U0 = H_U;
+    }
+    time = time_n + dt;
+    step++;
+    return 0;
+  }
+
+  // src/stats/mod_stats.f90:271-336 + mod_fv_solver.f90:3643-3716
+  void stats(dpm_stats_t* s) {
+    double sums[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, umax = 0.0;
+    for (int64_t c = 0; c < nc; ++c) {
+      double v = m.volume[c];
+      const double* u = &U[3 * c];
+      const double* g = &grad_U[9 * c];
+      sums[0] += 0.5 * (u[0] * u[0] + u[1] * u[1] + u[2] * u[2]) * v;
+      sums[1] += v;
+      double S11 = g[0], S22 = g[4], S33 = g[8];
+      double S12 = 0.5 * (g[1] + g[3]), S13 = 0.5 * (g[2] + g[6]), S23 = 0.5 * (g[5] + g[7]);
+      double SS = S11 * S11 + S22 * S22 + S33 * S33 + 2.0 * (S12 * S12 + S13 * S13 + S23 * S23);
+      sums[2] += (P.nu + nu_sgs[c]) * SS * v;
+      for (int k = 0; k < 3; ++k) sums[3 + k] += u[k] * v;
+      sums[6] += nu_sgs[c] * v;
+      umax = std::max(umax, std::sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]));
+    }
+    for (int q = 0; q < m.n_patches; ++q) {
+      if (pc[q].bc_id != BC_WALL_MODEL) continue;
+      for (int64_t f = 0; f < m.patch_nfaces[q]; ++f) {
+        int64_t fb = m.patch_start[q] + f;
+        const double* t = &tau_w[3 * fb];
+        sums[7] += std::sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]) * m.area[nfi + fb];
+        sums[8] += m.area[nfi + fb];
+      }
+    }
+    s->time = time;
+    s->E = sums[0] / sums[1];
+    s->eps = 2.0 * sums[2] / sums[1];
+    double mb[3] = {sums[3] / sums[1], sums[4] / sums[1], sums[5] / sums[1]};
+    s->Ub = std::sqrt(mb[0] * mb[0] + mb[1] * mb[1] + mb[2] * mb[2]);
+    s->nu_sgs_mean = sums[6] / sums[1];
+    s->tauw_mean = sums[8] > SMALL ? sums[7] / sums[8] : 0.0;
+    s->Umax = umax;
+    // face-flux divergence
+    std::vector<double> div(nc, 0.0);
+    for (int64_t i = 0; i < nfp; ++i) {
+      if (ps_skip[i]) continue;
+      int o = ps_owner[i], n = ps_nb[i];
+      double fl = face_flux[ps_mesh[i]];
+      div[o] += fl * inv_vol[o];
+      div[n] -= fl * inv_vol[n];
+    }
+    for (int64_t fb : nper_bf) {
+      int o = m.owner[nfi + fb];
+      div[o] += face_flux[nfi + fb] * inv_vol[o];
+    }
+    double mx = 0.0, as = 0.0, vs = 0.0;
+    for (int64_t c = 0; c < nc; ++c) {
+      mx = std::max(mx, std::fabs(div[c]));
+      as += std::fabs(div[c]) * m.volume[c];
+      vs += m.volume[c];
+    }
+    s->max_abs_divU = mx;
+    s->volavg_abs_divU = as / vs;
+    s->dt_used = last_dt;
+    s->p_solves = last_solves;
+    s->p_iters = last_iters;
+    s->p_resid_max = last_resid;
+    apply_velocity_bc(-1, false);  // solver_divergence_metrics refreshes U_bnd without gradients
+  }
+};
+
+}  // namespace orc
+
+// ------------------------------------------------------------------------------------------
+// C entry points used by the tests (ctypes) and by the CPU-baseline leg of bench.py.
+extern "C" {
+
+void* orc_create(const dpm_raw_mesh_t* raw, const dpm_patch_cfg_t* patches, const dpm_params_t* prm, int nthreads) {
+  auto* s = new orc::Solver();
+  s->nthreads = nthreads > 0 ? nthreads : 1;
+  std::string err;
+  if (s->init(raw, patches, prm, &err)) {
+    std::fprintf(stderr, "orc_create: %s\n", err.c_str());
+    delete s;
+    return nullptr;
+  }
+  return s;
+}
+void orc_destroy(void* h) { delete static_cast<orc::Solver*>(h); }
+void orc_sizes(void* h, int64_t* out) {
+  auto* s = static_cast<orc::Solver*>(h);
+  out[0] = s->nc; out[1] = s->nf; out[2] = s->nfi; out[3] = s->nb; out[4] = s->nfp;
+  out[5] = s->skip_nonortho; out[6] = s->skip_grad_p; out[7] = s->diag_interface;
+}
+void orc_geometry(void* h, double* centroid, double* volume) {
+  auto* s = static_cast<orc::Solver*>(h);
+  if (centroid) std::memcpy(centroid, s->m.centroid.data(), sizeof(double) * 3 * s->nc);
+  if (volume) std::memcpy(volume, s->m.volume.data(), sizeof(double) * s->nc);
+}
+void orc_vertex_bounds(void* h, double* lo, double* hi) {
+  auto* s = static_cast<orc::Solver*>(h);
+  for (int k = 0; k < 3; ++k) { lo[k] = 1e308; hi[k] = -1e308; }
+  for (int64_t v = 0; v < s->m.n_vertices; ++v)
+    for (int k = 0; k < 3; ++k) {
+      lo[k] = std::min(lo[k], s->m.vertices[3 * v + k]);
+      hi[k] = std::max(hi[k], s->m.vertices[3 * v + k]);
+    }
+}
+void orc_set_state(void* h, const double* U, const double* p, const double* T) {
+  auto* s = static_cast<orc::Solver*>(h);
+  if (U) std::memcpy(s->U.data(), U, sizeof(double) * 3 * s->nc);
+  if (p) std::memcpy(s->p.data(), p, sizeof(double) * s->nc);
+  if (T) std::memcpy(s->T.data(), T, sizeof(double) * s->nc);
+}
+void orc_get_state(void* h, double* U, double* p, double* nu_sgs, double* grad_U, double* face_flux) {
+  auto* s = static_cast<orc::Solver*>(h);
+  if (U) std::memcpy(U, s->U.data(), sizeof(double) * 3 * s->nc);
+  if (p) std::memcpy(p, s->p.data(), sizeof(double) * s->nc);
+  if (nu_sgs) std::memcpy(nu_sgs, s->nu_sgs.data(), sizeof(double) * s->nc);
+  if (grad_U) std::memcpy(grad_U, s->grad_U.data(), sizeof(double) * 9 * s->nc);
+  if (face_flux) std::memcpy(face_flux, s->U_face.data(), sizeof(double) * s->nf);
+}
+int orc_project_once(void* h, double dt) { return static_cast<orc::Solver*>(h)->project_once(dt); }
+int orc_advance(void* h, double dt) { return static_cast<orc::Solver*>(h)->advance(dt); }
+void orc_stats(void* h, dpm_stats_t* out) { static_cast<orc::Solver*>(h)->stats(out); }
+double orc_time(void* h) { return static_cast<orc::Solver*>(h)->time; }
+int orc_compute_dt(void* h, double* dt) { return static_cast<orc::Solver*>(h)->compute_dt(*dt); }
+
+// Single-operator checks on arbitrary inputs (same arguments as the product's dpm_* operators).
+void orc_ls_gradient_vector(void* h, const double* U, const double* U_bnd, double* g) {
+  static_cast<orc::Solver*>(h)->ls_gradient_vector(U, U_bnd, g);
+}
+void orc_advection(void* h, int scheme, const double* U, const double* U_bnd, const double* flux, const double* gU,
+                   double* rhs) {
+  auto* s = static_cast<orc::Solver*>(h);
+  std::memcpy(s->U.data(), U, sizeof(double) * 3 * s->nc);
+  std::memcpy(s->U_bnd.data(), U_bnd, sizeof(double) * 3 * s->nb);
+  std::memcpy(s->U_face.data(), flux, sizeof(double) * s->nf);
+  std::memcpy(s->grad_U.data(), gU, sizeof(double) * 9 * s->nc);
+  int keep = s->P.scheme;
+  s->P.scheme = scheme;
+  s->advection(rhs);
+  s->P.scheme = keep;
+}
+void orc_viscous(void* h, const double* U, const double* nu_sgs, const double* gU, const double* U_bnd, double* rhs) {
+  auto* s = static_cast<orc::Solver*>(h);
+  std::memcpy(s->U.data(), U, sizeof(double) * 3 * s->nc);
+  std::memcpy(s->nu_sgs.data(), nu_sgs, sizeof(double) * s->nc);
+  std::memcpy(s->grad_U.data(), gU, sizeof(double) * 9 * s->nc);
+  std::memcpy(s->U_bnd.data(), U_bnd, sizeof(double) * 3 * s->nb);
+  s->viscous(rhs);
+}
+void orc_sgs(void* h, int model, const double* gU, const double* U, double dt_stab, double* nu) {
+  auto* s = static_cast<orc::Solver*>(h);
+  std::memcpy(s->grad_U.data(), gU, sizeof(double) * 9 * s->nc);
+  std::memcpy(s->U.data(), U, sizeof(double) * 3 * s->nc);
+  int keep = s->P.sgs_model;
+  s->P.sgs_model = model;
+  s->sgs_viscosity(dt_stab);
+  s->P.sgs_model = keep;
+  std::memcpy(nu, s->nu_sgs.data(), sizeof(double) * s->nc);
+}
+void orc_wall_model(void* h, const double* U, double* tau) {
+  auto* s = static_cast<orc::Solver*>(h);
+  std::memcpy(s->U.data(), U, sizeof(double) * 3 * s->nc);
+  s->wall_model(0.0);
+  std::memcpy(tau, s->tau_w.data(), sizeof(double) * 3 * s->nb);
+}
+double orc_amd_point(const double* alpha, const double* G, double c_amd) { return orc::amd_point(alpha, G, c_amd); }
+void orc_wall_stress_newton(double u_par, double y_w, double nu, double* u_tau, double* tau) {
+  bool capped;
+  orc::wall_stress_newton(u_par, y_w, nu, *u_tau, *tau, capped);
+}
+// Plain PETSc-semantics CG on the handle's assembled Poisson operator.
+int orc_poisson_solve(void* h, const double* rhs, double* x, double rtol, double atol, int maxit, int* its, double* res) {
+  auto* s = static_cast<orc::Solver*>(h);
+  return s->cg(rhs, x, rtol, atol, maxit, false, its, res);
+}
+void orc_poisson_matvec(void* h, const double* x, double* y) { static_cast<orc::Solver*>(h)->matvec(x, y); }
+}

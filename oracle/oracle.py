@@ -1,0 +1,123 @@
+"""ORACLE — test infrastructure only (the parity checker and the timed CPU baseline).
+
+ctypes binding of oracle/oracle.cpp, the CPU restatement of the reference's RK3W time step.
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may use this module.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from dopamine_b200 import abi
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
+_lib = None
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        vp, dp, ip = C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int)
+        L.orc_create.restype = vp
+        L.orc_create.argtypes = [C.POINTER(abi.RawMeshT), C.POINTER(abi.PatchCfgT), C.POINTER(abi.ParamsT), C.c_int]
+        L.orc_destroy.argtypes = [vp]
+        L.orc_sizes.argtypes = [vp, C.POINTER(C.c_int64)]
+        L.orc_geometry.argtypes = [vp, dp, dp]
+        L.orc_vertex_bounds.argtypes = [vp, dp, dp]
+        L.orc_set_state.argtypes = [vp, dp, dp, dp]
+        L.orc_get_state.argtypes = [vp, dp, dp, dp, dp, dp]
+        L.orc_project_once.argtypes = [vp, C.c_double]
+        L.orc_project_once.restype = C.c_int
+        L.orc_advance.argtypes = [vp, C.c_double]
+        L.orc_advance.restype = C.c_int
+        L.orc_stats.argtypes = [vp, C.POINTER(abi.StatsT)]
+        L.orc_time.argtypes = [vp]
+        L.orc_time.restype = C.c_double
+        L.orc_compute_dt.argtypes = [vp, dp]
+        L.orc_compute_dt.restype = C.c_int
+        L.orc_ls_gradient_vector.argtypes = [vp, dp, dp, dp]
+        L.orc_advection.argtypes = [vp, C.c_int, dp, dp, dp, dp, dp]
+        L.orc_viscous.argtypes = [vp, dp, dp, dp, dp, dp]
+        L.orc_sgs.argtypes = [vp, C.c_int, dp, dp, C.c_double, dp]
+        L.orc_wall_model.argtypes = [vp, dp, dp]
+        L.orc_amd_point.argtypes = [dp, dp, C.c_double]
+        L.orc_amd_point.restype = C.c_double
+        L.orc_wall_stress_newton.argtypes = [C.c_double, C.c_double, C.c_double, dp, dp]
+        L.orc_poisson_solve.argtypes = [vp, dp, dp, C.c_double, C.c_double, C.c_int, ip, dp]
+        L.orc_poisson_solve.restype = C.c_int
+        L.orc_poisson_matvec.argtypes = [vp, dp, dp]
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class Oracle:
+    """CPU FVSolver restatement on one case (dopamine_b200.cases.Case)."""
+
+    def __init__(self, case, nthreads=1, params=None):
+        L = lib()
+        self.case = case
+        self._mesh = abi.RawMeshView(case.mesh)
+        self._patches = abi.patch_cfgs(case.patches)
+        self._params = params if params is not None else case.make_params()
+        self.h = L.orc_create(C.byref(self._mesh.struct), self._patches, C.byref(self._params), nthreads)
+        if not self.h:
+            raise RuntimeError("oracle mesh set-up failed")
+        sz = (C.c_int64 * 8)()
+        L.orc_sizes(self.h, sz)
+        self.nc, self.nf, self.nfi, self.nb, self.nfp = (int(sz[i]) for i in range(5))
+        self.skip_nonortho, self.skip_grad_p, self.diag_interface = bool(sz[5]), bool(sz[6]), bool(sz[7])
+        self.centroid = np.zeros((self.nc, 3))
+        self.volume = np.zeros(self.nc)
+        L.orc_geometry(self.h, _p(self.centroid), _p(self.volume))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_destroy(self.h)
+            self.h = None
+
+    def set_state(self, U=None, p=None, T=None):
+        U = None if U is None else np.ascontiguousarray(U, dtype=np.float64)
+        p = None if p is None else np.ascontiguousarray(p, dtype=np.float64)
+        T = None if T is None else np.ascontiguousarray(T, dtype=np.float64)
+        lib().orc_set_state(self.h, _p(U), _p(p), _p(T))
+
+    def state(self):
+        U = np.zeros((self.nc, 3)); p = np.zeros(self.nc); nu = np.zeros(self.nc)
+        g = np.zeros((self.nc, 3, 3)); ff = np.zeros(self.nf)
+        lib().orc_get_state(self.h, _p(U), _p(p), _p(nu), _p(g), _p(ff))
+        return {"U": U, "p": p, "nu_sgs": nu, "grad_U": g, "face_flux": ff}
+
+    def initialise(self):
+        """apply_initial_conditions: profile (+ noise and an extra projection) + project_once."""
+        U = self.case.initial_velocity(self.centroid)
+        self.set_state(U=U, p=np.zeros(self.nc))
+        dtp = 8.0 / 15.0 * self._params.dt
+        if self.case.noise > 0.0:
+            self._check(lib().orc_project_once(self.h, dtp))
+        self._check(lib().orc_project_once(self.h, dtp))
+
+    def advance(self, dt=None):
+        self._check(lib().orc_advance(self.h, self._params.dt if dt is None else dt))
+
+    def stats(self):
+        s = abi.StatsT()
+        lib().orc_stats(self.h, C.byref(s))
+        return s.as_dict()
+
+    @staticmethod
+    def _check(rc):
+        if rc != 0:
+            raise RuntimeError(f"oracle status {rc}")

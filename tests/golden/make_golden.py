@@ -1,0 +1,32 @@
+"""Regenerates tests/golden/*.csv: the reference's regression statistics (golden vectors) for the
+cases whose meshes are reproducible without gmsh, reduced to the columns the reference's own
+comparison uses (tests/regression/compare_stats.py: time, E, Umax, Ub, tauw_mean, nu_sgs_mean,
+max_abs_divU).  Run in a checkout that has the reference tree:
+
+    python tests/golden/make_golden.py /path/to/reference
+"""
+import csv
+import os
+import sys
+
+CASES = ("tgv", "tgv_skew", "tgv_skew_chk", "pdrop", "hydro", "hydrowall")
+COLS = ("step", "time", "E", "Umax", "Ub", "tauw_mean", "nu_sgs_mean", "max_abs_divU", "dt")
+
+
+def main(ref_root):
+    here = os.path.dirname(os.path.abspath(__file__))
+    for case in CASES:
+        src = os.path.join(ref_root, "tests", "regression", "reference", f"{case}_np1.csv")
+        with open(src, newline="") as fh:
+            rows = list(csv.DictReader(fh))
+        dst = os.path.join(here, f"{case}_np1.csv")
+        with open(dst, "w", newline="") as fh:
+            w = csv.writer(fh)
+            w.writerow(COLS)
+            for r in rows:
+                w.writerow([r[c].strip() for c in COLS])
+        print(f"{dst}: {len(rows)} rows")
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
