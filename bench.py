@@ -1,0 +1,275 @@
+#!/usr/bin/env python3
+"""Benchmark of the RK3W fractional-step hot path on B200.
+
+Default workload: the turbulent-channel configuration (96 x 64 x 64 hex cells, tanh-stretched,
+KEP advection, Vreman SGS, log-law wall model, constant pressure-gradient forcing, plain FP64
+Jacobi-PCG), synthetic inputs (seeded laminar-plus-noise initial state).  One "step" is one
+RK3W time step (three stages, three Poisson solves) of the whole mesh.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--config channel|tgv]
+
+value   : cell-steps/s with the state resident in HBM (CUDA events around K steps, max over ranks)
+e2e     : the same metric through the C ABI with host buffers: every step uploads the state
+          (U, p) from pinned host memory, advances, and reads the state back
+roofline: the Poisson PCG kernel (dominant): algorithmic bytes per launch / average launch time
+cpu_baseline: the CPU restatement of the reference step (oracle) on this host's cores, on a
+          bounded sample of the same workload.
+Multi-GPU: the north-star path is single-GPU; N GPUs run N independent replicas (weak scaling).
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cell-steps/s & Poisson ms/step, learned+mixed vs plain FP64 PCG, 1 B200"
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock and throttle-reason samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index=0):
+        self.gpu = gpu_index
+        self.samples = []
+        self._stop = threading.Event()
+        self._proc = None
+
+    def start(self):
+        try:
+            self._proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except Exception:
+            self._proc = None
+
+    def _read(self):
+        for line in self._proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.samples.append(parts)
+
+    def stop(self):
+        if self._proc:
+            self._proc.terminate()
+            try:
+                self._proc.wait(timeout=5)
+            except Exception:
+                self._proc.kill()
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": len(self.samples)}
+        if self.samples:
+            sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+            mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+            out["sm_mhz"] = statistics.median(sm) if sm else None
+            out["sm_max_mhz"] = max(mx) if mx else None
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            reasons = set()
+            for s in self.samples:
+                for k, nm in enumerate(names):
+                    if s[5 + k].lower() == "active":
+                        reasons.add(nm)
+            out["reasons"] = sorted(reasons)
+        return out
+
+
+def make_case(name):
+    from dopamine_b200 import cases
+    if name == "channel":
+        return cases.channel_config(96, 64, 64)
+    if name == "tgv":
+        return cases.tgv_config(64)
+    raise ValueError(name)
+
+
+def pcg_bytes_per_iteration(s):
+    """Algorithmic bytes of one PCG iteration (both phases), per the ELL operator width."""
+    nc = s.nc
+    wa = 7  # hex mesh: diagonal + 6 neighbours
+    phase_a = nc * (wa * (4 + 8) + 8 + 8 + 8 + 8)   # cols, vals, z, p_old, write p_new, write q
+    phase_b = nc * (5 * 8 + 3 * 8)                  # x, p, r, q, dinv in; x, r, z out
+    return phase_a + phase_b
+
+
+def run_gpu(args, rank, world):
+    import torch
+    from dopamine_b200.solver import Solver, lib
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    case = make_case(args.config)
+    s = Solver(case, device=dev)
+    s.initialise()
+    nc = s.nc
+    for _ in range(args.warmup):
+        s.advance()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(dev) if rank == 0 else None
+    if sampler:
+        sampler.start()
+    l0 = s.kernel_launches()
+    step_ms, pois_ms, its, solves = [], [], 0, 0
+    for _ in range(args.steps):
+        s.advance()
+        st = s.stats()
+        a, b = s.last_timing()
+        step_ms.append(a)
+        pois_ms.append(b)
+        its += st["p_iters"]
+        solves += st["p_solves"]
+    launches = s.kernel_launches() - l0
+    t_dev = sum(step_ms) / 1e3
+    # ---- end to end through the C ABI with host buffers
+    L = lib()
+    host = s.sync_host()
+    U = np.ascontiguousarray(host["U"])
+    p = np.ascontiguousarray(host["p"])
+    dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        rc = L.dpm_upload_state(s.h, dp(U), dp(p), None)
+        rc |= L.dpm_advance(s.h, s.params.dt)
+        rc |= L.dpm_download_state(s.h, dp(U), dp(p), None, None)
+        if rc:
+            raise RuntimeError(f"e2e step failed {rc}")
+    t_e2e = time.perf_counter() - t0
+    clocks = sampler.stop() if sampler else None
+    if world > 1:
+        t = torch.tensor([t_dev, t_e2e], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        t_dev, t_e2e = float(t[0]), float(t[1])
+    return dict(nc=nc, t_dev=t_dev, t_e2e=t_e2e, step_ms=step_ms, pois_ms=pois_ms, its=its, solves=solves,
+                launches=launches, clocks=clocks, solver=s)
+
+
+def cpu_baseline(case_name, budget_s=20.0, nthreads=None):
+    """The oracle (CPU restatement of the reference step) on this host, bounded sample."""
+    from oracle.oracle import Oracle
+    nthreads = nthreads or os.cpu_count() or 1
+    case = make_case(case_name)
+    o = Oracle(case, nthreads=nthreads)
+    o.initialise()
+    t0 = time.perf_counter()
+    steps = 0
+    while True:
+        o.advance()
+        steps += 1
+        if time.perf_counter() - t0 >= budget_s or steps >= 3:
+            break
+    dt = time.perf_counter() - t0
+    return dict(value=o.nc * steps / dt, unit="cell-steps/s", cores=nthreads, kind="port",
+                sample=f"{steps} RK3W step(s) of the {case_name} workload ({o.nc} cells) after the initial projection, "
+                       f"{dt:.1f} s, oracle with {nthreads} OpenMP threads")
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="dopamine_b200")
+    ap.add_argument("--config", default="channel")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    cfg_name = {"channel": "channel 96x64x64 Re_tau=395, KEP, Vreman, log-law wall model, FP64 Jacobi-PCG",
+                "tgv": "Taylor-Green 64^3, CDS, FP64 Jacobi-PCG"}[args.config]
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        cb = cpu_baseline(args.config, budget_s=60.0)
+        line = {
+            "impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "cell-steps/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": cfg_name, "form": "plain FP64 Jacobi-PCG (CPU restatement)"},
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": cb["value"], "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line))
+        return 0
+
+    if world > 1:
+        import torch
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    r = run_gpu(args, rank, world)
+    s = r["solver"]
+    if world > 1:
+        import torch
+        torch.distributed.barrier()
+    if rank != 0:
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return 0
+    nc, K = r["nc"], args.steps
+    value = world * nc * K / r["t_dev"]
+    e2e = world * nc * K / r["t_e2e"]
+    peak, peak_kind = measured_peaks()
+    bytes_it = pcg_bytes_per_iteration(s)
+    pois_s = sum(r["pois_ms"]) / 1e3
+    achieved = bytes_it * r["its"] / pois_s / 1e9 if pois_s > 0 else 0.0
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "pcg_traffic.json")
+    if os.path.exists(prof):
+        try:
+            traffic = json.load(open(prof)).get("dram_bytes_per_launch")
+        except Exception:
+            traffic = None
+    line = {
+        "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world, "steps": K,
+        "warmup": args.warmup, "ms_per_step": 1e3 * r["t_dev"] / K, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": cfg_name, "cells": nc, "form": "plain FP64 Jacobi-PCG",
+                   "poisson_ms_per_step": 1e3 * pois_s / K, "pcg_iterations_per_step": r["its"] / K,
+                   "poisson_solves_per_step": r["solves"] / K,
+                   "l2": "inputs larger than L2: static operator data streamed each step exceeds 126 MB",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "e2e": {"value": e2e, "unit": "cell-steps/s", "h2d_bytes_per_step": 32 * nc, "d2h_bytes_per_step": 32 * nc},
+        "roofline": {"kernel": "k_pcg (persistent Jacobi-PCG)", "bound": "hbm", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
+                     "bytes_per_iteration": bytes_it},
+        "gpu_launches": r["launches"],
+        "clocks": r["clocks"],
+    }
+    if not args.no_cpu_baseline:
+        cb = cpu_baseline(args.config, budget_s=20.0)
+        line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    print(json.dumps(line))
+    s.close()
+    if world > 1:
+        import torch
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -278,6 +278,6 @@ def channel_config(nx=96, ny=64, nz=64, n_steps=1000, retau=395.0, noise_seed=20
     dt = 0.3 * dx / (1.5 * ub)
     return Case(f"channel{nx}x{ny}x{nz}", mesh, patches,
                 dict(scheme=abi.SCHEME_KEP, sgs_model=abi.SGS_VREMAN, wall_model=abi.WM_LOGLAW,
-                     nu=nu, dt=dt, cfl_max=0.5, p_tol=1e-8, f_const=(1.0, 0.0, 0.0)),
+                     nu=nu, dt=dt, cfl_max=0.5, p_tol=1e-10, f_const=(1.0, 0.0, 0.0)),
                 "channel", 1.5 * ub, noise=0.10, noise_seed=noise_seed, n_steps=n_steps,
                 description=f"channel {nx}x{ny}x{nz} Re_tau={retau:g}, KEP, Vreman, log-law wall model")

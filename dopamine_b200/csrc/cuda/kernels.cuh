@@ -1,0 +1,1015 @@
+// Explicit-operator kernels of the RK3W step.  One thread per face or per cell; every per-cell
+// sum runs over the cell's faces in ascending face order (the order in which the reference's
+// face loop reaches the cell), so results do not depend on thread scheduling and no atomics are
+// needed.  Each kernel cites the reference routine it implements.
+#pragma once
+#include "common.cuh"
+
+namespace dpm {
+namespace gpu {
+
+__device__ __forceinline__ double dot3v(const double* a, int sa, int ia, const double* b, int sb, int ib) {
+  return a[ia] * b[ib] + a[sa + ia] * b[sb + ib] + a[2 * sa + ia] * b[2 * sb + ib];
+}
+__device__ __forceinline__ bool finite_d(double x) { return fabs(x) <= 1.7976931348623157e308; }
+
+__device__ __forceinline__ double blend_weight(double skew) {
+  double t = (skew - 0.15) / (0.25 - 0.15);
+  t = t < 0.0 ? 0.0 : (t > 1.0 ? 1.0 : t);
+  return 1.0 - t * t * (3.0 - 2.0 * t);
+}
+
+// ------------------------------------------------------------------------------------------
+// Boundary values.  filt: -1 all faces, 0 non-periodic only, 1 periodic only.
+// src/bc/mod_bc.f90:196-380 (apply_velocity_bc)
+__global__ void k_velocity_bc(Dev d, const double* __restrict__ U, const double* __restrict__ gU, double* Ub,
+                              int filt, int have_grad) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= d.nb) return;
+  const int nc = d.nc, nf = d.nf, nb = d.nb;
+  int f = d.nfi + b, bc = d.bbc[b];
+  if (filt == 1 && bc != BC_PERIODIC) return;
+  if (filt == 0 && bc == BC_PERIODIC) return;
+  int o = d.fo[f];
+  double u0 = Ub[b], u1 = Ub[nb + b], u2 = Ub[2 * nb + b];
+  double n0 = d.nrm[f], n1 = d.nrm[nf + f], n2 = d.nrm[2 * nf + f];
+  switch (bc) {
+    case BC_INLET:
+      u0 = d.bUval[b]; u1 = d.bUval[nb + b]; u2 = d.bUval[2 * nb + b];
+      break;
+    case BC_OUTLET:
+    case BC_ZEROGRADIENT: {
+      u0 = U[o]; u1 = U[nc + o]; u2 = U[2 * nc + o];
+      if (have_grad) {
+        double d0 = d.fcen[f] - d.cen[o], d1 = d.fcen[nf + f] - d.cen[nc + o], d2 = d.fcen[2 * nf + f] - d.cen[2 * nc + o];
+        // gU[(3j+i)nc + c] = dU_j/dx_i
+        u0 = u0 + gU[0 * nc + o] * d0 + gU[1 * nc + o] * d1 + gU[2 * nc + o] * d2;
+        u1 = u1 + gU[3 * nc + o] * d0 + gU[4 * nc + o] * d1 + gU[5 * nc + o] * d2;
+        u2 = u2 + gU[6 * nc + o] * d0 + gU[7 * nc + o] * d1 + gU[8 * nc + o] * d2;
+      }
+      break;
+    }
+    case BC_WALL_NOSLIP:
+    case BC_WALL_MODEL:
+      u0 = u1 = u2 = 0.0;
+      break;
+    case BC_WALL_VELOCITY: {
+      u0 = d.bUval[b]; u1 = d.bUval[nb + b]; u2 = d.bUval[2 * nb + b];
+      double un = u0 * n0 + u1 * n1 + u2 * n2;
+      u0 = u0 - un * n0; u1 = u1 - un * n1; u2 = u2 - un * n2;
+      break;
+    }
+    case BC_PERIODIC: {
+      u0 = U[o]; u1 = U[nc + o]; u2 = U[2 * nc + o];
+      int pn = d.bpnb[b];
+      if (pn >= 0) {
+        double w = d.bpgc[b];
+        u0 = w * u0 + (1.0 - w) * U[pn];
+        u1 = w * u1 + (1.0 - w) * U[nc + pn];
+        u2 = w * u2 + (1.0 - w) * U[2 * nc + pn];
+      }
+      break;
+    }
+    case BC_SLIP:
+    case BC_SYMMETRY: {
+      u0 = U[o]; u1 = U[nc + o]; u2 = U[2 * nc + o];
+      double un = u0 * n0 + u1 * n1 + u2 * n2;
+      u0 = u0 - un * n0; u1 = u1 - un * n1; u2 = u2 - un * n2;
+      break;
+    }
+    default:
+      break;
+  }
+  Ub[b] = u0; Ub[nb + b] = u1; Ub[2 * nb + b] = u2;
+}
+
+// src/bc/mod_bc.f90:383-486 (apply_pressure_bc)
+__global__ void k_pressure_bc(Dev d, const double* __restrict__ pf, const double* __restrict__ gp, double* pb,
+                              int filt, int have_grad, int increment) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= d.nb) return;
+  const int nc = d.nc, nf = d.nf;
+  int f = d.nfi + b, bc = d.bbc[b];
+  if (filt == 1 && bc != BC_PERIODIC) return;
+  if (filt == 0 && bc == BC_PERIODIC) return;
+  int o = d.fo[f];
+  double v;
+  if (bc == BC_OUTLET) {
+    v = (increment ? 0.0 : 1.0) * d.bpval[b];
+  } else if (bc == BC_PERIODIC) {
+    int pn = d.bpnb[b];
+    v = pn >= 0 ? d.bpgc[b] * pf[o] + (1.0 - d.bpgc[b]) * pf[pn] : pf[o];
+  } else if (is_wall_bc(bc)) {
+    v = pf[o] - 0.0;
+  } else if (have_grad) {
+    double d0 = d.fcen[f] - d.cen[o], d1 = d.fcen[nf + f] - d.cen[nc + o], d2 = d.fcen[2 * nf + f] - d.cen[2 * nc + o];
+    v = pf[o] + gp[o] * d0 + gp[nc + o] * d1 + gp[2 * nc + o] * d2;
+  } else {
+    v = pf[o];
+  }
+  pb[b] = v;
+}
+
+// ------------------------------------------------------------------------------------------
+// Least-squares gradients (src/numerics/mod_gradient.f90:425-613, 307-423).  The stencil is an
+// ELL list [W][nc]; weights are read once per call with coalesced loads.
+__global__ void __launch_bounds__(TPB) k_ls_gradient_vector(Dev d, const double* __restrict__ U,
+                                                            const double* __restrict__ Ub, double* __restrict__ gU) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.nc) return;
+  const int nc = d.nc, nb = d.nb, W = d.W;
+  const double uc0 = U[c], uc1 = U[nc + c], uc2 = U[2 * nc + c];
+  double a[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int s = 0; s < W; ++s) {
+    int v = __ldg(&d.ls_idx[s * nc + c]);
+    if (v == PADI) break;
+    double un0, un1, un2;
+    if (v >= 0) {
+      un0 = U[v]; un1 = U[nc + v]; un2 = U[2 * nc + v];
+    } else {
+      int b = -v - 1;
+      if (b < nb) { un0 = Ub[b]; un1 = Ub[nb + b]; un2 = Ub[2 * nb + b]; }
+      else { un0 = uc0; un1 = uc1; un2 = uc2; }
+    }
+    double w0 = __ldg(&d.ls_w[(0 * W + s) * nc + c]);
+    double w1 = __ldg(&d.ls_w[(1 * W + s) * nc + c]);
+    double w2 = __ldg(&d.ls_w[(2 * W + s) * nc + c]);
+    double du0 = un0 - uc0, du1 = un1 - uc1, du2 = un2 - uc2;
+    a[0] += w0 * du0; a[1] += w1 * du0; a[2] += w2 * du0;
+    a[3] += w0 * du1; a[4] += w1 * du1; a[5] += w2 * du1;
+    a[6] += w0 * du2; a[7] += w1 * du2; a[8] += w2 * du2;
+  }
+#pragma unroll
+  for (int j = 0; j < 9; ++j) gU[j * nc + c] = a[j];
+}
+
+__global__ void __launch_bounds__(TPB) k_ls_gradient_scalar(Dev d, const double* __restrict__ phi,
+                                                            const double* __restrict__ pb, double* __restrict__ g) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.nc) return;
+  const int nc = d.nc, nb = d.nb, W = d.W;
+  const double pc = phi[c];
+  double a0 = 0, a1 = 0, a2 = 0;
+  for (int s = 0; s < W; ++s) {
+    int v = __ldg(&d.ls_idx[s * nc + c]);
+    if (v == PADI) break;
+    double pv;
+    if (v >= 0) pv = phi[v];
+    else {
+      int b = -v - 1;
+      pv = b < nb ? pb[b] : pc;
+    }
+    double dd = pv - pc;
+    a0 += __ldg(&d.ls_w[(0 * W + s) * nc + c]) * dd;
+    a1 += __ldg(&d.ls_w[(1 * W + s) * nc + c]) * dd;
+    a2 += __ldg(&d.ls_w[(2 * W + s) * nc + c]) * dd;
+  }
+  g[c] = a0; g[nc + c] = a1; g[2 * nc + c] = a2;
+}
+
+// ------------------------------------------------------------------------------------------
+// SGS eddy viscosity.  Vreman (src/sgs/mod_vreman.f90:50-153), Smagorinsky (:295-364),
+// AMD (src/sgs/mod_amd.f90:31-207).  model: 1 Vreman, 2 Smagorinsky, 3 AMD.
+__device__ __forceinline__ double amd_point_d(const double* a, const double* G, double c_amd) {
+  double asq = 0.0;
+  for (int j = 0; j < 3; ++j)
+    for (int i = 0; i < 3; ++i) asq += a[i + 3 * j] * a[i + 3 * j];
+  double num = 0.0;
+  for (int n = 0; n < 3; ++n)
+    for (int m = 0; m < 3; ++m) {
+      double beta = 0.0;
+      for (int j = 0; j < 3; ++j)
+        for (int i = 0; i < 3; ++i) beta += G[i + 3 * j] * a[i + 3 * m] * a[j + 3 * n];
+      num -= beta * a[m + 3 * n];
+    }
+  double trg = G[0] + G[4] + G[8];
+  if (asq > 1.0e-20 && num > 1.0e-12 * trg * asq * sqrt(asq)) return c_amd * num / asq;
+  return 0.0;
+}
+
+__device__ __forceinline__ double det3_d(const double* A) {
+  return A[0] * (A[4] * A[8] - A[7] * A[5]) - A[3] * (A[1] * A[8] - A[7] * A[2]) + A[6] * (A[1] * A[5] - A[4] * A[2]);
+}
+
+__global__ void __launch_bounds__(TPB) k_sgs(Dev d, int model, const double* __restrict__ gU, double* __restrict__ nu,
+                                             double dt_stab, double c_amd) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.nc) return;
+  const int nc = d.nc;
+  double a[9], G[9];
+#pragma unroll
+  for (int j = 0; j < 9; ++j) { a[j] = gU[j * nc + c]; G[j] = d.G[j * nc + c]; }
+  double res = 0.0;
+  if (model == 1) {
+    double beta[9];
+    for (int j = 0; j < 3; ++j)
+      for (int i = 0; i <= j; ++i) {
+        double s = 0.0;
+        for (int n = 0; n < 3; ++n)
+          for (int m = 0; m < 3; ++m) s += G[m + 3 * n] * a[m + 3 * i] * a[n + 3 * j];
+        beta[i + 3 * j] = s;
+      }
+    double asq = a[0] * a[0] + a[3] * a[3] + a[6] * a[6] + a[1] * a[1] + a[4] * a[4] + a[7] * a[7] + a[2] * a[2] +
+                 a[5] * a[5] + a[8] * a[8];
+    double B = beta[0] * beta[4] - beta[3] * beta[3] + beta[0] * beta[8] - beta[6] * beta[6] + beta[4] * beta[8] -
+               beta[7] * beta[7];
+    double nuc = (asq > SMALLD && B > 0.0) ? 0.025 * sqrt(B / asq) : 0.0;
+    double cap = 0.4 * pow(d.vol[c], 2.0 / 3.0) / fmax(dt_stab, SMALLD);
+    res = fmin(nuc, cap);
+  } else if (model == 2) {
+    double SS = 0.0;
+    for (int j = 0; j < 3; ++j)
+      for (int i = 0; i < 3; ++i) {
+        double s = 0.5 * (a[i + 3 * j] + a[j + 3 * i]);
+        SS += s * s;
+      }
+    double Sn = sqrt(2.0 * SS);
+    double delta = fmax(pow(fmax(det3_d(G), 0.0), 1.0 / 6.0), SMALLD);
+    double nuc = (0.1 * delta) * (0.1 * delta) * Sn;
+    res = fmin(nuc, 0.4 * delta * delta / fmax(dt_stab, SMALLD));
+  } else if (model == 3) {
+    double nuc = amd_point_d(a, G, c_amd);
+    res = fmin(nuc, 0.4 * pow(d.vol[c], 2.0 / 3.0) / fmax(dt_stab, SMALLD));
+  }
+  nu[c] = res;
+}
+
+// ------------------------------------------------------------------------------------------
+// Log-law (Reichardt) wall model, src/sgs/mod_wall_model.f90:50-114 and apply_wall_model_bc
+// (:176-313).  Newton iterations are bounded (50), as in the reference.
+__device__ void wall_newton_d(double u_par, double y_w, double nu, double& u_tau, double& tau_mag) {
+  const double KAPPA = 0.41, A1I = 1.0 / 11.0, A2 = 0.33;
+  const double C_BUF = 5.2 - log(KAPPA) / KAPPA;
+  if (u_par <= SMALLD || y_w <= SMALLD) { u_tau = 0.0; tau_mag = 0.0; return; }
+  u_tau = fmax(0.01 * u_par, sqrt(nu * u_par / (y_w + SMALLD)));
+  double ywn = y_w * (1.0 / (nu + SMALLD));
+  for (int it = 0; it < 50; ++it) {
+    double yp = u_tau * ywn;
+    double e1 = exp(-yp * A1I), e2 = exp(-A2 * yp);
+    double up = log(1.0 + KAPPA * yp) / KAPPA + C_BUF * (1.0 - e1 - yp * A1I * e2);
+    double dup = 1.0 / (1.0 + KAPPA * yp) + C_BUF * (A1I * e1 - A1I * e2 + yp * A1I * A2 * e2);
+    double f = u_par / (u_tau + SMALLD) - up;
+    double df = -u_par / (u_tau * u_tau + SMALLD) - dup * ywn;
+    double un = u_tau - f / (df + (df >= 0.0 ? SMALLD : -SMALLD));
+    un = fmin(fmax(un, 0.1 * u_tau), 10.0 * u_tau);
+    if (fabs(un - u_tau) < 1.0e-8 * un) { u_tau = un; break; }
+    u_tau = un;
+  }
+  tau_mag = u_tau * u_tau;
+}
+
+// filter: 0 off; 1 fixed time constant (weight w_filt); 2 adaptive (tf_fac).  seed: first call.
+__global__ void k_wall_model(Dev d, const double* __restrict__ U, double* tau, double* upf, double nu, int filter,
+                             int seed, double w_filt, double dt_f, double tf_fac) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= d.nb) return;
+  if (d.bbc[b] != BC_WALL_MODEL) return;
+  const int nc = d.nc, nf = d.nf, nb = d.nb;
+  int f = d.nfi + b, o = d.fo[f];
+  double n0 = d.nrm[f], n1 = d.nrm[nf + f], n2 = d.nrm[2 * nf + f];
+  double yw = d.yw[b];
+  double un = U[o] * n0 + U[nc + o] * n1 + U[2 * nc + o] * n2;
+  double u0 = U[o] - un * n0, u1 = U[nc + o] - un * n1, u2 = U[2 * nc + o] - un * n2;
+  if (filter) {
+    if (seed) {
+      upf[b] = u0; upf[nb + b] = u1; upf[2 * nb + b] = u2;
+    } else {
+      double e = w_filt;
+      if (filter == 2) {
+        e = 0.0;
+        if (dt_f > 0.0) {
+          double f0 = upf[b], f1 = upf[nb + b], f2 = upf[2 * nb + b];
+          double upm = sqrt(f0 * f0 + f1 * f1 + f2 * f2), utp, tp;
+          wall_newton_d(upm, yw, nu, utp, tp);
+          e = 1.0;
+          if (utp > SMALLD) e = fmin(1.0, dt_f * 0.41 * utp / (tf_fac * yw));
+        }
+      }
+      upf[b] = upf[b] + e * (u0 - upf[b]);
+      upf[nb + b] = upf[nb + b] + e * (u1 - upf[nb + b]);
+      upf[2 * nb + b] = upf[2 * nb + b] + e * (u2 - upf[2 * nb + b]);
+    }
+    u0 = upf[b]; u1 = upf[nb + b]; u2 = upf[2 * nb + b];
+  }
+  double um = sqrt(u0 * u0 + u1 * u1 + u2 * u2), ut, tm;
+  wall_newton_d(um, yw, nu, ut, tm);
+  double sc = -tm / (um + SMALLD);
+  tau[b] = sc * u0; tau[nb + b] = sc * u1; tau[2 * nb + b] = sc * u2;
+}
+
+// AMD wall-cell correction: replaces the wall-normal gradient of the tangential velocity by the
+// log-law value u_tau/(kappa y) in cells owning wall-model faces (src/sgs/mod_amd.f90:148-197).
+__global__ void k_amd_wall(Dev d, const double* __restrict__ U, const double* __restrict__ gU, double* nu_sgs,
+                           double nu, double c_amd, double dt_stab) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.nc) return;
+  const int nc = d.nc, nf = d.nf;
+  for (int s = 0; s < d.SB; ++s) {
+    int b = d.cbn[s * nc + c];
+    if (b == PADI) break;
+    if (d.bbc[b] != BC_WALL_MODEL) continue;
+    int f = d.nfi + b;
+    double nr[3] = {-d.nrm[f], -d.nrm[nf + f], -d.nrm[2 * nf + f]};
+    double dd[3] = {d.fcen[f] - d.cen[c], d.fcen[nf + f] - d.cen[nc + c], d.fcen[2 * nf + f] - d.cen[2 * nc + c]};
+    double yw = fabs(dd[0] * nr[0] + dd[1] * nr[1] + dd[2] * nr[2]);
+    double u[3] = {U[c], U[nc + c], U[2 * nc + c]};
+    double un = u[0] * nr[0] + u[1] * nr[1] + u[2] * nr[2];
+    double ut[3] = {u[0] - un * nr[0], u[1] - un * nr[1], u[2] - un * nr[2]};
+    double utm = sqrt(ut[0] * ut[0] + ut[1] * ut[1] + ut[2] * ut[2]);
+    if (utm <= 1.0e-14 || yw <= SMALLD) continue;
+    double utau, tm;
+    wall_newton_d(utm, yw, nu, utau, tm);
+    double gw = utau / (0.41 * yw);
+    double a[9], G[9];
+    for (int j = 0; j < 9; ++j) { a[j] = gU[j * nc + c]; G[j] = d.G[j * nc + c]; }
+    double dold[3], dt_[3];
+    for (int j = 0; j < 3; ++j) dold[j] = nr[0] * a[0 + 3 * j] + nr[1] * a[1 + 3 * j] + nr[2] * a[2 + 3 * j];
+    double dn = dold[0] * nr[0] + dold[1] * nr[1] + dold[2] * nr[2];
+    for (int j = 0; j < 3; ++j) dt_[j] = gw * ut[j] / utm - (dold[j] - dn * nr[j]);
+    for (int j = 0; j < 3; ++j)
+      for (int i = 0; i < 3; ++i) a[i + 3 * j] += nr[i] * dt_[j];
+    double nuc = amd_point_d(a, G, c_amd);
+    nu_sgs[c] = fmin(nuc, 0.4 * pow(d.vol[c], 2.0 / 3.0) / fmax(dt_stab, SMALLD));
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// Advection face values for the reconstruction schemes (QUICK, van Leer, Koren):
+// src/numerics/mod_advection.f90:2386-2791.
+struct ReconCtx {
+  int up, down;
+  double xu[3], xd[3], xf[3], sh[3], dir[3], s_face, s_down;
+};
+
+__device__ bool recon_context_d(const Dev& d, int f, double Fn, ReconCtx& c) {
+  const int nc = d.nc, nf = d.nf;
+  c.up = c.down = -1;
+  for (int k = 0; k < 3; ++k) { c.xu[k] = c.xd[k] = c.sh[k] = c.dir[k] = 0.0; c.xf[k] = d.fcen[k * nf + f]; }
+  c.s_face = c.s_down = 0.0;
+  int o = d.fo[f], n = d.fn[f];
+  if (n >= 0) {
+    if (Fn >= 0.0) { c.up = o; c.down = n; } else { c.up = n; c.down = o; }
+    for (int k = 0; k < 3; ++k) { c.xu[k] = d.cen[k * nc + c.up]; c.xd[k] = d.cen[k * nc + c.down]; }
+  } else {
+    int b = f - d.nfi;
+    if (d.bbc[b] != BC_PERIODIC) return false;
+    int pcell = d.bpnb[b];
+    int pb = d.bpair[b];
+    int pf = pb >= 0 ? d.nfi + pb : -1;
+    if (pcell < 0) return false;
+    double dper;
+    if (pf >= 0) dper = d.dcf[f] + d.dcf[pf];
+    else if (d.bpdcf[b] > SMALLD) dper = d.dcf[f] + d.bpdcf[b];
+    else dper = 2.0 * d.dcf[f];
+    double sh[3];
+    for (int k = 0; k < 3; ++k) sh[k] = (d.cen[k * nc + o] + dper * d.nrm[k * nf + f]) - d.cen[k * nc + pcell];
+    if (Fn >= 0.0) {
+      c.up = o; c.down = pcell;
+      for (int k = 0; k < 3; ++k) { c.xu[k] = d.cen[k * nc + o]; c.xd[k] = d.cen[k * nc + pcell] + sh[k]; }
+    } else {
+      c.up = pcell; c.down = o;
+      for (int k = 0; k < 3; ++k) { c.sh[k] = sh[k]; c.xu[k] = d.cen[k * nc + pcell] + c.sh[k]; c.xd[k] = d.cen[k * nc + o]; }
+    }
+  }
+  double dv[3];
+  for (int k = 0; k < 3; ++k) dv[k] = c.xf[k] - c.xu[k];
+  double dn = sqrt(dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2]);
+  if (dn <= SMALLD) {
+    for (int k = 0; k < 3; ++k) dv[k] = c.xd[k] - c.xu[k];
+    dn = sqrt(dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2]);
+  }
+  if (dn <= SMALLD) return false;
+  for (int k = 0; k < 3; ++k) c.dir[k] = dv[k] / dn;
+  double a[3], bb[3];
+  for (int k = 0; k < 3; ++k) { a[k] = c.xf[k] - c.xu[k]; bb[k] = c.xd[k] - c.xu[k]; }
+  c.s_face = a[0] * c.dir[0] + a[1] * c.dir[1] + a[2] * c.dir[2];
+  c.s_down = bb[0] * c.dir[0] + bb[1] * c.dir[1] + bb[2] * c.dir[2];
+  if (c.s_face <= SMALLD || c.s_down <= c.s_face) {
+    for (int k = 0; k < 3; ++k) dv[k] = c.xd[k] - c.xu[k];
+    dn = sqrt(dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2]);
+    if (dn <= SMALLD) return false;
+    for (int k = 0; k < 3; ++k) c.dir[k] = dv[k] / dn;
+    c.s_face = a[0] * c.dir[0] + a[1] * c.dir[1] + a[2] * c.dir[2];
+    c.s_down = bb[0] * c.dir[0] + bb[1] * c.dir[1] + bb[2] * c.dir[2];
+  }
+  if (c.s_down <= SMALLD) return false;
+  c.s_face = fmin(fmax(c.s_face, 0.0), c.s_down);
+  return true;
+}
+
+__device__ int far_upwind_d(const Dev& d, const ReconCtx& c) {
+  const int nc = d.nc;
+  int far = -1;
+  if (c.up < 0 || c.up >= nc || c.down >= nc) return far;
+  double best_align = -1.0, best_perp2 = 1.0e308;
+  for (int s = 0; s < d.S; ++s) {
+    int fj = d.cf[s * nc + c.up];
+    if (fj == PADI) break;
+    int n = d.fo[fj];
+    if (n == c.up) n = d.fn[fj];
+    if (n < 0 && fj >= d.nfi) {
+      int b = fj - d.nfi;
+      if (d.bbc[b] == BC_PERIODIC) n = d.bpnb[b];
+    }
+    if (n == c.down || n < 0) continue;
+    double dv[3];
+    for (int k = 0; k < 3; ++k) dv[k] = d.cen[k * nc + n] + c.sh[k] - c.xu[k];
+    double s_ = dv[0] * c.dir[0] + dv[1] * c.dir[1] + dv[2] * c.dir[2];
+    if (s_ >= -1.0e-12) continue;
+    double dist2 = fmax(dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2], SMALLD);
+    double align = -s_ / sqrt(dist2);
+    double perp2 = fmax(0.0, dist2 - s_ * s_);
+    if (align > best_align + 1.0e-12 || (fabs(align - best_align) <= 1.0e-12 && perp2 < best_perp2 - 1.0e-12) ||
+        (fabs(align - best_align) <= 1.0e-12 && fabs(perp2 - best_perp2) <= 1.0e-12 && n < far)) {
+      best_align = align; best_perp2 = perp2; far = n;
+    }
+  }
+  return far;
+}
+
+__device__ __forceinline__ double clampv_d(double x, double lo, double hi) {
+  double l = fmin(lo, hi), h = fmax(lo, hi);
+  return fmin(fmax(x, l), h);
+}
+
+__device__ void quick3_d(const Dev& d, const ReconCtx& c, const double* U, const double* gU, double* phi) {
+  const int nc = d.nc;
+  bool hg = c.up < nc && c.down < nc;
+  double pU[3], pD[3], g[3][3];
+  for (int k = 0; k < 3; ++k) {
+    pU[k] = U[k * nc + c.up];
+    pD[k] = U[k * nc + c.down];
+    for (int i = 0; i < 3; ++i) g[k][i] = hg ? gU[(3 * k + i) * nc + c.up] : 0.0;
+  }
+  auto axial = [&](double far, double up, const double* gg, const double* dv, double s) {
+    double t0 = dv[0] - s * c.dir[0], t1 = dv[1] - s * c.dir[1], t2 = dv[2] - s * c.dir[2];
+    return far - up - (gg[0] * t0 + gg[1] * t1 + gg[2] * t2);
+  };
+  double dv[3] = {c.xd[0] - c.xu[0], c.xd[1] - c.xu[1], c.xd[2] - c.xu[2]};
+  double dist2 = fmax(dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2], SMALLD);
+  double w = 1.0 / dist2;
+  double a11 = w * c.s_down * c.s_down, a12 = a11 * c.s_down, a22 = a12 * c.s_down, lden = a11;
+  int nfit = 1;
+  double b1[3], b2[3], ln[3];
+  for (int k = 0; k < 3; ++k) {
+    double dp = axial(pD[k], pU[k], g[k], dv, c.s_down);
+    b1[k] = w * c.s_down * dp;
+    b2[k] = w * c.s_down * c.s_down * dp;
+    ln[k] = b1[k];
+  }
+  if (c.up < nc && c.down < nc) {
+    for (int s = 0; s < d.S; ++s) {
+      int fj = d.cf[s * nc + c.up];
+      if (fj == PADI) break;
+      int n = d.fo[fj];
+      if (n == c.up) n = d.fn[fj];
+      if (n < 0 || n == c.down) continue;
+      double dd[3];
+      for (int k = 0; k < 3; ++k) dd[k] = d.cen[k * nc + n] + c.sh[k] - c.xu[k];
+      double s_ = dd[0] * c.dir[0] + dd[1] * c.dir[1] + dd[2] * c.dir[2];
+      if (s_ >= -1.0e-12) continue;
+      double d2 = fmax(dd[0] * dd[0] + dd[1] * dd[1] + dd[2] * dd[2], SMALLD);
+      if (s_ * s_ < 0.25 * d2) continue;
+      double al = fmin(1.0, -s_ / sqrt(d2));
+      double wt = (0.25 + al * al) / d2;
+      a11 += wt * s_ * s_; a12 += wt * s_ * s_ * s_; a22 += wt * s_ * s_ * s_ * s_; lden += wt * s_ * s_;
+      for (int k = 0; k < 3; ++k) {
+        double dp = axial(U[k * nc + n], pU[k], g[k], dd, s_);
+        b1[k] += wt * s_ * dp; b2[k] += wt * s_ * s_ * dp; ln[k] += wt * s_ * dp;
+      }
+      nfit++;
+    }
+  }
+  double det = a11 * a22 - a12 * a12;
+  for (int k = 0; k < 3; ++k) {
+    double a1, a2;
+    if (nfit >= 2 && fabs(det) > SMALLD) { a1 = (b1[k] * a22 - b2[k] * a12) / det; a2 = (-b1[k] * a12 + b2[k] * a11) / det; }
+    else if (lden > SMALLD) { a1 = ln[k] / lden; a2 = 0.0; }
+    else { a1 = (pD[k] - pU[k]) / fmax(c.s_down, SMALLD); a2 = 0.0; }
+    double v = pU[k] + a1 * c.s_face + a2 * c.s_face * c.s_face;
+    phi[k] = clampv_d(v, fmin(pU[k], pD[k]), fmax(pU[k], pD[k]));
+  }
+}
+
+__device__ double tvd_d(const Dev& d, int scheme, const double* phi, const ReconCtx& c, int far) {
+  const int nc = d.nc;
+  double pU = phi[c.up], pD = phi[c.down];
+  double sdn = (pD - pU) / fmax(c.s_down, SMALLD), psi = 0.0;
+  if (far >= 0 && fabs(sdn) > SMALLD) {
+    double xf0 = d.cen[far] + c.sh[0] - c.xu[0], xf1 = d.cen[nc + far] + c.sh[1] - c.xu[1],
+           xf2 = d.cen[2 * nc + far] + c.sh[2] - c.xu[2];
+    double s_up = -(xf0 * c.dir[0] + xf1 * c.dir[1] + xf2 * c.dir[2]);
+    if (s_up > SMALLD) {
+      double r = ((pU - phi[far]) / s_up) / sdn;
+      if (scheme == 1) {
+        psi = (r + fabs(r)) / (1.0 + fabs(r));
+        psi = fmax(0.0, fmin(psi, 2.0));
+      } else {
+        psi = fmax(0.0, fmin(fmin(2.0 * r, (1.0 + 2.0 * r) / 3.0), 2.0));
+      }
+    }
+  }
+  return clampv_d(pU + psi * sdn * c.s_face, fmin(pU, pD), fmax(pU, pD));
+}
+
+// ------------------------------------------------------------------------------------------
+// Face fluxes of the explicit right-hand side: advective Fn*phi_f (KEP, CDS, QUICK, van Leer,
+// Koren; src/numerics/mod_advection.f90:1013-1635) and viscous stress (src/numerics/mod_viscous.f90:37-282),
+// written per face; k_cell_explicit gathers them per cell.
+__global__ void __launch_bounds__(TPB) k_face_explicit(Dev d, int scheme, double nu, const double* __restrict__ U,
+                                                       const double* __restrict__ Ub, const double* __restrict__ gU,
+                                                       const double* __restrict__ nus, const double* __restrict__ Uface,
+                                                       double* __restrict__ fadv, double* __restrict__ fvis,
+                                                       double* __restrict__ fdiv) {
+  int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= d.nf) return;
+  const int nc = d.nc, nf = d.nf, nb = d.nb;
+  const int o = d.fo[f], n = d.fn[f];
+  const double sf0 = d.sf[f], sf1 = d.sf[nf + f], sf2 = d.sf[2 * nf + f];
+  const int b = f - d.nfi;
+  const int bc = n >= 0 ? -1 : d.bbc[b];
+  double phi[3], Fn;
+  // ---- advection
+  if (scheme == 4) {  // KEP
+    int npr = -1;
+    double Ufv[3];
+    if (n >= 0) {
+      Fn = Uface[f];
+      for (int k = 0; k < 3; ++k) phi[k] = 0.5 * (U[k * nc + o] + U[k * nc + n]);
+    } else {
+      if (bc == BC_PERIODIC) npr = d.bpnb[b];
+      if (bc == BC_PERIODIC && npr >= 0) {
+        double w = d.bpgc[b];
+        for (int k = 0; k < 3; ++k) Ufv[k] = w * U[k * nc + o] + (1.0 - w) * U[k * nc + npr];
+      } else {
+        for (int k = 0; k < 3; ++k) Ufv[k] = Ub[k * nb + b];
+      }
+      if (bc == BC_PERIODIC || bc == BC_OUTLET) Fn = Uface[f];
+      else if (is_wall_bc(bc)) Fn = 0.0;
+      else Fn = Ufv[0] * sf0 + Ufv[1] * sf1 + Ufv[2] * sf2;
+      for (int k = 0; k < 3; ++k) phi[k] = npr >= 0 ? 0.5 * (U[k * nc + o] + U[k * nc + npr]) : Ufv[k];
+    }
+    fdiv[f] = Fn;
+  } else if (scheme == 3) {  // CDS
+    int npr = -1;
+    if (n >= 0) Fn = Uface[f];
+    else if (bc == BC_PERIODIC || bc == BC_OUTLET) Fn = Uface[f];
+    else if (is_wall_bc(bc)) Fn = 0.0;
+    else Fn = Ub[b] * sf0 + Ub[nb + b] * sf1 + Ub[2 * nb + b] * sf2;
+    bool rec = n >= 0;
+    if (!rec && bc == BC_PERIODIC) { npr = d.bpnb[b]; rec = npr >= 0; }
+    int ns = rec ? (n >= 0 ? n : npr) : -1;
+    for (int k = 0; k < 3; ++k) {
+      double ph;
+      if (rec) {
+        double g = f >= d.nfi ? d.bpgc[b] : d.gc[f];
+        double plain = g * U[k * nc + o] + (1.0 - g) * U[k * nc + ns];
+        if (f < d.nfi) {
+          double gm0 = g * gU[(3 * k + 0) * nc + o] + (1.0 - g) * gU[(3 * k + 0) * nc + ns];
+          double gm1 = g * gU[(3 * k + 1) * nc + o] + (1.0 - g) * gU[(3 * k + 1) * nc + ns];
+          double gm2 = g * gU[(3 * k + 2) * nc + o] + (1.0 - g) * gU[(3 * k + 2) * nc + ns];
+          double pe = plain + (gm0 * d.eps[f] + gm1 * d.eps[nf + f] + gm2 * d.eps[2 * nf + f]);
+          double wb = d.wbl[f];
+          if (wb < 1.0) pe = plain + wb * (pe - plain);
+          ph = pe;
+        } else {
+          ph = plain;
+        }
+      } else {
+        ph = Ub[k * nb + b];
+      }
+      if (!finite_d(ph)) ph = 0.0;
+      phi[k] = ph;
+    }
+  } else {  // QUICK (5), van Leer (1), Koren (2)
+    if (n >= 0) Fn = Uface[f];
+    else Fn = is_wall_bc(bc) ? 0.0 : Uface[f];
+    ReconCtx ctx;
+    bool ok = recon_context_d(d, f, Fn, ctx);
+    int far = -1;
+    if (ok && scheme != 5) far = far_upwind_d(d, ctx);
+    if (!finite_d(Fn)) Fn = 0.0;
+    double pq[3] = {0, 0, 0};
+    if (ok && scheme == 5) quick3_d(d, ctx, U, gU, pq);
+    for (int k = 0; k < 3; ++k) {
+      double ph;
+      if (ok) {
+        ph = scheme == 5 ? pq[k] : tvd_d(d, scheme, U + (size_t)k * nc, ctx, far);
+        if (!finite_d(ph)) ph = (Fn >= 0.0 || n < 0) ? U[k * nc + o] : U[k * nc + n];
+      } else {
+        ph = Ub[k * nb + b];
+      }
+      if (!finite_d(ph)) ph = 0.0;
+      phi[k] = ph;
+    }
+  }
+  for (int k = 0; k < 3; ++k) fadv[k * nf + f] = Fn * phi[k];
+
+  // ---- viscous stress (owner orientation)
+  double st[3] = {0, 0, 0};
+  const double area = d.area[f];
+  auto stress = [&](int nbc, double g, double nu_eff, const double* dn_, double dl) {
+    double sdd = (sf0 * dn_[0] + sf1 * dn_[1] + sf2 * dn_[2]) / dl;
+    double dp0 = sf0 - (sdd / dl) * dn_[0], dp1 = sf1 - (sdd / dl) * dn_[1], dp2 = sf2 - (sdd / dl) * dn_[2];
+    double wo = area * fmax(0.0, fmin(1.0, sdd / (area + SMALLD)));
+    double gf[9];
+    for (int j = 0; j < 9; ++j) gf[j] = g * gU[j * nc + o] + (1.0 - g) * gU[j * nc + nbc];
+    for (int k = 0; k < 3; ++k) {
+      double t1 = (U[k * nc + nbc] - U[k * nc + o]) * wo / dl;
+      double t2 = gf[3 * k + 0] * dp0 + gf[3 * k + 1] * dp1 + gf[3 * k + 2] * dp2;
+      double t3 = gf[k] * sf0 + gf[3 + k] * sf1 + gf[6 + k] * sf2;
+      st[k] = nu_eff * (t1 + t2 + t3);
+    }
+  };
+  if (n >= 0) {
+    double g = d.gc[f];
+    double ne = nu + g * nus[o] + (1.0 - g) * nus[n];
+    double dn_[3] = {d.cen[n] - d.cen[o], d.cen[nc + n] - d.cen[nc + o], d.cen[2 * nc + n] - d.cen[2 * nc + o]};
+    double dl = sqrt(dn_[0] * dn_[0] + dn_[1] * dn_[1] + dn_[2] * dn_[2]) + SMALLD;
+    stress(n, g, ne, dn_, dl);
+  } else if (bc == BC_PERIODIC) {
+    int npr = d.bpnb[b];
+    int pb = d.bpair[b];
+    int pf = pb >= 0 ? d.nfi + pb : -1;
+    if (npr >= 0) {
+      double dper, gcp;
+      if (pf >= 0) { dper = d.dcf[f] + d.dcf[pf]; gcp = d.dcf[pf] / (dper + SMALLD); }
+      else if (d.bpdcf[b] > SMALLD) { dper = d.dcf[f] + d.bpdcf[b]; gcp = d.bpdcf[b] / (dper + SMALLD); }
+      else { dper = 2.0 * d.dcf[f]; gcp = 0.5; }
+      double ne = nu + gcp * nus[o] + (1.0 - gcp) * nus[npr];
+      double dn_[3] = {dper * d.nrm[f], dper * d.nrm[nf + f], dper * d.nrm[2 * nf + f]};
+      stress(npr, gcp, ne, dn_, dper + SMALLD);
+    } else {
+      double ne = nu + nus[o];
+      for (int k = 0; k < 3; ++k) st[k] = ne * ((Ub[k * nb + b] - U[k * nc + o]) / (d.dcf[f] + SMALLD)) * area;
+    }
+  } else if (bc != BC_WALL_MODEL) {
+    double ne = nu + nus[o];
+    double dn_[3] = {d.fcen[f] - d.cen[o], d.fcen[nf + f] - d.cen[nc + o], d.fcen[2 * nf + f] - d.cen[2 * nc + o]};
+    double dl = sqrt(dn_[0] * dn_[0] + dn_[1] * dn_[1] + dn_[2] * dn_[2]) + SMALLD;
+    double sdd = (sf0 * dn_[0] + sf1 * dn_[1] + sf2 * dn_[2]) / dl;
+    double dp0 = sf0 - (sdd / dl) * dn_[0], dp1 = sf1 - (sdd / dl) * dn_[1], dp2 = sf2 - (sdd / dl) * dn_[2];
+    double wo = area * fmax(0.0, fmin(1.0, sdd / (area + SMALLD)));
+    for (int k = 0; k < 3; ++k) {
+      double t1 = (Ub[k * nb + b] - U[k * nc + o]) * wo / dl;
+      double t2 = gU[(3 * k + 0) * nc + o] * dp0 + gU[(3 * k + 1) * nc + o] * dp1 + gU[(3 * k + 2) * nc + o] * dp2;
+      double t3 = gU[k * nc + o] * sf0 + gU[(3 + k) * nc + o] * sf1 + gU[(6 + k) * nc + o] * sf2;
+      st[k] = ne * (t1 + t2 + t3);
+    }
+  }
+  for (int k = 0; k < 3; ++k) fvis[k * nf + f] = st[k];
+}
+
+// Per-cell gather of the explicit fluxes into H = conv + visc + f (+ Boussinesq, + wall
+// traction), then the RK3W predictor U += dt (alpha_k H + beta_k H_prev)
+// (src/solver/mod_fv_solver.f90:1617-1762, 2238-2276, 1322-1333).  H is kept for the next stage.
+struct ExplicitArgs {
+  int scheme;
+  double f0, f1, f2;
+  int bous;
+  double beta, T_ref, g0, g1, g2;
+  double dt, a_k, b_k;
+  int predict;  // 0: only H (operator checks)
+};
+__global__ void __launch_bounds__(TPB) k_cell_explicit(Dev d, ExplicitArgs a, double* __restrict__ U,
+                                                       const double* __restrict__ T, const double* __restrict__ fadv,
+                                                       const double* __restrict__ fvis, const double* __restrict__ fdiv,
+                                                       const double* __restrict__ tau, double* __restrict__ H,
+                                                       const double* __restrict__ H0, double* __restrict__ conv_out,
+                                                       double* __restrict__ visc_out) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.nc) return;
+  const int nc = d.nc, nf = d.nf, nb = d.nb;
+  const double iv = d.ivol[c];
+  double cv[3] = {0, 0, 0}, vs[3] = {0, 0, 0}, dv = 0.0;
+  for (int s = 0; s < d.S; ++s) {
+    int f = d.cf[s * nc + c];
+    if (f == PADI) break;
+    bool own = d.fo[f] == c;
+    for (int k = 0; k < 3; ++k) {
+      double av = fadv[k * nf + f], sv = fvis[k * nf + f];
+      if (own) { cv[k] -= av * iv; vs[k] += sv * iv; }
+      else { cv[k] += av * iv; vs[k] -= sv * iv; }
+    }
+    if (a.scheme == 4) dv = own ? dv + fdiv[f] : dv - fdiv[f];
+  }
+  double u[3] = {U[c], U[nc + c], U[2 * nc + c]};
+  if (a.scheme == 4)
+    for (int k = 0; k < 3; ++k) cv[k] += 0.5 * u[k] * dv * iv;
+  const double fb[3] = {a.f0, a.f1, a.f2}, gv[3] = {a.g0, a.g1, a.g2};
+  double h[3];
+  for (int k = 0; k < 3; ++k) {
+    h[k] = cv[k] + vs[k] + fb[k];
+    if (a.bous) h[k] = h[k] - a.beta * (T[c] - a.T_ref) * gv[k];
+  }
+  for (int s = 0; s < d.SB; ++s) {
+    int b = d.cbn[s * nc + c];
+    if (b == PADI) break;
+    if (d.bbc[b] != BC_WALL_MODEL) continue;
+    double w = d.area[d.nfi + b] / d.vol[c];
+    for (int k = 0; k < 3; ++k) h[k] = h[k] + tau[k * nb + b] * w;
+  }
+  for (int k = 0; k < 3; ++k) {
+    H[k * nc + c] = h[k];
+    if (conv_out) conv_out[k * nc + c] = cv[k];
+    if (visc_out) visc_out[k * nc + c] = vs[k];
+  }
+  if (a.predict)
+    for (int k = 0; k < 3; ++k) U[k * nc + c] = u[k] + a.dt * (a.a_k * h[k] + a.b_k * H0[k * nc + c]);
+}
+
+// ------------------------------------------------------------------------------------------
+// Cell velocity correction U -= dt T^-1 sum_f g_f n_f (src/solver/mod_fv_solver.f90:2927-3151).
+struct CorrArgs {
+  double dt;
+  int do_cross, ptot;
+  double f0, f1, f2, bb, T_ref, g0, g1, g2;
+};
+__device__ __forceinline__ double ps_cross_d(const Dev& d, const double* gp, int i, int o, int n) {
+  const int nc = d.nc, nfp = d.nfp;
+  double gw = d.psgcw[i], cr = 0.0;
+  for (int j = 0; j < 3; ++j) cr += (gw * gp[j * nc + o] + (1.0 - gw) * gp[j * nc + n]) * d.psk[j * nfp + i];
+  return cr;
+}
+__global__ void __launch_bounds__(TPB) k_correct_velocity(Dev d, CorrArgs a, const double* __restrict__ p,
+                                                          const double* __restrict__ gp, const double* __restrict__ T,
+                                                          double* __restrict__ U, double* __restrict__ gpc) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.nc) return;
+  const int nc = d.nc, nf = d.nf, nb = d.nb;
+  double g[3] = {0, 0, 0};
+  for (int s = 0; s < d.SP; ++s) {
+    int e = d.cps[s * nc + c];
+    if (e == PADI) break;
+    int i = e >= 0 ? e : ~e;
+    int o = d.pso[i], n = d.psn[i], fm = d.psf[i];
+    double gf = d.psc[i] * (p[n] - p[o]);
+    if (a.do_cross) gf = gf + ps_cross_d(d, gp, i, o, n);
+    for (int k = 0; k < 3; ++k) g[k] = g[k] + gf * d.nrm[k * nf + fm];
+  }
+  for (int s = 0; s < d.SB; ++s) {
+    int b = d.cbn[s * nc + c];
+    if (b == PADI) break;
+    if (d.bbc[b] != BC_OUTLET) continue;
+    int f = d.nfi + b;
+    double gf = d.bcb[b] * ((a.ptot ? d.bpval[b] : 0.0) - p[c]);
+    if (a.do_cross) gf = gf + (gp[c] * d.bkout[b] + gp[nc + c] * d.bkout[nb + b] + gp[2 * nc + c] * d.bkout[2 * nb + b]);
+    for (int k = 0; k < 3; ++k) g[k] = g[k] + gf * d.nrm[k * nf + f];
+  }
+  if (!a.do_cross) {
+    for (int s = 0; s < d.SB; ++s) {
+      int b = d.cbn[s * nc + c];
+      if (b == PADI) break;
+      int bc = d.bbc[b];
+      if (bc == BC_OUTLET || bc == BC_PERIODIC) continue;
+      int f = d.nfi + b;
+      double tt = T ? T[c] : a.T_ref;
+      double v0 = a.f0 - a.bb * (tt - a.T_ref) * a.g0, v1 = a.f1 - a.bb * (tt - a.T_ref) * a.g1,
+             v2 = a.f2 - a.bb * (tt - a.T_ref) * a.g2;
+      double n0 = d.nrm[f], n1 = d.nrm[nf + f], n2 = d.nrm[2 * nf + f];
+      double fn = (v0 * n0 + v1 * n1 + v2 * n2) * d.area[f];
+      g[0] = g[0] + fn * n0; g[1] = g[1] + fn * n1; g[2] = g[2] + fn * n2;
+    }
+  }
+  const double* Ti = d.Tinv;
+  double t[9];
+  for (int j = 0; j < 9; ++j) t[j] = Ti[j * nc + c];
+  double g1 = t[0] * g[0] + t[3] * g[1] + t[6] * g[2];
+  double g2 = t[1] * g[0] + t[4] * g[1] + t[7] * g[2];
+  double g3 = t[2] * g[0] + t[5] * g[1] + t[8] * g[2];
+  gpc[c] = g1; gpc[nc + c] = g2; gpc[2 * nc + c] = g3;
+  U[c] = U[c] - a.dt * g1;
+  U[nc + c] = U[nc + c] - a.dt * g2;
+  U[2 * nc + c] = U[2 * nc + c] - a.dt * g3;
+}
+
+// ------------------------------------------------------------------------------------------
+// Predicted face flux with Rhie-Chow and deferred cross term (src/solver/mod_fv_solver.f90:2389-2752),
+// one thread per mesh face; the non-canonical face of a periodic pair evaluates its canonical
+// twin and takes the opposite sign (the reference's antisymmetric resync).
+__device__ __forceinline__ double ps_flux_d(const Dev& d, int i, double dt, const double* U, const double* gU,
+                                            const double* gprc, const double* phi) {
+  const int nc = d.nc, nf = d.nf, nfp = d.nfp;
+  int o = d.pso[i], n = d.psn[i], fm = d.psf[i];
+  double gcf = d.psgcf[i];
+  double sf0 = d.sf[fm], sf1 = d.sf[nf + fm], sf2 = d.sf[2 * nf + fm];
+  double Uf[3];
+  for (int j = 0; j < 3; ++j) Uf[j] = gcf * U[j * nc + o] + (1.0 - gcf) * U[j * nc + n];
+  if (fm < d.nfi) {
+    double wb = d.wbl[fm], g = d.gc[fm];
+    for (int j = 0; j < 3; ++j) {
+      double plain = Uf[j];
+      double ue = g * U[j * nc + o] + (1.0 - g) * U[j * nc + n];
+      double gm0 = g * gU[(3 * j + 0) * nc + o] + (1.0 - g) * gU[(3 * j + 0) * nc + n];
+      double gm1 = g * gU[(3 * j + 1) * nc + o] + (1.0 - g) * gU[(3 * j + 1) * nc + n];
+      double gm2 = g * gU[(3 * j + 2) * nc + o] + (1.0 - g) * gU[(3 * j + 2) * nc + n];
+      ue = ue + gm0 * d.eps[fm] + gm1 * d.eps[nf + fm] + gm2 * d.eps[2 * nf + fm];
+      Uf[j] = plain + wb * (ue - plain);
+    }
+  }
+  double flux = Uf[0] * sf0 + Uf[1] * sf1 + Uf[2] * sf2;
+  double k0 = d.pskrc[i], k1 = d.pskrc[nfp + i], k2 = d.pskrc[2 * nfp + i];
+  double gm0 = gcf * gprc[o] + (1.0 - gcf) * gprc[n];
+  double gm1 = gcf * gprc[nc + o] + (1.0 - gcf) * gprc[nc + n];
+  double gm2 = gcf * gprc[2 * nc + o] + (1.0 - gcf) * gprc[2 * nc + n];
+  double rc = (gm0 * (sf0 - k0) + gm1 * (sf1 - k1) + gm2 * (sf2 - k2)) - d.psc[i] * (phi[n] - phi[o]);
+  return flux + dt * rc;
+}
+
+__global__ void __launch_bounds__(TPB) k_face_flux(Dev d, double dt, const double* __restrict__ U,
+                                                   const double* __restrict__ gU, const double* __restrict__ gprc,
+                                                   const double* __restrict__ phi, const double* __restrict__ Ub,
+                                                   const double* __restrict__ gp, int with_cross,
+                                                   double* __restrict__ ff, double* __restrict__ pscross) {
+  int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= d.nf) return;
+  const int nf = d.nf, nb = d.nb;
+  if (f < d.nfi) {
+    ff[f] = ps_flux_d(d, f, dt, U, gU, gprc, phi);
+    if (with_cross) pscross[f] = ps_cross_d(d, gp, f, d.pso[f], d.psn[f]);
+    return;
+  }
+  int b = f - d.nfi, bc = d.bbc[b];
+  if (bc == BC_PERIODIC) {
+    int i = d.bps[b];
+    if (i < 0) {  // unpaired periodic face: owner-side flux (never reached on a paired mesh)
+      int o = d.fo[f];
+      ff[f] = U[o] * d.sf[f] + U[d.nc + o] * d.sf[nf + f] + U[2 * d.nc + o] * d.sf[2 * nf + f];
+      return;
+    }
+    double fl = ps_flux_d(d, i, dt, U, gU, gprc, phi);
+    ff[f] = d.bcanon[b] ? fl : -fl;
+    if (with_cross && d.bcanon[b]) pscross[i] = ps_cross_d(d, gp, i, d.pso[i], d.psn[i]);
+    return;
+  }
+  ff[f] = is_wall_bc(bc) ? 0.0 : (Ub[b] * d.sf[f] + Ub[nb + b] * d.sf[nf + f] + Ub[2 * nb + b] * d.sf[2 * nf + f]);
+}
+
+// rhs_p = -(1/dt) sum_f q_f + deferred cross terms, gathered per cell in the reference's order.
+__global__ void __launch_bounds__(TPB) k_rhs_gather(Dev d, double rdt, int with_cross, const double* __restrict__ ff,
+                                                    const double* __restrict__ pscross, const double* __restrict__ gp,
+                                                    double* __restrict__ rhs) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.nc) return;
+  const int nc = d.nc, nb = d.nb;
+  double r = 0.0;
+  for (int s = 0; s < d.SP; ++s) {
+    int e = d.cps[s * nc + c];
+    if (e == PADI) break;
+    if (e >= 0) r -= ff[d.psf[e]];
+    else r += ff[d.psf[~e]];
+  }
+  for (int s = 0; s < d.SB; ++s) {
+    int b = d.cbn[s * nc + c];
+    if (b == PADI) break;
+    if (d.bbc[b] == BC_PERIODIC) continue;
+    r -= ff[d.nfi + b];
+  }
+  r *= rdt;
+  if (with_cross) {
+    for (int s = 0; s < d.SP; ++s) {
+      int e = d.cps[s * nc + c];
+      if (e == PADI) break;
+      if (e >= 0) r += pscross[e];
+      else r -= pscross[~e];
+    }
+    for (int s = 0; s < d.SB; ++s) {
+      int b = d.cbn[s * nc + c];
+      if (b == PADI) break;
+      if (d.bbc[b] != BC_OUTLET) continue;
+      r += gp[c] * d.bkout[b] + gp[nc + c] * d.bkout[nb + b] + gp[2 * nc + c] * d.bkout[2 * nb + b];
+    }
+  }
+  rhs[c] = r;
+}
+
+// Flux correction with the pressure increment (src/solver/mod_fv_solver.f90:2756-2902); writes the
+// divergence-free flux to Uf (reads the predicted flux ff).
+__global__ void __launch_bounds__(TPB) k_correct_face_flux(Dev d, double dt, int ptot, int with_cross,
+                                                           const double* __restrict__ p, const double* __restrict__ gp,
+                                                           const double* __restrict__ ff, double* __restrict__ Uf) {
+  int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= d.nf) return;
+  const int nc = d.nc, nb = d.nb;
+  auto corr = [&](int i, double x) {
+    int o = d.pso[i], n = d.psn[i];
+    x = x - dt * d.psc[i] * (p[n] - p[o]);
+    if (with_cross) x = x - dt * ps_cross_d(d, gp, i, o, n);
+    return x;
+  };
+  if (f < d.nfi) { Uf[f] = corr(f, ff[f]); return; }
+  int b = f - d.nfi, bc = d.bbc[b];
+  if (bc == BC_PERIODIC) {
+    int i = d.bps[b];
+    if (i < 0) { Uf[f] = ff[f]; return; }
+    double v = corr(i, ff[d.psf[i]]);
+    Uf[f] = d.bcanon[b] ? v : -v;
+    return;
+  }
+  if (bc == BC_OUTLET) {
+    int o = d.fo[f];
+    double v = ff[f] - dt * d.bcb[b] * ((ptot ? d.bpval[b] : 0.0) - p[o]);
+    if (with_cross) v = v - dt * (gp[o] * d.bkout[b] + gp[nc + o] * d.bkout[nb + b] + gp[2 * nc + o] * d.bkout[2 * nb + b]);
+    Uf[f] = v;
+    return;
+  }
+  Uf[f] = ff[f];
+}
+
+// ------------------------------------------------------------------------------------------
+// Convective and diffusive CFL rates per cell (src/solver/mod_fv_solver.f90:3718-3871).
+__global__ void __launch_bounds__(TPB) k_cfl_cell(Dev d, double nu, int ready, const double* __restrict__ U,
+                                                  const double* __restrict__ Uf, const double* __restrict__ nus,
+                                                  double* __restrict__ conv, double* __restrict__ diff) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.nc) return;
+  const int nc = d.nc, nf = d.nf;
+  double fs = 0.0, ds = 0.0;
+  for (int s = 0; s < d.S; ++s) {
+    int f = d.cf[s * nc + c];
+    if (f == PADI) break;
+    int o = d.fo[f], n = d.fn[f];
+    double sf0 = d.sf[f], sf1 = d.sf[nf + f], sf2 = d.sf[2 * nf + f];
+    double area = sqrt(sf0 * sf0 + sf1 * sf1 + sf2 * sf2);
+    double uf = ready ? Uf[f] : (U[o] * sf0 + U[nc + o] * sf1 + U[2 * nc + o] * sf2);
+    fs += fabs(uf);
+    double w = area / fmax(d.dcf[f], SMALLD);
+    if (n >= 0) {
+      double g = d.gc[f];
+      double ne = nu + g * fmax(0.0, nus[o]) + (1.0 - g) * fmax(0.0, nus[n]);
+      ds += ne * w;
+    } else if (d.bbc[f - d.nfi] != BC_WALL_MODEL) {
+      ds += (nu + fmax(0.0, nus[c])) * w;
+    }
+  }
+  conv[c] = fs / (d.vol[c] + SMALLD);
+  diff[c] = ds / (d.vol[c] + SMALLD);
+}
+
+// Face-flux divergence per cell (src/solver/mod_fv_solver.f90:3532-3580).
+__global__ void __launch_bounds__(TPB) k_flux_divergence(Dev d, const double* __restrict__ Uf, double* __restrict__ div) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.nc) return;
+  const int nc = d.nc;
+  const double iv = d.ivol[c];
+  double v = 0.0;
+  for (int s = 0; s < d.SP; ++s) {
+    int e = d.cps[s * nc + c];
+    if (e == PADI) break;
+    if (e >= 0) v += Uf[d.psf[e]] * iv;
+    else v -= Uf[d.psf[~e]] * iv;
+  }
+  for (int s = 0; s < d.SB; ++s) {
+    int b = d.cbn[s * nc + c];
+    if (b == PADI) break;
+    if (d.bbc[b] == BC_PERIODIC) continue;
+    v += Uf[d.nfi + b] * iv;
+  }
+  div[c] = v;
+}
+
+// ------------------------------------------------------------------------------------------
+// Small elementwise kernels.
+__global__ void k_rotational(int n, double* p, const double* nus, const double* rhs, const double* ivol, double nu,
+                             double dt) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < n) p[c] = p[c] + (nu + nus[c]) * rhs[c] * dt * ivol[c];
+}
+__global__ void k_add(int n, double* p, const double* q) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < n) p[c] = p[c] + q[c];
+}
+__global__ void k_sub(int n, double* a, const double* b) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < n) a[c] = a[c] - b[c];
+}
+__global__ void k_shift(int n, double* p, const double* shift) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < n) p[c] = p[c] - *shift;
+}
+__global__ void k_fill(int n, double* p, double v) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < n) p[c] = v;
+}
+__global__ void k_aos_to_soa(int n, const double* aos, double* soa) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < n) { soa[c] = aos[3 * c]; soa[n + c] = aos[3 * c + 1]; soa[2 * n + c] = aos[3 * c + 2]; }
+}
+__global__ void k_soa_to_aos(int n, const double* soa, double* aos) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < n) { aos[3 * c] = soa[c]; aos[3 * c + 1] = soa[n + c]; aos[3 * c + 2] = soa[2 * n + c]; }
+}
+// grad(3,3,n) Fortran layout (i fastest, then j, then cell) <-> SoA [(3j+i)][n]
+__global__ void k_grad_soa_to_aos(int n, const double* soa, double* aos) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < n)
+    for (int j = 0; j < 9; ++j) aos[9 * c + j] = soa[j * n + c];
+}
+__global__ void k_grad_aos_to_soa(int n, const double* aos, double* soa) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < n)
+    for (int j = 0; j < 9; ++j) soa[j * n + c] = aos[9 * c + j];
+}
+
+}  // namespace gpu
+}  // namespace dpm

@@ -1,0 +1,1064 @@
+// Device-resident RK3W fractional-step solver and its C ABI (include/dopamine_b200.h).
+//
+// The stage sequence mirrors advance_rk3w (src/solver/mod_fv_solver.f90:1180-1614): BC refresh,
+// velocity gradients, SGS viscosity, wall model, explicit right-hand side and predictor,
+// pre-correction with the old pressure, second gradient pass, Poisson block with Jasak
+// correctors, flux and velocity projection, rotational pressure correction, pressure update.
+// All fields stay in HBM; the host only launches kernels and reads back the few scalars that
+// steer the control flow (CFL-clamped dt, corrector exit test, Krylov status).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../../include/dopamine_b200.h"
+#include "../host/mesh.hpp"
+#include "../host/ops.hpp"
+#include "common.cuh"
+#include "kernels.cuh"
+#include "pcg.cuh"
+
+namespace dpm {
+namespace gpu {
+
+const double RK3W_ALPHA[3] = {8.0 / 15.0, 5.0 / 12.0, 3.0 / 4.0};  // src/mod_parameters.f90:64-71
+const double RK3W_BETA[3] = {0.0, -17.0 / 60.0, -5.0 / 12.0};
+const double RK3W_GAMMA[3] = {8.0 / 15.0, 2.0 / 15.0, 1.0 / 3.0};
+const double RK3W_C[3] = {0.0, 8.0 / 15.0, 2.0 / 3.0};
+
+#define CK(x)                                                                                      \
+  do {                                                                                             \
+    cudaError_t e_ = (x);                                                                          \
+    if (e_ != cudaSuccess) {                                                                       \
+      std::fprintf(stderr, "dopamine_b200: CUDA error %s at %s:%d\n", cudaGetErrorString(e_), __FILE__, \
+                   __LINE__);                                                                      \
+      return DPM_ERR_CUDA;                                                                         \
+    }                                                                                              \
+  } while (0)
+
+struct DMem {
+  std::vector<void*> ptrs;
+  ~DMem() {
+    for (void* p : ptrs) cudaFree(p);
+  }
+  template <class T>
+  T* alloc(size_t n) {
+    void* p = nullptr;
+    if (cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)) != cudaSuccess) return nullptr;
+    cudaMemset(p, 0, std::max<size_t>(n, 1) * sizeof(T));
+    ptrs.push_back(p);
+    return static_cast<T*>(p);
+  }
+  template <class T>
+  T* upload(const std::vector<T>& v) {
+    T* p = alloc<T>(v.size());
+    if (p && !v.empty()) cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
+    return p;
+  }
+};
+
+inline int nblk(int64_t n) { return (int)((n + TPB - 1) / TPB); }
+
+// ---- deterministic reductions: per-block partials, then one block sums them in order --------
+enum RedMode { RED_MAXABS = 0, RED_SUM2 = 1, RED_UBULK = 2, RED_STATS = 3, RED_MAX2 = 4, RED_DIVSTAT = 5 };
+constexpr int RED_NV = 10;
+
+struct RedArgs {
+  int mode, n;
+  const double *a, *b, *c, *vol, *gU, *nus;
+  double nu;
+};
+
+__global__ void __launch_bounds__(TPB) k_reduce_partial(RedArgs r, double* partials) {
+  double v[RED_NV];
+  for (int k = 0; k < RED_NV; ++k) v[k] = 0.0;
+  const int n = r.n;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    switch (r.mode) {
+      case RED_MAXABS: v[0] = fmax(v[0], fabs(r.a[i])); break;
+      case RED_SUM2: v[0] += r.a[i] * r.b[i]; v[1] += r.b[i]; break;
+      case RED_UBULK: {
+        double u0 = r.a[i], u1 = r.a[n + i], u2 = r.a[2 * n + i];
+        v[0] += sqrt(u0 * u0 + u1 * u1 + u2 * u2) * r.vol[i];
+        v[1] += r.vol[i];
+        break;
+      }
+      case RED_MAX2: v[0] = fmax(v[0], r.a[i]); v[1] = fmax(v[1], r.b[i]); break;
+      case RED_STATS: {
+        double vv = r.vol[i];
+        double u0 = r.a[i], u1 = r.a[n + i], u2 = r.a[2 * n + i];
+        const double* g = r.gU;
+        double S11 = g[0 * n + i], S22 = g[4 * n + i], S33 = g[8 * n + i];
+        double S12 = 0.5 * (g[1 * n + i] + g[3 * n + i]), S13 = 0.5 * (g[2 * n + i] + g[6 * n + i]);
+        double S23 = 0.5 * (g[5 * n + i] + g[7 * n + i]);
+        double SS = S11 * S11 + S22 * S22 + S33 * S33 + 2.0 * (S12 * S12 + S13 * S13 + S23 * S23);
+        v[0] += 0.5 * (u0 * u0 + u1 * u1 + u2 * u2) * vv;
+        v[1] += vv;
+        v[2] += (r.nu + r.nus[i]) * SS * vv;
+        v[3] += u0 * vv; v[4] += u1 * vv; v[5] += u2 * vv;
+        v[6] += r.nus[i] * vv;
+        v[7] = fmax(v[7], sqrt(u0 * u0 + u1 * u1 + u2 * u2));
+        break;
+      }
+      case RED_DIVSTAT: v[0] = fmax(v[0], fabs(r.a[i])); v[1] += fabs(r.a[i]) * r.vol[i]; v[2] += r.vol[i]; break;
+    }
+  }
+  __shared__ double sh[TPB / 32][RED_NV];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int k = 0; k < RED_NV; ++k) {
+    bool mx = (r.mode == RED_MAXABS && k == 0) || (r.mode == RED_MAX2 && k < 2) || (r.mode == RED_STATS && k == 7) ||
+              (r.mode == RED_DIVSTAT && k == 0);
+    double t = v[k];
+    for (int o = 16; o > 0; o >>= 1) {
+      double u = __shfl_down_sync(0xffffffffu, t, o);
+      t = mx ? fmax(t, u) : t + u;
+    }
+    if (lane == 0) sh[w][k] = t;
+  }
+  __syncthreads();
+  if (threadIdx.x < RED_NV) {
+    int k = threadIdx.x;
+    bool mx = (r.mode == RED_MAXABS && k == 0) || (r.mode == RED_MAX2 && k < 2) || (r.mode == RED_STATS && k == 7) ||
+              (r.mode == RED_DIVSTAT && k == 0);
+    double t = sh[0][k];
+    for (int j = 1; j < TPB / 32; ++j) t = mx ? fmax(t, sh[j][k]) : t + sh[j][k];
+    partials[blockIdx.x * RED_NV + k] = t;
+  }
+}
+
+__global__ void k_reduce_final(int mode, int nparts, const double* partials, double* out) {
+  int k = threadIdx.x;
+  if (k >= RED_NV) return;
+  bool mx = (mode == RED_MAXABS && k == 0) || (mode == RED_MAX2 && k < 2) || (mode == RED_STATS && k == 7) ||
+            (mode == RED_DIVSTAT && k == 0);
+  double t = mx ? 0.0 : 0.0;
+  for (int j = 0; j < nparts; ++j) t = mx ? fmax(t, partials[j * RED_NV + k]) : t + partials[j * RED_NV + k];
+  out[k] = t;
+}
+
+// anchor_pressure_to_outlet (mod_fv_solver.f90:3610-3641): shift = sum(p V) / V_total.
+__global__ void k_anchor_shift(const double* sums, double vtot, double* shift) { *shift = vtot > 0.0 ? sums[0] / vtot : 0.0; }
+
+// ------------------------------------------------------------------------------------------
+struct Solver {
+  int device = 0;
+  cudaStream_t st = nullptr;
+  Mesh m;
+  StaticOps S;
+  dpm_params_t P{};
+  std::vector<dpm_patch_cfg_t> pc;
+  DMem mem;
+  Dev d{};
+  Fld F{};
+  int nc = 0, nf = 0, nb = 0, nfp = 0;
+  // scratch
+  double *red_part = nullptr, *red_out = nullptr, *scratch_c = nullptr, *scratch_c2 = nullptr;
+  double *aos_buf = nullptr;
+  double *conv_tmp = nullptr, *visc_tmp = nullptr;
+  // PCG workspace
+  double *cg_r, *cg_z, *cg_p0, *cg_p1, *cg_q, *cg_bp, *cg_x, *cg_part, *cg_dout;
+  unsigned* cg_bar;
+  int* cg_status;
+  int cg_grid = 0;
+  bool cg_coop = true;
+  // state
+  double time = 0.0;
+  int64_t step = 0;
+  bool u_face_ready = false;
+  bool filt_ready = false;
+  int64_t launches = 0;
+  dpm_stats_t last{};
+  double last_step_ms = 0.0, last_poisson_ms = 0.0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, evp0 = nullptr, evp1 = nullptr;
+  double poisson_ms_acc = 0.0;
+
+  ~Solver() {
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (evp0) cudaEventDestroy(evp0);
+    if (evp1) cudaEventDestroy(evp1);
+    if (st) cudaStreamDestroy(st);
+  }
+
+  int init(const dpm_raw_mesh_t* raw, const dpm_patch_cfg_t* patches, const dpm_params_t* prm, int dev) {
+    device = dev;
+    CK(cudaSetDevice(device));
+    CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    CK(cudaEventCreate(&ev0)); CK(cudaEventCreate(&ev1)); CK(cudaEventCreate(&evp0)); CK(cudaEventCreate(&evp1));
+    RawMesh r;
+    r.n_nodes = raw->n_nodes; r.xyz = raw->xyz; r.n_cells = raw->n_cells; r.cell_type = raw->cell_type;
+    r.cell_off = raw->cell_off; r.cell_nodes = raw->cell_nodes; r.n_bfaces = raw->n_bfaces;
+    r.bface_off = raw->bface_off; r.bface_nodes = raw->bface_nodes; r.bface_patch = raw->bface_patch;
+    r.n_patches = raw->n_patches;
+    std::vector<int> pbc(raw->n_patches);
+    for (int i = 0; i < raw->n_patches; ++i) pbc[i] = patches[i].bc_id;
+    std::string err;
+    if (build_mesh(r, pbc.data(), m, &err)) {
+      std::fprintf(stderr, "dopamine_b200: mesh set-up failed: %s\n", err.c_str());
+      return DPM_ERR_MESH;
+    }
+    P = *prm;
+    pc.assign(patches, patches + raw->n_patches);
+    if (build_static_ops(m, pc.data(), P, S)) return DPM_ERR_MESH;
+    if (m.n_cells > 2000000000LL || m.n_faces > 2000000000LL) return DPM_ERR_UNSUPPORTED;
+    nc = (int)m.n_cells; nf = (int)m.n_faces; nb = (int)m.n_bnd_faces; nfp = (int)S.nfp;
+    return upload();
+  }
+
+  template <class T>
+  static std::vector<T> soa3(const std::vector<T>& aos, int64_t n) {
+    std::vector<T> s(3 * n);
+    for (int64_t i = 0; i < n; ++i)
+      for (int k = 0; k < 3; ++k) s[k * n + i] = aos[3 * i + k];
+    return s;
+  }
+  template <class T>
+  static std::vector<T> soa9(const std::vector<T>& aos, int64_t n) {
+    std::vector<T> s(9 * n);
+    for (int64_t i = 0; i < n; ++i)
+      for (int k = 0; k < 9; ++k) s[k * n + i] = aos[9 * i + k];
+    return s;
+  }
+
+  int upload() {
+    const int64_t nfi = m.n_int_faces;
+    d.nc = nc; d.nf = nf; d.nfi = (int)nfi; d.nb = nb; d.nfp = nfp;
+    d.S = S.S; d.SP = S.SP; d.SB = S.SB; d.W = S.W; d.WA = S.WA;
+    std::vector<double> ivol(nc);
+    for (int c = 0; c < nc; ++c) ivol[c] = 1.0 / std::max(m.volume[c], SMALL);
+    d.vol = mem.upload(m.volume);
+    d.ivol = mem.upload(ivol);
+    d.cen = mem.upload(soa3(m.centroid, nc));
+    d.Tinv = mem.upload(soa9(S.Tinv, nc));
+    d.G = mem.upload(soa9(S.G, nc));
+    d.cf = mem.upload(S.cell_face);
+    d.cps = mem.upload(S.cell_ps);
+    d.cbn = mem.upload(S.cell_bnd);
+    d.ls_idx = mem.upload(S.ls_idx);
+    d.ls_w = mem.upload(S.ls_w);
+    d.fo = mem.upload(m.owner);
+    d.fn = mem.upload(m.neighbour);
+    d.sf = mem.upload(soa3(m.sf, nf));
+    d.nrm = mem.upload(soa3(m.normal, nf));
+    d.fcen = mem.upload(soa3(m.centre, nf));
+    d.eps = mem.upload(soa3(m.eps, nf));
+    d.area = mem.upload(m.area);
+    d.gc = mem.upload(m.gc);
+    d.wbl = mem.upload(S.wblend);
+    d.dcf = mem.upload(m.d_cf);
+    std::vector<int> bps(nb, -1), bcanon(nb, 0);
+    for (int i = (int)nfi; i < nfp; ++i) {
+      int b = S.ps_f[i] - (int)nfi;
+      bps[b] = i;
+      bcanon[b] = 1;
+      int pb = m.periodic_pair[b];
+      if (pb >= 0) bps[pb] = i;
+    }
+    std::vector<double> bU(3 * nb, 0.0), bp(nb, 0.0);
+    for (int b = 0; b < nb; ++b) {
+      int p = m.patch[nfi + b];
+      if (p < 0) continue;
+      for (int k = 0; k < 3; ++k) bU[k * nb + b] = pc[p].U_val[k];
+      bp[b] = pc[p].p_val;
+    }
+    d.bbc = mem.upload(S.bnd_bc);
+    d.bpnb = mem.upload(S.bnd_pnb);
+    d.bpair = mem.upload(m.periodic_pair);
+    d.bps = mem.upload(bps);
+    d.bcanon = mem.upload(bcanon);
+    d.bpgc = mem.upload(m.periodic_gc);
+    d.bpdcf = mem.upload(m.periodic_pair_dcf);
+    d.bcb = mem.upload(S.bnd_cb);
+    d.bkout = mem.upload(S.bnd_kout);
+    d.yw = mem.upload(S.y_w);
+    d.bUval = mem.upload(bU);
+    d.bpval = mem.upload(bp);
+    d.pso = mem.upload(S.ps_o);
+    d.psn = mem.upload(S.ps_n);
+    d.psf = mem.upload(S.ps_f);
+    d.psc = mem.upload(S.ps_coeff);
+    d.psgcf = mem.upload(S.ps_gcf);
+    d.psgcw = mem.upload(S.ps_gcw);
+    d.psk = mem.upload(S.ps_k);
+    d.pskrc = mem.upload(S.ps_krc);
+    d.Acol = mem.upload(S.A_col);
+    d.Aval = mem.upload(S.A_val);
+    std::vector<double> dinv(nc);
+    for (int c = 0; c < nc; ++c) dinv[c] = 1.0 / S.diag[c];
+    d.Adinv = mem.upload(dinv);
+    // fields
+    F.U = mem.alloc<double>(3 * nc);
+    F.p = mem.alloc<double>(nc); F.p_old = mem.alloc<double>(nc); F.phi_prev = mem.alloc<double>(nc);
+    F.nu_sgs = mem.alloc<double>(nc); F.rhs = mem.alloc<double>(nc); F.T = mem.alloc<double>(nc);
+    F.Ub = mem.alloc<double>(3 * nb); F.pb = mem.alloc<double>(nb); F.phi_prev_b = mem.alloc<double>(nb);
+    F.tau = mem.alloc<double>(3 * nb); F.upf = mem.alloc<double>(3 * nb);
+    F.gU = mem.alloc<double>(9 * nc); F.gp = mem.alloc<double>(3 * nc); F.gp_rc = mem.alloc<double>(3 * nc);
+    F.gpc = mem.alloc<double>(3 * nc); F.H = mem.alloc<double>(3 * nc); F.H0 = mem.alloc<double>(3 * nc);
+    F.ff = mem.alloc<double>(nf); F.Uf = mem.alloc<double>(nf);
+    F.fadv = mem.alloc<double>(3 * nf); F.fvis = mem.alloc<double>(3 * nf); F.fdiv = mem.alloc<double>(nf);
+    F.ps_cross = mem.alloc<double>(nfp);
+    F.ptot = mem.alloc<double>(nc); F.ptot_b = mem.alloc<double>(nb); F.phi_it = mem.alloc<double>(nc);
+    red_part = mem.alloc<double>(RED_NV * 2048);
+    red_out = mem.alloc<double>(RED_NV);
+    scratch_c = mem.alloc<double>(nc); scratch_c2 = mem.alloc<double>(nc);
+    aos_buf = mem.alloc<double>(9 * (size_t)std::max(nc, nf));
+    conv_tmp = mem.alloc<double>(3 * nc); visc_tmp = mem.alloc<double>(3 * nc);
+    cg_r = mem.alloc<double>(nc); cg_z = mem.alloc<double>(nc); cg_p0 = mem.alloc<double>(nc);
+    cg_p1 = mem.alloc<double>(nc); cg_q = mem.alloc<double>(nc); cg_bp = mem.alloc<double>(nc);
+    cg_x = mem.alloc<double>(nc);
+    cg_bar = mem.alloc<unsigned>(2); cg_status = mem.alloc<int>(4); cg_dout = mem.alloc<double>(4);
+    if (!cg_dout || !F.fadv || !aos_buf) return DPM_ERR_CUDA;
+    // cooperative grid for the persistent PCG
+    int dev_sms = 0, per_sm = 0, coop = 0;
+    CK(cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, device));
+    CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg<double>, TPB, 0));
+    cg_coop = coop != 0 && per_sm > 0;
+    if (!cg_coop) return DPM_ERR_UNSUPPORTED;
+    cg_grid = std::min(dev_sms * per_sm, std::max(1, nblk(nc)));
+    cg_grid = std::min(cg_grid, 2048);
+    cg_part = mem.alloc<double>(2 * 4 * (size_t)cg_grid);
+    // initial fields: T = T_ref, velocity from an inlet patch (initialize_velocity_from_bc)
+    launch_fill(F.T, nc, P.T_ref);
+    double u0[3] = {0, 0, 0};
+    for (auto& q : pc)
+      if (q.bc_id == BC_INLET) { for (int k = 0; k < 3; ++k) u0[k] = q.U_val[k]; break; }
+    for (int k = 0; k < 3; ++k) launch_fill(F.U + (size_t)k * nc, nc, u0[k]);
+    CK(cudaGetLastError());
+    return 0;
+  }
+
+  void launch_fill(double* p, int64_t n, double v) {
+    k_fill<<<nblk(n), TPB, 0, st>>>((int)n, p, v);
+    launches++;
+  }
+
+  // ---------------------------------------------------------------- building blocks
+  void velocity_bc(int filt, int have_grad) {
+    if (nb == 0) return;
+    k_velocity_bc<<<nblk(nb), TPB, 0, st>>>(d, F.U, F.gU, F.Ub, filt, have_grad);
+    launches++;
+  }
+  void pressure_bc(const double* pf, int filt, int have_grad, int incr) {
+    if (nb == 0) return;
+    k_pressure_bc<<<nblk(nb), TPB, 0, st>>>(d, pf, F.gp, F.pb, filt, have_grad, incr);
+    launches++;
+  }
+  void refresh_halos_and_bc() {
+    velocity_bc(0, 1);
+    pressure_bc(F.p, 0, !S.skip_grad_p, 0);
+    velocity_bc(1, 1);
+    pressure_bc(F.p, 1, 0, 0);
+  }
+  void velocity_bc_refresh() {
+    velocity_bc(0, 1);
+    velocity_bc(1, 1);
+  }
+  void grad_U() {
+    k_ls_gradient_vector<<<nblk(nc), TPB, 0, st>>>(d, F.U, F.Ub, F.gU);
+    launches++;
+  }
+  void grad_scalar(const double* phi, const double* pb, double* g) {
+    k_ls_gradient_scalar<<<nblk(nc), TPB, 0, st>>>(d, phi, pb, g);
+    launches++;
+  }
+  void pressure_gradient() {
+    if (!S.skip_grad_p) grad_scalar(F.p, F.pb, F.gp);
+  }
+  void copy(double* dst, const double* src, size_t n) { cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyDeviceToDevice, st); }
+
+  int reduce(RedArgs r, double* host_out, int nv) {
+    int g = std::min(nblk(r.n), 2048);
+    if (g < 1) g = 1;
+    k_reduce_partial<<<g, TPB, 0, st>>>(r, red_part);
+    k_reduce_final<<<1, 32, 0, st>>>(r.mode, g, red_part, red_out);
+    launches += 2;
+    if (host_out) {
+      CK(cudaMemcpyAsync(host_out, red_out, nv * sizeof(double), cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+    }
+    return 0;
+  }
+
+  void anchor_pressure() {
+    if (S.n_outlet > 0) return;
+    RedArgs r{};
+    r.mode = RED_SUM2; r.n = nc; r.a = F.p; r.b = d.vol;
+    reduce(r, nullptr, 0);
+    k_anchor_shift<<<1, 1, 0, st>>>(red_out, S.V_total, red_out + 8);
+    k_shift<<<nblk(nc), TPB, 0, st>>>(nc, F.p, red_out + 8);
+    launches += 2;
+  }
+
+  int atol_dynamic(double dt, double& atol) {
+    RedArgs r{};
+    r.mode = RED_UBULK; r.n = nc; r.a = F.U; r.vol = d.vol;
+    double o[2];
+    int rc = reduce(r, o, 2);
+    if (rc) return rc;
+    double us = o[0] / std::max(o[1], SMALL);
+    atol = std::max(1.0e-12 * std::max(us, 1.0) * S.V_min / dt, 1.0e-15);
+    return 0;
+  }
+
+  void sgs(double dt_stab) {
+    if (P.sgs_model == DPM_SGS_NONE) {
+      launch_fill(F.nu_sgs, nc, 0.0);
+      return;
+    }
+    k_sgs<<<nblk(nc), TPB, 0, st>>>(d, P.sgs_model, F.gU, F.nu_sgs, dt_stab, P.c_amd);
+    launches++;
+    if (P.sgs_model == DPM_SGS_AMD && P.amd_wall_gradient && nb > 0) {
+      k_amd_wall<<<nblk(nc), TPB, 0, st>>>(d, F.U, F.gU, F.nu_sgs, P.nu, P.c_amd, dt_stab);
+      launches++;
+    }
+  }
+
+  void wall_model(double dt_filter) {
+    if (nb == 0) return;
+    if (P.wall_model == DPM_WM_NONE) {
+      launch_fill(F.tau, 3 * (int64_t)nb, 0.0);
+      return;
+    }
+    double t_use = P.wall_model_filter_time, tf = P.wall_model_filter_tf_fac;
+    bool adaptive = tf > SMALL;
+    int filter = adaptive ? 2 : (t_use > SMALL ? 1 : 0);
+    double w_filt = (filter == 1) ? dt_filter / (t_use + dt_filter) : 0.0;
+    k_wall_model<<<nblk(nb), TPB, 0, st>>>(d, F.U, F.tau, F.upf, P.nu, filter, filt_ready ? 0 : 1, w_filt, dt_filter, tf);
+    launches++;
+    if (filter) filt_ready = true;
+  }
+
+  void explicit_rhs(double dt, double a_k, double b_k, int predict) {
+    k_face_explicit<<<nblk(nf), TPB, 0, st>>>(d, P.scheme, P.nu, F.U, F.Ub, F.gU, F.nu_sgs, F.Uf, F.fadv, F.fvis, F.fdiv);
+    ExplicitArgs a{};
+    a.scheme = P.scheme;
+    a.f0 = P.f_const[0]; a.f1 = P.f_const[1]; a.f2 = P.f_const[2];
+    a.bous = P.boussinesq; a.beta = P.beta; a.T_ref = P.T_ref; a.g0 = P.g[0]; a.g1 = P.g[1]; a.g2 = P.g[2];
+    a.dt = dt; a.a_k = a_k; a.b_k = b_k; a.predict = predict;
+    k_cell_explicit<<<nblk(nc), TPB, 0, st>>>(d, a, F.U, F.T, F.fadv, F.fvis, F.fdiv, F.tau, F.H, F.H0,
+                                                predict ? nullptr : conv_tmp, predict ? nullptr : visc_tmp);
+    launches += 2;
+  }
+
+  void correct_velocity(double dt, bool with_cross, bool ptot) {
+    CorrArgs a{};
+    a.dt = dt;
+    a.do_cross = with_cross && !S.skip_nonortho;
+    a.ptot = ptot;
+    a.f0 = P.f_const[0]; a.f1 = P.f_const[1]; a.f2 = P.f_const[2];
+    a.bb = P.boussinesq ? P.beta : 0.0; a.T_ref = P.T_ref; a.g0 = P.g[0]; a.g1 = P.g[1]; a.g2 = P.g[2];
+    k_correct_velocity<<<nblk(nc), TPB, 0, st>>>(d, a, F.p, F.gp, F.T, F.U, F.gpc);
+    launches++;
+  }
+
+  void face_fluxes_and_rhs(double dt, bool incr) {
+    if (!S.skip_grad_p) {
+      if (incr) {
+        copy(F.ptot, F.phi_prev, nc);
+        copy(F.ptot_b, F.phi_prev_b, nb);
+        k_add<<<nblk(nc), TPB, 0, st>>>(nc, F.ptot, F.p);
+        if (nb) k_add<<<nblk(nb), TPB, 0, st>>>(nb, F.ptot_b, F.pb);
+        launches += 2;
+        grad_scalar(F.ptot, F.ptot_b, F.gp);
+      } else {
+        grad_scalar(F.p, F.pb, F.gp);
+      }
+    }
+    int wc = !S.skip_nonortho;
+    k_face_flux<<<nblk(nf), TPB, 0, st>>>(d, dt, F.U, F.gU, F.gp_rc, F.phi_prev, F.Ub, F.gp, wc, F.ff, F.ps_cross);
+    k_rhs_gather<<<nblk(nc), TPB, 0, st>>>(d, 1.0 / std::max(dt, SMALL), wc, F.ff, F.ps_cross, F.gp, F.rhs);
+    launches += 2;
+  }
+
+  void correct_face_fluxes(double dt, bool ptot) {
+    k_correct_face_flux<<<nblk(nf), TPB, 0, st>>>(d, dt, ptot, !S.skip_nonortho, F.p, F.gp, F.ff, F.Uf);
+    launches++;
+  }
+
+  // ---------------------------------------------------------------- Poisson solve
+  int pcg(const double* rhs, double* x, double rtol, double atol, int maxit, int guess_zero, int* its, double* resid,
+          int* reason) {
+    PcgArgs<double> a{};
+    a.n = nc; a.WA = S.WA; a.col = d.Acol; a.val = d.Aval; a.dinv = d.Adinv;
+    a.b = rhs; a.x = x; a.r = cg_r; a.z = cg_z; a.p0 = cg_p0; a.p1 = cg_p1; a.q = cg_q; a.bp = cg_bp;
+    a.partials = cg_part; a.bar = cg_bar; a.status = cg_status; a.dout = cg_dout;
+    a.rtol = rtol; a.atol = atol; a.maxit = maxit; a.nullsp = S.dir_rows.empty() ? 1 : 0; a.guess_zero = guess_zero;
+    CK(cudaMemsetAsync(cg_bar, 0, 2 * sizeof(unsigned), st));
+    CK(cudaMemsetAsync(cg_status, 0, 4 * sizeof(int), st));
+    void* args[] = {&a};
+    CK(cudaLaunchCooperativeKernel((void*)k_pcg<double>, dim3(cg_grid), dim3(TPB), args, 0, st));
+    launches++;
+    int h_st[4];
+    double h_d[4];
+    CK(cudaMemcpyAsync(h_st, cg_status, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(h_d, cg_dout, 4 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (h_st[2]) {
+      std::fprintf(stderr, "dopamine_b200: PCG grid barrier timed out\n");
+      return DPM_ERR_CUDA;
+    }
+    *reason = h_st[0];
+    *its = h_st[1];
+    *resid = h_d[0];
+    return 0;
+  }
+
+  // pressure_solver_solve + fvm_petsc_solve_pressure: NaN scrub, Dirichlet rows when the
+  // pressure is total, BJACOBI-style retry from a zero guess on failure.
+  int pressure_solve(double tol, double atol, bool ptot, int* its_out, double* res_out) {
+    const double* rhs = F.rhs;
+    if (ptot && !S.dir_rows.empty()) {
+      std::vector<double> add(nc, 0.0);
+      for (size_t k = 0; k < S.dir_rows.size(); ++k) add[S.dir_rows[k]] += S.dir_vals[k];
+      CK(cudaMemcpyAsync(scratch_c2, add.data(), nc * sizeof(double), cudaMemcpyHostToDevice, st));
+      copy(scratch_c, F.rhs, nc);
+      k_add<<<nblk(nc), TPB, 0, st>>>(nc, scratch_c, scratch_c2);
+      launches++;
+      rhs = scratch_c;
+    }
+    int maxit = std::max(P.p_max_iter, 2000), its = 0, reason = 0;
+    double res = 0.0;
+    cudaEventRecord(evp0, st);
+    int rc = pcg(rhs, F.p, tol, atol, maxit, 0, &its, &res, &reason);
+    if (rc) return rc;
+    if (reason < 0) {
+      rc = pcg(rhs, F.p, tol, atol, 4 * maxit, 1, &its, &res, &reason);
+      if (rc) return rc;
+      if (reason < 0 && !(reason == -3 && (res < tol * 1.0e4 || res < atol * 1.0e3))) return -(1000 + reason);
+    }
+    cudaEventRecord(evp1, st);
+    cudaEventSynchronize(evp1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, evp0, evp1);
+    poisson_ms_acc += ms;
+    *its_out = its;
+    *res_out = res;
+    return 0;
+  }
+
+  // ---------------------------------------------------------------- solver_project_once
+  int project_once(double dt) {
+    launch_fill(F.rhs, nc, 0.0);
+    launch_fill(F.phi_prev, nc, 0.0);
+    if (nb) launch_fill(F.phi_prev_b, nb, 0.0);
+    launch_fill(F.gp_rc, 3 * (int64_t)nc, 0.0);
+    refresh_halos_and_bc();
+    face_fluxes_and_rhs(dt, false);
+    if (P.p_max_iter > 0) {
+      double atol;
+      int rc = atol_dynamic(dt, atol);
+      if (rc) return rc;
+      int its;
+      double res;
+      rc = pressure_solve(P.p_tol, atol, true, &its, &res);
+      if (rc) return rc;
+    }
+    anchor_pressure();
+    correct_face_fluxes(dt, true);
+    copy(F.ff, F.Uf, nf);
+    u_face_ready = true;
+    pressure_bc(F.p, -1, 0, 0);
+    correct_velocity(dt, true, true);
+    velocity_bc(-1, 0);
+    if (P.use_rotational_projection) {
+      k_rotational<<<nblk(nc), TPB, 0, st>>>(nc, F.p, F.nu_sgs, F.rhs, d.ivol, P.nu, dt);
+      launches++;
+      pressure_bc(F.p, -1, 0, 0);
+    }
+    copy(F.p_old, F.p, nc);
+    copy(F.phi_prev, F.p, nc);
+    copy(F.phi_prev_b, F.pb, nb);
+    pressure_bc(F.p, -1, 0, 0);
+    pressure_gradient();
+    CK(cudaStreamSynchronize(st));
+    CK(cudaGetLastError());
+    return 0;
+  }
+
+  // ---------------------------------------------------------------- CFL (solver_compute_dt)
+  int compute_dt(double& dt) {
+    k_cfl_cell<<<nblk(nc), TPB, 0, st>>>(d, P.nu, u_face_ready, F.U, F.Uf, F.nu_sgs, scratch_c, scratch_c2);
+    launches++;
+    RedArgs r{};
+    r.mode = RED_MAX2; r.n = nc; r.a = scratch_c; r.b = scratch_c2;
+    double o[2];
+    int rc = reduce(r, o, 2);
+    if (rc) return rc;
+    double dc = 1e308, dd = 1e308;
+    if (o[0] > SMALL) dc = P.cfl_max / o[0];
+    if (o[1] > SMALL) dd = 1.0 / o[1];
+    dt = std::min(dc, dd);
+    if (!(dt > 0.0)) dt = P.dt;
+    dt = std::min(dt, P.dt);
+    if (!(dt > 0.0)) dt = P.dt;
+    else if (dt < 1.0e-6 * P.dt) return DPM_ERR_DT_COLLAPSE;
+    return 0;
+  }
+
+  // ---------------------------------------------------------------- solver_advance
+  int advance(double dt_in) {
+    double dt = dt_in;
+    if (!P.adapt_dt) {
+      double ds;
+      int rc = compute_dt(ds);
+      if (rc) return rc;
+      if (dt > ds) dt = ds;
+    }
+    poisson_ms_acc = 0.0;
+    cudaEventRecord(ev0, st);
+    last.dt_used = dt;
+    last.p_solves = 0; last.p_iters = 0; last.p_resid_max = 0.0;
+    launch_fill(F.H, 3 * (int64_t)nc, 0.0);
+    launch_fill(F.H0, 3 * (int64_t)nc, 0.0);
+    launch_fill(F.rhs, nc, 0.0);
+    double time_n = time;
+    for (int k = 0; k < 3; ++k) {
+      double gk_dt = RK3W_GAMMA[k] * dt;
+      time = time_n + RK3W_C[k] * dt;
+      refresh_halos_and_bc();
+      grad_U();
+      sgs(gk_dt);
+      wall_model(k == 0 ? dt : 0.0);
+      explicit_rhs(dt, RK3W_ALPHA[k], RK3W_BETA[k], 1);
+      velocity_bc_refresh();
+      copy(F.p_old, F.p, nc);
+      correct_velocity(gk_dt, false, true);
+      copy(F.gp_rc, F.gpc, 3 * (size_t)nc);
+      velocity_bc_refresh();
+      grad_U();
+      copy(F.phi_prev, F.p, nc);
+      copy(F.phi_prev_b, F.pb, nb);
+      double atol;
+      int rc = atol_dynamic(gk_dt, atol);
+      if (rc) return rc;
+      int n_max;
+      double stag;
+      if (S.diag_interface) { n_max = std::min(S.n_nonortho_corr, 8); stag = 0.99; }
+      else { n_max = std::min(S.n_nonortho_corr, 3); stag = 0.9; }
+      if (P.nonortho_check) {
+        n_max = std::min(S.n_nonortho_corr, 8);
+        launch_fill(F.phi_it, nc, 0.0);
+      }
+      double dprev = 1e308, dphi_prev = 1e308;
+      for (int jno = 1; jno <= n_max; ++jno) {
+        face_fluxes_and_rhs(gk_dt, jno > 1);
+        double dcur = 0.0;
+        if (n_max > 1 && !P.nonortho_check) {
+          RedArgs r{};
+          r.mode = RED_MAXABS; r.n = nc; r.a = F.rhs;
+          rc = reduce(r, &dcur, 1);
+          if (rc) return rc;
+        }
+        if (jno == 1) launch_fill(F.p, nc, 0.0);
+        int its;
+        double res;
+        rc = pressure_solve(P.p_tol, atol, false, &its, &res);
+        if (rc) return rc;
+        last.p_solves++;
+        last.p_iters += its;
+        last.p_resid_max = std::max(last.p_resid_max, res);
+        pressure_bc(F.p, 0, !S.skip_grad_p, 1);
+        pressure_bc(F.p, 1, 0, 0);
+        if (P.nonortho_check) {
+          // |p - phi_it|_max and |p|_max, then phi_it = p
+          RedArgs r{};
+          copy(scratch_c, F.p, nc);
+          k_shift_vec(F.phi_it);
+          r.mode = RED_MAXABS; r.n = nc; r.a = scratch_c;
+          double dd;
+          rc = reduce(r, &dd, 1);
+          if (rc) return rc;
+          r.a = F.p;
+          double dpp;
+          rc = reduce(r, &dpp, 1);
+          if (rc) return rc;
+          copy(F.phi_it, F.p, nc);
+          if (jno > 1 && (dd < 1.0e-3 * dpp || dd > dphi_prev * stag)) break;
+          dphi_prev = dd;
+        } else if (jno > 1 && (dcur < atol || dcur > dprev * stag)) {
+          break;
+        }
+        dprev = dcur;
+      }
+      correct_face_fluxes(gk_dt, false);
+      copy(F.ff, F.Uf, nf);
+      u_face_ready = true;
+      correct_velocity(gk_dt, true, false);
+      velocity_bc_refresh();
+      if (P.use_rotational_projection) {
+        k_rotational<<<nblk(nc), TPB, 0, st>>>(nc, F.p, F.nu_sgs, F.rhs, d.ivol, P.nu, gk_dt);
+        launches++;
+        pressure_bc(F.p, 0, !S.skip_grad_p, 1);
+        pressure_bc(F.p, 1, 0, 0);
+      }
+      k_add<<<nblk(nc), TPB, 0, st>>>(nc, F.p, F.p_old);
+      launches++;
+      anchor_pressure();
+      pressure_bc(F.p, 0, !S.skip_grad_p, 0);
+      pressure_bc(F.p, 1, 0, 0);
+      pressure_gradient();
+      std::swap(F.H, F.H0);
+    }
+    time = time_n + dt;
+    step++;
+    cudaEventRecord(ev1, st);
+    CK(cudaEventSynchronize(ev1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ev0, ev1);
+    last_step_ms = ms;
+    last_poisson_ms = poisson_ms_acc;
+    CK(cudaGetLastError());
+    return 0;
+  }
+
+  // scratch_c = scratch_c - v (used for the increment norm of nonortho_check)
+  void k_shift_vec(const double* v) {
+    k_sub<<<nblk(nc), TPB, 0, st>>>(nc, scratch_c, v);
+    launches++;
+  }
+
+  // ---------------------------------------------------------------- statistics
+  int stats(dpm_stats_t* s) {
+    RedArgs r{};
+    r.mode = RED_STATS; r.n = nc; r.a = F.U; r.vol = d.vol; r.gU = F.gU; r.nus = F.nu_sgs; r.nu = P.nu;
+    double o[RED_NV];
+    int rc = reduce(r, o, RED_NV);
+    if (rc) return rc;
+    s->time = time;
+    s->E = o[0] / o[1];
+    s->eps = 2.0 * o[2] / o[1];
+    double mb0 = o[3] / o[1], mb1 = o[4] / o[1], mb2 = o[5] / o[1];
+    s->Ub = std::sqrt(mb0 * mb0 + mb1 * mb1 + mb2 * mb2);
+    s->nu_sgs_mean = o[6] / o[1];
+    s->Umax = o[7];
+    // wall shear (host: small)
+    s->tauw_mean = 0.0;
+    if (nb) {
+      std::vector<double> tau(3 * (size_t)nb);
+      CK(cudaMemcpyAsync(tau.data(), F.tau, tau.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+      double num = 0.0, den = 0.0;
+      for (int q = 0; q < m.n_patches; ++q) {
+        if (pc[q].bc_id != BC_WALL_MODEL) continue;
+        for (int64_t k = 0; k < m.patch_nfaces[q]; ++k) {
+          int64_t b = m.patch_start[q] + k;
+          double t0 = tau[b], t1 = tau[nb + b], t2 = tau[2 * (size_t)nb + b];
+          num += std::sqrt(t0 * t0 + t1 * t1 + t2 * t2) * m.area[m.n_int_faces + b];
+          den += m.area[m.n_int_faces + b];
+        }
+      }
+      s->tauw_mean = den > SMALL ? num / den : 0.0;
+    }
+    k_flux_divergence<<<nblk(nc), TPB, 0, st>>>(d, F.Uf, scratch_c);
+    launches++;
+    RedArgs r2{};
+    r2.mode = RED_DIVSTAT; r2.n = nc; r2.a = scratch_c; r2.vol = d.vol;
+    double o2[3];
+    rc = reduce(r2, o2, 3);
+    if (rc) return rc;
+    s->max_abs_divU = o2[0];
+    s->volavg_abs_divU = o2[1] / o2[2];
+    s->dt_used = last.dt_used;
+    s->p_solves = last.p_solves;
+    s->p_iters = last.p_iters;
+    s->p_resid_max = last.p_resid_max;
+    velocity_bc(-1, 0);  // solver_divergence_metrics refreshes U_bnd without gradients
+    CK(cudaStreamSynchronize(st));
+    return 0;
+  }
+};
+
+}  // namespace gpu
+}  // namespace dpm
+
+using dpm::gpu::Solver;
+struct dpm_solver {
+  std::unique_ptr<Solver> s;
+};
+
+// ------------------------------------------------------------------------------------------
+extern "C" {
+
+int dpm_create(const dpm_raw_mesh_t* mesh, const dpm_patch_cfg_t* patches, const dpm_params_t* params, int device,
+               dpm_solver_t** out) {
+  if (!mesh || !patches || !params || !out) return DPM_ERR_ARG;
+  auto* h = new dpm_solver();
+  h->s = std::make_unique<Solver>();
+  int rc = h->s->init(mesh, patches, params, device);
+  if (rc) {
+    delete h;
+    *out = nullptr;
+    return rc;
+  }
+  *out = h;
+  return DPM_OK;
+}
+
+int dpm_destroy(dpm_solver_t* s) {
+  if (!s) return DPM_ERR_ARG;
+  cudaSetDevice(s->s->device);
+  delete s;
+  return DPM_OK;
+}
+
+int dpm_n_cells(const dpm_solver_t* s, int64_t* n_cells, int64_t* n_faces, int64_t* n_bnd_faces) {
+  if (!s) return DPM_ERR_ARG;
+  if (n_cells) *n_cells = s->s->nc;
+  if (n_faces) *n_faces = s->s->nf;
+  if (n_bnd_faces) *n_bnd_faces = s->s->nb;
+  return DPM_OK;
+}
+
+int dpm_cell_geometry(const dpm_solver_t* s, double* centroid, double* volume) {
+  if (!s) return DPM_ERR_ARG;
+  const auto& m = s->s->m;
+  if (centroid) std::memcpy(centroid, m.centroid.data(), sizeof(double) * 3 * m.n_cells);
+  if (volume) std::memcpy(volume, m.volume.data(), sizeof(double) * m.n_cells);
+  return DPM_OK;
+}
+
+int dpm_upload_state(dpm_solver_t* h, const double* U, const double* p, const double* T) {
+  if (!h) return DPM_ERR_ARG;
+  Solver& s = *h->s;
+  CK(cudaSetDevice(s.device));
+  if (U) {
+    CK(cudaMemcpyAsync(s.aos_buf, U, 3 * sizeof(double) * s.nc, cudaMemcpyHostToDevice, s.st));
+    dpm::gpu::k_aos_to_soa<<<dpm::gpu::nblk(s.nc), dpm::gpu::TPB, 0, s.st>>>(s.nc, s.aos_buf, s.F.U);
+    s.launches++;
+  }
+  if (p) CK(cudaMemcpyAsync(s.F.p, p, sizeof(double) * s.nc, cudaMemcpyHostToDevice, s.st));
+  if (T) CK(cudaMemcpyAsync(s.F.T, T, sizeof(double) * s.nc, cudaMemcpyHostToDevice, s.st));
+  CK(cudaStreamSynchronize(s.st));
+  return DPM_OK;
+}
+
+int dpm_download_state(dpm_solver_t* h, double* U, double* p, double* T, double* nu_sgs) {
+  if (!h) return DPM_ERR_ARG;
+  Solver& s = *h->s;
+  CK(cudaSetDevice(s.device));
+  if (U) {
+    dpm::gpu::k_soa_to_aos<<<dpm::gpu::nblk(s.nc), dpm::gpu::TPB, 0, s.st>>>(s.nc, s.F.U, s.aos_buf);
+    s.launches++;
+    CK(cudaMemcpyAsync(U, s.aos_buf, 3 * sizeof(double) * s.nc, cudaMemcpyDeviceToHost, s.st));
+  }
+  if (p) CK(cudaMemcpyAsync(p, s.F.p, sizeof(double) * s.nc, cudaMemcpyDeviceToHost, s.st));
+  if (T) CK(cudaMemcpyAsync(T, s.F.T, sizeof(double) * s.nc, cudaMemcpyDeviceToHost, s.st));
+  if (nu_sgs) CK(cudaMemcpyAsync(nu_sgs, s.F.nu_sgs, sizeof(double) * s.nc, cudaMemcpyDeviceToHost, s.st));
+  CK(cudaStreamSynchronize(s.st));
+  return DPM_OK;
+}
+
+int dpm_download_face_flux(dpm_solver_t* h, double* face_flux) {
+  if (!h || !face_flux) return DPM_ERR_ARG;
+  Solver& s = *h->s;
+  CK(cudaMemcpyAsync(face_flux, s.F.Uf, sizeof(double) * s.nf, cudaMemcpyDeviceToHost, s.st));
+  CK(cudaStreamSynchronize(s.st));
+  return DPM_OK;
+}
+
+int dpm_download_gradient(dpm_solver_t* h, double* grad_U) {
+  if (!h || !grad_U) return DPM_ERR_ARG;
+  Solver& s = *h->s;
+  dpm::gpu::k_grad_soa_to_aos<<<dpm::gpu::nblk(s.nc), dpm::gpu::TPB, 0, s.st>>>(s.nc, s.F.gU, s.aos_buf);
+  s.launches++;
+  CK(cudaMemcpyAsync(grad_U, s.aos_buf, 9 * sizeof(double) * s.nc, cudaMemcpyDeviceToHost, s.st));
+  CK(cudaStreamSynchronize(s.st));
+  return DPM_OK;
+}
+
+int dpm_project_once(dpm_solver_t* h, double dt) {
+  if (!h) return DPM_ERR_ARG;
+  CK(cudaSetDevice(h->s->device));
+  return h->s->project_once(dt);
+}
+
+int dpm_advance(dpm_solver_t* h, double dt) {
+  if (!h) return DPM_ERR_ARG;
+  CK(cudaSetDevice(h->s->device));
+  return h->s->advance(dt);
+}
+
+int dpm_advance_n(dpm_solver_t* h, double dt, int n_steps) {
+  if (!h || n_steps < 0) return DPM_ERR_ARG;
+  CK(cudaSetDevice(h->s->device));
+  for (int i = 0; i < n_steps; ++i) {
+    int rc = h->s->advance(dt);
+    if (rc) return rc;
+  }
+  return DPM_OK;
+}
+
+int dpm_stats(dpm_solver_t* h, dpm_stats_t* out) {
+  if (!h || !out) return DPM_ERR_ARG;
+  CK(cudaSetDevice(h->s->device));
+  return h->s->stats(out);
+}
+
+int dpm_state_is_finite(dpm_solver_t* h, int* ok) {
+  if (!h || !ok) return DPM_ERR_ARG;
+  Solver& s = *h->s;
+  dpm::gpu::RedArgs r{};
+  r.mode = dpm::gpu::RED_SUM2;
+  r.n = 3 * s.nc;
+  r.a = s.F.U;
+  r.b = s.F.U;
+  double o[2];
+  int rc = s.reduce(r, o, 2);
+  if (rc) return rc;
+  r.n = s.nc; r.a = s.F.p; r.b = s.F.p;
+  double o2[2];
+  rc = s.reduce(r, o2, 2);
+  if (rc) return rc;
+  double t = o[1] + o2[1];
+  *ok = std::fabs(t) <= 1.7976931348623157e308 ? 1 : 0;
+  return DPM_OK;
+}
+
+int dpm_compute_dt(dpm_solver_t* h, double* dt) {
+  if (!h || !dt) return DPM_ERR_ARG;
+  return h->s->compute_dt(*dt);
+}
+
+int dpm_get_time(const dpm_solver_t* h, double* time) {
+  if (!h || !time) return DPM_ERR_ARG;
+  *time = h->s->time;
+  return DPM_OK;
+}
+
+int dpm_set_time(dpm_solver_t* h, double time) {
+  if (!h) return DPM_ERR_ARG;
+  h->s->time = time;
+  return DPM_OK;
+}
+
+int dpm_last_timing(const dpm_solver_t* h, double* step_ms, double* poisson_ms) {
+  if (!h) return DPM_ERR_ARG;
+  if (step_ms) *step_ms = h->s->last_step_ms;
+  if (poisson_ms) *poisson_ms = h->s->last_poisson_ms;
+  return DPM_OK;
+}
+
+int dpm_kernel_launches(const dpm_solver_t* h, int64_t* n) {
+  if (!h || !n) return DPM_ERR_ARG;
+  *n = h->s->launches;
+  return DPM_OK;
+}
+
+// ---- per-operator entry points --------------------------------------------------------------
+static int upload_vec3(Solver& s, const double* host_aos, double* dev_soa, int n) {
+  CK(cudaMemcpyAsync(s.aos_buf, host_aos, 3 * sizeof(double) * n, cudaMemcpyHostToDevice, s.st));
+  dpm::gpu::k_aos_to_soa<<<dpm::gpu::nblk(n), dpm::gpu::TPB, 0, s.st>>>(n, s.aos_buf, dev_soa);
+  s.launches++;
+  CK(cudaStreamSynchronize(s.st));
+  return 0;
+}
+static int download_vec3(Solver& s, const double* dev_soa, double* host_aos, int n) {
+  dpm::gpu::k_soa_to_aos<<<dpm::gpu::nblk(n), dpm::gpu::TPB, 0, s.st>>>(n, dev_soa, s.aos_buf);
+  s.launches++;
+  CK(cudaMemcpyAsync(host_aos, s.aos_buf, 3 * sizeof(double) * n, cudaMemcpyDeviceToHost, s.st));
+  CK(cudaStreamSynchronize(s.st));
+  return 0;
+}
+static int upload_grad(Solver& s, const double* host_aos) {
+  CK(cudaMemcpyAsync(s.aos_buf, host_aos, 9 * sizeof(double) * s.nc, cudaMemcpyHostToDevice, s.st));
+  dpm::gpu::k_grad_aos_to_soa<<<dpm::gpu::nblk(s.nc), dpm::gpu::TPB, 0, s.st>>>(s.nc, s.aos_buf, s.F.gU);
+  s.launches++;
+  CK(cudaStreamSynchronize(s.st));
+  return 0;
+}
+
+int dpm_ls_gradient_vector(dpm_solver_t* h, const double* U, const double* U_bnd, double* grad_U) {
+  if (!h || !U || !U_bnd || !grad_U) return DPM_ERR_ARG;
+  Solver& s = *h->s;
+  int rc = upload_vec3(s, U, s.F.U, s.nc);
+  if (!rc && s.nb) rc = upload_vec3(s, U_bnd, s.F.Ub, s.nb);
+  if (rc) return rc;
+  s.grad_U();
+  return dpm_download_gradient(h, grad_U);
+}
+
+int dpm_advection_rhs_vector(dpm_solver_t* h, int scheme, const double* U, const double* U_bnd,
+                             const double* face_flux, const double* grad_U, double* rhs) {
+  if (!h || !U || !U_bnd || !face_flux || !grad_U || !rhs) return DPM_ERR_ARG;
+  Solver& s = *h->s;
+  int rc = upload_vec3(s, U, s.F.U, s.nc);
+  if (!rc && s.nb) rc = upload_vec3(s, U_bnd, s.F.Ub, s.nb);
+  if (!rc) rc = upload_grad(s, grad_U);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(s.F.Uf, face_flux, sizeof(double) * s.nf, cudaMemcpyHostToDevice, s.st));
+  int keep = s.P.scheme;
+  double keep_nu = s.P.nu;
+  s.P.scheme = scheme;
+  // advection only: zero viscosity, zero SGS, zero body force -> H = conv
+  s.launch_fill(s.F.nu_sgs, s.nc, 0.0);
+  s.P.nu = 0.0;
+  dpm::gpu::k_face_explicit<<<dpm::gpu::nblk(s.nf), dpm::gpu::TPB, 0, s.st>>>(
+      s.d, scheme, 0.0, s.F.U, s.F.Ub, s.F.gU, s.F.nu_sgs, s.F.Uf, s.F.fadv, s.F.fvis, s.F.fdiv);
+  dpm::gpu::ExplicitArgs a{};
+  a.scheme = scheme;
+  dpm::gpu::k_cell_explicit<<<dpm::gpu::nblk(s.nc), dpm::gpu::TPB, 0, s.st>>>(
+      s.d, a, s.F.U, s.F.T, s.F.fadv, s.F.fvis, s.F.fdiv, s.F.tau, s.F.H, s.F.H0, s.conv_tmp, s.visc_tmp);
+  s.launches += 2;
+  s.P.scheme = keep;
+  s.P.nu = keep_nu;
+  return download_vec3(s, s.conv_tmp, rhs, s.nc);
+}
+
+int dpm_viscous_rhs_vector(dpm_solver_t* h, const double* U, double nu, const double* nu_sgs, const double* grad_U,
+                           const double* U_bnd, double* rhs) {
+  if (!h || !U || !nu_sgs || !grad_U || !U_bnd || !rhs) return DPM_ERR_ARG;
+  Solver& s = *h->s;
+  int rc = upload_vec3(s, U, s.F.U, s.nc);
+  if (!rc && s.nb) rc = upload_vec3(s, U_bnd, s.F.Ub, s.nb);
+  if (!rc) rc = upload_grad(s, grad_U);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(s.F.nu_sgs, nu_sgs, sizeof(double) * s.nc, cudaMemcpyHostToDevice, s.st));
+  s.launch_fill(s.F.Uf, s.nf, 0.0);
+  dpm::gpu::k_face_explicit<<<dpm::gpu::nblk(s.nf), dpm::gpu::TPB, 0, s.st>>>(
+      s.d, DPM_SCHEME_CDS, nu, s.F.U, s.F.Ub, s.F.gU, s.F.nu_sgs, s.F.Uf, s.F.fadv, s.F.fvis, s.F.fdiv);
+  dpm::gpu::ExplicitArgs a{};
+  a.scheme = DPM_SCHEME_CDS;
+  dpm::gpu::k_cell_explicit<<<dpm::gpu::nblk(s.nc), dpm::gpu::TPB, 0, s.st>>>(
+      s.d, a, s.F.U, s.F.T, s.F.fadv, s.F.fvis, s.F.fdiv, s.F.tau, s.F.H, s.F.H0, s.conv_tmp, s.visc_tmp);
+  s.launches += 2;
+  return download_vec3(s, s.visc_tmp, rhs, s.nc);
+}
+
+int dpm_sgs_viscosity(dpm_solver_t* h, int model, const double* U, const double* U_bnd, const double* grad_U,
+                      double dt_stab, double* nu_sgs) {
+  if (!h || !U || !grad_U || !nu_sgs) return DPM_ERR_ARG;
+  (void)U_bnd;
+  Solver& s = *h->s;
+  int rc = upload_vec3(s, U, s.F.U, s.nc);
+  if (!rc) rc = upload_grad(s, grad_U);
+  if (rc) return rc;
+  int keep = s.P.sgs_model;
+  s.P.sgs_model = model;
+  s.sgs(dt_stab);
+  s.P.sgs_model = keep;
+  CK(cudaMemcpyAsync(nu_sgs, s.F.nu_sgs, sizeof(double) * s.nc, cudaMemcpyDeviceToHost, s.st));
+  CK(cudaStreamSynchronize(s.st));
+  return DPM_OK;
+}
+
+int dpm_wall_model(dpm_solver_t* h, const double* U, double nu, double* tau_w) {
+  if (!h || !U || !tau_w) return DPM_ERR_ARG;
+  Solver& s = *h->s;
+  int rc = upload_vec3(s, U, s.F.U, s.nc);
+  if (rc) return rc;
+  double keep = s.P.nu;
+  s.P.nu = nu;
+  s.wall_model(0.0);
+  s.P.nu = keep;
+  if (s.nb) return download_vec3(s, s.F.tau, tau_w, s.nb);
+  return DPM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,217 @@
+"""ctypes binding of libdopamine_b200.so (C ABI in include/dopamine_b200.h).
+
+`Solver` mirrors the reference's FVSolver (src/solver/mod_fv_solver.f90:270-285): init,
+project_once, advance, compute_dt, stats, to_device / sync_host.  There is no CPU fallback: if the
+library or a CUDA device is missing, construction raises.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libdopamine_b200.so")
+_lib = None
+
+EXPORTED = (
+    "fvm_petsc_backend_available", "fvm_petsc_backend_initialize", "fvm_petsc_backend_finalize",
+    "fvm_petsc_set_pressure_solver", "fvm_petsc_device_io_supported", "fvm_petsc_set_io_on_device",
+    "fvm_petsc_insert_option", "fvm_petsc_set_device_local_rank", "fvm_petsc_solve_pressure",
+    "dpm_create", "dpm_destroy", "dpm_n_cells", "dpm_upload_state", "dpm_download_state",
+    "dpm_download_face_flux", "dpm_download_gradient", "dpm_cell_geometry", "dpm_project_once", "dpm_advance",
+    "dpm_advance_n", "dpm_stats", "dpm_state_is_finite", "dpm_compute_dt", "dpm_get_time", "dpm_set_time",
+    "dpm_last_timing", "dpm_kernel_launches", "dpm_ls_gradient_vector", "dpm_advection_rhs_vector",
+    "dpm_viscous_rhs_vector", "dpm_sgs_viscosity", "dpm_wall_model",
+)
+
+
+class DopamineError(RuntimeError):
+    pass
+
+
+def lib(build_if_missing=True):
+    """Load the product library; builds it from source when it is missing and nvcc is present."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        if not build_if_missing:
+            raise DopamineError(f"{LIB_PATH} not built")
+        from . import build as _build
+        _build.build()
+    L = C.CDLL(LIB_PATH)
+    vp, dp, ip, lp = C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int), C.POINTER(C.c_int64)
+    L.dpm_create.argtypes = [C.POINTER(abi.RawMeshT), C.POINTER(abi.PatchCfgT), C.POINTER(abi.ParamsT), C.c_int,
+                             C.POINTER(vp)]
+    L.dpm_destroy.argtypes = [vp]
+    L.dpm_n_cells.argtypes = [vp, lp, lp, lp]
+    L.dpm_cell_geometry.argtypes = [vp, dp, dp]
+    L.dpm_upload_state.argtypes = [vp, dp, dp, dp]
+    L.dpm_download_state.argtypes = [vp, dp, dp, dp, dp]
+    L.dpm_download_face_flux.argtypes = [vp, dp]
+    L.dpm_download_gradient.argtypes = [vp, dp]
+    L.dpm_project_once.argtypes = [vp, C.c_double]
+    L.dpm_advance.argtypes = [vp, C.c_double]
+    L.dpm_advance_n.argtypes = [vp, C.c_double, C.c_int]
+    L.dpm_stats.argtypes = [vp, C.POINTER(abi.StatsT)]
+    L.dpm_state_is_finite.argtypes = [vp, ip]
+    L.dpm_compute_dt.argtypes = [vp, dp]
+    L.dpm_get_time.argtypes = [vp, dp]
+    L.dpm_set_time.argtypes = [vp, C.c_double]
+    L.dpm_last_timing.argtypes = [vp, dp, dp]
+    L.dpm_kernel_launches.argtypes = [vp, lp]
+    L.dpm_ls_gradient_vector.argtypes = [vp, dp, dp, dp]
+    L.dpm_advection_rhs_vector.argtypes = [vp, C.c_int, dp, dp, dp, dp, dp]
+    L.dpm_viscous_rhs_vector.argtypes = [vp, dp, C.c_double, dp, dp, dp, dp]
+    L.dpm_sgs_viscosity.argtypes = [vp, C.c_int, dp, dp, dp, C.c_double, dp]
+    L.dpm_wall_model.argtypes = [vp, dp, C.c_double, dp]
+    L.fvm_petsc_solve_pressure.argtypes = [C.c_int, C.c_int, C.c_int, ip, ip, ip, ip, ip, dp, dp, dp, C.c_int,
+                                           C.c_int, C.c_double, C.c_double, ip, dp, C.c_int, dp, ip, dp]
+    L.fvm_petsc_set_pressure_solver.argtypes = [C.c_char_p]
+    L.fvm_petsc_insert_option.argtypes = [C.c_char_p]
+    L.fvm_petsc_set_io_on_device.argtypes = [C.c_int]
+    L.fvm_petsc_set_device_local_rank.argtypes = [C.c_int]
+    _lib = L
+    return L
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _check(rc, what):
+    if rc != 0:
+        raise DopamineError(f"{what} failed with status {rc}")
+
+
+class Solver:
+    """Device-resident RK3W solver on one GPU for a dopamine_b200.cases.Case."""
+
+    def __init__(self, case, device=0, params=None):
+        L = lib()
+        self.case = case
+        self._mesh = abi.RawMeshView(case.mesh)
+        self._patches = abi.patch_cfgs(case.patches)
+        self.params = params if params is not None else case.make_params()
+        h = C.c_void_p()
+        _check(L.dpm_create(C.byref(self._mesh.struct), self._patches, C.byref(self.params), device, C.byref(h)),
+               "dpm_create")
+        self.h = h
+        nc, nf, nb = C.c_int64(), C.c_int64(), C.c_int64()
+        L.dpm_n_cells(self.h, C.byref(nc), C.byref(nf), C.byref(nb))
+        self.nc, self.nf, self.nb = nc.value, nf.value, nb.value
+        self.centroid = np.zeros((self.nc, 3))
+        self.volume = np.zeros(self.nc)
+        L.dpm_cell_geometry(self.h, _p(self.centroid), _p(self.volume))
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().dpm_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def to_device(self, U=None, p=None, T=None):
+        U = None if U is None else np.ascontiguousarray(U, dtype=np.float64)
+        p = None if p is None else np.ascontiguousarray(p, dtype=np.float64)
+        T = None if T is None else np.ascontiguousarray(T, dtype=np.float64)
+        _check(lib().dpm_upload_state(self.h, _p(U), _p(p), _p(T)), "dpm_upload_state")
+
+    def sync_host(self):
+        U = np.zeros((self.nc, 3)); p = np.zeros(self.nc); T = np.zeros(self.nc); nu = np.zeros(self.nc)
+        _check(lib().dpm_download_state(self.h, _p(U), _p(p), _p(T), _p(nu)), "dpm_download_state")
+        return {"U": U, "p": p, "T": T, "nu_sgs": nu}
+
+    def face_flux(self):
+        ff = np.zeros(self.nf)
+        _check(lib().dpm_download_face_flux(self.h, _p(ff)), "dpm_download_face_flux")
+        return ff
+
+    def grad_U(self):
+        g = np.zeros((self.nc, 3, 3))
+        _check(lib().dpm_download_gradient(self.h, _p(g)), "dpm_download_gradient")
+        return g
+
+    def project_once(self, dt):
+        _check(lib().dpm_project_once(self.h, dt), "dpm_project_once")
+
+    def initialise(self):
+        """apply_initial_conditions (src/init/mod_initconditions.f90:38-112): profile, optional noise
+        with an extra projection, then project_once at dt_proj = gamma_1 dt."""
+        U = self.case.initial_velocity(self.centroid)
+        self.to_device(U=U, p=np.zeros(self.nc))
+        dtp = 8.0 / 15.0 * self.params.dt
+        if self.case.noise > 0.0:
+            self.project_once(dtp)
+        self.project_once(dtp)
+
+    def advance(self, dt=None):
+        _check(lib().dpm_advance(self.h, self.params.dt if dt is None else dt), "dpm_advance")
+
+    def advance_n(self, n, dt=None):
+        _check(lib().dpm_advance_n(self.h, self.params.dt if dt is None else dt, n), "dpm_advance_n")
+
+    def compute_dt(self):
+        v = C.c_double()
+        _check(lib().dpm_compute_dt(self.h, C.byref(v)), "dpm_compute_dt")
+        return v.value
+
+    def state_is_finite(self):
+        ok = C.c_int()
+        _check(lib().dpm_state_is_finite(self.h, C.byref(ok)), "dpm_state_is_finite")
+        return bool(ok.value)
+
+    def stats(self):
+        s = abi.StatsT()
+        _check(lib().dpm_stats(self.h, C.byref(s)), "dpm_stats")
+        return s.as_dict()
+
+    def last_timing(self):
+        a, b = C.c_double(), C.c_double()
+        lib().dpm_last_timing(self.h, C.byref(a), C.byref(b))
+        return a.value, b.value
+
+    def kernel_launches(self):
+        n = C.c_int64()
+        lib().dpm_kernel_launches(self.h, C.byref(n))
+        return n.value
+
+    @property
+    def time(self):
+        v = C.c_double()
+        lib().dpm_get_time(self.h, C.byref(v))
+        return v.value
+
+    # ---- per-operator entry points ----------------------------------------------------------
+    def ls_gradient_vector(self, U, U_bnd):
+        g = np.zeros((self.nc, 3, 3))
+        _check(lib().dpm_ls_gradient_vector(self.h, _p(np.ascontiguousarray(U)), _p(np.ascontiguousarray(U_bnd)),
+                                            _p(g)), "dpm_ls_gradient_vector")
+        return g
+
+    def advection_rhs_vector(self, scheme, U, U_bnd, face_flux, grad_U):
+        r = np.zeros((self.nc, 3))
+        _check(lib().dpm_advection_rhs_vector(self.h, scheme, _p(np.ascontiguousarray(U)),
+                                              _p(np.ascontiguousarray(U_bnd)), _p(np.ascontiguousarray(face_flux)),
+                                              _p(np.ascontiguousarray(grad_U)), _p(r)), "dpm_advection_rhs_vector")
+        return r
+
+    def viscous_rhs_vector(self, U, nu, nu_sgs, grad_U, U_bnd):
+        r = np.zeros((self.nc, 3))
+        _check(lib().dpm_viscous_rhs_vector(self.h, _p(np.ascontiguousarray(U)), nu, _p(np.ascontiguousarray(nu_sgs)),
+                                            _p(np.ascontiguousarray(grad_U)), _p(np.ascontiguousarray(U_bnd)), _p(r)),
+               "dpm_viscous_rhs_vector")
+        return r
+
+    def sgs_viscosity(self, model, U, grad_U, dt_stab):
+        nu = np.zeros(self.nc)
+        _check(lib().dpm_sgs_viscosity(self.h, model, _p(np.ascontiguousarray(U)), None,
+                                       _p(np.ascontiguousarray(grad_U)), dt_stab, _p(nu)), "dpm_sgs_viscosity")
+        return nu
+
+    def wall_model(self, U, nu):
+        tau = np.zeros((self.nb, 3))
+        _check(lib().dpm_wall_model(self.h, _p(np.ascontiguousarray(U)), nu, _p(tau)), "dpm_wall_model")
+        return tau

@@ -179,8 +179,12 @@ int dpm_n_cells(const dpm_solver_t* s, int64_t* n_cells, int64_t* n_faces, int64
 int dpm_upload_state(dpm_solver_t* s, const double* U, const double* p, const double* T);
 /* solver_sync_host (mod_fv_solver.f90:3326): any output pointer may be NULL. */
 int dpm_download_state(dpm_solver_t* s, double* U, double* p, double* T, double* nu_sgs);
-/* Fields that only the projection produces: face flux (n_faces) and the cell pressure gradient. */
+/* Divergence-free face flux of the last projection (n_faces, mesh face order). */
 int dpm_download_face_flux(dpm_solver_t* s, double* face_flux);
+/* Velocity gradient of the last gradient pass, grad_U(3,3,nc). */
+int dpm_download_gradient(dpm_solver_t* s, double* grad_U);
+/* Cell centroids (3,nc) and volumes (nc) computed by the mesh set-up. */
+int dpm_cell_geometry(const dpm_solver_t* s, double* centroid, double* volume);
 /* solver_project_once (mod_fv_solver.f90:837-918). */
 int dpm_project_once(dpm_solver_t* s, double dt);
 /* solver_advance (mod_fv_solver.f90:920-958): CFL clamp of a fixed dt, RK3W, time += dt.
@@ -195,7 +199,7 @@ int dpm_state_is_finite(dpm_solver_t* s, int* ok);
 int dpm_compute_dt(dpm_solver_t* s, double* dt);
 int dpm_get_time(const dpm_solver_t* s, double* time);
 int dpm_set_time(dpm_solver_t* s, double time);
-/* Device time of the last dpm_advance*/ /* in ms: total and Poisson part. */
+/* Device time (CUDA events) of the last dpm_advance, in ms: whole step and Poisson solves. */
 int dpm_last_timing(const dpm_solver_t* s, double* step_ms, double* poisson_ms);
 /* Kernel launch count since the handle was created (own kernels only). */
 int dpm_kernel_launches(const dpm_solver_t* s, int64_t* n);

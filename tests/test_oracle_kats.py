@@ -1,0 +1,74 @@
+"""Known-answer and identity checks of the oracle, ported from the reference's unit tests
+(tests/unit/test_amd.f90, test_nonortho_limiter.f90, test_mesh_geometry.f90) plus the log-law
+inversion of the wall model."""
+import ctypes as C
+import math
+
+import numpy as np
+import pytest
+
+from dopamine_b200 import abi, cases
+from oracle import oracle as O
+
+C3 = 1.0 / 3.0
+
+
+def amd(a, g, c):
+    a = np.asfortranarray(a, dtype=np.float64)
+    g = np.asfortranarray(g, dtype=np.float64)
+    return O.lib().orc_amd_point(a.ctypes.data_as(C.POINTER(C.c_double)), g.ctypes.data_as(C.POINTER(C.c_double)), c)
+
+
+def test_amd_known_answers():
+    # tests/unit/test_amd.f90: seven hand-evaluated cases at 1e-12
+    g = np.eye(3)
+    a = np.zeros((3, 3)); a[1, 0] = 3.0
+    assert abs(amd(a, g, C3)) <= 1e-12                      # pure shear
+    a = np.zeros((3, 3)); a[1, 0] = -2.0; a[0, 1] = 2.0
+    assert abs(amd(a, g, C3)) <= 1e-12                      # solid-body rotation
+    a = np.diag([1.0, 1.0, -2.0])
+    assert abs(amd(a, g, C3) - C3) <= 1e-12                 # isotropic filter, axisymmetric strain
+    g2 = np.diag([4.0, 1.0, 1.0])
+    assert abs(amd(a, g2, C3) - 0.5 * C3) <= 1e-12          # anisotropic filter
+    assert abs(amd(-a, g, C3)) <= 1e-12                     # backscatter clipped
+    assert abs(amd(np.zeros((3, 3)), g, C3)) <= 1e-12       # quiescent
+    a5 = np.diag([5.0, 5.0, -10.0])
+    assert abs(amd(a5, g, 2 * C3) - 2 * C3 * 5.0) <= 1e-12 * 10  # linear in constant and gradient
+
+
+def reichardt_uplus(yp):
+    kappa, a1, a2 = 0.41, 11.0, 0.33
+    cb = 5.2 - math.log(kappa) / kappa
+    return math.log(1 + kappa * yp) / kappa + cb * (1 - math.exp(-yp / a1) - yp / a1 * math.exp(-a2 * yp))
+
+
+@pytest.mark.parametrize("utau,yw,nu", [(0.05, 0.01, 1e-5), (1.0, 0.05, 1.0 / 395), (0.3, 1.0, 1.5e-5)])
+def test_wall_newton_inverts_reichardt(utau, yw, nu):
+    u_par = utau * reichardt_uplus(utau * yw / nu)
+    ut, tau = C.c_double(), C.c_double()
+    O.lib().orc_wall_stress_newton(u_par, yw, nu, C.byref(ut), C.byref(tau))
+    assert abs(ut.value - utau) <= 1e-6 * utau
+    assert abs(tau.value - ut.value ** 2) <= 1e-14
+
+
+def test_ls_gradient_exact_for_linear_field_and_closed_cells():
+    """Least-squares gradients reproduce a linear field exactly (interior cells) on a skewed mesh;
+    sum of outward face area vectors of every closed cell vanishes."""
+    case = cases.regression_case("hydrowall")
+    o = O.Oracle(case)
+    g0 = np.array([0.3, -1.2, 2.0])
+    c0 = o.centroid
+    U = np.zeros((o.nc, 3))
+    U[:, 0] = c0 @ g0
+    L = O.lib()
+    dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+    # boundary values from the same linear field at the face centres is not exposed; use a
+    # periodic-free interior check: cells whose stencil has no boundary entry
+    Ub = np.zeros((o.nb, 3))
+    g = np.zeros((o.nc, 3, 3))
+    L.orc_ls_gradient_vector(o.h, dp(U), dp(Ub), dp(g))
+    lo, hi = case.mesh.vertex_bounds()
+    inner = np.all((c0 > lo + 0.2) & (c0 < hi - 0.2), axis=1)
+    assert inner.sum() > 50
+    np.testing.assert_allclose(g[inner, 0, :], np.tile(g0, (inner.sum(), 1)), rtol=0, atol=1e-10)
+    assert abs(o.volume.sum() - 1.0) < 1e-12
