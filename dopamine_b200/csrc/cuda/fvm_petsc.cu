@@ -36,14 +36,15 @@ struct Ctx {
   int *col = nullptr, *status = nullptr;
   unsigned* bar = nullptr;
   double *val = nullptr, *dinv = nullptr, *b = nullptr, *x = nullptr, *r = nullptr, *z = nullptr, *p0 = nullptr,
-         *p1 = nullptr, *q = nullptr, *bp = nullptr, *part = nullptr, *dout = nullptr;
+         *p1 = nullptr, *q = nullptr, *bp = nullptr, *part = nullptr, *dout = nullptr, *tot = nullptr;
+  void* kernel = nullptr;
   void release() {
-    void* ps[] = {col, status, bar, val, dinv, b, x, r, z, p0, p1, q, bp, part, dout};
+    void* ps[] = {col, status, bar, val, dinv, b, x, r, z, p0, p1, q, bp, part, dout, tot};
     for (void* p : ps)
       if (p) cudaFree(p);
     col = status = nullptr;
     bar = nullptr;
-    val = dinv = b = x = r = z = p0 = p1 = q = bp = part = dout = nullptr;
+    val = dinv = b = x = r = z = p0 = p1 = q = bp = part = dout = tot = nullptr;
     ready = false;
   }
 };
@@ -92,7 +93,10 @@ int build(int n, int nfaces, const int* l2g, const int* fo, const int* fnl, cons
     }
     WA = std::max<int>(WA, (int)cols[i].size());
   }
-  std::vector<int> hc((size_t)WA * n, PADI);
+  if (WA > 16) return -12;
+  std::vector<int> hc((size_t)WA * n);
+  for (int w = 0; w < WA; ++w)
+    for (int i = 0; i < n; ++i) hc[(size_t)w * n + i] = i;  // padding (self, 0)
   std::vector<double> hv((size_t)WA * n, 0.0), hd(n, 1.0);
   for (int i = 0; i < n; ++i)
     for (size_t s = 0; s < cols[i].size(); ++s) {
@@ -111,10 +115,21 @@ int build(int n, int nfaces, const int* l2g, const int* fo, const int* fnl, cons
   cudaMemcpy(g_ctx.dinv, hd.data(), n * sizeof(double), cudaMemcpyHostToDevice);
   int sms = 0, per_sm = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g_ctx.device);
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg<double>, TPB, 0) != cudaSuccess || per_sm < 1)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg<double, 0, 0>, PCG_TPB, 0) != cudaSuccess || per_sm < 1)
     return -26;
-  g_ctx.grid = std::min(std::min(sms * per_sm, (n + TPB - 1) / TPB), 2048);
+  g_ctx.grid = std::min(sms * per_sm, (n + PCG_TPB - 1) / PCG_TPB);
   if (g_ctx.grid < 1) g_ctx.grid = 1;
+  int cpt = 0;
+  g_ctx.kernel = pcg_kernel_for<double>(n, g_ctx.grid, WA, &cpt);
+  int per_sm2 = 0;
+  cudaFuncSetAttribute(g_ctx.kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 5);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, g_ctx.kernel, PCG_TPB, 0) != cudaSuccess || per_sm2 < 1)
+    return -26;
+  if (sms * per_sm2 < g_ctx.grid) {
+    g_ctx.grid = sms * per_sm2;
+    g_ctx.kernel = pcg_kernel_for<double>(n, g_ctx.grid, WA, &cpt);
+    cudaFuncSetAttribute(g_ctx.kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 5);
+  }
   if (dalloc(&g_ctx.part, 8 * (size_t)g_ctx.grid)) return -11;
   g_ctx.n = n;
   g_ctx.nfaces = nfaces;
@@ -128,12 +143,13 @@ int run_pcg(double rtol, double atol, int maxit, int guess_zero, int* reason, in
   PcgArgs<double> a{};
   a.n = g_ctx.n; a.WA = g_ctx.WA; a.col = g_ctx.col; a.val = g_ctx.val; a.dinv = g_ctx.dinv;
   a.b = g_ctx.b; a.x = g_ctx.x; a.r = g_ctx.r; a.z = g_ctx.z; a.p0 = g_ctx.p0; a.p1 = g_ctx.p1; a.q = g_ctx.q;
-  a.bp = g_ctx.bp; a.partials = g_ctx.part; a.bar = g_ctx.bar; a.status = g_ctx.status; a.dout = g_ctx.dout;
+  a.bp = g_ctx.bp; a.partials = g_ctx.part; a.bar = g_ctx.bar; a.status = g_ctx.status;
+  a.dout = g_ctx.dout;
   a.rtol = rtol; a.atol = atol; a.maxit = maxit; a.nullsp = g_ctx.n_dir > 0 ? 0 : 1; a.guess_zero = guess_zero;
   cudaMemsetAsync(g_ctx.bar, 0, 2 * sizeof(unsigned), g_ctx.st);
   cudaMemsetAsync(g_ctx.status, 0, 4 * sizeof(int), g_ctx.st);
   void* args[] = {&a};
-  if (cudaLaunchCooperativeKernel((void*)k_pcg<double>, dim3(g_ctx.grid), dim3(TPB), args, 0, g_ctx.st) != cudaSuccess)
+  if (cudaLaunchCooperativeKernel(g_ctx.kernel, dim3(g_ctx.grid), dim3(PCG_TPB), args, 0, g_ctx.st) != cudaSuccess)
     return -33;
   int hs[4];
   double hd[4];

@@ -4,18 +4,19 @@
 // when ||r|| <= max(rtol ||b||, atol), nonzero initial guess, constant null space removed from the
 // right-hand side and from every preconditioned residual when no Dirichlet row exists
 // (src/solver/pressure_backend_petsc.c:381-463, 816-876).  This kernel runs the same recurrence
-// with the whole solve on the device: every iteration is two grid-wide phases separated by a
-// grid barrier, each phase reduces its dot products per block, and every block then sums the
-// per-block partials in the same fixed order, so all blocks take identical convergence decisions
-// and the result does not depend on scheduling.
+// with the whole solve on the device:
 //
-// Phase A: p = (z - mean z) + beta/beta_old p_old (built on the fly for neighbours, ping-pong
-//          buffers), q = A p, partial p.q
-// Phase B: x += a p, r -= a q, z = D^-1 r, partials r.r, z.r, sum z, sum r
+//   phase A: p = (z - mean z) + (beta/beta_old) p_old, built on the fly for neighbour cells
+//            (ping-pong p buffers), q = A p, partial p.q            -> grid all-reduce
+//   phase B: x += a p, r -= a q, z = D^-1 r, partials r.r, sum z, sum r, z.r  -> grid all-reduce
 //
-// The grid barrier is a counter plus generation word; waits are bounded (DPM_BARRIER_SPIN_LIMIT)
-// and a timeout sets an error status instead of hanging.  The launch is cooperative, which
-// guarantees that all blocks are co-resident.
+// Rows of A are stored ELL [width][n] with sorted columns and padded to a fixed width with
+// (self, 0) entries, so each row is a fully unrolled set of independent loads.  A and 1/diag are
+// read through the read-only path and stay L1-resident across iterations; the vectors that
+// neighbours read (z, p) go through L2 (ld.cg), which is where other SMs' writes are visible.
+// Each thread keeps its own cells' x, r, z and p in registers when the mesh fits (CPT cells per
+// thread).  Grid all-reduces are deterministic (see grid_allreduce).  The launch is cooperative,
+// which guarantees co-residency of all blocks; every wait is bounded.
 #pragma once
 #include "common.cuh"
 
@@ -25,6 +26,8 @@ namespace gpu {
 #ifndef DPM_BARRIER_SPIN_LIMIT
 #define DPM_BARRIER_SPIN_LIMIT (1u << 26)
 #endif
+
+constexpr int PCG_TPB = 1024;
 
 template <class V>
 struct PcgArgs {
@@ -36,7 +39,7 @@ struct PcgArgs {
   V* x;                // initial guess in, solution out
   V *r, *z, *p0, *p1, *q, *bp;
   double* partials;    // [2][nblocks][4]
-  unsigned* bar;       // [0] arrival counter, [1] generation
+  unsigned* bar;       // [0] monotonic arrival counter
   int* status;         // [0] reason, [1] iterations, [2] barrier timeout
   double* dout;        // [0] true residual ||b - A x||, [1] last ||r||, [2] ||b'||
   double rtol, atol;
@@ -46,38 +49,20 @@ struct PcgArgs {
 __device__ __forceinline__ double ld_cg(const double* p) { return __ldcg(p); }
 __device__ __forceinline__ float ld_cg(const float* p) { return __ldcg(p); }
 
-// Bounded grid barrier.  Returns false on timeout.
-__device__ __forceinline__ bool grid_sync(unsigned* bar, unsigned nblocks, unsigned& gen, int* status) {
-  __shared__ int s_ok;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    int ok = 1;
-    unsigned g = gen;
-    __threadfence();
-    unsigned arrived = atomicAdd(&bar[0], 1u);
-    if (arrived == nblocks - 1) {
-      atomicExch(&bar[0], 0u);
-      __threadfence();
-      atomicExch(&bar[1], g + 1u);
-    } else {
-      unsigned spins = 0;
-      while (atomicAdd(&bar[1], 0u) == g) {
-        if (++spins > DPM_BARRIER_SPIN_LIMIT) { ok = 0; atomicExch(&status[2], 1); break; }
-        __nanosleep(64);
-      }
-    }
-    __threadfence();
-    gen = g + 1u;
-    s_ok = ok && (atomicAdd(&status[2], 0) == 0);
-  }
-  __syncthreads();
-  return s_ok != 0;
-}
-
+// Grid-wide deterministic all-reduce + barrier.  Each block reduces its NV values (fixed shuffle
+// tree), thread 0 writes them into the partial buffer of this barrier (two buffers alternate) and
+// arrives on a monotonic counter; once all blocks have arrived, warp 0 of every block reads all
+// partials with a fixed lane-to-block mapping and reduces them with the same shuffle tree, so all
+// blocks hold bit-identical totals.  Two __syncthreads per call; the wait is bounded and returns
+// false on timeout.
 template <int NV>
-__device__ __forceinline__ void block_partial(double (&v)[NV], double* out) {
-  __shared__ double sh[32][NV];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+__device__ __forceinline__ bool grid_allreduce(double (&v)[NV], double* partials, unsigned* bar, unsigned& gen,
+                                               int* status, double (&res)[NV]) {
+  __shared__ double sh[32][4];
+  __shared__ double shr[4];
+  __shared__ int s_ok;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  double* buf = partials + (size_t)(gen & 1u) * 4 * gridDim.x;
 #pragma unroll
   for (int k = 0; k < NV; ++k)
     for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
@@ -86,220 +71,319 @@ __device__ __forceinline__ void block_partial(double (&v)[NV], double* out) {
     for (int k = 0; k < NV; ++k) sh[w][k] = v[k];
   __syncthreads();
   if (w == 0) {
+    double t[NV];
 #pragma unroll
     for (int k = 0; k < NV; ++k) {
-      double t = lane < nw ? sh[lane][k] : 0.0;
-      for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
-      if (lane == 0) out[k] = t;
+      t[k] = lane < nw ? sh[lane][k] : 0.0;
+      for (int o = 16; o > 0; o >>= 1) t[k] += __shfl_down_sync(0xffffffffu, t[k], o);
     }
-  }
-  __syncthreads();
-}
-
-// Every block sums the per-block partials in the same order.
-template <int NV>
-__device__ __forceinline__ void grid_total(const double* partials, int nblocks, double (&res)[NV]) {
-  __shared__ double tot[NV];
-  if (threadIdx.x < 32) {
-    const int lane = threadIdx.x;
-    double v[NV];
+    const unsigned target = (gen + 1u) * gridDim.x;
+    int ok = 1;
+    if (lane == 0) {
 #pragma unroll
-    for (int k = 0; k < NV; ++k) v[k] = 0.0;
-    for (int b = lane; b < nblocks; b += 32)
+      for (int k = 0; k < NV; ++k) buf[blockIdx.x * 4 + k] = t[k];
+      __threadfence();
+      atomicAdd(&bar[0], 1u);
+      unsigned spins = 0;
+      for (;;) {
+        unsigned cur;
+        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(cur) : "l"(&bar[0]) : "memory");
+        if ((int)(cur - target) >= 0) break;
+        if (++spins > DPM_BARRIER_SPIN_LIMIT) { ok = 0; atomicExch(&status[2], 1); break; }
+        if (spins > 32) __nanosleep(20);
+      }
+      __threadfence();
+    }
+    ok = __shfl_sync(0xffffffffu, ok, 0);
+    double u[NV];
 #pragma unroll
-      for (int k = 0; k < NV; ++k) v[k] += __ldcg(&partials[b * 4 + k]);
+    for (int k = 0; k < NV; ++k) u[k] = 0.0;
+    if (ok)
+      for (int b = lane; b < (int)gridDim.x; b += 32)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) u[k] += __ldcg(&buf[b * 4 + k]);
 #pragma unroll
     for (int k = 0; k < NV; ++k) {
-      for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
-      if (lane == 0) tot[k] = v[k];
+      for (int o = 16; o > 0; o >>= 1) u[k] += __shfl_down_sync(0xffffffffu, u[k], o);
+      if (lane == 0) shr[k] = u[k];
     }
+    if (lane == 0) s_ok = ok;
   }
   __syncthreads();
+  gen = gen + 1u;
 #pragma unroll
-  for (int k = 0; k < NV; ++k) res[k] = tot[k];
-  __syncthreads();
+  for (int k = 0; k < NV; ++k) res[k] = shr[k];
+  return s_ok != 0;
 }
 
-template <class V>
-__global__ void __launch_bounds__(TPB) k_pcg(PcgArgs<V> a) {
-  const int n = a.n, WA = a.WA;
-  const unsigned nblk = gridDim.x;
+__device__ __forceinline__ int classify(double dp, double ttol, double atol, double rnorm0) {
+  if (!(fabs(dp) <= 1.7976931348623157e308)) return -9;   // KSP_DIVERGED_NANORINF
+  if (dp <= ttol) return dp < atol ? 3 : 2;               // KSP_CONVERGED_ATOL / _RTOL
+  if (dp >= 1.0e5 * rnorm0) return -4;                    // KSP_DIVERGED_DTOL
+  return 0;
+}
+
+// Row i of A times the vector v (ELL, padded rows: no early exit, all loads independent).
+template <class V, int WT>
+__device__ __forceinline__ double spmv_row(const PcgArgs<V>& a, int i, const V* v) {
+  const int n = a.n;
+  constexpr int W = WT > 0 ? WT : 16;
+  const int WA = WT > 0 ? WT : a.WA;
+  int c[W];
+#pragma unroll
+  for (int w = 0; w < W; ++w)
+    if (w < WA) c[w] = __ldg(&a.col[w * n + i]);
+  double x[W];
+#pragma unroll
+  for (int w = 0; w < W; ++w)
+    if (w < WA) x[w] = (double)ld_cg(&v[c[w]]);
+  double s = 0.0;
+#pragma unroll
+  for (int w = 0; w < W; ++w)
+    if (w < WA) s += (double)__ldcg(&a.val[w * n + i]) * x[w];
+  return s;
+}
+
+// Row i of A times p = (z - mz) + bb p_old (first iteration: p = z - mz), p formed on the fly.
+template <class V, int WT>
+__device__ __forceinline__ double spmv_row_p(const PcgArgs<V>& a, int i, const V* pold, double mz, double bb,
+                                             bool first) {
+  const int n = a.n;
+  constexpr int W = WT > 0 ? WT : 16;
+  const int WA = WT > 0 ? WT : a.WA;
+  int c[W];
+#pragma unroll
+  for (int w = 0; w < W; ++w)
+    if (w < WA) c[w] = __ldg(&a.col[w * n + i]);
+  double zz[W], pp[W];
+#pragma unroll
+  for (int w = 0; w < W; ++w)
+    if (w < WA) {
+      zz[w] = (double)ld_cg(&a.z[c[w]]);
+      pp[w] = first ? 0.0 : (double)ld_cg(&pold[c[w]]);
+    }
+  double s = 0.0;
+#pragma unroll
+  for (int w = 0; w < W; ++w)
+    if (w < WA) {
+      double pj = zz[w] - mz;
+      if (!first) pj = pj + bb * pp[w];
+      s += (double)__ldcg(&a.val[w * n + i]) * (double)(V)pj;
+    }
+  return s;
+}
+
+// CPT > 0: exactly CPT cells per thread, own x, r, z, p held in registers
+//          (requires n <= grid * blockDim * CPT).
+// CPT == 0: grid-stride loops with the own-cell vectors in global memory (any n).
+// WT: fixed padded row width (7 on hexahedral meshes), 0 = runtime width <= 16.
+template <class V, int CPT, int WT>
+__global__ void __launch_bounds__(PCG_TPB, 1) k_pcg(PcgArgs<V> a) {
+  const int n = a.n;
   const int stride = gridDim.x * blockDim.x;
   const int i0 = blockIdx.x * blockDim.x + threadIdx.x;
   unsigned gen = 0;
-  if (i0 == 0) { /* generation word is reset by the host before launch */ }
-  double* part0 = a.partials;
-  double* part1 = a.partials + 4 * nblk;
-  int ph = 0;
-  auto part = [&]() { double* p = ph ? part1 : part0; ph ^= 1; return p; };
+  constexpr int NR = CPT > 0 ? CPT : 1;
+  double rx[NR], rr_[NR], rz[NR], rp[NR], rq[NR], rd[NR];
 
-  // ---- b' = b - mean(b) (null space), r = b' - A x, ||r||, ||b'||
+  // ---- b' = b - mean(b) when the constant null space is active
   double mb = 0.0;
   if (a.nullsp) {
-    double v[1] = {0.0};
+    double v[1] = {0.0}, t[1];
     for (int i = i0; i < n; i += stride) v[0] += (double)a.b[i];
-    double* P = part();
-    block_partial<1>(v, P + 4 * blockIdx.x);
-    if (!grid_sync(a.bar, nblk, gen, a.status)) return;
-    double t[1];
-    grid_total<1>(P, nblk, t);
+    if (!grid_allreduce<1>(v, a.partials, a.bar, gen, a.status, t)) return;
     mb = t[0] / (double)n;
   }
-  if (a.guess_zero)
+  if (a.guess_zero) {
     for (int i = i0; i < n; i += stride) a.x[i] = (V)0;
-  {
-    double v[2] = {0.0, 0.0};
-    for (int i = i0; i < n; i += stride) {
-      V bi = a.b[i];
-      V bpi = a.nullsp ? (V)((double)bi - mb) : bi;
-      a.bp[i] = bpi;
-      double s = 0.0;
-      for (int w = 0; w < WA; ++w) {
-        int j = __ldg(&a.col[w * n + i]);
-        if (j == PADI) break;
-        s += (double)__ldg(&a.val[w * n + i]) * (double)ld_cg(&a.x[j]);
+    double v[1] = {0.0}, t[1];
+    if (!grid_allreduce<1>(v, a.partials, a.bar, gen, a.status, t)) return;
+  }
+  // ---- r = b' - A x
+  double v2[2] = {0.0, 0.0}, t2[2];
+  if (CPT > 0) {
+#pragma unroll
+    for (int k = 0; k < NR; ++k) {
+      int i = i0 + k * stride;
+      if (i < n) {
+        double bi = (double)a.b[i];
+        double bpi = (double)(V)(a.nullsp ? bi - mb : bi);
+        double ri = bpi - spmv_row<V, WT>(a, i, a.x);
+        rx[k] = (double)a.x[i];
+        rr_[k] = (double)(V)ri;
+        rd[k] = (double)__ldg(&a.dinv[i]);
+        v2[0] += rr_[k] * rr_[k];
+        v2[1] += bpi * bpi;
       }
-      double ri = (double)bpi - s;
-      a.r[i] = (V)ri;
-      v[0] += ri * ri;
-      v[1] += (double)bpi * (double)bpi;
     }
-    double* P = part();
-    block_partial<2>(v, P + 4 * blockIdx.x);
-    if (!grid_sync(a.bar, nblk, gen, a.status)) return;
-    double t[2];
-    grid_total<2>(P, nblk, t);
-    double dp = sqrt(t[0]), sn = sqrt(t[1]);
-    double rnorm0 = a.guess_zero ? dp : (sn == 0.0 ? dp : sn);
-    a.dout[2] = sn;
-    // stash scalars in registers of every thread
-    a.dout[1] = dp;
-    double ttol = fmax(a.rtol * rnorm0, a.atol);
-    int reason = 0;
-    if (!(fabs(dp) <= 1.7976931348623157e308)) reason = -9;
-    else if (dp <= ttol) reason = dp < a.atol ? 3 : 2;
-    else if (dp >= 1.0e5 * rnorm0) reason = -4;
-    int its = 0;
-    if (!reason) {
-      // z = D^-1 r ; sums for the null-space projection and beta
-      double v4[4] = {0, 0, 0, 0};
+  } else {
+    for (int i = i0; i < n; i += stride) {
+      double bi = (double)a.b[i];
+      double bpi = (double)(V)(a.nullsp ? bi - mb : bi);
+      double ri = (double)(V)(bpi - spmv_row<V, WT>(a, i, a.x));
+      a.r[i] = (V)ri;
+      v2[0] += ri * ri;
+      v2[1] += bpi * bpi;
+    }
+  }
+  if (!grid_allreduce<2>(v2, a.partials, a.bar, gen, a.status, t2)) return;
+  double dp = sqrt(t2[0]);
+  const double sn = sqrt(t2[1]);
+  const double rnorm0 = a.guess_zero ? dp : (sn == 0.0 ? dp : sn);
+  const double ttol = fmax(a.rtol * rnorm0, a.atol);
+  int reason = classify(dp, ttol, a.atol, rnorm0);
+  int its = 0;
+  if (!reason) {
+    // ---- z = D^-1 r
+    double v4[4] = {0, 0, 0, 0}, t4[4];
+    if (CPT > 0) {
+#pragma unroll
+      for (int k = 0; k < NR; ++k) {
+        int i = i0 + k * stride;
+        if (i < n) {
+          rz[k] = (double)(V)(rr_[k] * rd[k]);
+          a.z[i] = (V)rz[k];
+          v4[0] += rz[k]; v4[1] += rr_[k]; v4[2] += rz[k] * rr_[k];
+        }
+      }
+    } else {
       for (int i = i0; i < n; i += stride) {
         double ri = (double)a.r[i];
-        double zi = (double)(V)(ri * (double)a.dinv[i]);
+        double zi = (double)(V)(ri * (double)__ldg(&a.dinv[i]));
         a.z[i] = (V)zi;
-        v4[0] += zi;
-        v4[1] += ri;
-        v4[2] += zi * ri;
-      }
-      double* P = part();
-      block_partial<4>(v4, P + 4 * blockIdx.x);
-      if (!grid_sync(a.bar, nblk, gen, a.status)) return;
-      double t4[4];
-      grid_total<4>(P, nblk, t4);
-      double mz = a.nullsp ? t4[0] / (double)n : 0.0;
-      double beta = a.nullsp ? t4[2] - mz * t4[1] : t4[2];
-      double betaold = 0.0, dpi = 0.0, dpiold = 0.0;
-      V* pold = a.p0;
-      V* pnew = a.p1;
-      int it = 0;
-      do {
-        its = it + 1;
-        if (beta == 0.0) { reason = 3; break; }
-        if (it > 0 && beta * betaold < 0.0) { reason = -8; break; }
-        const double bb = it == 0 ? 0.0 : beta / betaold;
-        // ---- phase A
-        {
-          double v1[1] = {0.0};
-          for (int i = i0; i < n; i += stride) {
-            double s = 0.0;
-            for (int w = 0; w < WA; ++w) {
-              int j = __ldg(&a.col[w * n + i]);
-              if (j == PADI) break;
-              double pj = (double)ld_cg(&a.z[j]) - mz;
-              if (it > 0) pj = pj + bb * (double)ld_cg(&pold[j]);
-              s += (double)__ldg(&a.val[w * n + i]) * (double)(V)pj;
-            }
-            double pi = (double)a.z[i] - mz;
-            if (it > 0) pi = pi + bb * (double)pold[i];
-            pnew[i] = (V)pi;
-            a.q[i] = (V)s;
-            v1[0] += (double)(V)pi * (double)(V)s;
-          }
-          double* P = part();
-          block_partial<1>(v1, P + 4 * blockIdx.x);
-          if (!grid_sync(a.bar, nblk, gen, a.status)) return;
-          double t1[1];
-          grid_total<1>(P, nblk, t1);
-          dpiold = dpi;
-          dpi = t1[0];
-        }
-        betaold = beta;
-        if (dpi == 0.0 || (it > 0 && ((dpi > 0) - (dpi < 0)) * ((dpiold > 0) - (dpiold < 0)) < 0)) {
-          reason = dpi == 0.0 ? 3 : -10;
-          break;
-        }
-        const double al = beta / dpi;
-        // ---- phase B
-        {
-          double v4b[4] = {0, 0, 0, 0};
-          for (int i = i0; i < n; i += stride) {
-            double pi = (double)pnew[i];
-            a.x[i] = (V)((double)a.x[i] + al * pi);
-            double ri = (double)a.r[i] - al * (double)a.q[i];
-            V rv = (V)ri;
-            a.r[i] = rv;
-            double rr = (double)rv;
-            double zi = (double)(V)(rr * (double)a.dinv[i]);
-            a.z[i] = (V)zi;
-            v4b[0] += rr * rr;
-            v4b[1] += zi;
-            v4b[2] += rr;
-            v4b[3] += zi * rr;
-          }
-          double* P = part();
-          block_partial<4>(v4b, P + 4 * blockIdx.x);
-          if (!grid_sync(a.bar, nblk, gen, a.status)) return;
-          double t4b[4];
-          grid_total<4>(P, nblk, t4b);
-          dp = sqrt(t4b[0]);
-          if (!(fabs(dp) <= 1.7976931348623157e308)) reason = -9;
-          else if (dp <= ttol) reason = dp < a.atol ? 3 : 2;
-          else if (dp >= 1.0e5 * rnorm0) reason = -4;
-          if (reason) break;
-          mz = a.nullsp ? t4b[1] / (double)n : 0.0;
-          beta = a.nullsp ? t4b[3] - mz * t4b[2] : t4b[3];
-        }
-        V* t = pold; pold = pnew; pnew = t;
-        it++;
-      } while (it < a.maxit);
-      if (!reason && it >= a.maxit) reason = -3;
-      a.dout[1] = dp;
-    }
-    // ---- true residual ||b - A x|| with the caller's right-hand side (KSPBuildResidual)
-    {
-      if (!grid_sync(a.bar, nblk, gen, a.status)) return;  // x complete everywhere
-      double v1[1] = {0.0};
-      for (int i = i0; i < n; i += stride) {
-        double s = 0.0;
-        for (int w = 0; w < WA; ++w) {
-          int j = __ldg(&a.col[w * n + i]);
-          if (j == PADI) break;
-          s += (double)__ldg(&a.val[w * n + i]) * (double)ld_cg(&a.x[j]);
-        }
-        double d = (double)a.b[i] - s;
-        v1[0] += d * d;
-      }
-      double* P = part();
-      block_partial<1>(v1, P + 4 * blockIdx.x);
-      if (!grid_sync(a.bar, nblk, gen, a.status)) return;
-      double t1[1];
-      grid_total<1>(P, nblk, t1);
-      if (blockIdx.x == 0 && threadIdx.x == 0) {
-        a.dout[0] = sqrt(t1[0]);
-        a.status[0] = reason;
-        a.status[1] = its;
+        v4[0] += zi; v4[1] += ri; v4[2] += zi * ri;
       }
     }
+    if (!grid_allreduce<4>(v4, a.partials, a.bar, gen, a.status, t4)) return;
+    double mz = a.nullsp ? t4[0] / (double)n : 0.0;
+    double beta = a.nullsp ? t4[2] - mz * t4[1] : t4[2];
+    double betaold = 0.0, dpi = 0.0, dpiold = 0.0;
+    V* pold = a.p0;
+    V* pnew = a.p1;
+    int it = 0;
+    do {
+      its = it + 1;
+      if (beta == 0.0) { reason = 3; break; }
+      if (it > 0 && beta * betaold < 0.0) { reason = -8; break; }
+      const double bb = it == 0 ? 0.0 : beta / betaold;
+      const bool first = it == 0;
+      // ---- phase A: p, q = A p, p.q
+      double v1[1] = {0.0}, t1[1];
+      if (CPT > 0) {
+#pragma unroll
+        for (int k = 0; k < NR; ++k) {
+          int i = i0 + k * stride;
+          if (i < n) {
+            double pi = rz[k] - mz;
+            if (!first) pi = pi + bb * rp[k];
+            rp[k] = (double)(V)pi;
+            pnew[i] = (V)rp[k];
+            rq[k] = (double)(V)spmv_row_p<V, WT>(a, i, pold, mz, bb, first);
+            v1[0] += rp[k] * rq[k];
+          }
+        }
+      } else {
+        for (int i = i0; i < n; i += stride) {
+          double pi = (double)a.z[i] - mz;
+          if (!first) pi = pi + bb * (double)pold[i];
+          pi = (double)(V)pi;
+          pnew[i] = (V)pi;
+          double qi = (double)(V)spmv_row_p<V, WT>(a, i, pold, mz, bb, first);
+          a.q[i] = (V)qi;
+          v1[0] += pi * qi;
+        }
+      }
+      if (!grid_allreduce<1>(v1, a.partials, a.bar, gen, a.status, t1)) return;
+      dpiold = dpi;
+      dpi = t1[0];
+      betaold = beta;
+      if (dpi == 0.0 || (it > 0 && ((dpi > 0) - (dpi < 0)) * ((dpiold > 0) - (dpiold < 0)) < 0)) {
+        reason = dpi == 0.0 ? 3 : -10;
+        break;
+      }
+      const double al = beta / dpi;
+      // ---- phase B: x, r, z and the four sums
+      double w4[4] = {0, 0, 0, 0}, s4[4];
+      if (CPT > 0) {
+#pragma unroll
+        for (int k = 0; k < NR; ++k) {
+          int i = i0 + k * stride;
+          if (i < n) {
+            rx[k] = (double)(V)(rx[k] + al * rp[k]);
+            rr_[k] = (double)(V)(rr_[k] - al * rq[k]);
+            rz[k] = (double)(V)(rr_[k] * rd[k]);
+            a.z[i] = (V)rz[k];
+            w4[0] += rr_[k] * rr_[k]; w4[1] += rz[k]; w4[2] += rr_[k]; w4[3] += rz[k] * rr_[k];
+          }
+        }
+      } else {
+        for (int i = i0; i < n; i += stride) {
+          double pi = (double)pnew[i];
+          a.x[i] = (V)((double)a.x[i] + al * pi);
+          double ri = (double)(V)((double)a.r[i] - al * (double)a.q[i]);
+          a.r[i] = (V)ri;
+          double zi = (double)(V)(ri * (double)__ldg(&a.dinv[i]));
+          a.z[i] = (V)zi;
+          w4[0] += ri * ri; w4[1] += zi; w4[2] += ri; w4[3] += zi * ri;
+        }
+      }
+      if (!grid_allreduce<4>(w4, a.partials, a.bar, gen, a.status, s4)) return;
+      dp = sqrt(s4[0]);
+      reason = classify(dp, ttol, a.atol, rnorm0);
+      if (reason) break;
+      mz = a.nullsp ? s4[1] / (double)n : 0.0;
+      beta = a.nullsp ? s4[3] - mz * s4[2] : s4[3];
+      V* t = pold; pold = pnew; pnew = t;
+      it++;
+    } while (it < a.maxit);
+    if (!reason && it >= a.maxit) reason = -3;
+  }
+  // ---- write back x, then the true residual ||b - A x|| with the caller's b (KSPBuildResidual)
+  if (CPT > 0) {
+#pragma unroll
+    for (int k = 0; k < NR; ++k) {
+      int i = i0 + k * stride;
+      if (i < n) a.x[i] = (V)rx[k];
+    }
+  }
+  double v1[1] = {0.0}, t1[1];
+  if (!grid_allreduce<1>(v1, a.partials, a.bar, gen, a.status, t1)) return;
+  for (int i = i0; i < n; i += stride) {
+    double d = (double)a.b[i] - spmv_row<V, WT>(a, i, a.x);
+    v1[0] += d * d;
+  }
+  if (!grid_allreduce<1>(v1, a.partials, a.bar, gen, a.status, t1)) return;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    a.dout[0] = sqrt(t1[0]);
+    a.dout[1] = dp;
+    a.dout[2] = sn;
+    a.status[0] = reason;
+    a.status[1] = its;
+  }
+}
+
+// Host helper: picks the instantiation for the mesh size (register-resident when it fits) and
+// row width (fixed 7 for hexahedral meshes).
+template <class V>
+inline void* pcg_kernel_for(int n, int grid, int width, int* cpt_out) {
+  const long cap = (long)grid * PCG_TPB;
+  int cpt = n <= cap ? 1 : n <= 2 * cap ? 2 : n <= 3 * cap ? 3 : n <= 4 * cap ? 4 : 0;
+  *cpt_out = cpt;
+  if (width == 7) {
+    switch (cpt) {
+      case 1: return (void*)k_pcg<V, 1, 7>;
+      case 2: return (void*)k_pcg<V, 2, 7>;
+      case 3: return (void*)k_pcg<V, 3, 7>;
+      case 4: return (void*)k_pcg<V, 4, 7>;
+      default: return (void*)k_pcg<V, 0, 7>;
+    }
+  }
+  switch (cpt) {
+    case 1: return (void*)k_pcg<V, 1, 0>;
+    case 2: return (void*)k_pcg<V, 2, 0>;
+    case 3: return (void*)k_pcg<V, 3, 0>;
+    case 4: return (void*)k_pcg<V, 4, 0>;
+    default: return (void*)k_pcg<V, 0, 0>;
   }
 }
 

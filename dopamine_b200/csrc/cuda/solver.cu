@@ -163,6 +163,8 @@ struct Solver {
   double *conv_tmp = nullptr, *visc_tmp = nullptr;
   // PCG workspace
   double *cg_r, *cg_z, *cg_p0, *cg_p1, *cg_q, *cg_bp, *cg_x, *cg_part, *cg_dout;
+  void* cg_kernel = nullptr;
+  int cg_cpt = 0;
   unsigned* cg_bar;
   int* cg_status;
   int cg_grid = 0;
@@ -318,12 +320,25 @@ struct Solver {
     int dev_sms = 0, per_sm = 0, coop = 0;
     CK(cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, device));
     CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg<double>, TPB, 0));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg<double, 0, 0>, PCG_TPB, 0));
     cg_coop = coop != 0 && per_sm > 0;
     if (!cg_coop) return DPM_ERR_UNSUPPORTED;
-    cg_grid = std::min(dev_sms * per_sm, std::max(1, nblk(nc)));
-    cg_grid = std::min(cg_grid, 2048);
-    cg_part = mem.alloc<double>(2 * 4 * (size_t)cg_grid);
+    cg_grid = std::min(dev_sms * per_sm, std::max(1, (nc + PCG_TPB - 1) / PCG_TPB));
+    cg_kernel = pcg_kernel_for<double>(nc, cg_grid, S.WA, &cg_cpt);
+    // A and 1/diag should stay in L1 across iterations: prefer the largest L1 carveout (set before
+    // the occupancy query, which the cooperative launch check must agree with).
+    CK(cudaFuncSetAttribute(cg_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 5));
+    {
+      int per_sm2 = 0;
+      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, cg_kernel, PCG_TPB, 0));
+      if (per_sm2 < 1) return DPM_ERR_UNSUPPORTED;
+      if (dev_sms * per_sm2 < cg_grid) {  // fewer co-resident blocks: re-pick with the smaller grid
+        cg_grid = dev_sms * per_sm2;
+        cg_kernel = pcg_kernel_for<double>(nc, cg_grid, S.WA, &cg_cpt);
+        CK(cudaFuncSetAttribute(cg_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 5));
+      }
+    }
+    cg_part = mem.alloc<double>(8 * (size_t)cg_grid);
     // initial fields: T = T_ref, velocity from an inlet patch (initialize_velocity_from_bc)
     launch_fill(F.T, nc, P.T_ref);
     double u0[3] = {0, 0, 0};
@@ -493,7 +508,7 @@ struct Solver {
     CK(cudaMemsetAsync(cg_bar, 0, 2 * sizeof(unsigned), st));
     CK(cudaMemsetAsync(cg_status, 0, 4 * sizeof(int), st));
     void* args[] = {&a};
-    CK(cudaLaunchCooperativeKernel((void*)k_pcg<double>, dim3(cg_grid), dim3(TPB), args, 0, st));
+    CK(cudaLaunchCooperativeKernel(cg_kernel, dim3(cg_grid), dim3(PCG_TPB), args, 0, st));
     launches++;
     int h_st[4];
     double h_d[4];

@@ -213,6 +213,11 @@ int build_static_ops(const Mesh& m, const dpm_patch_cfg_t* pc, const dpm_params_
     ell_from_lists(cols, nc, w1, S.A_col, PAD);
     ell_from_lists(vals, nc, w2, S.A_val, 0.0);
     S.WA = w1;
+    // pad every row to the full width with (self, 0): fixed-length rows, no early exit on the GPU
+    for (int64_t c = 0; c < nc; ++c)
+      for (int w = 0; w < S.WA; ++w)
+        if (S.A_col[(size_t)w * nc + c] == PAD) S.A_col[(size_t)w * nc + c] = (int)c;
+    if (S.WA > 16) return DPM_ERR_UNSUPPORTED;
   }
   // Per-cell lists.
   {
