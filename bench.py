@@ -113,6 +113,19 @@ def pcg_bytes_per_iteration(s):
     return phase_a + phase_b
 
 
+def pcg_traffic_per_launch():
+    """DRAM bytes (read + write) of one k_pcg launch on this workload, from the committed ncu
+    summary (one capture, its command inside the file); None when the summary is absent."""
+    path = os.path.join(ROOT, "profiles", "k_pcg_channel96x64x64.md")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return int(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
 def run_gpu(args, rank, world):
     import torch
     from dopamine_b200.solver import Solver, lib
@@ -237,13 +250,7 @@ def main():
     bytes_it = pcg_bytes_per_iteration(s)
     pois_s = sum(r["pois_ms"]) / 1e3
     achieved = bytes_it * r["its"] / pois_s / 1e9 if pois_s > 0 else 0.0
-    traffic = None
-    prof = os.path.join(ROOT, "profiles", "pcg_traffic.json")
-    if os.path.exists(prof):
-        try:
-            traffic = json.load(open(prof)).get("dram_bytes_per_launch")
-        except Exception:
-            traffic = None
+    traffic = pcg_traffic_per_launch() if args.config == "channel" else None
     line = {
         "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world, "steps": K,
         "warmup": args.warmup, "ms_per_step": 1e3 * r["t_dev"] / K, "higher_is_better": True, "scaling": "weak",
