@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libdopamine_b200.so")
-CU_SOURCES = ["csrc/cuda/solver.cu", "csrc/cuda/fvm_petsc.cu"]
+CU_SOURCES = ["csrc/cuda/solver.cu", "csrc/cuda/fvm_petsc.cu", "csrc/cuda/noalloc.cu"]
 CPP_SOURCES = ["csrc/host/mesh.cpp", "csrc/host/ops.cpp"]
 HEADERS = ["csrc/cuda/common.cuh", "csrc/cuda/kernels.cuh", "csrc/cuda/pcg.cuh", "csrc/host/mesh.hpp",
            "csrc/host/ops.hpp", "../include/dopamine_b200.h"]

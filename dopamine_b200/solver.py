@@ -23,7 +23,7 @@ EXPORTED = (
     "dpm_download_face_flux", "dpm_download_gradient", "dpm_cell_geometry", "dpm_project_once", "dpm_advance",
     "dpm_advance_n", "dpm_stats", "dpm_state_is_finite", "dpm_compute_dt", "dpm_get_time", "dpm_set_time",
     "dpm_last_timing", "dpm_kernel_launches", "dpm_ls_gradient_vector", "dpm_advection_rhs_vector",
-    "dpm_viscous_rhs_vector", "dpm_sgs_viscosity", "dpm_wall_model",
+    "dpm_viscous_rhs_vector", "dpm_sgs_viscosity", "dpm_wall_model", "dpm_pcg_solve_noalloc",
 )
 
 
@@ -73,6 +73,8 @@ def lib(build_if_missing=True):
     L.fvm_petsc_insert_option.argtypes = [C.c_char_p]
     L.fvm_petsc_set_io_on_device.argtypes = [C.c_int]
     L.fvm_petsc_set_device_local_rank.argtypes = [C.c_int]
+    L.dpm_pcg_solve_noalloc.argtypes = [C.c_int, C.c_int, vp, vp, vp, vp, vp, C.c_double, C.c_double, C.c_int,
+                                        C.c_int, vp, ip, dp]
     _lib = L
     return L
 

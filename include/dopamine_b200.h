@@ -223,6 +223,26 @@ int dpm_sgs_viscosity(dpm_solver_t* s, int model, const double* U, const double*
 /* apply_wall_model_bc (src/sgs/mod_wall_model.f90:176): tau_w(3,nbnd). */
 int dpm_wall_model(dpm_solver_t* s, const double* U, double nu, double* tau_w);
 
+/* ---- allocation-free Jacobi-PCG solve --------------------------------------------------------
+ * No counterpart in the reference.  For callers that cannot allocate device memory when they
+ * solve (hosts whose device memory is owned by their own pool allocator, or latency-bound loops
+ * where cudaMalloc's implicit synchronization is unacceptable).  All pointers are DEVICE
+ * pointers owned by the caller: the operator in padded ELL form [row_width][n_cells] (col, val;
+ * padding entries are (own row, 0.0)), the inverse diagonal, the right-hand side and the
+ * solution x (used as the initial guess, overwritten).  Work vectors live in a fixed
+ * file-scope device array of DPM_NOALLOC_MAX_CELLS cells (about 5.3 MB, held by every GPU that
+ * loads the library until exit); larger systems or rows wider than 16 return DPM_ERR_ARG.
+ * Same stopping rule as fvm_petsc_solve_pressure (unpreconditioned norm, PETSc KSPCG test);
+ * null_space != 0 projects the constant mode out of the right-hand side.  The first call on a
+ * device looks up the array's address and must come before any stream capture.  Every call
+ * shares the array: calls that overlap on the GPU race and must be serialized by the caller.
+ * Blocks until the solve on `stream` (a cudaStream_t, NULL = legacy default) has finished. */
+#define DPM_NOALLOC_MAX_CELLS 131072
+int dpm_pcg_solve_noalloc(int n_cells, int row_width, const int* col, const double* val,
+                          const double* inv_diag, const double* rhs, double* x, double rtol, double atol,
+                          int max_iterations, int null_space, void* stream, int* iteration_count,
+                          double* residual_norm);
+
 #ifdef __cplusplus
 }
 #endif
