@@ -95,6 +95,13 @@ class ClockSampler:
         return out
 
 
+FORMS = {"pcg": "plain FP64 Jacobi-PCG",
+         "fcg": "FP64 flexible CG, two-level preconditioner (FP32 part-local Chebyshev + coarse)"}
+
+
+KERNELS = {"pcg": "k_pcg (persistent Jacobi-PCG)", "fcg": "k_fcg (persistent two-level flexible CG)"}
+
+
 def make_case(name):
     from dopamine_b200 import cases
     if name == "channel":
@@ -104,10 +111,14 @@ def make_case(name):
     raise ValueError(name)
 
 
-def pcg_bytes_per_iteration(s):
-    """Algorithmic bytes of one PCG iteration (both phases), per the ELL operator width."""
+def pcg_bytes_per_iteration(s, psolver="pcg"):
+    """Algorithmic bytes of one Krylov iteration, per the ELL operator width (hex: 7)."""
     nc = s.nc
     wa = 7  # hex mesh: diagonal + 6 neighbours
+    if psolver == "fcg":
+        # w = A z: cols + vals, z gathered once per cell, z written once; the part-local smoother
+        # and the own-cell vectors live in shared memory and registers
+        return nc * (wa * (4 + 8) + 8 + 8)
     phase_a = nc * (wa * (4 + 8) + 8 + 8 + 8 + 8)   # cols, vals, z, p_old, write p_new, write q
     phase_b = nc * (5 * 8 + 3 * 8)                  # x, p, r, q, dinv in; x, r, z out
     return phase_a + phase_b
@@ -133,6 +144,8 @@ def run_gpu(args, rank, world):
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(dev)
     case = make_case(args.config)
+    if args.psolver == "fcg":
+        case.params["p_solver"] = 1  # DPM_PSOLVER_TWOLEVEL_FCG
     s = Solver(case, device=dev)
     s.initialise()
     nc = s.nc
@@ -208,6 +221,8 @@ def main():
     ap.add_argument("--impl", default="dopamine_b200")
     ap.add_argument("--config", default="channel")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--psolver", default="pcg", choices=["pcg", "fcg"],
+                    help="pcg: plain FP64 Jacobi-PCG; fcg: flexible CG, two-level part-local preconditioner")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -247,21 +262,21 @@ def main():
     value = world * nc * K / r["t_dev"]
     e2e = world * nc * K / r["t_e2e"]
     peak, peak_kind = measured_peaks()
-    bytes_it = pcg_bytes_per_iteration(s)
+    bytes_it = pcg_bytes_per_iteration(s, args.psolver)
     pois_s = sum(r["pois_ms"]) / 1e3
     achieved = bytes_it * r["its"] / pois_s / 1e9 if pois_s > 0 else 0.0
-    traffic = pcg_traffic_per_launch() if args.config == "channel" else None
+    traffic = pcg_traffic_per_launch() if args.config == "channel" and args.psolver == "pcg" else None
     line = {
         "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world, "steps": K,
         "warmup": args.warmup, "ms_per_step": 1e3 * r["t_dev"] / K, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": cfg_name, "cells": nc, "form": "plain FP64 Jacobi-PCG",
+        "config": {"workload": cfg_name, "cells": nc, "form": FORMS[args.psolver],
                    "poisson_ms_per_step": 1e3 * pois_s / K, "pcg_iterations_per_step": r["its"] / K,
                    "poisson_solves_per_step": r["solves"] / K,
                    "l2": "inputs larger than L2: static operator data streamed each step exceeds 126 MB",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
         "e2e": {"value": e2e, "unit": "cell-steps/s", "h2d_bytes_per_step": 32 * nc, "d2h_bytes_per_step": 32 * nc},
-        "roofline": {"kernel": "k_pcg (persistent Jacobi-PCG)", "bound": "hbm", "achieved": achieved, "peak": peak,
+        "roofline": {"kernel": KERNELS[args.psolver], "bound": "hbm", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
                      "bytes_per_iteration": bytes_it},
         "gpu_launches": r["launches"],

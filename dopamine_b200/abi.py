@@ -21,6 +21,7 @@ SCHEME_BY_NAME = {"VANLEER_TVD": 1, "KOREN_TVD": 2, "CDS": 3, "KEP": 4, "QUICK":
 SGS_NONE, SGS_VREMAN, SGS_SMAGORINSKY, SGS_AMD = 0, 1, 2, 3
 WM_LOGLAW, WM_NONE = 0, 1
 FORM_FP64, FORM_MIXED = 0, 1
+PSOLVER_JACOBI_PCG, PSOLVER_TWOLEVEL_FCG = 0, 1
 
 EL_TET4, EL_HEX8, EL_PRISM6, EL_PYR5 = 4, 5, 6, 7
 
@@ -56,6 +57,8 @@ class ParamsT(C.Structure):
         ("scalar_scheme", C.c_int), ("scalar_diffusivity", C.c_double * 4), ("scalar_pr_t", C.c_double * 4),
         ("c_amd", C.c_double), ("amd_wall_gradient", C.c_int), ("wall_model_height", C.c_double),
         ("wall_model_filter_time", C.c_double), ("wall_model_filter_tf_fac", C.c_double), ("form", C.c_int),
+        ("p_solver", C.c_int), ("p_smooth_degree", C.c_int), ("p_smooth_lmin", C.c_double),
+        ("p_smooth_lmax", C.c_double),
     ]
 
 
@@ -100,6 +103,10 @@ def default_params(**kw):
     p.c_amd = 1.0 / 3.0
     p.amd_wall_gradient = 1
     p.form = FORM_FP64
+    p.p_solver = PSOLVER_JACOBI_PCG
+    p.p_smooth_degree = 6
+    p.p_smooth_lmin = 0.05
+    p.p_smooth_lmax = 2.0
     for k, v in kw.items():
         if k in ("f_const", "g"):
             arr = getattr(p, k)

@@ -15,8 +15,9 @@ ROOT = os.path.dirname(HERE)
 OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libdopamine_b200.so")
 CU_SOURCES = ["csrc/cuda/solver.cu", "csrc/cuda/fvm_petsc.cu", "csrc/cuda/noalloc.cu"]
-CPP_SOURCES = ["csrc/host/mesh.cpp", "csrc/host/ops.cpp"]
-HEADERS = ["csrc/cuda/common.cuh", "csrc/cuda/kernels.cuh", "csrc/cuda/pcg.cuh", "csrc/host/mesh.hpp",
+CPP_SOURCES = ["csrc/host/mesh.cpp", "csrc/host/ops.cpp", "csrc/host/twolevel.cpp"]
+HEADERS = ["csrc/cuda/common.cuh", "csrc/cuda/kernels.cuh", "csrc/cuda/pcg.cuh", "csrc/cuda/fcg.cuh",
+           "csrc/host/twolevel.hpp", "csrc/host/mesh.hpp",
            "csrc/host/ops.hpp", "../include/dopamine_b200.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -1,0 +1,428 @@
+// Flexible conjugate gradients with a two-level (part-local Chebyshev + coarse) preconditioner,
+// as one persistent cooperative kernel: the "chosen form" pressure solve.
+//
+// Cells are renumbered into P compact parts, one per thread block (dopamine_b200/csrc/host/
+// twolevel.cpp); part b owns rows [b*C, b*C + size_b).  Per iteration (FCG(1), Notay 2000):
+//
+//   z  = y_b + S_b(r)          y = E^-1 c, c = Z^T r (one value per part, all-gathered);
+//                              S_b: `degree` Chebyshev steps on D^-1 A_bb in shared memory (FP32)
+//   grid barrier               (z is read by neighbour parts)
+//   w  = A z                   FP64, global ELL
+//   all-reduce                 z.r, z.q, z.w, r.r and the null-space sums; all-gather per part
+//                              sum r, sum w, sum q
+//   beta = -z'.q / (p.q)_old,  p.q = z'.w + 2 beta z'.q + beta^2 (p.q)_old,  alpha = z'.r / p.q
+//   p = z' + beta p,  q = w + beta q,  x += alpha p,  r -= alpha q,  c = sum r - alpha (sum w + beta sum q)
+//
+// so an iteration has one barrier and one all-reduce, like the Jacobi-PCG kernel, while the
+// preconditioner works without any grid-wide wait.  The stopping rule is the reference's
+// (unpreconditioned ||r|| <= max(rtol ||b'||, atol), src/solver/pressure_backend_petsc.c:816-876),
+// tested on the current residual at the top of each iteration.  Krylov vectors, reductions and
+// the coarse solve are FP64; only the part-local smoother runs in FP32.
+#pragma once
+#include "pcg.cuh"
+
+namespace dpm {
+namespace gpu {
+
+constexpr int FCG_TPB = 1024;
+constexpr int FCG_SLOT = 16;  // doubles per block in the reduce/gather buffer
+constexpr int FCG_NV = 8;     // reduced sums
+constexpr int FCG_NG = 3;     // gathered per-part values
+
+struct FcgArgs {
+  int n, P, C, WL, maxit, nullsp, guess_zero, degree;
+  const int* perm;        // perm[new] = old
+  const int* col;         // [WA][n] new numbering, padded (self, 0)
+  const double* val;      // [WA][n]
+  const double* dinv;     // [n] new numbering
+  const unsigned* lpk;    // [WL][n] local column (low 16 bits) | bf16 a_ij / a_ii (high 16 bits)
+  const double* einv;     // [P][P]
+  const double* b;        // right-hand side, original numbering
+  double* x;              // guess in / solution out, original numbering
+  double* xs;             // [n] scratch, new numbering
+  double* zs;             // [n] scratch, new numbering
+  double* partials;       // [2][P][FCG_SLOT]
+  unsigned* bar;          // [0] arrival counter
+  int* status;            // [0] reason, [1] iterations, [2] barrier timeout
+  double* dout;           // [0] true residual, [1] last ||r||, [2] ||b'||
+  double rtol, atol;
+  float theta, delta;     // Chebyshev interval [theta - delta, theta + delta] of D^-1 A_bb
+};
+
+// Bounded grid barrier on the same monotonic counter as grid_allreduce (one arrival per block).
+__device__ __forceinline__ bool grid_barrier(unsigned* bar, unsigned& gen, int* status) {
+  __shared__ int s_okb;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    const unsigned target = (gen + 1u) * gridDim.x;
+    __threadfence();
+    atomicAdd(&bar[0], 1u);
+    unsigned spins = 0;
+    for (;;) {
+      unsigned cur;
+      asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(cur) : "l"(&bar[0]) : "memory");
+      if ((int)(cur - target) >= 0) break;
+      if (++spins > DPM_BARRIER_SPIN_LIMIT) { ok = 0; atomicExch(&status[2], 1); break; }
+      if (spins > 32) __nanosleep(20);
+    }
+    __threadfence();
+    s_okb = ok;
+  }
+  __syncthreads();
+  gen = gen + 1u;
+  return s_okb != 0;
+}
+
+// All-reduce of the first NV of v (deterministic, as grid_allreduce) plus an all-gather of the
+// block totals of the last NG into gat[k*P + block] (shared memory: every block gets every
+// block's values).  v holds per-thread partials of all NV + NG values.  All reductions of the
+// FCG kernel go through here so that every generation uses the same slot layout of the
+// double-buffered partials.
+template <int NV, int NG>
+__device__ __forceinline__ bool grid_reduce_gather(double (&v)[NV + NG], double* partials, unsigned* bar,
+                                                   unsigned& gen, int* status, double (&res)[NV], double* gat) {
+  constexpr int NT = NV + NG;
+  static_assert(NT <= FCG_SLOT, "slot too small");
+  __shared__ double sh[32][NT];
+  __shared__ double shr[NV > 0 ? NV : 1];
+  __shared__ int s_ok;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int P = gridDim.x;
+  double* buf = partials + (size_t)(gen & 1u) * FCG_SLOT * P;
+#pragma unroll
+  for (int k = 0; k < NT; ++k)
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < NT; ++k) sh[w][k] = v[k];
+  __syncthreads();
+  if (w == 0) {
+    double t[NT];
+#pragma unroll
+    for (int k = 0; k < NT; ++k) {
+      t[k] = lane < nw ? sh[lane][k] : 0.0;
+      for (int o = 16; o > 0; o >>= 1) t[k] += __shfl_down_sync(0xffffffffu, t[k], o);
+    }
+    int ok = 1;
+    if (lane == 0) {
+#pragma unroll
+      for (int k = 0; k < NT; ++k) buf[blockIdx.x * FCG_SLOT + k] = t[k];
+      const unsigned target = (gen + 1u) * gridDim.x;
+      __threadfence();
+      atomicAdd(&bar[0], 1u);
+      unsigned spins = 0;
+      for (;;) {
+        unsigned cur;
+        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(cur) : "l"(&bar[0]) : "memory");
+        if ((int)(cur - target) >= 0) break;
+        if (++spins > DPM_BARRIER_SPIN_LIMIT) { ok = 0; atomicExch(&status[2], 1); break; }
+        if (spins > 32) __nanosleep(20);
+      }
+      __threadfence();
+    }
+    ok = __shfl_sync(0xffffffffu, ok, 0);
+    if (lane == 0) s_ok = ok;
+  }
+  __syncthreads();
+  const bool ok = s_ok != 0;
+  if (ok) {
+    if (w == 0) {
+      double u[NV > 0 ? NV : 1];
+#pragma unroll
+      for (int k = 0; k < NV; ++k) u[k] = 0.0;
+      for (int b = lane; b < P; b += 32)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) u[k] += __ldcg(&buf[b * FCG_SLOT + k]);
+#pragma unroll
+      for (int k = 0; k < NV; ++k) {
+        for (int o = 16; o > 0; o >>= 1) u[k] += __shfl_down_sync(0xffffffffu, u[k], o);
+        if (lane == 0) shr[k] = u[k];
+      }
+    }
+    for (int idx = threadIdx.x; idx < NG * P; idx += blockDim.x) {
+      const int k = idx / P, b = idx - k * P;
+      gat[idx] = __ldcg(&buf[b * FCG_SLOT + NV + k]);
+    }
+  }
+  __syncthreads();
+  gen = gen + 1u;
+#pragma unroll
+  for (int k = 0; k < NV; ++k) res[k] = ok ? shr[k] : 0.0;
+  return ok;
+}
+
+// Row i (new numbering) of A times v, global ELL with fixed width WT (0: runtime width <= 16).
+template <int WT>
+__device__ __forceinline__ double fcg_row(const FcgArgs& a, int WA, int i, const double* v) {
+  const int n = a.n;
+  constexpr int W = WT > 0 ? WT : 16;
+  const int wa = WT > 0 ? WT : WA;
+  int c[W];
+#pragma unroll
+  for (int w = 0; w < W; ++w)
+    if (w < wa) c[w] = __ldg(&a.col[w * n + i]);
+  double x[W];
+#pragma unroll
+  for (int w = 0; w < W; ++w)
+    if (w < wa) x[w] = __ldcg(&v[c[w]]);
+  double s = 0.0;
+#pragma unroll
+  for (int w = 0; w < W; ++w)
+    if (w < wa) s += __ldcg(&a.val[w * n + i]) * x[w];
+  return s;
+}
+
+// Dynamic shared memory of the kernel for a given set-up.
+inline size_t fcg_smem_bytes(int P, int C, int WL) {
+  return (size_t)2 * P * sizeof(double)                 // gathered sums r, own E^-1 row
+         + (size_t)FCG_NG * P * sizeof(double)           // gather landing area
+         + (size_t)3 * C * sizeof(double)                // own x, p, q
+         + (size_t)C * sizeof(float)                     // own 1/diag (FP32, smoother)
+         + (size_t)WL * C * sizeof(unsigned)             // packed local rows
+         + (size_t)2 * C * sizeof(float);                // Chebyshev direction, double-buffered
+}
+
+// CPT: cells per thread (C <= CPT * FCG_TPB); WT: global row width (7 for hexahedra, 0 = runtime).
+template <int CPT, int WT>
+__global__ void __launch_bounds__(FCG_TPB, 1) k_fcg(FcgArgs a, int WA) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int P = a.P, C = a.C, WL = a.WL, n = a.n;
+  double* s_c = reinterpret_cast<double*>(smem);          // [P] c = Z^T r
+  double* s_er = s_c + P;                                  // [P] row b of E^-1
+  double* s_gat = s_er + P;                                // [NG][P]
+  double* s_x = s_gat + FCG_NG * P;                        // [C] own x
+  double* s_p = s_x + C;                                   // [C] own p
+  double* s_q = s_p + C;                                   // [C] own q
+  float* s_dinv = reinterpret_cast<float*>(s_q + C);       // [C]
+  unsigned* s_lpk = reinterpret_cast<unsigned*>(s_dinv + C);  // [WL][C]
+  float* s_d0 = reinterpret_cast<float*>(s_lpk + (size_t)WL * C);  // [C]
+  float* s_d1 = s_d0 + C;                                  // [C]
+  __shared__ double s_y;
+
+  constexpr int LW = WT > 0 ? WT - 1 : 16;  // unrolled bound of the local row width
+  const int b = blockIdx.x;
+  const int base = b * C;
+  const int size = min(C, n - base);
+  unsigned gen = 0;
+
+  // ---- stage the part's local operator and E^-1 row
+  for (int s = 0; s < WL; ++s)
+    for (int l = threadIdx.x; l < size; l += blockDim.x) s_lpk[s * C + l] = a.lpk[(size_t)s * n + base + l];
+  for (int j = threadIdx.x; j < P; j += blockDim.x) s_er[j] = a.einv[(size_t)b * P + j];
+
+  // own-cell state: r in registers; x, p, q and the FP32 1/diag in shared memory
+  double rr[CPT];
+#define OWN(k) (threadIdx.x + (k) * FCG_TPB < size)
+#pragma unroll
+  for (int k = 0; k < CPT; ++k) {
+    const int l = threadIdx.x + k * FCG_TPB;
+    rr[k] = 0.0;
+    if (OWN(k)) {
+      s_p[l] = 0.0;
+      s_q[l] = 0.0;
+      const int i = base + l;
+      const int o = __ldg(&a.perm[i]);
+      const double x0 = a.guess_zero ? 0.0 : a.x[o];
+      s_x[l] = x0;
+      rr[k] = a.b[o];  // b for now
+      s_dinv[l] = (float)__ldg(&a.dinv[i]);
+      a.xs[i] = x0;
+    }
+  }
+  // ---- b' = b - mean(b) (null space), r = b' - A x, c = Z^T r
+  double mb = 0.0;
+  {
+    double v[1] = {0.0}, t[1];
+#pragma unroll
+    for (int k = 0; k < CPT; ++k)
+      if (OWN(k)) v[0] += rr[k];
+    if (!grid_reduce_gather<1, 0>(v, a.partials, a.bar, gen, a.status, t, s_gat)) return;  // publishes xs
+    mb = a.nullsp ? t[0] / (double)n : 0.0;
+  }
+  double v2[2 + 1], t2[2];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) v2[k] = 0.0;
+#pragma unroll
+  for (int k = 0; k < CPT; ++k)
+    if (OWN(k)) {
+      const int i = base + threadIdx.x + k * FCG_TPB;
+      const double bp = rr[k] - mb;
+      rr[k] = bp - fcg_row<WT>(a, WA, i, a.xs);
+      v2[0] += rr[k] * rr[k];
+      v2[1] += bp * bp;
+      v2[2] += rr[k];  // gathered: part sum of r
+    }
+  if (!grid_reduce_gather<2, 1>(v2, a.partials, a.bar, gen, a.status, t2, s_gat)) return;
+  for (int j = threadIdx.x; j < P; j += blockDim.x) s_c[j] = s_gat[j];
+  double dp = sqrt(t2[0]);
+  const double sn = sqrt(t2[1]);
+  const double rnorm0 = a.guess_zero ? dp : (sn == 0.0 ? dp : sn);
+  const double ttol = fmax(a.rtol * rnorm0, a.atol);
+  int reason = classify(dp, ttol, a.atol, rnorm0);
+  int its = 0;
+  double pq_old = 1.0;
+  const float th = a.theta, de = a.delta;
+  const float sig = th / de;
+  while (!reason) {
+    if (its >= a.maxit) { reason = -3; break; }
+    __syncthreads();  // s_c complete
+    // ---- coarse value of this part: y_b = sum_j E^-1[b][j] c[j]
+    if (threadIdx.x < 32) {
+      double s = 0.0;
+      for (int j = threadIdx.x; j < P; j += 32) s += s_er[j] * s_c[j];
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+      if (threadIdx.x == 0) s_y = s;
+    }
+    // ---- part-local Chebyshev on D^-1 A_bb z = D^-1 r (FP32, shared memory).  With the
+    // scaled residual s = D^-1 (r - A_bb z):  z += d;  s -= D^-1 A_bb d = d + sum a~_ij d_j;
+    // d = c1 d + c2 s  (Saad, Iterative Methods, alg. 12.1, on the Jacobi-scaled operator).
+    float zc[CPT], sc[CPT], dc[CPT];
+#pragma unroll
+    for (int k = 0; k < CPT; ++k) {
+      sc[k] = OWN(k) ? s_dinv[threadIdx.x + k * FCG_TPB] * (float)rr[k] : 0.0f;
+      dc[k] = sc[k] / th;
+      zc[k] = 0.0f;
+    }
+    float rho = 1.0f / sig;
+    float* dcur = s_d0;
+    float* dnext = s_d1;
+    for (int j = 0; j < a.degree; ++j) {
+#pragma unroll
+      for (int k = 0; k < CPT; ++k) {
+        zc[k] += dc[k];
+        if (OWN(k)) dcur[threadIdx.x + k * FCG_TPB] = dc[k];
+      }
+      if (j == a.degree - 1) break;
+      __syncthreads();
+      const float rhon = 1.0f / (2.0f * sig - rho);
+      const float c1 = rhon * rho, c2 = 2.0f * rhon / de;
+#pragma unroll
+      for (int k = 0; k < CPT; ++k)
+        if (OWN(k)) {
+          const int l = threadIdx.x + k * FCG_TPB;
+          float ad = dc[k];
+#pragma unroll
+          for (int s = 0; s < LW; ++s)
+            if (s < WL) {
+              const unsigned e = s_lpk[s * C + l];
+              ad = fmaf(__uint_as_float(e & 0xFFFF0000u), dcur[e & 0xFFFFu], ad);
+            }
+          sc[k] -= ad;
+          dc[k] = c1 * dc[k] + c2 * sc[k];
+        }
+      rho = rhon;
+      float* t = dcur; dcur = dnext; dnext = t;
+    }
+    __syncthreads();  // s_y visible
+    const double yb = s_y;
+    // ---- z to global, barrier, w = A z and the sums
+    double rz[CPT];
+#pragma unroll
+    for (int k = 0; k < CPT; ++k) {
+      rz[k] = (double)zc[k] + yb;
+      if (OWN(k)) a.zs[base + threadIdx.x + k * FCG_TPB] = rz[k];
+    }
+    if (!grid_barrier(a.bar, gen, a.status)) return;
+    double v[FCG_NV + FCG_NG], t[FCG_NV];
+#pragma unroll
+    for (int k = 0; k < FCG_NV + FCG_NG; ++k) v[k] = 0.0;
+    double rw[CPT];
+#pragma unroll
+    for (int k = 0; k < CPT; ++k) {
+      rw[k] = 0.0;
+      if (OWN(k)) {
+        const int i = base + threadIdx.x + k * FCG_TPB;
+        rw[k] = fcg_row<WT>(a, WA, i, a.zs);
+        const double qk = s_q[threadIdx.x + k * FCG_TPB];
+        v[0] += rz[k] * rr[k];
+        v[1] += rz[k] * qk;
+        v[2] += rz[k] * rw[k];
+        v[3] += rz[k];
+        v[4] += rr[k] * rr[k];
+        v[5] += rr[k];
+        v[6] += qk;
+        v[7] += rw[k];
+        v[8] += rr[k];   // gathered: part sums of r, w, q
+        v[9] += rw[k];
+        v[10] += qk;
+      }
+    }
+    if (!grid_reduce_gather<FCG_NV, FCG_NG>(v, a.partials, a.bar, gen, a.status, t, s_gat)) return;
+    dp = sqrt(t[4]);
+    reason = classify(dp, ttol, a.atol, rnorm0);
+    if (reason) break;
+    const double m = a.nullsp ? t[3] / (double)n : 0.0;
+    const double zr = t[0] - m * t[5], zq = t[1] - m * t[6], zw = t[2] - m * t[7];
+    const double beta = its == 0 ? 0.0 : -zq / pq_old;
+    const double pq = zw + 2.0 * beta * zq + beta * beta * pq_old;
+    if (!(pq > 0.0)) { reason = pq == 0.0 ? 3 : -10; break; }
+    const double al = zr / pq;
+#pragma unroll
+    for (int k = 0; k < CPT; ++k)
+      if (OWN(k)) {
+        const int l = threadIdx.x + k * FCG_TPB;
+        const double pk = (rz[k] - m) + beta * s_p[l];
+        const double qk = rw[k] + beta * s_q[l];
+        s_p[l] = pk;
+        s_q[l] = qk;
+        s_x[l] += al * pk;
+        rr[k] -= al * qk;
+      }
+    for (int j = threadIdx.x; j < P; j += blockDim.x)
+      s_c[j] = s_gat[j] - al * (s_gat[P + j] + beta * s_gat[2 * P + j]);
+    pq_old = pq;
+    ++its;
+  }
+  // ---- write back x (original numbering) and the true residual ||b - A x||
+  double v1[1] = {0.0}, t1[1];
+#pragma unroll
+  for (int k = 0; k < CPT; ++k)
+    if (OWN(k)) {
+      const int i = base + threadIdx.x + k * FCG_TPB;
+      const double xi = s_x[threadIdx.x + k * FCG_TPB];
+      a.xs[i] = xi;
+      a.x[__ldg(&a.perm[i])] = xi;
+    }
+  if (!grid_barrier(a.bar, gen, a.status)) return;
+#pragma unroll
+  for (int k = 0; k < CPT; ++k)
+    if (OWN(k)) {
+      const int i = base + threadIdx.x + k * FCG_TPB;
+      const double d = a.b[__ldg(&a.perm[i])] - fcg_row<WT>(a, WA, i, a.xs);
+      v1[0] += d * d;
+    }
+  if (!grid_reduce_gather<1, 0>(v1, a.partials, a.bar, gen, a.status, t1, s_gat)) return;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    a.dout[0] = sqrt(t1[0]);
+    a.dout[1] = dp;
+    a.dout[2] = sn;
+    a.status[0] = reason;
+    a.status[1] = its;
+  }
+#undef OWN
+}
+
+inline void* fcg_kernel_for(int C, int width, int* cpt_out) {
+  const int cpt = (C + FCG_TPB - 1) / FCG_TPB;
+  *cpt_out = cpt;
+  if (width == 7) {
+    switch (cpt) {
+      case 1: return (void*)k_fcg<1, 7>;
+      case 2: return (void*)k_fcg<2, 7>;
+      case 3: return (void*)k_fcg<3, 7>;
+      case 4: return (void*)k_fcg<4, 7>;
+      default: return nullptr;
+    }
+  }
+  switch (cpt) {
+    case 1: return (void*)k_fcg<1, 0>;
+    case 2: return (void*)k_fcg<2, 0>;
+    case 3: return (void*)k_fcg<3, 0>;
+    case 4: return (void*)k_fcg<4, 0>;
+    default: return nullptr;
+  }
+}
+
+}  // namespace gpu
+}  // namespace dpm

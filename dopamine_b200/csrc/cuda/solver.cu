@@ -20,7 +20,9 @@
 #include "../../../include/dopamine_b200.h"
 #include "../host/mesh.hpp"
 #include "../host/ops.hpp"
+#include "../host/twolevel.hpp"
 #include "common.cuh"
+#include "fcg.cuh"
 #include "kernels.cuh"
 #include "pcg.cuh"
 
@@ -132,14 +134,20 @@ __global__ void __launch_bounds__(TPB) k_reduce_partial(RedArgs r, double* parti
   }
 }
 
-__global__ void k_reduce_final(int mode, int nparts, const double* partials, double* out) {
-  int k = threadIdx.x;
+// One warp per component: lane l folds partials l, l+32, ... in order, then a fixed shuffle tree,
+// so the result does not depend on scheduling.
+__global__ void __launch_bounds__(32 * RED_NV) k_reduce_final(int mode, int nparts, const double* partials, double* out) {
+  const int k = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (k >= RED_NV) return;
   bool mx = (mode == RED_MAXABS && k == 0) || (mode == RED_MAX2 && k < 2) || (mode == RED_STATS && k == 7) ||
             (mode == RED_DIVSTAT && k == 0);
-  double t = mx ? 0.0 : 0.0;
-  for (int j = 0; j < nparts; ++j) t = mx ? fmax(t, partials[j * RED_NV + k]) : t + partials[j * RED_NV + k];
-  out[k] = t;
+  double t = 0.0;
+  for (int j = lane; j < nparts; j += 32) t = mx ? fmax(t, partials[j * RED_NV + k]) : t + partials[j * RED_NV + k];
+  for (int o = 16; o > 0; o >>= 1) {
+    double u = __shfl_down_sync(0xffffffffu, t, o);
+    t = mx ? fmax(t, u) : t + u;
+  }
+  if (lane == 0) out[k] = t;
 }
 
 // anchor_pressure_to_outlet (mod_fv_solver.f90:3610-3641): shift = sum(p V) / V_total.
@@ -169,6 +177,12 @@ struct Solver {
   int* cg_status;
   int cg_grid = 0;
   bool cg_coop = true;
+  // two-level flexible CG (p_solver == DPM_PSOLVER_TWOLEVEL_FCG)
+  bool use_fcg = false;
+  FcgArgs fa{};
+  int fcg_WA = 0;
+  void* fcg_kernel = nullptr;
+  size_t fcg_smem = 0;
   // state
   double time = 0.0;
   int64_t step = 0;
@@ -339,6 +353,12 @@ struct Solver {
       }
     }
     cg_part = mem.alloc<double>(8 * (size_t)cg_grid);
+    if (P.p_solver == DPM_PSOLVER_TWOLEVEL_FCG) {
+      int rc = setup_fcg(dev_sms);
+      if (rc) return rc;
+    } else if (P.p_solver != DPM_PSOLVER_JACOBI_PCG) {
+      return DPM_ERR_ARG;
+    }
     // initial fields: T = T_ref, velocity from an inlet patch (initialize_velocity_from_bc)
     launch_fill(F.T, nc, P.T_ref);
     double u0[3] = {0, 0, 0};
@@ -392,7 +412,7 @@ struct Solver {
     int g = std::min(nblk(r.n), 2048);
     if (g < 1) g = 1;
     k_reduce_partial<<<g, TPB, 0, st>>>(r, red_part);
-    k_reduce_final<<<1, 32, 0, st>>>(r.mode, g, red_part, red_out);
+    k_reduce_final<<<1, 32 * RED_NV, 0, st>>>(r.mode, g, red_part, red_out);
     launches += 2;
     if (host_out) {
       CK(cudaMemcpyAsync(host_out, red_out, nv * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -497,9 +517,75 @@ struct Solver {
     launches++;
   }
 
+  // Two-level FCG set-up: one part per SM (the kernel needs one co-resident block per part and
+  // its part's local operator in shared memory).
+  int setup_fcg(int dev_sms) {
+    TwoLevel T;
+    const bool nullsp = S.dir_rows.empty();
+    int rc = build_two_level(nc, S.WA, S.A_col.data(), S.A_val.data(), m.centroid.data(), dev_sms, nullsp, T);
+    if (rc) return DPM_ERR_UNSUPPORTED;
+    int cpt = 0;
+    fcg_kernel = fcg_kernel_for(T.C, T.WA, &cpt);
+    fcg_smem = fcg_smem_bytes(T.P, T.C, T.WL);
+    if (!fcg_kernel || fcg_smem > 200 * 1024) return DPM_ERR_UNSUPPORTED;
+    CK(cudaFuncSetAttribute(fcg_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fcg_smem));
+    int per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fcg_kernel, FCG_TPB, fcg_smem));
+    if (per_sm < 1 || T.P > dev_sms * per_sm) return DPM_ERR_UNSUPPORTED;
+    fa = FcgArgs{};
+    fa.n = nc; fa.P = T.P; fa.C = T.C; fa.WL = T.WL;
+    fa.perm = mem.upload(T.perm);
+    fa.col = mem.upload(T.col);
+    fa.val = mem.upload(T.val);
+    fa.dinv = mem.upload(T.dinv);
+    fa.lpk = mem.upload(T.lpk);
+    fa.einv = mem.upload(T.einv);
+    fa.xs = mem.alloc<double>(nc);
+    fa.zs = mem.alloc<double>(nc);
+    fa.partials = mem.alloc<double>((size_t)2 * FCG_SLOT * T.P);
+    fa.bar = cg_bar; fa.status = cg_status; fa.dout = cg_dout;
+    fa.nullsp = nullsp ? 1 : 0;
+    fa.degree = P.p_smooth_degree > 0 ? P.p_smooth_degree : 6;
+    const double lmin = P.p_smooth_lmin > 0.0 ? P.p_smooth_lmin : 0.05;
+    const double lmax = P.p_smooth_lmax > 0.0 ? P.p_smooth_lmax : 2.0;
+    if (!(lmax > lmin)) return DPM_ERR_ARG;
+    fa.theta = (float)(0.5 * (lmax + lmin));
+    fa.delta = (float)(0.5 * (lmax - lmin));
+    fcg_WA = T.WA;
+    if (!fa.partials || !fa.zs) return DPM_ERR_CUDA;
+    use_fcg = true;
+    return 0;
+  }
+
+  int fcg(const double* rhs, double* x, double rtol, double atol, int maxit, int guess_zero, int* its, double* resid,
+          int* reason) {
+    FcgArgs a = fa;
+    a.b = rhs; a.x = x; a.rtol = rtol; a.atol = atol; a.maxit = maxit; a.guess_zero = guess_zero;
+    CK(cudaMemsetAsync(cg_bar, 0, 2 * sizeof(unsigned), st));
+    CK(cudaMemsetAsync(cg_status, 0, 4 * sizeof(int), st));
+    int wa = fcg_WA;
+    void* args[] = {&a, &wa};
+    CK(cudaLaunchCooperativeKernel(fcg_kernel, dim3(a.P), dim3(FCG_TPB), args, fcg_smem, st));
+    launches++;
+    int h_st[4];
+    double h_d[4];
+    CK(cudaMemcpyAsync(h_st, cg_status, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(h_d, cg_dout, 4 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (h_st[2]) {
+      std::fprintf(stderr, "dopamine_b200: FCG grid barrier timed out\n");
+      return DPM_ERR_CUDA;
+    }
+    *reason = h_st[0];
+    *its = h_st[1];
+    *resid = h_d[0];
+    return 0;
+  }
+
   // ---------------------------------------------------------------- Poisson solve
   int pcg(const double* rhs, double* x, double rtol, double atol, int maxit, int guess_zero, int* its, double* resid,
           int* reason) {
+    if (use_fcg) return fcg(rhs, x, rtol, atol, maxit, guess_zero, its, resid, reason);
     PcgArgs<double> a{};
     a.n = nc; a.WA = S.WA; a.col = d.Acol; a.val = d.Aval; a.dinv = d.Adinv;
     a.b = rhs; a.x = x; a.r = cg_r; a.z = cg_z; a.p0 = cg_p0; a.p1 = cg_p1; a.q = cg_q; a.bp = cg_bp;

@@ -60,6 +60,8 @@ extern "C" {
 #define DPM_WM_NONE 1
 
 /* Pressure-solve forms. */
+#define DPM_PSOLVER_JACOBI_PCG 0
+#define DPM_PSOLVER_TWOLEVEL_FCG 1
 #define DPM_FORM_FP64 0     /* plain: FP64 Jacobi-PCG                                    */
 #define DPM_FORM_MIXED 1    /* FP32 inner PCG inside FP64 defect correction              */
 
@@ -118,6 +120,14 @@ typedef struct dpm_params {
   int amd_wall_gradient;
   double wall_model_height, wall_model_filter_time, wall_model_filter_tf_fac;
   int form;                   /* DPM_FORM_*                                                  */
+  /* Pressure solver (no counterpart in the reference's namelists, which select PETSc options):
+   * DPM_PSOLVER_JACOBI_PCG mirrors `-pc_type jacobi`; DPM_PSOLVER_TWOLEVEL_FCG is flexible CG
+   * with a part-local Chebyshev smoother of degree p_smooth_degree on the interval
+   * [p_smooth_lmin, p_smooth_lmax] of D^-1 A plus a one-value-per-part coarse correction.
+   * Zero / non-positive smoother settings select the defaults (6, 0.05, 2.0). */
+  int p_solver;
+  int p_smooth_degree;
+  double p_smooth_lmin, p_smooth_lmax;
 } dpm_params_t;
 
 /* Per-step integral statistics (src/stats/mod_stats.f90:compute_stats_sums and

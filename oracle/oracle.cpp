@@ -152,6 +152,11 @@ struct Solver {
   std::vector<int64_t> A_off;
   std::vector<int> A_col;
   std::vector<double> A_val;
+  // optional record of the pressure systems solved (right-hand side, initial guess, atol), for
+  // tests that study the solver on the systems the time step produces
+  bool record = false;
+  std::vector<std::vector<double>> rec_rhs, rec_x0;
+  std::vector<double> rec_atol;
 
   // non-orthogonal caches (mod_fv_solver.f90:detect_nonortho_skip, build_nonortho_cache)
   bool skip_nonortho = false, skip_grad_p = false;
@@ -1529,6 +1534,11 @@ struct Solver {
     int maxit = std::max(P.p_max_iter, 2000);
     int its;
     double res;
+    if (record) {
+      rec_rhs.push_back(rw);
+      rec_x0.push_back(pw);
+      rec_atol.push_back(atol);
+    }
     int reason = cg(rw.data(), pw.data(), tol, atol, maxit, false, &its, &res);
     if (reason < 0) {
       reason = cg(rw.data(), pw.data(), tol, atol, 4 * maxit, true, &its, &res);
@@ -1891,4 +1901,29 @@ int orc_poisson_solve(void* h, const double* rhs, double* x, double rtol, double
   return s->cg(rhs, x, rtol, atol, maxit, false, its, res);
 }
 void orc_poisson_matvec(void* h, const double* x, double* y) { static_cast<orc::Solver*>(h)->matvec(x, y); }
+// Poisson operator as CSR (nnz first with null arrays, then filled).
+int64_t orc_poisson_csr(void* h, int64_t* off, int* col, double* val) {
+  auto* s = static_cast<orc::Solver*>(h);
+  if (off) std::memcpy(off, s->A_off.data(), sizeof(int64_t) * s->A_off.size());
+  if (col) std::memcpy(col, s->A_col.data(), sizeof(int) * s->A_col.size());
+  if (val) std::memcpy(val, s->A_val.data(), sizeof(double) * s->A_val.size());
+  return (int64_t)s->A_col.size();
+}
+void orc_record_poisson(void* h, int on) {
+  auto* s = static_cast<orc::Solver*>(h);
+  s->record = on != 0;
+  s->rec_rhs.clear();
+  s->rec_x0.clear();
+  s->rec_atol.clear();
+}
+// k-th recorded system; returns the number recorded.
+int orc_recorded_poisson(void* h, int k, double* rhs, double* x0, double* atol) {
+  auto* s = static_cast<orc::Solver*>(h);
+  if (k >= 0 && k < (int)s->rec_rhs.size()) {
+    std::memcpy(rhs, s->rec_rhs[k].data(), sizeof(double) * s->nc);
+    std::memcpy(x0, s->rec_x0[k].data(), sizeof(double) * s->nc);
+    *atol = s->rec_atol[k];
+  }
+  return (int)s->rec_rhs.size();
+}
 }

@@ -55,6 +55,11 @@ def lib():
         L.orc_poisson_solve.argtypes = [vp, dp, dp, C.c_double, C.c_double, C.c_int, ip, dp]
         L.orc_poisson_solve.restype = C.c_int
         L.orc_poisson_matvec.argtypes = [vp, dp, dp]
+        L.orc_poisson_csr.argtypes = [vp, C.POINTER(C.c_int64), ip, dp]
+        L.orc_poisson_csr.restype = C.c_int64
+        L.orc_record_poisson.argtypes = [vp, C.c_int]
+        L.orc_recorded_poisson.argtypes = [vp, C.c_int, dp, dp, dp]
+        L.orc_recorded_poisson.restype = C.c_int
         _lib = L
     return _lib
 
@@ -116,6 +121,31 @@ class Oracle:
         s = abi.StatsT()
         lib().orc_stats(self.h, C.byref(s))
         return s.as_dict()
+
+    def poisson_csr(self):
+        """The assembled pressure operator as (offsets, columns, values)."""
+        L = lib()
+        nnz = L.orc_poisson_csr(self.h, None, None, None)
+        off = np.zeros(self.nc + 1, dtype=np.int64)
+        col = np.zeros(nnz, dtype=np.int32)
+        val = np.zeros(nnz)
+        L.orc_poisson_csr(self.h, off.ctypes.data_as(C.POINTER(C.c_int64)), col.ctypes.data_as(C.POINTER(C.c_int)),
+                          _p(val))
+        return off, col, val
+
+    def record_poisson(self, on=True):
+        lib().orc_record_poisson(self.h, 1 if on else 0)
+
+    def recorded_poisson(self):
+        """[(rhs, initial guess, atol)] of the pressure solves since record_poisson(True)."""
+        L = lib()
+        out = []
+        n = L.orc_recorded_poisson(self.h, -1, None, None, None)
+        for k in range(n):
+            b, x0, at = np.zeros(self.nc), np.zeros(self.nc), C.c_double()
+            L.orc_recorded_poisson(self.h, k, _p(b), _p(x0), C.byref(at))
+            out.append((b, x0, at.value))
+        return out
 
     @staticmethod
     def _check(rc):
