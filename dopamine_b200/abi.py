@@ -108,9 +108,9 @@ def default_params(**kw):
     p.p_smooth_lmin = 0.05
     p.p_smooth_lmax = 2.0
     for k, v in kw.items():
-        if k in ("f_const", "g"):
+        if k in ("f_const", "g", "scalar_diffusivity", "scalar_pr_t"):
             arr = getattr(p, k)
-            for i in range(3):
+            for i in range(len(v)):
                 arr[i] = v[i]
         else:
             setattr(p, k, v)
@@ -127,6 +127,10 @@ def patch_cfgs(patches):
             arr[i].U_val[k] = v
         arr[i].p_val = pd.get("p", 0.0)
         arr[i].T_val = pd.get("T", 0.0)
+        for k, v in enumerate(pd.get("scalar_mode", (0, 0, 0, 0))):
+            arr[i].scalar_mode[k] = v
+        for k, v in enumerate(pd.get("scalar_value", (0.0, 0.0, 0.0, 0.0))):
+            arr[i].scalar_value[k] = v
     return arr
 
 

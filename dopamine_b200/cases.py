@@ -118,6 +118,37 @@ def channel_box(nx, ny, nz, lx, ly, lz, stretch):
     return structured_box(X, Y, Z, names=("x0", "xL", "bottom_wall", "top_wall", "z0", "zL"))
 
 
+def bump_nodes(n, coef):
+    """Node positions in [0, 1] of a transfinite line of n cells "Using Bump coef" (gmsh): the
+    local cell size varies quadratically along the line, the end cells being `coef` times the
+    middle one.  Positions are the closed-form inverse of the cumulative point density
+    1 / (1 + 4 (coef - 1) x^2), x in [-1/2, 1/2], sampled at equal increments."""
+    u = 2.0 * np.arange(n + 1) / n - 1.0
+    if abs(coef - 1.0) < 1e-14:
+        x = 0.5 * u
+    elif coef < 1.0:
+        q = math.sqrt(1.0 - coef)
+        x = np.tanh(u * math.atanh(q)) / (2.0 * q)
+    else:
+        q = math.sqrt(coef - 1.0)
+        x = np.tan(u * math.atan(q)) / (2.0 * q)
+    x = 0.5 + x
+    x[0], x[-1] = 0.0, 1.0
+    return x
+
+
+def wall_box(nx, ny, nz, lx, ly, lz, bump_z):
+    """Box of examples/RayleighBernard/RB.geo: x, y periodic, walls at z = 0 and z = lz, uniform
+    in x and y, "Bump" grading bump_z in z.  Patches in the reference's order."""
+    x = np.arange(nx + 1) * (lx / nx)
+    y = np.arange(ny + 1) * (ly / ny)
+    z = lz * bump_nodes(nz, bump_z)
+    X, Y, Z = np.meshgrid(x, y, z, indexing="ij")
+    m = structured_box(X, Y, Z, names=("periodic_x0", "periodic_xL", "periodic_y0", "periodic_yL",
+                                       "bottom_wall", "top_wall"))
+    return m
+
+
 # ------------------------------------------------------------------------------------------
 # Initial conditions (src/init/mod_initconditions.f90)
 # ------------------------------------------------------------------------------------------
@@ -247,10 +278,36 @@ def regression_case(name):
                     dict(scheme=abi.SCHEME_CDS, nu=1.0e-2, dt=2.0e-3, cfl_max=0.5, p_tol=1e-12,
                          n_nonortho_corr=4, rhie_chow_dual=0, f_const=(0.0, 0.0, -1.0)),
                     "uniform", 0.0, n_steps=20, stats_every=10)
+    if name == "rb":
+        # 24x24x16 Rayleigh-Benard: fixed-temperature walls T=1 (bottom) / 0 (top), Boussinesq
+        patches = [{"bc": "periodic"}] * 4 + [{"bc": "fixedTemp", "T": 1.0}, {"bc": "fixedTemp", "T": 0.0}]
+        return Case(name, wall_box(24, 24, 16, 2.0, 2.0, 1.0, 0.25), patches,
+                    dict(scheme=abi.SCHEME_KEP, temperature_scheme=abi.SCHEME_VANLEER_TVD, nu=6.3246e-4,
+                         alpha_T=6.3246e-4, beta=1.0, T_ref=0.5, g=(0.0, 0.0, -1.0), boussinesq=1, dt=5.0e-2,
+                         cfl_max=0.5, p_tol=1e-10, p_max_iter=500, rhie_chow_dual=0, sgs_model=abi.SGS_NONE,
+                         wall_model=abi.WM_NONE),
+                    "uniform", 1.0e-2, n_steps=20)
+    if name in ("channel", "amd", "graded"):
+        # 32x16x16 wall-bounded box 2pi x 2pi x 1 with a Taylor-Green field, KEP, log-law wall
+        # model, f_x = 1, one passive tracer with a Dirichlet value 1 on the bottom wall
+        L = 6.283185307179586
+        bump = 0.01 if name == "graded" else 0.25
+        wall = {"bc": "wallModel"}
+        patches = [{"bc": "periodic"}] * 4 + [dict(wall, scalar_mode=(1, 0, 0, 0), scalar_value=(1.0, 0, 0, 0)),
+                                              dict(wall)]
+        prm = dict(scheme=abi.SCHEME_KEP, sgs_model=abi.SGS_AMD if name == "amd" else abi.SGS_VREMAN,
+                   wall_model=abi.WM_LOGLAW, nu=2.5316e-3, f_const=(1.0, 0.0, 0.0), dt=2.0e-3, cfl_max=0.5,
+                   p_tol=1e-10, p_max_iter=1000, rhie_chow_dual=0, n_scalars=1,
+                   scalar_scheme=abi.SCHEME_VANLEER_TVD, scalar_diffusivity=(1.0e-3, 0, 0, 0),
+                   scalar_pr_t=(1.0, 0, 0, 0))
+        if name == "amd":
+            prm["wall_model_filter_tf_fac"] = 1.0
+        return Case(name, wall_box(32, 16, 16, L, L, 1.0, bump), patches, prm, "taylor_green", 1.0, n_steps=20)
     raise KeyError(name)
 
 
-REGRESSION_CASES = ("tgv", "tgv_skew", "tgv_skew_chk", "pdrop", "hydro", "hydrowall")
+REGRESSION_CASES = ("tgv", "tgv_skew", "tgv_skew_chk", "pdrop", "hydro", "hydrowall", "rb", "channel", "amd",
+                    "graded")
 
 
 def tgv_config(n=32, n_steps=200, scheme=abi.SCHEME_CDS):

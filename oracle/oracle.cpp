@@ -128,6 +128,10 @@ struct Solver {
 
   // primary fields (AoS, Fortran layout)
   std::vector<double> U, p, p_old, T, nu_sgs, U_bnd, p_bnd, phi_prev, phi_prev_bnd, tau_w;
+  // temperature and passive scalars (scalar-major [s][nc] / [s][nb] / [s][nc][3])
+  std::vector<double> T_bnd, grad_T, H_T, H_T0, conv_T, visc_T;
+  int ns = 0;
+  std::vector<double> Cs, C_bnd, grad_C, H_C, H_C0, conv_C, visc_C;
   std::vector<double> grad_U, face_flux, U_face, inv_vol;
   std::vector<double> H_U, H_U0, rhs_p, conv_U, visc_U, gp, gp_rc, gp_cell, p_tot, p_tot_bnd, phi_it, Tinv;
   std::vector<uint8_t> built;
@@ -194,6 +198,18 @@ struct Solver {
     nu_sgs.assign(nc, 0.0); U_bnd.assign(3 * nb, 0.0); p_bnd.assign(nb, 0.0);
     phi_prev.assign(nc, 0.0); phi_prev_bnd.assign(nb, 0.0); tau_w.assign(3 * nb, 0.0);
     grad_U.assign(9 * nc, 0.0); face_flux.assign(nf, 0.0); U_face.assign(nf, 0.0);
+    T_bnd.assign(nb, P.T_ref); grad_T.assign(3 * nc, 0.0); H_T.assign(nc, 0.0); H_T0.assign(nc, 0.0);
+    conv_T.assign(nc, 0.0); visc_T.assign(nc, 0.0);
+    ns = std::max(0, std::min(P.n_scalars, 4));
+    Cs.assign((size_t)ns * nc, 0.0); C_bnd.assign((size_t)ns * nb, 0.0); grad_C.assign((size_t)ns * 3 * nc, 0.0);
+    H_C.assign((size_t)ns * nc, 0.0); H_C0.assign((size_t)ns * nc, 0.0); conv_C.assign(nc, 0.0); visc_C.assign(nc, 0.0);
+    auto scalar_ok = [](int sch) {
+      return sch == DPM_SCHEME_CDS || sch == DPM_SCHEME_QUICK || sch == DPM_SCHEME_VANLEER_TVD || sch == DPM_SCHEME_KOREN_TVD;
+    };
+    if ((P.boussinesq && !scalar_ok(P.temperature_scheme)) || (ns > 0 && !scalar_ok(P.scalar_scheme))) {
+      if (err) *err = "scalar advection scheme must be CDS, QUICK, VANLEER_TVD or KOREN_TVD";
+      return DPM_ERR_UNSUPPORTED;
+    }
     inv_vol.resize(nc);
     for (int64_t c = 0; c < nc; ++c) inv_vol[c] = 1.0 / std::max(m.volume[c], SMALL);
     H_U.assign(3 * nc, 0.0); H_U0.assign(3 * nc, 0.0); rhs_p.assign(nc, 0.0);
@@ -211,6 +227,8 @@ struct Solver {
       if (pc[q].bc_id == BC_OUTLET) n_outlet += m.patch_nfaces[q];
     apply_velocity_bc(-1, false);
     apply_pressure_bc(p.data(), -1, false, false);
+    apply_temperature_bc(-1);
+    for (int sc = 0; sc < ns; ++sc) apply_scalar_bc(sc, -1);
     // initialize_velocity_from_bc
     double u0[3] = {0, 0, 0};
     for (int q = 0; q < m.n_patches; ++q)
@@ -573,11 +591,80 @@ struct Solver {
     }
   }
 
-  void refresh_halos_and_bc() {  // src/solver/mod_fv_solver.f90:985-1001
+  void refresh_halos_and_bc() {  // src/solver/mod_fv_solver.f90:985-1001, 2024-2059
     apply_velocity_bc(0, true);
     apply_pressure_bc(p.data(), 0, !skip_grad_p, false);
+    apply_temperature_bc(0);
+    for (int sc = 0; sc < ns; ++sc) apply_scalar_bc(sc, 0);
     apply_velocity_bc(1, true);
     apply_pressure_bc(p.data(), 1, !skip_grad_p, false);
+    apply_temperature_bc(1);
+    for (int sc = 0; sc < ns; ++sc) apply_scalar_bc(sc, 1);
+  }
+
+  // src/bc/mod_bc.f90:489-588 (apply_temperature_bc; every caller passes grad_T, so the default
+  // branch always extrapolates with it).  The ABL-inlet profile is not part of this path.
+  void apply_temperature_bc(int filt) {
+    for (int64_t fb = 0; fb < nb; ++fb) {
+      int64_t fg = nfi + fb;
+      int bc = bc_of_face(fg);
+      if (filt == 1 && bc != BC_PERIODIC) continue;
+      if (filt == 0 && bc == BC_PERIODIC) continue;
+      int o = m.owner[fg];
+      switch (bc) {
+        case BC_INLET:
+        case BC_FIXEDTEMP:
+          T_bnd[fb] = pc[m.patch[fg]].T_val;
+          break;
+        case BC_PERIODIC: {
+          int pnb = m.periodic_partner_cell(fb);
+          if (pnb >= 0 && pnb != o) T_bnd[fb] = m.periodic_gc[fb] * T[o] + (1.0 - m.periodic_gc[fb]) * T[pnb];
+          else T_bnd[fb] = T[o];
+          break;
+        }
+        default: {
+          double d[3];
+          for (int k = 0; k < 3; ++k) d[k] = m.centre[3 * fg + k] - m.centroid[3 * o + k];
+          T_bnd[fb] = T[o] + grad_T[3 * o] * d[0] + grad_T[3 * o + 1] * d[1] + grad_T[3 * o + 2] * d[2];
+        }
+      }
+    }
+  }
+
+  // src/bc/mod_bc.f90:591-680 (apply_passive_scalar_bc; modes 0 zero gradient, 1 Dirichlet,
+  // 2 Neumann with a constant flux per area; the face diffusivity uses the global Pr_t, as the
+  // reference's callers pass it, mod_fv_solver.f90:2049-2056)
+  void apply_scalar_bc(int sc, int filt) {
+    const double* C = &Cs[(size_t)sc * nc];
+    double* Cb = &C_bnd[(size_t)sc * nb];
+    for (int64_t fb = 0; fb < nb; ++fb) {
+      int64_t fg = nfi + fb;
+      int bc = bc_of_face(fg);
+      if (filt == 1 && bc != BC_PERIODIC) continue;
+      if (filt == 0 && bc == BC_PERIODIC) continue;
+      int o = m.owner[fg];
+      if (bc == BC_PERIODIC) {
+        int pnb = m.periodic_partner_cell(fb);
+        if (pnb >= 0 && pnb != o) Cb[fb] = m.periodic_gc[fb] * C[o] + (1.0 - m.periodic_gc[fb]) * C[pnb];
+        else Cb[fb] = C[o];
+        continue;
+      }
+      const int q = m.patch[fg];
+      const int mode = q >= 0 ? pc[q].scalar_mode[sc] : 0;
+      if (mode == 1) {
+        Cb[fb] = pc[q].scalar_value[sc];
+      } else if (mode == 2) {
+        double alpha = P.scalar_diffusivity[sc] + nu_sgs[o] / P.Pr_t;
+        double d = std::max(m.d_cf[fg], SMALL);
+        Cb[fb] = alpha > SMALL ? C[o] + pc[q].scalar_value[sc] * d / alpha : C[o];
+      } else {
+        Cb[fb] = C[o];
+      }
+    }
+  }
+  void apply_scalar_bcs_all() {  // apply_scalar_bc (mod_fv_solver.f90:2005-2022), after each step
+    apply_temperature_bc(-1);
+    for (int sc = 0; sc < ns; ++sc) apply_scalar_bc(sc, -1);
   }
   void velocity_bc_refresh() {  // the apply_velocity_bc pair after each U update
     apply_velocity_bc(0, true);
@@ -633,7 +720,13 @@ struct Solver {
       for (int i = 0; i < 3; ++i) g[3 * c + i] = acc[i];
     }
   }
-  void compute_all_gradients() { ls_gradient_vector(U.data(), U_bnd.data(), grad_U.data()); }
+  // src/solver/mod_fv_solver.f90:1003-1077 (least-squares branch)
+  void compute_all_gradients() {
+    ls_gradient_vector(U.data(), U_bnd.data(), grad_U.data());
+    if (P.boussinesq) ls_gradient_scalar(T.data(), T_bnd.data(), grad_T.data());
+    for (int sc = 0; sc < ns; ++sc)
+      ls_gradient_scalar(&Cs[(size_t)sc * nc], &C_bnd[(size_t)sc * nb], &grad_C[(size_t)sc * 3 * nc]);
+  }
   void compute_pressure_gradient() {
     if (skip_grad_p) return;
     ls_gradient_scalar(p.data(), p_bnd.data(), gp.data());
@@ -978,14 +1071,16 @@ struct Solver {
     return std::min(std::max(x, l), h);
   }
 
-  // mod_advection.f90:2632-2722 (3-component QUICK fit on the upwind cell's neighbours)
-  void quick3(const Ctx& c, double* phi_f) const {
+  // mod_advection.f90:2632-2722: QUICK fit on the upwind cell's neighbours, K components at once
+  // (phi_at(cell, k), grad_at(cell, k, i) give the field and its cell gradient).
+  template <int K, class PhiAt, class GradAt>
+  void quick_fit(const Ctx& c, PhiAt phi_at, GradAt grad_at, double* phi_f) const {
     bool have_grad = c.up < nc && c.down < nc;
-    double phU[3], phD[3], gup[3][3];
-    for (int k = 0; k < 3; ++k) {
-      phU[k] = U[3 * c.up + k];
-      phD[k] = U[3 * c.down + k];
-      for (int i = 0; i < 3; ++i) gup[k][i] = have_grad ? grad_U[9 * c.up + 3 * k + i] : 0.0;
+    double phU[K], phD[K], gup[K][3];
+    for (int k = 0; k < K; ++k) {
+      phU[k] = phi_at(c.up, k);
+      phD[k] = phi_at(c.down, k);
+      for (int i = 0; i < 3; ++i) gup[k][i] = have_grad ? grad_at(c.up, k, i) : 0.0;
     }
     auto axial = [&](double far, double up, const double* g, const double* dv, double s) {
       double t[3];
@@ -998,8 +1093,8 @@ struct Solver {
     double w = 1.0 / dist2;
     double a11 = w * c.s_down * c.s_down, a12 = a11 * c.s_down, a22 = a12 * c.s_down, lin_den = a11;
     int nfit = 1;
-    double b1[3], b2[3], ln[3];
-    for (int k = 0; k < 3; ++k) {
+    double b1[K], b2[K], ln[K];
+    for (int k = 0; k < K; ++k) {
       double dp = axial(phD[k], phU[k], gup[k], dv, c.s_down);
       b1[k] = w * c.s_down * dp;
       b2[k] = w * c.s_down * c.s_down * dp;
@@ -1020,15 +1115,15 @@ struct Solver {
         double al = std::min(1.0, -s / std::sqrt(d2));
         double wt = (0.25 + al * al) / d2;
         a11 += wt * s * s; a12 += wt * s * s * s; a22 += wt * s * s * s * s; lin_den += wt * s * s;
-        for (int k = 0; k < 3; ++k) {
-          double dp = axial(U[3 * n + k], phU[k], gup[k], d, s);
+        for (int k = 0; k < K; ++k) {
+          double dp = axial(phi_at(n, k), phU[k], gup[k], d, s);
           b1[k] += wt * s * dp; b2[k] += wt * s * s * dp; ln[k] += wt * s * dp;
         }
         nfit++;
       }
     }
     double det = a11 * a22 - a12 * a12;
-    for (int k = 0; k < 3; ++k) {
+    for (int k = 0; k < K; ++k) {
       double a1, a2;
       if (nfit >= 2 && std::fabs(det) > SMALL) {
         a1 = (b1[k] * a22 - b2[k] * a12) / det;
@@ -1041,6 +1136,10 @@ struct Solver {
       double v = phU[k] + a1 * c.s_face + a2 * c.s_face * c.s_face;
       phi_f[k] = clampv(v, std::min(phU[k], phD[k]), std::max(phU[k], phD[k]));
     }
+  }
+  void quick3(const Ctx& c, double* phi_f) const {
+    quick_fit<3>(c, [&](int cell, int k) { return U[3 * (int64_t)cell + k]; },
+                 [&](int cell, int k, int i) { return grad_U[9 * (int64_t)cell + 3 * k + i]; }, phi_f);
   }
 
   // mod_advection.f90:2725-2791
@@ -1186,6 +1285,126 @@ struct Solver {
     }
   }
 
+  // advection_rhs_scalar_cds_soa / _recon_soa (src/numerics/mod_advection.f90:267-675): face flux
+  // is the projected U_face on every non-wall face, zero on walls.
+  void advection_scalar(int scheme, const double* phi, const double* phib, const double* gphi, double* rhs) {
+    std::fill(rhs, rhs + nc, 0.0);
+    for (int64_t f = 0; f < nf; ++f) {
+      int o = m.owner[f], n = m.neighbour[f];
+      int64_t fb = f >= nfi ? f - nfi : 0;
+      int bc = n >= 0 ? -1 : bc_of_face(f);
+      double Fn = (n < 0 && is_wall(bc)) ? 0.0 : U_face[f];
+      double phf;
+      if (scheme == DPM_SCHEME_CDS) {
+        int npr = -1;
+        bool has_rec = n >= 0;
+        if (!has_rec && bc == BC_PERIODIC) {
+          npr = periodic_nb(fb, o);
+          has_rec = npr >= 0;
+        }
+        if (has_rec) {
+          int ns_ = n >= 0 ? n : npr;
+          double gcv = f >= nfi ? m.periodic_gc[fb] : m.gc[f];
+          double plain = gcv * phi[o] + (1.0 - gcv) * phi[ns_];
+          if (f < nfi) {
+            double gm[3];
+            for (int i = 0; i < 3; ++i) gm[i] = gcv * gphi[3 * o + i] + (1.0 - gcv) * gphi[3 * (int64_t)ns_ + i];
+            double ph = plain + dot3(gm, &m.eps[3 * f]);
+            double wb = refine_blend_weight(m.skew[f]);
+            if (wb < 1.0) ph = plain + wb * (ph - plain);
+            phf = ph;
+          } else {
+            phf = plain;
+          }
+          if (!finite(phf)) phf = (Fn >= 0.0 || n < 0) ? phi[o] : phi[n];
+        } else {
+          phf = phib[fb];
+        }
+      } else {
+        Ctx c;
+        bool ok = recon_context(f, Fn, c);
+        if (ok) {
+          if (scheme == DPM_SCHEME_QUICK) {
+            quick_fit<1>(c, [&](int cell, int) { return phi[cell]; },
+                         [&](int cell, int, int i) { return gphi[3 * (int64_t)cell + i]; }, &phf);
+          } else {
+            phf = tvd(scheme, phi, 1, c, far_upwind(c));
+          }
+          if (!finite(phf)) phf = (Fn >= 0.0 || n < 0) ? phi[o] : phi[n];
+        } else {
+          phf = phib[fb];
+        }
+      }
+      if (!finite(Fn)) Fn = 0.0;
+      if (!finite(phf)) phf = 0.0;
+      rhs[o] -= Fn * phf * inv_vol[o];
+      if (n >= 0) rhs[n] += Fn * phf * inv_vol[n];
+    }
+  }
+
+  // src/numerics/mod_viscous.f90:286-507 (viscous_rhs_scalar): alpha_eff = alpha + nu_t / Pr_t,
+  // over-relaxed normal part with the clamped orthogonality weight, gc-mean gradient on the
+  // transverse part; every non-periodic boundary face by the Jasak split against phi_bnd.
+  void viscous_scalar(const double* phi, double alpha, double prt, const double* gphi, const double* phib,
+                      double* rhs) {
+    std::fill(rhs, rhs + nc, 0.0);
+    for (int64_t f = 0; f < nf; ++f) {
+      int o = m.owner[f], n = m.neighbour[f];
+      const double* sf = &m.sf[3 * f];
+      double flux = 0.0;
+      auto pair_flux = [&](int nbc, double gcv, double aeff, const double* d_on, double dlen) {
+        double sdd = dot3(sf, d_on) / dlen;
+        double dperp[3], gf[3];
+        for (int k = 0; k < 3; ++k) {
+          dperp[k] = sf[k] - (sdd / dlen) * d_on[k];
+          gf[k] = gcv * gphi[3 * o + k] + (1.0 - gcv) * gphi[3 * (int64_t)nbc + k];
+        }
+        double dphi = (phi[nbc] - phi[o]) * ortho_weight(sdd, m.area[f]) / dlen + dot3(gf, dperp);
+        return aeff * dphi;
+      };
+      auto bnd_flux = [&](int64_t fb) {
+        double aeff = alpha + nu_sgs[o] / prt;
+        double d[3];
+        for (int k = 0; k < 3; ++k) d[k] = m.centre[3 * f + k] - m.centroid[3 * o + k];
+        double dl = std::sqrt(dot3(d, d)) + SMALL;
+        double sdd = dot3(sf, d) / dl, dperp[3];
+        for (int k = 0; k < 3; ++k) dperp[k] = sf[k] - (sdd / dl) * d[k];
+        double dphi = (phib[fb] - phi[o]) * ortho_weight(sdd, m.area[f]) / dl + dot3(&gphi[3 * o], dperp);
+        return aeff * dphi;
+      };
+      if (n >= 0) {
+        double gcv = m.gc[f];
+        double aeff = alpha + (gcv * nu_sgs[o] + (1.0 - gcv) * nu_sgs[n]) / prt;
+        double d[3];
+        for (int k = 0; k < 3; ++k) d[k] = m.centroid[3 * n + k] - m.centroid[3 * o + k];
+        flux = pair_flux(n, gcv, aeff, d, std::sqrt(dot3(d, d)) + SMALL);
+      } else {
+        int64_t fb = f - nfi;
+        if (bc_of_face(f) == BC_PERIODIC) {
+          int npr = periodic_nb(fb, o);
+          int pb = m.periodic_pair[fb];
+          int64_t pf = pb >= 0 ? nfi + pb : -1;
+          if (npr >= 0) {
+            double dper, gcp;
+            if (pf >= 0) { dper = m.d_cf[f] + m.d_cf[pf]; gcp = m.d_cf[pf] / (dper + SMALL); }
+            else if (m.periodic_pair_dcf[fb] > SMALL) { dper = m.d_cf[f] + m.periodic_pair_dcf[fb]; gcp = m.periodic_pair_dcf[fb] / (dper + SMALL); }
+            else { dper = 2.0 * m.d_cf[f]; gcp = 0.5; }
+            double aeff = alpha + (gcp * nu_sgs[o] + (1.0 - gcp) * nu_sgs[npr]) / prt;
+            const double* nh = &m.normal[3 * f];
+            double d[3] = {dper * nh[0], dper * nh[1], dper * nh[2]};
+            flux = pair_flux(npr, gcp, aeff, d, dper + SMALL);
+          } else {
+            flux = bnd_flux(fb);
+          }
+        } else {
+          flux = bnd_flux(fb);
+        }
+      }
+      rhs[o] += flux * inv_vol[o];
+      if (n >= 0) rhs[n] -= flux * inv_vol[n];
+    }
+  }
+
   // src/solver/mod_fv_solver.f90:1617-1762 (momentum part)
   void explicit_rhs() {
     advection(conv_U.data());
@@ -1203,6 +1422,22 @@ struct Solver {
       int o = m.owner[fg];
       double w = m.area[fg] / m.volume[o];
       for (int k = 0; k < 3; ++k) H_U[3 * o + k] = H_U[3 * o + k] + tau_w[3 * fb + k] * w;
+    }
+    // temperature (solved when Boussinesq is on) and passive scalars
+    if (P.boussinesq) {
+      advection_scalar(P.temperature_scheme, T.data(), T_bnd.data(), grad_T.data(), conv_T.data());
+      viscous_scalar(T.data(), P.alpha_T, P.Pr_t, grad_T.data(), T_bnd.data(), visc_T.data());
+      for (int64_t c = 0; c < nc; ++c) H_T[c] = conv_T[c] + visc_T[c];
+    } else {
+      std::fill(H_T.begin(), H_T.end(), 0.0);
+    }
+    for (int sc = 0; sc < ns; ++sc) {
+      const double* C = &Cs[(size_t)sc * nc];
+      const double* Cb = &C_bnd[(size_t)sc * nb];
+      const double* gC = &grad_C[(size_t)sc * 3 * nc];
+      advection_scalar(P.scalar_scheme, C, Cb, gC, conv_C.data());
+      viscous_scalar(C, P.scalar_diffusivity[sc], P.scalar_pr_t[sc], gC, Cb, visc_C.data());
+      for (int64_t c = 0; c < nc; ++c) H_C[(size_t)sc * nc + c] = conv_C[c] + visc_C[c];
     }
   }
 
@@ -1648,6 +1883,10 @@ struct Solver {
     std::fill(H_U.begin(), H_U.end(), 0.0);
     std::fill(rhs_p.begin(), rhs_p.end(), 0.0);
     std::fill(H_U0.begin(), H_U0.end(), 0.0);
+    std::fill(H_T.begin(), H_T.end(), 0.0);
+    std::fill(H_T0.begin(), H_T0.end(), 0.0);
+    std::fill(H_C.begin(), H_C.end(), 0.0);
+    std::fill(H_C0.begin(), H_C0.end(), 0.0);
     double time_n = time;
     for (int k = 0; k < 3; ++k) {
       double gk_dt = RK3W_GAMMA[k] * dt;
@@ -1661,6 +1900,8 @@ struct Solver {
       double a_k = RK3W_ALPHA[k], b_k = RK3W_BETA[k];
       for (int64_t c = 0; c < nc; ++c)
         for (int j = 0; j < 3; ++j) U[3 * c + j] = U[3 * c + j] + dt * (a_k * H_U[3 * c + j] + b_k * H_U0[3 * c + j]);
+      for (int64_t c = 0; c < nc; ++c) T[c] = T[c] + dt * (a_k * H_T[c] + b_k * H_T0[c]);
+      for (size_t i = 0; i < Cs.size(); ++i) Cs[i] = Cs[i] + dt * (a_k * H_C[i] + b_k * H_C0[i]);
       velocity_bc_refresh();
       p_old = p;
       correct_velocity(gk_dt, false, true);
@@ -1724,7 +1965,10 @@ struct Solver {
       apply_pressure_bc(p.data(), 1, false, false);
       compute_pressure_gradient();
       H_U0 = H_U;
+      H_T0 = H_T;
+      H_C0 = H_C;
     }
+    apply_scalar_bcs_all();
     time = time_n + dt;
     step++;
     return 0;
@@ -1843,6 +2087,17 @@ void orc_get_state(void* h, double* U, double* p, double* nu_sgs, double* grad_U
   if (nu_sgs) std::memcpy(nu_sgs, s->nu_sgs.data(), sizeof(double) * s->nc);
   if (grad_U) std::memcpy(grad_U, s->grad_U.data(), sizeof(double) * 9 * s->nc);
   if (face_flux) std::memcpy(face_flux, s->U_face.data(), sizeof(double) * s->nf);
+}
+// Temperature [nc] and passive scalars [n_scalars][nc] (scalar-major), either may be NULL.
+void orc_get_scalars(void* h, double* T, double* C) {
+  auto* s = static_cast<orc::Solver*>(h);
+  if (T) std::memcpy(T, s->T.data(), sizeof(double) * s->nc);
+  if (C && !s->Cs.empty()) std::memcpy(C, s->Cs.data(), sizeof(double) * s->Cs.size());
+}
+void orc_set_scalars(void* h, const double* T, const double* C) {
+  auto* s = static_cast<orc::Solver*>(h);
+  if (T) std::memcpy(s->T.data(), T, sizeof(double) * s->nc);
+  if (C && !s->Cs.empty()) std::memcpy(s->Cs.data(), C, sizeof(double) * s->Cs.size());
 }
 int orc_project_once(void* h, double dt) { return static_cast<orc::Solver*>(h)->project_once(dt); }
 int orc_advance(void* h, double dt) { return static_cast<orc::Solver*>(h)->advance(dt); }

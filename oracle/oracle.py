@@ -58,6 +58,8 @@ def lib():
         L.orc_poisson_csr.argtypes = [vp, C.POINTER(C.c_int64), ip, dp]
         L.orc_poisson_csr.restype = C.c_int64
         L.orc_record_poisson.argtypes = [vp, C.c_int]
+        L.orc_get_scalars.argtypes = [vp, dp, dp]
+        L.orc_set_scalars.argtypes = [vp, dp, dp]
         L.orc_recorded_poisson.argtypes = [vp, C.c_int, dp, dp, dp]
         L.orc_recorded_poisson.restype = C.c_int
         _lib = L
@@ -121,6 +123,19 @@ class Oracle:
         s = abi.StatsT()
         lib().orc_stats(self.h, C.byref(s))
         return s.as_dict()
+
+    def scalars(self):
+        """(T [nc], C [n_scalars, nc])."""
+        ns = max(0, min(int(self._params.n_scalars), 4))
+        T = np.zeros(self.nc)
+        Cs = np.zeros((ns, self.nc))
+        lib().orc_get_scalars(self.h, _p(T), _p(Cs) if ns else None)
+        return T, Cs
+
+    def set_scalars(self, T=None, C=None):
+        T = None if T is None else np.ascontiguousarray(T, dtype=np.float64)
+        C = None if C is None else np.ascontiguousarray(C, dtype=np.float64)
+        lib().orc_set_scalars(self.h, _p(T), _p(C))
 
     def poisson_csr(self):
         """The assembled pressure operator as (offsets, columns, values)."""

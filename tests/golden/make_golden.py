@@ -1,5 +1,5 @@
 """Regenerates tests/golden/*.csv: the reference's regression statistics (golden vectors) for the
-cases whose meshes are reproducible without gmsh, reduced to the columns the reference's own
+cases on this path, reduced to the columns the reference's own
 comparison uses (tests/regression/compare_stats.py: time, E, Umax, Ub, tauw_mean, nu_sgs_mean,
 max_abs_divU).  Run in a checkout that has the reference tree:
 
@@ -9,7 +9,8 @@ import csv
 import os
 import sys
 
-CASES = ("tgv", "tgv_skew", "tgv_skew_chk", "pdrop", "hydro", "hydrowall")
+CASES = ("tgv", "tgv_skew", "tgv_skew_chk", "pdrop", "hydro", "hydrowall", "rb", "channel", "amd", "graded",
+         "channel_most")
 COLS = ("step", "time", "E", "Umax", "Ub", "tauw_mean", "nu_sgs_mean", "max_abs_divU", "dt")
 
 

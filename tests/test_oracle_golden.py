@@ -4,6 +4,12 @@ tests/golden/<case>_np1.csv are the reference's tests/regression/reference CSVs 
 gfortran CPU build), reduced to the compared columns by tests/golden/make_golden.py.  The check is
 the reference's own (tests/regression/compare_stats.py): integral quantities within rtol 1e-6,
 face-flux divergence below 1e-9.
+
+Coverage: KEP / CDS / QUICK momentum advection, skewed and graded meshes, non-orthogonal
+correctors, outlets and walls (tgv*, pdrop, hydro*); Vreman and AMD with the log-law wall model
+and its filter (channel, amd, graded); temperature transport with van Leer TVD, fixed-temperature
+walls and Boussinesq buoyancy (rb).  The graded wall boxes are the reference's RB.geo meshes,
+rebuilt with the closed-form "Bump" node distribution (dopamine_b200.cases.bump_nodes).
 """
 import csv
 import os
@@ -37,7 +43,8 @@ def run_case(name, steps=None):
     return ref, out
 
 
-@pytest.mark.parametrize("name", ["tgv_skew", "tgv_skew_chk", "pdrop", "hydro", "hydrowall", "tgv"])
+@pytest.mark.parametrize("name", ["tgv_skew", "tgv_skew_chk", "pdrop", "hydro", "hydrowall", "tgv", "rb", "channel",
+                                  "amd", "graded"])
 def test_oracle_matches_reference_csv(name):
     ref, got = run_case(name)
     for step, s in got.items():
