@@ -19,7 +19,7 @@ BC_BY_NAME = {
 SCHEME_VANLEER_TVD, SCHEME_KOREN_TVD, SCHEME_CDS, SCHEME_KEP, SCHEME_QUICK = 1, 2, 3, 4, 5
 SCHEME_BY_NAME = {"VANLEER_TVD": 1, "KOREN_TVD": 2, "CDS": 3, "KEP": 4, "QUICK": 5}
 SGS_NONE, SGS_VREMAN, SGS_SMAGORINSKY, SGS_AMD = 0, 1, 2, 3
-WM_LOGLAW, WM_NONE = 0, 1
+WM_LOGLAW, WM_NONE, WM_MOST = 0, 1, 2
 FORM_FP64, FORM_MIXED = 0, 1
 PSOLVER_JACOBI_PCG, PSOLVER_TWOLEVEL_FCG = 0, 1
 
@@ -58,7 +58,8 @@ class ParamsT(C.Structure):
         ("c_amd", C.c_double), ("amd_wall_gradient", C.c_int), ("wall_model_height", C.c_double),
         ("wall_model_filter_time", C.c_double), ("wall_model_filter_tf_fac", C.c_double), ("form", C.c_int),
         ("p_solver", C.c_int), ("p_smooth_degree", C.c_int), ("p_smooth_lmin", C.c_double),
-        ("p_smooth_lmax", C.c_double),
+        ("p_smooth_lmax", C.c_double), ("abl_z0_m", C.c_double), ("abl_z0_h", C.c_double),
+        ("abl_T_surface", C.c_double), ("abl_L_obukhov", C.c_double), ("abl_compute_L", C.c_int),
     ]
 
 
@@ -107,6 +108,11 @@ def default_params(**kw):
     p.p_smooth_degree = 6
     p.p_smooth_lmin = 0.05
     p.p_smooth_lmax = 2.0
+    p.abl_z0_m = 0.1
+    p.abl_z0_h = 0.01
+    p.abl_T_surface = 300.0
+    p.abl_L_obukhov = 0.0
+    p.abl_compute_L = 1
     for k, v in kw.items():
         if k in ("f_const", "g", "scalar_diffusivity", "scalar_pr_t"):
             arr = getattr(p, k)

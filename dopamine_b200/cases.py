@@ -287,6 +287,18 @@ def regression_case(name):
                          cfl_max=0.5, p_tol=1e-10, p_max_iter=500, rhie_chow_dual=0, sgs_model=abi.SGS_NONE,
                          wall_model=abi.WM_NONE),
                     "uniform", 1.0e-2, n_steps=20)
+    if name == "channel_most":
+        # as 'channel' with the MOST wall model (z0_m 1e-3, z0_h 1e-4, T_surface 298) and Boussinesq
+        L = 6.283185307179586
+        wall = {"bc": "wallModel"}
+        patches = [{"bc": "periodic"}] * 4 + [dict(wall, scalar_mode=(1, 0, 0, 0), scalar_value=(1.0, 0, 0, 0)),
+                                              dict(wall)]
+        prm = dict(scheme=abi.SCHEME_KEP, sgs_model=abi.SGS_VREMAN, wall_model=abi.WM_MOST, nu=2.5316e-3,
+                   f_const=(1.0, 0.0, 0.0), g=(0.0, 0.0, -9.80665), boussinesq=1, dt=2.0e-3, cfl_max=0.5,
+                   p_tol=1e-10, p_max_iter=1000, rhie_chow_dual=0, n_scalars=1, scalar_scheme=abi.SCHEME_VANLEER_TVD,
+                   scalar_diffusivity=(1.0e-3, 0, 0, 0), scalar_pr_t=(1.0, 0, 0, 0), abl_z0_m=1.0e-3,
+                   abl_z0_h=1.0e-4, abl_T_surface=298.0)
+        return Case(name, wall_box(32, 16, 16, L, L, 1.0, 0.25), patches, prm, "taylor_green", 1.0, n_steps=20)
     if name in ("channel", "amd", "graded"):
         # 32x16x16 wall-bounded box 2pi x 2pi x 1 with a Taylor-Green field, KEP, log-law wall
         # model, f_x = 1, one passive tracer with a Dirichlet value 1 on the bottom wall
@@ -307,7 +319,7 @@ def regression_case(name):
 
 
 REGRESSION_CASES = ("tgv", "tgv_skew", "tgv_skew_chk", "pdrop", "hydro", "hydrowall", "rb", "channel", "amd",
-                    "graded")
+                    "graded", "channel_most")
 
 
 def tgv_config(n=32, n_steps=200, scheme=abi.SCHEME_CDS):

@@ -432,11 +432,14 @@ __device__ __forceinline__ double clampv_d(double x, double lo, double hi) {
   return fmin(fmax(x, l), h);
 }
 
-__device__ void quick3_d(const Dev& d, const ReconCtx& c, const double* U, const double* gU, double* phi) {
+// QUICK fit of K components at once (U: [K][nc], gU: [3K][nc], component k's gradient in rows
+// 3k..3k+2); K = 3 for momentum, 1 for a scalar.
+template <int K>
+__device__ void quick_d(const Dev& d, const ReconCtx& c, const double* U, const double* gU, double* phi) {
   const int nc = d.nc;
   bool hg = c.up < nc && c.down < nc;
-  double pU[3], pD[3], g[3][3];
-  for (int k = 0; k < 3; ++k) {
+  double pU[K], pD[K], g[K][3];
+  for (int k = 0; k < K; ++k) {
     pU[k] = U[k * nc + c.up];
     pD[k] = U[k * nc + c.down];
     for (int i = 0; i < 3; ++i) g[k][i] = hg ? gU[(3 * k + i) * nc + c.up] : 0.0;
@@ -450,8 +453,8 @@ __device__ void quick3_d(const Dev& d, const ReconCtx& c, const double* U, const
   double w = 1.0 / dist2;
   double a11 = w * c.s_down * c.s_down, a12 = a11 * c.s_down, a22 = a12 * c.s_down, lden = a11;
   int nfit = 1;
-  double b1[3], b2[3], ln[3];
-  for (int k = 0; k < 3; ++k) {
+  double b1[K], b2[K], ln[K];
+  for (int k = 0; k < K; ++k) {
     double dp = axial(pD[k], pU[k], g[k], dv, c.s_down);
     b1[k] = w * c.s_down * dp;
     b2[k] = w * c.s_down * c.s_down * dp;
@@ -473,7 +476,7 @@ __device__ void quick3_d(const Dev& d, const ReconCtx& c, const double* U, const
       double al = fmin(1.0, -s_ / sqrt(d2));
       double wt = (0.25 + al * al) / d2;
       a11 += wt * s_ * s_; a12 += wt * s_ * s_ * s_; a22 += wt * s_ * s_ * s_ * s_; lden += wt * s_ * s_;
-      for (int k = 0; k < 3; ++k) {
+      for (int k = 0; k < K; ++k) {
         double dp = axial(U[k * nc + n], pU[k], g[k], dd, s_);
         b1[k] += wt * s_ * dp; b2[k] += wt * s_ * s_ * dp; ln[k] += wt * s_ * dp;
       }
@@ -481,7 +484,7 @@ __device__ void quick3_d(const Dev& d, const ReconCtx& c, const double* U, const
     }
   }
   double det = a11 * a22 - a12 * a12;
-  for (int k = 0; k < 3; ++k) {
+  for (int k = 0; k < K; ++k) {
     double a1, a2;
     if (nfit >= 2 && fabs(det) > SMALLD) { a1 = (b1[k] * a22 - b2[k] * a12) / det; a2 = (-b1[k] * a12 + b2[k] * a11) / det; }
     else if (lden > SMALLD) { a1 = ln[k] / lden; a2 = 0.0; }
@@ -489,6 +492,10 @@ __device__ void quick3_d(const Dev& d, const ReconCtx& c, const double* U, const
     double v = pU[k] + a1 * c.s_face + a2 * c.s_face * c.s_face;
     phi[k] = clampv_d(v, fmin(pU[k], pD[k]), fmax(pU[k], pD[k]));
   }
+}
+__device__ __forceinline__ void quick3_d(const Dev& d, const ReconCtx& c, const double* U, const double* gU,
+                                         double* phi) {
+  quick_d<3>(d, c, U, gU, phi);
 }
 
 __device__ double tvd_d(const Dev& d, int scheme, const double* phi, const ReconCtx& c, int far) {

@@ -1,0 +1,180 @@
+// Temperature and passive-scalar transport: boundary values, face fluxes and the per-cell
+// gather with the RK3W update.  Same structure as the momentum path (per-face fluxes, then a
+// gather in ascending face order per cell, so no atomics and the reference's summation order).
+#pragma once
+#include "kernels.cuh"
+
+namespace dpm {
+namespace gpu {
+
+// Boundary values of a cell scalar (src/bc/mod_bc.f90:489-588 apply_temperature_bc, :591-680
+// apply_passive_scalar_bc).  kind 0 = temperature: inlet / fixed-temperature faces take bval,
+// periodic faces the gc-weighted partner value, every other face the owner value extrapolated
+// with the cell gradient g ([3][nc]).  kind 1 = passive scalar: periodic as above, else the
+// face's mode (0 zero gradient, 1 Dirichlet bsval, 2 Neumann flux bsval with the face
+// diffusivity alpha + nu_t / prt).  filt: -1 all faces, 0 non-periodic, 1 periodic.
+__global__ void k_scalar_bc(Dev d, int kind, const double* __restrict__ phi, const double* __restrict__ g,
+                            double* __restrict__ pb, int filt, const double* __restrict__ bval,
+                            const int* __restrict__ bmode, const double* __restrict__ bsval, double alpha,
+                            double prt, const double* __restrict__ nus) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= d.nb) return;
+  const int nc = d.nc, nf = d.nf;
+  const int f = d.nfi + b, bc = d.bbc[b];
+  if (filt == 1 && bc != BC_PERIODIC) return;
+  if (filt == 0 && bc == BC_PERIODIC) return;
+  const int o = d.fo[f];
+  double v;
+  if (bc == BC_PERIODIC) {
+    const int pn = d.bpnb[b];
+    v = pn >= 0 ? d.bpgc[b] * phi[o] + (1.0 - d.bpgc[b]) * phi[pn] : phi[o];
+  } else if (kind == 0) {
+    if (bc == BC_INLET || bc == BC_FIXEDTEMP) {
+      v = bval[b];
+    } else {
+      double d0 = d.fcen[f] - d.cen[o], d1 = d.fcen[nf + f] - d.cen[nc + o], d2 = d.fcen[2 * nf + f] - d.cen[2 * nc + o];
+      v = phi[o] + g[o] * d0 + g[nc + o] * d1 + g[2 * nc + o] * d2;
+    }
+  } else {
+    const int mode = bmode[b];
+    if (mode == 1) {
+      v = bsval[b];
+    } else if (mode == 2) {
+      const double a = alpha + nus[o] / prt;
+      const double dd = fmax(d.dcf[f], SMALLD);
+      v = a > SMALLD ? phi[o] + bsval[b] * dd / a : phi[o];
+    } else {
+      v = phi[o];
+    }
+  }
+  pb[b] = v;
+}
+
+// Per-face advective flux Fn * phi_f (src/numerics/mod_advection.f90:267-675: CDS with the eps
+// correction, QUICK, van Leer, Koren; Fn is the projected U_face, zero on walls) and diffusive
+// flux (src/numerics/mod_viscous.f90:286-507: alpha_eff = alpha + nu_t / prt, clamped
+// orthogonality weight, gc-mean gradient on the transverse part, Jasak split on boundaries).
+__global__ void __launch_bounds__(TPB) k_face_scalar(Dev d, int scheme, const double* __restrict__ phi,
+                                                     const double* __restrict__ pb, const double* __restrict__ g,
+                                                     const double* __restrict__ nus, double alpha, double prt,
+                                                     const double* __restrict__ Uface, double* __restrict__ fadv,
+                                                     double* __restrict__ fdif) {
+  int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= d.nf) return;
+  const int nc = d.nc, nf = d.nf;
+  const int o = d.fo[f], n = d.fn[f];
+  const int b = f - d.nfi;
+  const int bc = n >= 0 ? -1 : d.bbc[b];
+  double Fn = (n < 0 && is_wall_bc(bc)) ? 0.0 : Uface[f];
+  double ph;
+  if (scheme == 3) {  // CDS
+    int npr = -1;
+    bool rec = n >= 0;
+    if (!rec && bc == BC_PERIODIC) { npr = d.bpnb[b]; rec = npr >= 0; }
+    if (rec) {
+      const int ns = n >= 0 ? n : npr;
+      const double w = f >= d.nfi ? d.bpgc[b] : d.gc[f];
+      const double plain = w * phi[o] + (1.0 - w) * phi[ns];
+      if (f < d.nfi) {
+        double gm0 = w * g[o] + (1.0 - w) * g[ns];
+        double gm1 = w * g[nc + o] + (1.0 - w) * g[nc + ns];
+        double gm2 = w * g[2 * nc + o] + (1.0 - w) * g[2 * nc + ns];
+        double pe = plain + (gm0 * d.eps[f] + gm1 * d.eps[nf + f] + gm2 * d.eps[2 * nf + f]);
+        const double wb = d.wbl[f];
+        if (wb < 1.0) pe = plain + wb * (pe - plain);
+        ph = pe;
+      } else {
+        ph = plain;
+      }
+      if (!finite_d(ph)) ph = (Fn >= 0.0 || n < 0) ? phi[o] : phi[n];
+    } else {
+      ph = pb[b];
+    }
+  } else {  // QUICK (5), van Leer (1), Koren (2)
+    ReconCtx ctx;
+    const bool ok = recon_context_d(d, f, Fn, ctx);
+    if (ok) {
+      if (scheme == 5) quick_d<1>(d, ctx, phi, g, &ph);
+      else ph = tvd_d(d, scheme, phi, ctx, far_upwind_d(d, ctx));
+      if (!finite_d(ph)) ph = (Fn >= 0.0 || n < 0) ? phi[o] : phi[n];
+    } else {
+      ph = pb[b];
+    }
+  }
+  if (!finite_d(Fn)) Fn = 0.0;
+  if (!finite_d(ph)) ph = 0.0;
+  fadv[f] = Fn * ph;
+
+  // ---- diffusion (owner orientation)
+  const double sf0 = d.sf[f], sf1 = d.sf[nf + f], sf2 = d.sf[2 * nf + f];
+  const double area = d.area[f];
+  auto pair_flux = [&](int nbc, double w, double aeff, const double* dn_, double dl) {
+    const double sdd = (sf0 * dn_[0] + sf1 * dn_[1] + sf2 * dn_[2]) / dl;
+    const double dp0 = sf0 - (sdd / dl) * dn_[0], dp1 = sf1 - (sdd / dl) * dn_[1], dp2 = sf2 - (sdd / dl) * dn_[2];
+    const double wo = area * fmax(0.0, fmin(1.0, sdd / (area + SMALLD)));
+    const double gf0 = w * g[o] + (1.0 - w) * g[nbc];
+    const double gf1 = w * g[nc + o] + (1.0 - w) * g[nc + nbc];
+    const double gf2 = w * g[2 * nc + o] + (1.0 - w) * g[2 * nc + nbc];
+    const double dphi = (phi[nbc] - phi[o]) * wo / dl + (gf0 * dp0 + gf1 * dp1 + gf2 * dp2);
+    return aeff * dphi;
+  };
+  auto bnd_flux = [&]() {
+    const double aeff = alpha + nus[o] / prt;
+    const double dn_[3] = {d.fcen[f] - d.cen[o], d.fcen[nf + f] - d.cen[nc + o], d.fcen[2 * nf + f] - d.cen[2 * nc + o]};
+    const double dl = sqrt(dn_[0] * dn_[0] + dn_[1] * dn_[1] + dn_[2] * dn_[2]) + SMALLD;
+    const double sdd = (sf0 * dn_[0] + sf1 * dn_[1] + sf2 * dn_[2]) / dl;
+    const double dp0 = sf0 - (sdd / dl) * dn_[0], dp1 = sf1 - (sdd / dl) * dn_[1], dp2 = sf2 - (sdd / dl) * dn_[2];
+    const double wo = area * fmax(0.0, fmin(1.0, sdd / (area + SMALLD)));
+    const double dphi = (pb[b] - phi[o]) * wo / dl + (g[o] * dp0 + g[nc + o] * dp1 + g[2 * nc + o] * dp2);
+    return aeff * dphi;
+  };
+  double flux;
+  if (n >= 0) {
+    const double w = d.gc[f];
+    const double aeff = alpha + (w * nus[o] + (1.0 - w) * nus[n]) / prt;
+    const double dn_[3] = {d.cen[n] - d.cen[o], d.cen[nc + n] - d.cen[nc + o], d.cen[2 * nc + n] - d.cen[2 * nc + o]};
+    flux = pair_flux(n, w, aeff, dn_, sqrt(dn_[0] * dn_[0] + dn_[1] * dn_[1] + dn_[2] * dn_[2]) + SMALLD);
+  } else if (bc == BC_PERIODIC && d.bpnb[b] >= 0) {
+    const int npr = d.bpnb[b];
+    const int pr = d.bpair[b];
+    const int pf = pr >= 0 ? d.nfi + pr : -1;
+    double dper, gcp;
+    if (pf >= 0) { dper = d.dcf[f] + d.dcf[pf]; gcp = d.dcf[pf] / (dper + SMALLD); }
+    else if (d.bpdcf[b] > SMALLD) { dper = d.dcf[f] + d.bpdcf[b]; gcp = d.bpdcf[b] / (dper + SMALLD); }
+    else { dper = 2.0 * d.dcf[f]; gcp = 0.5; }
+    const double aeff = alpha + (gcp * nus[o] + (1.0 - gcp) * nus[npr]) / prt;
+    const double dn_[3] = {dper * d.nrm[f], dper * d.nrm[nf + f], dper * d.nrm[2 * nf + f]};
+    flux = pair_flux(npr, gcp, aeff, dn_, dper + SMALLD);
+  } else {
+    flux = bnd_flux();
+  }
+  fdif[f] = flux;
+}
+
+// Per-cell gather: H = conv + diff in ascending face order; with predict, the RK3W update
+// phi += dt (a_k H + b_k H0) in place (src/solver/mod_fv_solver.f90:1322-1350).
+__global__ void __launch_bounds__(TPB) k_cell_scalar(Dev d, const double* __restrict__ fadv,
+                                                     const double* __restrict__ fdif, double* __restrict__ H,
+                                                     const double* __restrict__ H0, double* __restrict__ phi,
+                                                     double* __restrict__ conv_out, double* __restrict__ dif_out,
+                                                     double dt, double a_k, double b_k, int predict) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.nc) return;
+  const int nc = d.nc;
+  const double iv = d.ivol[c];
+  double cv = 0.0, vs = 0.0;
+  for (int s = 0; s < d.S; ++s) {
+    const int f = d.cf[s * nc + c];
+    if (f == PADI) break;
+    if (d.fo[f] == c) { cv -= fadv[f] * iv; vs += fdif[f] * iv; }
+    else { cv += fadv[f] * iv; vs -= fdif[f] * iv; }
+  }
+  const double h = cv + vs;
+  H[c] = h;
+  if (conv_out) conv_out[c] = cv;
+  if (dif_out) dif_out[c] = vs;
+  if (predict) phi[c] = phi[c] + dt * (a_k * h + b_k * H0[c]);
+}
+
+}  // namespace gpu
+}  // namespace dpm

@@ -25,6 +25,7 @@
 #include "fcg.cuh"
 #include "kernels.cuh"
 #include "pcg.cuh"
+#include "scalars.cuh"
 
 namespace dpm {
 namespace gpu {
@@ -177,6 +178,12 @@ struct Solver {
   int* cg_status;
   int cg_grid = 0;
   bool cg_coop = true;
+  // temperature (transported when Boussinesq is on) and passive scalars, scalar-major
+  double *Tb = nullptr, *gT = nullptr, *HT = nullptr, *HT0 = nullptr;
+  int ns = 0;
+  double *Cs = nullptr, *Cb = nullptr, *gC = nullptr, *HC = nullptr, *HC0 = nullptr;
+  double *sc_fadv = nullptr, *sc_fdif = nullptr, *bTval = nullptr, *bsval = nullptr;
+  int* bsmode = nullptr;
   // two-level flexible CG (p_solver == DPM_PSOLVER_TWOLEVEL_FCG)
   bool use_fcg = false;
   FcgArgs fa{};
@@ -353,6 +360,10 @@ struct Solver {
       }
     }
     cg_part = mem.alloc<double>(8 * (size_t)cg_grid);
+    {
+      int rc = setup_scalars();
+      if (rc) return rc;
+    }
     if (P.p_solver == DPM_PSOLVER_TWOLEVEL_FCG) {
       int rc = setup_fcg(dev_sms);
       if (rc) return rc;
@@ -388,8 +399,10 @@ struct Solver {
   void refresh_halos_and_bc() {
     velocity_bc(0, 1);
     pressure_bc(F.p, 0, !S.skip_grad_p, 0);
+    scalar_bcs(0);
     velocity_bc(1, 1);
     pressure_bc(F.p, 1, 0, 0);
+    scalar_bcs(1);
   }
   void velocity_bc_refresh() {
     velocity_bc(0, 1);
@@ -515,6 +528,90 @@ struct Solver {
   void correct_face_fluxes(double dt, bool ptot) {
     k_correct_face_flux<<<nblk(nf), TPB, 0, st>>>(d, dt, ptot, !S.skip_nonortho, F.p, F.gp, F.ff, F.Uf);
     launches++;
+  }
+
+  // Temperature and passive scalars: fields, per-face boundary data (fixed temperature, scalar
+  // mode and value per boundary face) and flux scratch.
+  int setup_scalars() {
+    auto ok_scheme = [](int sch) {
+      return sch == DPM_SCHEME_CDS || sch == DPM_SCHEME_QUICK || sch == DPM_SCHEME_VANLEER_TVD ||
+             sch == DPM_SCHEME_KOREN_TVD;
+    };
+    ns = std::max(0, std::min(P.n_scalars, 4));
+    if ((P.boussinesq && !ok_scheme(P.temperature_scheme)) || (ns > 0 && !ok_scheme(P.scalar_scheme)))
+      return DPM_ERR_UNSUPPORTED;
+    Tb = mem.alloc<double>(std::max(nb, 1)); gT = mem.alloc<double>(3 * (size_t)nc);
+    HT = mem.alloc<double>(nc); HT0 = mem.alloc<double>(nc);
+    sc_fadv = mem.alloc<double>(nf); sc_fdif = mem.alloc<double>(nf);
+    std::vector<double> tv(std::max(nb, 1), P.T_ref), sv((size_t)std::max(ns, 1) * std::max(nb, 1), 0.0);
+    std::vector<int> sm((size_t)std::max(ns, 1) * std::max(nb, 1), 0);
+    for (int b = 0; b < nb; ++b) {
+      const int q = m.patch[nfi_() + b];
+      if (q < 0) continue;
+      tv[b] = pc[q].T_val;
+      for (int k = 0; k < ns; ++k) {
+        sm[(size_t)k * nb + b] = pc[q].scalar_mode[k];
+        sv[(size_t)k * nb + b] = pc[q].scalar_value[k];
+      }
+    }
+    bTval = mem.upload(tv);
+    bsmode = mem.upload(sm);
+    bsval = mem.upload(sv);
+    if (!Tb || !gT || !HT || !HT0 || !sc_fadv || !sc_fdif || !bTval || !bsmode || !bsval) return DPM_ERR_CUDA;
+    launch_fill(Tb, std::max(nb, 1), P.T_ref);
+    launch_fill(gT, 3 * (int64_t)nc, 0.0);
+    if (ns > 0) {
+      Cs = mem.alloc<double>((size_t)ns * nc); Cb = mem.alloc<double>((size_t)ns * std::max(nb, 1));
+      gC = mem.alloc<double>((size_t)ns * 3 * nc);
+      HC = mem.alloc<double>((size_t)ns * nc); HC0 = mem.alloc<double>((size_t)ns * nc);
+      if (!Cs || !Cb || !gC || !HC || !HC0) return DPM_ERR_CUDA;
+      launch_fill(Cs, (int64_t)ns * nc, 0.0);
+      launch_fill(Cb, (int64_t)ns * std::max(nb, 1), 0.0);
+      launch_fill(gC, (int64_t)ns * 3 * nc, 0.0);
+    }
+    return 0;
+  }
+  int nfi_() const { return (int)m.n_int_faces; }
+
+  void temperature_bc(int filt) {
+    if (nb == 0) return;
+    k_scalar_bc<<<nblk(nb), TPB, 0, st>>>(d, 0, F.T, gT, Tb, filt, bTval, nullptr, nullptr, 0.0, 1.0, F.nu_sgs);
+    launches++;
+  }
+  void scalar_bc(int k, int filt) {
+    if (nb == 0) return;
+    k_scalar_bc<<<nblk(nb), TPB, 0, st>>>(d, 1, Cs + (size_t)k * nc, nullptr, Cb + (size_t)k * nb, filt, nullptr,
+                                          bsmode + (size_t)k * nb, bsval + (size_t)k * nb, P.scalar_diffusivity[k],
+                                          P.Pr_t, F.nu_sgs);
+    launches++;
+  }
+  void scalar_bcs(int filt) {
+    if (P.boussinesq) temperature_bc(filt);  // T_bnd is only read when T is transported
+    for (int k = 0; k < ns; ++k) scalar_bc(k, filt);
+  }
+  // cell gradients of U, of T when it is transported, and of every passive scalar
+  void grad_all() {
+    grad_U();
+    if (P.boussinesq) grad_scalar(F.T, Tb, gT);
+    for (int k = 0; k < ns; ++k) grad_scalar(Cs + (size_t)k * nc, Cb + (size_t)k * nb, gC + (size_t)k * 3 * nc);
+  }
+  // explicit right-hand side and RK3W update of T and the scalars (after the momentum predictor,
+  // which reads the old T for the buoyancy term)
+  void scalar_transport(int scheme, double* phi, const double* pbv, const double* g, double alpha, double prt,
+                        double* H, const double* H0, double dt, double a_k, double b_k, int predict,
+                        double* conv_out, double* dif_out) {
+    k_face_scalar<<<nblk(nf), TPB, 0, st>>>(d, scheme, phi, pbv, g, F.nu_sgs, alpha, prt, F.Uf, sc_fadv, sc_fdif);
+    k_cell_scalar<<<nblk(nc), TPB, 0, st>>>(d, sc_fadv, sc_fdif, H, H0, phi, conv_out, dif_out, dt, a_k, b_k, predict);
+    launches += 2;
+  }
+  void scalars_rhs(double dt, double a_k, double b_k) {
+    if (P.boussinesq)
+      scalar_transport(P.temperature_scheme, F.T, Tb, gT, P.alpha_T, P.Pr_t, HT, HT0, dt, a_k, b_k, 1, nullptr,
+                       nullptr);
+    for (int k = 0; k < ns; ++k)
+      scalar_transport(P.scalar_scheme, Cs + (size_t)k * nc, Cb + (size_t)k * nb, gC + (size_t)k * 3 * nc,
+                       P.scalar_diffusivity[k], P.scalar_pr_t[k], HC + (size_t)k * nc, HC0 + (size_t)k * nc, dt, a_k,
+                       b_k, 1, nullptr, nullptr);
   }
 
   // Two-level FCG set-up: one part per SM (the kernel needs one co-resident block per part and
@@ -719,21 +816,30 @@ struct Solver {
     launch_fill(F.H, 3 * (int64_t)nc, 0.0);
     launch_fill(F.H0, 3 * (int64_t)nc, 0.0);
     launch_fill(F.rhs, nc, 0.0);
+    if (P.boussinesq) {
+      launch_fill(HT, nc, 0.0);
+      launch_fill(HT0, nc, 0.0);
+    }
+    if (ns > 0) {
+      launch_fill(HC, (int64_t)ns * nc, 0.0);
+      launch_fill(HC0, (int64_t)ns * nc, 0.0);
+    }
     double time_n = time;
     for (int k = 0; k < 3; ++k) {
       double gk_dt = RK3W_GAMMA[k] * dt;
       time = time_n + RK3W_C[k] * dt;
       refresh_halos_and_bc();
-      grad_U();
+      grad_all();
       sgs(gk_dt);
       wall_model(k == 0 ? dt : 0.0);
       explicit_rhs(dt, RK3W_ALPHA[k], RK3W_BETA[k], 1);
+      scalars_rhs(dt, RK3W_ALPHA[k], RK3W_BETA[k]);
       velocity_bc_refresh();
       copy(F.p_old, F.p, nc);
       correct_velocity(gk_dt, false, true);
       copy(F.gp_rc, F.gpc, 3 * (size_t)nc);
       velocity_bc_refresh();
-      grad_U();
+      grad_all();
       copy(F.phi_prev, F.p, nc);
       copy(F.phi_prev_b, F.pb, nb);
       double atol;
@@ -806,7 +912,10 @@ struct Solver {
       pressure_bc(F.p, 1, 0, 0);
       pressure_gradient();
       std::swap(F.H, F.H0);
+      std::swap(HT, HT0);
+      std::swap(HC, HC0);
     }
+    scalar_bcs(-1);
     time = time_n + dt;
     step++;
     cudaEventRecord(ev1, st);
@@ -953,6 +1062,32 @@ int dpm_download_state(dpm_solver_t* h, double* U, double* p, double* T, double*
   if (T) CK(cudaMemcpyAsync(T, s.F.T, sizeof(double) * s.nc, cudaMemcpyDeviceToHost, s.st));
   if (nu_sgs) CK(cudaMemcpyAsync(nu_sgs, s.F.nu_sgs, sizeof(double) * s.nc, cudaMemcpyDeviceToHost, s.st));
   CK(cudaStreamSynchronize(s.st));
+  return DPM_OK;
+}
+
+int dpm_upload_scalars(dpm_solver_t* h, const double* C) {
+  if (!h || !C) return DPM_ERR_ARG;
+  Solver& s = *h->s;
+  if (s.ns == 0) return DPM_OK;
+  CK(cudaSetDevice(s.device));
+  std::vector<double> soa((size_t)s.ns * s.nc);
+  for (int c = 0; c < s.nc; ++c)
+    for (int k = 0; k < s.ns; ++k) soa[(size_t)k * s.nc + c] = C[(size_t)c * s.ns + k];
+  CK(cudaMemcpyAsync(s.Cs, soa.data(), sizeof(double) * soa.size(), cudaMemcpyHostToDevice, s.st));
+  CK(cudaStreamSynchronize(s.st));
+  return DPM_OK;
+}
+
+int dpm_download_scalars(dpm_solver_t* h, double* C) {
+  if (!h || !C) return DPM_ERR_ARG;
+  Solver& s = *h->s;
+  if (s.ns == 0) return DPM_OK;
+  CK(cudaSetDevice(s.device));
+  std::vector<double> soa((size_t)s.ns * s.nc);
+  CK(cudaMemcpyAsync(soa.data(), s.Cs, sizeof(double) * soa.size(), cudaMemcpyDeviceToHost, s.st));
+  CK(cudaStreamSynchronize(s.st));
+  for (int c = 0; c < s.nc; ++c)
+    for (int k = 0; k < s.ns; ++k) C[(size_t)c * s.ns + k] = soa[(size_t)k * s.nc + c];
   return DPM_OK;
 }
 
@@ -1110,6 +1245,43 @@ int dpm_advection_rhs_vector(dpm_solver_t* h, int scheme, const double* U, const
   s.P.scheme = keep;
   s.P.nu = keep_nu;
   return download_vec3(s, s.conv_tmp, rhs, s.nc);
+}
+
+// Scalar operators on caller data: phi [n], phi_bnd [n_bnd], grad_phi (3, n) Fortran layout.
+static int scalar_operator(Solver& s, int scheme, const double* phi, const double* phi_bnd, const double* face_flux,
+                           const double* grad_phi, const double* nu_sgs, double alpha, double prt, double* conv,
+                           double* dif) {
+  CK(cudaSetDevice(s.device));
+  double* ph = s.scratch_c;
+  CK(cudaMemcpyAsync(ph, phi, sizeof(double) * s.nc, cudaMemcpyHostToDevice, s.st));
+  if (s.nb) CK(cudaMemcpyAsync(s.Tb, phi_bnd, sizeof(double) * s.nb, cudaMemcpyHostToDevice, s.st));
+  CK(cudaMemcpyAsync(s.aos_buf, grad_phi, 3 * sizeof(double) * s.nc, cudaMemcpyHostToDevice, s.st));
+  dpm::gpu::k_aos_to_soa<<<dpm::gpu::nblk(s.nc), dpm::gpu::TPB, 0, s.st>>>(s.nc, s.aos_buf, s.gT);
+  if (face_flux) CK(cudaMemcpyAsync(s.F.Uf, face_flux, sizeof(double) * s.nf, cudaMemcpyHostToDevice, s.st));
+  else s.launch_fill(s.F.Uf, s.nf, 0.0);
+  if (nu_sgs) CK(cudaMemcpyAsync(s.F.nu_sgs, nu_sgs, sizeof(double) * s.nc, cudaMemcpyHostToDevice, s.st));
+  else s.launch_fill(s.F.nu_sgs, s.nc, 0.0);
+  s.scalar_transport(scheme, ph, s.Tb, s.gT, alpha, prt, s.HT, s.HT0, 0.0, 0.0, 0.0, 0, s.conv_tmp, s.visc_tmp);
+  s.launches++;
+  if (conv) CK(cudaMemcpyAsync(conv, s.conv_tmp, sizeof(double) * s.nc, cudaMemcpyDeviceToHost, s.st));
+  if (dif) CK(cudaMemcpyAsync(dif, s.visc_tmp, sizeof(double) * s.nc, cudaMemcpyDeviceToHost, s.st));
+  CK(cudaStreamSynchronize(s.st));
+  return DPM_OK;
+}
+
+int dpm_advection_rhs_scalar(dpm_solver_t* h, int scheme, const double* phi, const double* phi_bnd,
+                             const double* face_flux, const double* grad_phi, double* rhs) {
+  if (!h || !phi || !phi_bnd || !face_flux || !grad_phi || !rhs) return DPM_ERR_ARG;
+  if (scheme != DPM_SCHEME_CDS && scheme != DPM_SCHEME_QUICK && scheme != DPM_SCHEME_VANLEER_TVD &&
+      scheme != DPM_SCHEME_KOREN_TVD)
+    return DPM_ERR_UNSUPPORTED;
+  return scalar_operator(*h->s, scheme, phi, phi_bnd, face_flux, grad_phi, nullptr, 0.0, 1.0, rhs, nullptr);
+}
+
+int dpm_viscous_rhs_scalar(dpm_solver_t* h, const double* phi, double alpha, const double* nu_sgs, double Pr_t,
+                           const double* grad_phi, const double* phi_bnd, double* rhs) {
+  if (!h || !phi || !nu_sgs || !grad_phi || !phi_bnd || !rhs || !(Pr_t > 0.0)) return DPM_ERR_ARG;
+  return scalar_operator(*h->s, DPM_SCHEME_CDS, phi, phi_bnd, nullptr, grad_phi, nu_sgs, alpha, Pr_t, nullptr, rhs);
 }
 
 int dpm_viscous_rhs_vector(dpm_solver_t* h, const double* U, double nu, const double* nu_sgs, const double* grad_U,

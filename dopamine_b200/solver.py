@@ -24,6 +24,7 @@ EXPORTED = (
     "dpm_advance_n", "dpm_stats", "dpm_state_is_finite", "dpm_compute_dt", "dpm_get_time", "dpm_set_time",
     "dpm_last_timing", "dpm_kernel_launches", "dpm_ls_gradient_vector", "dpm_advection_rhs_vector",
     "dpm_viscous_rhs_vector", "dpm_sgs_viscosity", "dpm_wall_model", "dpm_pcg_solve_noalloc",
+    "dpm_advection_rhs_scalar", "dpm_viscous_rhs_scalar", "dpm_upload_scalars", "dpm_download_scalars",
 )
 
 
@@ -67,6 +68,10 @@ def lib(build_if_missing=True):
     L.dpm_viscous_rhs_vector.argtypes = [vp, dp, C.c_double, dp, dp, dp, dp]
     L.dpm_sgs_viscosity.argtypes = [vp, C.c_int, dp, dp, dp, C.c_double, dp]
     L.dpm_wall_model.argtypes = [vp, dp, C.c_double, dp]
+    L.dpm_advection_rhs_scalar.argtypes = [vp, C.c_int, dp, dp, dp, dp, dp]
+    L.dpm_viscous_rhs_scalar.argtypes = [vp, dp, C.c_double, dp, C.c_double, dp, dp, dp]
+    L.dpm_upload_scalars.argtypes = [vp, dp]
+    L.dpm_download_scalars.argtypes = [vp, dp]
     L.fvm_petsc_solve_pressure.argtypes = [C.c_int, C.c_int, C.c_int, ip, ip, ip, ip, ip, dp, dp, dp, C.c_int,
                                            C.c_int, C.c_double, C.c_double, ip, dp, C.c_int, dp, ip, dp]
     L.fvm_petsc_set_pressure_solver.argtypes = [C.c_char_p]
@@ -212,6 +217,34 @@ class Solver:
         _check(lib().dpm_sgs_viscosity(self.h, model, _p(np.ascontiguousarray(U)), None,
                                        _p(np.ascontiguousarray(grad_U)), dt_stab, _p(nu)), "dpm_sgs_viscosity")
         return nu
+
+    def advection_rhs_scalar(self, scheme, phi, phi_bnd, face_flux, grad_phi):
+        rhs = np.zeros(self.nc)
+        _check(lib().dpm_advection_rhs_scalar(self.h, scheme, _p(np.ascontiguousarray(phi)),
+                                              _p(np.ascontiguousarray(phi_bnd)), _p(np.ascontiguousarray(face_flux)),
+                                              _p(np.ascontiguousarray(grad_phi)), _p(rhs)), "dpm_advection_rhs_scalar")
+        return rhs
+
+    def viscous_rhs_scalar(self, phi, alpha, nu_sgs, pr_t, grad_phi, phi_bnd):
+        rhs = np.zeros(self.nc)
+        _check(lib().dpm_viscous_rhs_scalar(self.h, _p(np.ascontiguousarray(phi)), alpha,
+                                            _p(np.ascontiguousarray(nu_sgs)), pr_t, _p(np.ascontiguousarray(grad_phi)),
+                                            _p(np.ascontiguousarray(phi_bnd)), _p(rhs)), "dpm_viscous_rhs_scalar")
+        return rhs
+
+    def scalars(self):
+        """(T [nc], C [n_scalars, nc])."""
+        ns = max(0, min(int(self.params.n_scalars), 4))
+        T = self.sync_host()["T"]
+        Cf = np.zeros((self.nc, ns))
+        if ns:
+            _check(lib().dpm_download_scalars(self.h, _p(Cf)), "dpm_download_scalars")
+        return T, np.ascontiguousarray(Cf.T)
+
+    def set_scalars(self, C):
+        """C [n_scalars, nc]."""
+        Cf = np.ascontiguousarray(np.asarray(C, dtype=np.float64).T)
+        _check(lib().dpm_upload_scalars(self.h, _p(Cf)), "dpm_upload_scalars")
 
     def wall_model(self, U, nu):
         tau = np.zeros((self.nb, 3))

@@ -58,6 +58,7 @@ extern "C" {
 /* Wall models (src/abl/mod_abl_types.f90 WM_*): log law (Reichardt) or none. */
 #define DPM_WM_LOGLAW 0
 #define DPM_WM_NONE 1
+#define DPM_WM_MOST 2       /* Monin-Obukhov surface layer (src/abl/mod_abl_wall.f90)      */
 
 /* Pressure-solve forms. */
 #define DPM_PSOLVER_JACOBI_PCG 0
@@ -86,8 +87,8 @@ typedef struct dpm_patch_cfg {
   double U_val[3];            /* inlet / moving-wall velocity                                */
   double p_val;               /* outlet pressure                                             */
   double T_val;               /* fixed temperature                                           */
-  int scalar_mode[4];         /* per passive scalar: 0 zero-gradient, 1 Dirichlet            */
-  double scalar_value[4];
+  int scalar_mode[4];         /* per passive scalar: 0 zero gradient, 1 Dirichlet (value),    */
+  double scalar_value[4];     /* 2 Neumann (value = flux per area, constant in time)          */
 } dpm_patch_cfg_t;
 
 /* Solver parameters (src/solver/mod_fv_solver.f90:solver_params_t), numerics pinned as the
@@ -128,6 +129,10 @@ typedef struct dpm_params {
   int p_solver;
   int p_smooth_degree;
   double p_smooth_lmin, p_smooth_lmax;
+  /* MOST wall model (src/abl/mod_abl_types.f90:ABLConfig): roughness lengths, surface
+   * temperature, initial Obukhov length (0 = neutral) and whether its domain mean is updated. */
+  double abl_z0_m, abl_z0_h, abl_T_surface, abl_L_obukhov;
+  int abl_compute_L;
 } dpm_params_t;
 
 /* Per-step integral statistics (src/stats/mod_stats.f90:compute_stats_sums and
@@ -232,6 +237,18 @@ int dpm_sgs_viscosity(dpm_solver_t* s, int model, const double* U, const double*
                       const double* grad_U, double dt_stab, double* nu_sgs);
 /* apply_wall_model_bc (src/sgs/mod_wall_model.f90:176): tau_w(3,nbnd). */
 int dpm_wall_model(dpm_solver_t* s, const double* U, double nu, double* tau_w);
+/* src/numerics/mod_advection.f90:56 advection_rhs_scalar (SoA fast paths :267-675): rhs[n] of a
+ * scalar phi[n] with boundary values phi_bnd[n_bnd], face flux[n_faces] and grad_phi(3, n);
+ * scheme CDS, QUICK, VANLEER_TVD or KOREN_TVD. */
+int dpm_advection_rhs_scalar(dpm_solver_t* s, int scheme, const double* phi, const double* phi_bnd,
+                             const double* face_flux, const double* grad_phi, double* rhs);
+/* src/numerics/mod_viscous.f90:286 viscous_rhs_scalar: diffusivity alpha + nu_sgs / Pr_t. */
+int dpm_viscous_rhs_scalar(dpm_solver_t* s, const double* phi, double alpha, const double* nu_sgs, double Pr_t,
+                           const double* grad_phi, const double* phi_bnd, double* rhs);
+/* Passive scalars C(n_scalars, n) in the reference's Fortran layout (src/solver/mod_fv_solver.f90:326,
+ * scalar index fastest); the temperature travels with dpm_upload_state / dpm_download_state. */
+int dpm_upload_scalars(dpm_solver_t* s, const double* C);
+int dpm_download_scalars(dpm_solver_t* s, double* C);
 
 /* ---- allocation-free Jacobi-PCG solve --------------------------------------------------------
  * No counterpart in the reference.  For callers that cannot allocate device memory when they

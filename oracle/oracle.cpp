@@ -132,6 +132,9 @@ struct Solver {
   std::vector<double> T_bnd, grad_T, H_T, H_T0, conv_T, visc_T;
   int ns = 0;
   std::vector<double> Cs, C_bnd, grad_C, H_C, H_C0, conv_C, visc_C;
+  // MOST surface layer: per-face Obukhov length and kinematic heat flux, domain-mean L
+  std::vector<double> L_bnd, q_w;
+  double L_obukhov = 0.0;
   std::vector<double> grad_U, face_flux, U_face, inv_vol;
   std::vector<double> H_U, H_U0, rhs_p, conv_U, visc_U, gp, gp_rc, gp_cell, p_tot, p_tot_bnd, phi_it, Tinv;
   std::vector<uint8_t> built;
@@ -203,6 +206,7 @@ struct Solver {
     ns = std::max(0, std::min(P.n_scalars, 4));
     Cs.assign((size_t)ns * nc, 0.0); C_bnd.assign((size_t)ns * nb, 0.0); grad_C.assign((size_t)ns * 3 * nc, 0.0);
     H_C.assign((size_t)ns * nc, 0.0); H_C0.assign((size_t)ns * nc, 0.0); conv_C.assign(nc, 0.0); visc_C.assign(nc, 0.0);
+    L_bnd.assign(nb, 0.0); q_w.assign(nb, 0.0); L_obukhov = P.abl_L_obukhov;
     auto scalar_ok = [](int sch) {
       return sch == DPM_SCHEME_CDS || sch == DPM_SCHEME_QUICK || sch == DPM_SCHEME_VANLEER_TVD || sch == DPM_SCHEME_KOREN_TVD;
     };
@@ -878,6 +882,109 @@ struct Solver {
     if (t_use > SMALL || adaptive) filt_ready = true;
   }
 
+  // ---------------------------------------------------------------- MOST surface layer
+  // src/abl/mod_abl_profiles.f90:51-86 (Businger-Dyer stable branch, Paulson unstable branch)
+  static double most_psi_m(double z) {
+    if (std::fabs(z) < 1.0e-6) return 0.0;
+    if (z > 0.0) return -5.0 * z;
+    double x = std::pow(1.0 - 16.0 * z, 0.25);
+    return 2.0 * std::log((1.0 + x) / 2.0) + std::log((1.0 + x * x) / 2.0) - 2.0 * std::atan(x) + M_PI / 2.0;
+  }
+  static double most_psi_h(double z) {
+    if (std::fabs(z) < 1.0e-6) return 0.0;
+    if (z > 0.0) return -5.0 * z;
+    double y = std::pow(1.0 - 16.0 * z, 0.5);
+    return 2.0 * std::log((1.0 + y) / 2.0);
+  }
+  static constexpr double MOST_KAPPA = 0.41, MOST_G = 9.81, MOST_L_CLIP = 5000.0;  // mod_parameters, mod_abl_wall
+  static double fsign(double a, double b) { return b >= 0.0 ? std::fabs(a) : -std::fabs(a); }
+  // L = u*^2 T_ref / (kappa g T*), kept away from 0 and clipped (mod_abl_wall.f90:L_from)
+  static double most_L_from(double us, double ts, double tref) {
+    if (std::fabs(ts) > SMALL) {
+      double L = us * us * tref / (MOST_KAPPA * MOST_G * ts);
+      L = fsign(std::max(std::fabs(L), 0.001), L);
+      if (std::fabs(L) > MOST_L_CLIP) L = fsign(MOST_L_CLIP, L);
+      return L;
+    }
+    return MOST_L_CLIP;
+  }
+  static void most_residuals(double us, double ts, double L, double up, double To, double Ts, double yw, double z0m,
+                             double z0h, double& Fu, double& FT) {
+    double pmz = most_psi_m(yw / L), pmz0 = most_psi_m(z0m / L);
+    double phz = most_psi_h(yw / L), phz0 = most_psi_h(z0h / L);
+    double dm = std::log(yw / z0m) - pmz + pmz0;
+    double dh = std::log(yw / z0h) - phz + phz0;
+    if (std::fabs(dm) < SMALL) dm = fsign(SMALL, dm);
+    if (std::fabs(dh) < SMALL) dh = fsign(SMALL, dh);
+    Fu = us - MOST_KAPPA * up / dm;
+    FT = ts - MOST_KAPPA * (To - Ts) / dh;
+  }
+  // src/abl/mod_abl_wall.f90:156-231 (most_iterate: relaxed Newton on (u*, T*) with a
+  // finite-difference Jacobian, L re-derived after every update)
+  static void most_iterate(double up, double To, double Ts, double yw, double z0m, double z0h, double L_init,
+                           double& us_out, double& ts_out, double& L_out) {
+    const double tref = To;
+    double us = std::max(SMALL, MOST_KAPPA * up / std::max(SMALL, std::log(yw / z0m)));
+    double ts = 0.1 * (To - Ts);
+    double L = std::fabs(L_init) < SMALL ? MOST_L_CLIP : L_init;
+    for (int it = 1; it <= 20; ++it) {
+      L = fsign(std::max(std::fabs(L), 0.001), L);
+      if (std::fabs(L) > MOST_L_CLIP) L = fsign(MOST_L_CLIP, L);
+      double Fu, FT, Fu_p, FT_p;
+      most_residuals(us, ts, L, up, To, Ts, yw, z0m, z0h, Fu, FT);
+      if (std::fabs(Fu) < 1.0e-8 && std::fabs(FT) < 1.0e-8) break;
+      double du_eps = std::max(1.0e-6, 1.0e-6 * std::fabs(us));
+      double dT_eps = std::max(1.0e-6, 1.0e-6 * std::fabs(ts));
+      most_residuals(us + du_eps, ts, most_L_from(us + du_eps, ts, tref), up, To, Ts, yw, z0m, z0h, Fu_p, FT_p);
+      double dFu_du = (Fu_p - Fu) / du_eps, dFT_du = (FT_p - FT) / du_eps;
+      most_residuals(us, ts + dT_eps, most_L_from(us, ts + dT_eps, tref), up, To, Ts, yw, z0m, z0h, Fu_p, FT_p);
+      double dFu_dT = (Fu_p - Fu) / dT_eps, dFT_dT = (FT_p - FT) / dT_eps;
+      double den = dFu_du * dFT_dT - dFu_dT * dFT_du;
+      if (std::fabs(den) < SMALL) break;
+      double dus = -(dFT_dT * Fu - dFu_dT * FT) / den;
+      double dts = -(dFu_du * FT - dFT_du * Fu) / den;
+      us = us + 0.5 * dus;
+      ts = ts + 0.5 * dts;
+      us = std::max(SMALL, std::min(us, 0.5 * up));
+      L = most_L_from(us, ts, tref);
+    }
+    us_out = us; ts_out = ts; L_out = L;
+  }
+  // src/abl/mod_abl_wall.f90:62-153 (abl_wall_model; global roughness, owner-cell sampling at the
+  // wall-normal distance of its centroid)
+  void most_wall_model(bool update_L) {
+    const double L_cfg = L_obukhov;
+    double L_sum = 0.0;
+    int64_t nwf = 0;
+    for (int64_t fb = 0; fb < nb; ++fb) {
+      int64_t fg = nfi + fb;
+      if (bc_of_face(fg) != BC_WALL_MODEL) continue;
+      int o = m.owner[fg];
+      const double* n = &m.normal[3 * fg];
+      double yw = std::fabs((m.centre[3 * fg] - m.centroid[3 * o]) * n[0] + (m.centre[3 * fg + 1] - m.centroid[3 * o + 1]) * n[1] +
+                            (m.centre[3 * fg + 2] - m.centroid[3 * o + 2]) * n[2]) + SMALL;
+      const double* u = &U[3 * o];
+      double un = u[0] * n[0] + u[1] * n[1] + u[2] * n[2];
+      double t0 = u[0] - un * n[0], t1 = u[1] - un * n[1], t2 = u[2] - un * n[2];
+      double upm = std::sqrt(t0 * t0 + t1 * t1 + t2 * t2);
+      if (upm > SMALL) { t0 /= upm; t1 /= upm; t2 /= upm; }
+      else { t0 = t1 = t2 = 0.0; }
+      double Lg = L_bnd[fb];
+      if (std::fabs(Lg) < SMALL) Lg = L_cfg;
+      double us, ts, Ln;
+      most_iterate(upm, T[o], P.abl_T_surface, yw, std::max(P.abl_z0_m, SMALL), std::max(P.abl_z0_h, SMALL), Lg, us,
+                   ts, Ln);
+      L_bnd[fb] = Ln;
+      L_sum += Ln;
+      nwf++;
+      tau_w[3 * fb] = -us * us * t0;
+      tau_w[3 * fb + 1] = -us * us * t1;
+      tau_w[3 * fb + 2] = -us * us * t2;
+      q_w[fb] = -us * ts;
+    }
+    if (P.abl_compute_L && update_L && nwf > 0) L_obukhov = L_sum / (double)nwf;
+  }
+
   // ---------------------------------------------------------------- advection
   int periodic_nb(int64_t fb, int o) const {  // soa_resolve_periodic_nb_dev, single-rank
     int n = m.periodic_partner_cell(fb);
@@ -1428,6 +1535,13 @@ struct Solver {
       advection_scalar(P.temperature_scheme, T.data(), T_bnd.data(), grad_T.data(), conv_T.data());
       viscous_scalar(T.data(), P.alpha_T, P.Pr_t, grad_T.data(), T_bnd.data(), visc_T.data());
       for (int64_t c = 0; c < nc; ++c) H_T[c] = conv_T[c] + visc_T[c];
+      if (P.wall_model == DPM_WM_MOST)  // add_wall_heat_flux_to_rhs (mod_fv_solver.f90:2279-2313)
+        for (int64_t fb = 0; fb < nb; ++fb) {
+          int64_t fg = nfi + fb;
+          if (bc_of_face(fg) != BC_WALL_MODEL) continue;
+          int o = m.owner[fg];
+          H_T[o] = H_T[o] + q_w[fb] * m.area[fg] / m.volume[o];
+        }
     } else {
       std::fill(H_T.begin(), H_T.end(), 0.0);
     }
@@ -1895,6 +2009,7 @@ struct Solver {
       compute_all_gradients();
       sgs_viscosity(gk_dt);
       if (P.wall_model == DPM_WM_NONE) std::fill(tau_w.begin(), tau_w.end(), 0.0);
+      else if (P.wall_model == DPM_WM_MOST) most_wall_model(k == 0);
       else wall_model(k == 0 ? dt : 0.0);
       explicit_rhs();
       double a_k = RK3W_ALPHA[k], b_k = RK3W_BETA[k];
@@ -2120,6 +2235,19 @@ void orc_advection(void* h, int scheme, const double* U, const double* U_bnd, co
   s->P.scheme = scheme;
   s->advection(rhs);
   s->P.scheme = keep;
+}
+// Scalar operators: phi [nc], phi_bnd [nb], grad_phi (3, nc) AoS.
+void orc_advection_scalar(void* h, int scheme, const double* phi, const double* phi_bnd, const double* flux,
+                          const double* gphi, double* rhs) {
+  auto* s = static_cast<orc::Solver*>(h);
+  std::memcpy(s->U_face.data(), flux, sizeof(double) * s->nf);
+  s->advection_scalar(scheme, phi, phi_bnd, gphi, rhs);
+}
+void orc_viscous_scalar(void* h, const double* phi, double alpha, const double* nu_sgs, double prt, const double* gphi,
+                        const double* phi_bnd, double* rhs) {
+  auto* s = static_cast<orc::Solver*>(h);
+  std::memcpy(s->nu_sgs.data(), nu_sgs, sizeof(double) * s->nc);
+  s->viscous_scalar(phi, alpha, prt, gphi, phi_bnd, rhs);
 }
 void orc_viscous(void* h, const double* U, const double* nu_sgs, const double* gU, const double* U_bnd, double* rhs) {
   auto* s = static_cast<orc::Solver*>(h);

@@ -59,6 +59,8 @@ def lib():
         L.orc_poisson_csr.restype = C.c_int64
         L.orc_record_poisson.argtypes = [vp, C.c_int]
         L.orc_get_scalars.argtypes = [vp, dp, dp]
+        L.orc_advection_scalar.argtypes = [vp, C.c_int, dp, dp, dp, dp, dp]
+        L.orc_viscous_scalar.argtypes = [vp, dp, C.c_double, dp, C.c_double, dp, dp, dp]
         L.orc_set_scalars.argtypes = [vp, dp, dp]
         L.orc_recorded_poisson.argtypes = [vp, C.c_int, dp, dp, dp]
         L.orc_recorded_poisson.restype = C.c_int

@@ -8,7 +8,8 @@ face-flux divergence below 1e-9.
 Coverage: KEP / CDS / QUICK momentum advection, skewed and graded meshes, non-orthogonal
 correctors, outlets and walls (tgv*, pdrop, hydro*); Vreman and AMD with the log-law wall model
 and its filter (channel, amd, graded); temperature transport with van Leer TVD, fixed-temperature
-walls and Boussinesq buoyancy (rb).  The graded wall boxes are the reference's RB.geo meshes,
+walls and Boussinesq buoyancy (rb); the MOST surface layer with its heat flux into a
+transported, buoyant temperature (channel_most).  The graded wall boxes are the reference's RB.geo meshes,
 rebuilt with the closed-form "Bump" node distribution (dopamine_b200.cases.bump_nodes).
 """
 import csv
@@ -44,7 +45,7 @@ def run_case(name, steps=None):
 
 
 @pytest.mark.parametrize("name", ["tgv_skew", "tgv_skew_chk", "pdrop", "hydro", "hydrowall", "tgv", "rb", "channel",
-                                  "amd", "graded"])
+                                  "amd", "graded", "channel_most"])
 def test_oracle_matches_reference_csv(name):
     ref, got = run_case(name)
     for step, s in got.items():
