@@ -151,13 +151,15 @@ __global__ void __launch_bounds__(TPB) k_face_scalar(Dev d, int scheme, const do
   fdif[f] = flux;
 }
 
-// Per-cell gather: H = conv + diff in ascending face order; with predict, the RK3W update
-// phi += dt (a_k H + b_k H0) in place (src/solver/mod_fv_solver.f90:1322-1350).
+// Per-cell gather: H = conv + diff in ascending face order, plus the MOST wall heat flux qw
+// (kinematic, per area) of wall-model faces when qw is given (src/solver/mod_fv_solver.f90:
+// 2279-2313); with predict, the RK3W update phi += dt (a_k H + b_k H0) in place (:1322-1350).
 __global__ void __launch_bounds__(TPB) k_cell_scalar(Dev d, const double* __restrict__ fadv,
                                                      const double* __restrict__ fdif, double* __restrict__ H,
                                                      const double* __restrict__ H0, double* __restrict__ phi,
                                                      double* __restrict__ conv_out, double* __restrict__ dif_out,
-                                                     double dt, double a_k, double b_k, int predict) {
+                                                     double dt, double a_k, double b_k, int predict,
+                                                     const double* __restrict__ qw) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= d.nc) return;
   const int nc = d.nc;
@@ -169,11 +171,101 @@ __global__ void __launch_bounds__(TPB) k_cell_scalar(Dev d, const double* __rest
     if (d.fo[f] == c) { cv -= fadv[f] * iv; vs += fdif[f] * iv; }
     else { cv += fadv[f] * iv; vs -= fdif[f] * iv; }
   }
-  const double h = cv + vs;
+  double h = cv + vs;
+  if (qw)
+    for (int s = 0; s < d.SB; ++s) {
+      const int b = d.cbn[s * nc + c];
+      if (b == PADI) break;
+      if (d.bbc[b] == BC_WALL_MODEL) h = h + qw[b] * d.area[d.nfi + b] / d.vol[c];
+    }
   H[c] = h;
   if (conv_out) conv_out[c] = cv;
   if (dif_out) dif_out[c] = vs;
   if (predict) phi[c] = phi[c] + dt * (a_k * h + b_k * H0[c]);
+}
+
+// ------------------------------------------------------------------------------------------
+// MOST surface layer (src/abl/mod_abl_wall.f90, src/abl/mod_abl_profiles.f90:51-86): per
+// wall-model face, u* and T* from the owner cell's tangential speed and temperature at its
+// wall-normal distance, by relaxed Newton with a finite-difference Jacobian; wall stress
+// -u*^2 t_hat, kinematic heat flux -u* T*, per-face Obukhov length carried to the next call.
+__device__ __forceinline__ double most_psi_m_d(double z) {
+  if (fabs(z) < 1.0e-6) return 0.0;
+  if (z > 0.0) return -5.0 * z;
+  const double x = pow(1.0 - 16.0 * z, 0.25);
+  return 2.0 * log((1.0 + x) / 2.0) + log((1.0 + x * x) / 2.0) - 2.0 * atan(x) + 1.5707963267948966;
+}
+__device__ __forceinline__ double most_psi_h_d(double z) {
+  if (fabs(z) < 1.0e-6) return 0.0;
+  if (z > 0.0) return -5.0 * z;
+  const double y = sqrt(1.0 - 16.0 * z);
+  return 2.0 * log((1.0 + y) / 2.0);
+}
+constexpr double MOST_KAPPA_D = 0.41, MOST_G_D = 9.81, MOST_L_CLIP_D = 5000.0;
+__device__ __forceinline__ double fsign_d(double a, double b) { return b >= 0.0 ? fabs(a) : -fabs(a); }
+__device__ __forceinline__ double most_L_from_d(double us, double ts, double tref) {
+  if (fabs(ts) > SMALLD) {
+    double L = us * us * tref / (MOST_KAPPA_D * MOST_G_D * ts);
+    L = fsign_d(fmax(fabs(L), 0.001), L);
+    if (fabs(L) > MOST_L_CLIP_D) L = fsign_d(MOST_L_CLIP_D, L);
+    return L;
+  }
+  return MOST_L_CLIP_D;
+}
+__device__ __forceinline__ void most_res_d(double us, double ts, double L, double up, double To, double Ts, double yw,
+                                           double z0m, double z0h, double& Fu, double& FT) {
+  double dm = log(yw / z0m) - most_psi_m_d(yw / L) + most_psi_m_d(z0m / L);
+  double dh = log(yw / z0h) - most_psi_h_d(yw / L) + most_psi_h_d(z0h / L);
+  if (fabs(dm) < SMALLD) dm = fsign_d(SMALLD, dm);
+  if (fabs(dh) < SMALLD) dh = fsign_d(SMALLD, dh);
+  Fu = us - MOST_KAPPA_D * up / dm;
+  FT = ts - MOST_KAPPA_D * (To - Ts) / dh;
+}
+__global__ void k_most(Dev d, const double* __restrict__ U, const double* __restrict__ T, double* __restrict__ tau,
+                       double* __restrict__ qw, double* __restrict__ Lb, double L_cfg, double Ts, double z0m,
+                       double z0h) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= d.nb || d.bbc[b] != BC_WALL_MODEL) return;
+  const int nc = d.nc, nf = d.nf, nb = d.nb;
+  const int f = d.nfi + b, o = d.fo[f];
+  const double n0 = d.nrm[f], n1 = d.nrm[nf + f], n2 = d.nrm[2 * nf + f];
+  const double yw = fabs((d.fcen[f] - d.cen[o]) * n0 + (d.fcen[nf + f] - d.cen[nc + o]) * n1 +
+                         (d.fcen[2 * nf + f] - d.cen[2 * nc + o]) * n2) + SMALLD;
+  const double u0 = U[o], u1 = U[nc + o], u2 = U[2 * nc + o];
+  const double un = u0 * n0 + u1 * n1 + u2 * n2;
+  double t0 = u0 - un * n0, t1 = u1 - un * n1, t2 = u2 - un * n2;
+  const double up = sqrt(t0 * t0 + t1 * t1 + t2 * t2);
+  if (up > SMALLD) { t0 /= up; t1 /= up; t2 /= up; }
+  else { t0 = t1 = t2 = 0.0; }
+  double Lg = Lb[b];
+  if (fabs(Lg) < SMALLD) Lg = L_cfg;
+  const double To = T[o], tref = To;
+  double us = fmax(SMALLD, MOST_KAPPA_D * up / fmax(SMALLD, log(yw / z0m)));
+  double ts = 0.1 * (To - Ts);
+  double L = fabs(Lg) < SMALLD ? MOST_L_CLIP_D : Lg;
+  for (int it = 1; it <= 20; ++it) {
+    L = fsign_d(fmax(fabs(L), 0.001), L);
+    if (fabs(L) > MOST_L_CLIP_D) L = fsign_d(MOST_L_CLIP_D, L);
+    double Fu, FT, Fu_p, FT_p;
+    most_res_d(us, ts, L, up, To, Ts, yw, z0m, z0h, Fu, FT);
+    if (fabs(Fu) < 1.0e-8 && fabs(FT) < 1.0e-8) break;
+    const double due = fmax(1.0e-6, 1.0e-6 * fabs(us)), dte = fmax(1.0e-6, 1.0e-6 * fabs(ts));
+    most_res_d(us + due, ts, most_L_from_d(us + due, ts, tref), up, To, Ts, yw, z0m, z0h, Fu_p, FT_p);
+    const double dFu_du = (Fu_p - Fu) / due, dFT_du = (FT_p - FT) / due;
+    most_res_d(us, ts + dte, most_L_from_d(us, ts + dte, tref), up, To, Ts, yw, z0m, z0h, Fu_p, FT_p);
+    const double dFu_dT = (Fu_p - Fu) / dte, dFT_dT = (FT_p - FT) / dte;
+    const double den = dFu_du * dFT_dT - dFu_dT * dFT_du;
+    if (fabs(den) < SMALLD) break;
+    us = us + 0.5 * (-(dFT_dT * Fu - dFu_dT * FT) / den);
+    ts = ts + 0.5 * (-(dFu_du * FT - dFT_du * Fu) / den);
+    us = fmax(SMALLD, fmin(us, 0.5 * up));
+    L = most_L_from_d(us, ts, tref);
+  }
+  Lb[b] = L;
+  tau[b] = -us * us * t0;
+  tau[nb + b] = -us * us * t1;
+  tau[2 * nb + b] = -us * us * t2;
+  qw[b] = -us * ts;
 }
 
 }  // namespace gpu

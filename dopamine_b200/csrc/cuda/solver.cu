@@ -184,6 +184,7 @@ struct Solver {
   double *Cs = nullptr, *Cb = nullptr, *gC = nullptr, *HC = nullptr, *HC0 = nullptr;
   double *sc_fadv = nullptr, *sc_fdif = nullptr, *bTval = nullptr, *bsval = nullptr;
   int* bsmode = nullptr;
+  double *most_L = nullptr, *most_qw = nullptr;  // MOST per-face Obukhov length and heat flux
   // two-level flexible CG (p_solver == DPM_PSOLVER_TWOLEVEL_FCG)
   bool use_fcg = false;
   FcgArgs fa{};
@@ -474,6 +475,14 @@ struct Solver {
       launch_fill(F.tau, 3 * (int64_t)nb, 0.0);
       return;
     }
+    if (P.wall_model == DPM_WM_MOST) {
+      // The reference also refreshes a domain-mean Obukhov length at stage 1; it only seeds faces
+      // whose own length is still zero, i.e. the first call, so the configured value is used.
+      k_most<<<nblk(nb), TPB, 0, st>>>(d, F.U, F.T, F.tau, most_qw, most_L, P.abl_L_obukhov, P.abl_T_surface,
+                                       std::max(P.abl_z0_m, SMALL), std::max(P.abl_z0_h, SMALL));
+      launches++;
+      return;
+    }
     double t_use = P.wall_model_filter_time, tf = P.wall_model_filter_tf_fac;
     bool adaptive = tf > SMALL;
     int filter = adaptive ? 2 : (t_use > SMALL ? 1 : 0);
@@ -559,6 +568,11 @@ struct Solver {
     bsval = mem.upload(sv);
     if (!Tb || !gT || !HT || !HT0 || !sc_fadv || !sc_fdif || !bTval || !bsmode || !bsval) return DPM_ERR_CUDA;
     launch_fill(Tb, std::max(nb, 1), P.T_ref);
+    most_L = mem.alloc<double>(std::max(nb, 1));
+    most_qw = mem.alloc<double>(std::max(nb, 1));
+    if (!most_L || !most_qw) return DPM_ERR_CUDA;
+    launch_fill(most_L, std::max(nb, 1), 0.0);
+    launch_fill(most_qw, std::max(nb, 1), 0.0);
     launch_fill(gT, 3 * (int64_t)nc, 0.0);
     if (ns > 0) {
       Cs = mem.alloc<double>((size_t)ns * nc); Cb = mem.alloc<double>((size_t)ns * std::max(nb, 1));
@@ -599,15 +613,16 @@ struct Solver {
   // which reads the old T for the buoyancy term)
   void scalar_transport(int scheme, double* phi, const double* pbv, const double* g, double alpha, double prt,
                         double* H, const double* H0, double dt, double a_k, double b_k, int predict,
-                        double* conv_out, double* dif_out) {
+                        double* conv_out, double* dif_out, const double* qw = nullptr) {
     k_face_scalar<<<nblk(nf), TPB, 0, st>>>(d, scheme, phi, pbv, g, F.nu_sgs, alpha, prt, F.Uf, sc_fadv, sc_fdif);
-    k_cell_scalar<<<nblk(nc), TPB, 0, st>>>(d, sc_fadv, sc_fdif, H, H0, phi, conv_out, dif_out, dt, a_k, b_k, predict);
+    k_cell_scalar<<<nblk(nc), TPB, 0, st>>>(d, sc_fadv, sc_fdif, H, H0, phi, conv_out, dif_out, dt, a_k, b_k, predict,
+                                            qw);
     launches += 2;
   }
   void scalars_rhs(double dt, double a_k, double b_k) {
     if (P.boussinesq)
       scalar_transport(P.temperature_scheme, F.T, Tb, gT, P.alpha_T, P.Pr_t, HT, HT0, dt, a_k, b_k, 1, nullptr,
-                       nullptr);
+                       nullptr, P.wall_model == DPM_WM_MOST ? most_qw : nullptr);
     for (int k = 0; k < ns; ++k)
       scalar_transport(P.scalar_scheme, Cs + (size_t)k * nc, Cb + (size_t)k * nb, gC + (size_t)k * 3 * nc,
                        P.scalar_diffusivity[k], P.scalar_pr_t[k], HC + (size_t)k * nc, HC0 + (size_t)k * nc, dt, a_k,

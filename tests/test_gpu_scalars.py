@@ -2,9 +2,9 @@
 
 Per-operator checks feed both sides the same arbitrary scalar field, boundary values, face flux,
 gradient and eddy viscosity (relative 1e-12); whole-step checks run the Rayleigh-Benard case
-(temperature with van Leer TVD, Boussinesq) and the wall-modelled channel with a Dirichlet tracer
-and compare U, T and the tracer after N steps (relative L2 1e-10); the GPU path also reproduces
-the reference's own rb CSV."""
+(temperature with van Leer TVD, Boussinesq), the wall-modelled channel with a Dirichlet tracer and
+its MOST variant, and compare U, T and the tracer after N steps (relative L2 1e-10; 1e-9 with
+MOST); the GPU path also reproduces the reference's own rb and channel_most CSVs."""
 import csv
 import os
 
@@ -67,7 +67,7 @@ def _l2(a, b, floor):
     return np.linalg.norm(a - b) / max(np.linalg.norm(b), floor * np.sqrt(b.size))
 
 
-@pytest.mark.parametrize("name,steps", [("rb", 4), ("channel", 4)])
+@pytest.mark.parametrize("name,steps", [("rb", 4), ("channel", 4), ("channel_most", 4)])
 def test_step_parity_with_scalars(name, steps):
     case = cases.regression_case(name)
     p = case.make_params()
@@ -80,12 +80,15 @@ def test_step_parity_with_scalars(name, steps):
         o.advance()
         s.advance()
         so, sg = o.state(), s.sync_host()
-        assert _l2(sg["U"], so["U"], 1e-3) <= FIELD_TOL, (name, k)
+        # MOST: u* comes from a Newton solve with a finite-difference Jacobian (steps of 1e-6),
+        # which turns last-bit differences of log/pow/atan into ~1e-10 differences of the stress
+        tol = 1e-9 if name == "channel_most" else FIELD_TOL
+        assert _l2(sg["U"], so["U"], 1e-3) <= tol, (name, k, _l2(sg["U"], so["U"], 1e-3))
         To, Co = o.scalars()
         Tg, Cg = s.scalars()
-        assert _l2(Tg, To, 1e-3) <= FIELD_TOL, (name, k, _l2(Tg, To, 1e-3))
+        assert _l2(Tg, To, 1e-3) <= tol, (name, k, _l2(Tg, To, 1e-3))
         if Co.size:
-            assert _l2(Cg, Co, 1e-3) <= FIELD_TOL, (name, k, _l2(Cg, Co, 1e-3))
+            assert _l2(Cg, Co, 1e-3) <= tol, (name, k, _l2(Cg, Co, 1e-3))
     if name == "rb":
         To, _ = o.scalars()
         assert To.max() > 0.5 + 1e-6 and To.min() < 0.5 - 1e-6  # the walls heat and cool the fluid
@@ -94,17 +97,19 @@ def test_step_parity_with_scalars(name, steps):
         assert Co.max() > 1e-3  # the tracer enters from the bottom wall
 
 
-def test_gpu_reproduces_reference_csv_rb():
-    """The GPU path against the reference's Rayleigh-Benard CSV (rtol 1e-6, divU <= 1e-9)."""
-    case = cases.regression_case("rb")
+@pytest.mark.parametrize("name", ["rb", "channel_most"])
+def test_gpu_reproduces_reference_csv(name):
+    """The GPU path against the reference's Rayleigh-Benard and MOST channel CSVs (rtol 1e-6,
+    divU <= 1e-9)."""
+    case = cases.regression_case(name)
     s = Solver(case)
     s.initialise()
-    path = os.path.join(os.path.dirname(__file__), "golden", "rb_np1.csv")
+    path = os.path.join(os.path.dirname(__file__), "golden", f"{name}_np1.csv")
     ref = {int(r["step"]): {k: float(v) for k, v in r.items() if k != "step"} for r in csv.DictReader(open(path))}
     for step in range(1, 21):
         s.advance()
         st = s.stats()
         r = ref[step]
-        for col in ("time", "E", "Umax", "Ub"):
+        for col in ("time", "E", "Umax", "Ub", "tauw_mean"):
             assert abs(st[col] - r[col]) <= 1e-6 * max(abs(r[col]), 1e-6), (step, col, st[col], r[col])
         assert st["max_abs_divU"] <= 1e-9
