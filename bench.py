@@ -2,16 +2,19 @@
 """Benchmark of the RK3W fractional-step hot path on B200.
 
 Default workload: the turbulent-channel configuration (96 x 64 x 64 hex cells, tanh-stretched,
-KEP advection, Vreman SGS, log-law wall model, constant pressure-gradient forcing, plain FP64
-Jacobi-PCG), synthetic inputs (seeded laminar-plus-noise initial state).  One "step" is one
-RK3W time step (three stages, three Poisson solves) of the whole mesh.
+KEP advection, Vreman SGS, log-law wall model, constant pressure-gradient forcing), synthetic
+inputs (seeded laminar-plus-noise initial state).  One "step" is one RK3W time step (three
+stages, three Poisson solves) of the whole mesh.  The timed form is the chosen pressure solve
+(--psolver fcg: flexible CG with the two-level preconditioner); on one GPU the plain FP64
+Jacobi-PCG form is timed beside it on the same workload and reported in the config.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--config channel|tgv]
+                    [--psolver fcg|pcg] [--no-plain]
 
 value   : cell-steps/s with the state resident in HBM (CUDA events around K steps, max over ranks)
 e2e     : the same metric through the C ABI with host buffers: every step uploads the state
           (U, p) from pinned host memory, advances, and reads the state back
-roofline: the Poisson PCG kernel (dominant): algorithmic bytes per launch / average launch time
+roofline: the Poisson kernel (dominant): algorithmic bytes per launch / average launch time
 cpu_baseline: the CPU restatement of the reference step (oracle) on this host's cores, on a
           bounded sample of the same workload.
 Multi-GPU: the north-star path is single-GPU; N GPUs run N independent replicas (weak scaling).
@@ -96,7 +99,8 @@ class ClockSampler:
 
 
 FORMS = {"pcg": "plain FP64 Jacobi-PCG",
-         "fcg": "FP64 flexible CG, two-level preconditioner (FP32 part-local Chebyshev + coarse)"}
+         "fcg": "FP64 flexible CG, deflated two-level preconditioner (148 parts, FP32 part-local Chebyshev "
+                "degree 6 in shared memory + one coarse value per part)"}
 
 
 KERNELS = {"pcg": "k_pcg (persistent Jacobi-PCG)", "fcg": "k_fcg (persistent two-level flexible CG)"}
@@ -118,7 +122,8 @@ def pcg_bytes_per_iteration(s, psolver="pcg"):
     if psolver == "fcg":
         # w = A z: cols + vals, z gathered once per cell, z written once; the part-local smoother
         # and the own-cell vectors live in shared memory and registers
-        return nc * (wa * (4 + 8) + 8 + 8)
+        # plus the deflation data (row sum, cross-coupling offsets) of the own rows
+        return nc * (wa * (4 + 8) + 8 + 8 + 8)
     phase_a = nc * (wa * (4 + 8) + 8 + 8 + 8 + 8)   # cols, vals, z, p_old, write p_new, write q
     phase_b = nc * (5 * 8 + 3 * 8)                  # x, p, r, q, dinv in; x, r, z out
     return phase_a + phase_b
@@ -193,6 +198,26 @@ def run_gpu(args, rank, world):
                 launches=launches, clocks=clocks, solver=s)
 
 
+def time_plain(args, dev, steps=3):
+    """The plain FP64 Jacobi-PCG form on the same workload: device ms per step and Poisson ms
+    per step (CUDA events inside the library), after one warm-up step."""
+    from dopamine_b200.solver import Solver
+    case = make_case(args.config)
+    case.params["p_solver"] = 0
+    s = Solver(case, device=dev)
+    s.initialise()
+    s.advance()
+    step_ms, pois_ms, its = [], [], 0
+    for _ in range(steps):
+        s.advance()
+        a, b = s.last_timing()
+        step_ms.append(a)
+        pois_ms.append(b)
+        its += s.stats()["p_iters"]
+    s.close()
+    return sum(step_ms) / steps, sum(pois_ms) / steps, its / steps
+
+
 def cpu_baseline(case_name, budget_s=20.0, nthreads=None):
     """The oracle (CPU restatement of the reference step) on this host, bounded sample."""
     from oracle.oracle import Oracle
@@ -221,14 +246,15 @@ def main():
     ap.add_argument("--impl", default="dopamine_b200")
     ap.add_argument("--config", default="channel")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--psolver", default="pcg", choices=["pcg", "fcg"],
+    ap.add_argument("--no-plain", action="store_true", help="skip timing the plain FP64 Jacobi-PCG form")
+    ap.add_argument("--psolver", default="fcg", choices=["pcg", "fcg"],
                     help="pcg: plain FP64 Jacobi-PCG; fcg: flexible CG, two-level part-local preconditioner")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
-    cfg_name = {"channel": "channel 96x64x64 Re_tau=395, KEP, Vreman, log-law wall model, FP64 Jacobi-PCG",
-                "tgv": "Taylor-Green 64^3, CDS, FP64 Jacobi-PCG"}[args.config]
+    cfg_name = {"channel": "channel 96x64x64 Re_tau=395, KEP, Vreman, log-law wall model",
+                "tgv": "Taylor-Green 64^3, CDS"}[args.config]
 
     if args.impl == "reference":
         if rank != 0:
@@ -282,6 +308,11 @@ def main():
         "gpu_launches": r["launches"],
         "clocks": r["clocks"],
     }
+    if args.psolver != "pcg" and not args.no_plain and world == 1:
+        pm, pp, pit = time_plain(args, int(os.environ.get("LOCAL_RANK", "0")))
+        line["config"]["plain_fp64_pcg"] = {"ms_per_step": pm, "poisson_ms_per_step": pp,
+                                            "pcg_iterations_per_step": pit,
+                                            "speedup_of_this_form": pm / line["ms_per_step"]}
     if not args.no_cpu_baseline:
         cb = cpu_baseline(args.config, budget_s=20.0)
         line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}

@@ -4,8 +4,10 @@
 // Cells are renumbered into P compact parts, one per thread block (dopamine_b200/csrc/host/
 // twolevel.cpp); part b owns rows [b*C, b*C + size_b).  Per iteration (FCG(1), Notay 2000):
 //
-//   z  = y_b + S_b(r)          y = E^-1 c, c = Z^T r (one value per part, all-gathered);
-//                              S_b: `degree` Chebyshev steps on D^-1 A_bb in shared memory (FP32)
+//   z  = y_b + S_b(r - A Z y)  y = E^-1 c, c = Z^T r (one value per part, all-gathered);
+//                              S_b: `degree` Chebyshev steps on D^-1 A_bb in shared memory (FP32);
+//                              A Z y needs y of the neighbouring parts only at part-boundary
+//                              rows (deflated two-level form; without `deflate`: S_b(r))
 //   grid barrier               (z is read by neighbour parts)
 //   w  = A z                   FP64, global ELL
 //   all-reduce                 z.r, z.q, z.w, r.r and the null-space sums; all-gather per part
@@ -36,7 +38,12 @@ struct FcgArgs {
   const double* val;      // [WA][n]
   const double* dinv;     // [n] new numbering
   const unsigned* lpk;    // [WL][n] local column (low 16 bits) | bf16 a_ij / a_ii (high 16 bits)
-  const double* einv;     // [P][P]
+  const double* einv_nb;  // [P][NB][P] E^-1 rows of each part's slots (slot 0 = the part)
+  int NB, deflate;        // slots per part; 1 = smooth r - A Z y instead of r (deflated form)
+  const float* srow;      // [n] intra-part row sum
+  const int* xoff;        // [n+1] cross-part couplings of each row
+  const unsigned char* xslot;
+  const float* xval;
   const double* b;        // right-hand side, original numbering
   double* x;              // guess in / solution out, original numbering
   double* xs;             // [n] scratch, new numbering
@@ -174,8 +181,8 @@ __device__ __forceinline__ double fcg_row(const FcgArgs& a, int WA, int i, const
 }
 
 // Dynamic shared memory of the kernel for a given set-up.
-inline size_t fcg_smem_bytes(int P, int C, int WL) {
-  return (size_t)2 * P * sizeof(double)                 // gathered sums r, own E^-1 row
+inline size_t fcg_smem_bytes(int P, int C, int WL, int NB) {
+  return (size_t)(1 + NB) * P * sizeof(double)          // gathered sums r, E^-1 rows of the slots
          + (size_t)FCG_NG * P * sizeof(double)           // gather landing area
          + (size_t)3 * C * sizeof(double)                // own x, p, q
          + (size_t)C * sizeof(float)                     // own 1/diag (FP32, smoother)
@@ -189,8 +196,8 @@ __global__ void __launch_bounds__(FCG_TPB, 1) k_fcg(FcgArgs a, int WA) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int P = a.P, C = a.C, WL = a.WL, n = a.n;
   double* s_c = reinterpret_cast<double*>(smem);          // [P] c = Z^T r
-  double* s_er = s_c + P;                                  // [P] row b of E^-1
-  double* s_gat = s_er + P;                                // [NG][P]
+  double* s_er = s_c + P;                                  // [NB][P] E^-1 rows of this part's slots
+  double* s_gat = s_er + (size_t)a.NB * P;                 // [NG][P]
   double* s_x = s_gat + FCG_NG * P;                        // [C] own x
   double* s_p = s_x + C;                                   // [C] own p
   double* s_q = s_p + C;                                   // [C] own q
@@ -198,7 +205,7 @@ __global__ void __launch_bounds__(FCG_TPB, 1) k_fcg(FcgArgs a, int WA) {
   unsigned* s_lpk = reinterpret_cast<unsigned*>(s_dinv + C);  // [WL][C]
   float* s_d0 = reinterpret_cast<float*>(s_lpk + (size_t)WL * C);  // [C]
   float* s_d1 = s_d0 + C;                                  // [C]
-  __shared__ double s_y;
+  __shared__ double s_yn[32];  // coarse values of this part's slots (slot 0 = own part)
 
   constexpr int LW = WT > 0 ? WT - 1 : 16;  // unrolled bound of the local row width
   const int b = blockIdx.x;
@@ -209,7 +216,7 @@ __global__ void __launch_bounds__(FCG_TPB, 1) k_fcg(FcgArgs a, int WA) {
   // ---- stage the part's local operator and E^-1 row
   for (int s = 0; s < WL; ++s)
     for (int l = threadIdx.x; l < size; l += blockDim.x) s_lpk[s * C + l] = a.lpk[(size_t)s * n + base + l];
-  for (int j = threadIdx.x; j < P; j += blockDim.x) s_er[j] = a.einv[(size_t)b * P + j];
+  for (int j = threadIdx.x; j < a.NB * P; j += blockDim.x) s_er[j] = a.einv_nb[(size_t)b * a.NB * P + j];
 
   // own-cell state: r in registers; x, p, q and the FP32 1/diag in shared memory
   double rr[CPT];
@@ -267,20 +274,33 @@ __global__ void __launch_bounds__(FCG_TPB, 1) k_fcg(FcgArgs a, int WA) {
   while (!reason) {
     if (its >= a.maxit) { reason = -3; break; }
     __syncthreads();  // s_c complete
-    // ---- coarse value of this part: y_b = sum_j E^-1[b][j] c[j]
-    if (threadIdx.x < 32) {
-      double s = 0.0;
-      for (int j = threadIdx.x; j < P; j += 32) s += s_er[j] * s_c[j];
-      for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-      if (threadIdx.x == 0) s_y = s;
+    // ---- coarse values y = E^-1 c of this part and its neighbour parts (warp w: slot w)
+    {
+      const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+      if (w < a.NB) {
+        double s = 0.0;
+        for (int j = lane; j < P; j += 32) s += s_er[(size_t)w * P + j] * s_c[j];
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+        if (lane == 0) s_yn[w] = s;
+      }
     }
+    __syncthreads();
+    const double yb = s_yn[0];
     // ---- part-local Chebyshev on D^-1 A_bb z = D^-1 r (FP32, shared memory).  With the
     // scaled residual s = D^-1 (r - A_bb z):  z += d;  s -= D^-1 A_bb d = d + sum a~_ij d_j;
     // d = c1 d + c2 s  (Saad, Iterative Methods, alg. 12.1, on the Jacobi-scaled operator).
     float zc[CPT], sc[CPT], dc[CPT];
 #pragma unroll
     for (int k = 0; k < CPT; ++k) {
-      sc[k] = OWN(k) ? s_dinv[threadIdx.x + k * FCG_TPB] * (float)rr[k] : 0.0f;
+      double rk = rr[k];
+      if (a.deflate && OWN(k)) {  // r - (A Z y)_i
+        const int i = base + threadIdx.x + k * FCG_TPB;
+        double azy = yb * (double)__ldg(&a.srow[i]);
+        const int e1 = __ldg(&a.xoff[i + 1]);
+        for (int e = __ldg(&a.xoff[i]); e < e1; ++e) azy += (double)__ldg(&a.xval[e]) * s_yn[__ldg(&a.xslot[e])];
+        rk -= azy;
+      }
+      sc[k] = OWN(k) ? s_dinv[threadIdx.x + k * FCG_TPB] * (float)rk : 0.0f;
       dc[k] = sc[k] / th;
       zc[k] = 0.0f;
     }
@@ -314,8 +334,7 @@ __global__ void __launch_bounds__(FCG_TPB, 1) k_fcg(FcgArgs a, int WA) {
       rho = rhon;
       float* t = dcur; dcur = dnext; dnext = t;
     }
-    __syncthreads();  // s_y visible
-    const double yb = s_y;
+    __syncthreads();
     // ---- z to global, barrier, w = A z and the sums
     double rz[CPT];
 #pragma unroll

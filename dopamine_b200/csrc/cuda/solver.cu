@@ -638,8 +638,8 @@ struct Solver {
     if (rc) return DPM_ERR_UNSUPPORTED;
     int cpt = 0;
     fcg_kernel = fcg_kernel_for(T.C, T.WA, &cpt);
-    fcg_smem = fcg_smem_bytes(T.P, T.C, T.WL);
-    if (!fcg_kernel || fcg_smem > 200 * 1024) return DPM_ERR_UNSUPPORTED;
+    fcg_smem = fcg_smem_bytes(T.P, T.C, T.WL, T.NB);
+    if (!fcg_kernel || fcg_smem > 219 * 1024) return DPM_ERR_UNSUPPORTED;
     CK(cudaFuncSetAttribute(fcg_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fcg_smem));
     int per_sm = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fcg_kernel, FCG_TPB, fcg_smem));
@@ -651,7 +651,13 @@ struct Solver {
     fa.val = mem.upload(T.val);
     fa.dinv = mem.upload(T.dinv);
     fa.lpk = mem.upload(T.lpk);
-    fa.einv = mem.upload(T.einv);
+    fa.einv_nb = mem.upload(T.einv_nb);
+    fa.NB = T.NB;
+    fa.deflate = T.deflate;
+    fa.srow = mem.upload(T.srow);
+    fa.xoff = mem.upload(T.xoff);
+    fa.xslot = mem.upload(T.xslot);
+    fa.xval = mem.upload(T.xval);
     fa.xs = mem.alloc<double>(nc);
     fa.zs = mem.alloc<double>(nc);
     fa.partials = mem.alloc<double>((size_t)2 * FCG_SLOT * T.P);

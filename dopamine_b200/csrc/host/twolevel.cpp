@@ -161,6 +161,70 @@ int build_two_level(int n, int WA, const int* A_col, const double* A_val, const 
     }
     for (int i = 0; i < P; ++i) T.einv[(size_t)i * P + k] = y[i];
   }
+  // ---- deflation data
+  std::vector<std::vector<int>> nb_of(P);
+  for (int i = 0; i < n; ++i) {
+    const int b = i / C;
+    for (int w = 0; w < WA; ++w) {
+      const double v = T.val[(size_t)w * n + i];
+      const int j = T.col[(size_t)w * n + i];
+      if (v != 0.0 && j / C != b) nb_of[b].push_back(j / C);
+    }
+  }
+  int NB = 1;
+  for (int b = 0; b < P; ++b) {
+    auto& l = nb_of[b];
+    std::sort(l.begin(), l.end());
+    l.erase(std::unique(l.begin(), l.end()), l.end());
+    NB = std::max<int>(NB, 1 + (int)l.size());
+  }
+  T.srow.assign(n, 0.0f);
+  T.xoff.assign(n + 1, 0);
+  if (NB <= 32) {
+    T.deflate = 1;
+    T.NB = NB;
+    T.nbr.assign((size_t)P * NB, -1);
+    T.einv_nb.assign((size_t)P * NB * P, 0.0);
+    for (int b = 0; b < P; ++b) {
+      T.nbr[(size_t)b * NB] = b;
+      for (size_t s = 0; s < nb_of[b].size(); ++s) T.nbr[(size_t)b * NB + 1 + s] = nb_of[b][s];
+      for (int s = 0; s < NB; ++s) {
+        const int q = T.nbr[(size_t)b * NB + s];
+        if (q >= 0)
+          std::copy(T.einv.begin() + (size_t)q * P, T.einv.begin() + (size_t)(q + 1) * P,
+                    T.einv_nb.begin() + ((size_t)b * NB + s) * P);
+      }
+    }
+    for (int i = 0; i < n; ++i) {
+      const int b = i / C;
+      double sr = 0.0;
+      for (int w = 0; w < WA; ++w) {
+        const double v = T.val[(size_t)w * n + i];
+        const int j = T.col[(size_t)w * n + i];
+        if (v == 0.0) continue;
+        if (j / C == b) {
+          sr += v;
+        } else {
+          const auto& l = nb_of[b];
+          const int s = 1 + (int)(std::lower_bound(l.begin(), l.end(), j / C) - l.begin());
+          T.xslot.push_back((unsigned char)s);
+          T.xval.push_back((float)v);
+        }
+      }
+      T.srow[i] = (float)sr;
+      T.xoff[i + 1] = (int)T.xval.size();
+    }
+  } else {
+    T.deflate = 0;
+    T.NB = 1;
+    T.nbr.assign(P, 0);
+    T.einv_nb = T.einv;
+    for (int b = 0; b < P; ++b) T.nbr[b] = b;
+  }
+  if (T.xval.empty()) {  // keep device arrays non-empty
+    T.xval.push_back(0.0f);
+    T.xslot.push_back(0);
+  }
   return 0;
 }
 

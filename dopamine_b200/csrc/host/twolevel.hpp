@@ -26,6 +26,17 @@ struct TwoLevel {
   // padded to WL entries with (own local index, 0)
   std::vector<unsigned> lpk;      // [WL][n]
   std::vector<double> einv;       // [P][P] inverse (or regularised inverse) of E
+  // Deflation of the coarse correction before smoothing: z = y_b + S_b(r - A Z y).  (A Z y)_i
+  // needs y of the parts next to i's part: NB slots per part (slot 0 = the part itself, then its
+  // neighbour parts), the E^-1 rows of those slots, and per cell the intra-part row sum and the
+  // cross-part couplings (slot, value).  deflate = 0 when a part has more than 31 neighbours.
+  int deflate = 0, NB = 1;
+  std::vector<int> nbr;           // [P][NB] part ids, -1 padded
+  std::vector<double> einv_nb;    // [P][NB][P]
+  std::vector<float> srow;        // [n] sum of the row's entries inside the part (diagonal included)
+  std::vector<int> xoff;          // [n+1] cross-part couplings of row i: xoff[i] .. xoff[i+1]-1
+  std::vector<unsigned char> xslot;  // slot of the coupled cell's part in its own part's list
+  std::vector<float> xval;        // coupling value a_ij
 };
 
 // A in padded ELL [WA][n] (padding = (own row, 0)), cell centres xyz[3*n]; nullsp = the
