@@ -68,7 +68,17 @@ class StatsT(C.Structure):
         ("time", C.c_double), ("E", C.c_double), ("eps", C.c_double), ("Umax", C.c_double), ("Ub", C.c_double),
         ("tauw_mean", C.c_double), ("nu_sgs_mean", C.c_double), ("max_abs_divU", C.c_double),
         ("volavg_abs_divU", C.c_double), ("dt_used", C.c_double), ("p_solves", C.c_int), ("p_iters", C.c_int),
-        ("p_resid_max", C.c_double),
+        ("p_resid_max", C.c_double), ("p_fallbacks", C.c_int),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class LearnReportT(C.Structure):
+    _fields_ = [
+        ("samples", C.c_int), ("val_solves", C.c_int), ("loss_initial", C.c_double), ("loss_final", C.c_double),
+        ("gamma", C.c_float), ("its_val_base", C.c_int), ("its_val_learned", C.c_int), ("train_ms", C.c_double),
     ]
 
     def as_dict(self):

@@ -54,6 +54,15 @@ struct FcgArgs {
   double* dout;           // [0] true residual, [1] last ||r||, [2] ||b'||
   double rtol, atol;
   float theta, delta;     // Chebyshev interval [theta - delta, theta + delta] of D^-1 A_bb
+  // learned term gamma * omega .* D^-1 rho0 added to the smoother output (omega [n], new numbering)
+  const float* omega;
+  float gamma;
+  // training-sample recording: every rec_stride-th iteration, slot rec_base + its / rec_stride
+  // (< rec_max) receives r, the preconditioned residual z, u = D^-1 rho0 and x ([slot][n], new
+  // numbering).  rec_stride = 0: off.
+  int rec_stride, rec_base, rec_max;
+  double *rec_r, *rec_z, *rec_u, *rec_x;
+  int stall_window;       // > 0: stop with reason -20 when ||r|| fell by < 10 % over that many iterations
 };
 
 // Bounded grid barrier on the same monotonic counter as grid_allreduce (one arrival per block).
@@ -269,6 +278,7 @@ __global__ void __launch_bounds__(FCG_TPB, 1) k_fcg(FcgArgs a, int WA) {
   int reason = classify(dp, ttol, a.atol, rnorm0);
   int its = 0;
   double pq_old = 1.0;
+  double dp_mark = dp;
   const float th = a.theta, de = a.delta;
   const float sig = th / de;
   while (!reason) {
@@ -290,6 +300,8 @@ __global__ void __launch_bounds__(FCG_TPB, 1) k_fcg(FcgArgs a, int WA) {
     // scaled residual s = D^-1 (r - A_bb z):  z += d;  s -= D^-1 A_bb d = d + sum a~_ij d_j;
     // d = c1 d + c2 s  (Saad, Iterative Methods, alg. 12.1, on the Jacobi-scaled operator).
     float zc[CPT], sc[CPT], dc[CPT];
+    const bool rec_now = a.rec_stride > 0 && its % a.rec_stride == 0 && a.rec_base + its / a.rec_stride < a.rec_max;
+    const size_t rec_off = rec_now ? (size_t)(a.rec_base + its / a.rec_stride) * n : 0;
 #pragma unroll
     for (int k = 0; k < CPT; ++k) {
       double rk = rr[k];
@@ -303,6 +315,15 @@ __global__ void __launch_bounds__(FCG_TPB, 1) k_fcg(FcgArgs a, int WA) {
       sc[k] = OWN(k) ? s_dinv[threadIdx.x + k * FCG_TPB] * (float)rk : 0.0f;
       dc[k] = sc[k] / th;
       zc[k] = 0.0f;
+      if (OWN(k)) {
+        const int i = base + threadIdx.x + k * FCG_TPB;
+        if (a.gamma != 0.0f) zc[k] = a.gamma * __ldg(&a.omega[i]) * sc[k];
+        if (rec_now) {
+          a.rec_r[rec_off + i] = rr[k];
+          a.rec_u[rec_off + i] = (double)sc[k];
+          a.rec_x[rec_off + i] = s_x[threadIdx.x + k * FCG_TPB];
+        }
+      }
     }
     float rho = 1.0f / sig;
     float* dcur = s_d0;
@@ -340,7 +361,10 @@ __global__ void __launch_bounds__(FCG_TPB, 1) k_fcg(FcgArgs a, int WA) {
 #pragma unroll
     for (int k = 0; k < CPT; ++k) {
       rz[k] = (double)zc[k] + yb;
-      if (OWN(k)) a.zs[base + threadIdx.x + k * FCG_TPB] = rz[k];
+      if (OWN(k)) {
+        a.zs[base + threadIdx.x + k * FCG_TPB] = rz[k];
+        if (rec_now) a.rec_z[rec_off + base + threadIdx.x + k * FCG_TPB] = rz[k];
+      }
     }
     if (!grid_barrier(a.bar, gen, a.status)) return;
     double v[FCG_NV + FCG_NG], t[FCG_NV];
@@ -371,6 +395,10 @@ __global__ void __launch_bounds__(FCG_TPB, 1) k_fcg(FcgArgs a, int WA) {
     dp = sqrt(t[4]);
     reason = classify(dp, ttol, a.atol, rnorm0);
     if (reason) break;
+    if (a.stall_window > 0 && its > 0 && its % a.stall_window == 0) {  // automatic fallback trigger
+      if (dp > 0.9 * dp_mark) { reason = -20; break; }
+      dp_mark = dp;
+    }
     const double m = a.nullsp ? t[3] / (double)n : 0.0;
     const double zr = t[0] - m * t[5], zq = t[1] - m * t[6], zw = t[2] - m * t[7];
     const double beta = its == 0 ? 0.0 : -zq / pq_old;

@@ -24,6 +24,7 @@
 #include "common.cuh"
 #include "fcg.cuh"
 #include "kernels.cuh"
+#include "learn.cuh"
 #include "pcg.cuh"
 #include "scalars.cuh"
 
@@ -185,6 +186,18 @@ struct Solver {
   double *sc_fadv = nullptr, *sc_fdif = nullptr, *bTval = nullptr, *bsval = nullptr;
   int* bsmode = nullptr;
   double *most_L = nullptr, *most_qw = nullptr;  // MOST per-face Obukhov length and heat flux
+  // learned term of the two-level preconditioner (learn.cuh)
+  int lp_S = 32, lp_count = 0, lp_stride = 10, lp_val_lo = 0;
+  bool lp_recording = false, lp_ready = false;
+  float lp_gamma = 0.0f;
+  float *lp_feat = nullptr, *lp_omega = nullptr, *lp_h1 = nullptr, *lp_h2 = nullptr, *lp_pre = nullptr,
+        *lp_dom = nullptr, *lp_prm = nullptr, *lp_m1 = nullptr, *lp_m2 = nullptr, *lp_grad = nullptr,
+        *lp_gpart = nullptr;
+  unsigned short* lp_wb = nullptr;
+  double *lp_r = nullptr, *lp_z = nullptr, *lp_u = nullptr, *lp_x = nullptr, *lp_azb = nullptr, *lp_av = nullptr,
+         *lp_dpart = nullptr, *lp_dsum = nullptr, *lp_coef = nullptr;
+  std::vector<int> lp_solve_of;  // solve index of each recorded slot
+  int lp_solves = 0, p_fallbacks = 0;
   // two-level flexible CG (p_solver == DPM_PSOLVER_TWOLEVEL_FCG)
   bool use_fcg = false;
   FcgArgs fa{};
@@ -671,14 +684,100 @@ struct Solver {
     fa.delta = (float)(0.5 * (lmax - lmin));
     fcg_WA = T.WA;
     if (!fa.partials || !fa.zs) return DPM_ERR_CUDA;
+    fa.stall_window = 50;
     use_fcg = true;
+    return setup_learned(T);
+  }
+
+  // Static per-cell features of the learned term, in the renumbered order:
+  // [1, intra-part coupling mass, cross-part coupling mass, max and min scaled coupling,
+  //  intra row-sum ratio, log diagonal scale, intra neighbour count / 6].
+  int setup_learned(const TwoLevel& T) {
+    const int n = T.n;
+    std::vector<float> f((size_t)LP_F * n, 0.0f);
+    double lmean = 0.0;
+    for (int i = 0; i < n; ++i) lmean += std::log(1.0 / T.dinv[i]);
+    lmean /= std::max(n, 1);
+    for (int i = 0; i < n; ++i) {
+      const int b = i / T.C;
+      double intra = 0.0, cross = 0.0, mx = 0.0, mn = 1e300;
+      int cnt = 0;
+      for (int w = 0; w < T.WA; ++w) {
+        const double v = T.val[(size_t)w * n + i];
+        const int j = T.col[(size_t)w * n + i];
+        if (v == 0.0 || j == i) continue;
+        const double sv = std::fabs(v) * T.dinv[i];
+        if (j / T.C == b) { intra += sv; cnt++; } else { cross += sv; }
+        mx = std::max(mx, sv);
+        mn = std::min(mn, sv);
+      }
+      if (mn > 1e299) mn = 0.0;
+      f[0 * (size_t)n + i] = 1.0f;
+      f[1 * (size_t)n + i] = (float)intra;
+      f[2 * (size_t)n + i] = (float)cross;
+      f[3 * (size_t)n + i] = (float)mx;
+      f[4 * (size_t)n + i] = (float)mn;
+      f[5 * (size_t)n + i] = (float)(T.srow[i] * T.dinv[i]);
+      f[6 * (size_t)n + i] = (float)((std::log(1.0 / T.dinv[i]) - lmean) / 5.0);
+      f[7 * (size_t)n + i] = (float)(cnt / 6.0);
+    }
+    lp_feat = mem.upload(f);
+    lp_omega = mem.alloc<float>(n);
+    lp_h1 = mem.alloc<float>((size_t)LP_H * n); lp_h2 = mem.alloc<float>((size_t)LP_H * n);
+    lp_pre = mem.alloc<float>(n); lp_dom = mem.alloc<float>(n);
+    lp_prm = mem.alloc<float>(LP_NP); lp_m1 = mem.alloc<float>(LP_NP); lp_m2 = mem.alloc<float>(LP_NP);
+    lp_grad = mem.alloc<float>(LP_NP);
+    lp_wb = mem.alloc<unsigned short>(LP_NP);
+    lp_gpart = mem.alloc<float>((size_t)LP_BWD_BLOCKS * LP_NP);
+    if (!lp_feat || !lp_omega || !lp_h1 || !lp_h2 || !lp_pre || !lp_dom || !lp_prm || !lp_wb || !lp_gpart)
+      return DPM_ERR_CUDA;
+    std::vector<float> p0 = lp_initial_params();
+    CK(cudaMemcpyAsync(lp_prm, p0.data(), sizeof(float) * LP_NP, cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(lp_m1, 0, sizeof(float) * LP_NP, st));
+    CK(cudaMemsetAsync(lp_m2, 0, sizeof(float) * LP_NP, st));
+    k_lp_round<<<(LP_NP + 255) / 256, 256, 0, st>>>(LP_NP, lp_prm, lp_wb);
+    launch_fill_f(lp_omega, n, 0.0f);
+    launches++;
+    fa.omega = lp_omega;
+    fa.gamma = 0.0f;
     return 0;
+  }
+  static constexpr int LP_BWD_BLOCKS = 296;
+  // Deterministic initial parameters: uniform in +-1/sqrt(fan_in) from SplitMix64, output bias -4
+  // so that omega starts near zero.
+  static std::vector<float> lp_initial_params() {
+    std::vector<float> p(LP_NP, 0.0f);
+    uint64_t x = 0x5EEDULL;
+    auto uni = [&]() {
+      x += 0x9E3779B97F4A7C15ULL;
+      uint64_t z = x;
+      z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+      z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+      z ^= z >> 31;
+      return (double)(z >> 11) * (1.0 / 9007199254740992.0) * 2.0 - 1.0;
+    };
+    for (int j = 0; j < 256; ++j) p[LP_W1 + j] = (float)(uni() * 0.25);
+    for (int j = 0; j < 256; ++j) p[LP_W2 + j] = (float)(uni() * 0.25);
+    for (int j = 0; j < 16; ++j) p[LP_W3 + j] = (float)(uni() * 0.25);
+    p[LP_B3] = -4.0f;
+    return p;
+  }
+  void launch_fill_f(float* q, int64_t m, float v) {
+    k_fill_f<<<nblk(m), TPB, 0, st>>>((int)m, q, v);
+    launches++;
   }
 
   int fcg(const double* rhs, double* x, double rtol, double atol, int maxit, int guess_zero, int* its, double* resid,
           int* reason) {
     FcgArgs a = fa;
     a.b = rhs; a.x = x; a.rtol = rtol; a.atol = atol; a.maxit = maxit; a.guess_zero = guess_zero;
+    a.gamma = lp_ready ? lp_gamma : 0.0f;
+    const bool rec = lp_recording && lp_count < lp_S;
+    if (rec) {
+      a.gamma = 0.0f;
+      a.rec_stride = lp_stride; a.rec_base = lp_count; a.rec_max = lp_S;
+      a.rec_r = lp_r; a.rec_z = lp_z; a.rec_u = lp_u; a.rec_x = lp_x;
+    }
     CK(cudaMemsetAsync(cg_bar, 0, 2 * sizeof(unsigned), st));
     CK(cudaMemsetAsync(cg_status, 0, 4 * sizeof(int), st));
     int wa = fcg_WA;
@@ -697,6 +796,172 @@ struct Solver {
     *reason = h_st[0];
     *its = h_st[1];
     *resid = h_d[0];
+    if (rec) {  // errors of the recorded iterates: e = x* - x_k (x* = the solve's final xs)
+      const int used = std::min(lp_S - lp_count, *its / lp_stride + 1);
+      if (used > 0) {
+        dim3 g(nblk(nc), used);
+        k_lp_err<<<g, TPB, 0, st>>>(nc, fa.xs, lp_x + (size_t)lp_count * nc);
+        launches++;
+        for (int k = 0; k < used; ++k) lp_solve_of.push_back(lp_solves);
+        lp_count += used;
+      }
+      lp_solves++;
+    }
+    return 0;
+  }
+
+  // ---------------------------------------------------------------- learned term: training
+  static constexpr int LP_DOT_BLOCKS = 64;
+  int learn_alloc() {
+    if (lp_r) return 0;
+    const size_t m = (size_t)lp_S * nc;
+    lp_r = mem.alloc<double>(m); lp_z = mem.alloc<double>(m); lp_u = mem.alloc<double>(m);
+    lp_x = mem.alloc<double>(m); lp_azb = mem.alloc<double>(m); lp_av = mem.alloc<double>(m);
+    lp_dpart = mem.alloc<double>((size_t)lp_S * LP_DOT_BLOCKS * 3);
+    lp_dsum = mem.alloc<double>((size_t)lp_S * 3);
+    lp_coef = mem.alloc<double>((size_t)lp_S * 2);
+    return (lp_r && lp_z && lp_u && lp_x && lp_azb && lp_av && lp_dpart && lp_dsum && lp_coef) ? 0 : DPM_ERR_CUDA;
+  }
+  // per-sample dot products {a.b} over the first S slots, to the host
+  int lp_dots(int S, const double* A1, const double* B1, const double* A2, const double* B2, const double* A3,
+              const double* B3, std::vector<double>& out) {
+    k_lp_dots3<<<dim3(LP_DOT_BLOCKS, S), 256, 0, st>>>(nc, A1, B1, A2, B2, A3, B3, lp_dpart);
+    k_lp_sum_samples<<<(3 * S + 127) / 128, 128, 0, st>>>(S, LP_DOT_BLOCKS, lp_dpart, lp_dsum);
+    launches += 2;
+    out.resize(3 * S);
+    CK(cudaMemcpyAsync(out.data(), lp_dsum, sizeof(double) * 3 * S, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return 0;
+  }
+  void lp_forward() {
+    k_lp_forward<<<(nc + 127) / 128, 256, 0, st>>>(nc, fa.C, fa.WL, fa.lpk, lp_feat, lp_wb, lp_prm, lp_omega, lp_h1,
+                                                   lp_h2, lp_pre);
+    launches++;
+  }
+  // Loss over the first S slots at the current parameters; with grad, the parameter gradient
+  // (into lp_grad).  base = {z.r, z.A z, e.r} per slot.
+  int lp_loss_grad(int S, const std::vector<double>& base, double* loss, bool grad) {
+    lp_forward();
+    k_lp_av<<<dim3(nblk(nc), S), 256, 0, st>>>(nc, fcg_WA, S, fa.col, fa.val, lp_omega, lp_u, lp_av);
+    k_lp_dots<<<dim3(LP_DOT_BLOCKS, S), 256, 0, st>>>(nc, S, lp_omega, lp_u, lp_r, lp_azb, lp_av, lp_dpart);
+    k_lp_sum_samples<<<(3 * S + 127) / 128, 128, 0, st>>>(S, LP_DOT_BLOCKS, lp_dpart, lp_dsum);
+    launches += 3;
+    std::vector<double> q(3 * S), coef(2 * S);
+    CK(cudaMemcpyAsync(q.data(), lp_dsum, sizeof(double) * 3 * S, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    double L = 0.0;
+    for (int k = 0; k < S; ++k) {
+      const double a = base[3 * k] + q[3 * k];
+      const double b = base[3 * k + 1] + 2.0 * q[3 * k + 1] + q[3 * k + 2];
+      const double c = base[3 * k + 2];
+      const double bc = std::max(b * c, 1e-300);
+      L += 1.0 - a * a / bc;
+      coef[2 * k] = 2.0 * a / bc;
+      coef[2 * k + 1] = 2.0 * a * a / (bc * std::max(b, 1e-300));
+    }
+    *loss = L / S;
+    if (!grad) return 0;
+    CK(cudaMemcpyAsync(lp_coef, coef.data(), sizeof(double) * 2 * S, cudaMemcpyHostToDevice, st));
+    k_lp_domega<<<nblk(nc), 256, 0, st>>>(nc, S, lp_coef, lp_u, lp_r, lp_azb, lp_av, lp_dom);
+    k_lp_backward<<<LP_BWD_BLOCKS, 128, 0, st>>>(nc, fa.C, fa.WL, fa.lpk, lp_feat, lp_wb, lp_prm, lp_h1, lp_h2, lp_pre,
+                                                 lp_dom, lp_gpart);
+    k_lp_sum_f<<<(LP_NP + 127) / 128, 128, 0, st>>>(LP_BWD_BLOCKS, LP_NP, lp_gpart, lp_grad);
+    launches += 3;
+    return 0;
+  }
+  int lp_train_slots() const {  // slots of all but the last recorded solve (that one is held out)
+    if (lp_count == 0) return 0;
+    const int last = lp_solve_of.back();
+    int k = 0;
+    while (k < lp_count && lp_solve_of[k] < last) ++k;
+    return k > 0 ? k : lp_count;
+  }
+  int lp_prepare(int S, std::vector<double>& base) {
+    k_lp_spmv<<<dim3(nblk(nc), S), 256, 0, st>>>(nc, fcg_WA, fa.col, fa.val, lp_z, lp_azb);
+    launches++;
+    return lp_dots(S, lp_z, lp_r, lp_z, lp_azb, lp_x, lp_r, base);  // lp_x holds e after recording
+  }
+  // Held-out solves: the right-hand side recorded at iteration 0 of each held-out solve (its x0 is
+  // 0), solved again from zero with the learned term scaled by g; total iterations.
+  int lp_validate(float g, int* its_total) {
+    *its_total = 0;
+    const float keep = lp_gamma;
+    const bool keep_ready = lp_ready;
+    lp_gamma = g;
+    lp_ready = true;
+    for (int k = lp_train_slots(); k < lp_count; ++k) {
+      if (k > 0 && lp_solve_of[k] == lp_solve_of[k - 1]) continue;  // first slot of each held-out solve
+      k_perm_scatter<<<nblk(nc), TPB, 0, st>>>(nc, fa.perm, lp_r + (size_t)k * nc, scratch_c);
+      launch_fill(scratch_c2, nc, 0.0);
+      launches++;
+      int its = 0, reason = 0;
+      double res = 0.0;
+      int rc = fcg(scratch_c, scratch_c2, P.p_tol, 1e-300, 2000, 1, &its, &res, &reason);
+      if (rc) return rc;
+      *its_total += its + (reason < 0 ? 100000 : 0);
+    }
+    lp_gamma = keep;
+    lp_ready = keep_ready;
+    return 0;
+  }
+  int learn_collect(int n_steps, int* n_samples) {
+    if (!use_fcg) return DPM_ERR_UNSUPPORTED;
+    int rc = learn_alloc();
+    if (rc) return rc;
+    lp_count = 0;
+    lp_solves = 0;
+    lp_solve_of.clear();
+    lp_recording = true;
+    for (int k = 0; k < n_steps && rc == 0; ++k) rc = advance(P.dt);
+    lp_recording = false;
+    if (n_samples) *n_samples = lp_count;
+    return rc;
+  }
+  int learn_train(int epochs, double lr, dpm_learn_report_t* rep) {
+    if (!use_fcg || lp_count == 0) return DPM_ERR_ARG;
+    auto t0 = std::chrono::steady_clock::now();
+    const int S = lp_train_slots();
+    std::vector<double> base;
+    int rc = lp_prepare(S, base);
+    if (rc) return rc;
+    double L0 = 0.0, L = 0.0;
+    rc = lp_loss_grad(S, base, &L0, false);
+    if (rc) return rc;
+    for (int e = 1; e <= epochs; ++e) {
+      rc = lp_loss_grad(S, base, &L, true);
+      if (rc) return rc;
+      k_lp_adam<<<(LP_NP + 127) / 128, 128, 0, st>>>(LP_NP, lp_prm, lp_m1, lp_m2, lp_grad, (float)lr, 0.9f, 0.999f,
+                                                    1e-8f, e, lp_wb);
+      launches++;
+    }
+    rc = lp_loss_grad(S, base, &L, false);  // final loss, omega of the trained network
+    if (rc) return rc;
+    // gate: the scale of the learned term that does best on the held-out solves (ties keep 0)
+    const float cand[3] = {0.0f, 0.5f, 1.0f};
+    int best_its = 0, its0 = 0;
+    float best = 0.0f;
+    for (int c = 0; c < 3; ++c) {
+      int its = 0;
+      rc = lp_validate(cand[c], &its);
+      if (rc) return rc;
+      if (c == 0) { its0 = its; best_its = its; }
+      else if (its < best_its) { best_its = its; best = cand[c]; }
+    }
+    lp_gamma = best;
+    lp_ready = true;
+    auto t1 = std::chrono::steady_clock::now();
+    if (rep) {
+      rep->samples = S;
+      rep->val_solves = 0;
+      for (int k = S; k < lp_count; ++k)
+        if (k == S || lp_solve_of[k] != lp_solve_of[k - 1]) rep->val_solves++;
+      rep->loss_initial = L0;
+      rep->loss_final = L;
+      rep->gamma = best;
+      rep->its_val_base = its0;
+      rep->its_val_learned = best_its;
+      rep->train_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    }
     return 0;
   }
 
@@ -704,6 +969,10 @@ struct Solver {
   int pcg(const double* rhs, double* x, double rtol, double atol, int maxit, int guess_zero, int* its, double* resid,
           int* reason) {
     if (use_fcg) return fcg(rhs, x, rtol, atol, maxit, guess_zero, its, resid, reason);
+    return pcg_plain(rhs, x, rtol, atol, maxit, guess_zero, its, resid, reason);
+  }
+  int pcg_plain(const double* rhs, double* x, double rtol, double atol, int maxit, int guess_zero, int* its,
+                double* resid, int* reason) {
     PcgArgs<double> a{};
     a.n = nc; a.WA = S.WA; a.col = d.Acol; a.val = d.Aval; a.dinv = d.Adinv;
     a.b = rhs; a.x = x; a.r = cg_r; a.z = cg_z; a.p0 = cg_p0; a.p1 = cg_p1; a.q = cg_q; a.bp = cg_bp;
@@ -747,8 +1016,15 @@ struct Solver {
     cudaEventRecord(evp0, st);
     int rc = pcg(rhs, F.p, tol, atol, maxit, 0, &its, &res, &reason);
     if (rc) return rc;
+    if (reason < 0 && use_fcg) {  // flexible CG stalled or failed: plain Jacobi-PCG takes over from its x
+      p_fallbacks++;
+      int its2 = 0;
+      rc = pcg_plain(rhs, F.p, tol, atol, maxit, 0, &its2, &res, &reason);
+      if (rc) return rc;
+      its += its2;
+    }
     if (reason < 0) {
-      rc = pcg(rhs, F.p, tol, atol, 4 * maxit, 1, &its, &res, &reason);
+      rc = pcg_plain(rhs, F.p, tol, atol, 4 * maxit, 1, &its, &res, &reason);
       if (rc) return rc;
       if (reason < 0 && !(reason == -3 && (res < tol * 1.0e4 || res < atol * 1.0e3))) return -(1000 + reason);
     }
@@ -997,6 +1273,7 @@ struct Solver {
     s->max_abs_divU = o2[0];
     s->volavg_abs_divU = o2[1] / o2[2];
     s->dt_used = last.dt_used;
+    s->p_fallbacks = p_fallbacks;
     s->p_solves = last.p_solves;
     s->p_iters = last.p_iters;
     s->p_resid_max = last.p_resid_max;
@@ -1084,6 +1361,85 @@ int dpm_download_state(dpm_solver_t* h, double* U, double* p, double* T, double*
   if (nu_sgs) CK(cudaMemcpyAsync(nu_sgs, s.F.nu_sgs, sizeof(double) * s.nc, cudaMemcpyDeviceToHost, s.st));
   CK(cudaStreamSynchronize(s.st));
   return DPM_OK;
+}
+
+int dpm_learn_collect(dpm_solver_t* h, int n_steps, int* n_samples) {
+  if (!h || n_steps < 1) return DPM_ERR_ARG;
+  CK(cudaSetDevice(h->s->device));
+  return h->s->learn_collect(n_steps, n_samples);
+}
+
+int dpm_learn_train(dpm_solver_t* h, int epochs, double lr, dpm_learn_report_t* report) {
+  if (!h || epochs < 0 || !(lr > 0.0)) return DPM_ERR_ARG;
+  CK(cudaSetDevice(h->s->device));
+  return h->s->learn_train(epochs, lr, report);
+}
+
+int dpm_learn_set_gamma(dpm_solver_t* h, double gamma) {
+  if (!h || !(gamma >= 0.0)) return DPM_ERR_ARG;
+  Solver& s = *h->s;
+  if (!s.use_fcg) return DPM_ERR_UNSUPPORTED;
+  s.lp_gamma = (float)gamma;
+  s.lp_ready = true;
+  return DPM_OK;
+}
+
+int dpm_learn_sizes(dpm_solver_t* h, int* sizes) {
+  if (!h || !sizes) return DPM_ERR_ARG;
+  Solver& s = *h->s;
+  if (!s.use_fcg) return DPM_ERR_UNSUPPORTED;
+  sizes[0] = s.nc; sizes[1] = s.fa.C; sizes[2] = s.fa.WL; sizes[3] = s.fcg_WA;
+  sizes[4] = s.lp_train_slots(); sizes[5] = dpm::gpu::LP_F; sizes[6] = dpm::gpu::LP_NP;
+  return DPM_OK;
+}
+
+int dpm_learn_export(dpm_solver_t* h, float* feat, unsigned* lpk, int* col, double* val, double* R, double* Z,
+                     double* U, double* E, float* params) {
+  if (!h) return DPM_ERR_ARG;
+  Solver& s = *h->s;
+  if (!s.use_fcg) return DPM_ERR_UNSUPPORTED;
+  CK(cudaSetDevice(s.device));
+  const size_t n = s.nc, S = s.lp_train_slots();
+  auto cp = [&](void* dst, const void* src, size_t bytes) -> int {
+    if (dst && src && bytes) CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s.st));
+    return 0;
+  };
+  cp(feat, s.lp_feat, sizeof(float) * dpm::gpu::LP_F * n);
+  cp(lpk, s.fa.lpk, sizeof(unsigned) * s.fa.WL * n);
+  cp(col, s.fa.col, sizeof(int) * s.fcg_WA * n);
+  cp(val, s.fa.val, sizeof(double) * s.fcg_WA * n);
+  cp(R, s.lp_r, sizeof(double) * S * n);
+  cp(Z, s.lp_z, sizeof(double) * S * n);
+  cp(U, s.lp_u, sizeof(double) * S * n);
+  cp(E, s.lp_x, sizeof(double) * S * n);
+  cp(params, s.lp_prm, sizeof(float) * dpm::gpu::LP_NP);
+  CK(cudaStreamSynchronize(s.st));
+  return DPM_OK;
+}
+
+int dpm_learn_loss_grad(dpm_solver_t* h, const float* params, double* loss, float* grad) {
+  if (!h || !loss) return DPM_ERR_ARG;
+  Solver& s = *h->s;
+  if (!s.use_fcg || s.lp_count == 0) return DPM_ERR_ARG;
+  CK(cudaSetDevice(s.device));
+  const int S = s.lp_train_slots();
+  std::vector<float> keep(dpm::gpu::LP_NP);
+  CK(cudaMemcpyAsync(keep.data(), s.lp_prm, sizeof(float) * keep.size(), cudaMemcpyDeviceToHost, s.st));
+  if (params) {
+    CK(cudaMemcpyAsync(s.lp_prm, params, sizeof(float) * dpm::gpu::LP_NP, cudaMemcpyHostToDevice, s.st));
+    dpm::gpu::k_lp_round<<<(dpm::gpu::LP_NP + 255) / 256, 256, 0, s.st>>>(dpm::gpu::LP_NP, s.lp_prm, s.lp_wb);
+  }
+  std::vector<double> base;
+  int rc = s.lp_prepare(S, base);
+  if (!rc) rc = s.lp_loss_grad(S, base, loss, grad != nullptr);
+  if (!rc && grad) CK(cudaMemcpyAsync(grad, s.lp_grad, sizeof(float) * dpm::gpu::LP_NP, cudaMemcpyDeviceToHost, s.st));
+  if (params) {  // leave the trained parameters as they were
+    CK(cudaMemcpyAsync(s.lp_prm, keep.data(), sizeof(float) * keep.size(), cudaMemcpyHostToDevice, s.st));
+    dpm::gpu::k_lp_round<<<(dpm::gpu::LP_NP + 255) / 256, 256, 0, s.st>>>(dpm::gpu::LP_NP, s.lp_prm, s.lp_wb);
+    s.lp_forward();
+  }
+  CK(cudaStreamSynchronize(s.st));
+  return rc;
 }
 
 int dpm_upload_scalars(dpm_solver_t* h, const double* C) {

@@ -25,6 +25,8 @@ EXPORTED = (
     "dpm_last_timing", "dpm_kernel_launches", "dpm_ls_gradient_vector", "dpm_advection_rhs_vector",
     "dpm_viscous_rhs_vector", "dpm_sgs_viscosity", "dpm_wall_model", "dpm_pcg_solve_noalloc",
     "dpm_advection_rhs_scalar", "dpm_viscous_rhs_scalar", "dpm_upload_scalars", "dpm_download_scalars",
+    "dpm_learn_collect", "dpm_learn_train", "dpm_learn_set_gamma", "dpm_learn_sizes", "dpm_learn_export",
+    "dpm_learn_loss_grad",
 )
 
 
@@ -71,6 +73,13 @@ def lib(build_if_missing=True):
     L.dpm_advection_rhs_scalar.argtypes = [vp, C.c_int, dp, dp, dp, dp, dp]
     L.dpm_viscous_rhs_scalar.argtypes = [vp, dp, C.c_double, dp, C.c_double, dp, dp, dp]
     L.dpm_upload_scalars.argtypes = [vp, dp]
+    fp = C.POINTER(C.c_float)
+    L.dpm_learn_collect.argtypes = [vp, C.c_int, ip]
+    L.dpm_learn_train.argtypes = [vp, C.c_int, C.c_double, C.POINTER(abi.LearnReportT)]
+    L.dpm_learn_set_gamma.argtypes = [vp, C.c_double]
+    L.dpm_learn_sizes.argtypes = [vp, ip]
+    L.dpm_learn_export.argtypes = [vp, fp, C.c_void_p, ip, dp, dp, dp, dp, dp, fp]
+    L.dpm_learn_loss_grad.argtypes = [vp, fp, dp, fp]
     L.dpm_download_scalars.argtypes = [vp, dp]
     L.fvm_petsc_solve_pressure.argtypes = [C.c_int, C.c_int, C.c_int, ip, ip, ip, ip, ip, dp, dp, dp, C.c_int,
                                            C.c_int, C.c_double, C.c_double, ip, dp, C.c_int, dp, ip, dp]
@@ -245,6 +254,44 @@ class Solver:
         """C [n_scalars, nc]."""
         Cf = np.ascontiguousarray(np.asarray(C, dtype=np.float64).T)
         _check(lib().dpm_upload_scalars(self.h, _p(Cf)), "dpm_upload_scalars")
+
+    # ---- learned term of the two-level preconditioner
+    def learn_collect(self, n_steps):
+        k = C.c_int(0)
+        _check(lib().dpm_learn_collect(self.h, n_steps, C.byref(k)), "dpm_learn_collect")
+        return k.value
+
+    def learn_train(self, epochs=100, lr=1e-2):
+        rep = abi.LearnReportT()
+        _check(lib().dpm_learn_train(self.h, epochs, lr, C.byref(rep)), "dpm_learn_train")
+        return rep.as_dict()
+
+    def learn_set_gamma(self, gamma):
+        _check(lib().dpm_learn_set_gamma(self.h, gamma), "dpm_learn_set_gamma")
+
+    def learn_export(self):
+        sz = (C.c_int * 7)()
+        _check(lib().dpm_learn_sizes(self.h, sz), "dpm_learn_sizes")
+        n, Cp, WL, WA, S, F, NP = (int(v) for v in sz)
+        out = dict(n=n, C=Cp, WL=WL, WA=WA, S=S, feat=np.zeros((F, n), dtype=np.float32),
+                   lpk=np.zeros((WL, n), dtype=np.uint32), col=np.zeros((WA, n), dtype=np.int32),
+                   val=np.zeros((WA, n)), R=np.zeros((S, n)), Z=np.zeros((S, n)), U=np.zeros((S, n)),
+                   E=np.zeros((S, n)), params=np.zeros(NP, dtype=np.float32))
+        fp = C.POINTER(C.c_float)
+        _check(lib().dpm_learn_export(self.h, out["feat"].ctypes.data_as(fp), out["lpk"].ctypes.data_as(C.c_void_p),
+                                      out["col"].ctypes.data_as(C.POINTER(C.c_int)), _p(out["val"]), _p(out["R"]),
+                                      _p(out["Z"]), _p(out["U"]), _p(out["E"]), out["params"].ctypes.data_as(fp)),
+               "dpm_learn_export")
+        return out
+
+    def learn_loss_grad(self, params=None):
+        fp = C.POINTER(C.c_float)
+        loss = C.c_double(0.0)
+        grad = np.zeros(561, dtype=np.float32)
+        pa = None if params is None else np.ascontiguousarray(params, dtype=np.float32)
+        _check(lib().dpm_learn_loss_grad(self.h, None if pa is None else pa.ctypes.data_as(fp), C.byref(loss),
+                                         grad.ctypes.data_as(fp)), "dpm_learn_loss_grad")
+        return loss.value, grad
 
     def wall_model(self, U, nu):
         tau = np.zeros((self.nb, 3))

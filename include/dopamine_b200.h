@@ -143,7 +143,17 @@ typedef struct dpm_stats {
   double dt_used;
   int p_solves, p_iters;
   double p_resid_max;
+  int p_fallbacks;            /* pressure solves handed from flexible CG to plain PCG (total)   */
 } dpm_stats_t;
+
+/* Outcome of dpm_learn_train. */
+typedef struct dpm_learn_report {
+  int samples, val_solves;    /* training samples; held-out solves used to set gamma            */
+  double loss_initial, loss_final;  /* A-angle loss over the samples before / after training    */
+  float gamma;                /* scale of the learned term kept (0: the term is switched off)   */
+  int its_val_base, its_val_learned;  /* held-out iterations with gamma = 0 and with gamma      */
+  double train_ms;
+} dpm_learn_report_t;
 
 /* ---------------------------------------------------------------------------------------- */
 /* 1. Pressure-solve seam (src/solver/pressure_backend_petsc.c)                              */
@@ -248,6 +258,31 @@ int dpm_viscous_rhs_scalar(dpm_solver_t* s, const double* phi, double alpha, con
 /* Passive scalars C(n_scalars, n) in the reference's Fortran layout (src/solver/mod_fv_solver.f90:326,
  * scalar index fastest); the temperature travels with dpm_upload_state / dpm_download_state. */
 int dpm_upload_scalars(dpm_solver_t* s, const double* C);
+
+/* ---- learned term of the two-level flexible-CG preconditioner (no counterpart in the
+ * reference).  A one-ring message-passing network (BF16 weights on tensor cores, FP32
+ * accumulate) maps static per-cell features of the pressure operator to omega_i >= 0, and the
+ * preconditioned residual gains gamma * omega .* D^-1 (r - A Z y).  Requires
+ * p_solver = DPM_PSOLVER_TWOLEVEL_FCG. */
+/* Advances n_steps time steps recording (residual, preconditioned residual, D^-1-scaled
+ * deflated residual, error) samples from the pressure solves (up to 32). */
+int dpm_learn_collect(dpm_solver_t* s, int n_steps, int* n_samples);
+/* Trains the network with Adam for `epochs` steps on all samples but those of the last recorded
+ * solve, then sets gamma in {0, 0.5, 1} by the held-out solves' iterations (0 kept on ties). */
+int dpm_learn_train(dpm_solver_t* s, int epochs, double lr, dpm_learn_report_t* report);
+/* Overrides gamma (0 switches the learned term off). */
+int dpm_learn_set_gamma(dpm_solver_t* s, double gamma);
+/* sizes[7] = {n_cells, cells per part, local row width, global row width, training samples,
+ * features per cell, parameters}. */
+int dpm_learn_sizes(dpm_solver_t* s, int* sizes);
+/* Copies the training problem to host buffers (renumbered order; any pointer may be NULL):
+ * features [F][n], packed local rows [WL][n], operator [WA][n], samples R, Z, U, E [S][n],
+ * current parameters [P]. */
+int dpm_learn_export(dpm_solver_t* s, float* feat, unsigned* lpk, int* col, double* val, double* R, double* Z,
+                     double* U, double* E, float* params);
+/* Loss and parameter gradient over the training samples at `params` (NULL: the current ones);
+ * the stored parameters are left unchanged. */
+int dpm_learn_loss_grad(dpm_solver_t* s, const float* params, double* loss, float* grad);
 int dpm_download_scalars(dpm_solver_t* s, double* C);
 
 /* ---- allocation-free Jacobi-PCG solve --------------------------------------------------------

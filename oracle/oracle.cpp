@@ -2148,6 +2148,7 @@ struct Solver {
     s->p_solves = last_solves;
     s->p_iters = last_iters;
     s->p_resid_max = last_resid;
+    s->p_fallbacks = 0;
     apply_velocity_bc(-1, false);  // solver_divergence_metrics refreshes U_bnd without gradients
   }
 };
@@ -2203,6 +2204,112 @@ void orc_get_state(void* h, double* U, double* p, double* nu_sgs, double* grad_U
   if (grad_U) std::memcpy(grad_U, s->grad_U.data(), sizeof(double) * 9 * s->nc);
   if (face_flux) std::memcpy(face_flux, s->U_face.data(), sizeof(double) * s->nf);
 }
+// ------------------------------------------------------------------------------------------
+// Learned term of the two-level preconditioner: loss and gradient in double, restating the
+// device network (dopamine_b200/csrc/cuda/learn.cuh) with its bf16 rounding points, for the
+// gradient check.  Network per cell: in = [bf16(f) ; bf16(sum_j a~_ij f_j)],
+// h1 = relu(W1b in + b1), h2 = relu(W2b bf16(h1) + b2), omega = 0.25 softplus(w3 . h2 + b3);
+// loss = mean_k 1 - (z.r)^2 / ((z.Az)(e.r)), z = zb + omega .* u.
+namespace {
+float orc_bf16(float x) {
+  uint32_t u;
+  std::memcpy(&u, &x, 4);
+  u += 0x7FFFu + ((u >> 16) & 1u);
+  u &= 0xFFFF0000u;
+  float y;
+  std::memcpy(&y, &u, 4);
+  return y;
+}
+}  // namespace
+int orc_lp_loss_grad(int n, int C, int WL, const uint32_t* lpk, const float* feat, int WA, const int* col,
+                     const double* val, int S, const double* R, const double* Z, const double* U, const double* E,
+                     const float* prm, double* loss, double* grad) {
+  const int F = 8, H = 16, W1 = 0, B1 = 256, W2 = 272, B2 = 528, W3 = 544, B3 = 560, NP = 561;
+  std::vector<double> wb(NP);
+  for (int j = 0; j < NP; ++j)
+    wb[j] = (j < B1 || (j >= W2 && j < B2)) ? (double)orc_bf16(prm[j]) : (double)prm[j];
+  std::vector<double> in((size_t)n * 16), h1((size_t)n * H), h2((size_t)n * H), pre(n), om(n);
+  for (int i = 0; i < n; ++i) {
+    const int base = (i / C) * C;
+    float agg[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int s2 = 0; s2 < WL; ++s2) {
+      const uint32_t e = lpk[(size_t)s2 * n + i];
+      uint32_t hb = e & 0xFFFF0000u;
+      float w;
+      std::memcpy(&w, &hb, 4);
+      if (w == 0.0f) continue;
+      const int j = base + (int)(e & 0xFFFFu);
+      for (int k = 0; k < F; ++k) agg[k] = std::fmaf(w, feat[(size_t)k * n + j], agg[k]);
+    }
+    for (int k = 0; k < F; ++k) {
+      in[(size_t)i * 16 + k] = orc_bf16(feat[(size_t)k * n + i]);
+      in[(size_t)i * 16 + F + k] = orc_bf16(agg[k]);
+    }
+    for (int o = 0; o < H; ++o) {
+      double t = wb[B1 + o];
+      for (int k = 0; k < 16; ++k) t += wb[W1 + o * 16 + k] * in[(size_t)i * 16 + k];
+      h1[(size_t)i * H + o] = std::max(t, 0.0);
+    }
+    for (int o = 0; o < H; ++o) {
+      double t = wb[B2 + o];
+      for (int k = 0; k < H; ++k) t += wb[W2 + o * 16 + k] * (double)orc_bf16((float)h1[(size_t)i * H + k]);
+      h2[(size_t)i * H + o] = std::max(t, 0.0);
+    }
+    double p = wb[B3];
+    for (int k = 0; k < H; ++k) p += wb[W3 + k] * h2[(size_t)i * H + k];
+    pre[i] = p;
+    om[i] = 0.25 * (p > 20.0 ? p : std::log1p(std::exp(p)));
+  }
+  auto spmv = [&](const std::vector<double>& x, std::vector<double>& y) {
+    for (int i = 0; i < n; ++i) {
+      double t = 0.0;
+      for (int w = 0; w < WA; ++w) t += val[(size_t)w * n + i] * x[col[(size_t)w * n + i]];
+      y[i] = t;
+    }
+  };
+  std::vector<double> z(n), Az(n), dom(n, 0.0);
+  double L = 0.0;
+  for (int k = 0; k < S; ++k) {
+    const double *r = R + (size_t)k * n, *zb = Z + (size_t)k * n, *u = U + (size_t)k * n, *e = E + (size_t)k * n;
+    for (int i = 0; i < n; ++i) z[i] = zb[i] + om[i] * u[i];
+    spmv(z, Az);
+    double a = 0.0, b = 0.0, c = 0.0;
+    for (int i = 0; i < n; ++i) { a += z[i] * r[i]; b += z[i] * Az[i]; c += e[i] * r[i]; }
+    const double bc = std::max(b * c, 1e-300);
+    L += 1.0 - a * a / bc;
+    const double c0 = 2.0 * a / bc, c1 = 2.0 * a * a / (bc * std::max(b, 1e-300));
+    for (int i = 0; i < n; ++i) dom[i] += -(c0 * r[i] - c1 * Az[i]) / S * u[i];
+  }
+  *loss = L / S;
+  if (!grad) return 0;
+  for (int j = 0; j < NP; ++j) grad[j] = 0.0;
+  for (int i = 0; i < n; ++i) {
+    const double p = pre[i];
+    const double dpre = dom[i] * 0.25 / (1.0 + std::exp(-p));
+    double d2[16], d1[16];
+    for (int k = 0; k < H; ++k) {
+      const double x2 = h2[(size_t)i * H + k];
+      grad[W3 + k] += dpre * x2;
+      d2[k] = x2 > 0.0 ? dpre * wb[W3 + k] : 0.0;
+    }
+    grad[B3] += dpre;
+    for (int o = 0; o < H; ++o) {
+      grad[B2 + o] += d2[o];
+      for (int k = 0; k < H; ++k) grad[W2 + o * 16 + k] += d2[o] * (double)orc_bf16((float)h1[(size_t)i * H + k]);
+    }
+    for (int k = 0; k < H; ++k) {
+      double t = 0.0;
+      for (int o = 0; o < H; ++o) t += d2[o] * wb[W2 + o * 16 + k];
+      d1[k] = h1[(size_t)i * H + k] > 0.0 ? t : 0.0;
+    }
+    for (int o = 0; o < H; ++o) {
+      grad[B1 + o] += d1[o];
+      for (int k = 0; k < 16; ++k) grad[W1 + o * 16 + k] += d1[o] * in[(size_t)i * 16 + k];
+    }
+  }
+  return 0;
+}
+
 // Temperature [nc] and passive scalars [n_scalars][nc] (scalar-major), either may be NULL.
 void orc_get_scalars(void* h, double* T, double* C) {
   auto* s = static_cast<orc::Solver*>(h);

@@ -59,6 +59,8 @@ def lib():
         L.orc_poisson_csr.restype = C.c_int64
         L.orc_record_poisson.argtypes = [vp, C.c_int]
         L.orc_get_scalars.argtypes = [vp, dp, dp]
+        L.orc_lp_loss_grad.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, dp,
+                                       C.c_int, dp, dp, dp, dp, C.c_void_p, dp, dp]
         L.orc_advection_scalar.argtypes = [vp, C.c_int, dp, dp, dp, dp, dp]
         L.orc_viscous_scalar.argtypes = [vp, dp, C.c_double, dp, C.c_double, dp, dp, dp]
         L.orc_set_scalars.argtypes = [vp, dp, dp]
