@@ -151,9 +151,19 @@ def run_gpu(args, rank, world):
     case = make_case(args.config)
     if args.psolver == "fcg":
         case.params["p_solver"] = 1  # DPM_PSOLVER_TWOLEVEL_FCG
+        if args.mixed:
+            case.params["form"] = 1  # DPM_FORM_MIXED
     s = Solver(case, device=dev)
     s.initialise()
     nc = s.nc
+    learn = None
+    if args.psolver == "fcg" and not args.no_learned:
+        # learned preconditioner term: samples from 3 steps' solves, 80 Adam steps, gamma set on the
+        # held-out solve (set-up work, outside the timed region; reported in the config)
+        n_samples = s.learn_collect(3)
+        learn = s.learn_train(epochs=80, lr=1e-2)
+        learn["collect_steps"] = 3
+        learn["samples_recorded"] = n_samples
     for _ in range(args.warmup):
         s.advance()
     if world > 1:
@@ -195,7 +205,7 @@ def run_gpu(args, rank, world):
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         t_dev, t_e2e = float(t[0]), float(t[1])
     return dict(nc=nc, t_dev=t_dev, t_e2e=t_e2e, step_ms=step_ms, pois_ms=pois_ms, its=its, solves=solves,
-                launches=launches, clocks=clocks, solver=s)
+                launches=launches, clocks=clocks, solver=s, learn=learn, fallbacks=s.stats()["p_fallbacks"])
 
 
 def time_plain(args, dev, steps=3):
@@ -247,6 +257,9 @@ def main():
     ap.add_argument("--config", default="channel")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip timing the plain FP64 Jacobi-PCG form")
+    ap.add_argument("--no-learned", action="store_true", help="two-level FCG without the learned term")
+    ap.add_argument("--mixed", action="store_true",
+                    help="precision form: FP32-operator inner iterations inside FP64 defect correction")
     ap.add_argument("--psolver", default="fcg", choices=["pcg", "fcg"],
                     help="pcg: plain FP64 Jacobi-PCG; fcg: flexible CG, two-level part-local preconditioner")
     args = ap.parse_args()
@@ -308,6 +321,13 @@ def main():
         "gpu_launches": r["launches"],
         "clocks": r["clocks"],
     }
+    if args.mixed and args.psolver == "fcg":
+        line["config"]["form"] += "; precision form (FP32-operator inner iterations, FP64 defect correction)"
+    if r["learn"] is not None:
+        line["config"]["learned_term"] = r["learn"]
+        line["config"]["form"] += "; learned one-ring term (gamma %g)" % r["learn"]["gamma"]
+    if args.psolver == "fcg":
+        line["config"]["fallbacks_to_plain_pcg"] = r["fallbacks"]
     if args.psolver != "pcg" and not args.no_plain and world == 1:
         pm, pp, pit = time_plain(args, int(os.environ.get("LOCAL_RANK", "0")))
         line["config"]["plain_fp64_pcg"] = {"ms_per_step": pm, "poisson_ms_per_step": pp,

@@ -63,6 +63,12 @@ struct FcgArgs {
   int rec_stride, rec_base, rec_max;
   double *rec_r, *rec_z, *rec_u, *rec_x;
   int stall_window;       // > 0: stop with reason -20 when ||r|| fell by < 10 % over that many iterations
+  // precision form: FP32 copy of the operator values and FP32 z for w = A z (products summed in
+  // FP64); the initial and the final residual stay FP64.  inner_rel > 0: also stop once
+  // ||r|| <= inner_rel * ||r_0|| (one pass of the outer FP64 defect correction).
+  const float* val32;
+  float* zs32;
+  double inner_rel;
 };
 
 // Bounded grid barrier on the same monotonic counter as grid_allreduce (one arrival per block).
@@ -168,9 +174,10 @@ __device__ __forceinline__ bool grid_reduce_gather(double (&v)[NV + NG], double*
   return ok;
 }
 
-// Row i (new numbering) of A times v, global ELL with fixed width WT (0: runtime width <= 16).
-template <int WT>
-__device__ __forceinline__ double fcg_row(const FcgArgs& a, int WA, int i, const double* v) {
+// Row i (new numbering) of A times v, global ELL with fixed width WT (0: runtime width <= 16);
+// VA / VV: value types of the operator and of the vector (double, or float in the precision form).
+template <int WT, class VA, class VV>
+__device__ __forceinline__ double fcg_row(const FcgArgs& a, const VA* val, int WA, int i, const VV* v) {
   const int n = a.n;
   constexpr int W = WT > 0 ? WT : 16;
   const int wa = WT > 0 ? WT : WA;
@@ -181,11 +188,11 @@ __device__ __forceinline__ double fcg_row(const FcgArgs& a, int WA, int i, const
   double x[W];
 #pragma unroll
   for (int w = 0; w < W; ++w)
-    if (w < wa) x[w] = __ldcg(&v[c[w]]);
+    if (w < wa) x[w] = (double)__ldcg(&v[c[w]]);
   double s = 0.0;
 #pragma unroll
   for (int w = 0; w < W; ++w)
-    if (w < wa) s += __ldcg(&a.val[w * n + i]) * x[w];
+    if (w < wa) s += (double)__ldcg(&val[w * n + i]) * x[w];
   return s;
 }
 
@@ -200,7 +207,7 @@ inline size_t fcg_smem_bytes(int P, int C, int WL, int NB) {
 }
 
 // CPT: cells per thread (C <= CPT * FCG_TPB); WT: global row width (7 for hexahedra, 0 = runtime).
-template <int CPT, int WT>
+template <int CPT, int WT, bool MIXED>
 __global__ void __launch_bounds__(FCG_TPB, 1) k_fcg(FcgArgs a, int WA) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int P = a.P, C = a.C, WL = a.WL, n = a.n;
@@ -264,7 +271,7 @@ __global__ void __launch_bounds__(FCG_TPB, 1) k_fcg(FcgArgs a, int WA) {
     if (OWN(k)) {
       const int i = base + threadIdx.x + k * FCG_TPB;
       const double bp = rr[k] - mb;
-      rr[k] = bp - fcg_row<WT>(a, WA, i, a.xs);
+      rr[k] = bp - fcg_row<WT>(a, a.val, WA, i, a.xs);
       v2[0] += rr[k] * rr[k];
       v2[1] += bp * bp;
       v2[2] += rr[k];  // gathered: part sum of r
@@ -274,7 +281,7 @@ __global__ void __launch_bounds__(FCG_TPB, 1) k_fcg(FcgArgs a, int WA) {
   double dp = sqrt(t2[0]);
   const double sn = sqrt(t2[1]);
   const double rnorm0 = a.guess_zero ? dp : (sn == 0.0 ? dp : sn);
-  const double ttol = fmax(a.rtol * rnorm0, a.atol);
+  const double ttol = fmax(fmax(a.rtol * rnorm0, a.atol), a.inner_rel > 0.0 ? a.inner_rel * dp : 0.0);
   int reason = classify(dp, ttol, a.atol, rnorm0);
   int its = 0;
   double pq_old = 1.0;
@@ -362,7 +369,13 @@ __global__ void __launch_bounds__(FCG_TPB, 1) k_fcg(FcgArgs a, int WA) {
     for (int k = 0; k < CPT; ++k) {
       rz[k] = (double)zc[k] + yb;
       if (OWN(k)) {
-        a.zs[base + threadIdx.x + k * FCG_TPB] = rz[k];
+        if (MIXED) {
+          const float zf = (float)rz[k];
+          a.zs32[base + threadIdx.x + k * FCG_TPB] = zf;
+          rz[k] = (double)zf;  // the z that A z is taken of
+        } else {
+          a.zs[base + threadIdx.x + k * FCG_TPB] = rz[k];
+        }
         if (rec_now) a.rec_z[rec_off + base + threadIdx.x + k * FCG_TPB] = rz[k];
       }
     }
@@ -376,7 +389,7 @@ __global__ void __launch_bounds__(FCG_TPB, 1) k_fcg(FcgArgs a, int WA) {
       rw[k] = 0.0;
       if (OWN(k)) {
         const int i = base + threadIdx.x + k * FCG_TPB;
-        rw[k] = fcg_row<WT>(a, WA, i, a.zs);
+        rw[k] = MIXED ? fcg_row<WT>(a, a.val32, WA, i, (const float*)a.zs32) : fcg_row<WT>(a, a.val, WA, i, a.zs);
         const double qk = s_q[threadIdx.x + k * FCG_TPB];
         v[0] += rz[k] * rr[k];
         v[1] += rz[k] * qk;
@@ -436,7 +449,7 @@ __global__ void __launch_bounds__(FCG_TPB, 1) k_fcg(FcgArgs a, int WA) {
   for (int k = 0; k < CPT; ++k)
     if (OWN(k)) {
       const int i = base + threadIdx.x + k * FCG_TPB;
-      const double d = a.b[__ldg(&a.perm[i])] - fcg_row<WT>(a, WA, i, a.xs);
+      const double d = a.b[__ldg(&a.perm[i])] - fcg_row<WT>(a, a.val, WA, i, a.xs);
       v1[0] += d * d;
     }
   if (!grid_reduce_gather<1, 0>(v1, a.partials, a.bar, gen, a.status, t1, s_gat)) return;
@@ -450,25 +463,29 @@ __global__ void __launch_bounds__(FCG_TPB, 1) k_fcg(FcgArgs a, int WA) {
 #undef OWN
 }
 
-inline void* fcg_kernel_for(int C, int width, int* cpt_out) {
-  const int cpt = (C + FCG_TPB - 1) / FCG_TPB;
-  *cpt_out = cpt;
+template <bool MIXED>
+inline void* fcg_kernel_sel(int cpt, int width) {
   if (width == 7) {
     switch (cpt) {
-      case 1: return (void*)k_fcg<1, 7>;
-      case 2: return (void*)k_fcg<2, 7>;
-      case 3: return (void*)k_fcg<3, 7>;
-      case 4: return (void*)k_fcg<4, 7>;
+      case 1: return (void*)k_fcg<1, 7, MIXED>;
+      case 2: return (void*)k_fcg<2, 7, MIXED>;
+      case 3: return (void*)k_fcg<3, 7, MIXED>;
+      case 4: return (void*)k_fcg<4, 7, MIXED>;
       default: return nullptr;
     }
   }
   switch (cpt) {
-    case 1: return (void*)k_fcg<1, 0>;
-    case 2: return (void*)k_fcg<2, 0>;
-    case 3: return (void*)k_fcg<3, 0>;
-    case 4: return (void*)k_fcg<4, 0>;
+    case 1: return (void*)k_fcg<1, 0, MIXED>;
+    case 2: return (void*)k_fcg<2, 0, MIXED>;
+    case 3: return (void*)k_fcg<3, 0, MIXED>;
+    case 4: return (void*)k_fcg<4, 0, MIXED>;
     default: return nullptr;
   }
+}
+inline void* fcg_kernel_for(int C, int width, bool mixed, int* cpt_out) {
+  const int cpt = (C + FCG_TPB - 1) / FCG_TPB;
+  *cpt_out = cpt;
+  return mixed ? fcg_kernel_sel<true>(cpt, width) : fcg_kernel_sel<false>(cpt, width);
 }
 
 }  // namespace gpu

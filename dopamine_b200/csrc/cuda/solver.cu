@@ -203,6 +203,8 @@ struct Solver {
   FcgArgs fa{};
   int fcg_WA = 0;
   void* fcg_kernel = nullptr;
+  bool fcg_mixed = false;
+  bool inner_rel_is_first_ = true;
   size_t fcg_smem = 0;
   // state
   double time = 0.0;
@@ -383,6 +385,8 @@ struct Solver {
       if (rc) return rc;
     } else if (P.p_solver != DPM_PSOLVER_JACOBI_PCG) {
       return DPM_ERR_ARG;
+    } else if (P.form == DPM_FORM_MIXED) {
+      return DPM_ERR_UNSUPPORTED;  // the precision form is built on the flexible CG
     }
     // initial fields: T = T_ref, velocity from an inlet patch (initialize_velocity_from_bc)
     launch_fill(F.T, nc, P.T_ref);
@@ -650,7 +654,8 @@ struct Solver {
     int rc = build_two_level(nc, S.WA, S.A_col.data(), S.A_val.data(), m.centroid.data(), dev_sms, nullsp, T);
     if (rc) return DPM_ERR_UNSUPPORTED;
     int cpt = 0;
-    fcg_kernel = fcg_kernel_for(T.C, T.WA, &cpt);
+    fcg_mixed = P.form == DPM_FORM_MIXED;
+    fcg_kernel = fcg_kernel_for(T.C, T.WA, fcg_mixed, &cpt);
     fcg_smem = fcg_smem_bytes(T.P, T.C, T.WL, T.NB);
     if (!fcg_kernel || fcg_smem > 219 * 1024) return DPM_ERR_UNSUPPORTED;
     CK(cudaFuncSetAttribute(fcg_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fcg_smem));
@@ -673,6 +678,12 @@ struct Solver {
     fa.xval = mem.upload(T.xval);
     fa.xs = mem.alloc<double>(nc);
     fa.zs = mem.alloc<double>(nc);
+    if (fcg_mixed) {
+      std::vector<float> v32(T.val.begin(), T.val.end());
+      fa.val32 = mem.upload(v32);
+      fa.zs32 = mem.alloc<float>(nc);
+      if (!fa.val32 || !fa.zs32) return DPM_ERR_CUDA;
+    }
     fa.partials = mem.alloc<double>((size_t)2 * FCG_SLOT * T.P);
     fa.bar = cg_bar; fa.status = cg_status; fa.dout = cg_dout;
     fa.nullsp = nullsp ? 1 : 0;
@@ -767,12 +778,33 @@ struct Solver {
     launches++;
   }
 
+  // Precision form: FP32-operator inner solves, each ending at 1e-5 of its own FP64 initial
+  // residual, restarted from the current x (whose residual every launch recomputes in FP64) until
+  // a launch finds the FP64 residual already below the target.
   int fcg(const double* rhs, double* x, double rtol, double atol, int maxit, int guess_zero, int* its, double* resid,
           int* reason) {
+    if (!fcg_mixed) return fcg_launch(rhs, x, rtol, atol, maxit, guess_zero, its, resid, reason, 0.0);
+    int tot = 0;
+    for (int outer = 0; outer < 8; ++outer) {
+      int it = 0;
+      inner_rel_is_first_ = outer == 0;  // samples are recorded in the first inner solve only
+      int rc = fcg_launch(rhs, x, rtol, atol, std::max(maxit - tot, 1), outer == 0 ? guess_zero : 0, &it, resid,
+                          reason, 1.0e-5);
+      if (rc) return rc;
+      tot += it;
+      if (*reason < 0 || it == 0 || tot >= maxit) break;
+    }
+    inner_rel_is_first_ = true;
+    *its = tot;
+    return 0;
+  }
+  int fcg_launch(const double* rhs, double* x, double rtol, double atol, int maxit, int guess_zero, int* its,
+                 double* resid, int* reason, double inner_rel) {
     FcgArgs a = fa;
+    a.inner_rel = inner_rel;
     a.b = rhs; a.x = x; a.rtol = rtol; a.atol = atol; a.maxit = maxit; a.guess_zero = guess_zero;
     a.gamma = lp_ready ? lp_gamma : 0.0f;
-    const bool rec = lp_recording && lp_count < lp_S;
+    const bool rec = lp_recording && lp_count < lp_S && inner_rel_is_first_;
     if (rec) {
       a.gamma = 0.0f;
       a.rec_stride = lp_stride; a.rec_base = lp_count; a.rec_max = lp_S;
@@ -850,16 +882,24 @@ struct Solver {
     CK(cudaMemcpyAsync(q.data(), lp_dsum, sizeof(double) * 3 * S, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     double L = 0.0;
+    int used = 0;
     for (int k = 0; k < S; ++k) {
       const double a = base[3 * k] + q[3 * k];
       const double b = base[3 * k + 1] + 2.0 * q[3 * k + 1] + q[3 * k + 2];
       const double c = base[3 * k + 2];
-      const double bc = std::max(b * c, 1e-300);
+      coef[2 * k] = coef[2 * k + 1] = 0.0;
+      // a sample whose error energy e.r is not positive (an iterate already at round-off) carries
+      // no information: it is left out of the loss
+      if (!(c > 0.0) || !(b > 0.0) || !std::isfinite(a)) continue;
+      const double bc = b * c;
       L += 1.0 - a * a / bc;
       coef[2 * k] = 2.0 * a / bc;
-      coef[2 * k + 1] = 2.0 * a * a / (bc * std::max(b, 1e-300));
+      coef[2 * k + 1] = 2.0 * a * a / (bc * b);
+      used++;
     }
-    *loss = L / S;
+    *loss = used > 0 ? L / used : 0.0;
+    const double scale = used > 0 ? (double)S / used : 0.0;  // k_lp_domega divides by S
+    for (auto& c : coef) c *= scale;
     if (!grad) return 0;
     CK(cudaMemcpyAsync(lp_coef, coef.data(), sizeof(double) * 2 * S, cudaMemcpyHostToDevice, st));
     k_lp_domega<<<nblk(nc), 256, 0, st>>>(nc, S, lp_coef, lp_u, lp_r, lp_azb, lp_av, lp_dom);

@@ -63,8 +63,11 @@ extern "C" {
 /* Pressure-solve forms. */
 #define DPM_PSOLVER_JACOBI_PCG 0
 #define DPM_PSOLVER_TWOLEVEL_FCG 1
-#define DPM_FORM_FP64 0     /* plain: FP64 Jacobi-PCG                                    */
-#define DPM_FORM_MIXED 1    /* FP32 inner PCG inside FP64 defect correction              */
+#define DPM_FORM_FP64 0     /* FP64 Krylov iterations                                    */
+#define DPM_FORM_MIXED 1    /* with DPM_PSOLVER_TWOLEVEL_FCG: inner iterations on an FP32 copy of
+                               the operator and an FP32 preconditioned vector, inside an FP64
+                               defect correction (each inner solve ends at 1e-5 of its FP64
+                               initial residual; the outer loop stops on the FP64 residual)   */
 
 /* Raw mesh, as a gmsh v4 file holds it (src/mesh/mod_gmsh_reader.f90:build_mesh_from_gmsh). */
 typedef struct dpm_raw_mesh {

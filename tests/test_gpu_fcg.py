@@ -63,3 +63,29 @@ def test_fcg_needs_far_fewer_iterations_on_the_channel():
         s.close()
     assert its[abi.PSOLVER_TWOLEVEL_FCG] * 2 <= its[abi.PSOLVER_JACOBI_PCG], its
     assert div[abi.PSOLVER_TWOLEVEL_FCG] <= 10 * div[abi.PSOLVER_JACOBI_PCG] + 1e-12, div
+
+
+@pytest.mark.parametrize("name,steps", [("tgv_skew", 3), ("channel", 3)])
+def test_precision_form_against_fp64_oracle(name, steps):
+    """Precision form (FP32-operator inner FCG inside FP64 defect correction) at the default
+    p_tol against the FP64 oracle: field error <= 1e-5 and divergence <= 1e-8, as the chosen forms
+    must meet; the measured errors are printed."""
+    case = cases.channel_config(nx=16, ny=12, nz=8, n_steps=steps) if name == "channel" else cases.regression_case(name)
+    po = case.make_params()
+    pg = case.make_params()
+    pg.p_solver = abi.PSOLVER_TWOLEVEL_FCG
+    pg.form = abi.FORM_MIXED
+    o = O.Oracle(case, params=po)
+    s = Solver(case, params=pg)
+    o.initialise()
+    s.initialise()
+    for _ in range(steps):
+        o.advance()
+        s.advance()
+    so, sg = o.state(), s.sync_host()
+    eu = _rel(sg["U"], so["U"])
+    ep = np.linalg.norm((sg["p"] - sg["p"].mean()) - (so["p"] - so["p"].mean())) / max(np.linalg.norm(so["p"]), 1e-30)
+    st = s.stats()
+    print(f"precision form {name}: U rel {eu:.2e}, p rel {ep:.2e}, divU {st['max_abs_divU']:.2e}")
+    assert eu <= 1e-5 and ep <= 1e-5
+    assert st["max_abs_divU"] <= DIV_TOL
