@@ -149,6 +149,141 @@ def wall_box(nx, ny, nz, lx, ly, lz, bump_z):
     return m
 
 
+def _jittered_grid(n, jitter, seed):
+    """Nodes of the unit cube's n^3 grid, interior nodes moved by a seeded uniform draw in
+    [-jitter, jitter] * h per coordinate (boundary nodes stay, so the box stays a periodic box)."""
+    h = 1.0 / n
+    g = np.arange(n + 1) * h
+    X, Y, Z = np.meshgrid(g, g, g, indexing="ij")
+    xyz = np.stack([X.ravel(order="F"), Y.ravel(order="F"), Z.ravel(order="F")], 1)  # id = i + (n+1)(j + (n+1)k)
+    r = _fast_uniform(xyz.size, seed).reshape(xyz.shape)
+    i = np.arange(n + 1)
+    I, J, K = np.meshgrid(i, i, i, indexing="ij")
+    interior = ((I > 0) & (I < n) & (J > 0) & (J < n) & (K > 0) & (K < n)).ravel(order="F")
+    xyz[interior] += jitter * h * (2.0 * r[interior] - 1.0)
+    return xyz
+
+
+def _hex_nodes(n, i, j, k):
+    nid = lambda a, b, c: a + (n + 1) * (b + (n + 1) * c)
+    return [nid(i, j, k), nid(i + 1, j, k), nid(i + 1, j + 1, k), nid(i, j + 1, k),
+            nid(i, j, k + 1), nid(i + 1, j, k + 1), nid(i + 1, j + 1, k + 1), nid(i, j + 1, k + 1)]
+
+
+_PATCHES6 = ("x0", "xL", "y0", "yL", "z0", "zL")
+
+
+def _assemble(xyz, cells, bfaces):
+    """cells: [(type, [nodes])], bfaces: [(patch, [nodes])] -> RawMesh."""
+    ct = np.array([c[0] for c in cells], dtype=np.int32)
+    cn = np.concatenate([np.asarray(c[1], dtype=np.int32) for c in cells])
+    co = np.concatenate([[0], np.cumsum([len(c[1]) for c in cells])]).astype(np.int64)
+    bp = np.array([b[0] for b in bfaces], dtype=np.int32)
+    bn = np.concatenate([np.asarray(b[1], dtype=np.int32) for b in bfaces])
+    bo = np.concatenate([[0], np.cumsum([len(b[1]) for b in bfaces])]).astype(np.int64)
+    return RawMesh(xyz=np.ascontiguousarray(xyz), cell_type=ct, cell_off=co, cell_nodes=cn, bface_off=bo,
+                   bface_nodes=bn, bface_patch=bp, patch_names=list(_PATCHES6))
+
+
+# hex faces on the box boundary: (patch, local quad) and the two triangles of the split along
+# the main diagonal v0-v6 (consistent across neighbours and across periodic pairs)
+_HEX_BFACES = {0: (0, 3, 7, 4), 1: (1, 2, 6, 5), 2: (0, 1, 5, 4), 3: (3, 2, 6, 7), 4: (0, 1, 2, 3), 5: (4, 5, 6, 7)}
+_KUHN_TRI = {0: ((0, 3, 7), (0, 7, 4)), 1: ((1, 2, 6), (1, 6, 5)), 2: ((0, 1, 5), (0, 5, 4)),
+             3: ((2, 3, 6), (3, 7, 6)), 4: ((0, 1, 2), (0, 2, 3)), 5: ((4, 5, 6), (4, 6, 7))}
+_KUHN_TETS = ((0, 1, 2, 6), (0, 2, 3, 6), (0, 3, 7, 6), (0, 7, 4, 6), (0, 4, 5, 6), (0, 5, 1, 6))
+
+
+def _boundary_sides(n, i, j, k):
+    out = []
+    if i == 0: out.append(0)
+    if i == n - 1: out.append(1)
+    if j == 0: out.append(2)
+    if j == n - 1: out.append(3)
+    if k == 0: out.append(4)
+    if k == n - 1: out.append(5)
+    return out
+
+
+def tet_box(n, jitter=0.2, seed=20261204):
+    """Unit cube of n^3 jittered hexes, each split into 6 tetrahedra around its main diagonal
+    (a conforming all-tet mesh; periodic pairs match)."""
+    xyz = _jittered_grid(n, jitter, seed)
+    cells, bf = [], []
+    for k in range(n):
+        for j in range(n):
+            for i in range(n):
+                v = _hex_nodes(n, i, j, k)
+                cells += [(abi.EL_TET4, [v[a] for a in t]) for t in _KUHN_TETS]
+                for sd in _boundary_sides(n, i, j, k):
+                    bf += [(sd, [v[a] for a in tri]) for tri in _KUHN_TRI[sd]]
+    return _assemble(xyz, cells, bf)
+
+
+def mixed_box(n, jitter=0.2, seed=20261205, prism_cols=0.3, pyramid_hex=0.3):
+    """Unit cube of n^3 jittered hexes in a conforming seeded mix: whole columns (fixed i, j)
+    split into two prisms each along the v0-v2 diagonal (triangles only on the column's z
+    faces), and, in the other columns, hexes split into 6 pyramids around an added centre node
+    (their faces stay quads); the rest stay hexes."""
+    xyz = _jittered_grid(n, jitter, seed)
+    rc = _fast_uniform(n * n, seed + 1)
+    rh = _fast_uniform(n ** 3, seed + 2)
+    extra = []
+    cells, bf = [], []
+    for k in range(n):
+        for j in range(n):
+            for i in range(n):
+                v = _hex_nodes(n, i, j, k)
+                col = rc[i + n * j] < prism_cols
+                sides = _boundary_sides(n, i, j, k)
+                if col:
+                    cells.append((abi.EL_PRISM6, [v[0], v[1], v[2], v[4], v[5], v[6]]))
+                    cells.append((abi.EL_PRISM6, [v[0], v[2], v[3], v[4], v[6], v[7]]))
+                    for sd in sides:
+                        if sd == 4:
+                            bf += [(4, [v[0], v[1], v[2]]), (4, [v[0], v[2], v[3]])]
+                        elif sd == 5:
+                            bf += [(5, [v[4], v[5], v[6]]), (5, [v[4], v[6], v[7]])]
+                        else:
+                            bf.append((sd, [v[a] for a in _HEX_BFACES[sd]]))
+                    continue
+                if rh[i + n * (j + n * k)] < pyramid_hex:
+                    c = len(xyz) + len(extra)
+                    extra.append(xyz[v].mean(axis=0))
+                    for quad in ((0, 1, 2, 3), (4, 5, 6, 7), (0, 1, 5, 4), (3, 2, 6, 7), (0, 3, 7, 4), (1, 2, 6, 5)):
+                        cells.append((abi.EL_PYR5, [v[a] for a in quad] + [c]))
+                else:
+                    cells.append((abi.EL_HEX8, v))
+                for sd in sides:
+                    bf.append((sd, [v[a] for a in _HEX_BFACES[sd]]))
+    if extra:
+        xyz = np.concatenate([xyz, np.array(extra)], axis=0)
+    return _assemble(xyz, cells, bf)
+
+
+def curl_noise_velocity(centroid, seed=20261206, k0=4.0, kmax=6):
+    """Divergence-free random field: U = curl A with A a sum of Fourier modes of the unit box
+    (integer wavevectors, 2 <= |k| <= kmax) whose amplitudes are seeded normal draws times a
+    Gaussian spectrum exp(-(|k| - k0)^2 / 2); scaled to unit RMS."""
+    r = np.arange(-kmax, kmax + 1)
+    K = np.stack(np.meshgrid(r, r, r, indexing="ij"), -1).reshape(-1, 3).astype(float)
+    kk = np.linalg.norm(K, axis=1)
+    K = K[(kk >= 2.0) & (kk <= kmax)]
+    kk = np.linalg.norm(K, axis=1)
+    u = _fast_uniform(4 * len(K), seed).reshape(len(K), 4)
+    amp = np.sqrt(-2.0 * np.log(np.maximum(u[:, :3], 1e-300))) * np.cos(2.0 * np.pi * u[:, 3:4])  # normal draws
+    amp *= np.exp(-0.5 * (kk - k0) ** 2)[:, None]
+    ph = 2.0 * np.pi * u[:, 3]
+    arg = 2.0 * np.pi * centroid @ K.T + ph[None, :]          # [n, modes]
+    c = np.cos(arg)
+    U = np.zeros_like(centroid)
+    tk = 2.0 * np.pi * K
+    # (curl A)_x = dAz/dy - dAy/dz, A_m = amp_m sin(arg)
+    U[:, 0] = c @ (tk[:, 1] * amp[:, 2] - tk[:, 2] * amp[:, 1])
+    U[:, 1] = c @ (tk[:, 2] * amp[:, 0] - tk[:, 0] * amp[:, 2])
+    U[:, 2] = c @ (tk[:, 0] * amp[:, 1] - tk[:, 1] * amp[:, 0])
+    return U / np.sqrt(np.mean(np.sum(U * U, axis=1)))
+
+
 # ------------------------------------------------------------------------------------------
 # Initial conditions (src/init/mod_initconditions.f90)
 # ------------------------------------------------------------------------------------------
@@ -236,6 +371,8 @@ class Case:
             U[:, 0] = self.ic_uref
         elif self.ic == "channel":
             U = channel_parabolic(centroid, lo, hi, self.ic_uref)
+        elif self.ic == "curl_noise":
+            U = self.ic_uref * curl_noise_velocity(centroid)
         else:
             raise ValueError(self.ic)
         if self.noise > 0.0:
@@ -350,3 +487,17 @@ def channel_config(nx=96, ny=64, nz=64, n_steps=1000, retau=395.0, noise_seed=20
                      nu=nu, dt=dt, cfl_max=0.5, p_tol=1e-10, f_const=(1.0, 0.0, 0.0)),
                 "channel", 1.5 * ub, noise=0.10, noise_seed=noise_seed, n_steps=n_steps,
                 description=f"channel {nx}x{ny}x{nz} Re_tau={retau:g}, KEP, Vreman, log-law wall model")
+
+
+def hybrid_config(n=16, kind="mixed", n_steps=10):
+    """Non-orthogonal unstructured box (third configuration, reduced size): unit cube of n^3
+    jittered (+-0.2 h) hexes as a conforming mix of hexes, prisms and pyramids ("mixed") or as
+    all tetrahedra ("tet"), periodic, AMD SGS, Koren TVD momentum advection, divergence-free
+    curl-noise initial velocity (peak |k| = 4)."""
+    mesh = mixed_box(n) if kind == "mixed" else tet_box(n)
+    h = 1.0 / n
+    return Case(f"hybrid_{kind}{n}", mesh, _periodic6(),
+                dict(scheme=abi.SCHEME_KOREN_TVD, sgs_model=abi.SGS_AMD, wall_model=abi.WM_NONE, nu=1.0e-3,
+                     dt=0.2 * h / 3.0, cfl_max=0.5, p_tol=1e-10, n_nonortho_corr=3),
+                "curl_noise", 1.0, n_steps=n_steps,
+                description=f"{kind} unstructured jittered unit box {n}^3, AMD, Koren")
