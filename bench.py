@@ -129,10 +129,11 @@ def pcg_bytes_per_iteration(s, psolver="pcg"):
     return phase_a + phase_b
 
 
-def pcg_traffic_per_launch():
-    """DRAM bytes (read + write) of one k_pcg launch on this workload, from the committed ncu
-    summary (one capture, its command inside the file); None when the summary is absent."""
-    path = os.path.join(ROOT, "profiles", "k_pcg_channel96x64x64.md")
+def pcg_traffic_per_launch(psolver="pcg"):
+    """DRAM bytes (read + write) of one launch of the Poisson kernel on this workload, from the
+    committed ncu summary (one capture, its command inside the file); None when absent."""
+    name = "k_fcg_channel96x64x64.md" if psolver == "fcg" else "k_pcg_channel96x64x64.md"
+    path = os.path.join(ROOT, "profiles", name)
     try:
         for line in open(path):
             if line.startswith("traffic_bytes_per_launch:"):
@@ -304,7 +305,7 @@ def main():
     bytes_it = pcg_bytes_per_iteration(s, args.psolver)
     pois_s = sum(r["pois_ms"]) / 1e3
     achieved = bytes_it * r["its"] / pois_s / 1e9 if pois_s > 0 else 0.0
-    traffic = pcg_traffic_per_launch() if args.config == "channel" and args.psolver == "pcg" else None
+    traffic = pcg_traffic_per_launch(args.psolver) if args.config == "channel" else None
     line = {
         "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world, "steps": K,
         "warmup": args.warmup, "ms_per_step": 1e3 * r["t_dev"] / K, "higher_is_better": True, "scaling": "weak",

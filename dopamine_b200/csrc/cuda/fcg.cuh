@@ -18,8 +18,9 @@
 // so an iteration has one barrier and one all-reduce, like the Jacobi-PCG kernel, while the
 // preconditioner works without any grid-wide wait.  The stopping rule is the reference's
 // (unpreconditioned ||r|| <= max(rtol ||b'||, atol), src/solver/pressure_backend_petsc.c:816-876),
-// tested on the current residual at the top of each iteration.  Krylov vectors, reductions and
-// the coarse solve are FP64; only the part-local smoother runs in FP32.
+// tested on the current residual at the top of each iteration.  Krylov vectors and reductions
+// are FP64; the part-local smoother runs in FP32 and the coarse solve uses FP32 rows of E^-1
+// with FP64 sums (both are preconditioner work only).
 #pragma once
 #include "pcg.cuh"
 
@@ -198,7 +199,8 @@ __device__ __forceinline__ double fcg_row(const FcgArgs& a, const VA* val, int W
 
 // Dynamic shared memory of the kernel for a given set-up.
 inline size_t fcg_smem_bytes(int P, int C, int WL, int NB) {
-  return (size_t)(1 + NB) * P * sizeof(double)          // gathered sums r, E^-1 rows of the slots
+  return (size_t)P * sizeof(double)                     // gathered sums r
+         + (size_t)NB * P * sizeof(float)                // E^-1 rows of the slots (FP32)
          + (size_t)FCG_NG * P * sizeof(double)           // gather landing area
          + (size_t)3 * C * sizeof(double)                // own x, p, q
          + (size_t)C * sizeof(float)                     // own 1/diag (FP32, smoother)
@@ -212,8 +214,7 @@ __global__ void __launch_bounds__(FCG_TPB, 1) k_fcg(FcgArgs a, int WA) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int P = a.P, C = a.C, WL = a.WL, n = a.n;
   double* s_c = reinterpret_cast<double*>(smem);          // [P] c = Z^T r
-  double* s_er = s_c + P;                                  // [NB][P] E^-1 rows of this part's slots
-  double* s_gat = s_er + (size_t)a.NB * P;                 // [NG][P]
+  double* s_gat = s_c + P;                                 // [NG][P]
   double* s_x = s_gat + FCG_NG * P;                        // [C] own x
   double* s_p = s_x + C;                                   // [C] own p
   double* s_q = s_p + C;                                   // [C] own q
@@ -221,6 +222,7 @@ __global__ void __launch_bounds__(FCG_TPB, 1) k_fcg(FcgArgs a, int WA) {
   unsigned* s_lpk = reinterpret_cast<unsigned*>(s_dinv + C);  // [WL][C]
   float* s_d0 = reinterpret_cast<float*>(s_lpk + (size_t)WL * C);  // [C]
   float* s_d1 = s_d0 + C;                                  // [C]
+  float* s_er = s_d1 + C;                                  // [NB][P] E^-1 rows of this part's slots (FP32)
   __shared__ double s_yn[32];  // coarse values of this part's slots (slot 0 = own part)
 
   constexpr int LW = WT > 0 ? WT - 1 : 16;  // unrolled bound of the local row width
@@ -232,7 +234,7 @@ __global__ void __launch_bounds__(FCG_TPB, 1) k_fcg(FcgArgs a, int WA) {
   // ---- stage the part's local operator and E^-1 row
   for (int s = 0; s < WL; ++s)
     for (int l = threadIdx.x; l < size; l += blockDim.x) s_lpk[s * C + l] = a.lpk[(size_t)s * n + base + l];
-  for (int j = threadIdx.x; j < a.NB * P; j += blockDim.x) s_er[j] = a.einv_nb[(size_t)b * a.NB * P + j];
+  for (int j = threadIdx.x; j < a.NB * P; j += blockDim.x) s_er[j] = (float)a.einv_nb[(size_t)b * a.NB * P + j];
 
   // own-cell state: r in registers; x, p, q and the FP32 1/diag in shared memory
   double rr[CPT];
@@ -296,7 +298,7 @@ __global__ void __launch_bounds__(FCG_TPB, 1) k_fcg(FcgArgs a, int WA) {
       const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
       if (w < a.NB) {
         double s = 0.0;
-        for (int j = lane; j < P; j += 32) s += s_er[(size_t)w * P + j] * s_c[j];
+        for (int j = lane; j < P; j += 32) s += (double)s_er[(size_t)w * P + j] * s_c[j];
         for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
         if (lane == 0) s_yn[w] = s;
       }

@@ -181,3 +181,22 @@ def test_step_parity_unstructured_amd_koren(kind):
         _compare_states(o, s, 1e-10, f"{kind} step {k + 1}")
     st, so = s.stats(), o.stats()
     assert abs(st["nu_sgs_mean"] - so["nu_sgs_mean"]) <= 1e-9 * so["nu_sgs_mean"]
+
+
+def test_step_parity_large_mesh_grid_stride_pcg():
+    """Above 4 cells per thread of the cooperative grid (606k cells on B200) the Jacobi-PCG kernel
+    keeps its vectors in global memory (the path of the 8.4M- and 20M-cell configurations):
+    Taylor-Green 90^3 (729k cells), one step against the multi-threaded oracle."""
+    import os
+    case = cases.tgv_config(n=90, n_steps=1)
+    p = case.make_params()
+    p.p_tol = 1e-12
+    o = O.Oracle(case, nthreads=os.cpu_count() or 1, params=p)
+    s = Solver(case, params=p)
+    assert s.nc > 4 * 148 * 1024
+    o.initialise()
+    s.initialise()
+    o.advance()
+    s.advance()
+    _compare_states(o, s, 1e-9, "tgv90 step 1")
+    assert s.stats()["max_abs_divU"] <= 1e-9
