@@ -103,7 +103,10 @@ FORMS = {"pcg": "plain FP64 Jacobi-PCG",
                 "degree 6 in shared memory + one coarse value per part)"}
 
 
-KERNELS = {"pcg": "k_pcg (persistent Jacobi-PCG)", "fcg": "k_fcg (persistent two-level flexible CG)"}
+FORMS["ml"] = ("FP64 flexible CG preconditioned by one FP32 aggregation-multigrid V-cycle (pairwise "
+               "aggregation, 3 passes per level, Chebyshev degree 3, dense coarsest level)")
+KERNELS = {"pcg": "k_pcg (persistent Jacobi-PCG)", "fcg": "k_fcg (persistent two-level flexible CG)",
+           "ml": "k_mlcg (persistent multilevel flexible CG)"}
 
 
 def make_case(name):
@@ -119,6 +122,12 @@ def pcg_bytes_per_iteration(s, psolver="pcg"):
     """Algorithmic bytes of one Krylov iteration, per the ELL operator width (hex: 7)."""
     nc = s.nc
     wa = 7  # hex mesh: diagonal + 6 neighbours
+    if psolver == "ml":
+        # fine level only (the coarser levels add about 1/7): 2k = 6 FP32 smoothing/restriction
+        # passes (cols + FP32 vals, b, d in/out, x in/out), the FP64 w = A z pass (cols, vals, z,
+        # r, q in, w out) and the update pass (z, w, p, q, x, r in; p, q, x, r out; b, d, x0 out)
+        k = 3
+        return nc * (2 * k * (wa * (4 + 4) + 16) + (wa * (4 + 8) + 4 + 8 + 16) + (12 + 32 + 32 + 12))
     if psolver == "fcg":
         # w = A z: cols + vals, z gathered once per cell, z written once; the part-local smoother
         # and the own-cell vectors live in shared memory and registers
@@ -132,7 +141,7 @@ def pcg_bytes_per_iteration(s, psolver="pcg"):
 def pcg_traffic_per_launch(psolver="pcg"):
     """DRAM bytes (read + write) of one launch of the Poisson kernel on this workload, from the
     committed ncu summary (one capture, its command inside the file); None when absent."""
-    name = "k_fcg_channel96x64x64.md" if psolver == "fcg" else "k_pcg_channel96x64x64.md"
+    name = {"fcg": "k_fcg_channel96x64x64.md", "ml": "k_mlcg_channel96x64x64.md"}.get(psolver, "k_pcg_channel96x64x64.md")
     path = os.path.join(ROOT, "profiles", name)
     try:
         for line in open(path):
@@ -150,6 +159,8 @@ def run_gpu(args, rank, world):
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(dev)
     case = make_case(args.config)
+    if args.psolver == "ml":
+        case.params["p_solver"] = 2  # DPM_PSOLVER_MULTILEVEL_FCG
     if args.psolver == "fcg":
         case.params["p_solver"] = 1  # DPM_PSOLVER_TWOLEVEL_FCG
         if args.mixed:
@@ -261,8 +272,9 @@ def main():
     ap.add_argument("--no-learned", action="store_true", help="two-level FCG without the learned term")
     ap.add_argument("--mixed", action="store_true",
                     help="precision form: FP32-operator inner iterations inside FP64 defect correction")
-    ap.add_argument("--psolver", default="fcg", choices=["pcg", "fcg"],
-                    help="pcg: plain FP64 Jacobi-PCG; fcg: flexible CG, two-level part-local preconditioner")
+    ap.add_argument("--psolver", default="fcg", choices=["pcg", "fcg", "ml"],
+                    help="pcg: plain FP64 Jacobi-PCG; fcg: flexible CG, two-level part-local preconditioner; "
+                         "ml: flexible CG, aggregation-multigrid V-cycle")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -327,7 +339,7 @@ def main():
     if r["learn"] is not None:
         line["config"]["learned_term"] = r["learn"]
         line["config"]["form"] += "; learned one-ring term (gamma %g)" % r["learn"]["gamma"]
-    if args.psolver == "fcg":
+    if args.psolver in ("fcg", "ml"):
         line["config"]["fallbacks_to_plain_pcg"] = r["fallbacks"]
     if args.psolver != "pcg" and not args.no_plain and world == 1:
         pm, pp, pit = time_plain(args, int(os.environ.get("LOCAL_RANK", "0")))

@@ -21,7 +21,7 @@ SCHEME_BY_NAME = {"VANLEER_TVD": 1, "KOREN_TVD": 2, "CDS": 3, "KEP": 4, "QUICK":
 SGS_NONE, SGS_VREMAN, SGS_SMAGORINSKY, SGS_AMD = 0, 1, 2, 3
 WM_LOGLAW, WM_NONE, WM_MOST = 0, 1, 2
 FORM_FP64, FORM_MIXED = 0, 1
-PSOLVER_JACOBI_PCG, PSOLVER_TWOLEVEL_FCG = 0, 1
+PSOLVER_JACOBI_PCG, PSOLVER_TWOLEVEL_FCG, PSOLVER_MULTILEVEL_FCG = 0, 1, 2
 
 EL_TET4, EL_HEX8, EL_PRISM6, EL_PYR5 = 4, 5, 6, 7
 
@@ -60,6 +60,7 @@ class ParamsT(C.Structure):
         ("p_solver", C.c_int), ("p_smooth_degree", C.c_int), ("p_smooth_lmin", C.c_double),
         ("p_smooth_lmax", C.c_double), ("abl_z0_m", C.c_double), ("abl_z0_h", C.c_double),
         ("abl_T_surface", C.c_double), ("abl_L_obukhov", C.c_double), ("abl_compute_L", C.c_int),
+        ("p_ml_degree", C.c_int), ("p_ml_overcorrect", C.c_double), ("p_ml_passes", C.c_int),
     ]
 
 
@@ -123,6 +124,9 @@ def default_params(**kw):
     p.abl_T_surface = 300.0
     p.abl_L_obukhov = 0.0
     p.abl_compute_L = 1
+    p.p_ml_degree = 3
+    p.p_ml_overcorrect = 1.6
+    p.p_ml_passes = 3
     for k, v in kw.items():
         if k in ("f_const", "g", "scalar_diffusivity", "scalar_pr_t"):
             arr = getattr(p, k)

@@ -154,9 +154,19 @@ __device__ __forceinline__ bool grid_reduce_gather(double (&v)[NV + NG], double*
       double u[NV > 0 ? NV : 1];
 #pragma unroll
       for (int k = 0; k < NV; ++k) u[k] = 0.0;
-      for (int b = lane; b < P; b += 32)
+      // all of a lane's partials are loaded before they are summed (in block order, as a plain
+      // loop would), so the loads are in flight together
+      for (int b0 = lane; b0 < P; b0 += 32 * 4) {
+        double pv[4][NV > 0 ? NV : 1];
 #pragma unroll
-        for (int k = 0; k < NV; ++k) u[k] += __ldcg(&buf[b * FCG_SLOT + k]);
+        for (int h = 0; h < 4; ++h)
+#pragma unroll
+          for (int k = 0; k < NV; ++k) pv[h][k] = b0 + 32 * h < P ? __ldcg(&buf[(b0 + 32 * h) * FCG_SLOT + k]) : 0.0;
+#pragma unroll
+        for (int h = 0; h < 4; ++h)
+#pragma unroll
+          for (int k = 0; k < NV; ++k) u[k] += pv[h][k];
+      }
 #pragma unroll
       for (int k = 0; k < NV; ++k) {
         for (int o = 16; o > 0; o >>= 1) u[k] += __shfl_down_sync(0xffffffffu, u[k], o);

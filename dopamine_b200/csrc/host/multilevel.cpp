@@ -1,0 +1,262 @@
+#include "multilevel.hpp"
+
+#include <algorithm>
+#include <cmath>
+
+namespace dpm {
+namespace {
+
+// Compressed rows with ascending columns (diagonal included).
+struct Csr {
+  int n = 0;
+  std::vector<int64_t> off;
+  std::vector<int> col;
+  std::vector<double> val;
+};
+
+Csr csr_from_ell(int n, int WA, const int* col, const double* val) {
+  Csr A;
+  A.n = n;
+  A.off.assign(n + 1, 0);
+  std::vector<std::pair<int, double>> row;
+  for (int i = 0; i < n; ++i) {
+    row.clear();
+    for (int s = 0; s < WA; ++s) {
+      const int j = col[(size_t)s * n + i];
+      const double v = val[(size_t)s * n + i];
+      if (j == i || v != 0.0) row.emplace_back(j, v);
+    }
+    std::sort(row.begin(), row.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+    for (size_t k = 0; k < row.size(); ++k) {
+      if (k > 0 && row[k].first == row[k - 1].first) {  // padding slots share the own column
+        A.val.back() += row[k].second;
+        continue;
+      }
+      A.col.push_back(row[k].first);
+      A.val.push_back(row[k].second);
+    }
+    A.off[i + 1] = (int64_t)A.col.size();
+  }
+  return A;
+}
+
+// One pass of pairwise aggregation: rows in order; an unpaired row takes its strongest unpaired
+// neighbour j (largest -a_ij, first in column order on ties) if -a_ij >= beta * max_k(-a_ik).
+int pairwise(const Csr& A, double beta, std::vector<int>& agg) {
+  agg.assign(A.n, -1);
+  int na = 0;
+  for (int i = 0; i < A.n; ++i) {
+    if (agg[i] >= 0) continue;
+    double mx = 0.0;
+    for (int64_t k = A.off[i]; k < A.off[i + 1]; ++k)
+      if (A.col[k] != i) mx = std::max(mx, -A.val[k]);
+    int best = -1;
+    double bv = 0.0;
+    for (int64_t k = A.off[i]; k < A.off[i + 1]; ++k) {
+      const int j = A.col[k];
+      if (j == i || agg[j] >= 0) continue;
+      const double s = -A.val[k];
+      if (s >= beta * mx && s > bv) {
+        bv = s;
+        best = j;
+      }
+    }
+    agg[i] = na;
+    if (best >= 0) agg[best] = na;
+    ++na;
+  }
+  return na;
+}
+
+// Member rows of every aggregate, ascending.
+void members(const std::vector<int>& agg, int na, std::vector<int64_t>& moff, std::vector<int>& mrow) {
+  moff.assign(na + 1, 0);
+  for (int a : agg) moff[a + 1]++;
+  for (int a = 0; a < na; ++a) moff[a + 1] += moff[a];
+  mrow.assign(agg.size(), 0);
+  std::vector<int64_t> fill(moff.begin(), moff.end() - 1);
+  for (size_t i = 0; i < agg.size(); ++i) mrow[fill[agg[i]]++] = (int)i;
+}
+
+// A_c = T^T A T for the aggregation T (row i -> column agg[i]); entries summed in the order
+// (aggregate member ascending, fine column ascending), so the result is reproducible.
+Csr galerkin(const Csr& A, const std::vector<int>& agg, int na) {
+  std::vector<int64_t> moff;
+  std::vector<int> mrow;
+  members(agg, na, moff, mrow);
+  Csr C;
+  C.n = na;
+  C.off.assign(na + 1, 0);
+  std::vector<int64_t> pos(na, -1);
+  std::vector<int> cols;
+  std::vector<double> vals;
+  for (int a = 0; a < na; ++a) {
+    cols.clear();
+    vals.clear();
+    for (int64_t m = moff[a]; m < moff[a + 1]; ++m) {
+      const int i = mrow[m];
+      for (int64_t k = A.off[i]; k < A.off[i + 1]; ++k) {
+        const int c = agg[A.col[k]];
+        if (pos[c] < 0) {
+          pos[c] = (int64_t)cols.size();
+          cols.push_back(c);
+          vals.push_back(0.0);
+        }
+        vals[pos[c]] += A.val[k];
+      }
+    }
+    std::vector<int> order(cols.size());
+    for (size_t k = 0; k < order.size(); ++k) order[k] = (int)k;
+    std::sort(order.begin(), order.end(), [&](int x, int y) { return cols[x] < cols[y]; });
+    for (int k : order) {
+      C.col.push_back(cols[k]);
+      C.val.push_back(vals[k]);
+      pos[cols[k]] = -1;
+    }
+    C.off[a + 1] = (int64_t)C.col.size();
+  }
+  return C;
+}
+
+// Largest eigenvalue of D^-1 A by 30 power steps from a fixed start vector.
+double lambda_max(const Csr& A, const std::vector<double>& dinv) {
+  std::vector<double> v(A.n), w(A.n);
+  for (int i = 0; i < A.n; ++i) v[i] = 1.0 + 0.5 * std::sin(0.7 * i + 0.3);
+  double lam = 0.0;
+  for (int it = 0; it < 30; ++it) {
+    double nv = 0.0, nw = 0.0;
+    for (int i = 0; i < A.n; ++i) {
+      double s = 0.0;
+      for (int64_t k = A.off[i]; k < A.off[i + 1]; ++k) s += A.val[k] * v[A.col[k]];
+      w[i] = dinv[i] * s;
+      nv += v[i] * v[i];
+      nw += w[i] * w[i];
+    }
+    if (!(nw > 0.0)) return 1.0;
+    lam = std::sqrt(nw / nv);
+    const double sc = 1.0 / std::sqrt(nw);
+    for (int i = 0; i < A.n; ++i) v[i] = w[i] * sc;
+  }
+  return lam;
+}
+
+bool cholesky_lower(std::vector<double>& a, int n) {
+  for (int j = 0; j < n; ++j) {
+    double d = a[(size_t)j * n + j];
+    for (int k = 0; k < j; ++k) d -= a[(size_t)j * n + k] * a[(size_t)j * n + k];
+    if (!(d > 0.0)) return false;
+    d = std::sqrt(d);
+    a[(size_t)j * n + j] = d;
+    for (int i = j + 1; i < n; ++i) {
+      double s = a[(size_t)i * n + j];
+      for (int k = 0; k < j; ++k) s -= a[(size_t)i * n + k] * a[(size_t)j * n + k];
+      a[(size_t)i * n + j] = s / d;
+    }
+  }
+  return true;
+}
+
+int dense_inverse(const Csr& A, bool nullsp, std::vector<float>& out) {
+  const int n = A.n;
+  std::vector<double> a((size_t)n * n, 0.0);
+  double tr = 0.0;
+  for (int i = 0; i < n; ++i)
+    for (int64_t k = A.off[i]; k < A.off[i + 1]; ++k) {
+      a[(size_t)i * n + A.col[k]] += A.val[k];
+      if (A.col[k] == i) tr += A.val[k];
+    }
+  if (nullsp) {  // constant mode lifted to the mean diagonal: (A + s 1 1^T) 1 = (tr / n) 1
+    const double s = tr / ((double)n * n);
+    for (auto& x : a) x += s;
+  }
+  if (!cholesky_lower(a, n)) return -4;
+  out.assign((size_t)n * n, 0.0f);
+  std::vector<double> y(n);
+  for (int c = 0; c < n; ++c) {  // column c of the inverse: L L^T y = e_c
+    for (int i = 0; i < n; ++i) {
+      double s = i == c ? 1.0 : 0.0;
+      for (int k = 0; k < i; ++k) s -= a[(size_t)i * n + k] * y[k];
+      y[i] = s / a[(size_t)i * n + i];
+    }
+    for (int i = n - 1; i >= 0; --i) {
+      double s = y[i];
+      for (int k = i + 1; k < n; ++k) s -= a[(size_t)k * n + i] * y[k];
+      y[i] = s / a[(size_t)i * n + i];
+    }
+    for (int i = 0; i < n; ++i) out[(size_t)i * n + c] = (float)y[i];
+  }
+  return 0;
+}
+
+MlLevel make_level(const Csr& A, const std::vector<int>& agg, int na, int& rc) {
+  MlLevel L;
+  rc = 0;
+  L.n = A.n;
+  for (int i = 0; i < A.n; ++i) L.W = std::max<int>(L.W, (int)(A.off[i + 1] - A.off[i]));
+  L.col.resize((size_t)L.W * A.n);
+  L.val.assign((size_t)L.W * A.n, 0.0f);
+  L.dinv.resize(A.n);
+  std::vector<double> dinv(A.n, 0.0);
+  for (int i = 0; i < A.n; ++i) {
+    int s = 0;
+    double dg = 0.0;
+    for (int64_t k = A.off[i]; k < A.off[i + 1]; ++k, ++s) {
+      L.col[(size_t)s * A.n + i] = A.col[k];
+      L.val[(size_t)s * A.n + i] = (float)A.val[k];
+      if (A.col[k] == i) dg = A.val[k];
+    }
+    for (; s < L.W; ++s) L.col[(size_t)s * A.n + i] = i;
+    if (!(dg > 0.0)) rc = -5;
+    dinv[i] = dg > 0.0 ? 1.0 / dg : 0.0;
+    L.dinv[i] = (float)dinv[i];
+  }
+  L.lmax = lambda_max(A, dinv);
+  L.agg = agg;
+  std::vector<int64_t> moff;
+  std::vector<int> mrow;
+  members(agg, na, moff, mrow);
+  for (int a = 0; a < na; ++a) L.M = std::max<int>(L.M, (int)(moff[a + 1] - moff[a]));
+  L.mem.assign((size_t)L.M * na, -1);
+  for (int a = 0; a < na; ++a)
+    for (int64_t m = moff[a]; m < moff[a + 1]; ++m) L.mem[(size_t)(m - moff[a]) * na + a] = mrow[m];
+  return L;
+}
+
+}  // namespace
+
+int build_multilevel(int n, int WA, const int* A_col, const double* A_val, bool nullsp, int passes, double beta,
+                     int ncoarse, int max_dense, Multilevel& M) {
+  if (n < 1 || WA < 1 || passes < 1 || ncoarse < 1) return -1;
+  M = Multilevel{};
+  Csr A = csr_from_ell(n, WA, A_col, A_val);
+  for (;;) {
+    M.sizes.push_back(A.n);
+    M.nnz.push_back((int64_t)A.col.size());
+    if (A.n <= ncoarse) break;
+    if ((int)M.lv.size() >= ML_MAX_LEVELS) {
+      if (A.n > max_dense) return -3;
+      break;
+    }
+    std::vector<int> agg_tot(A.n);
+    for (int i = 0; i < A.n; ++i) agg_tot[i] = i;
+    Csr Ac = A;
+    for (int p = 0; p < passes; ++p) {
+      std::vector<int> agg;
+      const int na = pairwise(Ac, beta, agg);
+      Ac = galerkin(Ac, agg, na);
+      for (int i = 0; i < A.n; ++i) agg_tot[i] = agg[agg_tot[i]];
+    }
+    if (Ac.n > 0.85 * A.n) {  // coarsening stalled: solve this level directly if it is small enough
+      if (A.n > max_dense) return -2;
+      break;
+    }
+    int rc = 0;
+    M.lv.push_back(make_level(A, agg_tot, Ac.n, rc));
+    if (rc) return rc;
+    A = std::move(Ac);
+  }
+  M.nC = A.n;
+  return dense_inverse(A, nullsp, M.cinv);
+}
+
+}  // namespace dpm

@@ -26,7 +26,7 @@ EXPORTED = (
     "dpm_viscous_rhs_vector", "dpm_sgs_viscosity", "dpm_wall_model", "dpm_pcg_solve_noalloc",
     "dpm_advection_rhs_scalar", "dpm_viscous_rhs_scalar", "dpm_upload_scalars", "dpm_download_scalars",
     "dpm_learn_collect", "dpm_learn_train", "dpm_learn_set_gamma", "dpm_learn_sizes", "dpm_learn_export",
-    "dpm_learn_loss_grad",
+    "dpm_learn_loss_grad", "dpm_multilevel_hierarchy",
 )
 
 
@@ -78,6 +78,8 @@ def lib(build_if_missing=True):
     L.dpm_learn_train.argtypes = [vp, C.c_int, C.c_double, C.POINTER(abi.LearnReportT)]
     L.dpm_learn_set_gamma.argtypes = [vp, C.c_double]
     L.dpm_learn_sizes.argtypes = [vp, ip]
+    L.dpm_multilevel_hierarchy.argtypes = [C.c_int, C.c_int, ip, dp, C.c_int, C.c_int, ip, C.POINTER(C.c_longlong),
+                                           C.c_int]
     L.dpm_learn_export.argtypes = [vp, fp, C.c_void_p, ip, dp, dp, dp, dp, dp, fp]
     L.dpm_learn_loss_grad.argtypes = [vp, fp, dp, fp]
     L.dpm_download_scalars.argtypes = [vp, dp]

@@ -63,6 +63,7 @@ extern "C" {
 /* Pressure-solve forms. */
 #define DPM_PSOLVER_JACOBI_PCG 0
 #define DPM_PSOLVER_TWOLEVEL_FCG 1
+#define DPM_PSOLVER_MULTILEVEL_FCG 2  /* FCG + FP32 aggregation-multigrid V-cycle (no reference counterpart) */
 #define DPM_FORM_FP64 0     /* FP64 Krylov iterations                                    */
 #define DPM_FORM_MIXED 1    /* with DPM_PSOLVER_TWOLEVEL_FCG: inner iterations on an FP32 copy of
                                the operator and an FP32 preconditioned vector, inside an FP64
@@ -136,6 +137,11 @@ typedef struct dpm_params {
    * temperature, initial Obukhov length (0 = neutral) and whether its domain mean is updated. */
   double abl_z0_m, abl_z0_h, abl_T_surface, abl_L_obukhov;
   int abl_compute_L;
+  /* DPM_PSOLVER_MULTILEVEL_FCG: Chebyshev steps per smoothing (0: 3), over-correction of the
+   * coarse correction (0: 1.6), pairwise-aggregation passes per level (0: 3). */
+  int p_ml_degree;
+  double p_ml_overcorrect;
+  int p_ml_passes;
 } dpm_params_t;
 
 /* Per-step integral statistics (src/stats/mod_stats.f90:compute_stats_sums and
@@ -287,6 +293,12 @@ int dpm_learn_export(dpm_solver_t* s, float* feat, unsigned* lpk, int* col, doub
  * the stored parameters are left unchanged. */
 int dpm_learn_loss_grad(dpm_solver_t* s, const float* params, double* loss, float* grad);
 int dpm_download_scalars(dpm_solver_t* s, double* C);
+
+/* Aggregation hierarchy of DPM_PSOLVER_MULTILEVEL_FCG for an operator in padded ELL [width][n]
+ * (host memory, no device needed): rows and non-zeros per level, coarsest last.  Returns the
+ * number of levels (<= max_levels) or a negative code. */
+int dpm_multilevel_hierarchy(int n, int width, const int* col, const double* val, int nullsp, int passes,
+                             int* sizes, long long* nnz, int max_levels);
 
 /* ---- allocation-free Jacobi-PCG solve --------------------------------------------------------
  * No counterpart in the reference.  For callers that cannot allocate device memory when they
