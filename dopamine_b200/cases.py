@@ -489,6 +489,30 @@ def channel_config(nx=96, ny=64, nz=64, n_steps=1000, retau=395.0, noise_seed=20
                 description=f"channel {nx}x{ny}x{nz} Re_tau={retau:g}, KEP, Vreman, log-law wall model")
 
 
+def rb_config(nx=256, ny=256, nz=128, n_steps=10, noise_seed=20261207):
+    """Rayleigh-Benard convection (fourth configuration): 4 x 4 x 1 box, periodic sides, walls at
+    z = 0 (T = 1) and z = 1 (T = 0) with Bump-graded spacing, Boussinesq with g beta dT H = 1,
+    Ra = 1e7 and Pr = 0.7 (nu = sqrt(Pr / Ra), kappa = nu / Pr), KEP momentum, Vreman SGS, van
+    Leer TVD temperature and two passive scalars (Dirichlet 1 on the bottom wall for the first,
+    on the top wall for the second).  The seeded perturbation is +-10 % multiplicative noise on a
+    uniform 1e-2 drift velocity."""
+    ra, pr = 1.0e7, 0.7
+    nu = math.sqrt(pr / ra)
+    kappa = nu / pr
+    bottom = {"bc": "fixedTemp", "T": 1.0, "scalar_mode": (1, 0, 0, 0), "scalar_value": (1.0, 0, 0, 0)}
+    top = {"bc": "fixedTemp", "T": 0.0, "scalar_mode": (0, 1, 0, 0), "scalar_value": (0, 1.0, 0, 0)}
+    patches = [{"bc": "periodic"}] * 4 + [bottom, top]
+    h = 4.0 / nx
+    prm = dict(scheme=abi.SCHEME_KEP, temperature_scheme=abi.SCHEME_VANLEER_TVD, nu=nu, alpha_T=kappa, beta=1.0,
+               T_ref=0.5, g=(0.0, 0.0, -1.0), boussinesq=1, dt=0.3 * h, cfl_max=0.5, p_tol=1e-10,
+               p_max_iter=20000, rhie_chow_dual=0, sgs_model=abi.SGS_VREMAN, wall_model=abi.WM_NONE, n_scalars=2,
+               scalar_scheme=abi.SCHEME_VANLEER_TVD, scalar_diffusivity=(kappa, kappa, 0, 0),
+               scalar_pr_t=(0.85, 0.85, 0, 0))
+    return Case(f"rb{nx}x{ny}x{nz}", wall_box(nx, ny, nz, 4.0, 4.0, 1.0, 0.25), patches, prm, "uniform", 1.0e-2,
+                noise=0.10, noise_seed=noise_seed, n_steps=n_steps,
+                description=f"Rayleigh-Benard {nx}x{ny}x{nz}, Ra=1e7, Pr=0.7, T + 2 scalars (van Leer), Vreman")
+
+
 def hybrid_config(n=16, kind="mixed", n_steps=10):
     """Non-orthogonal unstructured box (third configuration, reduced size): unit cube of n^3
     jittered (+-0.2 h) hexes as a conforming mix of hexes, prisms and pyramids ("mixed") or as

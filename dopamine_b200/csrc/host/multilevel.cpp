@@ -65,7 +65,34 @@ int pairwise(const Csr& A, double beta, std::vector<int>& agg) {
     if (best >= 0) agg[best] = na;
     ++na;
   }
-  return na;
+  // A row left alone (its strong neighbours were all taken, typically around one strongly
+  // coupled row) joins the aggregate of its strongest neighbour if that holds fewer than 3 rows,
+  // so that a pass keeps coarsening on irregular meshes; 3 passes then give at most 27 rows.
+  std::vector<int> size(na, 0);
+  for (int i = 0; i < A.n; ++i) size[agg[i]]++;
+  for (int i = 0; i < A.n; ++i) {
+    if (size[agg[i]] != 1) continue;
+    int best = -1;
+    double bv = 0.0;
+    for (int64_t k = A.off[i]; k < A.off[i + 1]; ++k) {
+      const int j = A.col[k];
+      if (j == i || size[agg[j]] >= 3 || -A.val[k] <= bv) continue;
+      bv = -A.val[k];
+      best = j;
+    }
+    if (best < 0) continue;
+    size[agg[i]] = 0;
+    agg[i] = agg[best];
+    size[agg[best]]++;
+  }
+  // renumber the aggregates densely, in order of first appearance
+  std::vector<int> remap(na, -1);
+  int m = 0;
+  for (int i = 0; i < A.n; ++i) {
+    if (remap[agg[i]] < 0) remap[agg[i]] = m++;
+    agg[i] = remap[agg[i]];
+  }
+  return m;
 }
 
 // Member rows of every aggregate, ascending.
