@@ -1,7 +1,11 @@
 // Drop-in replacement of the reference's pressure-solve C ABI (src/solver/pressure_backend_petsc.c).
 //
-// Same symbols, arguments and status codes as the PETSc backend; the solve is the device PCG of
-// pcg.cuh instead of KSPCG + BoomerAMG.  Conventions kept from the reference:
+// Same symbols, arguments and status codes as the PETSc backend.  The preconditioner names of
+// fvm_petsc_set_pressure_solver select the Krylov kernel: "boomeramg" and "gamg" (the
+// reference's algebraic-multigrid choices, pressure_backend_petsc.c:10, :533-537) run flexible CG
+// with the FP32 aggregation-multigrid V-cycle of mlcg.cuh; "jacobi" (or -pc_type jacobi through
+// fvm_petsc_insert_option), and the state before any selection, run the Jacobi-PCG of pcg.cuh.
+// Conventions kept from the reference:
 //  * indices are 1-based, face_neighbor_global <= 0 or skip_face != 0 drops a face;
 //  * the operator is assembled once and cached; it is rebuilt when n_cells, n_faces or the
 //    reference cell change (pressure_backend_petsc.c:687-715), coefficients are not re-read;
@@ -23,6 +27,7 @@
 #include "../../../include/dopamine_b200.h"
 #include "common.cuh"
 #include "pcg.cuh"
+#include "mlsolve.cuh"
 
 namespace {
 using namespace dpm::gpu;
@@ -38,7 +43,14 @@ struct Ctx {
   double *val = nullptr, *dinv = nullptr, *b = nullptr, *x = nullptr, *r = nullptr, *z = nullptr, *p0 = nullptr,
          *p1 = nullptr, *q = nullptr, *bp = nullptr, *part = nullptr, *dout = nullptr, *tot = nullptr;
   void* kernel = nullptr;
+  dpm::gpu::MlSolver* ml = nullptr;  // multilevel solve of the current operator (AMG names)
+  int ml_nullsp = -1;
+  std::vector<int> hcol;             // host copy of the operator, kept for the multilevel set-up
+  std::vector<double> hval;
   void release() {
+    delete ml;
+    ml = nullptr;
+    ml_nullsp = -1;
     void* ps[] = {col, status, bar, val, dinv, b, x, r, z, p0, p1, q, bp, part, dout, tot};
     for (void* p : ps)
       if (p) cudaFree(p);
@@ -54,6 +66,7 @@ bool g_initialized = false;
 int g_io_on_device = 0;
 int g_local_rank = 0;
 int g_force_maxit = 0;
+int g_multilevel = 0;  // 1: the AMG names were selected
 double g_force_rtol = -1.0;
 
 template <class T>
@@ -135,8 +148,31 @@ int build(int n, int nfaces, const int* l2g, const int* fo, const int* fnl, cons
   g_ctx.nfaces = nfaces;
   g_ctx.ref_row = ref_row;
   g_ctx.WA = WA;
+  g_ctx.hcol = std::move(hc);
+  g_ctx.hval = std::move(hv);
   g_ctx.ready = true;
   return 0;
+}
+
+// Multilevel solve of the cached operator; its hierarchy is built on first use and again when
+// the null-space setting changes.
+int run_ml(double rtol, double atol, int maxit, int* reason, int* its, double* resid) {
+  const int nullsp = g_ctx.n_dir > 0 ? 0 : 1;
+  if (!g_ctx.ml || g_ctx.ml_nullsp != nullsp) {
+    delete g_ctx.ml;
+    g_ctx.ml = new dpm::gpu::MlSolver();
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g_ctx.device);
+    if (g_ctx.ml->setup(g_ctx.n, g_ctx.WA, g_ctx.hcol.data(), g_ctx.hval.data(), g_ctx.col, g_ctx.val, nullsp != 0, 0,
+                        0, 0.0, sms, g_ctx.bar, g_ctx.status, g_ctx.dout)) {
+      delete g_ctx.ml;
+      g_ctx.ml = nullptr;
+      return -26;
+    }
+    g_ctx.ml_nullsp = nullsp;
+  }
+  int rc = g_ctx.ml->launch(g_ctx.b, g_ctx.x, rtol, atol, maxit, 0, g_ctx.st, reason, its, resid);
+  return rc ? -33 : 0;
 }
 
 int run_pcg(double rtol, double atol, int maxit, int guess_zero, int* reason, int* its, double* resid) {
@@ -196,7 +232,11 @@ int fvm_petsc_backend_finalize(void) {
   return 0;
 }
 
-void fvm_petsc_set_pressure_solver(const char* solver_name) { (void)solver_name; }
+void fvm_petsc_set_pressure_solver(const char* solver_name) {
+  if (!solver_name) return;
+  if (std::strncmp(solver_name, "boomeramg", 9) == 0 || std::strncmp(solver_name, "gamg", 4) == 0) g_multilevel = 1;
+  else if (std::strncmp(solver_name, "jacobi", 6) == 0) g_multilevel = 0;
+}
 
 int fvm_petsc_device_io_supported(void) { return 1; }
 
@@ -213,6 +253,10 @@ void fvm_petsc_insert_option(const char* opt) {
   };
   if (const char* v = val("-ksp_max_it")) g_force_maxit = std::atoi(v);
   if (const char* v = val("-ksp_rtol")) g_force_rtol = std::atof(v);
+  if (const char* v = val("-pc_type")) {
+    if (std::strncmp(v, "jacobi", 6) == 0) g_multilevel = 0;
+    else if (std::strncmp(v, "hypre", 5) == 0 || std::strncmp(v, "gamg", 4) == 0) g_multilevel = 1;
+  }
 }
 
 void fvm_petsc_set_device_local_rank(int local_rank) { g_local_rank = local_rank; }
@@ -251,10 +295,10 @@ int fvm_petsc_solve_pressure(int n_cells_local, int n_cells_global, int n_faces,
   if (g_force_rtol > 0.0) rtol = g_force_rtol;
   int reason = 0, its = 0;
   double res = 0.0;
-  int rc = run_pcg(rtol, atol, maxit, 0, &reason, &its, &res);
+  int rc = g_multilevel ? run_ml(rtol, atol, maxit, &reason, &its, &res) : run_pcg(rtol, atol, maxit, 0, &reason, &its, &res);
   if (rc) return rc;
   int status = 0;
-  if (reason < 0) {
+  if (reason < 0) {  // retry as the reference does after a failed solve: from zero, 4x the cap, Jacobi
     rc = run_pcg(rtol, atol, 4 * maxit, 1, &reason, &its, &res);
     if (rc) return rc;
     if (reason < 0 && !(reason == -3 && (res < rtol * 1.0e4 || res < atol * 1.0e3))) status = -(1000 + reason);

@@ -212,6 +212,8 @@ __device__ __forceinline__ double ml_row64(const MlArgs& a, int i, const V* x) {
   return s;
 }
 
+// (a template so that every translation unit that includes this header may instantiate it)
+template <int V>
 __global__ void __launch_bounds__(ML_TPB, 2) k_mlcg(MlArgs a) {
   __shared__ MlDevLevel s_lv[ML_LEVELS];
   __shared__ double s_gat[1];

@@ -26,7 +26,7 @@
 #include "fcg.cuh"
 #include "kernels.cuh"
 #include "learn.cuh"
-#include "mlcg.cuh"
+#include "mlsolve.cuh"
 #include "pcg.cuh"
 #include "scalars.cuh"
 
@@ -210,9 +210,7 @@ struct Solver {
   size_t fcg_smem = 0;
   // multilevel flexible CG (p_solver == DPM_PSOLVER_MULTILEVEL_FCG)
   bool use_ml = false;
-  MlArgs ma{};
-  int ml_grid = 0;
-  std::vector<int> ml_sizes;
+  MlSolver ml;
   // state
   double time = 0.0;
   int64_t step = 0;
@@ -710,104 +708,20 @@ struct Solver {
     return setup_learned(T);
   }
 
-  // Multilevel FCG set-up: aggregation hierarchy on the host, FP32 levels on the device, Chebyshev
-  // coefficients per level from the estimated spectrum of D^-1 A_l (interval [lmax/10, lmax],
-  // lmax = 1.1 x the power-iteration estimate).
+  // Multilevel FCG set-up (csrc/cuda/mlsolve.cuh): hierarchy on the host, FP32 levels on the
+  // device, the FP64 operator shared with the plain solve.
   int setup_ml(int dev_sms) {
-    Multilevel M;
     const bool nullsp = S.dir_rows.empty();
-    const int passes = P.p_ml_passes > 0 ? P.p_ml_passes : 3;
-    int rc = build_multilevel(nc, S.WA, S.A_col.data(), S.A_val.data(), nullsp, passes, 0.25, 300, 1024, M);
-    if (rc) return DPM_ERR_UNSUPPORTED;
-    const int nlev = (int)M.lv.size();
-    const int deg = P.p_ml_degree > 0 ? P.p_ml_degree : 3;
-    if (nlev > ML_LEVELS || deg > ML_DEG) return DPM_ERR_ARG;
-    int per_sm = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mlcg, ML_TPB, 0));
-    if (per_sm < 1) return DPM_ERR_UNSUPPORTED;
-    ml_grid = dev_sms * std::min(per_sm, 2);
-    const int64_t threads = (int64_t)ml_grid * ML_TPB;
-    std::vector<MlDevLevel> hl(nlev);
-    for (int l = 0; l < nlev; ++l) {
-      const MlLevel& L = M.lv[l];
-      MlDevLevel& D = hl[l];
-      D = MlDevLevel{};
-      D.n = L.n; D.W = L.W; D.M = L.M;
-      D.n_next = l + 1 < nlev ? M.lv[l + 1].n : M.nC;
-      D.MP = 1;
-      D.lgMP = 0;
-      while (D.MP < L.M) { D.MP *= 2; D.lgMP++; }
-      if (D.MP > 32) return DPM_ERR_UNSUPPORTED;
-      // lanes per row: spread small levels over up to 32 lanes (no more lanes than entries)
-      int g = 1;
-      D.lgG = 0;
-      while (g < 32 && (int64_t)L.n * g * 2 <= threads && 2 * g <= L.W) { g *= 2; D.lgG++; }
-      D.rows_per_pass = (int)std::min<int64_t>(4, std::max<int64_t>(1, (L.n + threads - 1) / threads));
-      g = 1;
-      D.lgGR = 0;
-      while (D.MP * g * 2 <= 32 && (int64_t)D.n_next * D.MP * g * 2 <= threads && 2 * g <= L.W) { g *= 2; D.lgGR++; }
-      D.col = mem.upload(L.col); D.val = mem.upload(L.val); D.dinv = mem.upload(L.dinv);
-      D.agg = mem.upload(L.agg); D.mem = mem.upload(L.mem);
-      D.b = mem.alloc<float>(L.n); D.x0 = mem.alloc<float>(L.n); D.x1 = mem.alloc<float>(L.n);
-      D.d = mem.alloc<float>(L.n);
-      if (!D.col || !D.val || !D.dinv || !D.agg || !D.mem || !D.b || !D.x0 || !D.x1 || !D.d) return DPM_ERR_CUDA;
-      const double lmax = 1.1 * L.lmax, lmin = 0.1 * lmax;
-      const double th = 0.5 * (lmax + lmin), de = 0.5 * (lmax - lmin), sig = th / de;
-      D.inv_theta = (float)(1.0 / th);
-      double rho = 1.0 / sig;
-      for (int j = 1; j < ML_DEG; ++j) {
-        const double rhon = 1.0 / (2.0 * sig - rho);
-        D.c1[j] = (float)(rhon * rho);
-        D.c2[j] = (float)(2.0 * rhon / de);
-        rho = rhon;
-      }
-    }
-    ma = MlArgs{};
-    ma.n = nc; ma.WA = S.WA; ma.nlev = nlev; ma.degree = deg; ma.nC = M.nC;
-    ma.col = d.Acol; ma.val = d.Aval;
-    if (nlev > 0) {
-      MlDevLevel* dl = mem.alloc<MlDevLevel>(nlev);
-      if (!dl) return DPM_ERR_CUDA;
-      CK(cudaMemcpyAsync(dl, hl.data(), sizeof(MlDevLevel) * nlev, cudaMemcpyHostToDevice, st));
-      CK(cudaStreamSynchronize(st));
-      ma.lv = dl;
-    }
-    ma.cinv = mem.upload(M.cinv);
-    ma.bC = mem.alloc<float>(M.nC); ma.xC = mem.alloc<float>(M.nC);
-    ma.oc = (float)(P.p_ml_overcorrect > 0.0 ? P.p_ml_overcorrect : 1.6);
-    ma.r = mem.alloc<double>(nc); ma.p = mem.alloc<double>(nc); ma.q = mem.alloc<double>(nc);
-    ma.w = mem.alloc<double>(nc);
-    ma.bar = cg_bar; ma.status = cg_status; ma.dout = cg_dout;
-    ma.nullsp = nullsp ? 1 : 0;
-    ma.stall_window = 50;
-    ma.partials = mem.alloc<double>((size_t)2 * FCG_SLOT * ml_grid);
-    if (!ma.cinv || !ma.bC || !ma.xC || !ma.r || !ma.p || !ma.q || !ma.w || !ma.partials) return DPM_ERR_CUDA;
-    ml_sizes = M.sizes;
+    int rc = ml.setup(nc, S.WA, S.A_col.data(), S.A_val.data(), d.Acol, d.Aval, nullsp, P.p_ml_passes, P.p_ml_degree,
+                      P.p_ml_overcorrect, dev_sms, cg_bar, cg_status, cg_dout);
+    if (rc) return rc;
     use_ml = true;
     return 0;
   }
   int ml_launch(const double* rhs, double* x, double rtol, double atol, int maxit, int guess_zero, int* its,
                 double* resid, int* reason) {
-    MlArgs a = ma;
-    a.b = rhs; a.x = x; a.rtol = rtol; a.atol = atol; a.maxit = maxit; a.guess_zero = guess_zero;
-    CK(cudaMemsetAsync(cg_bar, 0, 2 * sizeof(unsigned), st));
-    CK(cudaMemsetAsync(cg_status, 0, 4 * sizeof(int), st));
-    void* args[] = {&a};
-    CK(cudaLaunchCooperativeKernel((void*)k_mlcg, dim3(ml_grid), dim3(ML_TPB), args, 0, st));
     launches++;
-    int h_st[4];
-    double h_d[4];
-    CK(cudaMemcpyAsync(h_st, cg_status, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(h_d, cg_dout, 4 * sizeof(double), cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    if (h_st[2]) {
-      std::fprintf(stderr, "dopamine_b200: multilevel FCG grid barrier timed out\n");
-      return DPM_ERR_CUDA;
-    }
-    *reason = h_st[0];
-    *its = h_st[1];
-    *resid = h_d[0];
-    return 0;
+    return ml.launch(rhs, x, rtol, atol, maxit, guess_zero, st, reason, its, resid);
   }
 
   // Static per-cell features of the learned term, in the renumbered order:

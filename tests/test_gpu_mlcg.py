@@ -95,3 +95,32 @@ def test_mlcg_iterations_on_the_channel():
     assert its[abi.PSOLVER_MULTILEVEL_FCG] * 3 <= its[abi.PSOLVER_TWOLEVEL_FCG], its
     assert its[abi.PSOLVER_MULTILEVEL_FCG] * 10 <= its[abi.PSOLVER_JACOBI_PCG], its
     assert div[abi.PSOLVER_MULTILEVEL_FCG] <= 10 * div[abi.PSOLVER_JACOBI_PCG] + 1e-12, div
+
+
+def test_dropin_boomeramg_name_selects_the_multilevel_solve():
+    """The drop-in pressure ABI: after fvm_petsc_set_pressure_solver("boomeramg") (what the
+    reference's Fortran caller selects, src/solver/mod_pressure_solver.f90:136) the solve runs the
+    multilevel form; it reaches the same solution as the Jacobi-PCG selection in far fewer
+    iterations.  The selection is put back to Jacobi and the backend finalised afterwards."""
+    from test_zz_no_alloc import neumann_system, reference_solve
+    from dopamine_b200 import solver as S
+
+    L = S.lib()
+    n, fo, fn, coeff, diag = neumann_system(40, 36, 32, seed=12)
+    rhs = np.random.default_rng(8).standard_normal(n) + 0.3
+    try:
+        L.fvm_petsc_set_pressure_solver(b"jacobi")
+        x_j, its_j, _ = reference_solve(L, n, fo, fn, coeff, diag, rhs, np.zeros(n), 1e-10, 1e-50, 4000)
+        L.fvm_petsc_set_pressure_solver(b"boomeramg")
+        x_m, its_m, res_m = reference_solve(L, n, fo, fn, coeff, diag, rhs, np.zeros(n), 1e-10, 1e-50, 4000)
+    finally:
+        # the backend caches its operator by size, as the reference's does: drop it for later users
+        L.fvm_petsc_set_pressure_solver(b"jacobi")
+        L.fvm_petsc_backend_finalize()
+    rel = np.linalg.norm((x_m - x_m.mean()) - (x_j - x_j.mean())) / np.linalg.norm(x_j - x_j.mean())
+    print(f"drop-in: jacobi {its_j} its, multilevel {its_m} its, solution rel diff {rel:.2e}")
+    assert rel <= 1e-6, rel  # both stop at ||r|| <= 1e-10 ||b'||; the operator's condition number is ~1e4
+    assert 0 < its_m * 5 <= its_j, (its_m, its_j)
+    from test_zz_no_alloc import apply
+    bp = rhs - rhs.mean()
+    assert np.linalg.norm(bp - apply(n, fo, fn, coeff, diag, x_m)) <= 10 * 1e-10 * np.linalg.norm(bp)
