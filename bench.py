@@ -9,9 +9,9 @@ stages, three Poisson solves) of the whole mesh.  The timed form is the chosen p
 Jacobi-PCG form is timed beside it on the same workload and reported in the config.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                    [--config channel|tgv|rb|mixed] [--psolver fcg|pcg|ml] [--no-plain]
+                    [--config channel|tgv|rb|mixed|urban] [--psolver fcg|pcg|ml] [--no-plain]
 
-(the rb and mixed configurations exceed the two-level kernel's part size: run them with
+(the rb, mixed and urban configurations exceed the two-level kernel's part size: run them with
 --psolver ml)
 
 value   : cell-steps/s with the state resident in HBM (CUDA events around K steps, max over ranks)
@@ -122,6 +122,8 @@ def make_case(name):
         return cases.rb_config(256, 256, 128)
     if name == "mixed":
         return cases.hybrid_config(n=128, kind="mixed")
+    if name == "urban":
+        return cases.urban_config()
     raise ValueError(name)
 
 
@@ -273,7 +275,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="dopamine_b200")
-    ap.add_argument("--config", default="channel", choices=["channel", "tgv", "rb", "mixed"])
+    ap.add_argument("--config", default="channel", choices=["channel", "tgv", "rb", "mixed", "urban"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip timing the plain FP64 Jacobi-PCG form")
     ap.add_argument("--no-learned", action="store_true", help="two-level FCG without the learned term")
@@ -289,7 +291,9 @@ def main():
     cfg_name = {"channel": "channel 96x64x64 Re_tau=395, KEP, Vreman, log-law wall model",
                 "tgv": "Taylor-Green 64^3, CDS",
                 "rb": "Rayleigh-Benard 256x256x128 (8.4M cells), Ra=1e7, Pr=0.7, T + 2 scalars van Leer, Vreman",
-                "mixed": "jittered unit box 128^3 as hexes + prisms + pyramids (4.9M cells), AMD, Koren TVD"}[args.config]
+                "mixed": "jittered unit box 128^3 as hexes + prisms + pyramids (4.9M cells), AMD, Koren TVD",
+                "urban": "urban canopy 1000x1000x300 m, 400x400x125 with 200 seeded obstacles carved out "
+                         "(19.3M cells), MOST (L = -100 m), AMD, KEP, T + 1 scalar"}[args.config]
 
     if args.impl == "reference":
         if rank != 0:

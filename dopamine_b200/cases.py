@@ -149,6 +149,96 @@ def wall_box(nx, ny, nz, lx, ly, lz, bump_z):
     return m
 
 
+def urban_box(nx, ny, nz, lx=1000.0, ly=1000.0, lz=300.0, n_blocks=200, seed=20261208, side=(10.0, 60.0),
+              height=(10.0, 80.0), margin=40.0):
+    """Urban canopy: uniform hex box with seeded cuboid obstacles standing on the ground carved
+    out (fifth configuration).  Block i has sides side[0] + (side[1] - side[0]) u and height
+    height[0] + (height[1] - height[0]) u (u: SplitMix64 draws), its centre placed uniformly so
+    that it keeps `margin` from the lateral boundaries (which stay periodic); a cell is removed
+    when its centre lies inside a block.  Patches: x0, xL, y0, yL (lateral), ground, top,
+    obstacles (every face between a fluid cell and a removed one)."""
+    dx, dy, dz = lx / nx, ly / ny, lz / nz
+    r = _fast_uniform(5 * n_blocks, seed).reshape(n_blocks, 5)
+    sx = side[0] + (side[1] - side[0]) * r[:, 0]
+    sy = side[0] + (side[1] - side[0]) * r[:, 1]
+    hz = height[0] + (height[1] - height[0]) * r[:, 2]
+    cx = margin + 0.5 * sx + (lx - 2.0 * margin - sx) * r[:, 3]
+    cy = margin + 0.5 * sy + (ly - 2.0 * margin - sy) * r[:, 4]
+    solid = np.zeros((nz, ny, nx), dtype=bool)
+    for b in range(n_blocks):
+        # cells whose centre (i + 1/2) h lies in [c - s/2, c + s/2]
+        i0 = max(0, int(math.ceil((cx[b] - 0.5 * sx[b]) / dx - 0.5)))
+        i1 = min(nx - 1, int(math.floor((cx[b] + 0.5 * sx[b]) / dx - 0.5)))
+        j0 = max(0, int(math.ceil((cy[b] - 0.5 * sy[b]) / dy - 0.5)))
+        j1 = min(ny - 1, int(math.floor((cy[b] + 0.5 * sy[b]) / dy - 0.5)))
+        k1 = min(nz - 1, int(math.floor(hz[b] / dz - 0.5)))
+        if i1 >= i0 and j1 >= j0 and k1 >= 0:
+            solid[: k1 + 1, j0 : j1 + 1, i0 : i1 + 1] = True
+    fluid = ~solid
+    x = np.arange(nx + 1) * dx
+    y = np.arange(ny + 1) * dy
+    z = np.arange(nz + 1) * dz
+    X, Y, Z = np.meshgrid(x, y, z, indexing="ij")
+    xyz = np.stack([X.transpose(2, 1, 0).ravel(), Y.transpose(2, 1, 0).ravel(), Z.transpose(2, 1, 0).ravel()], axis=1)
+
+    def nid(i, j, k):
+        return i + (nx + 1) * (j + (ny + 1) * k)
+
+    k, j, i = np.nonzero(fluid)  # k, j, i order, as the structured box numbers its hexes
+    hexes = np.stack([nid(i, j, k), nid(i + 1, j, k), nid(i + 1, j + 1, k), nid(i, j + 1, k),
+                      nid(i, j, k + 1), nid(i + 1, j, k + 1), nid(i + 1, j + 1, k + 1), nid(i, j + 1, k + 1)], axis=1)
+    quads, patch = [], []
+
+    def add(pid, q):
+        quads.append(q)
+        patch.append(np.full(q.shape[0], pid, dtype=np.int32))
+
+    def xface(ip, j, k):
+        return np.stack([nid(ip, j, k), nid(ip, j + 1, k), nid(ip, j + 1, k + 1), nid(ip, j, k + 1)], 1)
+
+    def yface(i, jp, k):
+        return np.stack([nid(i, jp, k), nid(i + 1, jp, k), nid(i + 1, jp, k + 1), nid(i, jp, k + 1)], 1)
+
+    def zface(i, j, kp):
+        return np.stack([nid(i, j, kp), nid(i + 1, j, kp), nid(i + 1, j + 1, kp), nid(i, j + 1, kp)], 1)
+
+    k, j = np.nonzero(fluid[:, :, 0])
+    add(0, xface(0, j, k))
+    k, j = np.nonzero(fluid[:, :, nx - 1])
+    add(1, xface(nx, j, k))
+    k, i = np.nonzero(fluid[:, 0, :])
+    add(2, yface(i, 0, k))
+    k, i = np.nonzero(fluid[:, ny - 1, :])
+    add(3, yface(i, ny, k))
+    j, i = np.nonzero(fluid[0])
+    add(4, zface(i, j, 0))
+    j, i = np.nonzero(fluid[nz - 1])
+    add(5, zface(i, j, nz))
+    obs = []
+    m = fluid[:, :, :-1] != fluid[:, :, 1:]        # x-neighbours, one fluid one solid
+    k, j, i = np.nonzero(m)
+    obs.append(xface(i + 1, j, k))
+    m = fluid[:, :-1, :] != fluid[:, 1:, :]
+    k, j, i = np.nonzero(m)
+    obs.append(yface(i, j + 1, k))
+    m = fluid[:-1] != fluid[1:]
+    k, j, i = np.nonzero(m)
+    obs.append(zface(i, j, k + 1))
+    add(6, np.concatenate(obs))
+    q = np.concatenate(quads).astype(np.int32)
+    nh = hexes.shape[0]
+    return RawMesh(
+        xyz=np.ascontiguousarray(xyz, dtype=np.float64),
+        cell_type=np.full(nh, abi.EL_HEX8, dtype=np.int32),
+        cell_off=np.arange(0, 8 * nh + 1, 8, dtype=np.int64),
+        cell_nodes=hexes.astype(np.int32).ravel(),
+        bface_off=np.arange(0, 4 * q.shape[0] + 1, 4, dtype=np.int64),
+        bface_nodes=q.ravel(),
+        bface_patch=np.concatenate(patch),
+        patch_names=["x0", "xL", "y0", "yL", "ground", "top", "obstacles"],
+    )
+
+
 def _jittered_grid(n, jitter, seed):
     """Nodes of the unit cube's n^3 grid, interior nodes moved by a seeded uniform draw in
     [-jitter, jitter] * h per coordinate (boundary nodes stay, so the box stays a periodic box)."""
@@ -511,6 +601,32 @@ def rb_config(nx=256, ny=256, nz=128, n_steps=10, noise_seed=20261207):
     return Case(f"rb{nx}x{ny}x{nz}", wall_box(nx, ny, nz, 4.0, 4.0, 1.0, 0.25), patches, prm, "uniform", 1.0e-2,
                 noise=0.10, noise_seed=noise_seed, n_steps=n_steps,
                 description=f"Rayleigh-Benard {nx}x{ny}x{nz}, Ra=1e7, Pr=0.7, T + 2 scalars (van Leer), Vreman")
+
+
+def urban_config(nx=400, ny=400, nz=125, n_blocks=200, n_steps=10, lx=1000.0, ly=1000.0, lz=300.0,
+                 noise_seed=20261209):
+    """Urban-canopy atmospheric boundary layer (fifth configuration): lx x ly x lz metres with
+    seeded cuboid obstacles carved out (urban_box), periodic lateral boundaries, MOST wall model
+    on the ground and the obstacles (z0_m 0.1 m, z0_h 0.01 m, surface 302 K over 300 K air, Obukhov
+    length -100 m (unstable) held fixed), slip top, AMD SGS, KEP momentum, Boussinesq temperature and one
+    passive scalar (Dirichlet 1 on the ground) with van Leer TVD, constant streamwise pressure
+    gradient u_tau^2 / lz with u_tau = 0.5 m/s.  Initial state: 5 m/s streamwise with seeded
+    +-10 % multiplicative noise."""
+    mesh = urban_box(nx, ny, nz, lx, ly, lz, n_blocks)
+    wall = {"bc": "wallModel"}
+    patches = [{"bc": "periodic"}] * 4 + [dict(wall, scalar_mode=(1, 0, 0, 0), scalar_value=(1.0, 0, 0, 0)),
+                                          {"bc": "slip"}, dict(wall)]
+    dx = lx / nx
+    u0 = 5.0
+    prm = dict(scheme=abi.SCHEME_KEP, sgs_model=abi.SGS_AMD, wall_model=abi.WM_MOST, nu=1.5e-5, alpha_T=2.1e-5,
+               beta=1.0 / 300.0, T_ref=300.0, g=(0.0, 0.0, -9.81), boussinesq=1, temperature_scheme=abi.SCHEME_VANLEER_TVD,
+               f_const=(0.25 / lz, 0.0, 0.0), dt=0.3 * dx / (1.5 * u0), cfl_max=0.5, p_tol=1e-10, p_max_iter=20000,
+               rhie_chow_dual=0, n_scalars=1, scalar_scheme=abi.SCHEME_VANLEER_TVD, scalar_diffusivity=(2.1e-5, 0, 0, 0),
+               scalar_pr_t=(0.85, 0, 0, 0), abl_z0_m=0.1, abl_z0_h=0.01, abl_T_surface=302.0,
+               abl_L_obukhov=-100.0, abl_compute_L=0)
+    return Case(f"urban{nx}x{ny}x{nz}", mesh, patches, prm, "uniform", u0, noise=0.10, noise_seed=noise_seed,
+                n_steps=n_steps,
+                description=f"urban canopy {nx}x{ny}x{nz} ({mesh.n_cells} fluid cells, {n_blocks} blocks), MOST, AMD")
 
 
 def hybrid_config(n=16, kind="mixed", n_steps=10):
