@@ -167,6 +167,56 @@ __global__ void __launch_bounds__(TPB) k_ls_gradient_scalar(Dev d, const double*
   g[c] = a0; g[nc + c] = a1; g[2 * nc + c] = a2;
 }
 
+// Gradients of up to LS_SET scalar fields (temperature and passive scalars) in one pass: the
+// stencil indices and weights, the dominant traffic, are read once for all fields; each field's
+// sums are formed exactly as in k_ls_gradient_scalar.
+constexpr int LS_SET = 5;
+struct LsScalarSet {
+  int n;
+  const double* phi[LS_SET];
+  const double* pb[LS_SET];
+  double* g[LS_SET];
+};
+__global__ void __launch_bounds__(TPB) k_ls_gradient_scalars(Dev d, LsScalarSet q) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.nc) return;
+  const int nc = d.nc, nb = d.nb, W = d.W;
+  double pc[LS_SET], a0[LS_SET], a1[LS_SET], a2[LS_SET];
+#pragma unroll
+  for (int k = 0; k < LS_SET; ++k) {
+    pc[k] = k < q.n ? q.phi[k][c] : 0.0;
+    a0[k] = a1[k] = a2[k] = 0.0;
+  }
+  for (int s = 0; s < W; ++s) {
+    int v = __ldg(&d.ls_idx[s * nc + c]);
+    if (v == PADI) break;
+    const double w0 = __ldg(&d.ls_w[(0 * W + s) * nc + c]);
+    const double w1 = __ldg(&d.ls_w[(1 * W + s) * nc + c]);
+    const double w2 = __ldg(&d.ls_w[(2 * W + s) * nc + c]);
+#pragma unroll
+    for (int k = 0; k < LS_SET; ++k) {
+      if (k >= q.n) break;
+      double pv;
+      if (v >= 0) pv = q.phi[k][v];
+      else {
+        int b = -v - 1;
+        pv = b < nb ? q.pb[k][b] : pc[k];
+      }
+      double dd = pv - pc[k];
+      a0[k] += w0 * dd;
+      a1[k] += w1 * dd;
+      a2[k] += w2 * dd;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < LS_SET; ++k) {
+    if (k >= q.n) break;
+    q.g[k][c] = a0[k];
+    q.g[k][nc + c] = a1[k];
+    q.g[k][2 * nc + c] = a2[k];
+  }
+}
+
 // ------------------------------------------------------------------------------------------
 // SGS eddy viscosity.  Vreman (src/sgs/mod_vreman.f90:50-153), Smagorinsky (:295-364),
 // AMD (src/sgs/mod_amd.f90:31-207).  model: 1 Vreman, 2 Smagorinsky, 3 AMD.

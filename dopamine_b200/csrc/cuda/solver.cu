@@ -631,8 +631,17 @@ struct Solver {
   // cell gradients of U, of T when it is transported, and of every passive scalar
   void grad_all() {
     grad_U();
-    if (P.boussinesq) grad_scalar(F.T, Tb, gT);
-    for (int k = 0; k < ns; ++k) grad_scalar(Cs + (size_t)k * nc, Cb + (size_t)k * nb, gC + (size_t)k * 3 * nc);
+    LsScalarSet q{};  // temperature and passive scalars: one pass over the LS weights
+    if (P.boussinesq) {
+      q.phi[q.n] = F.T; q.pb[q.n] = Tb; q.g[q.n] = gT; q.n++;
+    }
+    for (int k = 0; k < ns; ++k) {
+      q.phi[q.n] = Cs + (size_t)k * nc; q.pb[q.n] = Cb + (size_t)k * nb; q.g[q.n] = gC + (size_t)k * 3 * nc; q.n++;
+    }
+    if (q.n > 0) {
+      k_ls_gradient_scalars<<<nblk(nc), TPB, 0, st>>>(d, q);
+      launches++;
+    }
   }
   // explicit right-hand side and RK3W update of T and the scalars (after the momentum predictor,
   // which reads the old T for the buoyancy term)
