@@ -217,6 +217,125 @@ __global__ void __launch_bounds__(TPB) k_ls_gradient_scalars(Dev d, LsScalarSet 
   }
 }
 
+// Green-Gauss gradients (src/numerics/mod_gradient.f90:38-304): grad_c = (1/V_c) sum_f phi_f S_f
+// gathered per cell over its faces in face order (the order in which the reference's face loop
+// adds them); phi_f = gc-interpolation on interior faces, plus the mean previous gradient . eps
+// (faded by the refinement blend) when a previous sweep is given; the boundary value otherwise.
+struct GgScalarSet {
+  int n;
+  const double* phi[LS_SET];
+  const double* pb[LS_SET];
+  const double* gprev[LS_SET];  // null: first sweep
+  double* g[LS_SET];
+};
+__global__ void __launch_bounds__(TPB) k_gg_gradient_scalars(Dev d, GgScalarSet q) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.nc) return;
+  const int nc = d.nc, nf = d.nf, nfi = d.nfi;
+  double a0[LS_SET], a1[LS_SET], a2[LS_SET];
+#pragma unroll
+  for (int k = 0; k < LS_SET; ++k) a0[k] = a1[k] = a2[k] = 0.0;
+  for (int s = 0; s < d.S; ++s) {
+    const int f = d.cf[s * nc + c];
+    if (f == PADI) break;
+    const double sf0 = d.sf[f], sf1 = d.sf[nf + f], sf2 = d.sf[2 * nf + f];
+    if (f < nfi) {
+      const int o = d.fo[f], n = d.fn[f];
+      const bool own = o == c;
+      const double w = d.gc[f];
+#pragma unroll
+      for (int k = 0; k < LS_SET; ++k) {
+        if (k >= q.n) break;
+        const double plain = w * q.phi[k][o] + (1.0 - w) * q.phi[k][n];
+        double pf = plain;
+        if (q.gprev[k]) {
+          const double* gp = q.gprev[k];
+          const double gm0 = w * gp[o] + (1.0 - w) * gp[n];
+          const double gm1 = w * gp[nc + o] + (1.0 - w) * gp[nc + n];
+          const double gm2 = w * gp[2 * nc + o] + (1.0 - w) * gp[2 * nc + n];
+          pf = plain + (gm0 * d.eps[f] + gm1 * d.eps[nf + f] + gm2 * d.eps[2 * nf + f]);
+          const double wb = d.wbl[f];
+          if (wb < 1.0) pf = plain + wb * (pf - plain);
+        }
+        if (own) { a0[k] = a0[k] + pf * sf0; a1[k] = a1[k] + pf * sf1; a2[k] = a2[k] + pf * sf2; }
+        else { a0[k] = a0[k] - pf * sf0; a1[k] = a1[k] - pf * sf1; a2[k] = a2[k] - pf * sf2; }
+      }
+    } else {
+      const int b = f - nfi;
+#pragma unroll
+      for (int k = 0; k < LS_SET; ++k) {
+        if (k >= q.n) break;
+        const double pf = q.pb[k][b];
+        a0[k] = a0[k] + pf * sf0; a1[k] = a1[k] + pf * sf1; a2[k] = a2[k] + pf * sf2;
+      }
+    }
+  }
+  const double v = d.vol[c];
+  const bool scale = v > 1.0e-30;
+  const double iv = 1.0 / v;
+#pragma unroll
+  for (int k = 0; k < LS_SET; ++k) {
+    if (k >= q.n) break;
+    q.g[k][c] = scale ? a0[k] * iv : a0[k];
+    q.g[k][nc + c] = scale ? a1[k] * iv : a1[k];
+    q.g[k][2 * nc + c] = scale ? a2[k] * iv : a2[k];
+  }
+}
+// gU[(i + 3 j) nc + c] = dU_j / dx_i
+__global__ void __launch_bounds__(TPB) k_gg_gradient_vector(Dev d, const double* __restrict__ U,
+                                                            const double* __restrict__ Ub, const double* gprev,
+                                                            double* __restrict__ gU) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.nc) return;
+  const int nc = d.nc, nf = d.nf, nfi = d.nfi, nb = d.nb;
+  double a[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int s = 0; s < d.S; ++s) {
+    const int f = d.cf[s * nc + c];
+    if (f == PADI) break;
+    const double sf[3] = {d.sf[f], d.sf[nf + f], d.sf[2 * nf + f]};
+    double uf[3];
+    bool own = true;
+    if (f < nfi) {
+      const int o = d.fo[f], n = d.fn[f];
+      own = o == c;
+      const double w = d.gc[f];
+      if (gprev) {
+        const double e0 = d.eps[f], e1 = d.eps[nf + f], e2 = d.eps[2 * nf + f];
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          const double gm0 = w * gprev[(0 + 3 * j) * nc + o] + (1.0 - w) * gprev[(0 + 3 * j) * nc + n];
+          const double gm1 = w * gprev[(1 + 3 * j) * nc + o] + (1.0 - w) * gprev[(1 + 3 * j) * nc + n];
+          const double gm2 = w * gprev[(2 + 3 * j) * nc + o] + (1.0 - w) * gprev[(2 + 3 * j) * nc + n];
+          uf[j] = w * U[j * nc + o] + (1.0 - w) * U[j * nc + n] + (gm0 * e0 + gm1 * e1 + gm2 * e2);
+        }
+        const double wb = d.wbl[f];
+        if (wb < 1.0)
+#pragma unroll
+          for (int j = 0; j < 3; ++j) {
+            const double plain = w * U[j * nc + o] + (1.0 - w) * U[j * nc + n];
+            uf[j] = plain + wb * (uf[j] - plain);
+          }
+      } else {
+#pragma unroll
+        for (int j = 0; j < 3; ++j) uf[j] = w * U[j * nc + o] + (1.0 - w) * U[j * nc + n];
+      }
+    } else {
+      const int b = f - nfi;
+#pragma unroll
+      for (int j = 0; j < 3; ++j) uf[j] = Ub[j * nb + b];
+    }
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+#pragma unroll
+      for (int i = 0; i < 3; ++i) a[i + 3 * j] = own ? a[i + 3 * j] + uf[j] * sf[i] : a[i + 3 * j] - uf[j] * sf[i];
+  }
+  const double v = d.vol[c];
+  const bool scale = v > 1.0e-30;
+  const double iv = 1.0 / v;
+#pragma unroll
+  for (int j = 0; j < 9; ++j) gU[j * nc + c] = scale ? a[j] * iv : a[j];
+}
+
 // ------------------------------------------------------------------------------------------
 // SGS eddy viscosity.  Vreman (src/sgs/mod_vreman.f90:50-153), Smagorinsky (:295-364),
 // AMD (src/sgs/mod_amd.f90:31-207).  model: 1 Vreman, 2 Smagorinsky, 3 AMD.

@@ -211,6 +211,7 @@ struct Solver {
   // multilevel flexible CG (p_solver == DPM_PSOLVER_MULTILEVEL_FCG)
   bool use_ml = false;
   MlSolver ml;
+  double *gg_prevU = nullptr, *gg_prevS = nullptr;  // Green-Gauss previous-sweep gradients
   // state
   double time = 0.0;
   int64_t step = 0;
@@ -357,6 +358,12 @@ struct Solver {
     cg_p1 = mem.alloc<double>(nc); cg_q = mem.alloc<double>(nc); cg_bp = mem.alloc<double>(nc);
     cg_x = mem.alloc<double>(nc);
     cg_bar = mem.alloc<unsigned>(2); cg_status = mem.alloc<int>(4); cg_dout = mem.alloc<double>(4);
+    if (P.gradient_scheme != DPM_GRAD_LEAST_SQUARES && P.gradient_scheme != DPM_GRAD_GREEN_GAUSS) return DPM_ERR_ARG;
+    if (gg()) {
+      gg_prevU = mem.alloc<double>((size_t)9 * nc);
+      gg_prevS = mem.alloc<double>((size_t)3 * LS_SET * nc);
+      if (!gg_prevU || !gg_prevS) return DPM_ERR_CUDA;
+    }
     if (!cg_dout || !F.fadv || !aos_buf) return DPM_ERR_CUDA;
     // cooperative grid for the persistent PCG
     int dev_sms = 0, per_sm = 0, coop = 0;
@@ -434,11 +441,47 @@ struct Solver {
     velocity_bc(0, 1);
     velocity_bc(1, 1);
   }
+  // Gradients: least squares, or Green-Gauss with gg_sweeps() sweeps (src/solver/
+  // mod_fv_solver.f90:1003-1077, :2341-2369); the sweeps after the first read the previous
+  // sweep's gradient, copied aside.
+  bool gg() const { return P.gradient_scheme == DPM_GRAD_GREEN_GAUSS; }
+  int gg_sweeps() const { return P.gg_iterations > 0 ? P.gg_iterations : 2; }
   void grad_U() {
-    k_ls_gradient_vector<<<nblk(nc), TPB, 0, st>>>(d, F.U, F.Ub, F.gU);
+    if (!gg()) {
+      k_ls_gradient_vector<<<nblk(nc), TPB, 0, st>>>(d, F.U, F.Ub, F.gU);
+      launches++;
+      return;
+    }
+    k_gg_gradient_vector<<<nblk(nc), TPB, 0, st>>>(d, F.U, F.Ub, nullptr, F.gU);
     launches++;
+    for (int it = 2; it <= gg_sweeps(); ++it) {
+      copy(gg_prevU, F.gU, (size_t)9 * nc);
+      k_gg_gradient_vector<<<nblk(nc), TPB, 0, st>>>(d, F.U, F.Ub, gg_prevU, F.gU);
+      launches++;
+    }
+  }
+  // Green-Gauss sweeps of a set of scalar fields (slot k of the previous-gradient scratch per field)
+  void gg_scalars(GgScalarSet q) {
+    for (int k = 0; k < LS_SET; ++k) q.gprev[k] = nullptr;
+    k_gg_gradient_scalars<<<nblk(nc), TPB, 0, st>>>(d, q);
+    launches++;
+    for (int it = 2; it <= gg_sweeps(); ++it) {
+      for (int k = 0; k < q.n; ++k) {
+        double* prev = gg_prevS + (size_t)k * 3 * nc;
+        copy(prev, q.g[k], (size_t)3 * nc);
+        q.gprev[k] = prev;
+      }
+      k_gg_gradient_scalars<<<nblk(nc), TPB, 0, st>>>(d, q);
+      launches++;
+    }
   }
   void grad_scalar(const double* phi, const double* pb, double* g) {
+    if (gg()) {
+      GgScalarSet q{};
+      q.n = 1; q.phi[0] = phi; q.pb[0] = pb; q.g[0] = g;
+      gg_scalars(q);
+      return;
+    }
     k_ls_gradient_scalar<<<nblk(nc), TPB, 0, st>>>(d, phi, pb, g);
     launches++;
   }
@@ -638,7 +681,12 @@ struct Solver {
     for (int k = 0; k < ns; ++k) {
       q.phi[q.n] = Cs + (size_t)k * nc; q.pb[q.n] = Cb + (size_t)k * nb; q.g[q.n] = gC + (size_t)k * 3 * nc; q.n++;
     }
-    if (q.n > 0) {
+    if (q.n > 0 && gg()) {
+      GgScalarSet h{};
+      h.n = q.n;
+      for (int k = 0; k < q.n; ++k) { h.phi[k] = q.phi[k]; h.pb[k] = q.pb[k]; h.g[k] = q.g[k]; }
+      gg_scalars(h);
+    } else if (q.n > 0) {
       k_ls_gradient_scalars<<<nblk(nc), TPB, 0, st>>>(d, q);
       launches++;
     }

@@ -64,6 +64,8 @@ extern "C" {
 #define DPM_PSOLVER_JACOBI_PCG 0
 #define DPM_PSOLVER_TWOLEVEL_FCG 1
 #define DPM_PSOLVER_MULTILEVEL_FCG 2  /* FCG + FP32 aggregation-multigrid V-cycle (no reference counterpart) */
+#define DPM_GRAD_LEAST_SQUARES 0
+#define DPM_GRAD_GREEN_GAUSS 1
 #define DPM_FORM_FP64 0     /* FP64 Krylov iterations                                    */
 #define DPM_FORM_MIXED 1    /* with DPM_PSOLVER_TWOLEVEL_FCG: inner iterations on an FP32 copy of
                                the operator and an FP32 preconditioned vector, inside an FP64
@@ -142,6 +144,11 @@ typedef struct dpm_params {
   int p_ml_degree;
   double p_ml_overcorrect;
   int p_ml_passes;
+  /* Cell gradients (src/solver/mod_fv_solver.f90:85-86 gradient_scheme, gg_iterations):
+   * DPM_GRAD_LEAST_SQUARES (default) or DPM_GRAD_GREEN_GAUSS with gg_iterations sweeps (the
+   * sweeps after the first add the eps.grad skewness correction; 0 means the reference's 2). */
+  int gradient_scheme;
+  int gg_iterations;
 } dpm_params_t;
 
 /* Per-step integral statistics (src/stats/mod_stats.f90:compute_stats_sums and

@@ -724,16 +724,133 @@ struct Solver {
       for (int i = 0; i < 3; ++i) g[3 * c + i] = acc[i];
     }
   }
-  // src/solver/mod_fv_solver.f90:1003-1077 (least-squares branch)
+  // src/numerics/mod_gradient.f90:38-168 (serial path): grad_c = (1/V_c) sum_f phi_f S_f, with
+  // phi_f the gc-interpolated face value (+ mean previous gradient . eps when gprev is given,
+  // faded by the refinement blend on interior faces) or the boundary value.  Each cell sums its
+  // faces in face order, as the face loop of the reference adds them.
+  void gg_gradient_scalar(const double* phi, const double* pb, double* g, const double* gprev) {
+#pragma omp parallel for schedule(static) num_threads(nthreads)
+    for (int64_t c = 0; c < nc; ++c) {
+      double acc[3] = {0, 0, 0};
+      for (int64_t k = m.cell_face_off[c]; k < m.cell_face_off[c + 1]; ++k) {
+        const int f = m.cell_faces[k];
+        const double* sf = &m.sf[3 * (size_t)f];
+        if (f < nfi) {
+          const int o = m.owner[f], n = m.neighbour[f];
+          const double w = m.gc[f];
+          double pf;
+          if (gprev) {
+            const double* e = &m.eps[3 * (size_t)f];
+            double gm[3];
+            for (int i = 0; i < 3; ++i) gm[i] = w * gprev[3 * (size_t)o + i] + (1.0 - w) * gprev[3 * (size_t)n + i];
+            const double plain = w * phi[o] + (1.0 - w) * phi[n];
+            pf = plain + (gm[0] * e[0] + gm[1] * e[1] + gm[2] * e[2]);
+            const double wb = refine_blend_weight(m.skew[f]);
+            if (wb < 1.0) pf = plain + wb * (pf - plain);
+          } else {
+            pf = w * phi[o] + (1.0 - w) * phi[n];
+          }
+          if (o == c) for (int i = 0; i < 3; ++i) acc[i] = acc[i] + pf * sf[i];
+          else for (int i = 0; i < 3; ++i) acc[i] = acc[i] - pf * sf[i];
+        } else {
+          const double pf = pb[f - nfi];
+          for (int i = 0; i < 3; ++i) acc[i] = acc[i] + pf * sf[i];
+        }
+      }
+      const double v = m.volume[c];
+      for (int i = 0; i < 3; ++i) g[3 * c + i] = v > SMALL ? acc[i] * (1.0 / v) : acc[i];
+    }
+  }
+  // src/numerics/mod_gradient.f90:172-304: the same per component, grad_U(i, j) = dU_j/dx_i.
+  void gg_gradient_vector(const double* Uc, const double* Ub, double* g, const double* gprev) {
+#pragma omp parallel for schedule(static) num_threads(nthreads)
+    for (int64_t c = 0; c < nc; ++c) {
+      double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+      for (int64_t k = m.cell_face_off[c]; k < m.cell_face_off[c + 1]; ++k) {
+        const int f = m.cell_faces[k];
+        const double* sf = &m.sf[3 * (size_t)f];
+        double uf[3];
+        bool own = true;
+        if (f < nfi) {
+          const int o = m.owner[f], n = m.neighbour[f];
+          own = o == c;
+          const double w = m.gc[f];
+          if (gprev) {
+            const double* e = &m.eps[3 * (size_t)f];
+            for (int j = 0; j < 3; ++j) {
+              double gm[3];
+              for (int i = 0; i < 3; ++i)
+                gm[i] = w * gprev[9 * (size_t)o + i + 3 * j] + (1.0 - w) * gprev[9 * (size_t)n + i + 3 * j];
+              uf[j] = w * Uc[3 * (size_t)o + j] + (1.0 - w) * Uc[3 * (size_t)n + j] + (gm[0] * e[0] + gm[1] * e[1] + gm[2] * e[2]);
+            }
+            const double wb = refine_blend_weight(m.skew[f]);
+            if (wb < 1.0)
+              for (int j = 0; j < 3; ++j) {
+                const double plain = w * Uc[3 * (size_t)o + j] + (1.0 - w) * Uc[3 * (size_t)n + j];
+                uf[j] = plain + wb * (uf[j] - plain);
+              }
+          } else {
+            for (int j = 0; j < 3; ++j) uf[j] = w * Uc[3 * (size_t)o + j] + (1.0 - w) * Uc[3 * (size_t)n + j];
+          }
+        } else {
+          for (int j = 0; j < 3; ++j) uf[j] = Ub[3 * (size_t)(f - nfi) + j];
+        }
+        for (int j = 0; j < 3; ++j)
+          for (int i = 0; i < 3; ++i) {
+            if (own) acc[i + 3 * j] = acc[i + 3 * j] + uf[j] * sf[i];
+            else acc[i + 3 * j] = acc[i + 3 * j] - uf[j] * sf[i];
+          }
+      }
+      const double v = m.volume[c];
+      for (int j = 0; j < 9; ++j) g[9 * c + j] = v > SMALL ? acc[j] * (1.0 / v) : acc[j];
+    }
+  }
+  bool green_gauss() const { return P.gradient_scheme == DPM_GRAD_GREEN_GAUSS; }
+  int gg_sweeps() const { return P.gg_iterations > 0 ? P.gg_iterations : 2; }
+  // src/solver/mod_fv_solver.f90:2341-2369 gradient_of_scalar
+  void gradient_of_scalar(const double* phi, const double* pb, double* g) {
+    if (!green_gauss()) {
+      ls_gradient_scalar(phi, pb, g);
+      return;
+    }
+    gg_gradient_scalar(phi, pb, g, nullptr);
+    std::vector<double> prev;
+    for (int it = 2; it <= gg_sweeps(); ++it) {
+      prev.assign(g, g + 3 * nc);
+      gg_gradient_scalar(phi, pb, g, prev.data());
+    }
+  }
+  // src/solver/mod_fv_solver.f90:1003-1077
   void compute_all_gradients() {
-    ls_gradient_vector(U.data(), U_bnd.data(), grad_U.data());
-    if (P.boussinesq) ls_gradient_scalar(T.data(), T_bnd.data(), grad_T.data());
+    if (!green_gauss()) {
+      ls_gradient_vector(U.data(), U_bnd.data(), grad_U.data());
+      if (P.boussinesq) ls_gradient_scalar(T.data(), T_bnd.data(), grad_T.data());
+      for (int sc = 0; sc < ns; ++sc)
+        ls_gradient_scalar(&Cs[(size_t)sc * nc], &C_bnd[(size_t)sc * nb], &grad_C[(size_t)sc * 3 * nc]);
+      return;
+    }
+    gg_gradient_vector(U.data(), U_bnd.data(), grad_U.data(), nullptr);
+    if (P.boussinesq) gg_gradient_scalar(T.data(), T_bnd.data(), grad_T.data(), nullptr);
     for (int sc = 0; sc < ns; ++sc)
-      ls_gradient_scalar(&Cs[(size_t)sc * nc], &C_bnd[(size_t)sc * nb], &grad_C[(size_t)sc * 3 * nc]);
+      gg_gradient_scalar(&Cs[(size_t)sc * nc], &C_bnd[(size_t)sc * nb], &grad_C[(size_t)sc * 3 * nc], nullptr);
+    std::vector<double> prev;
+    for (int it = 2; it <= gg_sweeps(); ++it) {
+      prev = grad_U;
+      gg_gradient_vector(U.data(), U_bnd.data(), grad_U.data(), prev.data());
+      if (P.boussinesq) {
+        prev = grad_T;
+        gg_gradient_scalar(T.data(), T_bnd.data(), grad_T.data(), prev.data());
+      }
+      for (int sc = 0; sc < ns; ++sc) {
+        double* gcs = &grad_C[(size_t)sc * 3 * nc];
+        prev.assign(gcs, gcs + 3 * nc);
+        gg_gradient_scalar(&Cs[(size_t)sc * nc], &C_bnd[(size_t)sc * nb], gcs, prev.data());
+      }
+    }
   }
   void compute_pressure_gradient() {
     if (skip_grad_p) return;
-    ls_gradient_scalar(p.data(), p_bnd.data(), gp.data());
+    gradient_of_scalar(p.data(), p_bnd.data(), gp.data());
   }
 
   // ---------------------------------------------------------------- SGS
@@ -1562,9 +1679,9 @@ struct Solver {
       if (incr) {
         for (int64_t c = 0; c < nc; ++c) p_tot[c] = phi_prev[c] + p[c];
         for (int64_t b = 0; b < nb; ++b) p_tot_bnd[b] = phi_prev_bnd[b] + p_bnd[b];
-        ls_gradient_scalar(p_tot.data(), p_tot_bnd.data(), gp.data());
+        gradient_of_scalar(p_tot.data(), p_tot_bnd.data(), gp.data());
       } else {
-        ls_gradient_scalar(p.data(), p_bnd.data(), gp.data());
+        gradient_of_scalar(p.data(), p_bnd.data(), gp.data());
       }
     }
     std::fill(rhs_p.begin(), rhs_p.end(), 0.0);
@@ -2181,6 +2298,10 @@ void orc_geometry(void* h, double* centroid, double* volume) {
   if (centroid) std::memcpy(centroid, s->m.centroid.data(), sizeof(double) * 3 * s->nc);
   if (volume) std::memcpy(volume, s->m.volume.data(), sizeof(double) * s->nc);
 }
+void orc_face_centres(void* h, double* fc) {
+  auto* s = static_cast<orc::Solver*>(h);
+  std::memcpy(fc, s->m.centre.data(), sizeof(double) * 3 * s->nf);
+}
 void orc_vertex_bounds(void* h, double* lo, double* hi) {
   auto* s = static_cast<orc::Solver*>(h);
   for (int k = 0; k < 3; ++k) { lo[k] = 1e308; hi[k] = -1e308; }
@@ -2330,6 +2451,16 @@ int orc_compute_dt(void* h, double* dt) { return static_cast<orc::Solver*>(h)->c
 // Single-operator checks on arbitrary inputs (same arguments as the product's dpm_* operators).
 void orc_ls_gradient_vector(void* h, const double* U, const double* U_bnd, double* g) {
   static_cast<orc::Solver*>(h)->ls_gradient_vector(U, U_bnd, g);
+}
+// Green-Gauss gradient of a cell scalar (cell-major g[3c + i]) with `sweeps` sweeps.
+void orc_gg_gradient_scalar(void* h, const double* phi, const double* pb, double* g, int sweeps) {
+  auto* s = static_cast<orc::Solver*>(h);
+  s->gg_gradient_scalar(phi, pb, g, nullptr);
+  std::vector<double> prev;
+  for (int it = 2; it <= sweeps; ++it) {
+    prev.assign(g, g + 3 * s->nc);
+    s->gg_gradient_scalar(phi, pb, g, prev.data());
+  }
 }
 void orc_advection(void* h, int scheme, const double* U, const double* U_bnd, const double* flux, const double* gU,
                    double* rhs) {

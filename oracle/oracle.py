@@ -45,6 +45,8 @@ def lib():
         L.orc_compute_dt.argtypes = [vp, dp]
         L.orc_compute_dt.restype = C.c_int
         L.orc_ls_gradient_vector.argtypes = [vp, dp, dp, dp]
+        L.orc_gg_gradient_scalar.argtypes = [vp, dp, dp, dp, C.c_int]
+        L.orc_face_centres.argtypes = [vp, dp]
         L.orc_advection.argtypes = [vp, C.c_int, dp, dp, dp, dp, dp]
         L.orc_viscous.argtypes = [vp, dp, dp, dp, dp, dp]
         L.orc_sgs.argtypes = [vp, C.c_int, dp, dp, C.c_double, dp]
