@@ -42,7 +42,8 @@ class RawMeshT(C.Structure):
 class PatchCfgT(C.Structure):
     _fields_ = [
         ("bc_id", C.c_int), ("U_val", C.c_double * 3), ("p_val", C.c_double), ("T_val", C.c_double),
-        ("scalar_mode", C.c_int * 4), ("scalar_value", C.c_double * 4),
+        ("scalar_mode", C.c_int * 4), ("scalar_value", C.c_double * 4), ("abl_z0_m", C.c_double),
+        ("abl_z0_h", C.c_double),
     ]
 
 
@@ -142,7 +143,8 @@ def default_params(**kw):
 
 
 def patch_cfgs(patches):
-    """patches: list of dicts {bc: name or id, U: (3,), p: float, T: float}."""
+    """patches: list of dicts {bc: name or id, U: (3,), p: float, T: float, scalar_mode, scalar_value,
+    z0_m, z0_h (MOST roughness of the patch; 0 = the global value)}."""
     arr = (PatchCfgT * max(1, len(patches)))()
     for i, pd in enumerate(patches):
         bc = pd["bc"]
@@ -155,6 +157,8 @@ def patch_cfgs(patches):
             arr[i].scalar_mode[k] = v
         for k, v in enumerate(pd.get("scalar_value", (0.0, 0.0, 0.0, 0.0))):
             arr[i].scalar_value[k] = v
+        arr[i].abl_z0_m = pd.get("z0_m", 0.0)
+        arr[i].abl_z0_h = pd.get("z0_h", 0.0)
     return arr
 
 

@@ -607,7 +607,8 @@ def urban_config(nx=400, ny=400, nz=125, n_blocks=200, n_steps=10, lx=1000.0, ly
                  noise_seed=20261209):
     """Urban-canopy atmospheric boundary layer (fifth configuration): lx x ly x lz metres with
     seeded cuboid obstacles carved out (urban_box), periodic lateral boundaries, MOST wall model
-    on the ground and the obstacles (z0_m 0.1 m, z0_h 0.01 m, surface 302 K over 300 K air, Obukhov
+    on the ground (z0_m 0.1 m, z0_h 0.01 m) and the obstacles (their own z0_m 0.05 m, z0_h 0.005 m,
+    the per-patch override), surface 302 K over 300 K air, Obukhov
     length -100 m (unstable) held fixed), slip top, AMD SGS, KEP momentum, Boussinesq temperature and one
     passive scalar (Dirichlet 1 on the ground) with van Leer TVD, constant streamwise pressure
     gradient u_tau^2 / lz with u_tau = 0.5 m/s.  Initial state: 5 m/s streamwise with seeded
@@ -615,7 +616,7 @@ def urban_config(nx=400, ny=400, nz=125, n_blocks=200, n_steps=10, lx=1000.0, ly
     mesh = urban_box(nx, ny, nz, lx, ly, lz, n_blocks)
     wall = {"bc": "wallModel"}
     patches = [{"bc": "periodic"}] * 4 + [dict(wall, scalar_mode=(1, 0, 0, 0), scalar_value=(1.0, 0, 0, 0)),
-                                          {"bc": "slip"}, dict(wall)]
+                                          {"bc": "slip"}, dict(wall, z0_m=0.05, z0_h=0.005)]
     dx = lx / nx
     u0 = 5.0
     prm = dict(scheme=abi.SCHEME_KEP, sgs_model=abi.SGS_AMD, wall_model=abi.WM_MOST, nu=1.5e-5, alpha_T=2.1e-5,

@@ -222,10 +222,11 @@ __device__ __forceinline__ void most_res_d(double us, double ts, double L, doubl
   FT = ts - MOST_KAPPA_D * (To - Ts) / dh;
 }
 __global__ void k_most(Dev d, const double* __restrict__ U, const double* __restrict__ T, double* __restrict__ tau,
-                       double* __restrict__ qw, double* __restrict__ Lb, double L_cfg, double Ts, double z0m,
-                       double z0h) {
+                       double* __restrict__ qw, double* __restrict__ Lb, double L_cfg, double Ts,
+                       const double* __restrict__ bz0m, const double* __restrict__ bz0h) {
   int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= d.nb || d.bbc[b] != BC_WALL_MODEL) return;
+  const double z0m = bz0m[b], z0h = bz0h[b];  // per-face roughness (patch value or the global one)
   const int nc = d.nc, nf = d.nf, nb = d.nb;
   const int f = d.nfi + b, o = d.fo[f];
   const double n0 = d.nrm[f], n1 = d.nrm[nf + f], n2 = d.nrm[2 * nf + f];

@@ -188,6 +188,7 @@ struct Solver {
   double *sc_fadv = nullptr, *sc_fdif = nullptr, *bTval = nullptr, *bsval = nullptr;
   int* bsmode = nullptr;
   double *most_L = nullptr, *most_qw = nullptr;  // MOST per-face Obukhov length and heat flux
+  double *most_z0m = nullptr, *most_z0h = nullptr;  // MOST per-face roughness lengths
   // learned term of the two-level preconditioner (learn.cuh)
   int lp_S = 32, lp_count = 0, lp_stride = 10, lp_val_lo = 0;
   bool lp_recording = false, lp_ready = false;
@@ -547,7 +548,7 @@ struct Solver {
       // The reference also refreshes a domain-mean Obukhov length at stage 1; it only seeds faces
       // whose own length is still zero, i.e. the first call, so the configured value is used.
       k_most<<<nblk(nb), TPB, 0, st>>>(d, F.U, F.T, F.tau, most_qw, most_L, P.abl_L_obukhov, P.abl_T_surface,
-                                       std::max(P.abl_z0_m, SMALL), std::max(P.abl_z0_h, SMALL));
+                                       most_z0m, most_z0h);
       launches++;
       return;
     }
@@ -638,7 +639,18 @@ struct Solver {
     launch_fill(Tb, std::max(nb, 1), P.T_ref);
     most_L = mem.alloc<double>(std::max(nb, 1));
     most_qw = mem.alloc<double>(std::max(nb, 1));
-    if (!most_L || !most_qw) return DPM_ERR_CUDA;
+    {  // per-face roughness: the patch's value when positive, else the global one
+      std::vector<double> z0m(std::max(nb, 1), std::max(P.abl_z0_m, SMALL)), z0h(std::max(nb, 1), std::max(P.abl_z0_h, SMALL));
+      for (int b = 0; b < nb; ++b) {
+        const int q = m.patch[nfi_() + b];
+        if (q < 0) continue;
+        if (pc[q].abl_z0_m > 0.0) z0m[b] = std::max(pc[q].abl_z0_m, SMALL);
+        if (pc[q].abl_z0_h > 0.0) z0h[b] = std::max(pc[q].abl_z0_h, SMALL);
+      }
+      most_z0m = mem.upload(z0m);
+      most_z0h = mem.upload(z0h);
+    }
+    if (!most_L || !most_qw || !most_z0m || !most_z0h) return DPM_ERR_CUDA;
     launch_fill(most_L, std::max(nb, 1), 0.0);
     launch_fill(most_qw, std::max(nb, 1), 0.0);
     launch_fill(gT, 3 * (int64_t)nc, 0.0);

@@ -95,6 +95,8 @@ typedef struct dpm_patch_cfg {
   double T_val;               /* fixed temperature                                           */
   int scalar_mode[4];         /* per passive scalar: 0 zero gradient, 1 Dirichlet (value),    */
   double scalar_value[4];     /* 2 Neumann (value = flux per area, constant in time)          */
+  double abl_z0_m, abl_z0_h;  /* MOST roughness lengths of this patch; <= 0: the global
+                               * abl_z0_m / abl_z0_h (src/abl/mod_abl_wall.f90:248-257)       */
 } dpm_patch_cfg_t;
 
 /* Solver parameters (src/solver/mod_fv_solver.f90:solver_params_t), numerics pinned as the

@@ -1089,8 +1089,11 @@ struct Solver {
       double Lg = L_bnd[fb];
       if (std::fabs(Lg) < SMALL) Lg = L_cfg;
       double us, ts, Ln;
-      most_iterate(upm, T[o], P.abl_T_surface, yw, std::max(P.abl_z0_m, SMALL), std::max(P.abl_z0_h, SMALL), Lg, us,
-                   ts, Ln);
+      // src/abl/mod_abl_wall.f90:45-50, :248-257: the patch's roughness when set, else the global
+      const dpm_patch_cfg_t& q = pc[m.patch[fg]];
+      const double z0m = std::max(q.abl_z0_m > 0.0 ? q.abl_z0_m : P.abl_z0_m, SMALL);
+      const double z0h = std::max(q.abl_z0_h > 0.0 ? q.abl_z0_h : P.abl_z0_h, SMALL);
+      most_iterate(upm, T[o], P.abl_T_surface, yw, z0m, z0h, Lg, us, ts, Ln);
       L_bnd[fb] = Ln;
       L_sum += Ln;
       nwf++;
