@@ -317,6 +317,16 @@ __global__ void k_perm_scatter(int n, const int* __restrict__ perm, const double
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) dst[perm[i]] = src[i];
 }
+__global__ void k_perm_gather(int n, const int* __restrict__ perm, const double* __restrict__ src,
+                              double* __restrict__ dst) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = src[perm[i]];
+}
+__global__ void k_perm_scatter_f(int n, const int* __restrict__ perm, const float* __restrict__ src,
+                                 float* __restrict__ dst) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dst[perm[i]] = src[i];
+}
 __global__ void k_fill_f(int n, float* p, float v) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) p[i] = v;

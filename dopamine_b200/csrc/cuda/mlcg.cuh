@@ -68,6 +68,16 @@ struct MlArgs {
   double* dout;           // [0] true residual, [1] last ||r||, [2] ||b'||
   double rtol, atol;
   int stall_window;
+  // learned term: gamma * omega .* D^-1 r added to the last fine-level smoothing step
+  // (omega [n] in this numbering; gamma = 0: off)
+  const float* omega;
+  float gamma;
+  // training-sample recording, as the two-level kernel does it: every rec_stride-th iteration,
+  // slot rec_base + its / rec_stride (< rec_max) receives r, z, u = D^-1 r and x at position
+  // pinv[i] (the learned term's part numbering).  rec_stride = 0: off.
+  int rec_stride, rec_base, rec_max;
+  const int* pinv;
+  double *rec_r, *rec_z, *rec_u, *rec_x;
 };
 
 // Row products over padded ELL rows of runtime width, in chunks of ML_CHUNK entries: all column
@@ -119,7 +129,7 @@ __device__ __forceinline__ float ml_part(const MlDevLevel& L, int i, const float
 // that their loads are in flight together.
 template <bool PRO, int R>
 __device__ __forceinline__ void ml_sweep_rows(const MlDevLevel& L, float c1, float c2, const float* xi, float* xo,
-                                              const float* xc, float oc, int g0, int T) {
+                                              const float* xc, float oc, int g0, int T, const float* om, float gam) {
   for (int i0 = g0; i0 < L.n; i0 += R * T) {
     int ii[R];
     float acc[R], b[R], q[R], x[R], d[R];
@@ -146,7 +156,7 @@ __device__ __forceinline__ void ml_sweep_rows(const MlDevLevel& L, float c1, flo
     for (int h = 0; h < R; ++h)
       if (i0 + h * T < L.n) {
         L.d[ii[h]] = d[h];
-        xo[ii[h]] = x[h] + d[h];
+        xo[ii[h]] = x[h] + d[h] + (om ? gam * __ldg(&om[ii[h]]) * q[h] * b[h] : 0.0f);
       }
   }
 }
@@ -158,13 +168,14 @@ __device__ __forceinline__ void ml_sweep_rows(const MlDevLevel& L, float c1, flo
 // (rows_per_pass) so that their loads are in flight together.
 template <bool PRO>
 __device__ __forceinline__ void ml_sweep(const MlDevLevel& L, float c1, float c2, const float* xi, float* xo,
-                                         const float* xc, float oc, int g0, int T) {
+                                         const float* xc, float oc, int g0, int T, const float* om = nullptr,
+                                         float gam = 0.0f) {
   if (L.lgG == 0) {
     switch (L.rows_per_pass) {
-      case 1: ml_sweep_rows<PRO, 1>(L, c1, c2, xi, xo, xc, oc, g0, T); return;
-      case 2: ml_sweep_rows<PRO, 2>(L, c1, c2, xi, xo, xc, oc, g0, T); return;
-      case 3: ml_sweep_rows<PRO, 3>(L, c1, c2, xi, xo, xc, oc, g0, T); return;
-      default: ml_sweep_rows<PRO, 4>(L, c1, c2, xi, xo, xc, oc, g0, T); return;
+      case 1: ml_sweep_rows<PRO, 1>(L, c1, c2, xi, xo, xc, oc, g0, T, om, gam); return;
+      case 2: ml_sweep_rows<PRO, 2>(L, c1, c2, xi, xo, xc, oc, g0, T, om, gam); return;
+      case 3: ml_sweep_rows<PRO, 3>(L, c1, c2, xi, xo, xc, oc, g0, T, om, gam); return;
+      default: ml_sweep_rows<PRO, 4>(L, c1, c2, xi, xo, xc, oc, g0, T, om, gam); return;
     }
   }
   const int lane = threadIdx.x & 31;
@@ -187,7 +198,7 @@ __device__ __forceinline__ void ml_sweep(const MlDevLevel& L, float c1, float c2
         d = c1 * __ldcg(&L.d[i]) + c2 * q * r;
       }
       L.d[i] = d;
-      xo[i] = x + d;
+      xo[i] = x + d + (om ? gam * __ldg(&om[i]) * q * __ldcg(&L.b[i]) : 0.0f);
     }
   }
 }
@@ -355,11 +366,14 @@ __global__ void __launch_bounds__(ML_TPB, 2) k_mlcg(MlArgs a) {
     for (int l = nlev - 1; l >= 0; --l) {
       const MlDevLevel& L = s_lv[l];
       int cur = (cur_mask >> l) & 1u;
-      ml_sweep<true>(L, 0.0f, 0.0f, cur ? L.x1 : L.x0, cur ? L.x0 : L.x1, xcoarse, a.oc, g0, T);
+      const float* om = (l == 0 && a.gamma != 0.0f) ? a.omega : nullptr;  // learned term: last fine step
+      ml_sweep<true>(L, 0.0f, 0.0f, cur ? L.x1 : L.x0, cur ? L.x0 : L.x1, xcoarse, a.oc, g0, T,
+                     deg == 1 ? om : nullptr, a.gamma);
       cur ^= 1;
       if (!grid_barrier(a.bar, gen, a.status)) return;
       for (int j = 1; j < deg; ++j) {
-        ml_sweep<false>(L, L.c1[j], L.c2[j], cur ? L.x1 : L.x0, cur ? L.x0 : L.x1, nullptr, 0.0f, g0, T);
+        ml_sweep<false>(L, L.c1[j], L.c2[j], cur ? L.x1 : L.x0, cur ? L.x0 : L.x1, nullptr, 0.0f, g0, T,
+                        j == deg - 1 ? om : nullptr, a.gamma);
         cur ^= 1;
         if (!grid_barrier(a.bar, gen, a.status)) return;
       }
@@ -370,6 +384,17 @@ __global__ void __launch_bounds__(ML_TPB, 2) k_mlcg(MlArgs a) {
     double v[FCG_NV], t[FCG_NV];
 #pragma unroll
     for (int k = 0; k < FCG_NV; ++k) v[k] = 0.0;
+    if (a.rec_stride > 0 && its % a.rec_stride == 0 && a.rec_base + its / a.rec_stride < a.rec_max && nlev > 0) {
+      const size_t off = (size_t)(a.rec_base + its / a.rec_stride) * n;
+      const MlDevLevel& L0 = s_lv[0];
+      for (int i = g0; i < n; i += T) {
+        const size_t o = off + __ldg(&a.pinv[i]);
+        a.rec_r[o] = __ldcg(&a.r[i]);
+        a.rec_z[o] = (double)__ldcg(&z[i]);
+        a.rec_u[o] = (double)(__ldg(&L0.dinv[i]) * __ldcg(&L0.b[i]));
+        a.rec_x[o] = __ldcg(&a.x[i]);
+      }
+    }
     for (int i0 = g0; i0 < n; i0 += 2 * T) {  // two rows per pass: their loads in flight together
       const int i1 = i0 + T;
       const bool h1 = i1 < n;

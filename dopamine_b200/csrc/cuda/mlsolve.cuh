@@ -125,11 +125,18 @@ struct MlSolver {
     return 0;
   }
 
-  // One solve on stream st; reason / its / resid as the Krylov kernels report them.
+  // One solve on stream st; reason / its / resid as the Krylov kernels report them.  extra: the
+  // learned-term and recording fields (omega, gamma, rec_*, pinv), or null.
   int launch(const double* b, double* x, double rtol, double atol, int maxit, int guess_zero, cudaStream_t st,
-             int* reason, int* its, double* resid) {
+             int* reason, int* its, double* resid, const MlArgs* extra = nullptr) {
     if (!ready()) return DPM_ERR_ARG;
     MlArgs a = base;
+    if (extra) {
+      a.omega = extra->omega; a.gamma = extra->gamma;
+      a.rec_stride = extra->rec_stride; a.rec_base = extra->rec_base; a.rec_max = extra->rec_max;
+      a.pinv = extra->pinv;
+      a.rec_r = extra->rec_r; a.rec_z = extra->rec_z; a.rec_u = extra->rec_u; a.rec_x = extra->rec_x;
+    }
     a.b = b; a.x = x; a.rtol = rtol; a.atol = atol; a.maxit = maxit; a.guess_zero = guess_zero;
     if (cudaMemsetAsync(a.bar, 0, 2 * sizeof(unsigned), st) != cudaSuccess) return DPM_ERR_CUDA;
     if (cudaMemsetAsync(a.status, 0, 4 * sizeof(int), st) != cudaSuccess) return DPM_ERR_CUDA;

@@ -212,6 +212,10 @@ struct Solver {
   // multilevel flexible CG (p_solver == DPM_PSOLVER_MULTILEVEL_FCG)
   bool use_ml = false;
   MlSolver ml;
+  bool ml_learn_ready = false;   // the learned term's partition and buffers exist for the multilevel form
+  int* ml_pinv = nullptr;        // [n] position of each cell in the learned term's numbering
+  float* ml_omega = nullptr;     // [n] omega in the mesh numbering
+  int dev_sms_ = 0;
   double *gg_prevU = nullptr, *gg_prevS = nullptr;  // Green-Gauss previous-sweep gradients
   // state
   double time = 0.0;
@@ -780,6 +784,7 @@ struct Solver {
   // Multilevel FCG set-up (csrc/cuda/mlsolve.cuh): hierarchy on the host, FP32 levels on the
   // device, the FP64 operator shared with the plain solve.
   int setup_ml(int dev_sms) {
+    dev_sms_ = dev_sms;
     const bool nullsp = S.dir_rows.empty();
     int rc = ml.setup(nc, S.WA, S.A_col.data(), S.A_val.data(), d.Acol, d.Aval, nullsp, P.p_ml_passes, P.p_ml_degree,
                       P.p_ml_overcorrect, dev_sms, cg_bar, cg_status, cg_dout);
@@ -789,8 +794,66 @@ struct Solver {
   }
   int ml_launch(const double* rhs, double* x, double rtol, double atol, int maxit, int guess_zero, int* its,
                 double* resid, int* reason) {
+    MlArgs e{};
+    if (ml_learn_ready && lp_ready) {
+      e.omega = ml_omega;
+      e.gamma = lp_gamma;
+    }
+    const bool rec = ml_learn_ready && lp_recording && lp_count < lp_S;
+    if (rec) {
+      e.gamma = 0.0f;
+      e.rec_stride = lp_stride; e.rec_base = lp_count; e.rec_max = lp_S; e.pinv = ml_pinv;
+      e.rec_r = lp_r; e.rec_z = lp_z; e.rec_u = lp_u; e.rec_x = lp_x;
+    }
     launches++;
-    return ml.launch(rhs, x, rtol, atol, maxit, guess_zero, st, reason, its, resid);
+    int rc = ml.launch(rhs, x, rtol, atol, maxit, guess_zero, st, reason, its, resid, &e);
+    if (rc) return rc;
+    if (rec) {  // errors of the recorded iterates, in the learned term's numbering: e = x* - x_k
+      const int used = std::min(lp_S - lp_count, *its / lp_stride + 1);
+      if (used > 0) {
+        k_perm_gather<<<nblk(nc), TPB, 0, st>>>(nc, fa.perm, x, fa.xs);
+        dim3 g(nblk(nc), used);
+        k_lp_err<<<g, TPB, 0, st>>>(nc, fa.xs, lp_x + (size_t)lp_count * nc);
+        launches += 2;
+        for (int k = 0; k < used; ++k) lp_solve_of.push_back(lp_solves);
+        lp_count += used;
+      }
+      lp_solves++;
+    }
+    return 0;
+  }
+  // The learned term on the multilevel form: an RCB partition into parts of <= 4096 cells gives
+  // the one-ring network its local rows and features (no coarse data), built on first use.
+  int ml_learn_setup() {
+    if (ml_learn_ready) return 0;
+    TwoLevel T;
+    const int P = std::max(dev_sms_, (nc + 4095) / 4096);
+    if (build_two_level(nc, S.WA, S.A_col.data(), S.A_val.data(), m.centroid.data(), P, S.dir_rows.empty(), T, false))
+      return DPM_ERR_UNSUPPORTED;
+    fa = FcgArgs{};
+    fa.n = nc; fa.P = T.P; fa.C = T.C; fa.WL = T.WL;
+    fa.perm = mem.upload(T.perm);
+    fa.col = mem.upload(T.col);
+    fa.val = mem.upload(T.val);
+    fa.dinv = mem.upload(T.dinv);
+    fa.lpk = mem.upload(T.lpk);
+    fa.xs = mem.alloc<double>(nc);
+    fcg_WA = T.WA;
+    std::vector<int> pinv(nc);
+    for (int i = 0; i < nc; ++i) pinv[T.perm[i]] = i;
+    ml_pinv = mem.upload(pinv);
+    ml_omega = mem.alloc<float>(nc);
+    if (!fa.perm || !fa.col || !fa.val || !fa.dinv || !fa.lpk || !fa.xs || !ml_pinv || !ml_omega) return DPM_ERR_CUDA;
+    launch_fill_f(ml_omega, nc, 0.0f);
+    int rc = setup_learned(T);
+    if (rc) return rc;
+    ml_learn_ready = true;
+    return 0;
+  }
+  void ml_sync_omega() {  // the trained omega into the mesh numbering
+    if (!ml_learn_ready) return;
+    k_perm_scatter_f<<<nblk(nc), TPB, 0, st>>>(nc, fa.perm, lp_omega, ml_omega);
+    launches++;
   }
 
   // Static per-cell features of the learned term, in the renumbered order:
@@ -1029,7 +1092,7 @@ struct Solver {
       launches++;
       int its = 0, reason = 0;
       double res = 0.0;
-      int rc = fcg(scratch_c, scratch_c2, P.p_tol, 1e-300, 2000, 1, &its, &res, &reason);
+      int rc = pcg(scratch_c, scratch_c2, P.p_tol, 1e-300, 2000, 1, &its, &res, &reason);
       if (rc) return rc;
       *its_total += its + (reason < 0 ? 100000 : 0);
     }
@@ -1038,8 +1101,10 @@ struct Solver {
     return 0;
   }
   int learn_collect(int n_steps, int* n_samples) {
-    if (!use_fcg) return DPM_ERR_UNSUPPORTED;
-    int rc = learn_alloc();
+    if (!use_fcg && !use_ml) return DPM_ERR_UNSUPPORTED;
+    int rc = use_ml ? ml_learn_setup() : 0;
+    if (rc) return rc;
+    rc = learn_alloc();
     if (rc) return rc;
     lp_count = 0;
     lp_solves = 0;
@@ -1051,7 +1116,7 @@ struct Solver {
     return rc;
   }
   int learn_train(int epochs, double lr, dpm_learn_report_t* rep) {
-    if (!use_fcg || lp_count == 0) return DPM_ERR_ARG;
+    if ((!use_fcg && !use_ml) || lp_count == 0) return DPM_ERR_ARG;
     auto t0 = std::chrono::steady_clock::now();
     const int S = lp_train_slots();
     std::vector<double> base;
@@ -1069,6 +1134,7 @@ struct Solver {
     }
     rc = lp_loss_grad(S, base, &L, false);  // final loss, omega of the trained network
     if (rc) return rc;
+    if (use_ml) ml_sync_omega();
     // gate: the scale of the learned term that does best on the held-out solves (ties keep 0)
     const float cand[3] = {0.0f, 0.5f, 1.0f};
     int best_its = 0, its0 = 0;
@@ -1512,7 +1578,7 @@ int dpm_learn_train(dpm_solver_t* h, int epochs, double lr, dpm_learn_report_t* 
 int dpm_learn_set_gamma(dpm_solver_t* h, double gamma) {
   if (!h || !(gamma >= 0.0)) return DPM_ERR_ARG;
   Solver& s = *h->s;
-  if (!s.use_fcg) return DPM_ERR_UNSUPPORTED;
+  if (!s.use_fcg && !(s.use_ml && s.ml_learn_ready)) return DPM_ERR_UNSUPPORTED;
   s.lp_gamma = (float)gamma;
   s.lp_ready = true;
   return DPM_OK;
@@ -1535,7 +1601,7 @@ int dpm_multilevel_hierarchy(int n, int width, const int* col, const double* val
 int dpm_learn_sizes(dpm_solver_t* h, int* sizes) {
   if (!h || !sizes) return DPM_ERR_ARG;
   Solver& s = *h->s;
-  if (!s.use_fcg) return DPM_ERR_UNSUPPORTED;
+  if (!s.use_fcg && !(s.use_ml && s.ml_learn_ready)) return DPM_ERR_UNSUPPORTED;
   sizes[0] = s.nc; sizes[1] = s.fa.C; sizes[2] = s.fa.WL; sizes[3] = s.fcg_WA;
   sizes[4] = s.lp_train_slots(); sizes[5] = dpm::gpu::LP_F; sizes[6] = dpm::gpu::LP_NP;
   return DPM_OK;
@@ -1545,7 +1611,7 @@ int dpm_learn_export(dpm_solver_t* h, float* feat, unsigned* lpk, int* col, doub
                      double* U, double* E, float* params) {
   if (!h) return DPM_ERR_ARG;
   Solver& s = *h->s;
-  if (!s.use_fcg) return DPM_ERR_UNSUPPORTED;
+  if (!s.use_fcg && !(s.use_ml && s.ml_learn_ready)) return DPM_ERR_UNSUPPORTED;
   CK(cudaSetDevice(s.device));
   const size_t n = s.nc, S = s.lp_train_slots();
   auto cp = [&](void* dst, const void* src, size_t bytes) -> int {
@@ -1568,7 +1634,7 @@ int dpm_learn_export(dpm_solver_t* h, float* feat, unsigned* lpk, int* col, doub
 int dpm_learn_loss_grad(dpm_solver_t* h, const float* params, double* loss, float* grad) {
   if (!h || !loss) return DPM_ERR_ARG;
   Solver& s = *h->s;
-  if (!s.use_fcg || s.lp_count == 0) return DPM_ERR_ARG;
+  if ((!s.use_fcg && !s.use_ml) || s.lp_count == 0) return DPM_ERR_ARG;
   CK(cudaSetDevice(s.device));
   const int S = s.lp_train_slots();
   std::vector<float> keep(dpm::gpu::LP_NP);

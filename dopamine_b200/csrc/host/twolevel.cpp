@@ -67,7 +67,7 @@ bool cholesky(std::vector<double>& a, int n) {
 }  // namespace
 
 int build_two_level(int n, int WA, const int* A_col, const double* A_val, const double* xyz, int P, bool nullsp,
-                    TwoLevel& T) {
+                    TwoLevel& T, bool coarse) {
   if (n < 1 || WA < 1 || P < 1) return -1;
   int C = (n + P - 1) / P;
   P = (n + C - 1) / C;  // every part non-empty
@@ -95,7 +95,7 @@ int build_two_level(int n, int WA, const int* A_col, const double* A_val, const 
   T.val.assign((size_t)WA * n, 0.0);
   T.dinv.assign(n, 1.0);
   std::vector<std::vector<std::pair<int, double>>> loc(n);
-  std::vector<double> E((size_t)P * P, 0.0);
+  std::vector<double> E(coarse ? (size_t)P * P : 0, 0.0);
   int WL = 0;
   for (int i = 0; i < n; ++i) {
     const int o = T.perm[i];
@@ -109,7 +109,7 @@ int build_two_level(int n, int WA, const int* A_col, const double* A_val, const 
       int j = iperm[c];
       row.push_back({j, v});
       if (j == i) dg += v;
-      E[(size_t)b * P + j / C] += v;
+      if (coarse) E[(size_t)b * P + j / C] += v;
     }
     std::sort(row.begin(), row.end());
     for (size_t s = 0; s < row.size(); ++s) {
@@ -135,6 +135,21 @@ int build_two_level(int n, int WA, const int* A_col, const double* A_val, const 
       }
       T.lpk[(size_t)s * n + i] = colv | (hi << 16);
     }
+  }
+  if (!coarse) {  // intra-part row sums only
+    T.srow.assign(n, 0.0f);
+    T.xoff.assign(n + 1, 0);
+    for (int i = 0; i < n; ++i) {
+      double sr = 0.0;
+      for (int w = 0; w < WA; ++w) {
+        const double v = T.val[(size_t)w * n + i];
+        if (v != 0.0 && T.col[(size_t)w * n + i] / C == i / C) sr += v;
+      }
+      T.srow[i] = (float)sr;
+    }
+    T.xval.assign(1, 0.0f);
+    T.xslot.assign(1, 0);
+    return 0;
   }
   // coarse operator: with the constant null space, E is singular along the constant vector;
   // adding (mean diag / P) 1 1^T makes it SPD and leaves E^-1 unchanged on the complement.

@@ -41,7 +41,9 @@ struct TwoLevel {
 
 // A in padded ELL [WA][n] (padding = (own row, 0)), cell centres xyz[3*n]; nullsp = the
 // operator has the constant null space (no Dirichlet rows).  Returns 0 or a negative code.
+// coarse = false: the partition, permuted operator, local rows and intra-part row sums only (the
+// learned term's structures on meshes whose parts do not fit the two-level kernel).
 int build_two_level(int n, int WA, const int* A_col, const double* A_val, const double* xyz, int P, bool nullsp,
-                    TwoLevel& T);
+                    TwoLevel& T, bool coarse = true);
 
 }  // namespace dpm
