@@ -178,7 +178,7 @@ def run_gpu(args, rank, world):
     s.initialise()
     nc = s.nc
     learn = None
-    if args.psolver == "fcg" and not args.no_learned:
+    if args.psolver in ("fcg", "ml") and not args.no_learned:
         # learned preconditioner term: samples from 3 steps' solves, 80 Adam steps, gamma set on the
         # held-out solve (set-up work, outside the timed region; reported in the config)
         n_samples = s.learn_collect(3)
@@ -278,7 +278,7 @@ def main():
     ap.add_argument("--config", default="channel", choices=["channel", "tgv", "rb", "mixed", "urban"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip timing the plain FP64 Jacobi-PCG form")
-    ap.add_argument("--no-learned", action="store_true", help="two-level FCG without the learned term")
+    ap.add_argument("--no-learned", action="store_true", help="flexible CG without the learned term")
     ap.add_argument("--mixed", action="store_true",
                     help="precision form: FP32-operator inner iterations inside FP64 defect correction")
     ap.add_argument("--psolver", default="fcg", choices=["pcg", "fcg", "ml"],
