@@ -161,6 +161,20 @@ def pcg_traffic_per_launch(psolver="pcg"):
     return None
 
 
+def max_over_ranks(values, device):
+    """Element-wise maximum of per-rank timings over the process group (replicas: the job is as
+    slow as its slowest rank)."""
+    import torch
+    t = torch.tensor(values, device=device, dtype=torch.float64)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return [float(v) for v in t]
+
+
+def whole_job_rate(world, cells, steps, seconds):
+    """cell-steps/s of N replicas that each advance `cells` cells `steps` times in `seconds`."""
+    return world * cells * steps / seconds
+
+
 def run_gpu(args, rank, world):
     import torch
     from dopamine_b200.solver import Solver, lib
@@ -208,8 +222,13 @@ def run_gpu(args, rank, world):
     # ---- end to end through the C ABI with host buffers
     L = lib()
     host = s.sync_host()
-    U = np.ascontiguousarray(host["U"])
-    p = np.ascontiguousarray(host["p"])
+    # pinned host buffers (page-locked through torch), filled with the current state
+    U_pin = torch.empty(host["U"].shape, dtype=torch.float64, pin_memory=True)
+    p_pin = torch.empty(host["p"].shape, dtype=torch.float64, pin_memory=True)
+    U = U_pin.numpy()
+    p = p_pin.numpy()
+    U[...] = host["U"]
+    p[...] = host["p"]
     dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -222,9 +241,7 @@ def run_gpu(args, rank, world):
     t_e2e = time.perf_counter() - t0
     clocks = sampler.stop() if sampler else None
     if world > 1:
-        t = torch.tensor([t_dev, t_e2e], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        t_dev, t_e2e = float(t[0]), float(t[1])
+        t_dev, t_e2e = max_over_ranks([t_dev, t_e2e], "cuda")
     return dict(nc=nc, t_dev=t_dev, t_e2e=t_e2e, step_ms=step_ms, pois_ms=pois_ms, its=its, solves=solves,
                 launches=launches, clocks=clocks, solver=s, learn=learn, fallbacks=s.stats()["p_fallbacks"])
 
@@ -324,8 +341,8 @@ def main():
             torch.distributed.destroy_process_group()
         return 0
     nc, K = r["nc"], args.steps
-    value = world * nc * K / r["t_dev"]
-    e2e = world * nc * K / r["t_e2e"]
+    value = whole_job_rate(world, nc, K, r["t_dev"])
+    e2e = whole_job_rate(world, nc, K, r["t_e2e"])
     peak, peak_kind = measured_peaks()
     bytes_it = pcg_bytes_per_iteration(s, args.psolver)
     pois_s = sum(r["pois_ms"]) / 1e3
