@@ -31,6 +31,7 @@ constexpr int FCG_TPB = 1024;
 constexpr int FCG_SLOT = 16;  // doubles per block in the reduce/gather buffer
 constexpr int FCG_NV = 8;     // reduced sums
 constexpr int FCG_NG = 3;     // gathered per-part values
+constexpr int FCG_MAX_GRID = 160;  // largest grid of the two-level kernel's reduce-gather (5 blocks per lane)
 
 struct FcgArgs {
   int n, P, C, WL, maxit, nullsp, guess_zero, degree;
@@ -100,9 +101,12 @@ __device__ __forceinline__ bool grid_barrier(unsigned* bar, unsigned& gen, int* 
 // All-reduce of the first NV of v (deterministic, as grid_allreduce) plus an all-gather of the
 // block totals of the last NG into gat[k*P + block] (shared memory: every block gets every
 // block's values).  v holds per-thread partials of all NV + NG values.  All reductions of the
-// FCG kernel go through here so that every generation uses the same slot layout of the
-// double-buffered partials.
-template <int NV, int NG>
+// FCG kernels go through here so that every generation uses the same slot layout of the
+// double-buffered partials.  Warp k reduces value k, both over the block's warps before the
+// barrier and over the blocks after it, with all of a lane's loads issued together; the order
+// of every sum is fixed (lane-ordered partials, then a shuffle tree), so results do not depend
+// on timing.  Supports up to 32 * RB blocks (RB: blocks per lane in the post-barrier read).
+template <int NV, int NG, int RB = FCG_MAX_GRID / 32>
 __device__ __forceinline__ bool grid_reduce_gather(double (&v)[NV + NG], double* partials, unsigned* bar,
                                                    unsigned& gen, int* status, double (&res)[NV], double* gat) {
   constexpr int NT = NV + NG;
@@ -120,62 +124,48 @@ __device__ __forceinline__ bool grid_reduce_gather(double (&v)[NV + NG], double*
 #pragma unroll
     for (int k = 0; k < NT; ++k) sh[w][k] = v[k];
   __syncthreads();
-  if (w == 0) {
-    double t[NT];
-#pragma unroll
-    for (int k = 0; k < NT; ++k) {
-      t[k] = lane < nw ? sh[lane][k] : 0.0;
-      for (int o = 16; o > 0; o >>= 1) t[k] += __shfl_down_sync(0xffffffffu, t[k], o);
-    }
+  if (w < NT) {  // warp w: value w over the block's warps
+    double t = lane < nw ? sh[lane][w] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+    if (lane == 0) buf[blockIdx.x * FCG_SLOT + w] = t;
+  }
+  __syncthreads();  // the partial stores precede thread 0's release below
+  if (threadIdx.x == 0) {
     int ok = 1;
-    if (lane == 0) {
-#pragma unroll
-      for (int k = 0; k < NT; ++k) buf[blockIdx.x * FCG_SLOT + k] = t[k];
-      const unsigned target = (gen + 1u) * gridDim.x;
-      __threadfence();
-      atomicAdd(&bar[0], 1u);
-      unsigned spins = 0;
-      for (;;) {
-        unsigned cur;
-        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(cur) : "l"(&bar[0]) : "memory");
-        if ((int)(cur - target) >= 0) break;
-        if (++spins > DPM_BARRIER_SPIN_LIMIT) { ok = 0; atomicExch(&status[2], 1); break; }
-        if (spins > 32) __nanosleep(20);
-      }
-      __threadfence();
+    const unsigned target = (gen + 1u) * gridDim.x;
+    __threadfence();
+    atomicAdd(&bar[0], 1u);
+    unsigned spins = 0;
+    for (;;) {
+      unsigned cur;
+      asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(cur) : "l"(&bar[0]) : "memory");
+      if ((int)(cur - target) >= 0) break;
+      if (++spins > DPM_BARRIER_SPIN_LIMIT) { ok = 0; atomicExch(&status[2], 1); break; }
+      if (spins > 32) __nanosleep(20);
     }
-    ok = __shfl_sync(0xffffffffu, ok, 0);
-    if (lane == 0) s_ok = ok;
+    __threadfence();
+    s_ok = ok && P <= 32 * RB;
+    if (P > 32 * RB) atomicExch(&status[2], 2);
   }
   __syncthreads();
   const bool ok = s_ok != 0;
   if (ok) {
-    if (w == 0) {
-      double u[NV > 0 ? NV : 1];
+    if (w < NV) {  // warp w: value w over the blocks, lane l sums blocks l, l + 32, ... in order
+      double pv[RB];
 #pragma unroll
-      for (int k = 0; k < NV; ++k) u[k] = 0.0;
-      // all of a lane's partials are loaded before they are summed (in block order, as a plain
-      // loop would), so the loads are in flight together
-      for (int b0 = lane; b0 < P; b0 += 32 * 4) {
-        double pv[4][NV > 0 ? NV : 1];
+      for (int h = 0; h < RB; ++h) pv[h] = lane + 32 * h < P ? __ldcg(&buf[(lane + 32 * h) * FCG_SLOT + w]) : 0.0;
+      double u = 0.0;
 #pragma unroll
-        for (int h = 0; h < 4; ++h)
-#pragma unroll
-          for (int k = 0; k < NV; ++k) pv[h][k] = b0 + 32 * h < P ? __ldcg(&buf[(b0 + 32 * h) * FCG_SLOT + k]) : 0.0;
-#pragma unroll
-        for (int h = 0; h < 4; ++h)
-#pragma unroll
-          for (int k = 0; k < NV; ++k) u[k] += pv[h][k];
-      }
-#pragma unroll
-      for (int k = 0; k < NV; ++k) {
-        for (int o = 16; o > 0; o >>= 1) u[k] += __shfl_down_sync(0xffffffffu, u[k], o);
-        if (lane == 0) shr[k] = u[k];
-      }
+      for (int h = 0; h < RB; ++h) u += pv[h];
+      for (int o = 16; o > 0; o >>= 1) u += __shfl_down_sync(0xffffffffu, u, o);
+      if (lane == 0) shr[w] = u;
     }
-    for (int idx = threadIdx.x; idx < NG * P; idx += blockDim.x) {
-      const int k = idx / P, b = idx - k * P;
-      gat[idx] = __ldcg(&buf[b * FCG_SLOT + NV + k]);
+    if (NG > 0) {  // the per-block values, read by the threads after the first NV warps
+      const int t0 = NV * 32 < (int)blockDim.x ? NV * 32 : 0;
+      for (int idx = (int)threadIdx.x - t0; idx >= 0 && idx < NG * P; idx += blockDim.x - t0) {
+        const int k = idx / P, b = idx - k * P;
+        gat[idx] = __ldcg(&buf[b * FCG_SLOT + NV + k]);
+      }
     }
   }
   __syncthreads();

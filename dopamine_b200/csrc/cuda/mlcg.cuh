@@ -26,6 +26,8 @@ namespace dpm {
 namespace gpu {
 
 constexpr int ML_TPB = 512;
+constexpr int ML_RB = 10;                  // blocks per lane in the reduce-gather: grids up to 320 blocks
+constexpr int ML_MAX_GRID = 32 * ML_RB;
 constexpr int ML_LEVELS = 12;
 constexpr int ML_DEG = 8;
 
@@ -263,7 +265,7 @@ __global__ void __launch_bounds__(ML_TPB, 2) k_mlcg(MlArgs a) {
       if (a.guess_zero) a.x[i] = 0.0;
       v[0] += a.b[i];
     }
-    if (!grid_reduce_gather<1, 0>(v, a.partials, a.bar, gen, a.status, t, s_gat)) return;  // publishes x
+    if (!grid_reduce_gather<1, 0, ML_RB>(v, a.partials, a.bar, gen, a.status, t, s_gat)) return;  // publishes x
     mb = a.nullsp ? t[0] / (double)n : 0.0;
   }
   double dp, sn;
@@ -279,7 +281,7 @@ __global__ void __launch_bounds__(ML_TPB, 2) k_mlcg(MlArgs a) {
       v[1] += bp * bp;
       start_level0(i, ri);
     }
-    if (!grid_reduce_gather<2, 0>(v, a.partials, a.bar, gen, a.status, t, s_gat)) return;
+    if (!grid_reduce_gather<2, 0, ML_RB>(v, a.partials, a.bar, gen, a.status, t, s_gat)) return;
     dp = sqrt(t[0]);
     sn = sqrt(t[1]);
   }
@@ -418,7 +420,7 @@ __global__ void __launch_bounds__(ML_TPB, 2) k_mlcg(MlArgs a) {
         v[7] += wi;
       }
     }
-    if (!grid_reduce_gather<FCG_NV, 0>(v, a.partials, a.bar, gen, a.status, t, s_gat)) return;
+    if (!grid_reduce_gather<FCG_NV, 0, ML_RB>(v, a.partials, a.bar, gen, a.status, t, s_gat)) return;
     dp = sqrt(t[4]);
     reason = classify(dp, ttol, a.atol, rnorm0);
     if (reason) break;
@@ -453,7 +455,7 @@ __global__ void __launch_bounds__(ML_TPB, 2) k_mlcg(MlArgs a) {
     const double di = a.b[i] - ml_row64(a, i, (const double*)a.x);
     v1[0] += di * di;
   }
-  if (!grid_reduce_gather<1, 0>(v1, a.partials, a.bar, gen, a.status, t1, s_gat)) return;
+  if (!grid_reduce_gather<1, 0, ML_RB>(v1, a.partials, a.bar, gen, a.status, t1, s_gat)) return;
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     a.dout[0] = sqrt(t1[0]);
     a.dout[1] = dp;

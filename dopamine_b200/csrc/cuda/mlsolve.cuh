@@ -65,7 +65,7 @@ struct MlSolver {
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mlcg<0>, ML_TPB, 0) != cudaSuccess || per_sm < 1)
       return DPM_ERR_UNSUPPORTED;
-    const int g = dev_sms * std::min(per_sm, 2);
+    const int g = std::min(dev_sms * std::min(per_sm, 2), ML_MAX_GRID);
     const int64_t threads = (int64_t)g * ML_TPB;
     std::vector<MlDevLevel> hl(nlev);
     for (int l = 0; l < nlev; ++l) {

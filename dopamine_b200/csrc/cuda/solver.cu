@@ -742,7 +742,7 @@ struct Solver {
     CK(cudaFuncSetAttribute(fcg_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fcg_smem));
     int per_sm = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fcg_kernel, FCG_TPB, fcg_smem));
-    if (per_sm < 1 || T.P > dev_sms * per_sm) return DPM_ERR_UNSUPPORTED;
+    if (per_sm < 1 || T.P > dev_sms * per_sm || T.P > FCG_MAX_GRID) return DPM_ERR_UNSUPPORTED;
     fa = FcgArgs{};
     fa.n = nc; fa.P = T.P; fa.C = T.C; fa.WL = T.WL;
     fa.perm = mem.upload(T.perm);
