@@ -103,7 +103,7 @@ class ClockSampler:
 
 FORMS = {"pcg": "plain FP64 Jacobi-PCG",
          "fcg": "FP64 flexible CG, deflated two-level preconditioner (148 parts, FP32 part-local Chebyshev "
-                "degree 6 in shared memory + one coarse value per part)"}
+                "degree 7 in shared memory + one coarse value per part)"}
 
 
 FORMS["ml"] = ("FP64 flexible CG preconditioned by one FP32 aggregation-multigrid V-cycle (pairwise "

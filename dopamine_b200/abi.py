@@ -119,7 +119,7 @@ def default_params(**kw):
     p.amd_wall_gradient = 1
     p.form = FORM_FP64
     p.p_solver = PSOLVER_JACOBI_PCG
-    p.p_smooth_degree = 6
+    p.p_smooth_degree = 7
     p.p_smooth_lmin = 0.05
     p.p_smooth_lmax = 2.0
     p.abl_z0_m = 0.1

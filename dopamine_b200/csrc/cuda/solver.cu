@@ -768,7 +768,7 @@ struct Solver {
     fa.partials = mem.alloc<double>((size_t)2 * FCG_SLOT * T.P);
     fa.bar = cg_bar; fa.status = cg_status; fa.dout = cg_dout;
     fa.nullsp = nullsp ? 1 : 0;
-    fa.degree = P.p_smooth_degree > 0 ? P.p_smooth_degree : 6;
+    fa.degree = P.p_smooth_degree > 0 ? P.p_smooth_degree : 7;
     const double lmin = P.p_smooth_lmin > 0.0 ? P.p_smooth_lmin : 0.05;
     const double lmax = P.p_smooth_lmax > 0.0 ? P.p_smooth_lmax : 2.0;
     if (!(lmax > lmin)) return DPM_ERR_ARG;
@@ -786,6 +786,8 @@ struct Solver {
   int setup_ml(int dev_sms) {
     dev_sms_ = dev_sms;
     const bool nullsp = S.dir_rows.empty();
+    // an aggregate holds up to 3^passes rows and the restriction gives it at most 32 lanes
+    if (P.p_ml_passes > 3) return DPM_ERR_ARG;
     int rc = ml.setup(nc, S.WA, S.A_col.data(), S.A_val.data(), d.Acol, d.Aval, nullsp, P.p_ml_passes, P.p_ml_degree,
                       P.p_ml_overcorrect, dev_sms, cg_bar, cg_status, cg_dout);
     if (rc) return rc;

@@ -142,7 +142,8 @@ typedef struct dpm_params {
   double abl_z0_m, abl_z0_h, abl_T_surface, abl_L_obukhov;
   int abl_compute_L;
   /* DPM_PSOLVER_MULTILEVEL_FCG: Chebyshev steps per smoothing (0: 3), over-correction of the
-   * coarse correction (0: 1.6), pairwise-aggregation passes per level (0: 3). */
+   * coarse correction (0: 1.6), pairwise-aggregation passes per level (0: 3; at most 3, as an
+   * aggregate of up to 3^passes rows must fit the 32 lanes of the restriction). */
   int p_ml_degree;
   double p_ml_overcorrect;
   int p_ml_passes;
