@@ -5,14 +5,15 @@ Default workload: the turbulent-channel configuration (96 x 64 x 64 hex cells, t
 KEP advection, Vreman SGS, log-law wall model, constant pressure-gradient forcing), synthetic
 inputs (seeded laminar-plus-noise initial state).  One "step" is one RK3W time step (three
 stages, three Poisson solves) of the whole mesh.  The timed form is the chosen pressure solve
-(--psolver fcg: flexible CG with the two-level preconditioner); on one GPU the plain FP64
+(flexible CG with the two-level preconditioner on this mesh, the multilevel one on meshes too
+large for it; both with the learned term trained and gated); on one GPU the plain FP64
 Jacobi-PCG form is timed beside it on the same workload and reported in the config.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                    [--config channel|tgv|rb|mixed|urban] [--psolver fcg|pcg|ml] [--no-plain]
+                    [--config channel|tgv|rb|mixed|urban] [--psolver auto|fcg|pcg|ml] [--no-plain]
 
-(the rb, mixed and urban configurations exceed the two-level kernel's part size: run them with
---psolver ml)
+(--psolver auto, the default, takes the two-level form when the mesh fits it — up to 4096 cells
+per SM — and the multilevel form otherwise, as for the rb, mixed and urban configurations)
 
 value   : cell-steps/s with the state resident in HBM (CUDA events around K steps, max over ranks)
 e2e     : the same metric through the C ABI with host buffers: every step uploads the state
@@ -182,16 +183,20 @@ def run_gpu(args, rank, world):
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(dev)
     case = make_case(args.config)
+    if args.psolver == "auto":
+        case.params["p_solver"] = 3  # DPM_PSOLVER_AUTO: two-level when the mesh fits it, else multilevel
     if args.psolver == "ml":
         case.params["p_solver"] = 2  # DPM_PSOLVER_MULTILEVEL_FCG
     if args.psolver == "fcg":
         case.params["p_solver"] = 1  # DPM_PSOLVER_TWOLEVEL_FCG
-        if args.mixed:
-            case.params["form"] = 1  # DPM_FORM_MIXED
+    if args.mixed and args.psolver in ("fcg", "auto"):
+        case.params["form"] = 1  # DPM_FORM_MIXED (the multilevel form's V-cycle is FP32 already)
     s = Solver(case, device=dev)
     s.initialise()
     nc = s.nc
     learn = None
+    if args.psolver == "auto":  # report the form the solver chose
+        args.psolver = {0: "pcg", 1: "fcg", 2: "ml"}[s.stats()["p_solver_used"]]
     if args.psolver in ("fcg", "ml") and not args.no_learned:
         # learned preconditioner term: samples from 3 steps' solves, 80 Adam steps, gamma set on the
         # held-out solve (set-up work, outside the timed region; reported in the config)
@@ -298,8 +303,9 @@ def main():
     ap.add_argument("--no-learned", action="store_true", help="flexible CG without the learned term")
     ap.add_argument("--mixed", action="store_true",
                     help="precision form: FP32-operator inner iterations inside FP64 defect correction")
-    ap.add_argument("--psolver", default="fcg", choices=["pcg", "fcg", "ml"],
-                    help="pcg: plain FP64 Jacobi-PCG; fcg: flexible CG, two-level part-local preconditioner; "
+    ap.add_argument("--psolver", default="auto", choices=["auto", "pcg", "fcg", "ml"],
+                    help="auto: fcg when the mesh fits the two-level kernel, else ml; pcg: plain FP64 "
+                         "Jacobi-PCG; fcg: flexible CG, two-level part-local preconditioner; "
                          "ml: flexible CG, aggregation-multigrid V-cycle")
     args = ap.parse_args()
 

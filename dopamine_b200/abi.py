@@ -21,7 +21,7 @@ SCHEME_BY_NAME = {"VANLEER_TVD": 1, "KOREN_TVD": 2, "CDS": 3, "KEP": 4, "QUICK":
 SGS_NONE, SGS_VREMAN, SGS_SMAGORINSKY, SGS_AMD = 0, 1, 2, 3
 WM_LOGLAW, WM_NONE, WM_MOST = 0, 1, 2
 FORM_FP64, FORM_MIXED = 0, 1
-PSOLVER_JACOBI_PCG, PSOLVER_TWOLEVEL_FCG, PSOLVER_MULTILEVEL_FCG = 0, 1, 2
+PSOLVER_JACOBI_PCG, PSOLVER_TWOLEVEL_FCG, PSOLVER_MULTILEVEL_FCG, PSOLVER_AUTO = 0, 1, 2, 3
 GRAD_LEAST_SQUARES, GRAD_GREEN_GAUSS = 0, 1
 
 EL_TET4, EL_HEX8, EL_PRISM6, EL_PYR5 = 4, 5, 6, 7
@@ -72,7 +72,7 @@ class StatsT(C.Structure):
         ("time", C.c_double), ("E", C.c_double), ("eps", C.c_double), ("Umax", C.c_double), ("Ub", C.c_double),
         ("tauw_mean", C.c_double), ("nu_sgs_mean", C.c_double), ("max_abs_divU", C.c_double),
         ("volavg_abs_divU", C.c_double), ("dt_used", C.c_double), ("p_solves", C.c_int), ("p_iters", C.c_int),
-        ("p_resid_max", C.c_double), ("p_fallbacks", C.c_int),
+        ("p_resid_max", C.c_double), ("p_fallbacks", C.c_int), ("p_solver_used", C.c_int),
     ]
 
     def as_dict(self):

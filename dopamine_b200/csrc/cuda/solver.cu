@@ -403,6 +403,11 @@ struct Solver {
     } else if (P.p_solver == DPM_PSOLVER_MULTILEVEL_FCG) {
       int rc = setup_ml(dev_sms);
       if (rc) return rc;
+    } else if (P.p_solver == DPM_PSOLVER_AUTO) {
+      // the two-level kernel keeps a part of <= 4096 cells per block, one block per SM
+      int rc = (nc + dev_sms - 1) / dev_sms <= 4096 ? setup_fcg(dev_sms) : DPM_ERR_UNSUPPORTED;
+      if (rc == DPM_ERR_UNSUPPORTED) rc = setup_ml(dev_sms);
+      if (rc) return rc;
     } else if (P.p_solver != DPM_PSOLVER_JACOBI_PCG) {
       return DPM_ERR_ARG;
     } else if (P.form == DPM_FORM_MIXED) {
@@ -1476,6 +1481,7 @@ struct Solver {
     s->volavg_abs_divU = o2[1] / o2[2];
     s->dt_used = last.dt_used;
     s->p_fallbacks = p_fallbacks;
+    s->p_solver_used = use_fcg ? DPM_PSOLVER_TWOLEVEL_FCG : (use_ml ? DPM_PSOLVER_MULTILEVEL_FCG : DPM_PSOLVER_JACOBI_PCG);
     s->p_solves = last.p_solves;
     s->p_iters = last.p_iters;
     s->p_resid_max = last.p_resid_max;

@@ -64,6 +64,7 @@ extern "C" {
 #define DPM_PSOLVER_JACOBI_PCG 0
 #define DPM_PSOLVER_TWOLEVEL_FCG 1
 #define DPM_PSOLVER_MULTILEVEL_FCG 2  /* FCG + FP32 aggregation-multigrid V-cycle (no reference counterpart) */
+#define DPM_PSOLVER_AUTO 3  /* the two-level form when the mesh fits it (<= 4096 cells per SM), else the multilevel form */
 #define DPM_GRAD_LEAST_SQUARES 0
 #define DPM_GRAD_GREEN_GAUSS 1
 #define DPM_FORM_FP64 0     /* FP64 Krylov iterations                                    */
@@ -163,6 +164,7 @@ typedef struct dpm_stats {
   int p_solves, p_iters;
   double p_resid_max;
   int p_fallbacks;            /* pressure solves handed from flexible CG to plain PCG (total)   */
+  int p_solver_used;          /* DPM_PSOLVER_* of the pressure solve in use (never AUTO)      */
 } dpm_stats_t;
 
 /* Outcome of dpm_learn_train. */

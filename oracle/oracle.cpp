@@ -2269,6 +2269,7 @@ struct Solver {
     s->p_iters = last_iters;
     s->p_resid_max = last_resid;
     s->p_fallbacks = 0;
+    s->p_solver_used = DPM_PSOLVER_JACOBI_PCG;
     apply_velocity_bc(-1, false);  // solver_divergence_metrics refreshes U_bnd without gradients
   }
 };

@@ -124,3 +124,31 @@ def test_dropin_boomeramg_name_selects_the_multilevel_solve():
     from test_zz_no_alloc import apply
     bp = rhs - rhs.mean()
     assert np.linalg.norm(bp - apply(n, fo, fn, coeff, diag, x_m)) <= 10 * 1e-10 * np.linalg.norm(bp)
+
+
+def test_auto_picks_the_form_that_fits():
+    """p_solver = DPM_PSOLVER_AUTO takes the two-level form while the mesh has at most 4096 cells
+    per SM and the multilevel form beyond; the stats report the form in use."""
+    small = cases.channel_config(nx=16, ny=12, nz=8, n_steps=1)
+    p = small.make_params()
+    p.p_solver = abi.PSOLVER_AUTO
+    s = Solver(small, params=p)
+    s.initialise()
+    s.advance()
+    assert s.stats()["p_solver_used"] == abi.PSOLVER_TWOLEVEL_FCG
+    s.close()
+    big = cases.channel_config(nx=128, ny=96, nz=64, n_steps=1)  # 786 432 cells: > 4096 per SM
+    div = {}
+    for form in (abi.PSOLVER_AUTO, abi.PSOLVER_JACOBI_PCG):
+        p = big.make_params()
+        p.p_solver = form
+        s = Solver(big, params=p)
+        s.initialise()
+        s.advance()
+        st = s.stats()
+        div[form] = st["max_abs_divU"]
+        if form == abi.PSOLVER_AUTO:
+            assert st["p_solver_used"] == abi.PSOLVER_MULTILEVEL_FCG
+        s.close()
+    # same relative stopping rule: the divergence left is of the plain form's order
+    assert div[abi.PSOLVER_AUTO] <= 10 * div[abi.PSOLVER_JACOBI_PCG] + 1e-12, div
