@@ -151,6 +151,127 @@ __global__ void __launch_bounds__(TPB) k_face_scalar(Dev d, int scheme, const do
   fdif[f] = flux;
 }
 
+// The same face fluxes for several fields at once (temperature and the passive scalars): the
+// face geometry, the upwind context and the far-upwind search are formed once per face and
+// shared; each field's arithmetic is that of k_face_scalar, expression for expression.
+struct ScalarFaceSet {
+  int n;
+  int scheme[LS_SET];
+  const double* phi[LS_SET];
+  const double* pb[LS_SET];
+  const double* g[LS_SET];
+  double alpha[LS_SET], prt[LS_SET];
+  double* fadv[LS_SET];
+  double* fdif[LS_SET];
+};
+__global__ void __launch_bounds__(TPB) k_face_scalars(Dev d, ScalarFaceSet q, const double* __restrict__ nus,
+                                                      const double* __restrict__ Uface) {
+  int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= d.nf) return;
+  const int nc = d.nc, nf = d.nf;
+  const int o = d.fo[f], n = d.fn[f];
+  const int b = f - d.nfi;
+  const int bc = n >= 0 ? -1 : d.bbc[b];
+  double Fn = (n < 0 && is_wall_bc(bc)) ? 0.0 : Uface[f];
+  bool need_ctx = false, need_far = false;
+#pragma unroll
+  for (int k = 0; k < LS_SET; ++k)
+    if (k < q.n && q.scheme[k] != 3) {
+      need_ctx = true;
+      if (q.scheme[k] != 5) need_far = true;
+    }
+  ReconCtx ctx;
+  bool ok = false;
+  int far = -1;
+  if (need_ctx) {
+    ok = recon_context_d(d, f, Fn, ctx);
+    if (ok && need_far) far = far_upwind_d(d, ctx);
+  }
+  // CDS interpolation partner and weight
+  int npr = -1;
+  bool rec = n >= 0;
+  if (!rec && bc == BC_PERIODIC) { npr = d.bpnb[b]; rec = npr >= 0; }
+  const int nsx = n >= 0 ? n : npr;
+  const double wcds = f >= d.nfi ? (rec ? d.bpgc[b] : 0.0) : d.gc[f];
+  // diffusion geometry (owner orientation)
+  const double sf0 = d.sf[f], sf1 = d.sf[nf + f], sf2 = d.sf[2 * nf + f];
+  const double area = d.area[f];
+  int kind, nbc = -1;
+  double w = 0.0, dn_[3], dl;
+  if (n >= 0) {
+    kind = 0;
+    nbc = n;
+    w = d.gc[f];
+    dn_[0] = d.cen[n] - d.cen[o]; dn_[1] = d.cen[nc + n] - d.cen[nc + o]; dn_[2] = d.cen[2 * nc + n] - d.cen[2 * nc + o];
+    dl = sqrt(dn_[0] * dn_[0] + dn_[1] * dn_[1] + dn_[2] * dn_[2]) + SMALLD;
+  } else if (bc == BC_PERIODIC && d.bpnb[b] >= 0) {
+    kind = 1;
+    nbc = d.bpnb[b];
+    const int pr = d.bpair[b];
+    const int pf = pr >= 0 ? d.nfi + pr : -1;
+    double dper;
+    if (pf >= 0) { dper = d.dcf[f] + d.dcf[pf]; w = d.dcf[pf] / (dper + SMALLD); }
+    else if (d.bpdcf[b] > SMALLD) { dper = d.dcf[f] + d.bpdcf[b]; w = d.bpdcf[b] / (dper + SMALLD); }
+    else { dper = 2.0 * d.dcf[f]; w = 0.5; }
+    dn_[0] = dper * d.nrm[f]; dn_[1] = dper * d.nrm[nf + f]; dn_[2] = dper * d.nrm[2 * nf + f];
+    dl = dper + SMALLD;
+  } else {
+    kind = 2;
+    dn_[0] = d.fcen[f] - d.cen[o]; dn_[1] = d.fcen[nf + f] - d.cen[nc + o]; dn_[2] = d.fcen[2 * nf + f] - d.cen[2 * nc + o];
+    dl = sqrt(dn_[0] * dn_[0] + dn_[1] * dn_[1] + dn_[2] * dn_[2]) + SMALLD;
+  }
+  const double sdd = (sf0 * dn_[0] + sf1 * dn_[1] + sf2 * dn_[2]) / dl;
+  const double dp0 = sf0 - (sdd / dl) * dn_[0], dp1 = sf1 - (sdd / dl) * dn_[1], dp2 = sf2 - (sdd / dl) * dn_[2];
+  const double wo = area * fmax(0.0, fmin(1.0, sdd / (area + SMALLD)));
+  const double nuf = kind == 2 ? nus[o] : (w * nus[o] + (1.0 - w) * nus[nbc]);
+  const double Fc = finite_d(Fn) ? Fn : 0.0;
+#pragma unroll
+  for (int k = 0; k < LS_SET; ++k) {
+    if (k >= q.n) break;
+    const double* phi = q.phi[k];
+    const double* g = q.g[k];
+    double ph;
+    if (q.scheme[k] == 3) {  // CDS
+      if (rec) {
+        const double plain = wcds * phi[o] + (1.0 - wcds) * phi[nsx];
+        if (f < d.nfi) {
+          double gm0 = wcds * g[o] + (1.0 - wcds) * g[nsx];
+          double gm1 = wcds * g[nc + o] + (1.0 - wcds) * g[nc + nsx];
+          double gm2 = wcds * g[2 * nc + o] + (1.0 - wcds) * g[2 * nc + nsx];
+          double pe = plain + (gm0 * d.eps[f] + gm1 * d.eps[nf + f] + gm2 * d.eps[2 * nf + f]);
+          const double wb = d.wbl[f];
+          if (wb < 1.0) pe = plain + wb * (pe - plain);
+          ph = pe;
+        } else {
+          ph = plain;
+        }
+        if (!finite_d(ph)) ph = (Fn >= 0.0 || n < 0) ? phi[o] : phi[n];
+      } else {
+        ph = q.pb[k][b];
+      }
+    } else if (ok) {  // QUICK (5), van Leer (1), Koren (2)
+      if (q.scheme[k] == 5) quick_d<1>(d, ctx, phi, g, &ph);
+      else ph = tvd_d(d, q.scheme[k], phi, ctx, far);
+      if (!finite_d(ph)) ph = (Fn >= 0.0 || n < 0) ? phi[o] : phi[n];
+    } else {
+      ph = q.pb[k][b];
+    }
+    if (!finite_d(ph)) ph = 0.0;
+    q.fadv[k][f] = Fc * ph;
+    const double aeff = q.alpha[k] + nuf / q.prt[k];
+    double dphi;
+    if (kind == 2) {
+      dphi = (q.pb[k][b] - phi[o]) * wo / dl + (g[o] * dp0 + g[nc + o] * dp1 + g[2 * nc + o] * dp2);
+    } else {
+      const double gf0 = w * g[o] + (1.0 - w) * g[nbc];
+      const double gf1 = w * g[nc + o] + (1.0 - w) * g[nc + nbc];
+      const double gf2 = w * g[2 * nc + o] + (1.0 - w) * g[2 * nc + nbc];
+      dphi = (phi[nbc] - phi[o]) * wo / dl + (gf0 * dp0 + gf1 * dp1 + gf2 * dp2);
+    }
+    q.fdif[k][f] = aeff * dphi;
+  }
+}
+
 // Per-cell gather: H = conv + diff in ascending face order, plus the MOST wall heat flux qw
 // (kinematic, per area) of wall-model faces when qw is given (src/solver/mod_fv_solver.f90:
 // 2279-2313); with predict, the RK3W update phi += dt (a_k H + b_k H0) in place (:1322-1350).

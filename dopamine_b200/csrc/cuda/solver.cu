@@ -629,7 +629,8 @@ struct Solver {
       return DPM_ERR_UNSUPPORTED;
     Tb = mem.alloc<double>(std::max(nb, 1)); gT = mem.alloc<double>(3 * (size_t)nc);
     HT = mem.alloc<double>(nc); HT0 = mem.alloc<double>(nc);
-    sc_fadv = mem.alloc<double>(nf); sc_fdif = mem.alloc<double>(nf);
+    // face fluxes per transported field (temperature, then the passive scalars)
+    sc_fadv = mem.alloc<double>((size_t)(ns + 1) * nf); sc_fdif = mem.alloc<double>((size_t)(ns + 1) * nf);
     std::vector<double> tv(std::max(nb, 1), P.T_ref), sv((size_t)std::max(ns, 1) * std::max(nb, 1), 0.0);
     std::vector<int> sm((size_t)std::max(ns, 1) * std::max(nb, 1), 0);
     for (int b = 0; b < nb; ++b) {
@@ -722,14 +723,34 @@ struct Solver {
                                             qw);
     launches += 2;
   }
+  // All transported fields together: one face pass for every field (the fields do not read each
+  // other), then each field's gather and RK3W update.
   void scalars_rhs(double dt, double a_k, double b_k) {
+    ScalarFaceSet q{};
+    double* H[LS_SET];
+    const double* H0[LS_SET];
+    double* phi[LS_SET];
+    const double* qw[LS_SET];
+    auto add = [&](int scheme, double* f, const double* pbv, const double* g, double alpha, double prt, double* h,
+                   const double* h0, const double* w) {
+      const int k = q.n++;
+      q.scheme[k] = scheme; q.phi[k] = f; q.pb[k] = pbv; q.g[k] = g; q.alpha[k] = alpha; q.prt[k] = prt;
+      q.fadv[k] = sc_fadv + (size_t)k * nf; q.fdif[k] = sc_fdif + (size_t)k * nf;
+      H[k] = h; H0[k] = h0; phi[k] = f; qw[k] = w;
+    };
     if (P.boussinesq)
-      scalar_transport(P.temperature_scheme, F.T, Tb, gT, P.alpha_T, P.Pr_t, HT, HT0, dt, a_k, b_k, 1, nullptr,
-                       nullptr, P.wall_model == DPM_WM_MOST ? most_qw : nullptr);
+      add(P.temperature_scheme, F.T, Tb, gT, P.alpha_T, P.Pr_t, HT, HT0, P.wall_model == DPM_WM_MOST ? most_qw : nullptr);
     for (int k = 0; k < ns; ++k)
-      scalar_transport(P.scalar_scheme, Cs + (size_t)k * nc, Cb + (size_t)k * nb, gC + (size_t)k * 3 * nc,
-                       P.scalar_diffusivity[k], P.scalar_pr_t[k], HC + (size_t)k * nc, HC0 + (size_t)k * nc, dt, a_k,
-                       b_k, 1, nullptr, nullptr);
+      add(P.scalar_scheme, Cs + (size_t)k * nc, Cb + (size_t)k * nb, gC + (size_t)k * 3 * nc, P.scalar_diffusivity[k],
+          P.scalar_pr_t[k], HC + (size_t)k * nc, HC0 + (size_t)k * nc, nullptr);
+    if (q.n == 0) return;
+    k_face_scalars<<<nblk(nf), TPB, 0, st>>>(d, q, F.nu_sgs, F.Uf);
+    launches++;
+    for (int k = 0; k < q.n; ++k) {
+      k_cell_scalar<<<nblk(nc), TPB, 0, st>>>(d, q.fadv[k], q.fdif[k], H[k], H0[k], phi[k], nullptr, nullptr, dt, a_k,
+                                              b_k, 1, qw[k]);
+      launches++;
+    }
   }
 
   // Two-level FCG set-up: one part per SM (the kernel needs one co-resident block per part and
