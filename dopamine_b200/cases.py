@@ -604,7 +604,7 @@ def rb_config(nx=256, ny=256, nz=128, n_steps=10, noise_seed=20261207):
 
 
 def urban_config(nx=400, ny=400, nz=125, n_blocks=200, n_steps=10, lx=1000.0, ly=1000.0, lz=300.0,
-                 noise_seed=20261209):
+                 noise_seed=20261209, scale=1.0):
     """Urban-canopy atmospheric boundary layer (fifth configuration): lx x ly x lz metres with
     seeded cuboid obstacles carved out (urban_box), periodic lateral boundaries, MOST wall model
     on the ground (z0_m 0.1 m, z0_h 0.01 m) and the obstacles (their own z0_m 0.05 m, z0_h 0.005 m,
@@ -612,19 +612,23 @@ def urban_config(nx=400, ny=400, nz=125, n_blocks=200, n_steps=10, lx=1000.0, ly
     length -100 m (unstable) held fixed), slip top, AMD SGS, KEP momentum, Boussinesq temperature and one
     passive scalar (Dirichlet 1 on the ground) with van Leer TVD, constant streamwise pressure
     gradient u_tau^2 / lz with u_tau = 0.5 m/s.  Initial state: 5 m/s streamwise with seeded
-    +-10 % multiplicative noise."""
-    mesh = urban_box(nx, ny, nz, lx, ly, lz, n_blocks)
+    +-10 % multiplicative noise.  `scale` multiplies the block sizes, their margin, the roughness
+    lengths and the Obukhov length (the domain lengths are given directly): a geometrically
+    scaled copy whose Poisson solves are governed by the relative tolerance rather than by the
+    reference's cell-volume-based absolute one, as parity tests at small sizes need."""
+    mesh = urban_box(nx, ny, nz, lx, ly, lz, n_blocks, side=(10.0 * scale, 60.0 * scale),
+                     height=(10.0 * scale, 80.0 * scale), margin=40.0 * scale)
     wall = {"bc": "wallModel"}
     patches = [{"bc": "periodic"}] * 4 + [dict(wall, scalar_mode=(1, 0, 0, 0), scalar_value=(1.0, 0, 0, 0)),
-                                          {"bc": "slip"}, dict(wall, z0_m=0.05, z0_h=0.005)]
+                                          {"bc": "slip"}, dict(wall, z0_m=0.05 * scale, z0_h=0.005 * scale)]
     dx = lx / nx
     u0 = 5.0
     prm = dict(scheme=abi.SCHEME_KEP, sgs_model=abi.SGS_AMD, wall_model=abi.WM_MOST, nu=1.5e-5, alpha_T=2.1e-5,
                beta=1.0 / 300.0, T_ref=300.0, g=(0.0, 0.0, -9.81), boussinesq=1, temperature_scheme=abi.SCHEME_VANLEER_TVD,
                f_const=(0.25 / lz, 0.0, 0.0), dt=0.3 * dx / (1.5 * u0), cfl_max=0.5, p_tol=1e-10, p_max_iter=20000,
                rhie_chow_dual=0, n_scalars=1, scalar_scheme=abi.SCHEME_VANLEER_TVD, scalar_diffusivity=(2.1e-5, 0, 0, 0),
-               scalar_pr_t=(0.85, 0, 0, 0), abl_z0_m=0.1, abl_z0_h=0.01, abl_T_surface=302.0,
-               abl_L_obukhov=-100.0, abl_compute_L=0)
+               scalar_pr_t=(0.85, 0, 0, 0), abl_z0_m=0.1 * scale, abl_z0_h=0.01 * scale, abl_T_surface=302.0,
+               abl_L_obukhov=-100.0 * scale, abl_compute_L=0)
     return Case(f"urban{nx}x{ny}x{nz}", mesh, patches, prm, "uniform", u0, noise=0.10, noise_seed=noise_seed,
                 n_steps=n_steps,
                 description=f"urban canopy {nx}x{ny}x{nz} ({mesh.n_cells} fluid cells, {n_blocks} blocks), MOST, AMD")

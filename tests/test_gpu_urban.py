@@ -1,5 +1,5 @@
 """GPU parity on the urban-canopy configuration at reduced size (24 x 24 x 12 cells, 4 seeded
-cuboid obstacles carved out): internal obstacle walls with the MOST wall model, periodic lateral
+cuboid obstacles carved out, geometrically scaled by 1/100): internal obstacle walls with the MOST wall model, periodic lateral
 boundaries, slip top, AMD SGS, KEP, Boussinesq temperature and one passive scalar.
 
 The plain path (Jacobi-PCG) must follow the oracle step by step (relative L2 1e-9 on U and the
@@ -18,7 +18,10 @@ pytestmark = pytest.mark.gpu
 
 
 def _case():
-    return cases.urban_config(nx=24, ny=24, nz=12, n_blocks=4, lx=240.0, ly=240.0, lz=72.0, n_steps=3)
+    # a 1/100 geometric copy (2.4 x 2.4 x 0.72 m, 0.1 m cells): at full scale the reference's
+    # absolute Poisson tolerance (1e-12 |U| V_min / dt) would dominate p_tol = 1e-13, and two
+    # different Krylov methods stopped there legitimately differ far above round-off
+    return cases.urban_config(nx=24, ny=24, nz=12, n_blocks=4, lx=2.4, ly=2.4, lz=0.72, n_steps=3, scale=0.01)
 
 
 def _l2(a, b):
