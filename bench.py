@@ -10,7 +10,7 @@ large for it; both with the learned term trained and gated); on one GPU the plai
 Jacobi-PCG form is timed beside it on the same workload and reported in the config.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                    [--config channel|tgv|rb|mixed|urban] [--psolver auto|fcg|pcg|ml] [--no-plain]
+                    [--config channel|channel3m|tgv|rb|mixed|urban] [--psolver auto|fcg|pcg|ml] [--no-plain]
 
 (--psolver auto, the default, takes the two-level form when the mesh fits it — up to 4096 cells
 per SM — and the multilevel form otherwise, as for the rb, mixed and urban configurations)
@@ -119,6 +119,8 @@ def make_case(name):
         return cases.channel_config(96, 64, 64)
     if name == "tgv":
         return cases.tgv_config(64)
+    if name == "channel3m":
+        return cases.channel_config(192, 128, 128)
     if name == "rb":
         return cases.rb_config(256, 256, 128)
     if name == "mixed":
@@ -297,7 +299,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="dopamine_b200")
-    ap.add_argument("--config", default="channel", choices=["channel", "tgv", "rb", "mixed", "urban"])
+    ap.add_argument("--config", default="channel", choices=["channel", "channel3m", "tgv", "rb", "mixed", "urban"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip timing the plain FP64 Jacobi-PCG form")
     ap.add_argument("--no-learned", action="store_true", help="flexible CG without the learned term")
@@ -313,6 +315,7 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     cfg_name = {"channel": "channel 96x64x64 Re_tau=395, KEP, Vreman, log-law wall model",
                 "tgv": "Taylor-Green 64^3, CDS",
+                "channel3m": "channel 192x128x128 (3.1M cells) Re_tau=395, KEP, Vreman, log-law wall model",
                 "rb": "Rayleigh-Benard 256x256x128 (8.4M cells), Ra=1e7, Pr=0.7, T + 2 scalars van Leer, Vreman",
                 "mixed": "jittered unit box 128^3 as hexes + prisms + pyramids (4.9M cells), AMD, Koren TVD",
                 "urban": "urban canopy 1000x1000x300 m, 400x400x125 with 200 seeded obstacles carved out "
