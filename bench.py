@@ -385,7 +385,7 @@ def main():
         line["config"]["plain_fp64_pcg"] = {"ms_per_step": pm, "poisson_ms_per_step": pp,
                                             "pcg_iterations_per_step": pit,
                                             "speedup_of_this_form": pm / line["ms_per_step"]}
-    if not args.no_cpu_baseline:
+    if not args.no_cpu_baseline and world == 1:  # the CPU baseline is reported at N = 1 only
         cb = cpu_baseline(args.config, budget_s=20.0)
         line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
     print(json.dumps(line))
