@@ -50,18 +50,20 @@ __device__ __forceinline__ double ld_cg(const double* p) { return __ldcg(p); }
 __device__ __forceinline__ float ld_cg(const float* p) { return __ldcg(p); }
 
 // Grid-wide deterministic all-reduce + barrier.  Each block reduces its NV values (fixed shuffle
-// tree), thread 0 writes them into the partial buffer of this barrier (two buffers alternate) and
-// arrives on a monotonic counter; once all blocks have arrived, warp 0 of every block reads all
-// partials with a fixed lane-to-block mapping and reduces them with the same shuffle tree, so all
-// blocks hold bit-identical totals.  Two __syncthreads per call; the wait is bounded and returns
-// false on timeout.
+// trees; warp k takes value k), writes them into the partial buffer of this barrier (two buffers
+// alternate) and thread 0 arrives on a monotonic counter; once all blocks have arrived, warp k of
+// every block reads value k of all partials with a fixed lane-to-block mapping, all of a lane's
+// loads of a round issued together, and reduces them with the same shuffle tree, so all blocks
+// hold bit-identical totals.  The wait is bounded and returns false on timeout.
 template <int NV>
 __device__ __forceinline__ bool grid_allreduce(double (&v)[NV], double* partials, unsigned* bar, unsigned& gen,
                                                int* status, double (&res)[NV]) {
+  constexpr int RB = 5;  // blocks per lane per round of the post-barrier read (one round up to 160 blocks)
   __shared__ double sh[32][4];
   __shared__ double shr[4];
   __shared__ int s_ok;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int P = gridDim.x;
   double* buf = partials + (size_t)(gen & 1u) * 4 * gridDim.x;
 #pragma unroll
   for (int k = 0; k < NV; ++k)
@@ -70,49 +72,45 @@ __device__ __forceinline__ bool grid_allreduce(double (&v)[NV], double* partials
 #pragma unroll
     for (int k = 0; k < NV; ++k) sh[w][k] = v[k];
   __syncthreads();
-  if (w == 0) {
-    double t[NV];
-#pragma unroll
-    for (int k = 0; k < NV; ++k) {
-      t[k] = lane < nw ? sh[lane][k] : 0.0;
-      for (int o = 16; o > 0; o >>= 1) t[k] += __shfl_down_sync(0xffffffffu, t[k], o);
-    }
-    const unsigned target = (gen + 1u) * gridDim.x;
+  if (w < NV) {  // warp w: value w over the block's warps
+    double t = lane < nw ? sh[lane][w] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+    if (lane == 0) buf[blockIdx.x * 4 + w] = t;
+  }
+  __syncthreads();  // the partial stores precede thread 0's release below
+  if (threadIdx.x == 0) {
     int ok = 1;
-    if (lane == 0) {
-#pragma unroll
-      for (int k = 0; k < NV; ++k) buf[blockIdx.x * 4 + k] = t[k];
-      __threadfence();
-      atomicAdd(&bar[0], 1u);
-      unsigned spins = 0;
-      for (;;) {
-        unsigned cur;
-        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(cur) : "l"(&bar[0]) : "memory");
-        if ((int)(cur - target) >= 0) break;
-        if (++spins > DPM_BARRIER_SPIN_LIMIT) { ok = 0; atomicExch(&status[2], 1); break; }
-        if (spins > 32) __nanosleep(20);
-      }
-      __threadfence();
+    const unsigned target = (gen + 1u) * gridDim.x;
+    __threadfence();
+    atomicAdd(&bar[0], 1u);
+    unsigned spins = 0;
+    for (;;) {
+      unsigned cur;
+      asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(cur) : "l"(&bar[0]) : "memory");
+      if ((int)(cur - target) >= 0) break;
+      if (++spins > DPM_BARRIER_SPIN_LIMIT) { ok = 0; atomicExch(&status[2], 1); break; }
+      if (spins > 32) __nanosleep(20);
     }
-    ok = __shfl_sync(0xffffffffu, ok, 0);
-    double u[NV];
+    __threadfence();
+    s_ok = ok;
+  }
+  __syncthreads();
+  if (s_ok && w < NV) {  // warp w: value w over the blocks, lane l sums blocks l, l + 32, ... in order
+    double u = 0.0;
+    for (int b0 = lane; b0 < P; b0 += 32 * RB) {
+      double pv[RB];
 #pragma unroll
-    for (int k = 0; k < NV; ++k) u[k] = 0.0;
-    if (ok)
-      for (int b = lane; b < (int)gridDim.x; b += 32)
+      for (int h = 0; h < RB; ++h) pv[h] = b0 + 32 * h < P ? __ldcg(&buf[(b0 + 32 * h) * 4 + w]) : 0.0;
 #pragma unroll
-        for (int k = 0; k < NV; ++k) u[k] += __ldcg(&buf[b * 4 + k]);
-#pragma unroll
-    for (int k = 0; k < NV; ++k) {
-      for (int o = 16; o > 0; o >>= 1) u[k] += __shfl_down_sync(0xffffffffu, u[k], o);
-      if (lane == 0) shr[k] = u[k];
+      for (int h = 0; h < RB; ++h) u += pv[h];
     }
-    if (lane == 0) s_ok = ok;
+    for (int o = 16; o > 0; o >>= 1) u += __shfl_down_sync(0xffffffffu, u, o);
+    if (lane == 0) shr[w] = u;
   }
   __syncthreads();
   gen = gen + 1u;
 #pragma unroll
-  for (int k = 0; k < NV; ++k) res[k] = shr[k];
+  for (int k = 0; k < NV; ++k) res[k] = s_ok ? shr[k] : 0.0;
   return s_ok != 0;
 }
 
