@@ -22,6 +22,7 @@ SGS_NONE, SGS_VREMAN, SGS_SMAGORINSKY, SGS_AMD = 0, 1, 2, 3
 WM_LOGLAW, WM_NONE, WM_MOST = 0, 1, 2
 FORM_FP64, FORM_MIXED = 0, 1
 PSOLVER_JACOBI_PCG, PSOLVER_TWOLEVEL_FCG, PSOLVER_MULTILEVEL_FCG, PSOLVER_AUTO = 0, 1, 2, 3
+OK, ERR_ARG, ERR_CUDA, ERR_MESH, ERR_NOT_FINITE, ERR_DT_COLLAPSE, ERR_UNSUPPORTED, ERR_BARRIER_TIMEOUT = 0, -1, -2, -3, -4, -5, -6, -7
 GRAD_LEAST_SQUARES, GRAD_GREEN_GAUSS = 0, 1
 
 EL_TET4, EL_HEX8, EL_PRISM6, EL_PYR5 = 4, 5, 6, 7
@@ -63,7 +64,8 @@ class ParamsT(C.Structure):
         ("p_smooth_lmax", C.c_double), ("abl_z0_m", C.c_double), ("abl_z0_h", C.c_double),
         ("abl_T_surface", C.c_double), ("abl_L_obukhov", C.c_double), ("abl_compute_L", C.c_int),
         ("p_ml_degree", C.c_int), ("p_ml_overcorrect", C.c_double), ("p_ml_passes", C.c_int),
-        ("gradient_scheme", C.c_int), ("gg_iterations", C.c_int),
+        ("gradient_scheme", C.c_int), ("gg_iterations", C.c_int), ("p_stall_window", C.c_int),
+        ("p_stall_ratio", C.c_double),
     ]
 
 

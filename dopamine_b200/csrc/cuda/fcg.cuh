@@ -52,7 +52,7 @@ struct FcgArgs {
   double* zs;             // [n] scratch, new numbering
   double* partials;       // [2][P][FCG_SLOT]
   unsigned* bar;          // [0] arrival counter
-  int* status;            // [0] reason, [1] iterations, [2] barrier timeout
+  int* status;            // [0] reason, [1] iterations, [2] barrier timeout, [3] poll limit (0: default)
   double* dout;           // [0] true residual, [1] last ||r||, [2] ||b'||
   double rtol, atol;
   float theta, delta;     // Chebyshev interval [theta - delta, theta + delta] of D^-1 A_bb
@@ -64,7 +64,8 @@ struct FcgArgs {
   // numbering).  rec_stride = 0: off.
   int rec_stride, rec_base, rec_max;
   double *rec_r, *rec_z, *rec_u, *rec_x;
-  int stall_window;       // > 0: stop with reason -20 when ||r|| fell by < 10 % over that many iterations
+  int stall_window;       // > 0: stop with reason -20 when ||r|| > stall_ratio * ||r|| of a window earlier
+  double stall_ratio;     // default 0.9 (less than 10 % reduction over the window)
   // precision form: FP32 copy of the operator values and FP32 z for w = A z (products summed in
   // FP64); the initial and the final residual stay FP64.  inner_rel > 0: also stop once
   // ||r|| <= inner_rel * ||r_0|| (one pass of the outer FP64 defect correction).
@@ -80,6 +81,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned* bar, unsigned& gen, int* 
   if (threadIdx.x == 0) {
     int ok = 1;
     const unsigned target = (gen + 1u) * gridDim.x;
+    const unsigned lim = spin_limit(status);
     __threadfence();
     atomicAdd(&bar[0], 1u);
     unsigned spins = 0;
@@ -87,7 +89,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned* bar, unsigned& gen, int* 
       unsigned cur;
       asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(cur) : "l"(&bar[0]) : "memory");
       if ((int)(cur - target) >= 0) break;
-      if (++spins > DPM_BARRIER_SPIN_LIMIT) { ok = 0; atomicExch(&status[2], 1); break; }
+      if (++spins > lim) { ok = 0; atomicExch(&status[2], 1); break; }
       if (spins > 32) __nanosleep(20);
     }
     __threadfence();
@@ -133,6 +135,7 @@ __device__ __forceinline__ bool grid_reduce_gather(double (&v)[NV + NG], double*
   if (threadIdx.x == 0) {
     int ok = 1;
     const unsigned target = (gen + 1u) * gridDim.x;
+    const unsigned lim = spin_limit(status);
     __threadfence();
     atomicAdd(&bar[0], 1u);
     unsigned spins = 0;
@@ -140,7 +143,7 @@ __device__ __forceinline__ bool grid_reduce_gather(double (&v)[NV + NG], double*
       unsigned cur;
       asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(cur) : "l"(&bar[0]) : "memory");
       if ((int)(cur - target) >= 0) break;
-      if (++spins > DPM_BARRIER_SPIN_LIMIT) { ok = 0; atomicExch(&status[2], 1); break; }
+      if (++spins > lim) { ok = 0; atomicExch(&status[2], 1); break; }
       if (spins > 32) __nanosleep(20);
     }
     __threadfence();
@@ -411,7 +414,7 @@ __global__ void __launch_bounds__(FCG_TPB, 1) k_fcg(FcgArgs a, int WA) {
     reason = classify(dp, ttol, a.atol, rnorm0);
     if (reason) break;
     if (a.stall_window > 0 && its > 0 && its % a.stall_window == 0) {  // automatic fallback trigger
-      if (dp > 0.9 * dp_mark) { reason = -20; break; }
+      if (dp > a.stall_ratio * dp_mark) { reason = -20; break; }
       dp_mark = dp;
     }
     const double m = a.nullsp ? t[3] / (double)n : 0.0;

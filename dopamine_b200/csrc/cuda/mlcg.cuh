@@ -66,10 +66,11 @@ struct MlArgs {
   double *r, *p, *q, *w;  // [n]
   double* partials;       // [2][grid][FCG_SLOT]
   unsigned* bar;
-  int* status;            // [0] reason, [1] iterations, [2] barrier timeout
+  int* status;            // [0] reason, [1] iterations, [2] barrier timeout, [3] poll limit (0: default)
   double* dout;           // [0] true residual, [1] last ||r||, [2] ||b'||
   double rtol, atol;
-  int stall_window;
+  int stall_window;        // > 0: stop with reason -20 when ||r|| > stall_ratio * ||r|| of a window earlier
+  double stall_ratio;
   // learned term: gamma * omega .* D^-1 r added to the last fine-level smoothing step
   // (omega [n] in this numbering; gamma = 0: off)
   const float* omega;
@@ -425,7 +426,7 @@ __global__ void __launch_bounds__(ML_TPB, 2) k_mlcg(MlArgs a) {
     reason = classify(dp, ttol, a.atol, rnorm0);
     if (reason) break;
     if (a.stall_window > 0 && its > 0 && its % a.stall_window == 0) {
-      if (dp > 0.9 * dp_mark) { reason = -20; break; }
+      if (dp > a.stall_ratio * dp_mark) { reason = -20; break; }
       dp_mark = dp;
     }
     const double m = a.nullsp ? t[3] / (double)n : 0.0;

@@ -20,6 +20,7 @@ struct MlSolver {
   int grid = 0;
   std::vector<int> sizes;      // rows per level, coarsest last
   std::vector<void*> owned;    // device allocations of this object
+  int spin_limit_override = 0;  // > 0: poll limit of the kernel's grid-wide waits (status[3])
 
   MlSolver() = default;
   MlSolver(const MlSolver&) = delete;
@@ -118,6 +119,7 @@ struct MlSolver {
     a.bar = bar; a.status = status; a.dout = dout;
     a.nullsp = nullsp ? 1 : 0;
     a.stall_window = 50;
+    a.stall_ratio = 0.9;
     if (!a.cinv || !a.bC || !a.xC || !a.r || !a.p || !a.q || !a.w || !a.partials) return DPM_ERR_CUDA;
     base = a;
     sizes = M.sizes;
@@ -140,6 +142,9 @@ struct MlSolver {
     a.b = b; a.x = x; a.rtol = rtol; a.atol = atol; a.maxit = maxit; a.guess_zero = guess_zero;
     if (cudaMemsetAsync(a.bar, 0, 2 * sizeof(unsigned), st) != cudaSuccess) return DPM_ERR_CUDA;
     if (cudaMemsetAsync(a.status, 0, 4 * sizeof(int), st) != cudaSuccess) return DPM_ERR_CUDA;
+    if (spin_limit_override &&
+        cudaMemcpyAsync(a.status + 3, &spin_limit_override, sizeof(int), cudaMemcpyHostToDevice, st) != cudaSuccess)
+      return DPM_ERR_CUDA;
     void* args[] = {&a};
     if (cudaLaunchCooperativeKernel((void*)k_mlcg<0>, dim3(grid), dim3(ML_TPB), args, 0, st) != cudaSuccess)
       return DPM_ERR_CUDA;
@@ -150,7 +155,7 @@ struct MlSolver {
     if (cudaStreamSynchronize(st) != cudaSuccess) return DPM_ERR_CUDA;
     if (h_st[2]) {
       std::fprintf(stderr, "dopamine_b200: multilevel FCG grid barrier timed out\n");
-      return DPM_ERR_CUDA;
+      return DPM_ERR_BARRIER_TIMEOUT;
     }
     *reason = h_st[0];
     *its = h_st[1];

@@ -12,13 +12,20 @@
 // Limits and behaviour a caller must know:
 //  * at most DPM_NOALLOC_MAX_CELLS cells and rows of at most 16 entries; larger problems are
 //    rejected with DPM_ERR_ARG and a message on stderr;
-//  * the scratch array (about 5.3 MB) is held by every GPU that loads the library, until exit;
+//  * the scratch array (about 5.3 MB) belongs to this library's device module.  The CUDA runtime
+//    loads modules lazily, so the array (and the solve kernels' code) is created on a device by
+//    the first call on that device, not when the library is loaded; from then on it is held
+//    until the process exits.  That first call can fail with DPM_ERR_CUDA when the device has no
+//    free memory left.  A call with max_iterations == 0 does only this per-device set-up (module
+//    load, every solve kernel variant, the array's address) and returns 0 without touching any
+//    array argument: make it before the host's pool reserves the device's memory, and before
+//    any stream capture;
 //  * all calls share that one array and it keeps the last call's contents; each call clears
 //    the parts that must start at zero (barrier counter, status words) itself;
 //  * calls that overlap on the GPU (two streams, or two host threads) race on the array and must
 //    be serialized by the caller;
-//  * the first call on a device looks up the array's device address (cudaGetSymbolAddress) and
-//    the kernel attributes; make that first call before any stream capture.
+//  * the array's device address is looked up (cudaGetSymbolAddress) on every call, so a device
+//    reset that reloads the module is followed correctly.
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -32,7 +39,6 @@ using namespace dpm::gpu;
 
 constexpr int kMaxCells = DPM_NOALLOC_MAX_CELLS;
 constexpr int kMaxBlocks = 1024;
-constexpr int kMaxDevices = 64;
 // doubles: r, z, p0, p1, q (5 x kMaxCells), partials (2 x 4 x kMaxBlocks), dout (4);
 // then unsigned bar (4) and int status (4)
 constexpr size_t kVecOff = 0;
@@ -43,19 +49,31 @@ constexpr size_t kScratchBytes = kNumDoubles * sizeof(double) + 64;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
-// Host-side cache of the array's device address per device (the symbol name itself is only a
-// host stand-in; a kernel handed it would read the wrong memory).
-void* g_scratch_dev[kMaxDevices] = {nullptr};
-
-int setup_device(int dev) {
-  if (g_scratch_dev[dev]) return 0;
-  void* ptr = nullptr;
-  cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
-  if (e != cudaSuccess || !ptr) {
+// The array's device address on the current device.  The symbol name itself is only a host
+// stand-in: a kernel handed it would read the wrong memory.  Loads the module on first use.
+int scratch_address(void** ptr) {
+  *ptr = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(ptr, g_noalloc_scratch);
+  if (e != cudaSuccess || !*ptr) {
     std::fprintf(stderr, "dpm_pcg_solve_noalloc: cudaGetSymbolAddress failed: %s\n", cudaGetErrorString(e));
     return DPM_ERR_CUDA;
   }
-  g_scratch_dev[dev] = ptr;
+  return 0;
+}
+
+// Every k_pcg instantiation the solve can pick (cells per thread 0..4, row width 7 or runtime):
+// querying their attributes makes the runtime load them now rather than at a later launch.
+int preload_kernels() {
+  const void* ks[] = {(const void*)k_pcg<double, 0, 7>, (const void*)k_pcg<double, 1, 7>,
+                      (const void*)k_pcg<double, 2, 7>, (const void*)k_pcg<double, 3, 7>,
+                      (const void*)k_pcg<double, 4, 7>, (const void*)k_pcg<double, 0, 0>,
+                      (const void*)k_pcg<double, 1, 0>, (const void*)k_pcg<double, 2, 0>,
+                      (const void*)k_pcg<double, 3, 0>, (const void*)k_pcg<double, 4, 0>};
+  for (const void* k : ks) {
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, k) != cudaSuccess) return DPM_ERR_CUDA;
+    if (cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 5) != cudaSuccess) return DPM_ERR_CUDA;
+  }
   return 0;
 }
 
@@ -72,12 +90,20 @@ extern "C" int dpm_pcg_solve_noalloc(int n_cells, int row_width, const int* col,
                  n_cells, row_width, kMaxCells);
     return DPM_ERR_ARG;
   }
-  if (!col || !val || !inv_diag || !rhs || !x || !iteration_count || !residual_norm || max_iterations < 0)
-    return DPM_ERR_ARG;
+  if (!iteration_count || !residual_norm || max_iterations < 0) return DPM_ERR_ARG;
   int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return DPM_ERR_CUDA;
-  int rc = setup_device(dev);
+  if (cudaGetDevice(&dev) != cudaSuccess) return DPM_ERR_CUDA;
+  void* scratch = nullptr;
+  int rc = scratch_address(&scratch);
   if (rc) return rc;
+  if (max_iterations == 0) {  // per-device set-up only: no array argument is read
+    rc = preload_kernels();
+    if (rc) return rc;
+    *iteration_count = 0;
+    *residual_norm = 0.0;
+    return DPM_OK;
+  }
+  if (!col || !val || !inv_diag || !rhs || !x) return DPM_ERR_ARG;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
 
   int sms = 0, per_sm = 0, cpt = 0;
@@ -101,7 +127,7 @@ extern "C" int dpm_pcg_solve_noalloc(int n_cells, int row_width, const int* col,
       return DPM_ERR_CUDA;
   }
 
-  double* base = static_cast<double*>(g_scratch_dev[dev]);
+  double* base = static_cast<double*>(scratch);
   unsigned* bar = reinterpret_cast<unsigned*>(base + kNumDoubles);
   int* status = reinterpret_cast<int*>(bar + 4);
   // barrier counter and status words must start at zero; the rest is overwritten by the solve

@@ -29,6 +29,14 @@ namespace gpu {
 
 constexpr int PCG_TPB = 1024;
 
+// Poll limit of a grid-wide wait: status[3] when the host set it (a failure-detection test makes
+// the wait run out this way), else DPM_BARRIER_SPIN_LIMIT.  Read by the waiting thread before it
+// arrives, so the load overlaps the arrival.
+__device__ __forceinline__ unsigned spin_limit(const int* status) {
+  const unsigned o = (unsigned)__ldcg(&status[3]);
+  return o ? o : (unsigned)DPM_BARRIER_SPIN_LIMIT;
+}
+
 template <class V>
 struct PcgArgs {
   int n, WA;
@@ -40,7 +48,7 @@ struct PcgArgs {
   V *r, *z, *p0, *p1, *q, *bp;
   double* partials;    // [2][nblocks][4]
   unsigned* bar;       // [0] monotonic arrival counter
-  int* status;         // [0] reason, [1] iterations, [2] barrier timeout
+  int* status;         // [0] reason, [1] iterations, [2] barrier timeout, [3] poll limit (0: default)
   double* dout;        // [0] true residual ||b - A x||, [1] last ||r||, [2] ||b'||
   double rtol, atol;
   int maxit, nullsp, guess_zero;
@@ -81,6 +89,7 @@ __device__ __forceinline__ bool grid_allreduce(double (&v)[NV], double* partials
   if (threadIdx.x == 0) {
     int ok = 1;
     const unsigned target = (gen + 1u) * gridDim.x;
+    const unsigned lim = spin_limit(status);
     __threadfence();
     atomicAdd(&bar[0], 1u);
     unsigned spins = 0;
@@ -88,7 +97,7 @@ __device__ __forceinline__ bool grid_allreduce(double (&v)[NV], double* partials
       unsigned cur;
       asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(cur) : "l"(&bar[0]) : "memory");
       if ((int)(cur - target) >= 0) break;
-      if (++spins > DPM_BARRIER_SPIN_LIMIT) { ok = 0; atomicExch(&status[2], 1); break; }
+      if (++spins > lim) { ok = 0; atomicExch(&status[2], 1); break; }
       if (spins > 32) __nanosleep(20);
     }
     __threadfence();

@@ -227,6 +227,7 @@ struct Solver {
   double last_step_ms = 0.0, last_poisson_ms = 0.0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, evp0 = nullptr, evp1 = nullptr;
   double poisson_ms_acc = 0.0;
+  int spin_limit = 0;  // > 0: poll limit of the Krylov kernels' grid-wide waits (failure-detection tests)
 
   ~Solver() {
     if (ev0) cudaEventDestroy(ev0);
@@ -802,7 +803,8 @@ struct Solver {
     fa.delta = (float)(0.5 * (lmax - lmin));
     fcg_WA = T.WA;
     if (!fa.partials || !fa.zs) return DPM_ERR_CUDA;
-    fa.stall_window = 50;
+    fa.stall_window = P.p_stall_window > 0 ? P.p_stall_window : 50;
+    fa.stall_ratio = P.p_stall_ratio > 0.0 ? P.p_stall_ratio : 0.9;
     use_fcg = true;
     return setup_learned(T);
   }
@@ -817,6 +819,8 @@ struct Solver {
     int rc = ml.setup(nc, S.WA, S.A_col.data(), S.A_val.data(), d.Acol, d.Aval, nullsp, P.p_ml_passes, P.p_ml_degree,
                       P.p_ml_overcorrect, dev_sms, cg_bar, cg_status, cg_dout);
     if (rc) return rc;
+    if (P.p_stall_window > 0) ml.base.stall_window = P.p_stall_window;
+    if (P.p_stall_ratio > 0.0) ml.base.stall_ratio = P.p_stall_ratio;
     use_ml = true;
     return 0;
   }
@@ -996,6 +1000,7 @@ struct Solver {
     }
     CK(cudaMemsetAsync(cg_bar, 0, 2 * sizeof(unsigned), st));
     CK(cudaMemsetAsync(cg_status, 0, 4 * sizeof(int), st));
+    if (spin_limit) CK(cudaMemcpyAsync(cg_status + 3, &spin_limit, sizeof(int), cudaMemcpyHostToDevice, st));
     int wa = fcg_WA;
     void* args[] = {&a, &wa};
     CK(cudaLaunchCooperativeKernel(fcg_kernel, dim3(a.P), dim3(FCG_TPB), args, fcg_smem, st));
@@ -1007,7 +1012,7 @@ struct Solver {
     CK(cudaStreamSynchronize(st));
     if (h_st[2]) {
       std::fprintf(stderr, "dopamine_b200: FCG grid barrier timed out\n");
-      return DPM_ERR_CUDA;
+      return DPM_ERR_BARRIER_TIMEOUT;
     }
     *reason = h_st[0];
     *its = h_st[1];
@@ -1208,6 +1213,7 @@ struct Solver {
     a.rtol = rtol; a.atol = atol; a.maxit = maxit; a.nullsp = S.dir_rows.empty() ? 1 : 0; a.guess_zero = guess_zero;
     CK(cudaMemsetAsync(cg_bar, 0, 2 * sizeof(unsigned), st));
     CK(cudaMemsetAsync(cg_status, 0, 4 * sizeof(int), st));
+    if (spin_limit) CK(cudaMemcpyAsync(cg_status + 3, &spin_limit, sizeof(int), cudaMemcpyHostToDevice, st));
     void* args[] = {&a};
     CK(cudaLaunchCooperativeKernel(cg_kernel, dim3(cg_grid), dim3(PCG_TPB), args, 0, st));
     launches++;
@@ -1218,7 +1224,7 @@ struct Solver {
     CK(cudaStreamSynchronize(st));
     if (h_st[2]) {
       std::fprintf(stderr, "dopamine_b200: PCG grid barrier timed out\n");
-      return DPM_ERR_CUDA;
+      return DPM_ERR_BARRIER_TIMEOUT;
     }
     *reason = h_st[0];
     *its = h_st[1];
@@ -1804,6 +1810,13 @@ int dpm_last_timing(const dpm_solver_t* h, double* step_ms, double* poisson_ms) 
 int dpm_kernel_launches(const dpm_solver_t* h, int64_t* n) {
   if (!h || !n) return DPM_ERR_ARG;
   *n = h->s->launches;
+  return DPM_OK;
+}
+
+int dpm_set_barrier_spin_limit(dpm_solver_t* h, long long spins) {
+  if (!h || spins < 0 || spins > 0x7fffffffLL) return DPM_ERR_ARG;
+  h->s->spin_limit = (int)spins;
+  h->s->ml.spin_limit_override = (int)spins;
   return DPM_OK;
 }
 

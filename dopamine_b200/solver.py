@@ -26,12 +26,14 @@ EXPORTED = (
     "dpm_viscous_rhs_vector", "dpm_sgs_viscosity", "dpm_wall_model", "dpm_pcg_solve_noalloc",
     "dpm_advection_rhs_scalar", "dpm_viscous_rhs_scalar", "dpm_upload_scalars", "dpm_download_scalars",
     "dpm_learn_collect", "dpm_learn_train", "dpm_learn_set_gamma", "dpm_learn_sizes", "dpm_learn_export",
-    "dpm_learn_loss_grad", "dpm_multilevel_hierarchy",
+    "dpm_learn_loss_grad", "dpm_multilevel_hierarchy", "dpm_set_barrier_spin_limit",
 )
 
 
 class DopamineError(RuntimeError):
-    pass
+    def __init__(self, msg, status=None):
+        super().__init__(msg)
+        self.status = status
 
 
 def lib(build_if_missing=True):
@@ -65,6 +67,7 @@ def lib(build_if_missing=True):
     L.dpm_set_time.argtypes = [vp, C.c_double]
     L.dpm_last_timing.argtypes = [vp, dp, dp]
     L.dpm_kernel_launches.argtypes = [vp, lp]
+    L.dpm_set_barrier_spin_limit.argtypes = [vp, C.c_longlong]
     L.dpm_ls_gradient_vector.argtypes = [vp, dp, dp, dp]
     L.dpm_advection_rhs_vector.argtypes = [vp, C.c_int, dp, dp, dp, dp, dp]
     L.dpm_viscous_rhs_vector.argtypes = [vp, dp, C.c_double, dp, dp, dp, dp]
@@ -101,7 +104,7 @@ def _p(a):
 
 def _check(rc, what):
     if rc != 0:
-        raise DopamineError(f"{what} failed with status {rc}")
+        raise DopamineError(f"{what} failed with status {rc}", rc)
 
 
 class Solver:
@@ -195,6 +198,10 @@ class Solver:
         n = C.c_int64()
         lib().dpm_kernel_launches(self.h, C.byref(n))
         return n.value
+
+    def set_barrier_spin_limit(self, spins):
+        """Poll limit of the Krylov kernels' grid-wide waits (0: the default, about a second)."""
+        _check(lib().dpm_set_barrier_spin_limit(self.h, int(spins)), "dpm_set_barrier_spin_limit")
 
     @property
     def time(self):

@@ -5,9 +5,11 @@
  *
  *  1. fvm_petsc_*  — the pressure-solve seam the reference already has.  Same symbol names,
  *     argument order and meaning as src/solver/pressure_backend_petsc.c (declared for Fortran in
- *     src/solver/mod_pressure_solver.f90:23-74), implemented here with a device-resident
- *     Jacobi-preconditioned conjugate gradient instead of PETSc/hypre.  A Fortran host that links
- *     this library instead of pressure_backend_petsc.c needs no source change.
+ *     src/solver/mod_pressure_solver.f90:23-74), implemented here with device-resident Krylov
+ *     solves instead of PETSc/hypre: Jacobi-preconditioned conjugate gradients ("jacobi") or
+ *     flexible CG preconditioned by an aggregation-multigrid V-cycle ("boomeramg" / "gamg", the
+ *     reference's default selection).  A Fortran host that links this library instead of
+ *     pressure_backend_petsc.c needs no source change.
  *
  *  2. dpm_*        — the explicit part of the time step plus the whole-step driver, mirroring the
  *     FVSolver interface (src/solver/mod_fv_solver.f90:270-285: init, advance, project_once,
@@ -40,6 +42,9 @@ extern "C" {
 #define DPM_ERR_NOT_FINITE (-4)
 #define DPM_ERR_DT_COLLAPSE (-5)
 #define DPM_ERR_UNSUPPORTED (-6)
+#define DPM_ERR_BARRIER_TIMEOUT (-7)  /* a grid-wide wait of a Krylov kernel ran out (see
+                                         dpm_set_barrier_spin_limit); the kernel returned and
+                                         the handle stays usable                               */
 /* Krylov failure after the fallback retry: -(1000 + reason), reason < 0 as in PETSc. */
 
 /* Advection schemes (src/mod_parameters.f90:54-60). */
@@ -107,7 +112,10 @@ typedef struct dpm_params {
   double dt;                  /* requested time step (clamped to the CFL limit)              */
   double cfl_max;
   double p_tol;               /* Poisson relative tolerance                                  */
-  int p_max_iter;
+  int p_max_iter;             /* Krylov iteration cap of one solve; the solve uses at least
+                               * 2000 (max(p_max_iter, 2000)) so that the Jacobi-PCG form is
+                               * not cut off on large meshes, and a capped solve is retried from
+                               * a zero guess with 4x the cap (pressure_backend_petsc.c:878-961) */
   int scheme;                 /* DPM_SCHEME_* for momentum                                   */
   int sgs_model;              /* DPM_SGS_*                                                   */
   int wall_model;             /* DPM_WM_*                                                    */
@@ -134,7 +142,7 @@ typedef struct dpm_params {
    * DPM_PSOLVER_JACOBI_PCG mirrors `-pc_type jacobi`; DPM_PSOLVER_TWOLEVEL_FCG is flexible CG
    * with a part-local Chebyshev smoother of degree p_smooth_degree on the interval
    * [p_smooth_lmin, p_smooth_lmax] of D^-1 A plus a one-value-per-part coarse correction.
-   * Zero / non-positive smoother settings select the defaults (6, 0.05, 2.0). */
+   * Zero / non-positive smoother settings select the defaults (7, 0.05, 2.0). */
   int p_solver;
   int p_smooth_degree;
   double p_smooth_lmin, p_smooth_lmax;
@@ -153,6 +161,11 @@ typedef struct dpm_params {
    * sweeps after the first add the eps.grad skewness correction; 0 means the reference's 2). */
   int gradient_scheme;
   int gg_iterations;
+  /* Stall guard of the flexible-CG forms: when ||r|| is above p_stall_ratio times its value
+   * p_stall_window iterations earlier, the solve is handed to plain Jacobi-PCG from its current
+   * iterate (dpm_stats_t.p_fallbacks).  Zero / non-positive: 50 iterations, ratio 0.9. */
+  int p_stall_window;
+  double p_stall_ratio;
 } dpm_params_t;
 
 /* Per-step integral statistics (src/stats/mod_stats.f90:compute_stats_sums and
@@ -185,8 +198,10 @@ int fvm_petsc_backend_available(void);
 int fvm_petsc_backend_initialize(void);
 /* src/solver/mod_pressure_solver.f90:33 — releases the cached operator and device memory. */
 int fvm_petsc_backend_finalize(void);
-/* src/solver/mod_pressure_solver.f90:37 — "boomeramg" / "gamg" are accepted and mapped to the
- * Jacobi PCG; "jacobi" / "pcg" select it explicitly. */
+/* src/solver/mod_pressure_solver.f90:37 — "boomeramg" / "gamg" select flexible CG with this
+ * library's FP32 aggregation-multigrid V-cycle (an algebraic multigrid, as hypre's BoomerAMG is
+ * in the reference); "jacobi" selects the Jacobi PCG, which is also what runs before any
+ * selection. */
 void fvm_petsc_set_pressure_solver(const char* solver_name);
 /* src/solver/mod_pressure_solver.f90:42 — 1: rhs/solution may be device pointers. */
 int fvm_petsc_device_io_supported(void);
@@ -200,7 +215,11 @@ void fvm_petsc_set_device_local_rank(int local_rank);
 /* src/solver/pressure_backend_petsc.c:648-668 (Fortran interface mod_pressure_solver.f90:60-73).
  * Solves A x = rhs, A = diag - sum_f coeff_f (off-diagonal), with conjugate gradients on the
  * unpreconditioned residual norm, ||r|| <= max(rtol ||b||, atol), nonzero initial guess
- * (solution on entry), constant null space when no Dirichlet rows exist.  Indices 1-based. */
+ * (solution on entry), constant null space when no Dirichlet rows exist.  Indices 1-based.
+ * As in the reference: non-finite entries of rhs and of the initial guess are zeroed; a failed
+ * solve is retried from a zero guess with Jacobi PCG and 4x the cap, and a DIVERGED_ITS retry
+ * whose residual is below 1e4 rtol or 1e3 atol is accepted; otherwise -(1000 + reason).  The cap
+ * is max(max_iterations, 2000) unless "-ksp_max_it N" was inserted, which sets it to N. */
 int fvm_petsc_solve_pressure(int n_cells_local, int n_cells_global, int n_faces,
                              const int* local_to_global, const int* face_owner,
                              const int* face_neighbor_local, const int* face_neighbor_global,
@@ -236,7 +255,7 @@ int dpm_project_once(dpm_solver_t* s, double dt);
 /* solver_advance (mod_fv_solver.f90:920-958): CFL clamp of a fixed dt, RK3W, time += dt.
  * Status DPM_ERR_DT_COLLAPSE mirrors solver_compute_dt's stop. */
 int dpm_advance(dpm_solver_t* s, double dt);
-/* n steps in one call, captured as a CUDA graph after the first; stats of the last step. */
+/* n steps in one call (dpm_advance n times); stats of the last step. */
 int dpm_advance_n(dpm_solver_t* s, double dt, int n_steps);
 int dpm_stats(dpm_solver_t* s, dpm_stats_t* out);
 /* solver_state_is_finite (mod_fv_solver.f90:3925-3945): *ok = 1 when U and p are finite. */
@@ -249,6 +268,12 @@ int dpm_set_time(dpm_solver_t* s, double time);
 int dpm_last_timing(const dpm_solver_t* s, double* step_ms, double* poisson_ms);
 /* Kernel launch count since the handle was created (own kernels only). */
 int dpm_kernel_launches(const dpm_solver_t* s, int64_t* n);
+/* Failure-detection hook: every grid-wide wait of this handle's Krylov kernels gives up after
+ * `spins` polls of its arrival counter (0 restores the default, 2^26 polls, about a second).  A
+ * wait that runs out sets the kernel's status word, every block returns, and the call that
+ * launched it returns DPM_ERR_BARRIER_TIMEOUT; the handle stays usable.  Tests use a tiny value
+ * to exercise that path without hanging or faulting the GPU. */
+int dpm_set_barrier_spin_limit(dpm_solver_t* s, long long spins);
 
 /* ---------------------------------------------------------------------------------------- */
 /* 3. Per-operator entry points: same arguments as the Fortran subroutines, operating on the */
@@ -319,13 +344,22 @@ int dpm_multilevel_hierarchy(int n, int width, const int* col, const double* val
  * pointers owned by the caller: the operator in padded ELL form [row_width][n_cells] (col, val;
  * padding entries are (own row, 0.0)), the inverse diagonal, the right-hand side and the
  * solution x (used as the initial guess, overwritten).  Work vectors live in a fixed
- * file-scope device array of DPM_NOALLOC_MAX_CELLS cells (about 5.3 MB, held by every GPU that
- * loads the library until exit); larger systems or rows wider than 16 return DPM_ERR_ARG.
- * Same stopping rule as fvm_petsc_solve_pressure (unpreconditioned norm, PETSc KSPCG test);
- * null_space != 0 projects the constant mode out of the right-hand side.  The first call on a
- * device looks up the array's address and must come before any stream capture.  Every call
- * shares the array: calls that overlap on the GPU race and must be serialized by the caller.
- * Blocks until the solve on `stream` (a cudaStream_t, NULL = legacy default) has finished. */
+ * file-scope device array of DPM_NOALLOC_MAX_CELLS cells (about 5.3 MB); larger systems or rows
+ * wider than 16 return DPM_ERR_ARG.
+ * First call per device: the CUDA runtime loads the library's device module lazily, so the
+ * array and the solve kernels are created on a device by the first call there (which can fail
+ * with DPM_ERR_CUDA if the device has no free memory) and are then held until the process
+ * exits.  A call with max_iterations == 0 (sizes in range, array pointers may be NULL) does only
+ * that set-up and returns 0: make it once per device before the host's pool reserves the
+ * device's memory, and before any stream capture.
+ * Stopping rule: the PETSc KSPCG test of fvm_petsc_solve_pressure (unpreconditioned norm,
+ * ||r|| <= max(rtol ||b||, atol)); null_space != 0 projects the constant mode out of the
+ * right-hand side.  Unlike fvm_petsc_solve_pressure there is no retry from a zero guess, no
+ * 2000-iteration floor on max_iterations and no zeroing of non-finite entries: a solve that
+ * reaches max_iterations returns -(1000 + KSP_DIVERGED_ITS) = -997.
+ * Every call shares the array: calls that overlap on the GPU race and must be serialized by the
+ * caller.  Blocks until the solve on `stream` (a cudaStream_t, NULL = legacy default) has
+ * finished. */
 #define DPM_NOALLOC_MAX_CELLS 131072
 int dpm_pcg_solve_noalloc(int n_cells, int row_width, const int* col, const double* val,
                           const double* inv_diag, const double* rhs, double* x, double rtol, double atol,

@@ -1,0 +1,143 @@
+"""GPU parity at the benchmark configurations' own sizes and forms.
+
+* Taylor-Green 32^3, CDS, plain FP64 Jacobi-PCG at the configuration's p_tol (1e-10), the full
+  200 steps against the FP64 oracle: velocity within 1e-10 relative L2 and the post-projection
+  face-flux divergence below 1e-12, the plain form's gates.
+* Channel 96x64x64 (393 216 cells), exactly as the channel benchmark runs it: two-level flexible
+  CG, learned term recorded over 3 steps, trained (80 Adam steps) and gated on the held-out solve,
+  then 3 more steps; the oracle takes the same 6 steps.  Chosen-form gates: field error <= 1e-5,
+  divergence <= 1e-8.
+* The precision form (FP32-operator inner iterations inside FP64 defect correction) over 20 steps
+  of a 48x32x32 channel against the FP64 oracle, each field's error printed and gated at 1e-5.
+* Urban canopy at full size (19.3 M cells), the form the urban benchmark times (multilevel
+  flexible CG with the learned term trained and gated), against the plain FP64 Jacobi-PCG GPU
+  path on the same steps: at this size the oracle is too slow for a test, so the comparison is
+  with the plain path, which the other tests pin to the oracle.  Fields U, p, T and the scalar to
+  1e-5, divergence to 1e-8.
+"""
+import numpy as np
+import pytest
+
+from dopamine_b200 import abi, cases
+from dopamine_b200.solver import Solver
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+CHOSEN_FIELD_TOL = 1e-5
+CHOSEN_DIV_TOL = 1e-8
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-3 * np.sqrt(b.size)))
+
+
+def _rel_p(a, b):
+    """Pressure is defined up to a constant on the periodic/walled boxes: compare mean-free."""
+    a = a - a.mean()
+    b = b - b.mean()
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def test_taylor_green_32_plain_fp64_200_steps():
+    case = cases.tgv_config(n=32, n_steps=200)
+    o = O.Oracle(case)
+    s = Solver(case)
+    assert s.params.p_tol == 1e-10 and s.params.p_solver == abi.PSOLVER_JACOBI_PCG
+    o.initialise()
+    s.initialise()
+    worst = 0.0
+    for k in range(200):
+        o.advance()
+        s.advance()
+        if (k + 1) % 20 == 0:
+            e = _rel(s.sync_host()["U"], o.state()["U"])
+            worst = max(worst, e)
+            assert e <= 1e-10, (k + 1, e)
+    st = s.stats()
+    print(f"C1 TGV 32^3 200 steps: worst U rel L2 {worst:.2e}, divU {st['max_abs_divU']:.2e}, E {st['E']:.9e}")
+    assert st["max_abs_divU"] <= 1e-12
+    assert abs(st["E"] - o.stats()["E"]) <= 1e-10 * o.stats()["E"]
+
+
+def test_channel_96x64x64_timed_form_against_oracle():
+    case = cases.channel_config(96, 64, 64)
+    pg = case.make_params()
+    pg.p_solver = abi.PSOLVER_TWOLEVEL_FCG
+    s = Solver(case, params=pg)
+    o = O.Oracle(case)
+    s.initialise()
+    o.initialise()
+    s.learn_collect(3)
+    rep = s.learn_train(epochs=80, lr=1e-2)
+    for _ in range(3):
+        o.advance()
+    for _ in range(3):
+        o.advance()
+        s.advance()
+    so, sg = o.state(), s.sync_host()
+    eu, ep = _rel(sg["U"], so["U"]), _rel_p(sg["p"], so["p"])
+    st = s.stats()
+    print(f"C2 channel timed form (gamma {rep['gamma']}): U rel {eu:.2e}, p rel {ep:.2e}, "
+          f"divU {st['max_abs_divU']:.2e}, oracle divU {o.stats()['max_abs_divU']:.2e}")
+    assert st["p_solver_used"] == abi.PSOLVER_TWOLEVEL_FCG
+    assert eu <= CHOSEN_FIELD_TOL and ep <= CHOSEN_FIELD_TOL
+    assert st["max_abs_divU"] <= CHOSEN_DIV_TOL
+
+
+def test_precision_form_20_steps_field_errors():
+    case = cases.channel_config(48, 32, 32, n_steps=20)
+    pg = case.make_params()
+    pg.p_solver = abi.PSOLVER_TWOLEVEL_FCG
+    pg.form = abi.FORM_MIXED
+    o = O.Oracle(case)
+    s = Solver(case, params=pg)
+    o.initialise()
+    s.initialise()
+    for k in range(20):
+        o.advance()
+        s.advance()
+    so, sg = o.state(), s.sync_host()
+    errs = {"U": _rel(sg["U"], so["U"]), "p": _rel_p(sg["p"], so["p"]),
+            "nu_sgs": _rel(sg["nu_sgs"], so["nu_sgs"])}
+    st = s.stats()
+    print("precision form, channel 48x32x32, 20 steps: " + ", ".join(f"{k} {v:.2e}" for k, v in errs.items())
+          + f", divU {st['max_abs_divU']:.2e}")
+    for k, v in errs.items():
+        assert v <= CHOSEN_FIELD_TOL, (k, v)
+    assert st["max_abs_divU"] <= CHOSEN_DIV_TOL
+
+
+def test_urban_full_size_chosen_form_against_plain_fp64():
+    case = cases.urban_config()
+    pc = case.make_params()
+    pc.p_solver = abi.PSOLVER_AUTO
+    chosen = Solver(case, params=pc)
+    chosen.initialise()
+    assert chosen.stats()["p_solver_used"] == abi.PSOLVER_MULTILEVEL_FCG
+    chosen.learn_collect(3)
+    rep = chosen.learn_train(epochs=80, lr=1e-2)
+    for _ in range(2):
+        chosen.advance()
+    sc = chosen.sync_host()
+    Tc, Cc = chosen.scalars()
+    stc = chosen.stats()
+    chosen.close()
+    pp = case.make_params()
+    pp.p_solver = abi.PSOLVER_JACOBI_PCG
+    plain = Solver(case, params=pp)
+    plain.initialise()
+    for _ in range(5):
+        plain.advance()
+    sp = plain.sync_host()
+    Tp, Cp = plain.scalars()
+    stp = plain.stats()
+    plain.close()
+    errs = {"U": _rel(sc["U"], sp["U"]), "p": _rel_p(sc["p"], sp["p"]), "T": _rel(Tc - 300.0, Tp - 300.0),
+            "C": _rel(Cc, Cp)}
+    print(f"urban 19.3M, multilevel + learned (gamma {rep['gamma']}) vs plain FP64, 5 steps: "
+          + ", ".join(f"{k} {v:.2e}" for k, v in errs.items())
+          + f", divU {stc['max_abs_divU']:.2e} (plain {stp['max_abs_divU']:.2e})")
+    for k, v in errs.items():
+        assert v <= CHOSEN_FIELD_TOL, (k, v)
+    assert stc["max_abs_divU"] <= CHOSEN_DIV_TOL

@@ -3,8 +3,11 @@ drop-in solve fvm_petsc_solve_pressure on the same singular (pure-Neumann) press
 
 Both run the same persistent PCG kernel, so the solutions must agree to the parity tolerance
 used for the other device operators (relative 1e-12), over two calls in a row: the second call
-starts from a non-zero guess and reuses the scratch array the first call left behind.  The file
-is named so that pytest collects it last; it also passes when run alone."""
+starts from a non-zero guess and reuses the scratch array the first call left behind.  Before
+them, a call with max_iterations = 0 does the per-device set-up a caller without allocation
+rights makes up front (module load, kernels, the static array's address); around the second
+solve the device's free memory must not change, which is the point of the entry point.  The
+file is named so that pytest collects it last; it also passes when run alone."""
 import ctypes as C
 
 import numpy as np
@@ -109,6 +112,11 @@ def test_noalloc_matches_allocating_solve_on_two_calls():
     d_val = torch.from_numpy(val.ravel().copy()).to(dev)
     d_dinv = torch.from_numpy(dinv).to(dev)
     rtol, atol, maxit = 1e-10, 1e-50, 2000
+    # per-device set-up call: no array argument is read
+    its0, res0 = C.c_int(-1), C.c_double(-1.0)
+    rc = L.dpm_pcg_solve_noalloc(n, width, None, None, None, None, None, rtol, atol, 0, 1, None, C.byref(its0),
+                                 C.byref(res0))
+    assert rc == 0 and its0.value == 0 and res0.value == 0.0
     rng = np.random.default_rng(5)
     guesses = [np.zeros(n), rng.standard_normal(n)]
     for call in range(2):
@@ -117,11 +125,15 @@ def test_noalloc_matches_allocating_solve_on_two_calls():
         d_rhs = torch.from_numpy(rhs).to(dev)
         d_x = torch.from_numpy(guesses[call].copy()).to(dev)
         torch.cuda.synchronize()
+        free_before = torch.cuda.mem_get_info(dev)[0]
         its, res = C.c_int(0), C.c_double(0.0)
         rc = L.dpm_pcg_solve_noalloc(n, width, d_col.data_ptr(), d_val.data_ptr(), d_dinv.data_ptr(),
                                      d_rhs.data_ptr(), d_x.data_ptr(), rtol, atol, maxit, 1,
                                      torch.cuda.current_stream().cuda_stream, C.byref(its), C.byref(res))
         assert rc == 0, (call, rc)
+        torch.cuda.synchronize()
+        if call == 1:  # set-up done long before: the solve itself takes no device memory
+            assert torch.cuda.mem_get_info(dev)[0] == free_before
         x = d_x.cpu().numpy()
         err = np.linalg.norm(x - x_ref) / np.linalg.norm(x_ref)
         assert err <= RTOL_PARITY, (call, err)
