@@ -1,26 +1,26 @@
 #!/usr/bin/env python3
 """Benchmark of the RK3W fractional-step hot path on B200.
 
-Default workload: the turbulent-channel configuration (96 x 64 x 64 hex cells, tanh-stretched,
-KEP advection, Vreman SGS, log-law wall model, constant pressure-gradient forcing), synthetic
-inputs (seeded laminar-plus-noise initial state).  One "step" is one RK3W time step (three
-stages, three Poisson solves) of the whole mesh.  The timed form is the chosen pressure solve
-(flexible CG with the two-level preconditioner on this mesh, the multilevel one on meshes too
-large for it; both with the learned term trained and gated); on one GPU the plain FP64
-Jacobi-PCG form is timed beside it on the same workload and reported in the config.
+Default workload: the urban-canopy configuration named by the metric ("learned+mixed vs plain
+FP64 PCG"): a 1000 x 1000 x 300 m box at 400 x 400 x 125 hexes with 200 seeded cuboid obstacles
+carved out (19.3 M cells), MOST wall model (L = -100 m), AMD SGS, KEP momentum, temperature plus
+one passive scalar (van Leer), synthetic inputs (seeded uniform flow with +-10 % noise).  One
+"step" is one RK3W time step (three stages, three Poisson solves) of the whole mesh.  The timed
+form is the chosen pressure solve (flexible CG with the two-level preconditioner when the mesh
+fits it, else with the FP32 aggregation-multigrid V-cycle; the learned term trained on 3
+recorded steps and gated on a held-out solve); on one GPU the plain FP64 Jacobi-PCG form is timed
+beside it on the same handle, mesh and state and reported in the config.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                    [--config channel|channel3m|tgv|rb|mixed|urban] [--psolver auto|fcg|pcg|ml] [--no-plain]
-
-(--psolver auto, the default, takes the two-level form when the mesh fits it — up to 4096 cells
-per SM — and the multilevel form otherwise, as for the rb, mixed and urban configurations)
+                    [--config urban|channel|channel3m|tgv|rb|mixed] [--psolver auto|fcg|pcg|ml] [--no-plain]
 
 value   : cell-steps/s with the state resident in HBM (CUDA events around K steps, max over ranks)
-e2e     : the same metric through the C ABI with host buffers: every step uploads the state
-          (U, p) from pinned host memory, advances, and reads the state back
+e2e     : the same metric through the C ABI with host buffers: every step uploads the transported
+          state (U, p, and T and the scalars when present) from pinned host memory, advances, and
+          reads it back
 roofline: the Poisson kernel (dominant): algorithmic bytes per launch / average launch time
 cpu_baseline: the CPU restatement of the reference step (oracle) on this host's cores, on a
-          bounded sample of the same workload.
+          bounded sample of the same workload (the sample is stated in the line).
 Multi-GPU: the north-star path is single-GPU; N GPUs run N independent replicas (weak scaling).
 """
 import argparse
@@ -113,6 +113,31 @@ KERNELS = {"pcg": "k_pcg (persistent Jacobi-PCG)", "fcg": "k_fcg (persistent two
            "ml": "k_mlcg (persistent multilevel flexible CG)"}
 
 
+CONFIG_NAMES = {
+    "urban": "urban canopy 1000x1000x300 m, 400x400x125 hexes with 200 seeded obstacles carved out (19.3M cells), "
+             "MOST (L = -100 m), AMD, KEP, T + 1 scalar van Leer",
+    "urban2m": "urban canopy 1000x1000x300 m at half resolution, 200x200x63 hexes with the same 200 obstacles "
+               "(2.4M cells), MOST (L = -100 m), AMD, KEP, T + 1 scalar van Leer",
+    "channel": "channel 96x64x64 Re_tau=395, KEP, Vreman, log-law wall model",
+    "tgv": "Taylor-Green 64^3, CDS",
+    "channel3m": "channel 192x128x128 (3.1M cells) Re_tau=395, KEP, Vreman, log-law wall model",
+    "rb": "Rayleigh-Benard 256x256x128 (8.4M cells), Ra=1e7, Pr=0.7, T + 2 scalars van Leer, Vreman",
+    "mixed": "jittered unit box 128^3 as hexes + prisms + pyramids (4.9M cells), AMD, Koren TVD",
+}
+
+# What stays in the 126 MB L2 and what streams from HBM, per workload (said in the line's config)
+L2_NOTE = {
+    "urban": "inputs larger than L2: the fine-level operator and vectors alone are ~1.5 GB; no flush needed",
+    "urban2m": "inputs larger than L2: the fine-level operator and vectors alone are ~0.2 GB; no flush needed",
+    "rb": "inputs larger than L2: the fine-level operator and vectors alone are ~0.7 GB; no flush needed",
+    "mixed": "inputs larger than L2: the fine-level operator and vectors alone are ~0.5 GB; no flush needed",
+    "channel3m": "inputs larger than L2: the fine-level operator and vectors alone are ~0.3 GB; no flush needed",
+    "channel": "step data larger than L2 (LS weights alone 245 MB, streamed each gradient pass); the Poisson "
+               "working set (operator 33 MB + vectors) is L2-resident, as the channel profiles show",
+    "tgv": "step data larger than L2 (LS weights 1.6 GB); the Poisson working set is partly L2-resident",
+}
+
+
 def make_case(name):
     from dopamine_b200 import cases
     if name == "channel":
@@ -127,7 +152,80 @@ def make_case(name):
         return cases.hybrid_config(n=128, kind="mixed")
     if name == "urban":
         return cases.urban_config()
+    if name == "urban2m":
+        return cases.urban_config(200, 200, 63)
     raise ValueError(name)
+
+
+def cpu_sample_case(name):
+    """The bounded CPU sample of a workload: the workload itself when the oracle steps it in
+    seconds, else the same generator at reduced resolution.  Jacobi-PCG iterations per solve grow
+    with the mesh's linear size, so a reduced mesh's CPU rate is an upper bound on the CPU's rate
+    at full size (the GPU/CPU ratio is understated, not inflated)."""
+    from dopamine_b200 import cases
+    if name == "urban":
+        return (cases.urban_config(100, 100, 32),
+                "the urban generator at 1/4 linear resolution (100x100x32 hexes, same 1000x1000x300 m domain, "
+                "the same 200 obstacles, 0.31M cells); Jacobi-PCG there needs ~1/3 of the full mesh's iterations "
+                "per cell, so this rate is an upper bound on the CPU's full-size rate")
+    if name == "urban2m":
+        return (cases.urban_config(100, 100, 32),
+                "the urban generator at 1/4 of the full linear resolution (100x100x32, 0.31M cells)")
+    if name == "rb":
+        return (cases.rb_config(64, 64, 32), "the Rayleigh-Benard generator at 1/4 linear resolution (64x64x32)")
+    if name == "mixed":
+        return (cases.hybrid_config(n=32, kind="mixed"), "the mixed-element generator at 1/4 linear resolution (n=32)")
+    if name == "channel3m":
+        return (cases.channel_config(96, 64, 64), "the channel generator at 1/2 linear resolution (96x64x64)")
+    return make_case(name), f"the {name} workload itself"
+
+
+def host_cores():
+    """(threads this process may use, physical cores of the host)."""
+    try:
+        threads = len(os.sched_getaffinity(0))
+    except AttributeError:
+        threads = os.cpu_count() or 1
+    phys = set()
+    try:
+        pid = cid = None
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("physical id"):
+                pid = line.split(":")[1].strip()
+            elif line.startswith("core id"):
+                cid = line.split(":")[1].strip()
+            elif not line.strip():
+                if cid is not None:
+                    phys.add((pid, cid))
+                pid = cid = None
+        if cid is not None:
+            phys.add((pid, cid))
+    except OSError:
+        pass
+    return threads, (len(phys) if phys else None)
+
+
+def cpu_run(case_name, budget_s, max_steps):
+    """The oracle (CPU restatement of the reference step) on this host's cores: time whole steps
+    of the bounded sample after its initial projection until `budget_s` or `max_steps`."""
+    from oracle.oracle import Oracle
+    threads, phys = host_cores()
+    case, what = cpu_sample_case(case_name)
+    o = Oracle(case, nthreads=threads)
+    o.initialise()
+    t0 = time.perf_counter()
+    steps = 0
+    while steps < max(1, max_steps):
+        o.advance()
+        steps += 1
+        if time.perf_counter() - t0 >= budget_s:
+            break
+    dt = time.perf_counter() - t0
+    return dict(value=o.nc * steps / dt, unit="cell-steps/s", cores=threads, physical_cores=phys, kind="port",
+                steps=steps,
+                sample=f"{steps} RK3W step(s) of {what} after the initial projection, {dt:.1f} s, oracle (CPU "
+                       f"restatement of the reference step, plain FP64 Jacobi-PCG) with {threads} OpenMP threads "
+                       f"on {phys if phys else 'an unknown number of'} physical cores")
 
 
 def pcg_bytes_per_iteration(s, psolver="pcg"):
@@ -150,15 +248,24 @@ def pcg_bytes_per_iteration(s, psolver="pcg"):
     return phase_a + phase_b
 
 
-def pcg_traffic_per_launch(psolver="pcg"):
+PROFILE = {("pcg", "channel"): "k_pcg_channel96x64x64.md", ("fcg", "channel"): "k_fcg_channel96x64x64.md",
+           ("ml", "channel"): "k_mlcg_channel96x64x64.md", ("ml", "urban"): "k_mlcg_urban.md"}
+
+
+def pcg_traffic_per_launch(psolver, config, nc, its_per_solve):
     """DRAM bytes (read + write) of one launch of the Poisson kernel on this workload, from the
-    committed ncu summary (one capture, its command inside the file); None when absent."""
-    name = {"fcg": "k_fcg_channel96x64x64.md", "ml": "k_mlcg_channel96x64x64.md"}.get(psolver, "k_pcg_channel96x64x64.md")
-    path = os.path.join(ROOT, "profiles", name)
+    committed ncu summary: either a capture of this workload (traffic_bytes_per_launch) or of a
+    smaller mesh of the same generator, scaled by cells x iterations
+    (traffic_bytes_per_cell_iteration); None when no summary exists."""
+    name = PROFILE.get((psolver, config))
+    if not name:
+        return None
     try:
-        for line in open(path):
+        for line in open(os.path.join(ROOT, "profiles", name)):
             if line.startswith("traffic_bytes_per_launch:"):
                 return int(line.split(":")[1])
+            if line.startswith("traffic_bytes_per_cell_iteration:"):
+                return int(float(line.split(":")[1]) * nc * its_per_solve)
     except OSError:
         pass
     return None
@@ -180,6 +287,7 @@ def whole_job_rate(world, cells, steps, seconds):
 
 def run_gpu(args, rank, world):
     import torch
+    from dopamine_b200 import abi
     from dopamine_b200.solver import Solver, lib
 
     dev = int(os.environ.get("LOCAL_RANK", "0"))
@@ -226,71 +334,62 @@ def run_gpu(args, rank, world):
         solves += st["p_solves"]
     launches = s.kernel_launches() - l0
     t_dev = sum(step_ms) / 1e3
-    # ---- end to end through the C ABI with host buffers
+    # ---- end to end through the C ABI with host buffers: the transported state (U, p, T when it
+    # is transported, the passive scalars) goes up from pinned host memory and comes back every step
     L = lib()
     host = s.sync_host()
-    # pinned host buffers (page-locked through torch), filled with the current state
-    U_pin = torch.empty(host["U"].shape, dtype=torch.float64, pin_memory=True)
-    p_pin = torch.empty(host["p"].shape, dtype=torch.float64, pin_memory=True)
-    U = U_pin.numpy()
-    p = p_pin.numpy()
+    with_T = bool(s.params.boussinesq)
+    ns = max(0, min(int(s.params.n_scalars), 4))
+
+    def pinned(shape):
+        return torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy()
+
+    U, p = pinned(host["U"].shape), pinned(host["p"].shape)
     U[...] = host["U"]
     p[...] = host["p"]
-    dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+    T = pinned(host["T"].shape) if with_T else None
+    if with_T:
+        T[...] = host["T"]
+    Cs = pinned((nc, ns)) if ns else None
+    if ns:
+        Cs[...] = s.scalars()[1].T
+    dp = lambda a: None if a is None else a.ctypes.data_as(C.POINTER(C.c_double))
+    bytes_per_dir = 8 * nc * (3 + 1 + (1 if with_T else 0) + ns)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        rc = L.dpm_upload_state(s.h, dp(U), dp(p), None)
+        rc = L.dpm_upload_state(s.h, dp(U), dp(p), dp(T))
+        if ns:
+            rc |= L.dpm_upload_scalars(s.h, dp(Cs))
         rc |= L.dpm_advance(s.h, s.params.dt)
-        rc |= L.dpm_download_state(s.h, dp(U), dp(p), None, None)
+        rc |= L.dpm_download_state(s.h, dp(U), dp(p), dp(T), None)
+        if ns:
+            rc |= L.dpm_download_scalars(s.h, dp(Cs))
         if rc:
             raise RuntimeError(f"e2e step failed {rc}")
     t_e2e = time.perf_counter() - t0
     clocks = sampler.stop() if sampler else None
     if world > 1:
         t_dev, t_e2e = max_over_ranks([t_dev, t_e2e], "cuda")
-    return dict(nc=nc, t_dev=t_dev, t_e2e=t_e2e, step_ms=step_ms, pois_ms=pois_ms, its=its, solves=solves,
-                launches=launches, clocks=clocks, solver=s, learn=learn, fallbacks=s.stats()["p_fallbacks"])
-
-
-def time_plain(args, dev, steps=3):
-    """The plain FP64 Jacobi-PCG form on the same workload: device ms per step and Poisson ms
-    per step (CUDA events inside the library), after one warm-up step."""
-    from dopamine_b200.solver import Solver
-    case = make_case(args.config)
-    case.params["p_solver"] = 0
-    s = Solver(case, device=dev)
-    s.initialise()
-    s.advance()
-    step_ms, pois_ms, its = [], [], 0
-    for _ in range(steps):
+    plain = None
+    if args.psolver != "pcg" and not args.no_plain and world == 1:
+        # the plain FP64 Jacobi-PCG form on the same handle, mesh and state: one warm-up step, then
+        # `plain_steps` steps timed by the library's CUDA events
+        s.select_pressure_solver(abi.PSOLVER_JACOBI_PCG)
         s.advance()
-        a, b = s.last_timing()
-        step_ms.append(a)
-        pois_ms.append(b)
-        its += s.stats()["p_iters"]
-    s.close()
-    return sum(step_ms) / steps, sum(pois_ms) / steps, its / steps
-
-
-def cpu_baseline(case_name, budget_s=20.0, nthreads=None):
-    """The oracle (CPU restatement of the reference step) on this host, bounded sample."""
-    from oracle.oracle import Oracle
-    nthreads = nthreads or os.cpu_count() or 1
-    case = make_case(case_name)
-    o = Oracle(case, nthreads=nthreads)
-    o.initialise()
-    t0 = time.perf_counter()
-    steps = 0
-    while True:
-        o.advance()
-        steps += 1
-        if time.perf_counter() - t0 >= budget_s or steps >= 3:
-            break
-    dt = time.perf_counter() - t0
-    return dict(value=o.nc * steps / dt, unit="cell-steps/s", cores=nthreads, kind="port",
-                sample=f"{steps} RK3W step(s) of the {case_name} workload ({o.nc} cells) after the initial projection, "
-                       f"{dt:.1f} s, oracle with {nthreads} OpenMP threads")
+        pm, pp, pit = [], [], 0
+        for _ in range(args.plain_steps):
+            s.advance()
+            a, b = s.last_timing()
+            pm.append(a)
+            pp.append(b)
+            pit += s.stats()["p_iters"]
+        plain = dict(ms_per_step=sum(pm) / len(pm), poisson_ms_per_step=sum(pp) / len(pp),
+                     pcg_iterations_per_step=pit / len(pm), steps=len(pm))
+        s.select_pressure_solver(3)
+    return dict(nc=nc, t_dev=t_dev, t_e2e=t_e2e, step_ms=step_ms, pois_ms=pois_ms, its=its, solves=solves,
+                launches=launches, clocks=clocks, solver=s, learn=learn, fallbacks=s.stats()["p_fallbacks"],
+                e2e_bytes=bytes_per_dir, plain=plain)
 
 
 def main():
@@ -299,9 +398,10 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="dopamine_b200")
-    ap.add_argument("--config", default="channel", choices=["channel", "channel3m", "tgv", "rb", "mixed", "urban"])
+    ap.add_argument("--config", default="urban", choices=list(CONFIG_NAMES))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip timing the plain FP64 Jacobi-PCG form")
+    ap.add_argument("--plain-steps", type=int, default=3, help="timed steps of the plain FP64 form")
     ap.add_argument("--no-learned", action="store_true", help="flexible CG without the learned term")
     ap.add_argument("--mixed", action="store_true",
                     help="precision form: FP32-operator inner iterations inside FP64 defect correction")
@@ -313,24 +413,20 @@ def main():
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
-    cfg_name = {"channel": "channel 96x64x64 Re_tau=395, KEP, Vreman, log-law wall model",
-                "tgv": "Taylor-Green 64^3, CDS",
-                "channel3m": "channel 192x128x128 (3.1M cells) Re_tau=395, KEP, Vreman, log-law wall model",
-                "rb": "Rayleigh-Benard 256x256x128 (8.4M cells), Ra=1e7, Pr=0.7, T + 2 scalars van Leer, Vreman",
-                "mixed": "jittered unit box 128^3 as hexes + prisms + pyramids (4.9M cells), AMD, Koren TVD",
-                "urban": "urban canopy 1000x1000x300 m, 400x400x125 with 200 seeded obstacles carved out "
-                         "(19.3M cells), MOST (L = -100 m), AMD, KEP, T + 1 scalar"}[args.config]
+    cfg_name = CONFIG_NAMES[args.config]
 
     if args.impl == "reference":
         if rank != 0:
             return 0
-        cb = cpu_baseline(args.config, budget_s=60.0)
+        # each timed step is one whole RK3W step of the bounded sample; as many of the requested
+        # steps as fit in about two minutes are timed, and the line says how many
+        cb = cpu_run(args.config, budget_s=120.0, max_steps=args.steps)
         line = {
             "impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "cell-steps/s",
-            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": cfg_name, "form": "plain FP64 Jacobi-PCG (CPU restatement)"},
-            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "n_gpus": args.gpus, "steps": cb["steps"], "warmup": 0, "steps_requested": args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": cfg_name, "form": "plain FP64 Jacobi-PCG (CPU restatement of the reference step)"},
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "physical_cores", "kind", "sample")},
             "e2e": {"value": cb["value"], "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         }
         print(json.dumps(line))
@@ -356,7 +452,8 @@ def main():
     bytes_it = pcg_bytes_per_iteration(s, args.psolver)
     pois_s = sum(r["pois_ms"]) / 1e3
     achieved = bytes_it * r["its"] / pois_s / 1e9 if pois_s > 0 else 0.0
-    traffic = pcg_traffic_per_launch(args.psolver) if args.config == "channel" else None
+    its_per_solve = r["its"] / max(r["solves"], 1)
+    traffic = pcg_traffic_per_launch(args.psolver, args.config, nc, its_per_solve)
     line = {
         "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world, "steps": K,
         "warmup": args.warmup, "ms_per_step": 1e3 * r["t_dev"] / K, "higher_is_better": True, "scaling": "weak",
@@ -364,12 +461,13 @@ def main():
         "config": {"workload": cfg_name, "cells": nc, "form": FORMS[args.psolver],
                    "poisson_ms_per_step": 1e3 * pois_s / K, "pcg_iterations_per_step": r["its"] / K,
                    "poisson_solves_per_step": r["solves"] / K,
-                   "l2": "inputs larger than L2: static operator data streamed each step exceeds 126 MB",
+                   "l2": L2_NOTE.get(args.config, "inputs larger than L2"),
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
-        "e2e": {"value": e2e, "unit": "cell-steps/s", "h2d_bytes_per_step": 32 * nc, "d2h_bytes_per_step": 32 * nc},
+        "e2e": {"value": e2e, "unit": "cell-steps/s", "h2d_bytes_per_step": r["e2e_bytes"],
+                "d2h_bytes_per_step": r["e2e_bytes"]},
         "roofline": {"kernel": KERNELS[args.psolver], "bound": "hbm", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
-                     "bytes_per_iteration": bytes_it},
+                     "bytes_per_iteration": bytes_it, "iterations_per_launch": its_per_solve},
         "gpu_launches": r["launches"],
         "clocks": r["clocks"],
     }
@@ -377,17 +475,18 @@ def main():
         line["config"]["form"] += "; precision form (FP32-operator inner iterations, FP64 defect correction)"
     if r["learn"] is not None:
         line["config"]["learned_term"] = r["learn"]
-        line["config"]["form"] += "; learned one-ring term (gamma %g)" % r["learn"]["gamma"]
+        g = r["learn"]["gamma"]
+        line["config"]["form"] += ("; learned one-ring term (gamma %g)" % g if g > 0 else
+                                   "; learned one-ring term trained, gated off (gamma 0) on the held-out solve")
     if args.psolver in ("fcg", "ml"):
         line["config"]["fallbacks_to_plain_pcg"] = r["fallbacks"]
-    if args.psolver != "pcg" and not args.no_plain and world == 1:
-        pm, pp, pit = time_plain(args, int(os.environ.get("LOCAL_RANK", "0")))
-        line["config"]["plain_fp64_pcg"] = {"ms_per_step": pm, "poisson_ms_per_step": pp,
-                                            "pcg_iterations_per_step": pit,
-                                            "speedup_of_this_form": pm / line["ms_per_step"]}
+    if r["plain"] is not None:
+        pl = r["plain"]
+        pl["speedup_of_this_form"] = pl["ms_per_step"] / line["ms_per_step"]
+        line["config"]["plain_fp64_pcg"] = pl
     if not args.no_cpu_baseline and world == 1:  # the CPU baseline is reported at N = 1 only
-        cb = cpu_baseline(args.config, budget_s=20.0)
-        line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        cb = cpu_run(args.config, budget_s=20.0, max_steps=3)
+        line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "physical_cores", "kind", "sample")}
     print(json.dumps(line))
     s.close()
     if world > 1:

@@ -1175,6 +1175,17 @@ __global__ void k_soa_to_aos(int n, const double* soa, double* aos) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c < n) { aos[3 * c] = soa[c]; aos[3 * c + 1] = soa[n + c]; aos[3 * c + 2] = soa[2 * n + c]; }
 }
+// C(k, n) Fortran layout (component fastest) <-> SoA [k][n], for the passive scalars
+__global__ void k_aos_to_soa_k(int n, int k, const double* aos, double* soa) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < n)
+    for (int j = 0; j < k; ++j) soa[(size_t)j * n + c] = aos[(size_t)k * c + j];
+}
+__global__ void k_soa_to_aos_k(int n, int k, const double* soa, double* aos) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < n)
+    for (int j = 0; j < k; ++j) aos[(size_t)k * c + j] = soa[(size_t)j * n + c];
+}
 // grad(3,3,n) Fortran layout (i fastest, then j, then cell) <-> SoA [(3j+i)][n]
 __global__ void k_grad_soa_to_aos(int n, const double* soa, double* aos) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;

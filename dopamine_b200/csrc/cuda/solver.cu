@@ -228,6 +228,8 @@ struct Solver {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, evp0 = nullptr, evp1 = nullptr;
   double poisson_ms_acc = 0.0;
   int spin_limit = 0;  // > 0: poll limit of the Krylov kernels' grid-wide waits (failure-detection tests)
+  bool force_plain = false;  // dpm_select_pressure_solver: plain Jacobi-PCG although a flexible form is set up
+  bool flexible() const { return (use_fcg || use_ml) && !force_plain; }
 
   ~Solver() {
     if (ev0) cudaEventDestroy(ev0);
@@ -1134,7 +1136,7 @@ struct Solver {
     return 0;
   }
   int learn_collect(int n_steps, int* n_samples) {
-    if (!use_fcg && !use_ml) return DPM_ERR_UNSUPPORTED;
+    if (!flexible()) return DPM_ERR_UNSUPPORTED;
     int rc = use_ml ? ml_learn_setup() : 0;
     if (rc) return rc;
     rc = learn_alloc();
@@ -1149,7 +1151,7 @@ struct Solver {
     return rc;
   }
   int learn_train(int epochs, double lr, dpm_learn_report_t* rep) {
-    if ((!use_fcg && !use_ml) || lp_count == 0) return DPM_ERR_ARG;
+    if (!flexible() || lp_count == 0) return DPM_ERR_ARG;
     auto t0 = std::chrono::steady_clock::now();
     const int S = lp_train_slots();
     std::vector<double> base;
@@ -1200,8 +1202,8 @@ struct Solver {
   // ---------------------------------------------------------------- Poisson solve
   int pcg(const double* rhs, double* x, double rtol, double atol, int maxit, int guess_zero, int* its, double* resid,
           int* reason) {
-    if (use_fcg) return fcg(rhs, x, rtol, atol, maxit, guess_zero, its, resid, reason);
-    if (use_ml) return ml_launch(rhs, x, rtol, atol, maxit, guess_zero, its, resid, reason);
+    if (use_fcg && !force_plain) return fcg(rhs, x, rtol, atol, maxit, guess_zero, its, resid, reason);
+    if (use_ml && !force_plain) return ml_launch(rhs, x, rtol, atol, maxit, guess_zero, its, resid, reason);
     return pcg_plain(rhs, x, rtol, atol, maxit, guess_zero, its, resid, reason);
   }
   int pcg_plain(const double* rhs, double* x, double rtol, double atol, int maxit, int guess_zero, int* its,
@@ -1250,7 +1252,7 @@ struct Solver {
     cudaEventRecord(evp0, st);
     int rc = pcg(rhs, F.p, tol, atol, maxit, 0, &its, &res, &reason);
     if (rc) return rc;
-    if (reason < 0 && (use_fcg || use_ml)) {  // flexible CG stalled or failed: plain Jacobi-PCG takes over from its x
+    if (reason < 0 && flexible()) {  // flexible CG stalled or failed: plain Jacobi-PCG takes over from its x
       p_fallbacks++;
       int its2 = 0;
       rc = pcg_plain(rhs, F.p, tol, atol, maxit, 0, &its2, &res, &reason);
@@ -1508,7 +1510,9 @@ struct Solver {
     s->volavg_abs_divU = o2[1] / o2[2];
     s->dt_used = last.dt_used;
     s->p_fallbacks = p_fallbacks;
-    s->p_solver_used = use_fcg ? DPM_PSOLVER_TWOLEVEL_FCG : (use_ml ? DPM_PSOLVER_MULTILEVEL_FCG : DPM_PSOLVER_JACOBI_PCG);
+    s->p_solver_used = force_plain ? DPM_PSOLVER_JACOBI_PCG
+                                   : (use_fcg ? DPM_PSOLVER_TWOLEVEL_FCG
+                                              : (use_ml ? DPM_PSOLVER_MULTILEVEL_FCG : DPM_PSOLVER_JACOBI_PCG));
     s->p_solves = last.p_solves;
     s->p_iters = last.p_iters;
     s->p_resid_max = last.p_resid_max;
@@ -1696,10 +1700,13 @@ int dpm_upload_scalars(dpm_solver_t* h, const double* C) {
   Solver& s = *h->s;
   if (s.ns == 0) return DPM_OK;
   CK(cudaSetDevice(s.device));
-  std::vector<double> soa((size_t)s.ns * s.nc);
-  for (int c = 0; c < s.nc; ++c)
-    for (int k = 0; k < s.ns; ++k) soa[(size_t)k * s.nc + c] = C[(size_t)c * s.ns + k];
-  CK(cudaMemcpyAsync(s.Cs, soa.data(), sizeof(double) * soa.size(), cudaMemcpyHostToDevice, s.st));
+  if (s.ns == 1) {  // C(1, n) is already one contiguous field
+    CK(cudaMemcpyAsync(s.Cs, C, sizeof(double) * s.nc, cudaMemcpyHostToDevice, s.st));
+  } else {  // C(ns, n), scalar index fastest: transposed on the device (aos_buf holds >= 9 n)
+    CK(cudaMemcpyAsync(s.aos_buf, C, sizeof(double) * s.ns * s.nc, cudaMemcpyHostToDevice, s.st));
+    dpm::gpu::k_aos_to_soa_k<<<dpm::gpu::nblk(s.nc), dpm::gpu::TPB, 0, s.st>>>(s.nc, s.ns, s.aos_buf, s.Cs);
+    s.launches++;
+  }
   CK(cudaStreamSynchronize(s.st));
   return DPM_OK;
 }
@@ -1709,11 +1716,14 @@ int dpm_download_scalars(dpm_solver_t* h, double* C) {
   Solver& s = *h->s;
   if (s.ns == 0) return DPM_OK;
   CK(cudaSetDevice(s.device));
-  std::vector<double> soa((size_t)s.ns * s.nc);
-  CK(cudaMemcpyAsync(soa.data(), s.Cs, sizeof(double) * soa.size(), cudaMemcpyDeviceToHost, s.st));
+  if (s.ns == 1) {
+    CK(cudaMemcpyAsync(C, s.Cs, sizeof(double) * s.nc, cudaMemcpyDeviceToHost, s.st));
+  } else {
+    dpm::gpu::k_soa_to_aos_k<<<dpm::gpu::nblk(s.nc), dpm::gpu::TPB, 0, s.st>>>(s.nc, s.ns, s.Cs, s.aos_buf);
+    s.launches++;
+    CK(cudaMemcpyAsync(C, s.aos_buf, sizeof(double) * s.ns * s.nc, cudaMemcpyDeviceToHost, s.st));
+  }
   CK(cudaStreamSynchronize(s.st));
-  for (int c = 0; c < s.nc; ++c)
-    for (int k = 0; k < s.ns; ++k) C[(size_t)c * s.ns + k] = soa[(size_t)k * s.nc + c];
   return DPM_OK;
 }
 
@@ -1810,6 +1820,18 @@ int dpm_last_timing(const dpm_solver_t* h, double* step_ms, double* poisson_ms) 
 int dpm_kernel_launches(const dpm_solver_t* h, int64_t* n) {
   if (!h || !n) return DPM_ERR_ARG;
   *n = h->s->launches;
+  return DPM_OK;
+}
+
+int dpm_select_pressure_solver(dpm_solver_t* h, int p_solver) {
+  if (!h) return DPM_ERR_ARG;
+  Solver& s = *h->s;
+  if (p_solver == DPM_PSOLVER_JACOBI_PCG) { s.force_plain = true; return DPM_OK; }
+  const bool ok = (p_solver == DPM_PSOLVER_TWOLEVEL_FCG && s.use_fcg) ||
+                  (p_solver == DPM_PSOLVER_MULTILEVEL_FCG && s.use_ml) ||
+                  (p_solver == DPM_PSOLVER_AUTO && (s.use_fcg || s.use_ml));
+  if (!ok) return DPM_ERR_UNSUPPORTED;
+  s.force_plain = false;
   return DPM_OK;
 }
 

@@ -27,6 +27,7 @@ EXPORTED = (
     "dpm_advection_rhs_scalar", "dpm_viscous_rhs_scalar", "dpm_upload_scalars", "dpm_download_scalars",
     "dpm_learn_collect", "dpm_learn_train", "dpm_learn_set_gamma", "dpm_learn_sizes", "dpm_learn_export",
     "dpm_learn_loss_grad", "dpm_multilevel_hierarchy", "dpm_set_barrier_spin_limit",
+    "dpm_select_pressure_solver",
 )
 
 
@@ -68,6 +69,7 @@ def lib(build_if_missing=True):
     L.dpm_last_timing.argtypes = [vp, dp, dp]
     L.dpm_kernel_launches.argtypes = [vp, lp]
     L.dpm_set_barrier_spin_limit.argtypes = [vp, C.c_longlong]
+    L.dpm_select_pressure_solver.argtypes = [vp, C.c_int]
     L.dpm_ls_gradient_vector.argtypes = [vp, dp, dp, dp]
     L.dpm_advection_rhs_vector.argtypes = [vp, C.c_int, dp, dp, dp, dp, dp]
     L.dpm_viscous_rhs_vector.argtypes = [vp, dp, C.c_double, dp, dp, dp, dp]
@@ -198,6 +200,10 @@ class Solver:
         n = C.c_int64()
         lib().dpm_kernel_launches(self.h, C.byref(n))
         return n.value
+
+    def select_pressure_solver(self, p_solver):
+        """Plain Jacobi-PCG (abi.PSOLVER_JACOBI_PCG) or back to the form the handle was created with."""
+        _check(lib().dpm_select_pressure_solver(self.h, int(p_solver)), "dpm_select_pressure_solver")
 
     def set_barrier_spin_limit(self, spins):
         """Poll limit of the Krylov kernels' grid-wide waits (0: the default, about a second)."""

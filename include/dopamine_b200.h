@@ -268,6 +268,11 @@ int dpm_set_time(dpm_solver_t* s, double time);
 int dpm_last_timing(const dpm_solver_t* s, double* step_ms, double* poisson_ms);
 /* Kernel launch count since the handle was created (own kernels only). */
 int dpm_kernel_launches(const dpm_solver_t* s, int64_t* n);
+/* Switches an existing handle's pressure solve: DPM_PSOLVER_JACOBI_PCG (always available) or
+ * back to the flexible-CG form it was created with (that form's value, or DPM_PSOLVER_AUTO);
+ * any other form returns DPM_ERR_UNSUPPORTED.  Lets the plain FP64 form be timed on the same
+ * handle, mesh and state as the chosen form. */
+int dpm_select_pressure_solver(dpm_solver_t* s, int p_solver);
 /* Failure-detection hook: every grid-wide wait of this handle's Krylov kernels gives up after
  * `spins` polls of its arrival counter (0 restores the default, 2^26 polls, about a second).  A
  * wait that runs out sets the kernel's status word, every block returns, and the call that
