@@ -301,6 +301,10 @@ def run_gpu(args, rank, world):
         case.params["p_solver"] = 1  # DPM_PSOLVER_TWOLEVEL_FCG
     if args.mixed and args.psolver in ("fcg", "auto"):
         case.params["form"] = 1  # DPM_FORM_MIXED (the multilevel form's V-cycle is FP32 already)
+    if args.ml_value_bits:
+        case.params["p_ml_value_bits"] = args.ml_value_bits
+    if args.ml_degree:
+        case.params["p_ml_degree"] = args.ml_degree
     s = Solver(case, device=dev)
     s.initialise()
     nc = s.nc
@@ -403,6 +407,10 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="skip timing the plain FP64 Jacobi-PCG form")
     ap.add_argument("--plain-steps", type=int, default=3, help="timed steps of the plain FP64 form")
     ap.add_argument("--no-learned", action="store_true", help="flexible CG without the learned term")
+    ap.add_argument("--ml-degree", type=int, default=0,
+                    help="multilevel form: Chebyshev steps per smoothing (0: library default, 3)")
+    ap.add_argument("--ml-value-bits", type=int, default=0, choices=[0, 16, 32],
+                    help="multilevel form: storage of the smoother's scaled off-diagonals (0: library default, 16)")
     ap.add_argument("--mixed", action="store_true",
                     help="precision form: FP32-operator inner iterations inside FP64 defect correction")
     ap.add_argument("--psolver", default="auto", choices=["auto", "pcg", "fcg", "ml"],

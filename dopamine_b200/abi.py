@@ -65,7 +65,7 @@ class ParamsT(C.Structure):
         ("abl_T_surface", C.c_double), ("abl_L_obukhov", C.c_double), ("abl_compute_L", C.c_int),
         ("p_ml_degree", C.c_int), ("p_ml_overcorrect", C.c_double), ("p_ml_passes", C.c_int),
         ("gradient_scheme", C.c_int), ("gg_iterations", C.c_int), ("p_stall_window", C.c_int),
-        ("p_stall_ratio", C.c_double),
+        ("p_stall_ratio", C.c_double), ("p_ml_value_bits", C.c_int),
     ]
 
 

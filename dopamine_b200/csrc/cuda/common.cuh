@@ -42,6 +42,12 @@ struct Dev {
   // matrix (ELL, sorted columns)
   const int* Acol;
   const double *Aval, *Adinv;
+  // TVD upwind context per face and flux sign (slot 0: F >= 0, slot 1: F < 0), [2][nf]; null when
+  // no TVD scheme is in use: far-upwind cell (-1: none, -2: no reconstruction context), the face
+  // and downwind distances along the upwind direction (the latter floored at 1e-30) and the
+  // far-upwind cell's distance behind the upwind cell
+  const int* tvd_far;
+  const double *tvd_sf, *tvd_sd, *tvd_su;
 };
 
 // Fields and work arrays.

@@ -217,6 +217,70 @@ __global__ void __launch_bounds__(TPB) k_ls_gradient_scalars(Dev d, LsScalarSet 
   }
 }
 
+// Velocity gradient and the gradients of NS scalar fields in one pass over the stencil: the
+// indices and weights (624 B per hex cell, the dominant traffic of both operators) are read once
+// instead of once per operator.  Each field's sums are formed exactly as in k_ls_gradient_vector
+// and k_ls_gradient_scalars (same stencil order, same products), so the results are the same.
+template <int NS>
+__global__ void __launch_bounds__(TPB) k_ls_gradient_all(Dev d, const double* __restrict__ U,
+                                                         const double* __restrict__ Ub, double* __restrict__ gU,
+                                                         LsScalarSet q) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.nc) return;
+  const int nc = d.nc, nb = d.nb, W = d.W;
+  const double uc0 = U[c], uc1 = U[nc + c], uc2 = U[2 * nc + c];
+  double a[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  double pc[NS], a0[NS], a1[NS], a2[NS];
+#pragma unroll
+  for (int k = 0; k < NS; ++k) {
+    pc[k] = q.phi[k][c];
+    a0[k] = a1[k] = a2[k] = 0.0;
+  }
+  for (int s = 0; s < W; ++s) {
+    int v = __ldg(&d.ls_idx[s * nc + c]);
+    if (v == PADI) break;
+    const double w0 = __ldg(&d.ls_w[(0 * W + s) * nc + c]);
+    const double w1 = __ldg(&d.ls_w[(1 * W + s) * nc + c]);
+    const double w2 = __ldg(&d.ls_w[(2 * W + s) * nc + c]);
+    double un0, un1, un2, pv[NS];
+    if (v >= 0) {
+      un0 = U[v]; un1 = U[nc + v]; un2 = U[2 * nc + v];
+#pragma unroll
+      for (int k = 0; k < NS; ++k) pv[k] = q.phi[k][v];
+    } else {
+      int b = -v - 1;
+      if (b < nb) {
+        un0 = Ub[b]; un1 = Ub[nb + b]; un2 = Ub[2 * nb + b];
+#pragma unroll
+        for (int k = 0; k < NS; ++k) pv[k] = q.pb[k][b];
+      } else {
+        un0 = uc0; un1 = uc1; un2 = uc2;
+#pragma unroll
+        for (int k = 0; k < NS; ++k) pv[k] = pc[k];
+      }
+    }
+    double du0 = un0 - uc0, du1 = un1 - uc1, du2 = un2 - uc2;
+    a[0] += w0 * du0; a[1] += w1 * du0; a[2] += w2 * du0;
+    a[3] += w0 * du1; a[4] += w1 * du1; a[5] += w2 * du1;
+    a[6] += w0 * du2; a[7] += w1 * du2; a[8] += w2 * du2;
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
+      double dd = pv[k] - pc[k];
+      a0[k] += w0 * dd;
+      a1[k] += w1 * dd;
+      a2[k] += w2 * dd;
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < 9; ++j) gU[j * nc + c] = a[j];
+#pragma unroll
+  for (int k = 0; k < NS; ++k) {
+    q.g[k][c] = a0[k];
+    q.g[k][nc + c] = a1[k];
+    q.g[k][2 * nc + c] = a2[k];
+  }
+}
+
 // Green-Gauss gradients (src/numerics/mod_gradient.f90:38-304): grad_c = (1/V_c) sum_f phi_f S_f
 // gathered per cell over its faces in face order (the order in which the reference's face loop
 // adds them); phi_f = gc-interpolation on interior faces, plus the mean previous gradient . eps
@@ -688,17 +752,77 @@ __device__ double tvd_d(const Dev& d, int scheme, const double* phi, const Recon
   return clampv_d(pU + psi * sdn * c.s_face, fmin(pU, pD), fmax(pU, pD));
 }
 
+// The TVD context does not change between steps: it depends on the face's geometry and on the
+// sign of the face flux only (recon_context_d branches on F >= 0), so it is formed once per face
+// and sign by k_tvd_context and read by the face kernels.  The values are those recon_context_d,
+// far_upwind_d and tvd_d form, expression for expression.
+__global__ void k_tvd_context(Dev d, int* far2, double* sf2, double* sd2, double* su2) {
+  int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= d.nf) return;
+  const int nc = d.nc, nf = d.nf;
+  for (int sg = 0; sg < 2; ++sg) {
+    ReconCtx c;
+    const bool ok = recon_context_d(d, f, sg ? -1.0 : 1.0, c);
+    int far = ok ? far_upwind_d(d, c) : -2;
+    double su = 0.0;
+    if (far >= 0) {
+      double xf0 = d.cen[far] + c.sh[0] - c.xu[0], xf1 = d.cen[nc + far] + c.sh[1] - c.xu[1],
+             xf2 = d.cen[2 * nc + far] + c.sh[2] - c.xu[2];
+      su = -(xf0 * c.dir[0] + xf1 * c.dir[1] + xf2 * c.dir[2]);
+      if (!(su > SMALLD)) far = -1;
+    }
+    far2[sg * nf + f] = far;
+    sf2[sg * nf + f] = ok ? c.s_face : 0.0;
+    sd2[sg * nf + f] = ok ? fmax(c.s_down, SMALLD) : 1.0;
+    su2[sg * nf + f] = su;
+  }
+}
+
+// Upwind and downwind cells of face f for flux sign slot sg (0: F >= 0); false when the face
+// has no reconstruction context (a non-periodic boundary face).
+__device__ __forceinline__ bool tvd_cells_d(const Dev& d, int f, int sg, int& up, int& down) {
+  const int o = d.fo[f], n = d.fn[f];
+  int m = n;
+  if (n < 0) {
+    const int b = f - d.nfi;
+    if (d.bbc[b] != BC_PERIODIC || d.bpnb[b] < 0) return false;
+    m = d.bpnb[b];
+  }
+  if (sg == 0) { up = o; down = m; } else { up = m; down = o; }
+  return true;
+}
+
+// tvd_d on the precomputed context of face f, sign slot sg
+__device__ __forceinline__ double tvd_pre_d(const Dev& d, int scheme, const double* phi, int f, int sg, int up,
+                                            int down, int far) {
+  const int nf = d.nf;
+  double pU = phi[up], pD = phi[down];
+  double sdn = (pD - pU) / d.tvd_sd[sg * nf + f], psi = 0.0;
+  if (far >= 0 && fabs(sdn) > SMALLD) {
+    double r = ((pU - phi[far]) / d.tvd_su[sg * nf + f]) / sdn;
+    if (scheme == 1) {
+      psi = (r + fabs(r)) / (1.0 + fabs(r));
+      psi = fmax(0.0, fmin(psi, 2.0));
+    } else {
+      psi = fmax(0.0, fmin(fmin(2.0 * r, (1.0 + 2.0 * r) / 3.0), 2.0));
+    }
+  }
+  return clampv_d(pU + psi * sdn * d.tvd_sf[sg * nf + f], fmin(pU, pD), fmax(pU, pD));
+}
+
 // ------------------------------------------------------------------------------------------
 // Face fluxes of the explicit right-hand side: advective Fn*phi_f (KEP, CDS, QUICK, van Leer,
 // Koren; src/numerics/mod_advection.f90:1013-1635) and viscous stress (src/numerics/mod_viscous.f90:37-282),
 // written per face; k_cell_explicit gathers them per cell.
-__global__ void __launch_bounds__(TPB) k_face_explicit(Dev d, int scheme, double nu, const double* __restrict__ U,
-                                                       const double* __restrict__ Ub, const double* __restrict__ gU,
-                                                       const double* __restrict__ nus, const double* __restrict__ Uface,
-                                                       double* __restrict__ fadv, double* __restrict__ fvis,
-                                                       double* __restrict__ fdiv) {
-  int f = blockIdx.x * blockDim.x + threadIdx.x;
-  if (f >= d.nf) return;
+// Advective and viscous flux of face f (owner orientation): the KEP / CDS / QUICK / van Leer / Koren
+// face value times the face flux, the viscous stress, and (KEP) the face flux itself for the
+// divergence term.  Shared by the face-parallel kernel and the cell-owned one, so a face's values
+// are the same whichever side forms them.
+__device__ __forceinline__ void face_explicit_d(const Dev& d, int scheme, double nu, const double* __restrict__ U,
+                                                const double* __restrict__ Ub, const double* __restrict__ gU,
+                                                const double* __restrict__ nus, const double* __restrict__ Uface,
+                                                int f, double* adv, double* vis, double& div) {
+  div = 0.0;
   const int nc = d.nc, nf = d.nf, nb = d.nb;
   const int o = d.fo[f], n = d.fn[f];
   const double sf0 = d.sf[f], sf1 = d.sf[nf + f], sf2 = d.sf[2 * nf + f];
@@ -725,7 +849,7 @@ __global__ void __launch_bounds__(TPB) k_face_explicit(Dev d, int scheme, double
       else Fn = Ufv[0] * sf0 + Ufv[1] * sf1 + Ufv[2] * sf2;
       for (int k = 0; k < 3; ++k) phi[k] = npr >= 0 ? 0.5 * (U[k * nc + o] + U[k * nc + npr]) : Ufv[k];
     }
-    fdiv[f] = Fn;
+    div = Fn;
   } else if (scheme == 3) {  // CDS
     int npr = -1;
     if (n >= 0) Fn = Uface[f];
@@ -761,16 +885,25 @@ __global__ void __launch_bounds__(TPB) k_face_explicit(Dev d, int scheme, double
     if (n >= 0) Fn = Uface[f];
     else Fn = is_wall_bc(bc) ? 0.0 : Uface[f];
     ReconCtx ctx;
-    bool ok = recon_context_d(d, f, Fn, ctx);
-    int far = -1;
-    if (ok && scheme != 5) far = far_upwind_d(d, ctx);
+    bool ok;
+    int far = -1, sg = 0, up = -1, down = -1;
+    if (scheme != 5 && d.tvd_far) {  // van Leer / Koren: the precomputed context
+      sg = Fn >= 0.0 ? 0 : 1;
+      far = d.tvd_far[sg * nf + f];
+      ok = far != -2 && tvd_cells_d(d, f, sg, up, down);
+    } else {
+      ok = recon_context_d(d, f, Fn, ctx);
+      if (ok && scheme != 5) far = far_upwind_d(d, ctx);
+    }
     if (!finite_d(Fn)) Fn = 0.0;
     double pq[3] = {0, 0, 0};
     if (ok && scheme == 5) quick3_d(d, ctx, U, gU, pq);
     for (int k = 0; k < 3; ++k) {
       double ph;
       if (ok) {
-        ph = scheme == 5 ? pq[k] : tvd_d(d, scheme, U + (size_t)k * nc, ctx, far);
+        ph = scheme == 5 ? pq[k]
+                         : (d.tvd_far ? tvd_pre_d(d, scheme, U + (size_t)k * nc, f, sg, up, down, far)
+                                      : tvd_d(d, scheme, U + (size_t)k * nc, ctx, far));
         if (!finite_d(ph)) ph = (Fn >= 0.0 || n < 0) ? U[k * nc + o] : U[k * nc + n];
       } else {
         ph = Ub[k * nb + b];
@@ -779,7 +912,7 @@ __global__ void __launch_bounds__(TPB) k_face_explicit(Dev d, int scheme, double
       phi[k] = ph;
     }
   }
-  for (int k = 0; k < 3; ++k) fadv[k * nf + f] = Fn * phi[k];
+  for (int k = 0; k < 3; ++k) adv[k] = Fn * phi[k];
 
   // ---- viscous stress (owner orientation)
   double st[3] = {0, 0, 0};
@@ -833,7 +966,24 @@ __global__ void __launch_bounds__(TPB) k_face_explicit(Dev d, int scheme, double
       st[k] = ne * (t1 + t2 + t3);
     }
   }
-  for (int k = 0; k < 3; ++k) fvis[k * nf + f] = st[k];
+  for (int k = 0; k < 3; ++k) vis[k] = st[k];
+}
+
+__global__ void __launch_bounds__(TPB) k_face_explicit(Dev d, int scheme, double nu, const double* __restrict__ U,
+                                                       const double* __restrict__ Ub, const double* __restrict__ gU,
+                                                       const double* __restrict__ nus, const double* __restrict__ Uface,
+                                                       double* __restrict__ fadv, double* __restrict__ fvis,
+                                                       double* __restrict__ fdiv) {
+  int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= d.nf) return;
+  const int nf = d.nf;
+  double adv[3], vis[3], div;
+  face_explicit_d(d, scheme, nu, U, Ub, gU, nus, Uface, f, adv, vis, div);
+  for (int k = 0; k < 3; ++k) {
+    fadv[k * nf + f] = adv[k];
+    fvis[k * nf + f] = vis[k];
+  }
+  if (scheme == 4) fdiv[f] = div;
 }
 
 // Per-cell gather of the explicit fluxes into H = conv + visc + f (+ Boussinesq, + wall
@@ -892,6 +1042,56 @@ __global__ void __launch_bounds__(TPB) k_cell_explicit(Dev d, ExplicitArgs a, do
   }
   if (a.predict)
     for (int k = 0; k < 3; ++k) U[k * nc + c] = u[k] + a.dt * (a.a_k * h[k] + a.b_k * H0[k * nc + c]);
+}
+
+// The same right-hand side and predictor as k_face_explicit + k_cell_explicit in one cell-owned
+// pass: each cell forms the fluxes of its own faces (face_explicit_d; an interior face is formed
+// by both of its cells, with identical values) and sums them in ascending face order as
+// k_cell_explicit does, so nothing goes through the per-face flux arrays.  Neighbouring cells
+// still read U, so the predicted velocity goes to Unew (the caller swaps the buffers).
+__global__ void __launch_bounds__(TPB) k_cell_momentum(Dev d, ExplicitArgs a, double nu, const double* __restrict__ U,
+                                                       const double* __restrict__ Ub, const double* __restrict__ gU,
+                                                       const double* __restrict__ nus, const double* __restrict__ Uface,
+                                                       const double* __restrict__ T, const double* __restrict__ tau,
+                                                       double* __restrict__ H, const double* __restrict__ H0,
+                                                       double* __restrict__ Unew) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.nc) return;
+  const int nc = d.nc, nb = d.nb;
+  const double iv = d.ivol[c];
+  double cv[3] = {0, 0, 0}, vs[3] = {0, 0, 0}, dv = 0.0;
+  for (int s = 0; s < d.S; ++s) {
+    int f = d.cf[s * nc + c];
+    if (f == PADI) break;
+    double adv[3], vis[3], div;
+    face_explicit_d(d, a.scheme, nu, U, Ub, gU, nus, Uface, f, adv, vis, div);
+    bool own = d.fo[f] == c;
+    for (int k = 0; k < 3; ++k) {
+      if (own) { cv[k] -= adv[k] * iv; vs[k] += vis[k] * iv; }
+      else { cv[k] += adv[k] * iv; vs[k] -= vis[k] * iv; }
+    }
+    if (a.scheme == 4) dv = own ? dv + div : dv - div;
+  }
+  double u[3] = {U[c], U[nc + c], U[2 * nc + c]};
+  if (a.scheme == 4)
+    for (int k = 0; k < 3; ++k) cv[k] += 0.5 * u[k] * dv * iv;
+  const double fb[3] = {a.f0, a.f1, a.f2}, gv[3] = {a.g0, a.g1, a.g2};
+  double h[3];
+  for (int k = 0; k < 3; ++k) {
+    h[k] = cv[k] + vs[k] + fb[k];
+    if (a.bous) h[k] = h[k] - a.beta * (T[c] - a.T_ref) * gv[k];
+  }
+  for (int s = 0; s < d.SB; ++s) {
+    int b = d.cbn[s * nc + c];
+    if (b == PADI) break;
+    if (d.bbc[b] != BC_WALL_MODEL) continue;
+    double w = d.area[d.nfi + b] / d.vol[c];
+    for (int k = 0; k < 3; ++k) h[k] = h[k] + tau[k * nb + b] * w;
+  }
+  for (int k = 0; k < 3; ++k) {
+    H[k * nc + c] = h[k];
+    Unew[k * nc + c] = u[k] + a.dt * (a.a_k * h[k] + a.b_k * H0[k * nc + c]);
+  }
 }
 
 // ------------------------------------------------------------------------------------------

@@ -12,7 +12,12 @@
 //
 // Cheb_k: k steps of Chebyshev iteration on D^-1 A_l over [lmax/10, lmax] (Saad, Iterative
 // Methods, alg. 12.1), T the piecewise-constant prolongation of the aggregates, oc the
-// over-correction of the unsmoothed-aggregation coarse correction.  Every smoothing step reads
+// over-correction of the unsmoothed-aggregation coarse correction.  The smoother reads each
+// level as D^-1 A = G + S: off-diagonal entries only, scaled by the row's diagonal and stored in
+// FP32 or in binary16 (SV = unsigned short: the half's bits), with the diagonal term g_i chosen
+// so that every stored row keeps the exact row sum; the level's right-hand side is kept scaled
+// (b / a_ii).  A sweep then reads columns, scaled values, g, b, x and d - no diagonal entry and
+// no 1/diagonal - and the restriction multiplies a member row's scaled residual back by a_ii.  Every smoothing step reads
 // neighbour values written by the step before, so each step ends at a grid barrier; the first
 // step of each down-smoothing is fused into the restriction that produces its right-hand side,
 // and the prolongation into the first up-smoothing step, so a V-cycle costs 2 k nlev + 1
@@ -20,6 +25,8 @@
 // two-level kernel (fcg.cuh); the stopping rule is the reference's, src/solver/
 // pressure_backend_petsc.c:816-876.
 #pragma once
+#include <cuda_fp16.h>
+
 #include "fcg.cuh"
 
 namespace dpm {
@@ -37,13 +44,15 @@ struct MlDevLevel {
   int lgMP;          // log2 MP
   int lgG;           // log2 of the lanes that share one row of a smoothing step
   int lgGR;          // log2 of the lanes that share one member row of the restriction
-  int rows_per_pass; // lgG == 0: rows a lane takes per pass (1..4)
-  const int* col;    // [W][n]
-  const float* val;  // [W][n]
-  const float* dinv; // [n]
+  int rows_per_pass; // lgG == 0: rows a lane takes per pass (1..2)
+  const int* col;    // [W][n] off-diagonal columns, padded with the own row (W = off-diagonal width)
+  const void* sv;    // [W][n] s_ij = a_ij / a_ii, FP32 or binary16 bits (padding 0)
+  const float* g;    // [n] diagonal term of the scaled row (1 up to the stored entries' rounding)
+  const float* diag; // [n] a_ii
+  const float* dinv; // [n] 1 / a_ii
   const int* agg;    // [n]
   const int* mem;    // [M][n_next], -1 padded
-  float* b;          // [n] right-hand side of this level
+  float* b;          // [n] scaled right-hand side b / a_ii of this level
   float* x0;         // [n] iterate, two buffers
   float* x1;
   float* d;          // [n] Chebyshev direction
@@ -89,12 +98,16 @@ struct MlArgs {
 // together instead of one dependent load pair per entry.
 constexpr int ML_CHUNK = 8;
 
-// Partial product of row i with the iterate over the entries k = sub, sub + G, sub + 2G, ...
+__device__ __forceinline__ float ml_sval(const float* p) { return __ldg(p); }
+__device__ __forceinline__ float ml_sval(const unsigned short* p) { return __half2float(__ushort_as_half(__ldg(p))); }
+
+// Partial sum of s_ij x_j over the off-diagonal entries k = sub, sub + G, sub + 2G, ... of row i
 // (G lanes share a row; G = 1: the whole row).  PRO: the iterate is the prolonged x + oc T x_c,
 // formed on the fly.
-template <bool PRO>
+template <class SV, bool PRO>
 __device__ __forceinline__ float ml_part(const MlDevLevel& L, int i, const float* x, const float* xc, float oc,
                                          int G, int sub) {
+  const SV* sv = static_cast<const SV*>(L.sv);
   float s = 0.0f;
   for (int k0 = sub; k0 < L.W; k0 += G * ML_CHUNK) {
     int c[ML_CHUNK];
@@ -104,7 +117,7 @@ __device__ __forceinline__ float ml_part(const MlDevLevel& L, int i, const float
       const int k = k0 + u * G;
       const size_t e = (size_t)k * L.n + i;
       c[u] = k < L.W ? __ldg(&L.col[e]) : i;
-      v[u] = k < L.W ? __ldg(&L.val[e]) : 0.0f;
+      v[u] = k < L.W ? ml_sval(&sv[e]) : 0.0f;
     }
     if (PRO) {
       int g[ML_CHUNK];
@@ -125,60 +138,57 @@ __device__ __forceinline__ float ml_part(const MlDevLevel& L, int i, const float
   return s;
 }
 
-// One Chebyshev step on level L for every row: r = b - A x_in, d = c1 d + c2 D^-1 r, x_out =
-// x_in + d.  PRO: the first step after the coarse correction, on the prolonged iterate
-// x_in + oc T x_c, with d = D^-1 r / theta.  Rows are spread over 2^lgG lanes on small levels
-// (partial sums combined by shuffles); on large levels each lane takes two rows per pass so
-// that their loads are in flight together.
-template <bool PRO, int R>
+// One Chebyshev step on level L for every row, in the scaled form: rs = b - g x_in - S x_in
+// (= D^-1 (b - A x_in)), d = c1 d + c2 rs, x_out = x_in + d.  PRO: the first step after the coarse
+// correction, on the prolonged iterate x_in + oc T x_c, with d = rs / theta.  On large levels
+// each lane takes R rows per pass so that their loads are in flight together.  om: the learned
+// term gam * omega_i * b_i (b scaled) added to x_out.
+template <class SV, bool PRO, int R>
 __device__ __forceinline__ void ml_sweep_rows(const MlDevLevel& L, float c1, float c2, const float* xi, float* xo,
                                               const float* xc, float oc, int g0, int T, const float* om, float gam) {
   for (int i0 = g0; i0 < L.n; i0 += R * T) {
     int ii[R];
-    float acc[R], b[R], q[R], x[R], d[R];
+    float acc[R], b[R], gg[R], x[R], dd[R];
 #pragma unroll
     for (int h = 0; h < R; ++h) {
       const int i = i0 + h * T;
       ii[h] = i < L.n ? i : i0;  // an absent row repeats row i0 (loads in bounds, no store)
     }
 #pragma unroll
-    for (int h = 0; h < R; ++h) acc[h] = ml_part<PRO>(L, ii[h], xi, xc, oc, 1, 0);
+    for (int h = 0; h < R; ++h) acc[h] = ml_part<SV, PRO>(L, ii[h], xi, xc, oc, 1, 0);
 #pragma unroll
     for (int h = 0; h < R; ++h) {
       b[h] = __ldcg(&L.b[ii[h]]);
-      q[h] = __ldg(&L.dinv[ii[h]]);
+      gg[h] = __ldg(&L.g[ii[h]]);
       x[h] = __ldcg(&xi[ii[h]]);
-      if (PRO) {
-        x[h] = fmaf(oc, __ldcg(&xc[__ldg(&L.agg[ii[h]])]), x[h]);
-        d[h] = L.inv_theta * q[h] * (b[h] - acc[h]);
-      } else {
-        d[h] = c1 * __ldcg(&L.d[ii[h]]) + c2 * q[h] * (b[h] - acc[h]);
-      }
+      dd[h] = PRO ? 0.0f : __ldcg(&L.d[ii[h]]);
+      if (PRO) x[h] = fmaf(oc, __ldcg(&xc[__ldg(&L.agg[ii[h]])]), x[h]);
     }
 #pragma unroll
-    for (int h = 0; h < R; ++h)
+    for (int h = 0; h < R; ++h) {
+      const float rs = b[h] - fmaf(gg[h], x[h], acc[h]);
+      const float d = PRO ? L.inv_theta * rs : fmaf(c1, dd[h], c2 * rs);
       if (i0 + h * T < L.n) {
-        L.d[ii[h]] = d[h];
-        xo[ii[h]] = x[h] + d[h] + (om ? gam * __ldg(&om[ii[h]]) * q[h] * b[h] : 0.0f);
+        L.d[ii[h]] = d;
+        xo[ii[h]] = x[h] + d + (om ? gam * __ldg(&om[ii[h]]) * b[h] : 0.0f);
       }
+    }
   }
 }
 
-// One Chebyshev step on level L for every row: r = b - A x_in, d = c1 d + c2 D^-1 r, x_out =
-// x_in + d.  PRO: the first step after the coarse correction, on the prolonged iterate
-// x_in + oc T x_c, with d = D^-1 r / theta.  Rows are spread over 2^lgG lanes on small levels
-// (partial sums combined by shuffles); on large levels each lane takes up to 4 rows per pass
-// (rows_per_pass) so that their loads are in flight together.
-template <bool PRO>
+// One Chebyshev step on level L for every row (see ml_sweep_rows).  Rows are spread over 2^lgG
+// lanes on small levels (partial sums combined by shuffles); on large levels each lane takes up
+// to 4 rows per pass (rows_per_pass).
+template <class SV, bool PRO>
 __device__ __forceinline__ void ml_sweep(const MlDevLevel& L, float c1, float c2, const float* xi, float* xo,
                                          const float* xc, float oc, int g0, int T, const float* om = nullptr,
                                          float gam = 0.0f) {
   if (L.lgG == 0) {
     switch (L.rows_per_pass) {
-      case 1: ml_sweep_rows<PRO, 1>(L, c1, c2, xi, xo, xc, oc, g0, T, om, gam); return;
-      case 2: ml_sweep_rows<PRO, 2>(L, c1, c2, xi, xo, xc, oc, g0, T, om, gam); return;
-      case 3: ml_sweep_rows<PRO, 3>(L, c1, c2, xi, xo, xc, oc, g0, T, om, gam); return;
-      default: ml_sweep_rows<PRO, 4>(L, c1, c2, xi, xo, xc, oc, g0, T, om, gam); return;
+      case 1: ml_sweep_rows<SV, PRO, 1>(L, c1, c2, xi, xo, xc, oc, g0, T, om, gam); return;
+      case 2: ml_sweep_rows<SV, PRO, 2>(L, c1, c2, xi, xo, xc, oc, g0, T, om, gam); return;
+      case 3: ml_sweep_rows<SV, PRO, 3>(L, c1, c2, xi, xo, xc, oc, g0, T, om, gam); return;
+      default: ml_sweep_rows<SV, PRO, 4>(L, c1, c2, xi, xo, xc, oc, g0, T, om, gam); return;
     }
   }
   const int lane = threadIdx.x & 31;
@@ -187,21 +197,16 @@ __device__ __forceinline__ void ml_sweep(const MlDevLevel& L, float c1, float c2
     const int u = u0 + lane;
     const bool ok = u < total;
     const int i = ok ? u >> L.lgG : 0, sub = u & (G - 1);
-    float acc = ok ? ml_part<PRO>(L, i, xi, xc, oc, G, sub) : 0.0f;
+    float acc = ok ? ml_part<SV, PRO>(L, i, xi, xc, oc, G, sub) : 0.0f;
     for (int o = G >> 1; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
     if (ok && sub == 0) {
-      const float r = __ldcg(&L.b[i]) - acc;
-      const float q = __ldg(&L.dinv[i]);
+      const float b = __ldcg(&L.b[i]);
       float x = __ldcg(&xi[i]);
-      float d;
-      if (PRO) {
-        x = fmaf(oc, __ldcg(&xc[__ldg(&L.agg[i])]), x);
-        d = L.inv_theta * q * r;
-      } else {
-        d = c1 * __ldcg(&L.d[i]) + c2 * q * r;
-      }
+      if (PRO) x = fmaf(oc, __ldcg(&xc[__ldg(&L.agg[i])]), x);
+      const float rs = b - fmaf(__ldg(&L.g[i]), x, acc);
+      const float d = PRO ? L.inv_theta * rs : fmaf(c1, __ldcg(&L.d[i]), c2 * rs);
       L.d[i] = d;
-      xo[i] = x + d + (om ? gam * __ldg(&om[i]) * q * __ldcg(&L.b[i]) : 0.0f);
+      xo[i] = x + d + (om ? gam * __ldg(&om[i]) * b : 0.0f);
     }
   }
 }
@@ -226,8 +231,8 @@ __device__ __forceinline__ double ml_row64(const MlArgs& a, int i, const V* x) {
   return s;
 }
 
-// (a template so that every translation unit that includes this header may instantiate it)
-template <int V>
+// SV: value type of the smoother's scaled off-diagonals, float or unsigned short (binary16 bits)
+template <class SV>
 __global__ void __launch_bounds__(ML_TPB, 2) k_mlcg(MlArgs a) {
   __shared__ MlDevLevel s_lv[ML_LEVELS];
   __shared__ double s_gat[1];
@@ -248,8 +253,8 @@ __global__ void __launch_bounds__(ML_TPB, 2) k_mlcg(MlArgs a) {
   auto start_level0 = [&](int i, double ri) {
     if (nlev > 0) {
       const MlDevLevel& L = s_lv[0];
-      const float bi = (float)ri;
-      const float di = L.inv_theta * __ldg(&L.dinv[i]) * bi;
+      const float bi = (float)ri * __ldg(&L.dinv[i]);  // scaled right-hand side
+      const float di = L.inv_theta * bi;
       L.b[i] = bi;
       L.d[i] = di;
       L.x0[i] = di;
@@ -302,16 +307,16 @@ __global__ void __launch_bounds__(ML_TPB, 2) k_mlcg(MlArgs a) {
       for (int j = 1; j < deg; ++j) {
         const float* xi = cur ? L.x1 : L.x0;
         float* xo = cur ? L.x0 : L.x1;
-        ml_sweep<false>(L, L.c1[j], L.c2[j], xi, xo, nullptr, 0.0f, g0, T);
+        ml_sweep<SV, false>(L, L.c1[j], L.c2[j], xi, xo, nullptr, 0.0f, g0, T);
         cur ^= 1;
         if (!grid_barrier(a.bar, gen, a.status)) return;
       }
       cur_mask = (cur_mask & ~(1u << l)) | ((unsigned)cur << l);
       const float* xf = cur ? L.x1 : L.x0;
       const bool last = l + 1 == nlev;
-      // lanes [aggregate][member slot][2^lgGR lanes per member row]: a lane sums its share of a
-      // member row's A x, the butterfly over the aggregate's 2^(lgMP + lgGR) lanes adds up
-      // sum_i (b_i - (A x)_i) in a fixed order
+      // lanes [aggregate][member slot][2^lgGR lanes per member row]: a lane forms its share of a
+      // member row's residual a_ii (b_i - g_i x_i - (S x)_i) (scaled form times the diagonal),
+      // the butterfly over the aggregate's 2^(lgMP + lgGR) lanes adds up sum_i r_i in a fixed order
       const int lgR = L.lgMP + L.lgGR, span = 1 << lgR, GR = 1 << L.lgGR;
       const int total = L.n_next << lgR;
       const int lane = threadIdx.x & 31;
@@ -323,8 +328,9 @@ __global__ void __launch_bounds__(ML_TPB, 2) k_mlcg(MlArgs a) {
         if (ok && m < L.M) {
           const int i = __ldg(&L.mem[(size_t)m * L.n_next + c]);
           if (i >= 0) {
-            sres = -ml_part<false>(L, i, xf, nullptr, 0.0f, GR, sub);
-            if (sub == 0) sres += __ldcg(&L.b[i]);
+            sres = -ml_part<SV, false>(L, i, xf, nullptr, 0.0f, GR, sub);
+            if (sub == 0) sres += __ldcg(&L.b[i]) - __ldg(&L.g[i]) * __ldcg(&xf[i]);
+            sres *= __ldg(&L.diag[i]);
           }
         }
         for (int o = span >> 1; o > 0; o >>= 1) sres += __shfl_xor_sync(0xffffffffu, sres, o);
@@ -333,8 +339,9 @@ __global__ void __launch_bounds__(ML_TPB, 2) k_mlcg(MlArgs a) {
             a.bC[c] = sres;
           } else {
             const MlDevLevel& N = s_lv[l + 1];
-            const float di = N.inv_theta * __ldg(&N.dinv[c]) * sres;
-            N.b[c] = sres;
+            const float bs = sres * __ldg(&N.dinv[c]);
+            const float di = N.inv_theta * bs;
+            N.b[c] = bs;
             N.d[c] = di;
             N.x0[c] = di;
           }
@@ -370,13 +377,13 @@ __global__ void __launch_bounds__(ML_TPB, 2) k_mlcg(MlArgs a) {
       const MlDevLevel& L = s_lv[l];
       int cur = (cur_mask >> l) & 1u;
       const float* om = (l == 0 && a.gamma != 0.0f) ? a.omega : nullptr;  // learned term: last fine step
-      ml_sweep<true>(L, 0.0f, 0.0f, cur ? L.x1 : L.x0, cur ? L.x0 : L.x1, xcoarse, a.oc, g0, T,
-                     deg == 1 ? om : nullptr, a.gamma);
+      ml_sweep<SV, true>(L, 0.0f, 0.0f, cur ? L.x1 : L.x0, cur ? L.x0 : L.x1, xcoarse, a.oc, g0, T,
+                         deg == 1 ? om : nullptr, a.gamma);
       cur ^= 1;
       if (!grid_barrier(a.bar, gen, a.status)) return;
       for (int j = 1; j < deg; ++j) {
-        ml_sweep<false>(L, L.c1[j], L.c2[j], cur ? L.x1 : L.x0, cur ? L.x0 : L.x1, nullptr, 0.0f, g0, T,
-                        j == deg - 1 ? om : nullptr, a.gamma);
+        ml_sweep<SV, false>(L, L.c1[j], L.c2[j], cur ? L.x1 : L.x0, cur ? L.x0 : L.x1, nullptr, 0.0f, g0, T,
+                            j == deg - 1 ? om : nullptr, a.gamma);
         cur ^= 1;
         if (!grid_barrier(a.bar, gen, a.status)) return;
       }
@@ -394,7 +401,7 @@ __global__ void __launch_bounds__(ML_TPB, 2) k_mlcg(MlArgs a) {
         const size_t o = off + __ldg(&a.pinv[i]);
         a.rec_r[o] = __ldcg(&a.r[i]);
         a.rec_z[o] = (double)__ldcg(&z[i]);
-        a.rec_u[o] = (double)(__ldg(&L0.dinv[i]) * __ldcg(&L0.b[i]));
+        a.rec_u[o] = (double)__ldcg(&L0.b[i]);  // D^-1 r: the level's scaled right-hand side
         a.rec_x[o] = __ldcg(&a.x[i]);
       }
     }

@@ -173,17 +173,23 @@ __global__ void __launch_bounds__(TPB) k_face_scalars(Dev d, ScalarFaceSet q, co
   const int b = f - d.nfi;
   const int bc = n >= 0 ? -1 : d.bbc[b];
   double Fn = (n < 0 && is_wall_bc(bc)) ? 0.0 : Uface[f];
-  bool need_ctx = false, need_far = false;
+  bool need_ctx = false, need_far = false, need_quick = false;
 #pragma unroll
   for (int k = 0; k < LS_SET; ++k)
     if (k < q.n && q.scheme[k] != 3) {
       need_ctx = true;
       if (q.scheme[k] != 5) need_far = true;
+      else need_quick = true;
     }
   ReconCtx ctx;
   bool ok = false;
-  int far = -1;
-  if (need_ctx) {
+  int far = -1, sg = 0, up = -1, down = -1;
+  const bool pre = need_ctx && !need_quick && d.tvd_far;  // van Leer / Koren only: precomputed context
+  if (pre) {
+    sg = Fn >= 0.0 ? 0 : 1;
+    far = d.tvd_far[sg * nf + f];
+    ok = far != -2 && tvd_cells_d(d, f, sg, up, down);
+  } else if (need_ctx) {
     ok = recon_context_d(d, f, Fn, ctx);
     if (ok && need_far) far = far_upwind_d(d, ctx);
   }
@@ -251,7 +257,7 @@ __global__ void __launch_bounds__(TPB) k_face_scalars(Dev d, ScalarFaceSet q, co
       }
     } else if (ok) {  // QUICK (5), van Leer (1), Koren (2)
       if (q.scheme[k] == 5) quick_d<1>(d, ctx, phi, g, &ph);
-      else ph = tvd_d(d, q.scheme[k], phi, ctx, far);
+      else ph = pre ? tvd_pre_d(d, q.scheme[k], phi, f, sg, up, down, far) : tvd_d(d, q.scheme[k], phi, ctx, far);
       if (!finite_d(ph)) ph = (Fn >= 0.0 || n < 0) ? phi[o] : phi[n];
     } else {
       ph = q.pb[k][b];

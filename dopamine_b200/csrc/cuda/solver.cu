@@ -173,6 +173,7 @@ struct Solver {
   double *red_part = nullptr, *red_out = nullptr, *scratch_c = nullptr, *scratch_c2 = nullptr;
   double *aos_buf = nullptr;
   double *conv_tmp = nullptr, *visc_tmp = nullptr;
+  double* U_spare = nullptr;  // second velocity buffer: the fused explicit pass writes the prediction here
   // PCG workspace
   double *cg_r, *cg_z, *cg_p0, *cg_p1, *cg_q, *cg_bp, *cg_x, *cg_part, *cg_dout;
   void* cg_kernel = nullptr;
@@ -345,6 +346,19 @@ struct Solver {
     std::vector<double> dinv(nc);
     for (int c = 0; c < nc; ++c) dinv[c] = 1.0 / S.diag[c];
     d.Adinv = mem.upload(dinv);
+    {  // TVD upwind context per face and flux sign, when a van Leer / Koren scheme is configured
+      auto is_tvd = [](int sch) { return sch == DPM_SCHEME_VANLEER_TVD || sch == DPM_SCHEME_KOREN_TVD; };
+      if (is_tvd(P.scheme) || (P.boussinesq && is_tvd(P.temperature_scheme)) ||
+          (P.n_scalars > 0 && is_tvd(P.scalar_scheme))) {
+        int* far2 = mem.alloc<int>(2 * (size_t)nf);
+        double *sf2 = mem.alloc<double>(2 * (size_t)nf), *sd2 = mem.alloc<double>(2 * (size_t)nf),
+               *su2 = mem.alloc<double>(2 * (size_t)nf);
+        if (!far2 || !sf2 || !sd2 || !su2) return DPM_ERR_CUDA;
+        k_tvd_context<<<nblk(nf), TPB, 0, st>>>(d, far2, sf2, sd2, su2);
+        launches++;
+        d.tvd_far = far2; d.tvd_sf = sf2; d.tvd_sd = sd2; d.tvd_su = su2;
+      }
+    }
     // fields
     F.U = mem.alloc<double>(3 * nc);
     F.p = mem.alloc<double>(nc); F.p_old = mem.alloc<double>(nc); F.phi_prev = mem.alloc<double>(nc);
@@ -362,6 +376,8 @@ struct Solver {
     scratch_c = mem.alloc<double>(nc); scratch_c2 = mem.alloc<double>(nc);
     aos_buf = mem.alloc<double>(9 * (size_t)std::max(nc, nf));
     conv_tmp = mem.alloc<double>(3 * nc); visc_tmp = mem.alloc<double>(3 * nc);
+    U_spare = mem.alloc<double>(3 * (size_t)nc);
+    if (!U_spare) return DPM_ERR_CUDA;
     cg_r = mem.alloc<double>(nc); cg_z = mem.alloc<double>(nc); cg_p0 = mem.alloc<double>(nc);
     cg_p1 = mem.alloc<double>(nc); cg_q = mem.alloc<double>(nc); cg_bp = mem.alloc<double>(nc);
     cg_x = mem.alloc<double>(nc);
@@ -574,14 +590,21 @@ struct Solver {
   }
 
   void explicit_rhs(double dt, double a_k, double b_k, int predict) {
-    k_face_explicit<<<nblk(nf), TPB, 0, st>>>(d, P.scheme, P.nu, F.U, F.Ub, F.gU, F.nu_sgs, F.Uf, F.fadv, F.fvis, F.fdiv);
     ExplicitArgs a{};
     a.scheme = P.scheme;
     a.f0 = P.f_const[0]; a.f1 = P.f_const[1]; a.f2 = P.f_const[2];
     a.bous = P.boussinesq; a.beta = P.beta; a.T_ref = P.T_ref; a.g0 = P.g[0]; a.g1 = P.g[1]; a.g2 = P.g[2];
     a.dt = dt; a.a_k = a_k; a.b_k = b_k; a.predict = predict;
-    k_cell_explicit<<<nblk(nc), TPB, 0, st>>>(d, a, F.U, F.T, F.fadv, F.fvis, F.fdiv, F.tau, F.H, F.H0,
-                                                predict ? nullptr : conv_tmp, predict ? nullptr : visc_tmp);
+    if (predict) {  // cell-owned fused pass, predicted velocity into the spare buffer
+      k_cell_momentum<<<nblk(nc), TPB, 0, st>>>(d, a, P.nu, F.U, F.Ub, F.gU, F.nu_sgs, F.Uf, F.T, F.tau, F.H, F.H0,
+                                                U_spare);
+      launches++;
+      std::swap(F.U, U_spare);
+      return;
+    }
+    k_face_explicit<<<nblk(nf), TPB, 0, st>>>(d, P.scheme, P.nu, F.U, F.Ub, F.gU, F.nu_sgs, F.Uf, F.fadv, F.fvis, F.fdiv);
+    k_cell_explicit<<<nblk(nc), TPB, 0, st>>>(d, a, F.U, F.T, F.fadv, F.fvis, F.fdiv, F.tau, F.H, F.H0, conv_tmp,
+                                                visc_tmp);
     launches += 2;
   }
 
@@ -698,7 +721,6 @@ struct Solver {
   }
   // cell gradients of U, of T when it is transported, and of every passive scalar
   void grad_all() {
-    grad_U();
     LsScalarSet q{};  // temperature and passive scalars: one pass over the LS weights
     if (P.boussinesq) {
       q.phi[q.n] = F.T; q.pb[q.n] = Tb; q.g[q.n] = gT; q.n++;
@@ -706,15 +728,25 @@ struct Solver {
     for (int k = 0; k < ns; ++k) {
       q.phi[q.n] = Cs + (size_t)k * nc; q.pb[q.n] = Cb + (size_t)k * nb; q.g[q.n] = gC + (size_t)k * 3 * nc; q.n++;
     }
-    if (q.n > 0 && gg()) {
-      GgScalarSet h{};
-      h.n = q.n;
-      for (int k = 0; k < q.n; ++k) { h.phi[k] = q.phi[k]; h.pb[k] = q.pb[k]; h.g[k] = q.g[k]; }
-      gg_scalars(h);
-    } else if (q.n > 0) {
-      k_ls_gradient_scalars<<<nblk(nc), TPB, 0, st>>>(d, q);
-      launches++;
+    if (gg() || q.n == 0) {
+      grad_U();
+      if (q.n > 0) {
+        GgScalarSet h{};
+        h.n = q.n;
+        for (int k = 0; k < q.n; ++k) { h.phi[k] = q.phi[k]; h.pb[k] = q.pb[k]; h.g[k] = q.g[k]; }
+        gg_scalars(h);
+      }
+      return;
     }
+    // least squares: U, T and the scalars in one pass over the stencil weights
+    switch (q.n) {
+      case 1: k_ls_gradient_all<1><<<nblk(nc), TPB, 0, st>>>(d, F.U, F.Ub, F.gU, q); break;
+      case 2: k_ls_gradient_all<2><<<nblk(nc), TPB, 0, st>>>(d, F.U, F.Ub, F.gU, q); break;
+      case 3: k_ls_gradient_all<3><<<nblk(nc), TPB, 0, st>>>(d, F.U, F.Ub, F.gU, q); break;
+      case 4: k_ls_gradient_all<4><<<nblk(nc), TPB, 0, st>>>(d, F.U, F.Ub, F.gU, q); break;
+      default: k_ls_gradient_all<5><<<nblk(nc), TPB, 0, st>>>(d, F.U, F.Ub, F.gU, q); break;
+    }
+    launches++;
   }
   // explicit right-hand side and RK3W update of T and the scalars (after the momentum predictor,
   // which reads the old T for the buoyancy term)
@@ -819,7 +851,7 @@ struct Solver {
     // an aggregate holds up to 3^passes rows and the restriction gives it at most 32 lanes
     if (P.p_ml_passes > 3) return DPM_ERR_ARG;
     int rc = ml.setup(nc, S.WA, S.A_col.data(), S.A_val.data(), d.Acol, d.Aval, nullsp, P.p_ml_passes, P.p_ml_degree,
-                      P.p_ml_overcorrect, dev_sms, cg_bar, cg_status, cg_dout);
+                      P.p_ml_overcorrect, dev_sms, cg_bar, cg_status, cg_dout, P.p_ml_value_bits);
     if (rc) return rc;
     if (P.p_stall_window > 0) ml.base.stall_window = P.p_stall_window;
     if (P.p_stall_ratio > 0.0) ml.base.stall_ratio = P.p_stall_ratio;

@@ -215,29 +215,77 @@ int dense_inverse(const Csr& A, bool nullsp, std::vector<float>& out) {
   return 0;
 }
 
+// IEEE binary16 bits of a finite double, round to nearest even (subnormals included; values
+// beyond the largest finite half saturate to it).
+unsigned short half_bits(double v) {
+  const unsigned short sign = std::signbit(v) ? 0x8000 : 0;
+  double a = std::fabs(v);
+  if (a >= 65504.0) return sign | 0x7bff;
+  if (a < std::ldexp(1.0, -24) * 0.5) return sign;
+  int e;
+  std::frexp(a, &e);  // a = m 2^e, m in [0.5, 1)
+  int ex = e - 1;     // a = (1.f) 2^ex
+  if (ex < -14) ex = -14;  // subnormal range: fixed exponent, 10-bit fraction of 2^-24 units
+  const double q = std::ldexp(a, 10 - ex);  // value in units of the last place
+  double r = std::nearbyint(q);             // round half to even (default rounding mode)
+  unsigned mant = (unsigned)r;
+  if (mant >= 2048) { mant >>= 1; ex += 1; }  // rounding carried into the next binade
+  if (ex > 15) return sign | 0x7bff;
+  if (mant < 1024) return sign | (unsigned short)mant;  // subnormal (ex == -14)
+  return sign | (unsigned short)(((ex + 15) << 10) | (mant - 1024));
+}
+
+double half_value(unsigned short h) {
+  const int e = (h >> 10) & 0x1f, f = h & 0x3ff;
+  const double m = e == 0 ? std::ldexp((double)f, -24) : std::ldexp(1024.0 + f, e - 25);
+  return (h & 0x8000) ? -m : m;
+}
+
 MlLevel make_level(const Csr& A, const std::vector<int>& agg, int na, int& rc) {
   MlLevel L;
   rc = 0;
   L.n = A.n;
   for (int i = 0; i < A.n; ++i) L.W = std::max<int>(L.W, (int)(A.off[i + 1] - A.off[i]));
-  L.col.resize((size_t)L.W * A.n);
-  L.val.assign((size_t)L.W * A.n, 0.0f);
   L.dinv.resize(A.n);
   std::vector<double> dinv(A.n, 0.0);
   for (int i = 0; i < A.n; ++i) {
-    int s = 0;
     double dg = 0.0;
-    for (int64_t k = A.off[i]; k < A.off[i + 1]; ++k, ++s) {
-      L.col[(size_t)s * A.n + i] = A.col[k];
-      L.val[(size_t)s * A.n + i] = (float)A.val[k];
+    for (int64_t k = A.off[i]; k < A.off[i + 1]; ++k)
       if (A.col[k] == i) dg = A.val[k];
-    }
-    for (; s < L.W; ++s) L.col[(size_t)s * A.n + i] = i;
     if (!(dg > 0.0)) rc = -5;
     dinv[i] = dg > 0.0 ? 1.0 / dg : 0.0;
     L.dinv[i] = (float)dinv[i];
   }
   L.lmax = lambda_max(A, dinv);
+  // scaled off-diagonal form of the smoother
+  for (int i = 0; i < A.n; ++i) L.Wo = std::max<int>(L.Wo, (int)(A.off[i + 1] - A.off[i]) - 1);
+  L.Wo = std::max(L.Wo, 1);
+  L.ocol.resize((size_t)L.Wo * A.n);
+  L.sv32.assign((size_t)L.Wo * A.n, 0.0f);
+  L.sv16.assign((size_t)L.Wo * A.n, 0);
+  L.g32.resize(A.n);
+  L.g16.resize(A.n);
+  L.diag.resize(A.n);
+  for (int i = 0; i < A.n; ++i) {
+    int s = 0;
+    double d32 = 1.0, d16 = 1.0;
+    for (int64_t k = A.off[i]; k < A.off[i + 1]; ++k) {
+      if (A.col[k] == i) continue;
+      const double sij = A.val[k] * dinv[i];
+      const float f = (float)sij;
+      const unsigned short h = half_bits(sij);
+      L.ocol[(size_t)s * A.n + i] = A.col[k];
+      L.sv32[(size_t)s * A.n + i] = f;
+      L.sv16[(size_t)s * A.n + i] = h;
+      d32 += sij - (double)f;
+      d16 += sij - half_value(h);
+      ++s;
+    }
+    for (; s < L.Wo; ++s) L.ocol[(size_t)s * A.n + i] = i;
+    L.g32[i] = (float)d32;
+    L.g16[i] = (float)d16;
+    L.diag[i] = (float)(dinv[i] > 0.0 ? 1.0 / dinv[i] : 0.0);
+  }
   L.agg = agg;
   std::vector<int64_t> moff;
   std::vector<int> mrow;

@@ -20,10 +20,19 @@ constexpr int ML_MAX_LEVELS = 12;
 constexpr int ML_MAX_DEGREE = 8;
 
 struct MlLevel {
-  int n = 0, W = 0, M = 0;        // rows, ELL width, members per aggregate (of the next level)
-  std::vector<int> col;           // [W][n], padded (own row, 0)
-  std::vector<float> val;         // [W][n]
+  int n = 0, W = 0, M = 0;        // rows, widest row (diagonal included), members per aggregate
   std::vector<float> dinv;        // [n]
+  // The same operator as the smoother reads it: off-diagonal entries only, scaled by the row's
+  // diagonal (D^-1 A = G + S), in ELL [Wo][n] padded with (own row, 0).  sv32 holds s_ij in FP32,
+  // sv16 the IEEE binary16 bits of s_ij (round to nearest even); g32 / g16 the diagonal term of
+  // the scaled row, 1 + sum_j (s_ij - stored s_ij), so that every stored row sums to the same
+  // value as the exact one (a rounded off-diagonal would otherwise shift the near-null space).
+  int Wo = 0;
+  std::vector<int> ocol;          // [Wo][n]
+  std::vector<float> sv32;        // [Wo][n]
+  std::vector<unsigned short> sv16;  // [Wo][n]
+  std::vector<float> g32, g16;    // [n]
+  std::vector<float> diag;        // [n] a_ii
   std::vector<int> agg;           // [n] row of the next level this row belongs to
   std::vector<int> mem;           // [M][n_next] rows of this level in each aggregate, -1 padded
   double lmax = 0.0;              // estimate of the largest eigenvalue of D^-1 A

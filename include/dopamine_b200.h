@@ -166,6 +166,10 @@ typedef struct dpm_params {
    * iterate (dpm_stats_t.p_fallbacks).  Zero / non-positive: 50 iterations, ratio 0.9. */
   int p_stall_window;
   double p_stall_ratio;
+  /* DPM_PSOLVER_MULTILEVEL_FCG: storage of the smoother's D^-1-scaled off-diagonal entries, 16
+   * (binary16, with a per-row diagonal term that keeps each stored row's sum exact) or 32 (FP32);
+   * 0: 32. */
+  int p_ml_value_bits;
 } dpm_params_t;
 
 /* Per-step integral statistics (src/stats/mod_stats.f90:compute_stats_sums and

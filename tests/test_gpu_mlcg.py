@@ -152,3 +152,34 @@ def test_auto_picks_the_form_that_fits():
         s.close()
     # same relative stopping rule: the divergence left is of the plain form's order
     assert div[abi.PSOLVER_AUTO] <= 10 * div[abi.PSOLVER_JACOBI_PCG] + 1e-12, div
+
+
+@pytest.mark.parametrize("bits", [32, 16])
+def test_mlcg_streamed_levels_match_plain_pcg(bits):
+    """A mesh large enough that the fine level streams its row tiles through shared memory (at
+    least 4 rows per thread of the cooperative grid): the multilevel form, with the smoother's
+    scaled off-diagonals in FP32 and in binary16, against the plain FP64 Jacobi-PCG path (which
+    the parity tests pin to the oracle) at a tight tolerance."""
+    case = cases.channel_config(nx=128, ny=96, nz=64, n_steps=2)
+    ref = None
+    for form in (abi.PSOLVER_JACOBI_PCG, abi.PSOLVER_MULTILEVEL_FCG):
+        p = case.make_params()
+        p.p_tol = 1e-13
+        p.p_solver = form
+        p.p_ml_value_bits = bits
+        s = Solver(case, params=p)
+        s.initialise()
+        s.advance()
+        s.advance()
+        U = s.sync_host()["U"]
+        st = s.stats()
+        s.close()
+        if ref is None:
+            ref = U
+            continue
+        err = np.linalg.norm(U - ref) / np.linalg.norm(ref)
+        its = st["p_iters"] / st["p_solves"]
+        print(f"streamed multilevel ({bits}-bit smoother), 786k cells: U rel {err:.2e}, {its:.1f} its/solve")
+        assert err <= 1e-9, err
+        assert st["max_abs_divU"] <= 1e-8
+        assert its <= 60, its
