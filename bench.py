@@ -107,10 +107,12 @@ FORMS = {"pcg": "plain FP64 Jacobi-PCG",
                 "degree 7 in shared memory + one coarse value per part)"}
 
 
-FORMS["ml"] = ("FP64 flexible CG preconditioned by one FP32 aggregation-multigrid V-cycle (pairwise "
-               "aggregation, 3 passes per level, Chebyshev degree 3, dense coarsest level)")
+FORMS["ml"] = ("FP64 flexible CG preconditioned by one aggregation-multigrid V-cycle on D^-1-scaled FP32 levels "
+               "(pairwise aggregation, 3 passes per level, dense coarsest level; meshes of >= 2^20 cells: "
+               "standalone full-occupancy kernels, Chebyshev degree 2; smaller: one persistent kernel, degree 3)")
 KERNELS = {"pcg": "k_pcg (persistent Jacobi-PCG)", "fcg": "k_fcg (persistent two-level flexible CG)",
-           "ml": "k_mlcg (persistent multilevel flexible CG)"}
+           "ml": "multilevel flexible CG (k_mlk_* standalone kernels on >= 2^20 cells, else persistent k_mlcg): "
+                 "whole pressure solve"}
 
 
 CONFIG_NAMES = {
@@ -228,26 +230,6 @@ def cpu_run(case_name, budget_s, max_steps):
                        f"on {phys if phys else 'an unknown number of'} physical cores")
 
 
-def pcg_bytes_per_iteration(s, psolver="pcg"):
-    """Algorithmic bytes of one Krylov iteration, per the ELL operator width (hex: 7)."""
-    nc = s.nc
-    wa = 7  # hex mesh: diagonal + 6 neighbours
-    if psolver == "ml":
-        # fine level only (the coarser levels add about 1/7): 2k = 6 FP32 smoothing/restriction
-        # passes (cols + FP32 vals, b, d in/out, x in/out), the FP64 w = A z pass (cols, vals, z,
-        # r, q in, w out) and the update pass (z, w, p, q, x, r in; p, q, x, r out; b, d, x0 out)
-        k = 3
-        return nc * (2 * k * (wa * (4 + 4) + 16) + (wa * (4 + 8) + 4 + 8 + 16) + (12 + 32 + 32 + 12))
-    if psolver == "fcg":
-        # w = A z: cols + vals, z gathered once per cell, z written once; the part-local smoother
-        # and the own-cell vectors live in shared memory and registers
-        # plus the deflation data (row sum, cross-coupling offsets) of the own rows
-        return nc * (wa * (4 + 8) + 8 + 8 + 8)
-    phase_a = nc * (wa * (4 + 8) + 8 + 8 + 8 + 8)   # cols, vals, z, p_old, write p_new, write q
-    phase_b = nc * (5 * 8 + 3 * 8)                  # x, p, r, q, dinv in; x, r, z out
-    return phase_a + phase_b
-
-
 PROFILE = {("pcg", "channel"): "k_pcg_channel96x64x64.md", ("fcg", "channel"): "k_fcg_channel96x64x64.md",
            ("ml", "channel"): "k_mlcg_channel96x64x64.md", ("ml", "urban"): "k_mlcg_urban.md"}
 
@@ -338,6 +320,9 @@ def run_gpu(args, rank, world):
         solves += st["p_solves"]
     launches = s.kernel_launches() - l0
     t_dev = sum(step_ms) / 1e3
+    # algorithmic bytes per Krylov iteration of the timed form, as the library counts them from
+    # its operator and (multilevel) hierarchy
+    bytes_it = s.stats()["p_bytes_per_iteration"]
     # ---- end to end through the C ABI with host buffers: the transported state (U, p, T when it
     # is transported, the passive scalars) goes up from pinned host memory and comes back every step
     L = lib()
@@ -392,6 +377,7 @@ def run_gpu(args, rank, world):
                      pcg_iterations_per_step=pit / len(pm), steps=len(pm))
         s.select_pressure_solver(3)
     return dict(nc=nc, t_dev=t_dev, t_e2e=t_e2e, step_ms=step_ms, pois_ms=pois_ms, its=its, solves=solves,
+                bytes_it=bytes_it,
                 launches=launches, clocks=clocks, solver=s, learn=learn, fallbacks=s.stats()["p_fallbacks"],
                 e2e_bytes=bytes_per_dir, plain=plain)
 
@@ -457,7 +443,7 @@ def main():
     value = whole_job_rate(world, nc, K, r["t_dev"])
     e2e = whole_job_rate(world, nc, K, r["t_e2e"])
     peak, peak_kind = measured_peaks()
-    bytes_it = pcg_bytes_per_iteration(s, args.psolver)
+    bytes_it = r["bytes_it"]
     pois_s = sum(r["pois_ms"]) / 1e3
     achieved = bytes_it * r["its"] / pois_s / 1e9 if pois_s > 0 else 0.0
     its_per_solve = r["its"] / max(r["solves"], 1)

@@ -75,6 +75,7 @@ class StatsT(C.Structure):
         ("tauw_mean", C.c_double), ("nu_sgs_mean", C.c_double), ("max_abs_divU", C.c_double),
         ("volavg_abs_divU", C.c_double), ("dt_used", C.c_double), ("p_solves", C.c_int), ("p_iters", C.c_int),
         ("p_resid_max", C.c_double), ("p_fallbacks", C.c_int), ("p_solver_used", C.c_int),
+        ("p_bytes_per_iteration", C.c_double),
     ]
 
     def as_dict(self):

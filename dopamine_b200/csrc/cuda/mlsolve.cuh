@@ -11,6 +11,7 @@
 #include "../../../include/dopamine_b200.h"
 #include "../host/multilevel.hpp"
 #include "mlcg.cuh"
+#include "mlkern.cuh"
 
 namespace dpm {
 namespace gpu {
@@ -21,6 +22,19 @@ struct MlSolver {
   std::vector<int> sizes;      // rows per level, coarsest last
   std::vector<void*> owned;    // device allocations of this object
   int spin_limit_override = 0;  // > 0: poll limit of the kernel's grid-wide waits (status[3])
+  // Multi-kernel form (mlkern.cuh) for fine levels of at least kernels_min_rows rows: the levels
+  // on the host for by-value launches, the Krylov state, partial sums, a residual scratch vector,
+  // and a pinned stop flag per batch of iterations with its event.
+  static constexpr int kernels_min_rows = 1 << 20;
+  static constexpr int iters_per_batch = 2;
+  bool multi = false;
+  double bytes_per_iteration = 0.0;  // algorithmic bytes of one Krylov iteration (roofline numerator)
+  std::vector<MlDevLevel> hlv;
+  MlkState* dS = nullptr;
+  double* kpart = nullptr;
+  float* kres = nullptr;
+  int* h_flag = nullptr;  // pinned, 2 entries
+  cudaEvent_t kev[2] = {nullptr, nullptr};
   bool half_values = false;     // smoother off-diagonals in binary16 (else FP32)
   void* kernel() const { return half_values ? (void*)k_mlcg<unsigned short> : (void*)k_mlcg<float>; }
 
@@ -32,6 +46,13 @@ struct MlSolver {
   void release() {
     for (void* p : owned) cudaFree(p);
     owned.clear();
+    if (h_flag) cudaFreeHost(h_flag);
+    h_flag = nullptr;
+    for (auto& e : kev)
+      if (e) { cudaEventDestroy(e); e = nullptr; }
+    multi = false;
+    hlv.clear();
+    dS = nullptr; kpart = nullptr; kres = nullptr;
     base = MlArgs{};
     grid = 0;
     sizes.clear();
@@ -66,7 +87,12 @@ struct MlSolver {
     if (build_multilevel(n, WA, h_col, h_val, nullsp, passes > 0 ? passes : 3, 0.25, 300, 1024, M))
       return DPM_ERR_UNSUPPORTED;
     const int nlev = (int)M.lv.size();
-    const int deg = degree > 0 ? degree : 3;
+    // Chebyshev steps per smoothing: 3 for the persistent kernel (each step costs a grid-wide
+    // barrier there), 2 for the multi-kernel form of large meshes, where the sweeps are bandwidth-
+    // bound (measured on the 19.3M-cell urban mesh: 294 vs 322 ms of Poisson solve per step,
+    // 113 vs 96 iterations)
+    const bool multi_form = n >= kernels_min_rows;
+    const int deg = degree > 0 ? degree : (multi_form ? 2 : 3);
     if (nlev > ML_LEVELS || deg > ML_DEG) return DPM_ERR_ARG;
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel(), ML_TPB, 0) != cudaSuccess || per_sm < 1)
@@ -136,6 +162,116 @@ struct MlSolver {
     base = a;
     sizes = M.sizes;
     grid = g;
+    multi = multi_form && nlev > 0;
+    // algorithmic bytes of one iteration (each array touched once per pass): per level and V-cycle
+    // deg - 1 down sweeps, the residual, the restriction, the prolongation and deg up sweeps (the
+    // first without the old direction); the coarse solve; the FP64 w = A z pass with the sums;
+    // the vector update with level 0's first step
+    {
+      const double svb = half_values ? 2.0 : 4.0;
+      double bytes = 0.0;
+      for (int l = 0; l < nlev; ++l) {
+        const MlLevel& L = M.lv[l];
+        const double nl = L.n, row = L.Wo * (4.0 + svb);
+        const double nn = l + 1 < nlev ? M.lv[l + 1].n : M.nC;
+        const double sweep = nl * (row + 24.0), first = nl * (row + 20.0), resid = nl * (row + 20.0);
+        const double restrict_ = nn * (L.M * 4.0 + 16.0) + nl * 4.0, prolong = nl * 12.0;
+        bytes += (2.0 * deg - 2.0) * sweep + first + resid + restrict_ + prolong;
+      }
+      bytes += (double)M.nC * M.nC * 4.0 + 8.0 * M.nC;
+      bytes += (double)n * (WA * 12.0 + 28.0) + (double)n * 92.0;
+      bytes_per_iteration = bytes;
+    }
+    if (multi) {
+      hlv = hl;
+      dS = alloc<MlkState>(1);
+      kpart = alloc<double>((size_t)MLK_RED_BLOCKS * MLK_NV);
+      kres = alloc<float>(hl[0].n);
+      if (!dS || !kpart || !kres) return DPM_ERR_CUDA;
+      if (cudaHostAlloc(&h_flag, 2 * sizeof(int), cudaHostAllocDefault) != cudaSuccess) return DPM_ERR_CUDA;
+      for (auto& e : kev)
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return DPM_ERR_CUDA;
+    }
+    return 0;
+  }
+
+  template <class SV>
+  void enqueue_iteration(const MlArgs& a, int G, cudaStream_t st) {
+    const int nlev = a.nlev, deg = a.degree;
+    auto nb = [](int64_t m) { return (int)((m + MLK_TPB - 1) / MLK_TPB); };
+    unsigned curmask = 0;
+    for (int l = 0; l < nlev; ++l) {
+      const MlDevLevel& L = hlv[l];
+      int cur = 0;
+      for (int j = 1; j < deg; ++j) {
+        k_mlk_sweep<SV><<<nb(L.n), MLK_TPB, 0, st>>>(L, L.c1[j], L.c2[j], 0, cur ? L.x1 : L.x0, cur ? L.x0 : L.x1,
+                                                     nullptr, 0.0f, dS);
+        cur ^= 1;
+      }
+      curmask |= (unsigned)cur << l;
+      const bool last = l + 1 == nlev;
+      k_mlk_resid<SV><<<nb(L.n), MLK_TPB, 0, st>>>(L, cur ? L.x1 : L.x0, kres, dS);
+      k_mlk_restrict<<<nb(L.n_next), MLK_TPB, 0, st>>>(L, kres, last ? L : hlv[l + 1], last ? 1 : 0, a.bC, dS);
+    }
+    k_mlk_coarse<<<nb((int64_t)a.nC * 32), MLK_TPB, 0, st>>>(a.nC, a.cinv, a.bC, a.xC, dS);
+    const float* xcoarse = a.xC;
+    for (int l = nlev - 1; l >= 0; --l) {
+      const MlDevLevel& L = hlv[l];
+      int cur = (curmask >> l) & 1u;
+      k_mlk_prolong<<<nb(L.n), MLK_TPB, 0, st>>>(L, cur ? L.x1 : L.x0, xcoarse, a.oc, dS);
+      for (int j = 0; j < deg; ++j) {
+        const float* om = (l == 0 && j == deg - 1 && a.gamma != 0.0f) ? a.omega : nullptr;
+        k_mlk_sweep<SV><<<nb(L.n), MLK_TPB, 0, st>>>(L, L.c1[j], L.c2[j], j == 0 ? 1 : 0, cur ? L.x1 : L.x0,
+                                                     cur ? L.x0 : L.x1, om, a.gamma, dS);
+        cur ^= 1;
+      }
+      xcoarse = cur ? L.x1 : L.x0;
+    }
+    const float* z = xcoarse;
+    if (a.rec_stride > 0) k_mlk_record<<<G, MLK_TPB, 0, st>>>(a, z, hlv[0].b, dS);
+    k_mlk_wz<float><<<G, MLK_TPB, 0, st>>>(a, z, kpart, dS);
+    k_mlk_rule<<<1, 32 * MLK_NV, 0, st>>>(a.n, G, kpart, dS);
+    k_mlk_update<float><<<nb(a.n), MLK_TPB, 0, st>>>(a, z, a.lv, dS);
+    k_mlk_next<<<1, 1, 0, st>>>(dS);
+  }
+
+  // The solve as standalone kernels: start, then batches of iters_per_batch iterations with the
+  // stop flag of each batch read back while the next batch runs, then the true residual.
+  int launch_multi(MlArgs& a, cudaStream_t st, int* reason, int* its, double* resid) {
+    MlkState h{};
+    h.rtol = a.rtol; h.atol = a.atol; h.maxit = a.maxit; h.nullsp = a.nullsp; h.guess_zero = a.guess_zero;
+    h.stall_window = a.stall_window; h.stall_ratio = a.stall_ratio;
+    if (cudaMemcpyAsync(dS, &h, sizeof(h), cudaMemcpyHostToDevice, st) != cudaSuccess) return DPM_ERR_CUDA;
+    const int G = std::min((a.n + MLK_TPB - 1) / MLK_TPB, MLK_RED_BLOCKS);
+    k_mlk_init_sum<<<G, MLK_TPB, 0, st>>>(a.n, a.b, a.x, a.guess_zero, kpart);
+    k_mlk_init_mean<<<1, 32, 0, st>>>(a.n, G, kpart, dS);
+    k_mlk_init_resid<<<G, MLK_TPB, 0, st>>>(a, a.lv, dS, kpart);
+    k_mlk_init_rule<<<1, 64, 0, st>>>(G, kpart, dS);
+    const int max_batches = (std::max(a.maxit, 0) + iters_per_batch - 1) / iters_per_batch + 1;
+    for (int bt = 0; bt < max_batches; ++bt) {
+      for (int k = 0; k < iters_per_batch; ++k) {
+        if (half_values) enqueue_iteration<unsigned short>(a, G, st);
+        else enqueue_iteration<float>(a, G, st);
+      }
+      if (cudaMemcpyAsync(&h_flag[bt & 1], &dS->done, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+          cudaEventRecord(kev[bt & 1], st) != cudaSuccess)
+        return DPM_ERR_CUDA;
+      if (bt > 0) {  // the previous batch's flag, read while this batch runs
+        if (cudaEventSynchronize(kev[(bt - 1) & 1]) != cudaSuccess) return DPM_ERR_CUDA;
+        if (h_flag[(bt - 1) & 1]) break;
+      }
+    }
+    if (cudaGetLastError() != cudaSuccess) return DPM_ERR_CUDA;
+    k_mlk_true_resid<<<G, MLK_TPB, 0, st>>>(a, kpart);
+    k_mlk_finish<<<1, 32, 0, st>>>(G, kpart, dS, a.status, a.dout);
+    int h_st[4];
+    double h_d[4];
+    if (cudaMemcpyAsync(h_st, a.status, 4 * sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess) return DPM_ERR_CUDA;
+    if (cudaMemcpyAsync(h_d, a.dout, 4 * sizeof(double), cudaMemcpyDeviceToHost, st) != cudaSuccess) return DPM_ERR_CUDA;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return DPM_ERR_CUDA;
+    *reason = h_st[0];
+    *its = h_st[1];
+    *resid = h_d[0];
     return 0;
   }
 
@@ -152,6 +288,7 @@ struct MlSolver {
       a.rec_r = extra->rec_r; a.rec_z = extra->rec_z; a.rec_u = extra->rec_u; a.rec_x = extra->rec_x;
     }
     a.b = b; a.x = x; a.rtol = rtol; a.atol = atol; a.maxit = maxit; a.guess_zero = guess_zero;
+    if (multi) return launch_multi(a, st, reason, its, resid);
     if (cudaMemsetAsync(a.bar, 0, 2 * sizeof(unsigned), st) != cudaSuccess) return DPM_ERR_CUDA;
     if (cudaMemsetAsync(a.status, 0, 4 * sizeof(int), st) != cudaSuccess) return DPM_ERR_CUDA;
     if (spin_limit_override &&

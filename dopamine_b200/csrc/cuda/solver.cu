@@ -1545,6 +1545,16 @@ struct Solver {
     s->p_solver_used = force_plain ? DPM_PSOLVER_JACOBI_PCG
                                    : (use_fcg ? DPM_PSOLVER_TWOLEVEL_FCG
                                               : (use_ml ? DPM_PSOLVER_MULTILEVEL_FCG : DPM_PSOLVER_JACOBI_PCG));
+    // algorithmic bytes per Krylov iteration: Jacobi-PCG phase A (row of A, z gathered, p old /
+    // new, q) and phase B (x, p, r, q, 1/diag in; x, r, z out); two-level FCG w = A z (row of A, z
+    // gathered and written, deflation row data: the smoother runs in shared memory and registers);
+    // multilevel from its hierarchy
+    {
+      const double n = nc, wa = S.WA;
+      if (s->p_solver_used == DPM_PSOLVER_MULTILEVEL_FCG) s->p_bytes_per_iteration = ml.bytes_per_iteration;
+      else if (s->p_solver_used == DPM_PSOLVER_TWOLEVEL_FCG) s->p_bytes_per_iteration = n * (wa * 12.0 + 24.0);
+      else s->p_bytes_per_iteration = n * (wa * 12.0 + 32.0) + n * 64.0;
+    }
     s->p_solves = last.p_solves;
     s->p_iters = last.p_iters;
     s->p_resid_max = last.p_resid_max;

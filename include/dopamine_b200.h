@@ -182,6 +182,9 @@ typedef struct dpm_stats {
   double p_resid_max;
   int p_fallbacks;            /* pressure solves handed from flexible CG to plain PCG (total)   */
   int p_solver_used;          /* DPM_PSOLVER_* of the pressure solve in use (never AUTO)      */
+  double p_bytes_per_iteration;  /* algorithmic bytes one Krylov iteration of that solve moves
+                                    (each array read or written once per pass): the roofline
+                                    numerator of the pressure solve                           */
 } dpm_stats_t;
 
 /* Outcome of dpm_learn_train. */

@@ -2270,6 +2270,7 @@ struct Solver {
     s->p_resid_max = last_resid;
     s->p_fallbacks = 0;
     s->p_solver_used = DPM_PSOLVER_JACOBI_PCG;
+    s->p_bytes_per_iteration = 0.0;  // no device traffic on the CPU
     apply_velocity_bc(-1, false);  // solver_divergence_metrics refreshes U_bnd without gradients
   }
 };
