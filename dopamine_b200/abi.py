@@ -130,7 +130,7 @@ def default_params(**kw):
     p.abl_T_surface = 300.0
     p.abl_L_obukhov = 0.0
     p.abl_compute_L = 1
-    p.p_ml_degree = 3
+    p.p_ml_degree = 0  # library default: 2 in the multi-kernel form (>= 2^20 cells), 3 in the persistent one
     p.p_ml_overcorrect = 1.6
     p.p_ml_passes = 3
     p.gradient_scheme = GRAD_LEAST_SQUARES

@@ -215,7 +215,9 @@ static __global__ void __launch_bounds__(MLK_TPB) k_mlk_record(MlArgs a, const f
   }
 }
 
-// ---- w = A z (FP64 operator) and the eight sums of the iteration
+// ---- w = A z (FP64 operator) and the eight sums of the iteration: one row per thread (as the
+// sweeps; a grid-stride loop over ~32 rows per thread ran at half the bandwidth), per-block
+// partials folded by k_mlk_fold before the scalar kernel
 template <class ZT>
 static __global__ void __launch_bounds__(MLK_TPB) k_mlk_wz(MlArgs a, const ZT* __restrict__ z, double* part,
                                                     const MlkState* S) {
@@ -223,7 +225,8 @@ static __global__ void __launch_bounds__(MLK_TPB) k_mlk_wz(MlArgs a, const ZT* _
   double v[MLK_NV];
 #pragma unroll
   for (int k = 0; k < MLK_NV; ++k) v[k] = 0.0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < a.n) {
     const double wi = ml_row64(a, i, z);
     const double zi = (double)__ldcg(&z[i]), qi = __ldcg(&a.q[i]), ri = __ldcg(&a.r[i]);
     a.w[i] = wi;
@@ -237,6 +240,17 @@ static __global__ void __launch_bounds__(MLK_TPB) k_mlk_wz(MlArgs a, const ZT* _
     v[7] += wi;
   }
   mlk_block_partials<MLK_NV>(v, part);
+}
+// block b sums partials b*256 .. b*256+255 (fixed order), NV values each
+template <int NV>
+static __global__ void __launch_bounds__(MLK_TPB) k_mlk_fold(int nparts, const double* __restrict__ in, double* out,
+                                                      const MlkState* S) {
+  if (S->done) return;
+  double v[NV];
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+#pragma unroll
+  for (int k = 0; k < NV; ++k) v[k] = j < nparts ? in[(size_t)j * NV + k] : 0.0;
+  mlk_block_partials<NV>(v, out);
 }
 // the FCG scalars and the stopping rule (k_mlcg's, after its reduce-and-gather)
 static __global__ void k_mlk_rule(int n, int nparts, const double* part, MlkState* S) {

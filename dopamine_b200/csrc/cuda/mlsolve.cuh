@@ -32,6 +32,7 @@ struct MlSolver {
   std::vector<MlDevLevel> hlv;
   MlkState* dS = nullptr;
   double* kpart = nullptr;
+  double* kpart2 = nullptr;  // per-block partials of w = A z (one block per 256 rows)
   float* kres = nullptr;
   int* h_flag = nullptr;  // pinned, 2 entries
   cudaEvent_t kev[2] = {nullptr, nullptr};
@@ -52,7 +53,7 @@ struct MlSolver {
       if (e) { cudaEventDestroy(e); e = nullptr; }
     multi = false;
     hlv.clear();
-    dS = nullptr; kpart = nullptr; kres = nullptr;
+    dS = nullptr; kpart = nullptr; kpart2 = nullptr; kres = nullptr;
     base = MlArgs{};
     grid = 0;
     sizes.clear();
@@ -185,9 +186,11 @@ struct MlSolver {
     if (multi) {
       hlv = hl;
       dS = alloc<MlkState>(1);
-      kpart = alloc<double>((size_t)MLK_RED_BLOCKS * MLK_NV);
+      const int64_t nfold = (((int64_t)n + MLK_TPB - 1) / MLK_TPB + MLK_TPB - 1) / MLK_TPB;  // fold blocks of w = A z
+      kpart = alloc<double>((size_t)std::max<int64_t>(MLK_RED_BLOCKS, nfold) * MLK_NV);
       kres = alloc<float>(hl[0].n);
-      if (!dS || !kpart || !kres) return DPM_ERR_CUDA;
+      kpart2 = alloc<double>((size_t)((n + MLK_TPB - 1) / MLK_TPB) * MLK_NV);
+      if (!dS || !kpart || !kres || !kpart2) return DPM_ERR_CUDA;
       if (cudaHostAlloc(&h_flag, 2 * sizeof(int), cudaHostAllocDefault) != cudaSuccess) return DPM_ERR_CUDA;
       for (auto& e : kev)
         if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return DPM_ERR_CUDA;
@@ -229,8 +232,10 @@ struct MlSolver {
     }
     const float* z = xcoarse;
     if (a.rec_stride > 0) k_mlk_record<<<G, MLK_TPB, 0, st>>>(a, z, hlv[0].b, dS);
-    k_mlk_wz<float><<<G, MLK_TPB, 0, st>>>(a, z, kpart, dS);
-    k_mlk_rule<<<1, 32 * MLK_NV, 0, st>>>(a.n, G, kpart, dS);
+    const int nw = nb(a.n), nf = (nw + MLK_TPB - 1) / MLK_TPB;
+    k_mlk_wz<float><<<nw, MLK_TPB, 0, st>>>(a, z, kpart2, dS);
+    k_mlk_fold<MLK_NV><<<nf, MLK_TPB, 0, st>>>(nw, kpart2, kpart, dS);
+    k_mlk_rule<<<1, 32 * MLK_NV, 0, st>>>(a.n, nf, kpart, dS);
     k_mlk_update<float><<<nb(a.n), MLK_TPB, 0, st>>>(a, z, a.lv, dS);
     k_mlk_next<<<1, 1, 0, st>>>(dS);
   }
