@@ -17,7 +17,7 @@ LIB = os.path.join(OUT_DIR, "libdopamine_b200.so")
 CU_SOURCES = ["csrc/cuda/solver.cu", "csrc/cuda/fvm_petsc.cu", "csrc/cuda/noalloc.cu"]
 CPP_SOURCES = ["csrc/host/mesh.cpp", "csrc/host/ops.cpp", "csrc/host/twolevel.cpp", "csrc/host/multilevel.cpp"]
 HEADERS = ["csrc/cuda/common.cuh", "csrc/cuda/kernels.cuh", "csrc/cuda/pcg.cuh", "csrc/cuda/fcg.cuh",
-           "csrc/cuda/learn.cuh", "csrc/cuda/scalars.cuh", "csrc/cuda/mlcg.cuh", "csrc/cuda/mlsolve.cuh", "csrc/cuda/mlkern.cuh",
+           "csrc/cuda/learn.cuh", "csrc/cuda/scalars.cuh", "csrc/cuda/mlcg.cuh", "csrc/cuda/mlsolve.cuh", "csrc/cuda/mlkern.cuh", "csrc/cuda/explicit32.cuh",
            "csrc/host/twolevel.hpp", "csrc/host/multilevel.hpp", "csrc/host/mesh.hpp",
            "csrc/host/ops.hpp", "../include/dopamine_b200.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -23,6 +23,7 @@
 #include "../host/twolevel.hpp"
 #include "../host/multilevel.hpp"
 #include "common.cuh"
+#include "explicit32.cuh"
 #include "fcg.cuh"
 #include "kernels.cuh"
 #include "learn.cuh"
@@ -174,6 +175,11 @@ struct Solver {
   double *aos_buf = nullptr;
   double *conv_tmp = nullptr, *visc_tmp = nullptr;
   double* U_spare = nullptr;  // second velocity buffer: the fused explicit pass writes the prediction here
+  // precision form, explicit half in FP32 (explicit32.cuh): FP32 geometry, first-pass gradients,
+  // scalar face fluxes
+  bool x32 = false;
+  Geo32 g32{};
+  float *gU32 = nullptr, *gS32 = nullptr, *sc_fadv32 = nullptr, *sc_fdif32 = nullptr;
   // PCG workspace
   double *cg_r, *cg_z, *cg_p0, *cg_p1, *cg_q, *cg_bp, *cg_x, *cg_part, *cg_dout;
   void* cg_kernel = nullptr;
@@ -414,6 +420,8 @@ struct Solver {
     cg_part = mem.alloc<double>(8 * (size_t)cg_grid);
     {
       int rc = setup_scalars();
+      if (rc) return rc;
+      rc = setup_x32();
       if (rc) return rc;
     }
     if (P.p_solver == DPM_PSOLVER_TWOLEVEL_FCG) {
@@ -702,6 +710,117 @@ struct Solver {
     return 0;
   }
   int nfi_() const { return (int)m.n_int_faces; }
+
+  // The precision form's FP32 explicit half: FP32 copies of the static geometry and LS weights
+  // (made on the device from the FP64 arrays), FP32 first-pass gradients and scalar face fluxes.
+  // Schemes it provides: KEP, CDS, van Leer, Koren; least-squares gradients.
+  int setup_x32() {
+    if (P.form != DPM_FORM_MIXED) return 0;
+    auto ok_mom = [](int s) {
+      return s == DPM_SCHEME_KEP || s == DPM_SCHEME_CDS || s == DPM_SCHEME_VANLEER_TVD || s == DPM_SCHEME_KOREN_TVD;
+    };
+    auto ok_sc = [](int s) { return s == DPM_SCHEME_CDS || s == DPM_SCHEME_VANLEER_TVD || s == DPM_SCHEME_KOREN_TVD; };
+    if (!ok_mom(P.scheme) || (P.boussinesq && !ok_sc(P.temperature_scheme)) || (ns > 0 && !ok_sc(P.scalar_scheme)) ||
+        gg())
+      return DPM_ERR_UNSUPPORTED;
+    auto f32 = [&](const double* src, size_t n) -> const float* {
+      float* dst = mem.alloc<float>(n);
+      if (!dst || !src) return dst;
+      k_to_f32<<<(unsigned)((n + TPB - 1) / TPB), TPB, 0, st>>>((int64_t)n, src, dst);
+      launches++;
+      return dst;
+    };
+    g32.vol = f32(d.vol, nc); g32.ivol = f32(d.ivol, nc); g32.cen = f32(d.cen, 3 * (size_t)nc);
+    g32.G = f32(d.G, 9 * (size_t)nc); g32.ls_w = f32(d.ls_w, 3 * (size_t)d.W * nc);
+    g32.sf = f32(d.sf, 3 * (size_t)nf); g32.nrm = f32(d.nrm, 3 * (size_t)nf); g32.fcen = f32(d.fcen, 3 * (size_t)nf);
+    g32.eps = f32(d.eps, 3 * (size_t)nf); g32.area = f32(d.area, nf); g32.gc = f32(d.gc, nf);
+    g32.wbl = f32(d.wbl, nf); g32.dcf = f32(d.dcf, nf);
+    g32.bpgc = f32(d.bpgc, std::max(nb, 1)); g32.bpdcf = f32(d.bpdcf, std::max(nb, 1));
+    if (d.tvd_far) {
+      g32.tvd_sf = f32(d.tvd_sf, 2 * (size_t)nf); g32.tvd_sd = f32(d.tvd_sd, 2 * (size_t)nf);
+      g32.tvd_su = f32(d.tvd_su, 2 * (size_t)nf);
+    }
+    gU32 = mem.alloc<float>(9 * (size_t)nc);
+    gS32 = mem.alloc<float>(3 * (size_t)(ns + 1) * nc);
+    sc_fadv32 = mem.alloc<float>((size_t)(ns + 1) * nf);
+    sc_fdif32 = mem.alloc<float>((size_t)(ns + 1) * nf);
+    if (!g32.vol || !g32.ls_w || !g32.sf || !g32.eps || !g32.dcf || !gU32 || !gS32 || !sc_fadv32 || !sc_fdif32)
+      return DPM_ERR_CUDA;
+    x32 = true;
+    return 0;
+  }
+  // first gradient pass of a stage in FP32 (U, T when transported, the scalars: one pass over the
+  // FP32 weights), and the FP64 gradient at the cells whose boundary values extrapolate with it
+  void grad_all32() {
+    LsScalarSet32 q{};
+    if (P.boussinesq) { q.phi[q.n] = F.T; q.pb[q.n] = Tb; q.g[q.n] = gS32; q.n++; }
+    for (int k = 0; k < ns; ++k) {
+      q.phi[q.n] = Cs + (size_t)k * nc; q.pb[q.n] = Cb + (size_t)k * nb; q.g[q.n] = gS32 + (size_t)q.n * 3 * nc; q.n++;
+    }
+    switch (q.n) {
+      case 0: k_ls32_gradient_all<0><<<nblk(nc), TPB, 0, st>>>(d, g32, F.U, F.Ub, gU32, q); break;
+      case 1: k_ls32_gradient_all<1><<<nblk(nc), TPB, 0, st>>>(d, g32, F.U, F.Ub, gU32, q); break;
+      case 2: k_ls32_gradient_all<2><<<nblk(nc), TPB, 0, st>>>(d, g32, F.U, F.Ub, gU32, q); break;
+      case 3: k_ls32_gradient_all<3><<<nblk(nc), TPB, 0, st>>>(d, g32, F.U, F.Ub, gU32, q); break;
+      case 4: k_ls32_gradient_all<4><<<nblk(nc), TPB, 0, st>>>(d, g32, F.U, F.Ub, gU32, q); break;
+      default: k_ls32_gradient_all<5><<<nblk(nc), TPB, 0, st>>>(d, g32, F.U, F.Ub, gU32, q); break;
+    }
+    launches++;
+    if (nb) {
+      k_grad32_to_bnd<<<nblk(nb), TPB, 0, st>>>(d, gU32, F.gU);
+      launches++;
+    }
+  }
+  void sgs32(double dt_stab) {
+    if (P.sgs_model == DPM_SGS_NONE) {
+      launch_fill(F.nu_sgs, nc, 0.0);
+      return;
+    }
+    k_sgs32<<<nblk(nc), TPB, 0, st>>>(d, g32, P.sgs_model, gU32, F.nu_sgs, (float)dt_stab, (float)P.c_amd);
+    launches++;
+    if (P.sgs_model == DPM_SGS_AMD && P.amd_wall_gradient && nb > 0) {
+      k_amd_wall32<<<nblk(nc), TPB, 0, st>>>(d, g32, F.U, gU32, F.nu_sgs, P.nu, (float)P.c_amd, (float)dt_stab);
+      launches++;
+    }
+  }
+  void explicit_rhs32(double dt, double a_k, double b_k) {
+    ExplicitArgs a{};
+    a.scheme = P.scheme;
+    a.f0 = P.f_const[0]; a.f1 = P.f_const[1]; a.f2 = P.f_const[2];
+    a.bous = P.boussinesq; a.beta = P.beta; a.T_ref = P.T_ref; a.g0 = P.g[0]; a.g1 = P.g[1]; a.g2 = P.g[2];
+    a.dt = dt; a.a_k = a_k; a.b_k = b_k; a.predict = 1;
+    k_cell_momentum32<<<nblk(nc), TPB, 0, st>>>(d, g32, a, (float)P.nu, F.U, F.Ub, gU32, F.nu_sgs, F.Uf, F.T, F.tau,
+                                                F.H, F.H0, U_spare);
+    launches++;
+    std::swap(F.U, U_spare);
+  }
+  void scalars_rhs32(double dt, double a_k, double b_k) {
+    ScalarFaceSet32 q{};
+    double* H[LS_SET];
+    const double* H0[LS_SET];
+    double* phi[LS_SET];
+    const double* qw[LS_SET];
+    auto add = [&](int scheme, double* f, const double* pbv, double alpha, double prt, double* h, const double* h0,
+                   const double* w) {
+      const int k = q.n++;
+      q.scheme[k] = scheme; q.phi[k] = f; q.pb[k] = pbv; q.g[k] = gS32 + (size_t)k * 3 * nc;
+      q.alpha[k] = (float)alpha; q.prt[k] = (float)prt;
+      q.fadv[k] = sc_fadv32 + (size_t)k * nf; q.fdif[k] = sc_fdif32 + (size_t)k * nf;
+      H[k] = h; H0[k] = h0; phi[k] = f; qw[k] = w;
+    };
+    if (P.boussinesq)
+      add(P.temperature_scheme, F.T, Tb, P.alpha_T, P.Pr_t, HT, HT0, P.wall_model == DPM_WM_MOST ? most_qw : nullptr);
+    for (int k = 0; k < ns; ++k)
+      add(P.scalar_scheme, Cs + (size_t)k * nc, Cb + (size_t)k * nb, P.scalar_diffusivity[k], P.scalar_pr_t[k],
+          HC + (size_t)k * nc, HC0 + (size_t)k * nc, nullptr);
+    if (q.n == 0) return;
+    k_face_scalars32<<<nblk(nf), TPB, 0, st>>>(d, g32, q, F.nu_sgs, F.Uf);
+    launches++;
+    for (int k = 0; k < q.n; ++k) {
+      k_cell_scalar32<<<nblk(nc), TPB, 0, st>>>(d, g32, q.fadv[k], q.fdif[k], H[k], H0[k], phi[k], dt, a_k, b_k, qw[k]);
+      launches++;
+    }
+  }
 
   void temperature_bc(int filt) {
     if (nb == 0) return;
@@ -1394,11 +1513,19 @@ struct Solver {
       double gk_dt = RK3W_GAMMA[k] * dt;
       time = time_n + RK3W_C[k] * dt;
       refresh_halos_and_bc();
-      grad_all();
-      sgs(gk_dt);
-      wall_model(k == 0 ? dt : 0.0);
-      explicit_rhs(dt, RK3W_ALPHA[k], RK3W_BETA[k], 1);
-      scalars_rhs(dt, RK3W_ALPHA[k], RK3W_BETA[k]);
+      if (x32) {  // precision form: gradients, SGS and flux assembly in FP32
+        grad_all32();
+        sgs32(gk_dt);
+        wall_model(k == 0 ? dt : 0.0);
+        explicit_rhs32(dt, RK3W_ALPHA[k], RK3W_BETA[k]);
+        scalars_rhs32(dt, RK3W_ALPHA[k], RK3W_BETA[k]);
+      } else {
+        grad_all();
+        sgs(gk_dt);
+        wall_model(k == 0 ? dt : 0.0);
+        explicit_rhs(dt, RK3W_ALPHA[k], RK3W_BETA[k], 1);
+        scalars_rhs(dt, RK3W_ALPHA[k], RK3W_BETA[k]);
+      }
       velocity_bc_refresh();
       copy(F.p_old, F.p, nc);
       correct_velocity(gk_dt, false, true);
