@@ -398,7 +398,8 @@ def main():
     ap.add_argument("--ml-value-bits", type=int, default=0, choices=[0, 16, 32],
                     help="multilevel form: storage of the smoother's scaled off-diagonals (0: library default, 16)")
     ap.add_argument("--mixed", action="store_true",
-                    help="precision form: FP32-operator inner iterations inside FP64 defect correction")
+                    help="precision form: FP32 gradients, SGS and flux assembly; with the two-level form also "
+                         "FP32-operator inner iterations inside FP64 defect correction")
     ap.add_argument("--psolver", default="auto", choices=["auto", "pcg", "fcg", "ml"],
                     help="auto: fcg when the mesh fits the two-level kernel, else ml; pcg: plain FP64 "
                          "Jacobi-PCG; fcg: flexible CG, two-level part-local preconditioner; "
@@ -465,8 +466,11 @@ def main():
         "gpu_launches": r["launches"],
         "clocks": r["clocks"],
     }
-    if args.mixed and args.psolver == "fcg":
-        line["config"]["form"] += "; precision form (FP32-operator inner iterations, FP64 defect correction)"
+    if args.mixed:
+        line["config"]["form"] += ("; precision form: first gradient pass, SGS and flux assembly in FP32 (FP64 state, "
+                                   "projection and wall-model Newton)" +
+                                   ("; FP32-operator inner Krylov iterations in FP64 defect correction"
+                                    if args.psolver == "fcg" else ""))
     if r["learn"] is not None:
         line["config"]["learned_term"] = r["learn"]
         g = r["learn"]["gamma"]

@@ -6,9 +6,10 @@ and backward kernels on samples that the pressure solves record.
   restatement (same bf16 rounding points) on the same recorded samples and parameters;
 * training: the A-angle loss decreases; the kept scale gamma never makes the held-out solves take
   more iterations than the preconditioner without the term (gamma = 0 is kept on ties);
-* ablation: the next time steps with and without the trained term, iterations per solve recorded
-  (the measured gain, whatever its sign, is printed; it must stay within 3 % of the base), and
-  the flow still matches the plain form's divergence bound.
+* ablation: the next time steps (solves the gate never saw) with and without the trained term:
+  when the gate kept the term (gamma > 0) it must take strictly fewer iterations there; when it
+  switched the term off, the two runs are the same solve.  The flow still meets the divergence
+  bound.  The measured iterations are printed.
 """
 import ctypes as C
 
@@ -75,14 +76,16 @@ def test_learned_training_and_ablation():
             assert st["max_abs_divU"] <= 1e-6
         its[g] = tot
     print("ablation iterations (gamma -> total over 2 steps):", its)
-    assert its[rep["gamma"]] <= 1.03 * its[0.0]
+    if rep["gamma"] > 0.0:
+        assert its[rep["gamma"]] < its[0.0], its
 
 
 def test_learned_term_on_the_multilevel_form():
     """The learned term on the multilevel form (p_solver = DPM_PSOLVER_MULTILEVEL_FCG): samples
     recorded by the multilevel kernel, the same training kernels, gamma gated on the held-out
     solve; then an ablation from the same state with the gated gamma: the steps converge
-    (divergence <= 1e-8, no fallback) in at most 3 % more iterations than without the term.  On
+    (divergence <= 1e-8, no fallback), and a kept term (gamma > 0) must take strictly fewer
+    iterations on those unseen solves.  On
     the channel the V-cycle leaves the one-ring term little to correct (A-angle loss ~0.12 against
     ~0.7 under the two-level preconditioner) and the gate measured gamma = 0."""
     case = cases.channel_config(nx=48, ny=32, nz=32)
@@ -110,4 +113,5 @@ def test_learned_term_on_the_multilevel_form():
             assert st["max_abs_divU"] <= 1e-8 and st["p_fallbacks"] == 0
         its[g] = tot
     print("multilevel ablation iterations (gamma -> total over 2 steps):", its)
-    assert its[rep["gamma"]] <= 1.03 * its[0.0]
+    if rep["gamma"] > 0.0:
+        assert its[rep["gamma"]] < its[0.0], its
