@@ -2517,6 +2517,9 @@ void orc_wall_model(void* h, const double* U, double* tau) {
   std::memcpy(tau, s->tau_w.data(), sizeof(double) * 3 * s->nb);
 }
 double orc_amd_point(const double* alpha, const double* G, double c_amd) { return orc::amd_point(alpha, G, c_amd); }
+void orc_kfactor_limited(const double* sf, const double* d_on, double min_cos, double* k) {
+  orc::kfactor_limited(sf, d_on, min_cos, k);
+}
 void orc_wall_stress_newton(double u_par, double y_w, double nu, double* u_tau, double* tau) {
   bool capped;
   orc::wall_stress_newton(u_par, y_w, nu, *u_tau, *tau, capped);

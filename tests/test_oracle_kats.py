@@ -1,6 +1,10 @@
-"""Known-answer and identity checks of the oracle, ported from the reference's unit tests
-(tests/unit/test_amd.f90, test_nonortho_limiter.f90, test_mesh_geometry.f90) plus the log-law
-inversion of the wall model."""
+"""Known-answer and identity checks of the oracle, ported from the reference's unit test
+tests/unit/test_amd.f90, plus the log-law inversion of the wall model.  The non-orthogonal
+k-vector test (test_nonortho_limiter.f90) and the geometry pins are in test_geometry_kats.py;
+the reference's concave-polygon face test (test_mesh_geometry.f90) exercises the OpenFOAM reader's
+area-weighted polygon routine (src/mesh/mod_mesh.f90:1415-1461), which this path does not use:
+cells arrive as gmsh-type elements whose faces take the vertex-mean fan of
+src/mesh/mod_gmsh_reader.f90:843-869."""
 import ctypes as C
 import math
 
