@@ -24,6 +24,7 @@ FORM_FP64, FORM_MIXED = 0, 1
 PSOLVER_JACOBI_PCG, PSOLVER_TWOLEVEL_FCG, PSOLVER_MULTILEVEL_FCG, PSOLVER_AUTO = 0, 1, 2, 3
 OK, ERR_ARG, ERR_CUDA, ERR_MESH, ERR_NOT_FINITE, ERR_DT_COLLAPSE, ERR_UNSUPPORTED, ERR_BARRIER_TIMEOUT = 0, -1, -2, -3, -4, -5, -6, -7
 GRAD_LEAST_SQUARES, GRAD_GREEN_GAUSS = 0, 1
+CELL_PROJECTION_LS, CELL_PROJECTION_EXACT = 0, 1
 
 EL_TET4, EL_HEX8, EL_PRISM6, EL_PYR5 = 4, 5, 6, 7
 
@@ -65,7 +66,8 @@ class ParamsT(C.Structure):
         ("abl_T_surface", C.c_double), ("abl_L_obukhov", C.c_double), ("abl_compute_L", C.c_int),
         ("p_ml_degree", C.c_int), ("p_ml_overcorrect", C.c_double), ("p_ml_passes", C.c_int),
         ("gradient_scheme", C.c_int), ("gg_iterations", C.c_int), ("p_stall_window", C.c_int),
-        ("p_stall_ratio", C.c_double), ("p_ml_value_bits", C.c_int),
+        ("p_stall_ratio", C.c_double), ("p_ml_value_bits", C.c_int), ("cell_projection", C.c_int),
+        ("cell_projection_tol", C.c_double),
     ]
 
 
@@ -75,7 +77,7 @@ class StatsT(C.Structure):
         ("tauw_mean", C.c_double), ("nu_sgs_mean", C.c_double), ("max_abs_divU", C.c_double),
         ("volavg_abs_divU", C.c_double), ("dt_used", C.c_double), ("p_solves", C.c_int), ("p_iters", C.c_int),
         ("p_resid_max", C.c_double), ("p_fallbacks", C.c_int), ("p_solver_used", C.c_int),
-        ("p_bytes_per_iteration", C.c_double),
+        ("p_bytes_per_iteration", C.c_double), ("cp_iters", C.c_int), ("cp_precond_iters", C.c_int),
     ]
 
     def as_dict(self):
@@ -135,6 +137,8 @@ def default_params(**kw):
     p.p_ml_passes = 3
     p.gradient_scheme = GRAD_LEAST_SQUARES
     p.gg_iterations = 2
+    p.cell_projection = CELL_PROJECTION_LS
+    p.cell_projection_tol = 0.1
     for k, v in kw.items():
         if k in ("f_const", "g", "scalar_diffusivity", "scalar_pr_t"):
             arr = getattr(p, k)

@@ -492,13 +492,31 @@ def regression_case(name):
                     dict(scheme=abi.SCHEME_KEP, nu=6.25e-4, dt=2.0e-2, cfl_max=0.6, p_tol=1e-10,
                          n_nonortho_corr=5, nonortho_check=1, rhie_chow_dual=1),
                     "taylor_green", 1.0, n_steps=30)
-    if name in ("pdrop", "hydro"):
+    if name in ("tgv_skew_exact", "default_skew"):
+        # the exact cell projection on the 45-degree box; default_skew states no numerics at all,
+        # and the reference's defaults are these (mod_input_parser.f90:197-201)
+        return Case(name, skewed_unit_box(16, 0.08), _periodic6(),
+                    dict(scheme=abi.SCHEME_KEP, nu=6.25e-4, dt=2.0e-2, cfl_max=0.6, p_tol=1e-10,
+                         n_nonortho_corr=3, rhie_chow_dual=1, cell_projection=abi.CELL_PROJECTION_EXACT),
+                    "taylor_green", 1.0, n_steps=30)
+    if name in ("pdrop", "hydro", "hydro_exact"):
         fz = 0.0 if name == "pdrop" else -1.0
         patches = [{"bc": "periodic"}] * 4 + [{"bc": "outlet", "p": 1.0}, {"bc": "outlet", "p": 0.0}]
-        return Case(name, skewed_unit_box(12, 0.04), patches,
-                    dict(scheme=abi.SCHEME_CDS, nu=1.0e-2, dt=2.0e-3, cfl_max=0.5, p_tol=1e-12,
-                         n_nonortho_corr=4, rhie_chow_dual=0, f_const=(0.0, 0.0, fz)),
-                    "uniform", 0.0, n_steps=20, stats_every=10)
+        prm = dict(scheme=abi.SCHEME_CDS, nu=1.0e-2, dt=2.0e-3, cfl_max=0.5, p_tol=1e-12,
+                   n_nonortho_corr=4, rhie_chow_dual=0, f_const=(0.0, 0.0, fz))
+        if name == "hydro_exact":
+            prm["cell_projection"] = abi.CELL_PROJECTION_EXACT
+        return Case(name, skewed_unit_box(12, 0.04), patches, prm, "uniform", 0.0, n_steps=20, stats_every=10)
+    if name in ("duct", "duct_exact"):
+        # 32x16x16 duct 4 x 1 x 1 on the RB.geo wall box: velocity inlet at x0, outlet p = 0 at xL,
+        # periodic in y, no-slip bottom and top
+        patches = [{"bc": "inlet", "U": (1.0, 0.0, 0.0)}, {"bc": "outlet", "p": 0.0}, {"bc": "periodic"},
+                   {"bc": "periodic"}, {"bc": "noSlip"}, {"bc": "noSlip"}]
+        prm = dict(scheme=abi.SCHEME_CDS, nu=1.0e-2, dt=1.0e-2, cfl_max=0.5, p_tol=1e-10, p_max_iter=1000,
+                   rhie_chow_dual=0, sgs_model=abi.SGS_NONE)
+        if name == "duct_exact":
+            prm["cell_projection"] = abi.CELL_PROJECTION_EXACT
+        return Case(name, wall_box(32, 16, 16, 4.0, 1.0, 1.0, 0.25), patches, prm, "uniform", 1.0, n_steps=20)
     if name == "hydrowall":
         patches = [{"bc": "noSlip"}] * 6
         return Case(name, skewed_unit_box(12, 0.04), patches,

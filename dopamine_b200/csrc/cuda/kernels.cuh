@@ -1195,7 +1195,7 @@ __device__ __forceinline__ double ps_flux_d(const Dev& d, int i, double dt, cons
 __global__ void __launch_bounds__(TPB) k_face_flux(Dev d, double dt, const double* __restrict__ U,
                                                    const double* __restrict__ gU, const double* __restrict__ gprc,
                                                    const double* __restrict__ phi, const double* __restrict__ Ub,
-                                                   const double* __restrict__ gp, int with_cross,
+                                                   const double* __restrict__ gp, int with_cross, int cproj,
                                                    double* __restrict__ ff, double* __restrict__ pscross) {
   int f = blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= d.nf) return;
@@ -1218,7 +1218,11 @@ __global__ void __launch_bounds__(TPB) k_face_flux(Dev d, double dt, const doubl
     if (with_cross && d.bcanon[b]) pscross[i] = ps_cross_d(d, gp, i, d.pso[i], d.psn[i]);
     return;
   }
-  ff[f] = is_wall_bc(bc) ? 0.0 : (Ub[b] * d.sf[f] + Ub[nb + b] * d.sf[nf + f] + Ub[2 * nb + b] * d.sf[2 * nf + f]);
+  double fl = is_wall_bc(bc) ? 0.0 : (Ub[b] * d.sf[f] + Ub[nb + b] * d.sf[nf + f] + Ub[2 * nb + b] * d.sf[2 * nf + f]);
+  // exact cell projection: the compact old-pressure term on outlet faces, so that the new pressure
+  // equals p_b there (mod_fv_solver.f90:2625-2633)
+  if (cproj && bc == BC_OUTLET) fl = fl - dt * d.bcb[b] * (d.bpval[b] - phi[d.fo[f]]);
+  ff[f] = fl;
 }
 
 // rhs_p = -(1/dt) sum_f q_f + deferred cross terms, gathered per cell in the reference's order.

@@ -22,6 +22,7 @@
 #include "../host/ops.hpp"
 #include "../host/twolevel.hpp"
 #include "../host/multilevel.hpp"
+#include "cellproj.cuh"
 #include "common.cuh"
 #include "explicit32.cuh"
 #include "fcg.cuh"
@@ -180,6 +181,13 @@ struct Solver {
   bool x32 = false;
   Geo32 g32{};
   float *gU32 = nullptr, *gS32 = nullptr, *sc_fadv32 = nullptr, *sc_fdif32 = nullptr;
+  // exact cell projection (cellproj.cuh): work vectors, partials and device scalars, allocated
+  // on first use; outer and preconditioner iterations of the current step
+  bool cp_on = false;
+  double *cp_x = nullptr, *cp_r = nullptr, *cp_z = nullptr, *cp_p = nullptr, *cp_q = nullptr, *cp_rold = nullptr,
+         *cp_v = nullptr, *cp_bconst = nullptr, *cp_part = nullptr;
+  CpState* cp_st = nullptr;
+  int cp_iters = 0, cp_precond_iters = 0;
   // PCG workspace
   double *cg_r, *cg_z, *cg_p0, *cg_p1, *cg_q, *cg_bp, *cg_x, *cg_part, *cg_dout;
   void* cg_kernel = nullptr;
@@ -264,6 +272,8 @@ struct Solver {
       return DPM_ERR_MESH;
     }
     P = *prm;
+    if (P.cell_projection != DPM_CELL_PROJECTION_LS && P.cell_projection != DPM_CELL_PROJECTION_EXACT) return DPM_ERR_ARG;
+    cp_on = P.cell_projection == DPM_CELL_PROJECTION_EXACT;
     pc.assign(patches, patches + raw->n_patches);
     if (build_static_ops(m, pc.data(), P, S)) return DPM_ERR_MESH;
     if (m.n_cells > 2000000000LL || m.n_faces > 2000000000LL) return DPM_ERR_UNSUPPORTED;
@@ -395,6 +405,7 @@ struct Solver {
       if (!gg_prevU || !gg_prevS) return DPM_ERR_CUDA;
     }
     if (!cg_dout || !F.fadv || !aos_buf) return DPM_ERR_CUDA;
+    if (cp_on && cp_alloc()) return DPM_ERR_CUDA;
     // cooperative grid for the persistent PCG
     int dev_sms = 0, per_sm = 0, coop = 0;
     CK(cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, device));
@@ -641,7 +652,8 @@ struct Solver {
       }
     }
     int wc = !S.skip_nonortho;
-    k_face_flux<<<nblk(nf), TPB, 0, st>>>(d, dt, F.U, F.gU, F.gp_rc, F.phi_prev, F.Ub, F.gp, wc, F.ff, F.ps_cross);
+    k_face_flux<<<nblk(nf), TPB, 0, st>>>(d, dt, F.U, F.gU, F.gp_rc, F.phi_prev, F.Ub, F.gp, wc, cp_on ? 1 : 0, F.ff,
+                                          F.ps_cross);
     k_rhs_gather<<<nblk(nc), TPB, 0, st>>>(d, 1.0 / std::max(dt, SMALL), wc, F.ff, F.ps_cross, F.gp, F.rhs);
     launches += 2;
   }
@@ -1425,6 +1437,111 @@ struct Solver {
     return 0;
   }
 
+  // ---------------------------------------------------------------- exact cell projection
+  int cp_alloc() {
+    if (cp_st) return 0;
+    cp_x = mem.alloc<double>(nc); cp_r = mem.alloc<double>(nc); cp_z = mem.alloc<double>(nc);
+    cp_p = mem.alloc<double>(nc); cp_q = mem.alloc<double>(nc); cp_rold = mem.alloc<double>(nc);
+    cp_bconst = mem.alloc<double>(nc); cp_v = mem.alloc<double>(3 * (size_t)nc);
+    cp_part = mem.alloc<double>((size_t)CP_RED_BLOCKS * CP_NPART);
+    cp_st = mem.alloc<CpState>(1);
+    return (cp_x && cp_r && cp_z && cp_p && cp_q && cp_rold && cp_bconst && cp_v && cp_part && cp_st) ? 0 : DPM_ERR_CUDA;
+  }
+  int cp_grid() const { return std::max(1, std::min(nblk(nc), CP_RED_BLOCKS)); }
+  double cp_tol() const { return std::max(P.cell_projection_tol > 0.0 ? P.cell_projection_tol : 0.1, 1.0e-8); }
+  // The projection's preconditioner (mod_fv_solver.f90:3277-3282): z = 0, then the handle's
+  // pressure solve to rtol 0.05 with at most 50 iterations, which the backend raises to its 2000
+  // floor (pressure_backend_petsc.c:844); a failed solve is retried from zero like pressure_solve.
+  int cp_precond(int* its_out) {
+    launch_fill(cp_z, nc, 0.0);
+    const double tol = 0.05, atol = 1.0e-50;
+    const int maxit = std::max(50, 2000);
+    int its = 0, reason = 0;
+    double res = 0.0;
+    int rc = pcg(cp_r, cp_z, tol, atol, maxit, 0, &its, &res, &reason);
+    if (rc) return rc;
+    if (reason < 0 && flexible()) {
+      p_fallbacks++;
+      int its2 = 0;
+      rc = pcg_plain(cp_r, cp_z, tol, atol, maxit, 0, &its2, &res, &reason);
+      if (rc) return rc;
+      its += its2;
+    }
+    if (reason < 0) {
+      rc = pcg_plain(cp_r, cp_z, tol, atol, 4 * maxit, 1, &its, &res, &reason);
+      if (rc) return rc;
+      if (reason < 0 && !(reason == -3 && (res < tol * 1.0e4 || res < atol * 1.0e3))) return -(1000 + reason);
+    }
+    *its_out = its;
+    return 0;
+  }
+  // cp_project (src/numerics/mod_cell_projection.f90:192-303) on the SoA velocity u; identity_pc
+  // replaces the pressure-solve preconditioner by z = r (the reference's unit test does so).
+  int cp_project(double* u, const double* bconst, double tol, int max_it, bool identity_pc, int* n_it) {
+    int rc = cp_alloc();
+    if (rc) return rc;
+    const int g = cp_grid();
+    launch_fill(cp_x, nc, 0.0);
+    k_cp_rhs<<<g, TPB, 0, st>>>(d, u, bconst, cp_r, cp_part);
+    k_cp_rule<<<1, 32, 0, st>>>(0, g, cp_part, tol, cp_st);
+    launches += 2;
+    CpState h{};
+    CK(cudaMemcpyAsync(&h, cp_st, sizeof(CpState), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    *n_it = 0;
+    if (h.stop) return 0;
+    auto precond = [&]() -> int {
+      if (identity_pc) {
+        copy(cp_z, cp_r, nc);
+        return 0;
+      }
+      int its = 0;
+      int rc2 = cp_precond(&its);
+      cp_precond_iters += its;
+      return rc2;
+    };
+    rc = precond();
+    if (rc) return rc;
+    k_cp_dots<<<g, TPB, 0, st>>>(nc, 1, cp_r, cp_rold, cp_z, cp_p, cp_part);
+    k_cp_rule<<<1, 32, 0, st>>>(1, g, cp_part, tol, cp_st);
+    launches += 2;
+    for (int it = 1; it <= max_it; ++it) {
+      *n_it = it;
+      k_cp_adjoint<<<nblk(nc), TPB, 0, st>>>(d, cp_p, cp_v);
+      k_cp_div_dot<<<g, TPB, 0, st>>>(d, cp_v, cp_p, cp_q, cp_part);
+      k_cp_rule<<<1, 32, 0, st>>>(2, g, cp_part, tol, cp_st);
+      k_cp_update<<<g, TPB, 0, st>>>(nc, cp_st, cp_p, cp_q, cp_x, cp_r, cp_rold, cp_part);
+      k_cp_rule<<<1, 32, 0, st>>>(3, g, cp_part, tol, cp_st);
+      launches += 5;
+      int stop = 0;
+      CK(cudaMemcpyAsync(&stop, &cp_st->stop, sizeof(int), cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+      if (stop) break;
+      rc = precond();
+      if (rc) return rc;
+      k_cp_dots<<<g, TPB, 0, st>>>(nc, 0, cp_r, cp_rold, cp_z, cp_p, cp_part);
+      k_cp_rule<<<1, 32, 0, st>>>(4, g, cp_part, tol, cp_st);
+      k_cp_direction<<<g, TPB, 0, st>>>(nc, cp_st, cp_z, cp_p);
+      launches += 3;
+    }
+    k_cp_adjoint<<<nblk(nc), TPB, 0, st>>>(d, cp_x, cp_v);
+    k_cp_apply<<<nblk(3 * (int64_t)nc), TPB, 0, st>>>(3 * nc, cp_v, u);
+    launches += 2;
+    CK(cudaGetLastError());
+    return 0;
+  }
+  // project_cells_exact (mod_fv_solver.f90:3223-3283)
+  int project_cells_exact(double dt) {
+    int rc = cp_alloc();
+    if (rc) return rc;
+    k_cp_boundary<<<nblk(nc), TPB, 0, st>>>(d, dt, F.U, F.Ub, cp_bconst);
+    launches++;
+    int n_it = 0;
+    rc = cp_project(F.U, cp_bconst, cp_tol(), 100, false, &n_it);
+    cp_iters += n_it;
+    return rc;
+  }
+
   // ---------------------------------------------------------------- solver_project_once
   int project_once(double dt) {
     launch_fill(F.rhs, nc, 0.0);
@@ -1447,7 +1564,12 @@ struct Solver {
     copy(F.ff, F.Uf, nf);
     u_face_ready = true;
     pressure_bc(F.p, -1, 0, 0);
-    correct_velocity(dt, true, true);
+    if (cp_on) {
+      int rc = project_cells_exact(dt);
+      if (rc) return rc;
+    } else {
+      correct_velocity(dt, true, true);
+    }
     velocity_bc(-1, 0);
     if (P.use_rotational_projection) {
       k_rotational<<<nblk(nc), TPB, 0, st>>>(nc, F.p, F.nu_sgs, F.rhs, d.ivol, P.nu, dt);
@@ -1497,6 +1619,7 @@ struct Solver {
     cudaEventRecord(ev0, st);
     last.dt_used = dt;
     last.p_solves = 0; last.p_iters = 0; last.p_resid_max = 0.0;
+    cp_iters = 0; cp_precond_iters = 0;
     launch_fill(F.H, 3 * (int64_t)nc, 0.0);
     launch_fill(F.H0, 3 * (int64_t)nc, 0.0);
     launch_fill(F.rhs, nc, 0.0);
@@ -1528,7 +1651,8 @@ struct Solver {
       }
       velocity_bc_refresh();
       copy(F.p_old, F.p, nc);
-      correct_velocity(gk_dt, false, true);
+      if (cp_on) launch_fill(F.gpc, 3 * (int64_t)nc, 0.0);  // nothing to add back (mod_fv_solver.f90:1373-1377)
+      else correct_velocity(gk_dt, false, true);
       copy(F.gp_rc, F.gpc, 3 * (size_t)nc);
       velocity_bc_refresh();
       grad_all();
@@ -1589,7 +1713,12 @@ struct Solver {
       correct_face_fluxes(gk_dt, false);
       copy(F.ff, F.Uf, nf);
       u_face_ready = true;
-      correct_velocity(gk_dt, true, false);
+      if (cp_on) {
+        rc = project_cells_exact(gk_dt);
+        if (rc) return rc;
+      } else {
+        correct_velocity(gk_dt, true, false);
+      }
       velocity_bc_refresh();
       if (P.use_rotational_projection) {
         k_rotational<<<nblk(nc), TPB, 0, st>>>(nc, F.p, F.nu_sgs, F.rhs, d.ivol, P.nu, gk_dt);
@@ -1669,6 +1798,8 @@ struct Solver {
     s->volavg_abs_divU = o2[1] / o2[2];
     s->dt_used = last.dt_used;
     s->p_fallbacks = p_fallbacks;
+    s->cp_iters = cp_iters;
+    s->cp_precond_iters = cp_precond_iters;
     s->p_solver_used = force_plain ? DPM_PSOLVER_JACOBI_PCG
                                    : (use_fcg ? DPM_PSOLVER_TWOLEVEL_FCG
                                               : (use_ml ? DPM_PSOLVER_MULTILEVEL_FCG : DPM_PSOLVER_JACOBI_PCG));
@@ -2156,6 +2287,43 @@ int dpm_wall_model(dpm_solver_t* h, const double* U, double nu, double* tau_w) {
   s.P.nu = keep;
   if (s.nb) return download_vec3(s, s.F.tau, tau_w, s.nb);
   return DPM_OK;
+}
+
+int dpm_cell_divergence(dpm_solver_t* h, const double* u, double* out) {
+  if (!h || !u || !out) return DPM_ERR_ARG;
+  Solver& s = *h->s;
+  int rc = s.cp_alloc();
+  if (!rc) rc = upload_vec3(s, u, s.cp_v, s.nc);
+  if (rc) return rc;
+  dpm::gpu::k_cp_divergence<<<dpm::gpu::nblk(s.nc), dpm::gpu::TPB, 0, s.st>>>(s.d, s.cp_v, s.cp_q);
+  s.launches++;
+  CK(cudaMemcpyAsync(out, s.cp_q, sizeof(double) * s.nc, cudaMemcpyDeviceToHost, s.st));
+  CK(cudaStreamSynchronize(s.st));
+  return DPM_OK;
+}
+
+int dpm_cell_adjoint_gradient(dpm_solver_t* h, const double* chi, double* v) {
+  if (!h || !chi || !v) return DPM_ERR_ARG;
+  Solver& s = *h->s;
+  int rc = s.cp_alloc();
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(s.cp_p, chi, sizeof(double) * s.nc, cudaMemcpyHostToDevice, s.st));
+  dpm::gpu::k_cp_adjoint<<<dpm::gpu::nblk(s.nc), dpm::gpu::TPB, 0, s.st>>>(s.d, s.cp_p, s.cp_v);
+  s.launches++;
+  return download_vec3(s, s.cp_v, v, s.nc);
+}
+
+int dpm_cell_project(dpm_solver_t* h, double* u, const double* bconst, double tol, int max_it, int identity_precond,
+                     int* n_it) {
+  if (!h || !u || !bconst || !n_it || max_it < 0 || !(tol >= 0.0)) return DPM_ERR_ARG;
+  Solver& s = *h->s;
+  int rc = s.cp_alloc();
+  if (!rc) rc = upload_vec3(s, u, s.U_spare, s.nc);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(s.cp_bconst, bconst, sizeof(double) * s.nc, cudaMemcpyHostToDevice, s.st));
+  rc = s.cp_project(s.U_spare, s.cp_bconst, tol, max_it, identity_precond != 0, n_it);
+  if (rc) return rc;
+  return download_vec3(s, s.U_spare, u, s.nc);
 }
 
 }  // extern "C"

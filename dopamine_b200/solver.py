@@ -27,7 +27,7 @@ EXPORTED = (
     "dpm_advection_rhs_scalar", "dpm_viscous_rhs_scalar", "dpm_upload_scalars", "dpm_download_scalars",
     "dpm_learn_collect", "dpm_learn_train", "dpm_learn_set_gamma", "dpm_learn_sizes", "dpm_learn_export",
     "dpm_learn_loss_grad", "dpm_multilevel_hierarchy", "dpm_set_barrier_spin_limit",
-    "dpm_select_pressure_solver",
+    "dpm_select_pressure_solver", "dpm_cell_divergence", "dpm_cell_adjoint_gradient", "dpm_cell_project",
 )
 
 
@@ -75,6 +75,9 @@ def lib(build_if_missing=True):
     L.dpm_viscous_rhs_vector.argtypes = [vp, dp, C.c_double, dp, dp, dp, dp]
     L.dpm_sgs_viscosity.argtypes = [vp, C.c_int, dp, dp, dp, C.c_double, dp]
     L.dpm_wall_model.argtypes = [vp, dp, C.c_double, dp]
+    L.dpm_cell_divergence.argtypes = [vp, dp, dp]
+    L.dpm_cell_adjoint_gradient.argtypes = [vp, dp, dp]
+    L.dpm_cell_project.argtypes = [vp, dp, dp, C.c_double, C.c_int, C.c_int, ip]
     L.dpm_advection_rhs_scalar.argtypes = [vp, C.c_int, dp, dp, dp, dp, dp]
     L.dpm_viscous_rhs_scalar.argtypes = [vp, dp, C.c_double, dp, C.c_double, dp, dp, dp]
     L.dpm_upload_scalars.argtypes = [vp, dp]
@@ -312,3 +315,23 @@ class Solver:
         tau = np.zeros((self.nb, 3))
         _check(lib().dpm_wall_model(self.h, _p(np.ascontiguousarray(U)), nu, _p(tau)), "dpm_wall_model")
         return tau
+
+    # exact cell projection operators (src/numerics/mod_cell_projection.f90)
+    def cell_divergence(self, u):
+        out = np.zeros(self.nc)
+        _check(lib().dpm_cell_divergence(self.h, _p(np.ascontiguousarray(u, dtype=np.float64)), _p(out)),
+               "dpm_cell_divergence")
+        return out
+
+    def cell_adjoint_gradient(self, chi):
+        v = np.zeros((self.nc, 3))
+        _check(lib().dpm_cell_adjoint_gradient(self.h, _p(np.ascontiguousarray(chi, dtype=np.float64)), _p(v)),
+               "dpm_cell_adjoint_gradient")
+        return v
+
+    def cell_project(self, u, bconst, tol, max_it, identity_precond=False):
+        u = np.array(u, dtype=np.float64, order="C", copy=True)
+        n_it = C.c_int(0)
+        _check(lib().dpm_cell_project(self.h, _p(u), _p(np.ascontiguousarray(bconst, dtype=np.float64)), tol, max_it,
+                                      1 if identity_precond else 0, C.byref(n_it)), "dpm_cell_project")
+        return u, n_it.value

@@ -72,6 +72,8 @@ extern "C" {
 #define DPM_PSOLVER_AUTO 3  /* the two-level form when the mesh fits it (<= 4096 cells per SM), else the multilevel form */
 #define DPM_GRAD_LEAST_SQUARES 0
 #define DPM_GRAD_GREEN_GAUSS 1
+#define DPM_CELL_PROJECTION_LS 0
+#define DPM_CELL_PROJECTION_EXACT 1
 #define DPM_FORM_FP64 0     /* FP64 Krylov iterations                                    */
 #define DPM_FORM_MIXED 1    /* with DPM_PSOLVER_TWOLEVEL_FCG: inner iterations on an FP32 copy of
                                the operator and an FP32 preconditioned vector, inside an FP64
@@ -170,6 +172,16 @@ typedef struct dpm_params {
    * (binary16, with a per-row diagonal term that keeps each stored row's sum exact) or 32 (FP32);
    * 0: 32. */
   int p_ml_value_bits;
+  /* Cell velocity after the face-flux projection (src/solver/mod_fv_solver.f90:91-92,
+   * src/io/mod_input_parser.f90:200-201, 305-306): DPM_CELL_PROJECTION_LS reconstructs it from the
+   * pressure gradient; DPM_CELL_PROJECTION_EXACT (the reference's default) projects it
+   * V-orthogonally onto zero divergence of the interpolated face flux
+   * (src/numerics/mod_cell_projection.f90), by flexible CG preconditioned with a pressure solve
+   * to relative tolerance 0.05, stopping when the last step's velocity energy is below
+   * cell_projection_tol^2 times the total (<= 0: 0.1; floored at 1e-8 as the reference's parser
+   * floors it). */
+  int cell_projection;
+  double cell_projection_tol;
 } dpm_params_t;
 
 /* Per-step integral statistics (src/stats/mod_stats.f90:compute_stats_sums and
@@ -185,6 +197,9 @@ typedef struct dpm_stats {
   double p_bytes_per_iteration;  /* algorithmic bytes one Krylov iteration of that solve moves
                                     (each array read or written once per pass): the roofline
                                     numerator of the pressure solve                           */
+  int cp_iters;               /* DPM_CELL_PROJECTION_EXACT: outer iterations of the last step's
+                                 cell projections (summed over its stages)                    */
+  int cp_precond_iters;       /* and the Krylov iterations of their preconditioning solves      */
 } dpm_stats_t;
 
 /* Outcome of dpm_learn_train. */
@@ -313,6 +328,19 @@ int dpm_advection_rhs_scalar(dpm_solver_t* s, int scheme, const double* phi, con
 /* src/numerics/mod_viscous.f90:286 viscous_rhs_scalar: diffusivity alpha + nu_sgs / Pr_t. */
 int dpm_viscous_rhs_scalar(dpm_solver_t* s, const double* phi, double alpha, const double* nu_sgs, double Pr_t,
                            const double* grad_phi, const double* phi_bnd, double* rhs);
+/* The exact cell projection's operators (src/numerics/mod_cell_projection.f90), on the
+ * handle's pressure faces and outlet faces whatever its cell_projection setting:
+ * cp_divergence (:84): out(nc) = B u, the outflow divergence of the gc-interpolated flux of
+ * u(3,nc); cp_adjoint_gradient (:129): v(3,nc) = V^-1 B^T chi; cp_project (:192): u <- u - V^-1 B^T
+ * chi with (B V^-1 B^T) chi = B u + bconst(nc) by flexible CG, stopping on max|r| <= 1e-12 max|b|
+ * or (after 2 iterations) a last step's velocity energy below tol^2 times the total, at most
+ * max_it iterations (n_it: those taken); preconditioned by the handle's pressure solve to
+ * rtol 0.05 as project_cells_exact does, or by z = r when identity_precond is non-zero (the form
+ * of the reference's unit test). */
+int dpm_cell_divergence(dpm_solver_t* s, const double* u, double* out);
+int dpm_cell_adjoint_gradient(dpm_solver_t* s, const double* chi, double* v);
+int dpm_cell_project(dpm_solver_t* s, double* u, const double* bconst, double tol, int max_it, int identity_precond,
+                     int* n_it);
 /* Passive scalars C(n_scalars, n) in the reference's Fortran layout (src/solver/mod_fv_solver.f90:326,
  * scalar index fastest); the temperature travels with dpm_upload_state / dpm_download_state. */
 int dpm_upload_scalars(dpm_solver_t* s, const double* C);

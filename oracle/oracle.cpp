@@ -15,6 +15,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <limits>
 #include <memory>
 #include <string>
 #include <vector>
@@ -177,6 +178,13 @@ struct Solver {
   std::vector<double> u_par_filt;
   bool filt_ready = false;
 
+  // exact cell projection (src/numerics/mod_cell_projection.f90:cell_proj_t): pressure-face list
+  // with interpolation weights, outlet faces, and the last step's iteration counts
+  bool cp_on = false;
+  std::vector<int> cp_own, cp_nbr, cp_bcell;
+  std::vector<double> cp_sf, cp_gc, cp_bsf;
+  int cp_iters = 0, cp_precond_iters = 0;
+
   // last-step diagnostics
   int last_solves = 0, last_iters = 0;
   double last_resid = 0.0, last_dt = 0.0;
@@ -195,6 +203,10 @@ struct Solver {
     int rc = build_mesh(r, pbc.data(), m, err);
     if (rc) return rc;
     P = *prm;
+    if (P.cell_projection != DPM_CELL_PROJECTION_LS && P.cell_projection != DPM_CELL_PROJECTION_EXACT) {
+      if (err) *err = "cell_projection must be LS or EXACT";
+      return DPM_ERR_ARG;
+    }
     pc.assign(patches, patches + raw->n_patches);
     nc = m.n_cells; nf = m.n_faces; nfi = m.n_int_faces; nb = m.n_bnd_faces;
     U.assign(3 * nc, 0.0); p.assign(nc, 0.0); p_old.assign(nc, 0.0); T.assign(nc, P.T_ref);
@@ -250,6 +262,7 @@ struct Solver {
     for (int64_t f = 0; f < nfi; ++f)
       if (m.is_refine[f]) { diag_interface = true; break; }
     build_filter_tensor();
+    build_cell_projection();
     return 0;
   }
 
@@ -1744,6 +1757,12 @@ struct Solver {
       int o = m.owner[fg];
       int bc = bc_of_face(fg);
       double flux = is_wall(bc) ? 0.0 : dot3(&U_bnd[3 * fb], &m.sf[3 * fg]);
+      if (cp_on && bc == BC_OUTLET) {  // compact old-pressure term, so that p_new = p_b there (:2625-2633)
+        double d[3];
+        for (int k = 0; k < 3; ++k) d[k] = m.centre[3 * fg + k] - m.centroid[3 * o + k];
+        double c_b = m.area[fg] / std::max(std::fabs(dot3(d, &m.normal[3 * fg])), SMALL);
+        flux = flux - dt * c_b * (pc[m.patch[fg]].p_val - phi_prev[o]);
+      }
       face_flux[fg] = flux;
       built[fg] = 1;
       rhs_p[o] -= flux;
@@ -2029,6 +2048,182 @@ struct Solver {
     return std::max(1.0e-12 * std::max(us, 1.0) * V_min / dt, p_atol_factor);
   }
 
+  // ------------------------------------------------------------------ exact cell projection
+  // src/solver/mod_fv_solver.f90:3163-3221 (build_cell_projection): the non-skipped pressure
+  // faces with their interpolation weight (periodic weight on periodic faces) and the outlet faces.
+  void build_cell_projection() {
+    cp_on = P.cell_projection == DPM_CELL_PROJECTION_EXACT;
+    cp_own.clear(); cp_nbr.clear(); cp_sf.clear(); cp_gc.clear(); cp_bcell.clear(); cp_bsf.clear();
+    for (int64_t i = 0; i < nfp; ++i) {
+      if (ps_skip[i]) continue;
+      int o = ps_owner[i], n = ps_nb[i];
+      int64_t fm = ps_mesh[i];
+      if (o < 0 || o >= nc || n < 0 || n >= nc || fm < 0 || fm >= nf) continue;
+      cp_own.push_back(o);
+      cp_nbr.push_back(n);
+      for (int k = 0; k < 3; ++k) cp_sf.push_back(m.sf[3 * fm + k]);
+      cp_gc.push_back(fm >= nfi ? m.periodic_gc[fm - nfi] : m.gc[fm]);
+    }
+    for (int64_t fb : nper_bf) {
+      int64_t fg = nfi + fb;
+      if (bc_of_face(fg) != BC_OUTLET) continue;
+      cp_bcell.push_back(m.owner[fg]);
+      for (int k = 0; k < 3; ++k) cp_bsf.push_back(m.sf[3 * fg + k]);
+    }
+  }
+  // src/numerics/mod_cell_projection.f90:84-127 (cp_divergence): outflow sum of the interpolated
+  // flux, accumulated in face order.
+  void cp_divergence(const double* u, double* out) const {
+    std::fill(out, out + nc, 0.0);
+    for (size_t f = 0; f < cp_own.size(); ++f) {
+      int o = cp_own[f], n = cp_nbr[f];
+      double w = cp_gc[f];
+      const double* sf = &cp_sf[3 * f];
+      double fl = (w * u[3 * o] + (1.0 - w) * u[3 * n]) * sf[0] + (w * u[3 * o + 1] + (1.0 - w) * u[3 * n + 1]) * sf[1] +
+                  (w * u[3 * o + 2] + (1.0 - w) * u[3 * n + 2]) * sf[2];
+      out[o] = out[o] + fl;
+      out[n] = out[n] - fl;
+    }
+    for (size_t f = 0; f < cp_bcell.size(); ++f) {
+      int o = cp_bcell[f];
+      const double* bs = &cp_bsf[3 * f];
+      out[o] = out[o] + (u[3 * o] * bs[0] + u[3 * o + 1] * bs[1] + u[3 * o + 2] * bs[2]);
+    }
+  }
+  // src/numerics/mod_cell_projection.f90:129-189 (cp_adjoint_gradient): v = V^-1 B^T chi.
+  void cp_adjoint(const double* chi, double* v) const {
+    std::fill(v, v + 3 * nc, 0.0);
+    for (size_t f = 0; f < cp_own.size(); ++f) {
+      int o = cp_own[f], n = cp_nbr[f];
+      double w = cp_gc[f], d = chi[o] - chi[n];
+      const double* sf = &cp_sf[3 * f];
+      for (int k = 0; k < 3; ++k) v[3 * o + k] = v[3 * o + k] + w * d * sf[k];
+      for (int k = 0; k < 3; ++k) v[3 * n + k] = v[3 * n + k] + (1.0 - w) * d * sf[k];
+    }
+    for (size_t f = 0; f < cp_bcell.size(); ++f) {
+      int o = cp_bcell[f];
+      for (int k = 0; k < 3; ++k) v[3 * o + k] = v[3 * o + k] + chi[o] * cp_bsf[3 * f + k];
+    }
+    for (int64_t c = 0; c < nc; ++c) {
+      double iv = 1.0 / m.volume[c];
+      for (int k = 0; k < 3; ++k) v[3 * c + k] = v[3 * c + k] * iv;
+    }
+  }
+  // The preconditioner of the projection (mod_fv_solver.f90:3277-3282): z = 0, then the pressure
+  // solve to rtol 0.05 with at most 50 iterations, which the backend raises to its 2000 floor
+  // (pressure_backend_petsc.c:844), with the backend's NaN scrub and retry.
+  int cp_precond(const double* r, double* z, int* its_out) {
+    std::vector<double> rw(r, r + nc);
+    for (auto& x : rw)
+      if (!finite(x)) x = 0.0;
+    std::fill(z, z + nc, 0.0);
+    const double tol = 0.05, atol = 1.0e-50;
+    const int maxit = std::max(50, 2000);
+    int its = 0;
+    double res = 0.0;
+    int reason = cg(rw.data(), z, tol, atol, maxit, false, &its, &res);
+    if (reason < 0) {
+      reason = cg(rw.data(), z, tol, atol, 4 * maxit, true, &its, &res);
+      if (reason < 0 && !(reason == -3 && (res < tol * 1.0e4 || res < atol * 1.0e3))) return -(1000 + reason);
+    }
+    *its_out = its;
+    return 0;
+  }
+  // src/numerics/mod_cell_projection.f90:192-303 (cp_project): u <- u - V^-1 B^T chi with
+  // (B V^-1 B^T) chi = B u + bconst by flexible PCG. identity_pc replaces the pressure-solve
+  // preconditioner by z = r (the reference's unit test does the same).
+  int cp_project(double* u, const double* bconst, double tol, int max_it, bool identity_pc, int* n_it) {
+    std::vector<double> b(nc, 0.0), x(nc, 0.0), r(nc, 0.0), z(nc, 0.0), pv(nc, 0.0), q(nc, 0.0), rold(nc, 0.0),
+        chi(nc, 0.0), v(3 * nc, 0.0);
+    auto precond = [&](int* its) -> int {
+      if (identity_pc) { z = r; *its = 0; return 0; }
+      return cp_precond(r.data(), z.data(), its);
+    };
+    cp_divergence(u, b.data());
+    double smax = 0.0;
+    for (int64_t c = 0; c < nc; ++c) {
+      b[c] = b[c] + bconst[c];
+      r[c] = b[c];
+      smax = std::max(smax, std::fabs(r[c]));
+    }
+    *n_it = 0;
+    const double bn = smax, tiny = std::numeric_limits<double>::min();
+    if (!(bn > tiny)) return 0;
+    int its = 0;
+    int rc = precond(&its);
+    if (rc) return rc;
+    cp_precond_iters += its;
+    double rz = 0.0;
+    for (int64_t c = 0; c < nc; ++c) {
+      pv[c] = z[c];
+      rz = rz + r[c] * z[c];
+    }
+    double en_tot = 0.0;
+    for (int it = 1; it <= max_it; ++it) {
+      *n_it = it;
+      chi = pv;
+      cp_adjoint(chi.data(), v.data());
+      cp_divergence(v.data(), q.data());
+      double pq = 0.0;
+      for (int64_t c = 0; c < nc; ++c) pq = pq + pv[c] * q[c];
+      if (std::fabs(pq) <= tiny) break;
+      double alpha = rz / pq;
+      double en_new = alpha * alpha * pq;
+      en_tot = en_tot + en_new;
+      smax = 0.0;
+      for (int64_t c = 0; c < nc; ++c) {
+        rold[c] = r[c];
+        x[c] = x[c] + alpha * pv[c];
+        r[c] = r[c] - alpha * q[c];
+        smax = std::max(smax, std::fabs(r[c]));
+      }
+      if (smax <= 1.0e-12 * bn || (it >= 2 && en_new <= tol * tol * en_tot)) break;
+      std::fill(z.begin(), z.end(), 0.0);
+      rc = precond(&its);
+      if (rc) return rc;
+      cp_precond_iters += its;
+      double s1 = 0.0, s2 = 0.0;
+      for (int64_t c = 0; c < nc; ++c) {
+        s1 = s1 + (r[c] - rold[c]) * z[c];
+        s2 = s2 + r[c] * z[c];
+      }
+      double beta = std::max(0.0, s1 / rz);
+      rz = s2;
+      for (int64_t c = 0; c < nc; ++c) pv[c] = z[c] + beta * pv[c];
+    }
+    chi = x;
+    cp_adjoint(chi.data(), v.data());
+    for (int64_t c = 0; c < nc; ++c)
+      for (int k = 0; k < 3; ++k) u[3 * c + k] = u[3 * c + k] - v[3 * c + k];
+    return 0;
+  }
+  double cp_tol() const {
+    double t = P.cell_projection_tol > 0.0 ? P.cell_projection_tol : 0.1;
+    return std::max(t, 1.0e-8);
+  }
+  // src/solver/mod_fv_solver.f90:3223-3283 (project_cells_exact): the outlet pressure acts on its
+  // cell as the boundary force -p_b S_f / V; Dirichlet-velocity faces give the fixed outflow.
+  int project_cells_exact(double dt) {
+    std::vector<double> bconst(nc, 0.0);
+    for (int64_t fb : nper_bf) {
+      int64_t fg = nfi + fb;
+      int o = m.owner[fg];
+      int bc = bc_of_face(fg);
+      if (is_wall(bc)) continue;
+      const double* sf = &m.sf[3 * fg];
+      if (bc == BC_OUTLET) {
+        double fl = dt * pc[m.patch[fg]].p_val / m.volume[o];
+        for (int k = 0; k < 3; ++k) U[3 * o + k] = U[3 * o + k] - fl * sf[k];
+      } else {
+        bconst[o] = bconst[o] + (U_bnd[3 * fb] * sf[0] + U_bnd[3 * fb + 1] * sf[1] + U_bnd[3 * fb + 2] * sf[2]);
+      }
+    }
+    int n_it = 0;
+    int rc = cp_project(U.data(), bconst.data(), cp_tol(), 100, false, &n_it);
+    cp_iters += n_it;
+    return rc;
+  }
+
   // src/solver/mod_fv_solver.f90:837-918
   int project_once(double dt) {
     std::fill(rhs_p.begin(), rhs_p.end(), 0.0);
@@ -2048,7 +2243,12 @@ struct Solver {
     U_face = face_flux;
     u_face_ready = true;
     apply_pressure_bc(p.data(), -1, false, false);
-    correct_velocity(dt, true, true);
+    if (cp_on) {
+      int rc = project_cells_exact(dt);
+      if (rc) return rc;
+    } else {
+      correct_velocity(dt, true, true);
+    }
     apply_velocity_bc(-1, false);
     if (P.use_rotational_projection) {
       for (int64_t c = 0; c < nc; ++c) p[c] = p[c] + (P.nu + nu_sgs[c]) * rhs_p[c] * dt * inv_vol[c];
@@ -2114,6 +2314,7 @@ struct Solver {
     }
     last_dt = dt;
     last_solves = 0; last_iters = 0; last_resid = 0.0;
+    cp_iters = 0; cp_precond_iters = 0;
     std::fill(H_U.begin(), H_U.end(), 0.0);
     std::fill(rhs_p.begin(), rhs_p.end(), 0.0);
     std::fill(H_U0.begin(), H_U0.end(), 0.0);
@@ -2139,7 +2340,8 @@ struct Solver {
       for (size_t i = 0; i < Cs.size(); ++i) Cs[i] = Cs[i] + dt * (a_k * H_C[i] + b_k * H_C0[i]);
       velocity_bc_refresh();
       p_old = p;
-      correct_velocity(gk_dt, false, true);
+      if (cp_on) std::fill(gp_cell.begin(), gp_cell.end(), 0.0);  // nothing to add back (mod_fv_solver.f90:1373-1377)
+      else correct_velocity(gk_dt, false, true);
       gp_rc = gp_cell;
       velocity_bc_refresh();
       compute_all_gradients();
@@ -2187,7 +2389,12 @@ struct Solver {
       correct_face_fluxes(gk_dt, false);
       U_face = face_flux;
       u_face_ready = true;
-      correct_velocity(gk_dt, true, false);
+      if (cp_on) {
+        int rc2 = project_cells_exact(gk_dt);
+        if (rc2) return rc2;
+      } else {
+        correct_velocity(gk_dt, true, false);
+      }
       velocity_bc_refresh();
       if (P.use_rotational_projection) {
         for (int64_t c = 0; c < nc; ++c) p[c] = p[c] + (P.nu + nu_sgs[c]) * rhs_p[c] * gk_dt * inv_vol[c];
@@ -2271,6 +2478,8 @@ struct Solver {
     s->p_fallbacks = 0;
     s->p_solver_used = DPM_PSOLVER_JACOBI_PCG;
     s->p_bytes_per_iteration = 0.0;  // no device traffic on the CPU
+    s->cp_iters = cp_iters;
+    s->cp_precond_iters = cp_precond_iters;
     apply_velocity_bc(-1, false);  // solver_divergence_metrics refreshes U_bnd without gradients
   }
 };
@@ -2517,6 +2726,12 @@ void orc_wall_model(void* h, const double* U, double* tau) {
   std::memcpy(tau, s->tau_w.data(), sizeof(double) * 3 * s->nb);
 }
 double orc_amd_point(const double* alpha, const double* G, double c_amd) { return orc::amd_point(alpha, G, c_amd); }
+// exact cell projection operators (src/numerics/mod_cell_projection.f90), u and v as (3, nc)
+void orc_cp_divergence(void* h, const double* u, double* out) { static_cast<orc::Solver*>(h)->cp_divergence(u, out); }
+void orc_cp_adjoint(void* h, const double* chi, double* v) { static_cast<orc::Solver*>(h)->cp_adjoint(chi, v); }
+int orc_cp_project(void* h, double* u, const double* bconst, double tol, int max_it, int identity, int* n_it) {
+  return static_cast<orc::Solver*>(h)->cp_project(u, bconst, tol, max_it, identity != 0, n_it);
+}
 void orc_kfactor_limited(const double* sf, const double* d_on, double min_cos, double* k) {
   orc::kfactor_limited(sf, d_on, min_cos, k);
 }

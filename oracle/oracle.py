@@ -55,6 +55,10 @@ def lib():
         L.orc_amd_point.restype = C.c_double
         L.orc_wall_stress_newton.argtypes = [C.c_double, C.c_double, C.c_double, dp, dp]
         L.orc_kfactor_limited.argtypes = [dp, dp, C.c_double, dp]
+        L.orc_cp_divergence.argtypes = [vp, dp, dp]
+        L.orc_cp_adjoint.argtypes = [vp, dp, dp]
+        L.orc_cp_project.argtypes = [vp, dp, dp, C.c_double, C.c_int, C.c_int, ip]
+        L.orc_cp_project.restype = C.c_int
         L.orc_poisson_solve.argtypes = [vp, dp, dp, C.c_double, C.c_double, C.c_int, ip, dp]
         L.orc_poisson_solve.restype = C.c_int
         L.orc_poisson_matvec.argtypes = [vp, dp, dp]

@@ -10,7 +10,7 @@ import os
 import sys
 
 CASES = ("tgv", "tgv_skew", "tgv_skew_chk", "pdrop", "hydro", "hydrowall", "rb", "channel", "amd", "graded",
-         "channel_most")
+         "channel_most", "duct", "duct_exact", "hydro_exact", "tgv_skew_exact", "default_skew")
 COLS = ("step", "time", "E", "Umax", "Ub", "tauw_mean", "nu_sgs_mean", "max_abs_divU", "dt")
 
 
