@@ -231,7 +231,7 @@ def cpu_run(case_name, budget_s, max_steps):
 
 
 PROFILE = {("pcg", "channel"): "k_pcg_channel96x64x64.md", ("fcg", "channel"): "k_fcg_channel96x64x64.md",
-           ("ml", "channel"): "k_mlcg_channel96x64x64.md", ("ml", "urban"): "k_mlcg_urban.md"}
+           ("ml", "channel"): "k_mlcg_channel96x64x64.md", ("ml", "urban"): "k_mlk_urban2m.md", ("ml", "urban2m"): "k_mlk_urban2m.md"}
 
 
 def pcg_traffic_per_launch(psolver, config, nc, its_per_solve):

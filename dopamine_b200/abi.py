@@ -78,6 +78,7 @@ class StatsT(C.Structure):
         ("volavg_abs_divU", C.c_double), ("dt_used", C.c_double), ("p_solves", C.c_int), ("p_iters", C.c_int),
         ("p_resid_max", C.c_double), ("p_fallbacks", C.c_int), ("p_solver_used", C.c_int),
         ("p_bytes_per_iteration", C.c_double), ("cp_iters", C.c_int), ("cp_precond_iters", C.c_int),
+        ("max_abs_divU_cell", C.c_double), ("volavg_abs_divU_cell", C.c_double),
     ]
 
     def as_dict(self):

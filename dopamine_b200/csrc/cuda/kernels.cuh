@@ -1348,6 +1348,38 @@ __global__ void __launch_bounds__(TPB) k_flux_divergence(Dev d, const double* __
   div[c] = v;
 }
 
+// Divergence of the gc-interpolated cell velocity (src/solver/mod_fv_solver.f90:3582-3607): the
+// boundary velocity on boundary faces, periodic ones included; per cell in face order.
+__global__ void __launch_bounds__(TPB) k_cell_velocity_divergence(Dev d, const double* __restrict__ U,
+                                                                  const double* __restrict__ Ub,
+                                                                  double* __restrict__ div) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.nc) return;
+  const int nc = d.nc, nf = d.nf, nfi = d.nfi, nb = d.nb;
+  const double iv = d.ivol[c];
+  double v = 0.0;
+  for (int s = 0; s < d.S; ++s) {
+    const int f = d.cf[s * nc + c];
+    if (f == PADI) break;
+    double u0, u1, u2;
+    bool own = true;
+    if (f < nfi) {
+      const int o = d.fo[f], n = d.fn[f];
+      const double g = d.gc[f];
+      own = o == c;
+      u0 = g * U[o] + (1.0 - g) * U[n];
+      u1 = g * U[nc + o] + (1.0 - g) * U[nc + n];
+      u2 = g * U[2 * nc + o] + (1.0 - g) * U[2 * nc + n];
+    } else {
+      const int b = f - nfi;
+      u0 = Ub[b]; u1 = Ub[nb + b]; u2 = Ub[2 * nb + b];
+    }
+    const double fl = u0 * d.sf[f] + u1 * d.sf[nf + f] + u2 * d.sf[2 * nf + f];
+    v = own ? v + fl * iv : v - fl * iv;
+  }
+  div[c] = v;
+}
+
 // ------------------------------------------------------------------------------------------
 // Small elementwise kernels.
 __global__ void k_rotational(int n, double* p, const double* nus, const double* rhs, const double* ivol, double nu,

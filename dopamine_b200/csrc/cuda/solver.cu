@@ -1817,6 +1817,12 @@ struct Solver {
     s->p_iters = last.p_iters;
     s->p_resid_max = last.p_resid_max;
     velocity_bc(-1, 0);  // solver_divergence_metrics refreshes U_bnd without gradients
+    k_cell_velocity_divergence<<<nblk(nc), TPB, 0, st>>>(d, F.U, F.Ub, scratch_c);
+    launches++;
+    rc = reduce(r2, o2, 3);
+    if (rc) return rc;
+    s->max_abs_divU_cell = o2[0];
+    s->volavg_abs_divU_cell = o2[1] / o2[2];
     CK(cudaStreamSynchronize(st));
     return 0;
   }

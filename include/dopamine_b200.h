@@ -200,6 +200,9 @@ typedef struct dpm_stats {
   int cp_iters;               /* DPM_CELL_PROJECTION_EXACT: outer iterations of the last step's
                                  cell projections (summed over its stages)                    */
   int cp_precond_iters;       /* and the Krylov iterations of their preconditioning solves      */
+  double max_abs_divU_cell, volavg_abs_divU_cell;  /* divergence of the gc-interpolated cell
+                                 velocity (src/solver/mod_fv_solver.f90:3582-3607), a different
+                                 operator from the projected face flux's, not zeroed by it        */
 } dpm_stats_t;
 
 /* Outcome of dpm_learn_train. */

@@ -2481,6 +2481,29 @@ struct Solver {
     s->cp_iters = cp_iters;
     s->cp_precond_iters = cp_precond_iters;
     apply_velocity_bc(-1, false);  // solver_divergence_metrics refreshes U_bnd without gradients
+    // cell_velocity_divergence (mod_fv_solver.f90:3582-3607): every mesh face in order, the
+    // gc-interpolated velocity inside, the boundary velocity on boundary (periodic too) faces
+    std::fill(div.begin(), div.end(), 0.0);
+    for (int64_t f = 0; f < nf; ++f) {
+      int o = m.owner[f], n = m.neighbour[f];
+      double uf[3];
+      if (n >= 0) {
+        double g = m.gc[f];
+        for (int k = 0; k < 3; ++k) uf[k] = g * U[3 * o + k] + (1.0 - g) * U[3 * n + k];
+      } else {
+        for (int k = 0; k < 3; ++k) uf[k] = U_bnd[3 * (f - nfi) + k];
+      }
+      double fl = dot3(uf, &m.sf[3 * f]);
+      div[o] += fl * inv_vol[o];
+      if (n >= 0) div[n] -= fl * inv_vol[n];
+    }
+    mx = 0.0; as = 0.0;
+    for (int64_t c = 0; c < nc; ++c) {
+      mx = std::max(mx, std::fabs(div[c]));
+      as += std::fabs(div[c]) * m.volume[c];
+    }
+    s->max_abs_divU_cell = mx;
+    s->volavg_abs_divU_cell = as / vs;
   }
 };
 

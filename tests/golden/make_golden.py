@@ -1,7 +1,7 @@
 """Regenerates tests/golden/*.csv: the reference's regression statistics (golden vectors) for the
 cases on this path, reduced to the columns the reference's own
 comparison uses (tests/regression/compare_stats.py: time, E, Umax, Ub, tauw_mean, nu_sgs_mean,
-max_abs_divU).  Run in a checkout that has the reference tree:
+max_abs_divU), plus the dissipation and the cell-velocity divergence columns.  Run in a checkout that has the reference tree:
 
     python tests/golden/make_golden.py /path/to/reference
 """
@@ -11,7 +11,8 @@ import sys
 
 CASES = ("tgv", "tgv_skew", "tgv_skew_chk", "pdrop", "hydro", "hydrowall", "rb", "channel", "amd", "graded",
          "channel_most", "duct", "duct_exact", "hydro_exact", "tgv_skew_exact", "default_skew")
-COLS = ("step", "time", "E", "Umax", "Ub", "tauw_mean", "nu_sgs_mean", "max_abs_divU", "dt")
+COLS = ("step", "time", "E", "eps", "Umax", "Ub", "tauw_mean", "nu_sgs_mean", "max_abs_divU", "max_abs_divU_cell",
+        "volavg_abs_divU_cell", "dt")
 
 
 def main(ref_root):

@@ -3,7 +3,8 @@
 tests/golden/<case>_np1.csv are the reference's tests/regression/reference CSVs (made by the
 gfortran CPU build), reduced to the compared columns by tests/golden/make_golden.py.  The check is
 the reference's own (tests/regression/compare_stats.py): integral quantities within rtol 1e-6,
-face-flux divergence below 1e-9.
+face-flux divergence below 1e-9; the dissipation and the cell-velocity divergence columns are held
+to the same 1e-6.
 
 Coverage: KEP / CDS / QUICK momentum advection, skewed and graded meshes, non-orthogonal
 correctors, outlets and walls (tgv*, pdrop, hydro*); Vreman and AMD with the log-law wall model
@@ -23,6 +24,7 @@ from oracle.oracle import Oracle
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
 RTOL, ATOL, DIV_MAX = 1.0e-6, 1.0e-12, 1.0e-9
 COMPARED = ("time", "E", "Umax", "Ub", "tauw_mean", "nu_sgs_mean")
+EXTRA = ("eps", "max_abs_divU_cell", "volavg_abs_divU_cell")
 
 
 def load(case):
@@ -45,7 +47,7 @@ def run_case(name, steps=None):
 
 
 @pytest.mark.parametrize("name", ["tgv_skew", "tgv_skew_chk", "pdrop", "hydro", "hydrowall", "tgv", "rb", "channel",
-                                  "amd", "graded", "channel_most"])
+                                  "amd", "graded", "channel_most", "duct"])
 def test_oracle_matches_reference_csv(name):
     ref, got = run_case(name)
     for step, s in got.items():
@@ -55,6 +57,11 @@ def test_oracle_matches_reference_csv(name):
             err = abs(a - b) / max(abs(a), ATOL / RTOL)
             assert err <= RTOL, f"{name} step {step} {col}: ref={a:.12e} oracle={b:.12e} rel={err:.2e}"
         assert s["max_abs_divU"] <= DIV_MAX, f"{name} step {step} divU {s['max_abs_divU']:.3e}"
+        # beyond the reference's own comparison: the dissipation and the cell-velocity divergence
+        for col in EXTRA:
+            a, b = r[col], s[col]
+            err = abs(a - b) / max(abs(a), ATOL / RTOL)
+            assert err <= RTOL, f"{name} step {step} {col}: ref={a:.12e} oracle={b:.12e} rel={err:.2e}"
 
 
 def test_oracle_dt_clamp_matches_reference():
