@@ -13,12 +13,14 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <filesystem>
 #include <memory>
 #include <string>
 #include <vector>
 
 #include "../../../include/dopamine_b200.h"
 #include "../host/mesh.hpp"
+#include "../host/fortran_records.hpp"
 #include "../host/ops.hpp"
 #include "../host/twolevel.hpp"
 #include "../host/multilevel.hpp"
@@ -30,6 +32,7 @@
 #include "learn.cuh"
 #include "mlsolve.cuh"
 #include "pcg.cuh"
+#include "sampling.cuh"
 #include "scalars.cuh"
 
 namespace dpm {
@@ -181,6 +184,10 @@ struct Solver {
   bool x32 = false;
   Geo32 g32{};
   float *gU32 = nullptr, *gS32 = nullptr, *sc_fadv32 = nullptr, *sc_fdif32 = nullptr;
+  // sample points (sampling.cuh): coordinates (3, n), owner cells, payload (6, n)
+  int samp_n = 0;
+  double *samp_pts = nullptr, *samp_payload = nullptr;
+  int* samp_owner = nullptr;
   // exact cell projection (cellproj.cuh): work vectors, partials and device scalars, allocated
   // on first use; outer and preconditioner iterations of the current step
   bool cp_on = false;
@@ -247,6 +254,7 @@ struct Solver {
   bool flexible() const { return (use_fcg || use_ml) && !force_plain; }
 
   ~Solver() {
+    free_samples();
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (evp0) cudaEventDestroy(evp0);
@@ -1437,6 +1445,235 @@ struct Solver {
     return 0;
   }
 
+  // ---------------------------------------------------------------- sampling (sampling.cuh)
+  void free_samples() {
+    if (samp_pts) cudaFree(samp_pts);
+    if (samp_payload) cudaFree(samp_payload);
+    if (samp_owner) cudaFree(samp_owner);
+    samp_pts = samp_payload = nullptr;
+    samp_owner = nullptr;
+    samp_n = 0;
+  }
+  // cache_object_owners (src/stats/mod_sampling.f90:520-562) for the points xyz(3, n)
+  int set_sample_points(int n, const double* xyz, int* owner_out) {
+    free_samples();
+    if (n <= 0) return 0;
+    CK(cudaMalloc(&samp_pts, 3 * sizeof(double) * n));
+    CK(cudaMalloc(&samp_payload, 6 * sizeof(double) * n));
+    CK(cudaMalloc(&samp_owner, sizeof(int) * n));
+    samp_n = n;
+    CK(cudaMemcpyAsync(samp_pts, xyz, 3 * sizeof(double) * n, cudaMemcpyHostToDevice, st));
+    k_sample_owner<<<(n + SAMPLE_TILE - 1) / SAMPLE_TILE, SAMPLE_TILE, 0, st>>>(d, n, samp_pts, samp_owner);
+    launches++;
+    if (owner_out) CK(cudaMemcpyAsync(owner_out, samp_owner, sizeof(int) * n, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    CK(cudaGetLastError());
+    return 0;
+  }
+  // sample_points_local (:493-518) on the current state; payload(6, n) to the host
+  int sample_points(double* payload) {
+    if (samp_n <= 0) return DPM_ERR_ARG;
+    k_sample_points<<<nblk(samp_n), TPB, 0, st>>>(d, samp_n, samp_pts, samp_owner, F.U, F.Ub, F.p, F.pb, F.T, Tb,
+                                                  F.nu_sgs, samp_payload);
+    launches++;
+    CK(cudaMemcpyAsync(payload, samp_payload, 6 * sizeof(double) * samp_n, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    CK(cudaGetLastError());
+    return 0;
+  }
+
+  // ---------------------------------------------------------------- checkpoint (mod_checkpoint_io.f90)
+  // A device array (SoA [k][n] when k > 1) in the Fortran layout (k, n) on the host.
+  int fetch(const double* dev, int n, int k, std::vector<double>& h) {
+    h.resize((size_t)n * k);
+    if (n == 0) return 0;
+    if (k == 1) {
+      CK(cudaMemcpyAsync(h.data(), dev, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    } else {
+      k_soa_to_aos_k<<<nblk(n), TPB, 0, st>>>(n, k, dev, aos_buf);
+      launches++;
+      CK(cudaMemcpyAsync(h.data(), aos_buf, sizeof(double) * (size_t)n * k, cudaMemcpyDeviceToHost, st));
+    }
+    CK(cudaStreamSynchronize(st));
+    return 0;
+  }
+  int store(double* dev, int n, int k, const std::vector<char>& rec) {
+    if ((int64_t)rec.size() != (int64_t)n * k * 8) return DPM_ERR_ARG;
+    if (n == 0) return 0;
+    if (k == 1) {
+      CK(cudaMemcpyAsync(dev, rec.data(), sizeof(double) * n, cudaMemcpyHostToDevice, st));
+    } else {
+      CK(cudaMemcpyAsync(aos_buf, rec.data(), sizeof(double) * (size_t)n * k, cudaMemcpyHostToDevice, st));
+      k_aos_to_soa_k<<<nblk(n), TPB, 0, st>>>(n, k, aos_buf, dev);
+      launches++;
+    }
+    CK(cudaStreamSynchronize(st));
+    return 0;
+  }
+  // header(8): 1 tau_w_bnd, 2 q_w_bnd, 4 L_bnd (MOST), 8 the wall-stress filter state, 16 eddies
+  int checkpoint_mask() const {
+    int mask = 1;
+    if (P.wall_model == DPM_WM_MOST) mask += 2 + 4;
+    if (filt_ready && P.wall_model == DPM_WM_LOGLAW) mask += 8;
+    return mask;
+  }
+  static std::string checkpoint_file(const char* dir, int file_step) {
+    char name[64];
+    std::snprintf(name, sizeof name, "checkpoint_%08d.bin", file_step);
+    return (std::filesystem::path(dir) / "processor0" / name).string();
+  }
+  // write_checkpoint (:15-138): <dir>/processor0/checkpoint_<step>.bin and <dir>/checkpoint_latest
+  int write_checkpoint(const char* dir, int file_step) {
+    std::error_code ec;
+    std::filesystem::create_directories(std::filesystem::path(dir) / "processor0", ec);
+    if (ec) return DPM_ERR_ARG;
+    const std::string fname = checkpoint_file(dir, file_step);
+    std::FILE* f = std::fopen(fname.c_str(), "wb");
+    if (!f) return DPM_ERR_ARG;
+    bool ok = true;
+    int rc = 0;
+    const int mask = checkpoint_mask();
+    int32_t hdr[8] = {(int32_t)nc, (int32_t)ns, 0, (int32_t)step, ns > 0 ? 1 : 0, 0, u_face_ready ? 1 : 0, mask};
+    ok = ok && frec::write_record(f, hdr, sizeof hdr);
+    ok = ok && frec::write_record(f, &time, sizeof time);
+    {
+      std::vector<int64_t> gid(nc);
+      for (int c = 0; c < nc; ++c) gid[c] = c + 1;
+      ok = ok && (nc == 0 || frec::write_record(f, gid.data(), 8 * (int64_t)nc));
+    }
+    std::vector<double> h;
+    auto put = [&](const double* dev, int n, int k) {
+      if (!ok || rc) return;
+      rc = fetch(dev, n, k, h);
+      if (!rc) ok = frec::write_record(f, h.data(), 8 * (int64_t)n * k);
+    };
+    if (nc > 0) {
+      put(F.U, nc, 3);
+      put(F.p, nc, 1);
+      put(F.T, nc, 1);
+      put(F.nu_sgs, nc, 1);
+      if (ns > 0) put(Cs, nc, ns);
+    }
+    if (u_face_ready) put(F.Uf, nf, 1);
+    put(F.tau, nb, 3);
+    if (mask & 2) put(most_qw, nb, 1);
+    if (mask & 4) put(most_L, nb, 1);
+    if (mask & 8) put(F.upf, nb, 3);
+    ok = (std::fclose(f) == 0) && ok;
+    if (rc) return rc;
+    if (!ok) return DPM_ERR_ARG;
+    std::FILE* l = std::fopen((std::filesystem::path(dir) / "checkpoint_latest").string().c_str(), "w");
+    if (!l) return DPM_ERR_ARG;
+    std::fprintf(l, "%d\n", file_step);
+    return std::fclose(l) == 0 ? 0 : DPM_ERR_ARG;
+  }
+  // read_checkpoint (:143-282) and refresh_after_restart (mod_fv_solver.f90:601-609); file_step
+  // < 0 reads the step that <dir>/checkpoint_latest names
+  int read_checkpoint(const char* dir, int file_step) {
+    if (file_step < 0) {
+      std::FILE* l = std::fopen((std::filesystem::path(dir) / "checkpoint_latest").string().c_str(), "r");
+      if (!l) return DPM_ERR_ARG;
+      int k = -1;
+      const int got = std::fscanf(l, "%d", &k);
+      std::fclose(l);
+      if (got != 1 || k < 0) return DPM_ERR_ARG;
+      file_step = k;
+    }
+    std::FILE* f = std::fopen(checkpoint_file(dir, file_step).c_str(), "rb");
+    if (!f) return DPM_ERR_ARG;
+    std::vector<char> rec;
+    auto next = [&]() { return frec::read_record(f, rec); };
+    int32_t hdr[8];
+    double t = 0.0;
+    int rc = DPM_ERR_ARG;
+    do {
+      if (!next() || rec.size() != sizeof hdr) break;
+      std::memcpy(hdr, rec.data(), sizeof hdr);
+      if (hdr[0] != nc || hdr[1] != ns) {
+        std::fprintf(stderr, "dopamine_b200: checkpoint has %d cells / %d scalars, this handle %d / %d\n", hdr[0],
+                     hdr[1], nc, ns);
+        rc = DPM_ERR_MESH;
+        break;
+      }
+      if (!frec::read_record_into(f, &t, sizeof t)) break;
+      if (nc > 0) {
+        if (!next() || (int64_t)rec.size() != 8 * (int64_t)nc) break;
+        const int64_t* gid = reinterpret_cast<const int64_t*>(rec.data());
+        bool same = true;
+        for (int c = 0; c < nc && same; ++c) same = gid[c] == c + 1;
+        if (!same) {  // the reference stops on a different partition (:205-206)
+          rc = DPM_ERR_MESH;
+          break;
+        }
+        if (!next() || store(F.U, nc, 3, rec)) break;
+        if (!next() || store(F.p, nc, 1, rec)) break;
+        if (!next() || store(F.T, nc, 1, rec)) break;
+        if (!next() || store(F.nu_sgs, nc, 1, rec)) break;
+        if (hdr[1] > 0 && (!next() || store(Cs, nc, ns, rec))) break;
+      }
+      if (hdr[6] == 1) {
+        if (!next() || store(F.Uf, nf, 1, rec)) break;
+        u_face_ready = true;
+      } else {
+        std::fprintf(stderr, "dopamine_b200: checkpoint has no face flux; it is rebuilt from the restored velocity\n");
+      }
+      const int mask = hdr[7];
+      bool bad = false;
+      if (mask & 1) bad = bad || !next() || store(F.tau, nb, 3, rec);
+      if (mask & 2) bad = bad || !next() || (P.wall_model == DPM_WM_MOST && store(most_qw, nb, 1, rec));
+      if (mask & 4) bad = bad || !next() || (P.wall_model == DPM_WM_MOST && store(most_L, nb, 1, rec));
+      if (mask & 8) {
+        bad = bad || !next() || store(F.upf, nb, 3, rec);
+        if (!bad) filt_ready = true;
+      }
+      if (mask & 16) {  // synthetic-eddy inflow state: not on this path, the records are skipped
+        bad = bad || !next() || !next() || !next();
+        std::fprintf(stderr, "dopamine_b200: checkpoint synthetic-eddy state ignored\n");
+      }
+      if (bad) break;
+      rc = 0;
+    } while (false);
+    std::fclose(f);
+    if (rc) return rc;
+    time = t;
+    step = hdr[3];
+    refresh_halos_and_bc();
+    grad_all();
+    pressure_gradient();
+    refresh_halos_and_bc();
+    grad_all();
+    if (!u_face_ready) {
+      rc = rebuild_face_flux();
+      if (rc) return rc;
+    }
+    CK(cudaStreamSynchronize(st));
+    CK(cudaGetLastError());
+    return 0;
+  }
+  // solver_rebuild_face_flux (mod_fv_solver.f90:612-654): one projection whose face flux is kept,
+  // everything else put back
+  int rebuild_face_flux() {
+    const size_t n3 = 3 * (size_t)nc;
+    std::vector<double> U0(n3), p0(nc), pb0(nb), Ub0(3 * (size_t)nb), ff0(nf), pold0(nc), pp0(nc), ppb0(nb), gp0(n3),
+        gprc0(n3);
+    auto down = [&](std::vector<double>& h, const double* dv) {
+      if (!h.empty()) cudaMemcpyAsync(h.data(), dv, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st);
+    };
+    auto up = [&](double* dv, const std::vector<double>& h) {
+      if (!h.empty()) cudaMemcpyAsync(dv, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, st);
+    };
+    down(U0, F.U); down(p0, F.p); down(pb0, F.pb); down(Ub0, F.Ub); down(ff0, F.ff); down(pold0, F.p_old);
+    down(pp0, F.phi_prev); down(ppb0, F.phi_prev_b); down(gp0, F.gp); down(gprc0, F.gp_rc);
+    CK(cudaStreamSynchronize(st));
+    int rc = project_once(P.dt);
+    if (rc) return rc;
+    up(F.U, U0); up(F.p, p0); up(F.pb, pb0); up(F.Ub, Ub0); up(F.ff, ff0); up(F.p_old, pold0);
+    up(F.phi_prev, pp0); up(F.phi_prev_b, ppb0); up(F.gp, gp0); up(F.gp_rc, gprc0);
+    CK(cudaStreamSynchronize(st));
+    u_face_ready = true;
+    return 0;
+  }
+
   // ---------------------------------------------------------------- exact cell projection
   int cp_alloc() {
     if (cp_st) return 0;
@@ -2293,6 +2530,30 @@ int dpm_wall_model(dpm_solver_t* h, const double* U, double nu, double* tau_w) {
   s.P.nu = keep;
   if (s.nb) return download_vec3(s, s.F.tau, tau_w, s.nb);
   return DPM_OK;
+}
+
+int dpm_write_checkpoint(dpm_solver_t* h, const char* checkpoint_dir, int step) {
+  if (!h || !checkpoint_dir || step < 0) return DPM_ERR_ARG;
+  CK(cudaSetDevice(h->s->device));
+  return h->s->write_checkpoint(checkpoint_dir, step);
+}
+
+int dpm_read_checkpoint(dpm_solver_t* h, const char* checkpoint_dir, int step) {
+  if (!h || !checkpoint_dir) return DPM_ERR_ARG;
+  CK(cudaSetDevice(h->s->device));
+  return h->s->read_checkpoint(checkpoint_dir, step);
+}
+
+int dpm_sampling_set_points(dpm_solver_t* h, int n_points, const double* xyz, int* owner_cell) {
+  if (!h || n_points < 0 || (n_points > 0 && !xyz)) return DPM_ERR_ARG;
+  CK(cudaSetDevice(h->s->device));
+  return h->s->set_sample_points(n_points, xyz, owner_cell);
+}
+
+int dpm_sample_points(dpm_solver_t* h, double* payload) {
+  if (!h || !payload) return DPM_ERR_ARG;
+  CK(cudaSetDevice(h->s->device));
+  return h->s->sample_points(payload);
 }
 
 int dpm_cell_divergence(dpm_solver_t* h, const double* u, double* out) {

@@ -28,6 +28,7 @@ EXPORTED = (
     "dpm_learn_collect", "dpm_learn_train", "dpm_learn_set_gamma", "dpm_learn_sizes", "dpm_learn_export",
     "dpm_learn_loss_grad", "dpm_multilevel_hierarchy", "dpm_set_barrier_spin_limit",
     "dpm_select_pressure_solver", "dpm_cell_divergence", "dpm_cell_adjoint_gradient", "dpm_cell_project",
+    "dpm_write_checkpoint", "dpm_read_checkpoint", "dpm_sampling_set_points", "dpm_sample_points",
 )
 
 
@@ -76,6 +77,10 @@ def lib(build_if_missing=True):
     L.dpm_sgs_viscosity.argtypes = [vp, C.c_int, dp, dp, dp, C.c_double, dp]
     L.dpm_wall_model.argtypes = [vp, dp, C.c_double, dp]
     L.dpm_cell_divergence.argtypes = [vp, dp, dp]
+    L.dpm_write_checkpoint.argtypes = [vp, C.c_char_p, C.c_int]
+    L.dpm_read_checkpoint.argtypes = [vp, C.c_char_p, C.c_int]
+    L.dpm_sampling_set_points.argtypes = [vp, C.c_int, dp, ip]
+    L.dpm_sample_points.argtypes = [vp, dp]
     L.dpm_cell_adjoint_gradient.argtypes = [vp, dp, dp]
     L.dpm_cell_project.argtypes = [vp, dp, dp, C.c_double, C.c_int, C.c_int, ip]
     L.dpm_advection_rhs_scalar.argtypes = [vp, C.c_int, dp, dp, dp, dp, dp]
@@ -315,6 +320,28 @@ class Solver:
         tau = np.zeros((self.nb, 3))
         _check(lib().dpm_wall_model(self.h, _p(np.ascontiguousarray(U)), nu, _p(tau)), "dpm_wall_model")
         return tau
+
+    # checkpoint and sampling (src/io/mod_checkpoint_io.f90, src/stats/mod_sampling.f90)
+    def write_checkpoint(self, checkpoint_dir, step):
+        _check(lib().dpm_write_checkpoint(self.h, os.fsencode(checkpoint_dir), int(step)), "dpm_write_checkpoint")
+
+    def read_checkpoint(self, checkpoint_dir, step=-1):
+        _check(lib().dpm_read_checkpoint(self.h, os.fsencode(checkpoint_dir), int(step)), "dpm_read_checkpoint")
+
+    def set_sample_points(self, xyz):
+        """xyz (n, 3); returns the 0-based owner cell of each point."""
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+        owner = np.zeros(len(xyz), dtype=np.int32)
+        _check(lib().dpm_sampling_set_points(self.h, len(xyz), _p(xyz), owner.ctypes.data_as(C.POINTER(C.c_int))),
+               "dpm_sampling_set_points")
+        self._n_samples = len(xyz)
+        return owner
+
+    def sample_points(self):
+        """(n, 6): U(3), p, T, nu_sgs at the points given to set_sample_points."""
+        out = np.zeros((getattr(self, "_n_samples", 0), 6))
+        _check(lib().dpm_sample_points(self.h, _p(out)), "dpm_sample_points")
+        return out
 
     # exact cell projection operators (src/numerics/mod_cell_projection.f90)
     def cell_divergence(self, u):

@@ -344,6 +344,27 @@ int dpm_cell_divergence(dpm_solver_t* s, const double* u, double* out);
 int dpm_cell_adjoint_gradient(dpm_solver_t* s, const double* chi, double* v);
 int dpm_cell_project(dpm_solver_t* s, double* u, const double* bconst, double tol, int max_it, int identity_precond,
                      int* n_it);
+/* ---- output on the device (src/io/mod_checkpoint_io.f90, src/stats/mod_sampling.f90) ---- */
+/* write_checkpoint / read_checkpoint (mod_checkpoint_io.f90:15-282): the reference's per-rank
+ * file <checkpoint_dir>/processor0/checkpoint_<step, 8 digits>.bin as sequential unformatted
+ * records (4-byte markers): header(8) = n_cells, n_scalars, 0, solver step, has scalars, 0, face
+ * flux present, wall-model mask (1 tau_w, 2 q_w, 4 L, 8 wall-stress filter); time; global ids
+ * 1..n_cells (int64); U(3,n); p; T; nu_sgs; C(n_scalars,n); U_face(n_faces); tau_w(3,n_bnd);
+ * q_w; L; the filter state (3,n_bnd) - and the manifest <checkpoint_dir>/checkpoint_latest.
+ * Fields leave the device one record at a time.  Reading (step < 0: the step the manifest
+ * names) restores them, rejects another mesh or partition (DPM_ERR_MESH), skips a synthetic-eddy
+ * record, then refreshes boundary values and gradients as solver_refresh_after_restart does and
+ * rebuilds a missing face flux (solver_rebuild_face_flux). */
+int dpm_write_checkpoint(dpm_solver_t* s, const char* checkpoint_dir, int step);
+int dpm_read_checkpoint(dpm_solver_t* s, const char* checkpoint_dir, int step);
+/* Sampling (mod_sampling.f90): dpm_sampling_set_points finds each point's owner, the cell with
+ * the nearest centroid (cache_object_owners :520-562; owner_cell(n) 0-based, may be NULL);
+ * dpm_sample_points fills payload(6, n) = U(3), p, T, nu_sgs at the points, the owner's value plus
+ * its Green-Gauss gradient times the offset from its centroid (sample_points_local :493-518), with
+ * the gradients taken as sampling_maybe_sample takes them (:171-177).  Only the payload crosses
+ * PCIe; the NetCDF files are written by the host (dopamine_b200/sampling.py). */
+int dpm_sampling_set_points(dpm_solver_t* s, int n_points, const double* xyz, int* owner_cell);
+int dpm_sample_points(dpm_solver_t* s, double* payload);
 /* Passive scalars C(n_scalars, n) in the reference's Fortran layout (src/solver/mod_fv_solver.f90:326,
  * scalar index fastest); the temperature travels with dpm_upload_state / dpm_download_state. */
 int dpm_upload_scalars(dpm_solver_t* s, const double* C);

@@ -2224,6 +2224,39 @@ struct Solver {
     return rc;
   }
 
+  // src/stats/mod_sampling.f90:520-562 (cache_object_owners, one rank) and :493-518
+  // (sample_points_local) with the gradients of sampling_maybe_sample (:171-177): one
+  // Green-Gauss pass with the boundary values of U, p and T, the owner's value for nu_sgs.
+  void sample_points(int np, const double* xyz, double* payload, int* owner) {
+    std::vector<double> gu(9 * nc), gpv(3 * nc), gt(3 * nc), gn(3 * nc), nub(nb);
+    for (int64_t b = 0; b < nb; ++b) nub[b] = nu_sgs[m.owner[nfi + b]];
+    gg_gradient_vector(U.data(), U_bnd.data(), gu.data(), nullptr);
+    gg_gradient_scalar(p.data(), p_bnd.data(), gpv.data(), nullptr);
+    gg_gradient_scalar(T.data(), T_bnd.data(), gt.data(), nullptr);
+    gg_gradient_scalar(nu_sgs.data(), nub.data(), gn.data(), nullptr);
+    for (int i = 0; i < np; ++i) {
+      const double* x = xyz + 3 * i;
+      double best = 1.7976931348623157e308;
+      int c = -1;
+      for (int64_t k = 0; k < nc; ++k) {
+        const double* ck = &m.centroid[3 * k];
+        double dx = ck[0] - x[0], dy = ck[1] - x[1], dz = ck[2] - x[2];
+        double d2 = (dx * dx + dy * dy) + dz * dz;
+        if (d2 < best) { best = d2; c = (int)k; }
+      }
+      if (owner) owner[i] = c;
+      double* out = payload + 6 * (size_t)i;
+      if (c < 0) { for (int k = 0; k < 6; ++k) out[k] = 0.0; continue; }
+      double d[3];
+      for (int k = 0; k < 3; ++k) d[k] = x[k] - m.centroid[3 * c + k];
+      for (int j = 0; j < 3; ++j)
+        out[j] = U[3 * c + j] + (gu[9 * c + 3 * j] * d[0] + gu[9 * c + 3 * j + 1] * d[1] + gu[9 * c + 3 * j + 2] * d[2]);
+      out[3] = p[c] + (gpv[3 * c] * d[0] + gpv[3 * c + 1] * d[1] + gpv[3 * c + 2] * d[2]);
+      out[4] = T[c] + (gt[3 * c] * d[0] + gt[3 * c + 1] * d[1] + gt[3 * c + 2] * d[2]);
+      out[5] = nu_sgs[c] + (gn[3 * c] * d[0] + gn[3 * c + 1] * d[1] + gn[3 * c + 2] * d[2]);
+    }
+  }
+
   // src/solver/mod_fv_solver.f90:837-918
   int project_once(double dt) {
     std::fill(rhs_p.begin(), rhs_p.end(), 0.0);
@@ -2754,6 +2787,9 @@ void orc_cp_divergence(void* h, const double* u, double* out) { static_cast<orc:
 void orc_cp_adjoint(void* h, const double* chi, double* v) { static_cast<orc::Solver*>(h)->cp_adjoint(chi, v); }
 int orc_cp_project(void* h, double* u, const double* bconst, double tol, int max_it, int identity, int* n_it) {
   return static_cast<orc::Solver*>(h)->cp_project(u, bconst, tol, max_it, identity != 0, n_it);
+}
+void orc_sample_points(void* h, int np, const double* xyz, double* payload, int* owner) {
+  static_cast<orc::Solver*>(h)->sample_points(np, xyz, payload, owner);
 }
 void orc_kfactor_limited(const double* sf, const double* d_on, double min_cos, double* k) {
   orc::kfactor_limited(sf, d_on, min_cos, k);

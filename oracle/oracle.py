@@ -55,6 +55,7 @@ def lib():
         L.orc_amd_point.restype = C.c_double
         L.orc_wall_stress_newton.argtypes = [C.c_double, C.c_double, C.c_double, dp, dp]
         L.orc_kfactor_limited.argtypes = [dp, dp, C.c_double, dp]
+        L.orc_sample_points.argtypes = [vp, C.c_int, dp, dp, ip]
         L.orc_cp_divergence.argtypes = [vp, dp, dp]
         L.orc_cp_adjoint.argtypes = [vp, dp, dp]
         L.orc_cp_project.argtypes = [vp, dp, dp, C.c_double, C.c_int, C.c_int, ip]
