@@ -67,8 +67,52 @@ class ParamsT(C.Structure):
         ("p_ml_degree", C.c_int), ("p_ml_overcorrect", C.c_double), ("p_ml_passes", C.c_int),
         ("gradient_scheme", C.c_int), ("gg_iterations", C.c_int), ("p_stall_window", C.c_int),
         ("p_stall_ratio", C.c_double), ("p_ml_value_bits", C.c_int), ("cell_projection", C.c_int),
-        ("cell_projection_tol", C.c_double),
+        ("cell_projection_tol", C.c_double), ("constant_mass_flux_forcing", C.c_int),
+        ("U_bulk_target", C.c_double * 3), ("use_harmonic_forcing", C.c_int), ("forcing_amp", C.c_double),
+        ("forcing_omega", C.c_double), ("forcing_phase", C.c_double), ("forcing_dir", C.c_double * 3),
+        ("use_rotation", C.c_int), ("omega_rot", C.c_double * 3), ("use_nudging", C.c_int),
+        ("nudging_tau", C.c_double), ("nudging_z_start", C.c_double), ("nudging_z_full", C.c_double),
+        ("nudging_horizontal_only", C.c_int),
     ]
+
+
+class ScalarSourceT(C.Structure):
+    _fields_ = [
+        ("enabled", C.c_int), ("scalar_id", C.c_int), ("src_kind", C.c_int), ("shape", C.c_int),
+        ("time_mode", C.c_int), ("magnitude", C.c_double), ("omega", C.c_double), ("phase", C.c_double),
+        ("center", C.c_double * 3), ("p0", C.c_double * 3), ("p1", C.c_double * 3), ("normal", C.c_double * 3),
+        ("half_thickness", C.c_double), ("radius", C.c_double), ("box_min", C.c_double * 3),
+        ("box_max", C.c_double * 3), ("tag_radius", C.c_double), ("n_tag_points", C.c_int),
+        ("tag_points", C.POINTER(C.c_double)),
+    ]
+
+
+SRC_POINT, SRC_LINE, SRC_SURFACE, SRC_VOLUME, SRC_OBJ = 1, 2, 3, 4, 5
+SHAPE_SPHERE, SHAPE_BOX, SHAPE_PLANE = 1, 2, 3
+TIME_CONSTANT, TIME_HARMONIC = 1, 2
+
+
+def scalar_sources(defs):
+    """dicts of ScalarSourceT fields -> (ctypes array, keep-alive list); the reference's defaults
+    (mod_scalar.f90:ScalarSourceDef) for what a dict leaves out."""
+    arr = (ScalarSourceT * max(1, len(defs)))()
+    keep = []
+    for i, dd in enumerate(defs):
+        s = arr[i]
+        s.enabled, s.scalar_id, s.src_kind, s.shape, s.time_mode = 1, 1, SRC_VOLUME, SHAPE_SPHERE, TIME_CONSTANT
+        s.normal[2] = 1.0
+        for k, v in dd.items():
+            if k == "tag_points":
+                pts = np.ascontiguousarray(v, dtype=np.float64).reshape(-1, 3)
+                keep.append(pts)
+                s.n_tag_points = len(pts)
+                s.tag_points = pts.ctypes.data_as(C.POINTER(C.c_double))
+            elif isinstance(getattr(s, k), C.Array):
+                for j, x in enumerate(v):
+                    getattr(s, k)[j] = x
+            else:
+                setattr(s, k, v)
+    return arr, keep
 
 
 class StatsT(C.Structure):
@@ -140,8 +184,11 @@ def default_params(**kw):
     p.gg_iterations = 2
     p.cell_projection = CELL_PROJECTION_LS
     p.cell_projection_tol = 0.1
+    p.forcing_dir[0] = 1.0
+    p.nudging_tau = 1800.0
+    p.nudging_horizontal_only = 1
     for k, v in kw.items():
-        if k in ("f_const", "g", "scalar_diffusivity", "scalar_pr_t"):
+        if k in ("f_const", "g", "scalar_diffusivity", "scalar_pr_t", "U_bulk_target", "forcing_dir", "omega_rot"):
             arr = getattr(p, k)
             for i in range(len(v)):
                 arr[i] = v[i]

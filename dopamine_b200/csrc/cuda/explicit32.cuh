@@ -412,10 +412,14 @@ __global__ void __launch_bounds__(TPB) k_cell_momentum32(Dev d, Geo32 g, Explici
     for (int k = 0; k < 3; ++k) cv[k] += 0.5f * (float)u[k] * dv * iv;
   const double fb[3] = {a.f0, a.f1, a.f2}, gv[3] = {a.g0, a.g1, a.g2};
   double h[3];
-  for (int k = 0; k < 3; ++k) {
-    h[k] = (double)(cv[k] + vs[k]) + fb[k];
-    if (a.bous) h[k] = h[k] - a.beta * (T[c] - a.T_ref) * gv[k];
+  for (int k = 0; k < 3; ++k) h[k] = (double)(cv[k] + vs[k]) + fb[k];
+  if (a.rot) {  // Coriolis, -2 Omega x U (mod_fv_solver.f90:1688-1692)
+    h[0] = h[0] - 2.0 * (a.om1 * u[2] - a.om2 * u[1]);
+    h[1] = h[1] - 2.0 * (a.om2 * u[0] - a.om0 * u[2]);
+    h[2] = h[2] - 2.0 * (a.om0 * u[1] - a.om1 * u[0]);
   }
+  if (a.bous)
+    for (int k = 0; k < 3; ++k) h[k] = h[k] - a.beta * (T[c] - a.T_ref) * gv[k];
   for (int s = 0; s < d.SB; ++s) {
     int b = d.cbn[s * nc + c];
     if (b == PADI) break;

@@ -991,7 +991,9 @@ __global__ void __launch_bounds__(TPB) k_face_explicit(Dev d, int scheme, double
 // (src/solver/mod_fv_solver.f90:1617-1762, 2238-2276, 1322-1333).  H is kept for the next stage.
 struct ExplicitArgs {
   int scheme;
-  double f0, f1, f2;
+  double f0, f1, f2;  // uniform body force: constant or mass-flux, plus the harmonic forcing
+  int rot;            // Coriolis with the rotation vector (om0, om1, om2)
+  double om0, om1, om2;
   int bous;
   double beta, T_ref, g0, g1, g2;
   double dt, a_k, b_k;
@@ -1024,10 +1026,14 @@ __global__ void __launch_bounds__(TPB) k_cell_explicit(Dev d, ExplicitArgs a, do
     for (int k = 0; k < 3; ++k) cv[k] += 0.5 * u[k] * dv * iv;
   const double fb[3] = {a.f0, a.f1, a.f2}, gv[3] = {a.g0, a.g1, a.g2};
   double h[3];
-  for (int k = 0; k < 3; ++k) {
-    h[k] = cv[k] + vs[k] + fb[k];
-    if (a.bous) h[k] = h[k] - a.beta * (T[c] - a.T_ref) * gv[k];
+  for (int k = 0; k < 3; ++k) h[k] = cv[k] + vs[k] + fb[k];
+  if (a.rot) {  // Coriolis, -2 Omega x U (mod_fv_solver.f90:1688-1692)
+    h[0] = h[0] - 2.0 * (a.om1 * u[2] - a.om2 * u[1]);
+    h[1] = h[1] - 2.0 * (a.om2 * u[0] - a.om0 * u[2]);
+    h[2] = h[2] - 2.0 * (a.om0 * u[1] - a.om1 * u[0]);
   }
+  if (a.bous)
+    for (int k = 0; k < 3; ++k) h[k] = h[k] - a.beta * (T[c] - a.T_ref) * gv[k];
   for (int s = 0; s < d.SB; ++s) {
     int b = d.cbn[s * nc + c];
     if (b == PADI) break;
@@ -1049,7 +1055,7 @@ __global__ void __launch_bounds__(TPB) k_cell_explicit(Dev d, ExplicitArgs a, do
 // by both of its cells, with identical values) and sums them in ascending face order as
 // k_cell_explicit does, so nothing goes through the per-face flux arrays.  Neighbouring cells
 // still read U, so the predicted velocity goes to Unew (the caller swaps the buffers).
-__global__ void __launch_bounds__(TPB) k_cell_momentum(Dev d, ExplicitArgs a, double nu, const double* __restrict__ U,
+__global__ void __launch_bounds__(TPB, 2) k_cell_momentum(Dev d, ExplicitArgs a, double nu, const double* __restrict__ U,
                                                        const double* __restrict__ Ub, const double* __restrict__ gU,
                                                        const double* __restrict__ nus, const double* __restrict__ Uface,
                                                        const double* __restrict__ T, const double* __restrict__ tau,
@@ -1077,10 +1083,14 @@ __global__ void __launch_bounds__(TPB) k_cell_momentum(Dev d, ExplicitArgs a, do
     for (int k = 0; k < 3; ++k) cv[k] += 0.5 * u[k] * dv * iv;
   const double fb[3] = {a.f0, a.f1, a.f2}, gv[3] = {a.g0, a.g1, a.g2};
   double h[3];
-  for (int k = 0; k < 3; ++k) {
-    h[k] = cv[k] + vs[k] + fb[k];
-    if (a.bous) h[k] = h[k] - a.beta * (T[c] - a.T_ref) * gv[k];
+  for (int k = 0; k < 3; ++k) h[k] = cv[k] + vs[k] + fb[k];
+  if (a.rot) {  // Coriolis, -2 Omega x U (mod_fv_solver.f90:1688-1692)
+    h[0] = h[0] - 2.0 * (a.om1 * u[2] - a.om2 * u[1]);
+    h[1] = h[1] - 2.0 * (a.om2 * u[0] - a.om0 * u[2]);
+    h[2] = h[2] - 2.0 * (a.om0 * u[1] - a.om1 * u[0]);
   }
+  if (a.bous)
+    for (int k = 0; k < 3; ++k) h[k] = h[k] - a.beta * (T[c] - a.T_ref) * gv[k];
   for (int s = 0; s < d.SB; ++s) {
     int b = d.cbn[s * nc + c];
     if (b == PADI) break;

@@ -28,6 +28,7 @@
 #include "common.cuh"
 #include "explicit32.cuh"
 #include "fcg.cuh"
+#include "forcing.cuh"
 #include "kernels.cuh"
 #include "learn.cuh"
 #include "mlsolve.cuh"
@@ -184,6 +185,13 @@ struct Solver {
   bool x32 = false;
   Geo32 g32{};
   float *gU32 = nullptr, *gS32 = nullptr, *sc_fadv32 = nullptr, *sc_fdif32 = nullptr;
+  // mass-flux forcing of the current step; Davies nudging profiles; passive-scalar sources
+  double mass_flux_force[3] = {0.0, 0.0, 0.0};
+  int nd_nt = 0, nd_nz = 0;
+  std::vector<double> nd_times_h, nd_z_h;
+  double *nd_z = nullptr, *nd_U = nullptr, *nd_T = nullptr;
+  std::vector<dpm_scalar_source_t> srcs;
+  std::vector<double*> src_tags;  // device tag points per source (null when none)
   // sample points (sampling.cuh): coordinates (3, n), owner cells, payload (6, n)
   int samp_n = 0;
   double *samp_pts = nullptr, *samp_payload = nullptr;
@@ -255,6 +263,9 @@ struct Solver {
 
   ~Solver() {
     free_samples();
+    free_sources();
+    for (double* p : {nd_z, nd_U, nd_T})
+      if (p) cudaFree(p);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (evp0) cudaEventDestroy(evp0);
@@ -442,6 +453,7 @@ struct Solver {
       if (rc) return rc;
       rc = setup_x32();
       if (rc) return rc;
+      if (x32 && P.use_nudging) return DPM_ERR_UNSUPPORTED;  // the FP32 explicit half fuses the predictor
     }
     if (P.p_solver == DPM_PSOLVER_TWOLEVEL_FCG) {
       int rc = setup_fcg(dev_sms);
@@ -616,10 +628,42 @@ struct Solver {
     if (filter) filt_ready = true;
   }
 
+  // body_force_now (src/solver/mod_fv_solver.f90:2903-2922): constant or mass-flux forcing plus the
+  // harmonic forcing at time t
+  void body_force(double t, double f[3]) const {
+    for (int k = 0; k < 3; ++k) f[k] = P.constant_mass_flux_forcing ? mass_flux_force[k] : P.f_const[k];
+    if (P.use_harmonic_forcing) {
+      const double* fd = P.forcing_dir;
+      const double dn = std::sqrt(fd[0] * fd[0] + fd[1] * fd[1] + fd[2] * fd[2]);
+      double hd[3] = {1.0, 0.0, 0.0};
+      if (dn > SMALL)
+        for (int k = 0; k < 3; ++k) hd[k] = fd[k] / dn;
+      const double hs = P.forcing_amp * std::cos(P.forcing_omega * t + P.forcing_phase);
+      for (int k = 0; k < 3; ++k) f[k] = f[k] + hs * hd[k];
+    }
+  }
+  void set_forces(ExplicitArgs& a) const {
+    double f[3];
+    body_force(time, f);
+    a.f0 = f[0]; a.f1 = f[1]; a.f2 = f[2];
+    a.rot = P.use_rotation ? 1 : 0;
+    a.om0 = P.omega_rot[0]; a.om1 = P.omega_rot[1]; a.om2 = P.omega_rot[2];
+  }
+  // update_mass_flux_forcing (mod_fv_solver.f90:959-983): (U_bulk_target - <U>) / dt
+  int update_mass_flux_forcing(double dt) {
+    RedArgs r{};
+    r.mode = RED_STATS; r.n = nc; r.a = F.U; r.vol = d.vol; r.gU = F.gU; r.nus = F.nu_sgs; r.nu = P.nu;
+    double o[RED_NV];
+    int rc = reduce(r, o, RED_NV);
+    if (rc) return rc;
+    for (int k = 0; k < 3; ++k) mass_flux_force[k] = (P.U_bulk_target[k] - o[3 + k] / std::max(S.V_total, SMALL)) / dt;
+    return 0;
+  }
+
   void explicit_rhs(double dt, double a_k, double b_k, int predict) {
     ExplicitArgs a{};
     a.scheme = P.scheme;
-    a.f0 = P.f_const[0]; a.f1 = P.f_const[1]; a.f2 = P.f_const[2];
+    set_forces(a);
     a.bous = P.boussinesq; a.beta = P.beta; a.T_ref = P.T_ref; a.g0 = P.g[0]; a.g1 = P.g[1]; a.g2 = P.g[2];
     a.dt = dt; a.a_k = a_k; a.b_k = b_k; a.predict = predict;
     if (predict) {  // cell-owned fused pass, predicted velocity into the spare buffer
@@ -640,7 +684,9 @@ struct Solver {
     a.dt = dt;
     a.do_cross = with_cross && !S.skip_nonortho;
     a.ptot = ptot;
-    a.f0 = P.f_const[0]; a.f1 = P.f_const[1]; a.f2 = P.f_const[2];
+    double fb[3];
+    body_force(time, fb);
+    a.f0 = fb[0]; a.f1 = fb[1]; a.f2 = fb[2];
     a.bb = P.boussinesq ? P.beta : 0.0; a.T_ref = P.T_ref; a.g0 = P.g[0]; a.g1 = P.g[1]; a.g2 = P.g[2];
     k_correct_velocity<<<nblk(nc), TPB, 0, st>>>(d, a, F.p, F.gp, F.T, F.U, F.gpc);
     launches++;
@@ -806,7 +852,7 @@ struct Solver {
   void explicit_rhs32(double dt, double a_k, double b_k) {
     ExplicitArgs a{};
     a.scheme = P.scheme;
-    a.f0 = P.f_const[0]; a.f1 = P.f_const[1]; a.f2 = P.f_const[2];
+    set_forces(a);
     a.bous = P.boussinesq; a.beta = P.beta; a.T_ref = P.T_ref; a.g0 = P.g[0]; a.g1 = P.g[1]; a.g2 = P.g[2];
     a.dt = dt; a.a_k = a_k; a.b_k = b_k; a.predict = 1;
     k_cell_momentum32<<<nblk(nc), TPB, 0, st>>>(d, g32, a, (float)P.nu, F.U, F.Ub, gU32, F.nu_sgs, F.Uf, F.T, F.tau,
@@ -899,7 +945,7 @@ struct Solver {
   }
   // All transported fields together: one face pass for every field (the fields do not read each
   // other), then each field's gather and RK3W update.
-  void scalars_rhs(double dt, double a_k, double b_k) {
+  void scalars_rhs(double dt, double a_k, double b_k, int predict = 1) {
     ScalarFaceSet q{};
     double* H[LS_SET];
     const double* H0[LS_SET];
@@ -922,7 +968,7 @@ struct Solver {
     launches++;
     for (int k = 0; k < q.n; ++k) {
       k_cell_scalar<<<nblk(nc), TPB, 0, st>>>(d, q.fadv[k], q.fdif[k], H[k], H0[k], phi[k], nullptr, nullptr, dt, a_k,
-                                              b_k, 1, qw[k]);
+                                              b_k, predict, qw[k]);
       launches++;
     }
   }
@@ -1445,6 +1491,74 @@ struct Solver {
     return 0;
   }
 
+  // ---------------------------------------------------------------- sources (forcing.cuh)
+  bool split_rhs() const { return P.use_nudging || !srcs.empty(); }
+  // compute_explicit_rhs's tail (mod_fv_solver.f90:1741-1760): scalar sources in their order, then
+  // the nudging of U and T, at the stage time
+  void add_sources_and_nudging() {
+    for (size_t i = 0; i < srcs.size(); ++i) {
+      const dpm_scalar_source_t& q = srcs[i];
+      if (!q.enabled || q.scalar_id < 1 || q.scalar_id > ns) continue;
+      k_scalar_source<<<nblk(nc), TPB, 0, st>>>(d, q, src_tags[i], time, HC + (size_t)(q.scalar_id - 1) * nc);
+      launches++;
+    }
+    if (P.use_nudging && nd_nt > 0) {
+      NudgeArgs a{};
+      interp_find(nd_times_h.data(), nd_nt, time, a.it1, a.it2, a.wt);
+      a.nz = nd_nz;
+      a.horiz = P.nudging_horizontal_only ? 1 : 0;
+      a.coeff = 1.0 / std::max(P.nudging_tau, NUDGE_SMALL);
+      if (P.dt > NUDGE_SMALL) a.coeff = std::min(a.coeff, 0.5 / P.dt);
+      a.zs = P.nudging_z_start;
+      a.zt = P.nudging_z_full;
+      a.z = nd_z; a.Up = nd_U; a.Tp = nd_T;
+      k_nudging<<<nblk(nc), TPB, 0, st>>>(d, a, F.U, F.T, F.H, HT);
+      launches++;
+    }
+  }
+  template <class T>
+  int dev_copy(T** dst, const T* src, size_t n) {
+    if (*dst) cudaFree(*dst);
+    *dst = nullptr;
+    CK(cudaMalloc(dst, std::max<size_t>(n, 1) * sizeof(T)));
+    if (n) CK(cudaMemcpy(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice));
+    return 0;
+  }
+  int set_nudging(int nt, int nz, const double* times, const double* z, const double* Up, const double* Tp) {
+    if (nt < 1 || nz < 1 || !times || !z || !Up || !Tp) return DPM_ERR_ARG;
+    if (x32) return DPM_ERR_UNSUPPORTED;
+    nd_nt = nt; nd_nz = nz;
+    nd_times_h.assign(times, times + nt);
+    nd_z_h.assign(z, z + nz);
+    int rc = dev_copy(&nd_z, z, (size_t)nz);
+    if (!rc) rc = dev_copy(&nd_U, Up, 3 * (size_t)nz * nt);
+    if (!rc) rc = dev_copy(&nd_T, Tp, (size_t)nz * nt);
+    return rc;
+  }
+  void free_sources() {
+    for (double* p : src_tags)
+      if (p) cudaFree(p);
+    src_tags.clear();
+    srcs.clear();
+  }
+  int set_sources(int n, const dpm_scalar_source_t* q) {
+    if (n < 0 || (n > 0 && !q)) return DPM_ERR_ARG;
+    if (n > 0 && x32) return DPM_ERR_UNSUPPORTED;
+    free_sources();
+    for (int i = 0; i < n; ++i) {
+      dpm_scalar_source_t s = q[i];
+      double* tags = nullptr;
+      if (s.n_tag_points > 0 && s.tag_points) {
+        int rc = dev_copy(&tags, s.tag_points, 3 * (size_t)s.n_tag_points);
+        if (rc) return rc;
+      }
+      s.tag_points = nullptr;
+      srcs.push_back(s);
+      src_tags.push_back(tags);
+    }
+    return 0;
+  }
+
   // ---------------------------------------------------------------- sampling (sampling.cuh)
   void free_samples() {
     if (samp_pts) cudaFree(samp_pts);
@@ -1852,6 +1966,10 @@ struct Solver {
       if (rc) return rc;
       if (dt > ds) dt = ds;
     }
+    if (P.constant_mass_flux_forcing) {
+      int rc = update_mass_flux_forcing(dt);
+      if (rc) return rc;
+    }
     poisson_ms_acc = 0.0;
     cudaEventRecord(ev0, st);
     last.dt_used = dt;
@@ -1860,7 +1978,7 @@ struct Solver {
     launch_fill(F.H, 3 * (int64_t)nc, 0.0);
     launch_fill(F.H0, 3 * (int64_t)nc, 0.0);
     launch_fill(F.rhs, nc, 0.0);
-    if (P.boussinesq) {
+    if (P.boussinesq || P.use_nudging) {
       launch_fill(HT, nc, 0.0);
       launch_fill(HT0, nc, 0.0);
     }
@@ -1879,6 +1997,25 @@ struct Solver {
         wall_model(k == 0 ? dt : 0.0);
         explicit_rhs32(dt, RK3W_ALPHA[k], RK3W_BETA[k]);
         scalars_rhs32(dt, RK3W_ALPHA[k], RK3W_BETA[k]);
+      } else if (split_rhs()) {  // sources or nudging: assemble H, add them, then predict
+        grad_all();
+        sgs(gk_dt);
+        wall_model(k == 0 ? dt : 0.0);
+        explicit_rhs(dt, RK3W_ALPHA[k], RK3W_BETA[k], 0);
+        if (!P.boussinesq) launch_fill(HT, nc, 0.0);
+        scalars_rhs(dt, RK3W_ALPHA[k], RK3W_BETA[k], 0);
+        add_sources_and_nudging();
+        const double a_k = RK3W_ALPHA[k], b_k = RK3W_BETA[k];
+        k_rk_predict<<<nblk(3 * (int64_t)nc), TPB, 0, st>>>(3 * (int64_t)nc, dt, a_k, b_k, F.H, F.H0, F.U);
+        launches++;
+        if (P.boussinesq || P.use_nudging) {
+          k_rk_predict<<<nblk(nc), TPB, 0, st>>>(nc, dt, a_k, b_k, HT, HT0, F.T);
+          launches++;
+        }
+        if (ns > 0) {
+          k_rk_predict<<<nblk((int64_t)ns * nc), TPB, 0, st>>>((int64_t)ns * nc, dt, a_k, b_k, HC, HC0, Cs);
+          launches++;
+        }
       } else {
         grad_all();
         sgs(gk_dt);
@@ -2554,6 +2691,19 @@ int dpm_sample_points(dpm_solver_t* h, double* payload) {
   if (!h || !payload) return DPM_ERR_ARG;
   CK(cudaSetDevice(h->s->device));
   return h->s->sample_points(payload);
+}
+
+int dpm_set_nudging_profiles(dpm_solver_t* h, int n_times, int n_levels, const double* times, const double* z_levels,
+                             const double* U_profile, const double* T_profile) {
+  if (!h) return DPM_ERR_ARG;
+  CK(cudaSetDevice(h->s->device));
+  return h->s->set_nudging(n_times, n_levels, times, z_levels, U_profile, T_profile);
+}
+
+int dpm_set_scalar_sources(dpm_solver_t* h, int n_sources, const dpm_scalar_source_t* sources) {
+  if (!h) return DPM_ERR_ARG;
+  CK(cudaSetDevice(h->s->device));
+  return h->s->set_sources(n_sources, sources);
 }
 
 int dpm_cell_divergence(dpm_solver_t* h, const double* u, double* out) {

@@ -18,12 +18,12 @@ constexpr int64_t kMaxSub = 2147483639;  // largest subrecord payload gfortran w
 
 inline bool write_marker(std::FILE* f, int32_t m) { return std::fwrite(&m, 4, 1, f) == 1; }
 
-inline bool write_record(std::FILE* f, const void* data, int64_t bytes) {
+inline bool write_record(std::FILE* f, const void* data, int64_t bytes, int64_t max_sub = kMaxSub) {
   const char* p = static_cast<const char*>(data);
   int64_t left = bytes;
   bool first = true;
   do {
-    const int64_t len = left > kMaxSub ? kMaxSub : left;
+    const int64_t len = left > max_sub ? max_sub : left;
     const bool more = left > len;
     if (!write_marker(f, more ? -(int32_t)len : (int32_t)len)) return false;
     if (len && std::fwrite(p, 1, (size_t)len, f) != (size_t)len) return false;

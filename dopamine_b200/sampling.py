@@ -14,7 +14,6 @@ and writes the reference's files:
   every dpm_stats_t field the reference prints, in its column order and number format.
 """
 import math
-import os
 
 import numpy as np
 
@@ -169,12 +168,15 @@ STATS_HEADER = ("step,time,E,eps,E_over_E0,eps_ref,Umax,max_abs_divU,volavg_abs_
 
 
 def _es18_9(x):
-    """Fortran ES18.9: one leading digit, 9 decimals, an E with a signed two-digit exponent,
-    right-justified in 18 columns."""
+    """Fortran ES18.9: one leading digit, 9 decimals and a signed exponent - 'E' and two digits,
+    or three digits without the 'E' beyond +-99 - right-justified in 18 columns."""
     if x == 0.0:
         return f"{'0.000000000E+00':>18}"
     m, e = f"{x:.9E}".split("E")
-    return f"{m + 'E' + ('+' if int(e) >= 0 else '-') + f'{abs(int(e)):02d}':>18}"
+    e = int(e)
+    sign = "+" if e >= 0 else "-"
+    tail = f"E{sign}{abs(e):02d}" if abs(e) <= 99 else f"{sign}{abs(e):03d}"
+    return f"{m + tail:>18}"
 
 
 class StatsWriter:

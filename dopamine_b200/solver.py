@@ -29,6 +29,7 @@ EXPORTED = (
     "dpm_learn_loss_grad", "dpm_multilevel_hierarchy", "dpm_set_barrier_spin_limit",
     "dpm_select_pressure_solver", "dpm_cell_divergence", "dpm_cell_adjoint_gradient", "dpm_cell_project",
     "dpm_write_checkpoint", "dpm_read_checkpoint", "dpm_sampling_set_points", "dpm_sample_points",
+    "dpm_set_nudging_profiles", "dpm_set_scalar_sources",
 )
 
 
@@ -81,6 +82,8 @@ def lib(build_if_missing=True):
     L.dpm_read_checkpoint.argtypes = [vp, C.c_char_p, C.c_int]
     L.dpm_sampling_set_points.argtypes = [vp, C.c_int, dp, ip]
     L.dpm_sample_points.argtypes = [vp, dp]
+    L.dpm_set_nudging_profiles.argtypes = [vp, C.c_int, C.c_int, dp, dp, dp, dp]
+    L.dpm_set_scalar_sources.argtypes = [vp, C.c_int, C.POINTER(abi.ScalarSourceT)]
     L.dpm_cell_adjoint_gradient.argtypes = [vp, dp, dp]
     L.dpm_cell_project.argtypes = [vp, dp, dp, C.c_double, C.c_int, C.c_int, ip]
     L.dpm_advection_rhs_scalar.argtypes = [vp, C.c_int, dp, dp, dp, dp, dp]
@@ -320,6 +323,20 @@ class Solver:
         tau = np.zeros((self.nb, 3))
         _check(lib().dpm_wall_model(self.h, _p(np.ascontiguousarray(U)), nu, _p(tau)), "dpm_wall_model")
         return tau
+
+    # right-hand-side sources (src/abl/mod_abl_weather.f90, src/mod_scalar.f90)
+    def set_nudging_profiles(self, times, z_levels, U_profile, T_profile):
+        """times (nt), z_levels (nz), U_profile (nt, nz, 3), T_profile (nt, nz)."""
+        t = np.ascontiguousarray(times, dtype=np.float64)
+        z = np.ascontiguousarray(z_levels, dtype=np.float64)
+        Up = np.ascontiguousarray(U_profile, dtype=np.float64)  # C (nt, nz, 3) = Fortran (3, nz, nt)
+        Tp = np.ascontiguousarray(T_profile, dtype=np.float64)
+        _check(lib().dpm_set_nudging_profiles(self.h, len(t), len(z), _p(t), _p(z), _p(Up), _p(Tp)),
+               "dpm_set_nudging_profiles")
+
+    def set_scalar_sources(self, defs):
+        arr, self._src_keep = abi.scalar_sources(defs)
+        _check(lib().dpm_set_scalar_sources(self.h, len(defs), arr), "dpm_set_scalar_sources")
 
     # checkpoint and sampling (src/io/mod_checkpoint_io.f90, src/stats/mod_sampling.f90)
     def write_checkpoint(self, checkpoint_dir, step):

@@ -182,6 +182,25 @@ typedef struct dpm_params {
    * floors it). */
   int cell_projection;
   double cell_projection_tol;
+  /* Body forces besides f_const (src/solver/mod_fv_solver.f90:45-58, :959-983, :1662-1699):
+   * constant_mass_flux_forcing replaces f_const by (U_bulk_target - <U>) / dt, recomputed at the
+   * start of every step from the volume-mean velocity; use_harmonic_forcing adds
+   * forcing_amp cos(forcing_omega t + forcing_phase) along forcing_dir (x when it is zero), t the
+   * stage time; use_rotation adds the Coriolis term -2 omega_rot x U. */
+  int constant_mass_flux_forcing;
+  double U_bulk_target[3];
+  int use_harmonic_forcing;
+  double forcing_amp, forcing_omega, forcing_phase, forcing_dir[3];
+  int use_rotation;
+  double omega_rot[3];
+  /* Davies nudging of U (and T) towards the profiles given by dpm_set_nudging_profiles
+   * (src/abl/mod_abl_weather.f90:233-366): relaxation rate 1/nudging_tau, clamped at 0.5/dt,
+   * in cells whose centroid height is at least nudging_z_start, ramped linearly to full strength
+   * at nudging_z_full (no ramp when that is not above z_start); the vertical velocity is left
+   * alone when nudging_horizontal_only (the reference's default). */
+  int use_nudging;
+  double nudging_tau, nudging_z_start, nudging_z_full;
+  int nudging_horizontal_only;
 } dpm_params_t;
 
 /* Per-step integral statistics (src/stats/mod_stats.f90:compute_stats_sums and
@@ -364,6 +383,38 @@ int dpm_read_checkpoint(dpm_solver_t* s, const char* checkpoint_dir, int step);
  * the gradients taken as sampling_maybe_sample takes them (:171-177).  Only the payload crosses
  * PCIe; the NetCDF files are written by the host (dopamine_b200/sampling.py). */
 int dpm_sampling_set_points(dpm_solver_t* s, int n_points, const double* xyz, int* owner_cell);
+/* Reference profiles of the Davies nudging (mod_abl_weather.f90: NudgingData): n_times times
+ * (ascending), n_levels heights (ascending), U_profile(3, n_levels, n_times) and
+ * T_profile(n_levels, n_times) in the Fortran layout; bilinear in (time, height), clamped at the
+ * ends (nudging_interpolate, interp_find_indices :289-366). */
+int dpm_set_nudging_profiles(dpm_solver_t* s, int n_times, int n_levels, const double* times, const double* z_levels,
+                             const double* U_profile, const double* T_profile);
+/* Passive-scalar sources (src/mod_scalar.f90:ScalarSourceDef, scalar_source_value_at :133-183,
+ * added to the scalar's right-hand side as add_scalar_source_terms does, mod_fv_solver.f90:1764-
+ * 1784): each source adds magnitude x time scale (1, or cos(omega t + phase) when harmonic) to
+ * every cell whose centroid it covers - a sphere (point, or a volume of shape sphere), the
+ * neighbourhood of a segment (line), a slab about a plane optionally within a radius (surface,
+ * or a volume of shape plane), a box, or the neighbourhood of tag points (obj).  scalar_id is
+ * 1-based as in the namelist. */
+typedef struct dpm_scalar_source {
+  int enabled, scalar_id, src_kind, shape, time_mode;
+  double magnitude, omega, phase;
+  double center[3], p0[3], p1[3], normal[3];
+  double half_thickness, radius, box_min[3], box_max[3], tag_radius;
+  int n_tag_points;
+  const double* tag_points;   /* (3, n_tag_points) */
+} dpm_scalar_source_t;
+#define DPM_SCALAR_SRC_POINT 1
+#define DPM_SCALAR_SRC_LINE 2
+#define DPM_SCALAR_SRC_SURFACE 3
+#define DPM_SCALAR_SRC_VOLUME 4
+#define DPM_SCALAR_SRC_OBJ 5
+#define DPM_SCALAR_SHAPE_SPHERE 1
+#define DPM_SCALAR_SHAPE_BOX 2
+#define DPM_SCALAR_SHAPE_PLANE 3
+#define DPM_SCALAR_TIME_CONSTANT 1
+#define DPM_SCALAR_TIME_HARMONIC 2
+int dpm_set_scalar_sources(dpm_solver_t* s, int n_sources, const dpm_scalar_source_t* sources);
 int dpm_sample_points(dpm_solver_t* s, double* payload);
 /* Passive scalars C(n_scalars, n) in the reference's Fortran layout (src/solver/mod_fv_solver.f90:326,
  * scalar index fastest); the temperature travels with dpm_upload_state / dpm_download_state. */

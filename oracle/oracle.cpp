@@ -178,6 +178,17 @@ struct Solver {
   std::vector<double> u_par_filt;
   bool filt_ready = false;
 
+  // body forces (mod_fv_solver.f90:959-983, :1662-1699), nudging profiles
+  // (src/abl/mod_abl_weather.f90:NudgingData) and passive-scalar sources (src/mod_scalar.f90)
+  double mass_flux_force[3] = {0.0, 0.0, 0.0};
+  int nd_nt = 0, nd_nz = 0;
+  std::vector<double> nd_times, nd_z, nd_U, nd_T;  // U (3, nz, nt), T (nz, nt) Fortran order
+  struct Src {
+    dpm_scalar_source_t d;
+    std::vector<double> tags;
+  };
+  std::vector<Src> srcs;
+
   // exact cell projection (src/numerics/mod_cell_projection.f90:cell_proj_t): pressure-face list
   // with interpolation weights, outlet faces, and the last step's iteration counts
   bool cp_on = false;
@@ -1649,9 +1660,17 @@ struct Solver {
   void explicit_rhs() {
     advection(conv_U.data());
     viscous(visc_U.data());
-    const double* fbg = P.f_const;
+    double fbg[3];
+    body_force(time, fbg);
+    const double* om = P.omega_rot;
     for (int64_t c = 0; c < nc; ++c) {
       for (int k = 0; k < 3; ++k) H_U[3 * c + k] = conv_U[3 * c + k] + visc_U[3 * c + k] + fbg[k];
+      if (P.use_rotation) {
+        const double* u = &U[3 * c];
+        H_U[3 * c] = H_U[3 * c] - 2.0 * (om[1] * u[2] - om[2] * u[1]);
+        H_U[3 * c + 1] = H_U[3 * c + 1] - 2.0 * (om[2] * u[0] - om[0] * u[2]);
+        H_U[3 * c + 2] = H_U[3 * c + 2] - 2.0 * (om[0] * u[1] - om[1] * u[0]);
+      }
       if (P.boussinesq)
         for (int k = 0; k < 3; ++k) H_U[3 * c + k] = H_U[3 * c + k] - P.beta * (T[c] - P.T_ref) * P.g[k];
     }
@@ -1685,6 +1704,157 @@ struct Solver {
       advection_scalar(P.scalar_scheme, C, Cb, gC, conv_C.data());
       viscous_scalar(C, P.scalar_diffusivity[sc], P.scalar_pr_t[sc], gC, Cb, visc_C.data());
       for (int64_t c = 0; c < nc; ++c) H_C[(size_t)sc * nc + c] = conv_C[c] + visc_C[c];
+    }
+    add_scalar_sources(time);
+    if (P.use_nudging) nudging_apply(time);
+  }
+
+  // body_force_now (mod_fv_solver.f90:2903-2922), as compute_explicit_rhs assembles it (:1662-1675)
+  void body_force(double t, double f[3]) const {
+    for (int k = 0; k < 3; ++k) f[k] = P.constant_mass_flux_forcing ? mass_flux_force[k] : P.f_const[k];
+    if (P.use_harmonic_forcing) {
+      const double* fd = P.forcing_dir;
+      double dn = std::sqrt(fd[0] * fd[0] + fd[1] * fd[1] + fd[2] * fd[2]);
+      double hd[3] = {1.0, 0.0, 0.0};
+      if (dn > SMALL)
+        for (int k = 0; k < 3; ++k) hd[k] = fd[k] / dn;
+      double hs = P.forcing_amp * std::cos(P.forcing_omega * t + P.forcing_phase);
+      for (int k = 0; k < 3; ++k) f[k] = f[k] + hs * hd[k];
+    }
+  }
+  // update_mass_flux_forcing (:959-983)
+  void update_mass_flux_forcing(double dt) {
+    double m1 = 0.0, m2 = 0.0, m3 = 0.0;
+    for (int64_t c = 0; c < nc; ++c) {
+      m1 = m1 + U[3 * c] * m.volume[c];
+      m2 = m2 + U[3 * c + 1] * m.volume[c];
+      m3 = m3 + U[3 * c + 2] * m.volume[c];
+    }
+    const double mom[3] = {m1, m2, m3};
+    for (int k = 0; k < 3; ++k) mass_flux_force[k] = (P.U_bulk_target[k] - mom[k] / std::max(V_total, SMALL)) / dt;
+  }
+  // interp_find_indices (src/abl/mod_abl_weather.f90:335-366), 0-based
+  static void interp_find(const std::vector<double>& a, double v, int& i1, int& i2, double& w) {
+    const int n = (int)a.size();
+    i1 = 0;
+    i2 = n - 1;
+    for (int i = 0; i < n - 1; ++i)
+      if (v >= a[i] && v <= a[i + 1]) { i1 = i; i2 = i + 1; break; }
+    const double den = a[i2] - a[i1];
+    if (std::fabs(den) < 1.0e-16) w = 0.0;
+    else w = std::max(0.0, std::min(1.0, (v - a[i1]) / den));
+  }
+  // nudging_apply_rhs + nudging_interpolate (:233-333), dt the handle's P.dt as the caller passes it
+  void nudging_apply(double t) {
+    if (nd_nt < 1) return;
+    const double zs = P.nudging_z_start, zt = P.nudging_z_full;
+    double coeff = 1.0 / std::max(P.nudging_tau, 1.0e-16);
+    if (P.dt > 1.0e-16) coeff = std::min(coeff, 0.5 / P.dt);
+    int it1, it2;
+    double wt;
+    interp_find(nd_times, t, it1, it2, wt);
+    for (int64_t c = 0; c < nc; ++c) {
+      const double z = m.centroid[3 * c + 2];
+      if (z < zs) continue;
+      const double ramp = zt > zs ? std::min(1.0, (z - zs) / (zt - zs)) : 1.0;
+      int iz1, iz2;
+      double wz;
+      interp_find(nd_z, z, iz1, iz2, wz);
+      auto Up = [&](int j, int iz, int it) { return nd_U[3 * ((size_t)iz + (size_t)nd_nz * it) + j]; };
+      auto Tp = [&](int iz, int it) { return nd_T[(size_t)iz + (size_t)nd_nz * it]; };
+      double ur[3];
+      for (int j = 0; j < 3; ++j)
+        ur[j] = (1.0 - wt) * (1.0 - wz) * Up(j, iz1, it1) + wt * (1.0 - wz) * Up(j, iz1, it2) +
+                (1.0 - wt) * wz * Up(j, iz2, it1) + wt * wz * Up(j, iz2, it2);
+      const double tr = (1.0 - wt) * (1.0 - wz) * Tp(iz1, it1) + wt * (1.0 - wz) * Tp(iz1, it2) +
+                        (1.0 - wt) * wz * Tp(iz2, it1) + wt * wz * Tp(iz2, it2);
+      H_U[3 * c] = H_U[3 * c] - ramp * coeff * (U[3 * c] - ur[0]);
+      H_U[3 * c + 1] = H_U[3 * c + 1] - ramp * coeff * (U[3 * c + 1] - ur[1]);
+      if (!P.nudging_horizontal_only) H_U[3 * c + 2] = H_U[3 * c + 2] - ramp * coeff * (U[3 * c + 2] - ur[2]);
+      H_T[c] = H_T[c] - ramp * coeff * (T[c] - tr);
+    }
+  }
+  // scalar_source_value_at (src/mod_scalar.f90:133-229)
+  static double source_value(const Src& s, const double* x, double t) {
+    const dpm_scalar_source_t& d = s.d;
+    if (!d.enabled) return 0.0;
+    auto dist2 = [](const double* a, const double* b) {
+      double r = 0.0;
+      for (int k = 0; k < 3; ++k) r = r + (a[k] - b[k]) * (a[k] - b[k]);
+      return r;
+    };
+    auto unit = [](const double* v, double* u) {
+      double n = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+      if (n <= SMALL) { u[0] = 0.0; u[1] = 0.0; u[2] = 1.0; }
+      else for (int k = 0; k < 3; ++k) u[k] = v[k] / n;
+    };
+    auto slab = [&](double half) {
+      double u[3], r[3];
+      unit(d.normal, u);
+      for (int k = 0; k < 3; ++k) r[k] = x[k] - d.center[k];
+      return std::fabs(r[0] * u[0] + r[1] * u[1] + r[2] * u[2]) <= std::max(half, SMALL);
+    };
+    double w = 0.0;
+    switch (d.src_kind) {
+      case DPM_SCALAR_SRC_POINT:
+        if (dist2(x, d.center) <= std::max(d.radius, SMALL) * std::max(d.radius, SMALL)) w = 1.0;
+        break;
+      case DPM_SCALAR_SRC_LINE: {
+        double ab[3], den = 0.0, tt = 0.0, pr[3];
+        for (int k = 0; k < 3; ++k) { ab[k] = d.p1[k] - d.p0[k]; den = den + ab[k] * ab[k]; }
+        double dd;
+        if (den <= SMALL) {
+          dd = std::sqrt(dist2(x, d.p0));
+        } else {
+          for (int k = 0; k < 3; ++k) tt = tt + (x[k] - d.p0[k]) * ab[k];
+          tt = std::max(0.0, std::min(1.0, tt / den));
+          for (int k = 0; k < 3; ++k) pr[k] = d.p0[k] + tt * ab[k];
+          dd = std::sqrt(dist2(x, pr));
+        }
+        if (dd <= std::max(d.radius, SMALL)) w = 1.0;
+        break;
+      }
+      case DPM_SCALAR_SRC_SURFACE:
+        if (slab(d.half_thickness)) {
+          if (d.radius > 0.0) { if (dist2(x, d.center) <= d.radius * d.radius) w = 1.0; }
+          else w = 1.0;
+        }
+        break;
+      case DPM_SCALAR_SRC_OBJ:
+        if (!s.tags.empty()) {
+          double dm = 1.7976931348623157e308;
+          for (size_t i = 0; i + 2 < s.tags.size(); i += 3) {
+            double di = std::sqrt(dist2(x, &s.tags[i]));
+            if (di < dm) dm = di;
+          }
+          if (dm <= std::max(d.tag_radius, SMALL)) w = 1.0;
+        }
+        break;
+      default:
+        if (d.shape == DPM_SCALAR_SHAPE_BOX) {
+          if (x[0] >= d.box_min[0] && x[1] >= d.box_min[1] && x[2] >= d.box_min[2] && x[0] <= d.box_max[0] &&
+              x[1] <= d.box_max[1] && x[2] <= d.box_max[2])
+            w = 1.0;
+        } else if (d.shape == DPM_SCALAR_SHAPE_PLANE) {
+          if (slab(d.half_thickness)) w = 1.0;
+        } else {
+          if (dist2(x, d.center) <= std::max(d.radius, SMALL) * std::max(d.radius, SMALL)) w = 1.0;
+        }
+    }
+    const double ts = d.time_mode == DPM_SCALAR_TIME_HARMONIC ? std::cos(d.omega * t + d.phase) : 1.0;
+    return d.magnitude * ts * w;
+  }
+  // add_scalar_source_terms (mod_fv_solver.f90:1764-1784)
+  void add_scalar_sources(double t) {
+    if (ns <= 0) return;
+    for (const Src& s : srcs) {
+      if (!s.d.enabled) continue;
+      const int sid = s.d.scalar_id;
+      if (sid < 1 || sid > ns) continue;
+      for (int64_t c = 0; c < nc; ++c) {
+        const double v = source_value(s, &m.centroid[3 * c], t);
+        if (std::fabs(v) > SMALL) H_C[(size_t)(sid - 1) * nc + c] = H_C[(size_t)(sid - 1) * nc + c] + v;
+      }
     }
   }
 
@@ -1877,12 +2047,14 @@ struct Solver {
     }
     if (!do_cross) {
       double bb = P.boussinesq ? P.beta : 0.0;
+      double fb_now[3];
+      body_force(time, fb_now);
       for (int64_t fb : nper_bf) {
         int64_t fg = nfi + fb;
         if (bc_of_face(fg) == BC_OUTLET) continue;
         int o = m.owner[fg];
         double d[3];
-        for (int k = 0; k < 3; ++k) d[k] = P.f_const[k] - bb * (T[o] - P.T_ref) * P.g[k];
+        for (int k = 0; k < 3; ++k) d[k] = fb_now[k] - bb * (T[o] - P.T_ref) * P.g[k];
         const double* nh = &m.normal[3 * fg];
         double fn = (d[0] * nh[0] + d[1] * nh[1] + d[2] * nh[2]) * m.area[fg];
         for (int k = 0; k < 3; ++k) gp_cell[3 * o + k] = gp_cell[3 * o + k] + fn * nh[k];
@@ -2345,6 +2517,7 @@ struct Solver {
       if (rc) return rc;
       if (dt > ds) dt = ds;
     }
+    if (P.constant_mass_flux_forcing) update_mass_flux_forcing(dt);
     last_dt = dt;
     last_solves = 0; last_iters = 0; last_resid = 0.0;
     cp_iters = 0; cp_precond_iters = 0;
@@ -2787,6 +2960,26 @@ void orc_cp_divergence(void* h, const double* u, double* out) { static_cast<orc:
 void orc_cp_adjoint(void* h, const double* chi, double* v) { static_cast<orc::Solver*>(h)->cp_adjoint(chi, v); }
 int orc_cp_project(void* h, double* u, const double* bconst, double tol, int max_it, int identity, int* n_it) {
   return static_cast<orc::Solver*>(h)->cp_project(u, bconst, tol, max_it, identity != 0, n_it);
+}
+void orc_set_nudging_profiles(void* h, int nt, int nz, const double* times, const double* z, const double* Up,
+                              const double* Tp) {
+  auto* s = static_cast<orc::Solver*>(h);
+  s->nd_nt = nt; s->nd_nz = nz;
+  s->nd_times.assign(times, times + nt);
+  s->nd_z.assign(z, z + nz);
+  s->nd_U.assign(Up, Up + 3 * (size_t)nz * nt);
+  s->nd_T.assign(Tp, Tp + (size_t)nz * nt);
+}
+void orc_set_scalar_sources(void* h, int n, const dpm_scalar_source_t* src) {
+  auto* s = static_cast<orc::Solver*>(h);
+  s->srcs.clear();
+  for (int i = 0; i < n; ++i) {
+    orc::Solver::Src q;
+    q.d = src[i];
+    if (src[i].n_tag_points > 0 && src[i].tag_points) q.tags.assign(src[i].tag_points, src[i].tag_points + 3 * (size_t)src[i].n_tag_points);
+    q.d.tag_points = nullptr;
+    s->srcs.push_back(q);
+  }
 }
 void orc_sample_points(void* h, int np, const double* xyz, double* payload, int* owner) {
   static_cast<orc::Solver*>(h)->sample_points(np, xyz, payload, owner);

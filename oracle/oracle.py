@@ -56,6 +56,8 @@ def lib():
         L.orc_wall_stress_newton.argtypes = [C.c_double, C.c_double, C.c_double, dp, dp]
         L.orc_kfactor_limited.argtypes = [dp, dp, C.c_double, dp]
         L.orc_sample_points.argtypes = [vp, C.c_int, dp, dp, ip]
+        L.orc_set_nudging_profiles.argtypes = [vp, C.c_int, C.c_int, dp, dp, dp, dp]
+        L.orc_set_scalar_sources.argtypes = [vp, C.c_int, C.POINTER(abi.ScalarSourceT)]
         L.orc_cp_divergence.argtypes = [vp, dp, dp]
         L.orc_cp_adjoint.argtypes = [vp, dp, dp]
         L.orc_cp_project.argtypes = [vp, dp, dp, C.c_double, C.c_int, C.c_int, ip]
@@ -159,6 +161,18 @@ class Oracle:
         L.orc_poisson_csr(self.h, off.ctypes.data_as(C.POINTER(C.c_int64)), col.ctypes.data_as(C.POINTER(C.c_int)),
                           _p(val))
         return off, col, val
+
+    def set_nudging_profiles(self, times, z_levels, U_profile, T_profile):
+        """times (nt), z_levels (nz), U_profile (nt, nz, 3), T_profile (nt, nz)."""
+        t = np.ascontiguousarray(times, dtype=np.float64)
+        z = np.ascontiguousarray(z_levels, dtype=np.float64)
+        Up = np.ascontiguousarray(U_profile, dtype=np.float64)
+        Tp = np.ascontiguousarray(T_profile, dtype=np.float64)
+        lib().orc_set_nudging_profiles(self.h, len(t), len(z), _p(t), _p(z), _p(Up), _p(Tp))
+
+    def set_scalar_sources(self, defs):
+        arr, self._src_keep = abi.scalar_sources(defs)
+        lib().orc_set_scalar_sources(self.h, len(defs), arr)
 
     def record_poisson(self, on=True):
         lib().orc_record_poisson(self.h, 1 if on else 0)
