@@ -9,11 +9,11 @@ import numpy as np
 
 # Boundary-condition ids (src/mod_parameters.f90:41-51)
 BC_INLET, BC_OUTLET, BC_WALL_NOSLIP, BC_WALL_MODEL, BC_SLIP, BC_PERIODIC = 1, 2, 3, 4, 5, 6
-BC_SYMMETRY, BC_FIXEDTEMP, BC_ZEROGRADIENT, BC_WALL_VELOCITY = 7, 8, 9, 10
+BC_SYMMETRY, BC_FIXEDTEMP, BC_ZEROGRADIENT, BC_WALL_VELOCITY, BC_ABL_INLET = 7, 8, 9, 10, 11
 BC_BY_NAME = {
     "inlet": BC_INLET, "outlet": BC_OUTLET, "noSlip": BC_WALL_NOSLIP, "wallModel": BC_WALL_MODEL,
     "slip": BC_SLIP, "periodic": BC_PERIODIC, "symmetry": BC_SYMMETRY, "fixedTemp": BC_FIXEDTEMP,
-    "zeroGradient": BC_ZEROGRADIENT, "wallVelocity": BC_WALL_VELOCITY,
+    "zeroGradient": BC_ZEROGRADIENT, "wallVelocity": BC_WALL_VELOCITY, "ablInlet": BC_ABL_INLET,
 }
 
 SCHEME_VANLEER_TVD, SCHEME_KOREN_TVD, SCHEME_CDS, SCHEME_KEP, SCHEME_QUICK = 1, 2, 3, 4, 5
@@ -25,6 +25,8 @@ PSOLVER_JACOBI_PCG, PSOLVER_TWOLEVEL_FCG, PSOLVER_MULTILEVEL_FCG, PSOLVER_AUTO =
 OK, ERR_ARG, ERR_CUDA, ERR_MESH, ERR_NOT_FINITE, ERR_DT_COLLAPSE, ERR_UNSUPPORTED, ERR_BARRIER_TIMEOUT = 0, -1, -2, -3, -4, -5, -6, -7
 GRAD_LEAST_SQUARES, GRAD_GREEN_GAUSS = 0, 1
 CELL_PROJECTION_LS, CELL_PROJECTION_EXACT = 0, 1
+SEM_DFSEM, SEM_JARRIN = 0, 1
+SEM_MEAN_LOG, SEM_MEAN_POWER = 0, 1
 
 EL_TET4, EL_HEX8, EL_PRISM6, EL_PYR5 = 4, 5, 6, 7
 
@@ -72,7 +74,11 @@ class ParamsT(C.Structure):
         ("forcing_omega", C.c_double), ("forcing_phase", C.c_double), ("forcing_dir", C.c_double * 3),
         ("use_rotation", C.c_int), ("omega_rot", C.c_double * 3), ("use_nudging", C.c_int),
         ("nudging_tau", C.c_double), ("nudging_z_start", C.c_double), ("nudging_z_full", C.c_double),
-        ("nudging_horizontal_only", C.c_int),
+        ("nudging_horizontal_only", C.c_int), ("abl_u_ref", C.c_double), ("abl_z_ref", C.c_double),
+        ("abl_T_ref", C.c_double), ("abl_wind_dir_deg", C.c_double), ("use_sem", C.c_int), ("sem_type", C.c_int),
+        ("sem_n_eddies", C.c_int), ("sem_seed", C.c_int), ("sem_mean_law", C.c_int), ("sem_sigma", C.c_double),
+        ("sem_alpha", C.c_double), ("sem_Iu_ref", C.c_double), ("sem_Iv_ratio", C.c_double),
+        ("sem_Iw_ratio", C.c_double), ("sem_rho_uw", C.c_double),
     ]
 
 
@@ -187,6 +193,9 @@ def default_params(**kw):
     p.forcing_dir[0] = 1.0
     p.nudging_tau = 1800.0
     p.nudging_horizontal_only = 1
+    p.abl_u_ref, p.abl_z_ref, p.abl_T_ref, p.abl_wind_dir_deg = 8.0, 100.0, 300.0, 270.0
+    p.use_sem, p.sem_type, p.sem_n_eddies, p.sem_seed, p.sem_mean_law = 0, SEM_DFSEM, 500, 0, SEM_MEAN_LOG
+    p.sem_sigma, p.sem_alpha, p.sem_Iu_ref, p.sem_Iv_ratio, p.sem_Iw_ratio, p.sem_rho_uw = 0.0, 0.2, 0.0, 0.75, 0.5, -0.3
     for k, v in kw.items():
         if k in ("f_const", "g", "scalar_diffusivity", "scalar_pr_t", "U_bulk_target", "forcing_dir", "omega_rot"):
             arr = getattr(p, k)

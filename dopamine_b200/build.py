@@ -18,7 +18,7 @@ CU_SOURCES = ["csrc/cuda/solver.cu", "csrc/cuda/fvm_petsc.cu", "csrc/cuda/noallo
 CPP_SOURCES = ["csrc/host/mesh.cpp", "csrc/host/ops.cpp", "csrc/host/twolevel.cpp", "csrc/host/multilevel.cpp"]
 HEADERS = ["csrc/cuda/common.cuh", "csrc/cuda/kernels.cuh", "csrc/cuda/pcg.cuh", "csrc/cuda/fcg.cuh",
            "csrc/cuda/learn.cuh", "csrc/cuda/scalars.cuh", "csrc/cuda/mlcg.cuh", "csrc/cuda/mlsolve.cuh", "csrc/cuda/mlkern.cuh", "csrc/cuda/explicit32.cuh",
-           "csrc/cuda/cellproj.cuh", "csrc/cuda/sampling.cuh", "csrc/cuda/forcing.cuh", "csrc/host/fortran_records.hpp",
+           "csrc/cuda/cellproj.cuh", "csrc/cuda/sampling.cuh", "csrc/cuda/forcing.cuh", "csrc/cuda/sem.cuh", "csrc/host/fortran_records.hpp",
            "csrc/host/twolevel.hpp", "csrc/host/multilevel.hpp", "csrc/host/mesh.hpp",
            "csrc/host/ops.hpp", "../include/dopamine_b200.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -507,6 +507,17 @@ def regression_case(name):
         if name == "hydro_exact":
             prm["cell_projection"] = abi.CELL_PROJECTION_EXACT
         return Case(name, skewed_unit_box(12, 0.04), patches, prm, "uniform", 0.0, n_steps=20, stats_every=10)
+    if name in ("inflow", "inflow_jarrin"):
+        # synthetic-eddy inflow on the 12^3 skewed box: ABL inlet at x0 (log law u_ref 1 at z_ref 0.5,
+        # z0 0.01, 300 eddies of scale 0.2), outlet p = 0 at xL, periodic y, slip z
+        patches = [{"bc": "ablInlet"}, {"bc": "outlet", "p": 0.0}, {"bc": "periodic"}, {"bc": "periodic"},
+                   {"bc": "slip"}, {"bc": "slip"}]
+        prm = dict(scheme=abi.SCHEME_CDS, nu=1.0e-3, dt=5.0e-3, cfl_max=0.5, p_tol=1e-12, p_max_iter=1000,
+                   n_nonortho_corr=3, rhie_chow_dual=0, sgs_model=abi.SGS_NONE, wall_model=abi.WM_NONE,
+                   abl_u_ref=1.0, abl_z_ref=0.5, abl_z0_m=0.01, abl_wind_dir_deg=270.0, use_sem=1,
+                   sem_type=abi.SEM_JARRIN if name == "inflow_jarrin" else abi.SEM_DFSEM, sem_n_eddies=300,
+                   sem_sigma=0.2)
+        return Case(name, skewed_unit_box(12, 0.04), patches, prm, "uniform", 1.0, n_steps=20, stats_every=5)
     if name in ("duct", "duct_exact"):
         # 32x16x16 duct 4 x 1 x 1 on the RB.geo wall box: velocity inlet at x0, outlet p = 0 at xL,
         # periodic in y, no-slip bottom and top

@@ -12,7 +12,8 @@ constexpr int TPB = 256;
 
 // Boundary-condition ids (src/mod_parameters.f90:41-51)
 constexpr int BC_INLET = 1, BC_OUTLET = 2, BC_WALL_NOSLIP = 3, BC_WALL_MODEL = 4, BC_SLIP = 5, BC_PERIODIC = 6,
-              BC_SYMMETRY = 7, BC_FIXEDTEMP = 8, BC_ZEROGRADIENT = 9, BC_WALL_VELOCITY = 10;
+              BC_SYMMETRY = 7, BC_FIXEDTEMP = 8, BC_ZEROGRADIENT = 9, BC_WALL_VELOCITY = 10,
+              BC_ABL_INLET = 11;
 
 __host__ __device__ inline bool is_wall_bc(int bc) {
   return bc == BC_WALL_NOSLIP || bc == BC_WALL_MODEL || bc == BC_WALL_VELOCITY || bc == BC_SLIP || bc == BC_SYMMETRY;
@@ -36,6 +37,7 @@ struct Dev {
   // boundary faces (b = f - nfi)
   const int *bbc, *bpnb, *bpair, *bps, *bcanon;  // bc id, periodic partner cell, pair b, canonical ps idx, is canonical
   const double *bpgc, *bpdcf, *bcb, *bkout, *yw, *bUval, *bpval;  // bkout, bUval [3][nb]
+  const double* abl_fluc;  // [3][nb] synthetic fluctuation of the ABL-inlet faces, null without one
   // pressure-solver faces
   const int *pso, *psn, *psf;
   const double *psc, *psgcf, *psgcw, *psk, *pskrc;  // psk, pskrc [3][nfp]

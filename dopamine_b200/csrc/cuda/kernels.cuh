@@ -37,6 +37,14 @@ __global__ void k_velocity_bc(Dev d, const double* __restrict__ U, const double*
     case BC_INLET:
       u0 = d.bUval[b]; u1 = d.bUval[nb + b]; u2 = d.bUval[2 * nb + b];
       break;
+    case BC_ABL_INLET:  // the log-law mean (per face, from set-up) plus the synthetic fluctuation
+      u0 = d.bUval[b]; u1 = d.bUval[nb + b]; u2 = d.bUval[2 * nb + b];
+      if (d.abl_fluc) {
+        u0 = u0 + d.abl_fluc[b];
+        u1 = u1 + d.abl_fluc[nb + b];
+        u2 = u2 + d.abl_fluc[2 * nb + b];
+      }
+      break;
     case BC_OUTLET:
     case BC_ZEROGRADIENT: {
       u0 = U[o]; u1 = U[nc + o]; u2 = U[2 * nc + o];

@@ -29,7 +29,7 @@ __global__ void k_scalar_bc(Dev d, int kind, const double* __restrict__ phi, con
     const int pn = d.bpnb[b];
     v = pn >= 0 ? d.bpgc[b] * phi[o] + (1.0 - d.bpgc[b]) * phi[pn] : phi[o];
   } else if (kind == 0) {
-    if (bc == BC_INLET || bc == BC_FIXEDTEMP) {
+    if (bc == BC_INLET || bc == BC_FIXEDTEMP || (bc == BC_ABL_INLET && kind == 0)) {
       v = bval[b];
     } else {
       double d0 = d.fcen[f] - d.cen[o], d1 = d.fcen[nf + f] - d.cen[nc + o], d2 = d.fcen[2 * nf + f] - d.cen[2 * nc + o];

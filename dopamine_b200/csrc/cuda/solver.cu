@@ -34,6 +34,7 @@
 #include "mlsolve.cuh"
 #include "pcg.cuh"
 #include "sampling.cuh"
+#include "sem.cuh"
 #include "scalars.cuh"
 
 namespace dpm {
@@ -185,6 +186,15 @@ struct Solver {
   bool x32 = false;
   Geo32 g32{};
   float *gU32 = nullptr, *gS32 = nullptr, *sc_fadv32 = nullptr, *sc_fdif32 = nullptr;
+  // synthetic-eddy inflow (sem.cuh): configuration, state (device arrays; the generator state
+  // advances in the device copy), ABL-inlet faces, their fluctuation and reduction partials
+  bool sem_on = false;
+  SemCfg sem_cfg{};
+  SemState sem_h{};
+  SemState* sem_d = nullptr;
+  int* sem_faces = nullptr;
+  int sem_nfaces = 0, sem_grid = 1;
+  double *sem_fluc = nullptr, *sem_part = nullptr;
   // mass-flux forcing of the current step; Davies nudging profiles; passive-scalar sources
   double mass_flux_force[3] = {0.0, 0.0, 0.0};
   int nd_nt = 0, nd_nz = 0;
@@ -350,11 +360,19 @@ struct Solver {
       if (pb >= 0) bps[pb] = i;
     }
     std::vector<double> bU(3 * nb, 0.0), bp(nb, 0.0);
+    const double wr = P.abl_wind_dir_deg * SEM_PI / 180.0;
     for (int b = 0; b < nb; ++b) {
       int p = m.patch[nfi + b];
       if (p < 0) continue;
       for (int k = 0; k < 3; ++k) bU[k * nb + b] = pc[p].U_val[k];
       bp[b] = pc[p].p_val;
+      if (pc[p].bc_id == BC_ABL_INLET) {  // neutral log law along the wind (mod_bc.f90:352-372)
+        const double z0 = pc[p].abl_z0_m > 0.0 ? pc[p].abl_z0_m : P.abl_z0_m;
+        const double um = sem_log_u(m.centre[3 * (nfi + b) + 2], sem_ustar(P.abl_u_ref, P.abl_z_ref, z0), z0);
+        bU[b] = -um * std::sin(wr);
+        bU[nb + b] = -um * std::cos(wr);
+        bU[2 * nb + b] = 0.0;
+      }
     }
     d.bbc = mem.upload(S.bnd_bc);
     d.bpnb = mem.upload(S.bnd_pnb);
@@ -425,6 +443,10 @@ struct Solver {
     }
     if (!cg_dout || !F.fadv || !aos_buf) return DPM_ERR_CUDA;
     if (cp_on && cp_alloc()) return DPM_ERR_CUDA;
+    {
+      int rc = setup_sem();
+      if (rc) return rc;
+    }
     // cooperative grid for the persistent PCG
     int dev_sms = 0, per_sm = 0, coop = 0;
     CK(cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, device));
@@ -737,6 +759,13 @@ struct Solver {
       const int q = m.patch[nfi_() + b];
       if (q < 0) continue;
       tv[b] = pc[q].T_val;
+      if (pc[q].bc_id == BC_ABL_INLET) {  // MOST neutral temperature profile (mod_bc.f90:557-562)
+        const double z0h = pc[q].abl_z0_h > 0.0 ? pc[q].abl_z0_h : P.abl_z0_h, z = m.centre[3 * (nfi_() + b) + 2];
+        const double ts = (P.abl_z_ref > z0h && z0h > SMALL)
+                              ? 0.41 * (P.abl_T_ref - P.abl_T_surface) / std::log(P.abl_z_ref / z0h) : 0.0;
+        tv[b] = (z <= z0h || std::fabs(ts) <= SMALL || z0h <= SMALL) ? P.abl_T_surface
+                                                                    : P.abl_T_surface + (ts / 0.41) * std::log(z / z0h);
+      }
       for (int k = 0; k < ns; ++k) {
         sm[(size_t)k * nb + b] = pc[q].scalar_mode[k];
         sv[(size_t)k * nb + b] = pc[q].scalar_value[k];
@@ -1491,6 +1520,152 @@ struct Solver {
     return 0;
   }
 
+  // ---------------------------------------------------------------- synthetic-eddy inflow (sem.cuh)
+  // sem_init (src/abl/mod_sem_inflow.f90:59-316): the inlet frame and its periodic directions, the
+  // eddy scales, the box and the seeded eddies; false (nothing to do) without an ABL inlet
+  int setup_sem() {
+    const int64_t nfi = m.n_int_faces;
+    std::vector<int> fl;
+    for (int b = 0; b < nb; ++b) {
+      const int q = m.patch[nfi + b];
+      if (q >= 0 && pc[q].bc_id == BC_ABL_INLET) fl.push_back(b);
+    }
+    if (!P.use_sem || fl.empty()) return 0;
+    sem_cfg = SemCfg{P.abl_u_ref, P.abl_z_ref, P.abl_z0_m, P.abl_wind_dir_deg, P.sem_alpha, P.sem_Iu_ref, P.sem_Iv_ratio,
+                     P.sem_Iw_ratio, P.sem_rho_uw, P.sem_mean_law == DPM_SEM_MEAN_POWER ? 1 : 0};
+    SemState s{};
+    auto dot = [](const double* a, const double* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; };
+    double ns[3] = {0, 0, 0}, xs[3] = {0, 0, 0}, asum = 0.0;
+    for (int b : fl) {
+      const int64_t f = nfi + b;
+      for (int k = 0; k < 3; ++k) { ns[k] = ns[k] + m.area[f] * m.normal[3 * f + k]; xs[k] = xs[k] + m.area[f] * m.centre[3 * f + k]; }
+      asum = asum + m.area[f];
+    }
+    const double nl = std::sqrt(ns[0] * ns[0] + ns[1] * ns[1] + ns[2] * ns[2]);
+    if (!(asum > SEM_SMALL) || nl <= SEM_SMALL) return 0;
+    for (int k = 0; k < 3; ++k) { s.n_in[k] = -ns[k] / nl; s.x_inlet[k] = xs[k] / asum; }
+    const double seed_axis[3] = {std::fabs(s.n_in[2]) < 0.9 ? 0.0 : 1.0, 0.0, std::fabs(s.n_in[2]) < 0.9 ? 1.0 : 0.0};
+    s.t1[0] = seed_axis[1] * s.n_in[2] - seed_axis[2] * s.n_in[1];
+    s.t1[1] = seed_axis[2] * s.n_in[0] - seed_axis[0] * s.n_in[2];
+    s.t1[2] = seed_axis[0] * s.n_in[1] - seed_axis[1] * s.n_in[0];
+    const double tl = std::max(std::sqrt(dot(s.t1, s.t1)), SEM_SMALL);
+    for (int k = 0; k < 3; ++k) s.t1[k] = s.t1[k] / tl;
+    s.t2[0] = s.n_in[1] * s.t1[2] - s.n_in[2] * s.t1[1];
+    s.t2[1] = s.n_in[2] * s.t1[0] - s.n_in[0] * s.t1[2];
+    s.t2[2] = s.n_in[0] * s.t1[1] - s.n_in[1] * s.t1[0];
+    const double HUGE_V = 1.7976931348623157e308;
+    double lo[2] = {HUGE_V, HUGE_V}, hi[2] = {-HUGE_V, -HUGE_V};
+    for (int b : fl) {
+      const int64_t f = nfi + b;
+      double dd[3];
+      for (int k = 0; k < 3; ++k) dd[k] = m.centre[3 * f + k] - s.x_inlet[k];
+      lo[0] = std::min(lo[0], dot(dd, s.t1)); hi[0] = std::max(hi[0], dot(dd, s.t1));
+      lo[1] = std::min(lo[1], dot(dd, s.t2)); hi[1] = std::max(hi[1], dot(dd, s.t2));
+    }
+    s.t1_min = lo[0]; s.t1_max = hi[0]; s.t2_min = lo[1]; s.t2_max = hi[1];
+    double plo[2] = {HUGE_V, HUGE_V}, phi[2] = {-HUGE_V, -HUGE_V};  // sem_detect_periodic (:131-165)
+    for (int k = 0; k < 2; ++k) {
+      const double* tk = k == 0 ? s.t1 : s.t2;
+      for (int b = 0; b < nb; ++b) {
+        const int q = m.patch[nfi + b];
+        if (q < 0 || pc[q].bc_id != BC_PERIODIC) continue;
+        const int64_t f = nfi + b;
+        if (std::fabs(dot(&m.normal[3 * f], tk)) < 0.99) continue;
+        double dd[3];
+        for (int j = 0; j < 3; ++j) dd[j] = m.centre[3 * f + j] - s.x_inlet[j];
+        plo[k] = std::min(plo[k], dot(dd, tk)); phi[k] = std::max(phi[k], dot(dd, tk));
+      }
+    }
+    if (phi[0] - plo[0] > SEM_SMALL && plo[0] <= s.t1_min + SEM_SMALL && phi[0] >= s.t1_max - SEM_SMALL) {
+      s.per1 = 1; s.period1 = phi[0] - plo[0]; s.per1_lo = plo[0];
+    }
+    if (phi[1] - plo[1] > SEM_SMALL && plo[1] <= s.t2_min + SEM_SMALL && phi[1] >= s.t2_max - SEM_SMALL) {
+      s.per2 = 1; s.period2 = phi[1] - plo[1]; s.per2_lo = plo[1];
+    }
+    // sem_setup (:211-297)
+    const int ne = std::max(1, P.sem_n_eddies);
+    s.n = ne;
+    s.sigma = P.sem_sigma <= SEM_SMALL ? 0.1 * std::min(s.t1_max - s.t1_min, s.t2_max - s.t2_min) : P.sem_sigma;
+    if (s.sigma <= SEM_SMALL) s.sigma = 0.1 * P.abl_z_ref;
+    s.dfsem = P.sem_type != DPM_SEM_JARRIN;
+    s.rsup = s.sigma;
+    if (s.dfsem) {  // sem_reference_scales (:795-841): the largest principal stress over the inlet heights
+      const int nlv = 65;
+      const double zlo = s.x_inlet[2] + s.t2_min, zhi = s.x_inlet[2] + s.t2_max;
+      double lmax = SEM_SMALL, Rm[9], Wr[9], lam[3], V[9];
+      for (int k = 1; k <= nlv; ++k) {
+        const double z = k < nlv ? zlo + (zhi - zlo) * (double)(k - 1) / (double)(nlv - 2) : P.abl_z_ref;
+        sem_stress(sem_cfg, z, Rm, Wr);
+        sem_eigen3(Rm, lam, V);
+        lmax = std::max(lmax, std::max(lam[0], std::max(lam[1], lam[2])));
+      }
+      s.lam_ref = lmax;
+    }
+    if ((s.per1 && s.rsup >= 0.5 * s.period1) || (s.per2 && s.rsup >= 0.5 * s.period2)) {
+      std::fprintf(stderr, "dopamine_b200: the eddy support must be below half the periodic inlet width\n");
+      return DPM_ERR_ARG;
+    }
+    if (s.per1) { s.t1_min = s.per1_lo; s.t1_max = s.per1_lo + s.period1; }
+    else { s.t1_min = s.t1_min - s.rsup; s.t1_max = s.t1_max + s.rsup; }
+    if (s.per2) { s.t2_min = s.per2_lo; s.t2_max = s.per2_lo + s.period2; }
+    else { s.t2_min = s.t2_min - s.rsup; s.t2_max = s.t2_max + s.rsup; }
+    s.box_volume = 2.0 * s.rsup * (s.t1_max - s.t1_min) * (s.t2_max - s.t2_min);
+    s.u_convect = std::max(P.abl_u_ref, SEM_SMALL);
+    s.rng = 88172645463325252ULL;
+    if (P.sem_seed != 0) {
+      s.rng = 88172645463325252ULL ^ ((unsigned long long)(long long)P.sem_seed * 2654435761ULL);
+      if (s.rng == 0) s.rng = 88172645463325252ULL;
+      for (int i = 0; i < 8; ++i) sem_rand(s.rng);
+    }
+    std::vector<double> pos(3 * (size_t)ne, 0.0), amp(3 * (size_t)ne, 0.0);
+    for (int i = 0; i < ne; ++i) {
+      const double sv = s.rsup * (2.0 * sem_rand(s.rng) - 1.0);
+      sem_place(s, pos.data(), amp.data(), i, sv, true);
+    }
+    for (int k = 0; k < 3; ++k) {  // sem_balance_amplitudes (:300-316)
+      double ssum = 0.0;
+      for (int i = 0; i < ne; ++i) ssum = ssum + amp[3 * i + k];
+      for (int i = 0; i < ne; ++i) {
+        if (std::fabs(ssum) < 1.0) break;
+        if (amp[3 * i + k] * ssum > 0.0) {
+          amp[3 * i + k] = -amp[3 * i + k];
+          ssum = ssum + 2.0 * amp[3 * i + k];
+        }
+      }
+    }
+    s.pos = mem.upload(pos);
+    s.amp = mem.upload(amp);
+    s.frame = mem.alloc<double>(9 * (size_t)ne);
+    s.sig = mem.alloc<double>(3 * (size_t)ne);
+    s.ampl = mem.alloc<double>(3 * (size_t)ne);
+    sem_d = mem.alloc<SemState>(1);
+    sem_faces = mem.upload(fl);
+    sem_nfaces = (int)fl.size();
+    sem_grid = std::max(1, std::min(nblk(sem_nfaces), SEM_FACE_BLOCKS_MAX));
+    sem_part = mem.alloc<double>(2 * (size_t)sem_grid);
+    sem_fluc = mem.alloc<double>(3 * (size_t)nb);
+    if (!s.pos || !s.amp || !s.frame || !s.sig || !s.ampl || !sem_d || !sem_faces || !sem_part || !sem_fluc)
+      return DPM_ERR_CUDA;
+    CK(cudaMemcpy(sem_d, &s, sizeof(SemState), cudaMemcpyHostToDevice));
+    sem_h = s;
+    d.abl_fluc = sem_fluc;
+    sem_on = true;
+    return update_sem(false, 0.0);
+  }
+  // update_sem_inflow (mod_fv_solver.f90:2062-2119) for the eddies' current positions
+  int update_sem(bool look_ahead, double tau) {
+    if (!sem_on) return 0;
+    if (sem_h.dfsem) {
+      k_sem_prepare<<<(sem_h.n + 127) / 128, 128, 0, st>>>(sem_cfg, sem_h);
+      launches++;
+    }
+    k_sem_faces<<<sem_grid, TPB, 0, st>>>(d, sem_cfg, sem_h, sem_nfaces, sem_faces, look_ahead ? 1 : 0, tau, sem_fluc,
+                                          sem_part);
+    k_sem_finish<<<sem_grid, TPB, 0, st>>>(d, sem_nfaces, sem_faces, sem_grid, sem_part, sem_fluc);
+    launches += 2;
+    return 0;
+  }
+
   // ---------------------------------------------------------------- sources (forcing.cuh)
   bool split_rhs() const { return P.use_nudging || !srcs.empty(); }
   // compute_explicit_rhs's tail (mod_fv_solver.f90:1741-1760): scalar sources in their order, then
@@ -1629,6 +1804,7 @@ struct Solver {
     int mask = 1;
     if (P.wall_model == DPM_WM_MOST) mask += 2 + 4;
     if (filt_ready && P.wall_model == DPM_WM_LOGLAW) mask += 8;
+    if (sem_on) mask += 16;
     return mask;
   }
   static std::string checkpoint_file(const char* dir, int file_step) {
@@ -1673,6 +1849,21 @@ struct Solver {
     if (mask & 2) put(most_qw, nb, 1);
     if (mask & 4) put(most_L, nb, 1);
     if (mask & 8) put(F.upf, nb, 3);
+    if ((mask & 16) && ok && !rc) {  // eddy count and generator state, positions, signs (:127-131)
+      SemState cur{};
+      if (cudaMemcpy(&cur, sem_d, sizeof(SemState), cudaMemcpyDeviceToHost) != cudaSuccess) rc = DPM_ERR_CUDA;
+      char head[12];
+      const int32_t n32 = sem_h.n;
+      const int64_t r64 = (int64_t)cur.rng;
+      std::memcpy(head, &n32, 4);
+      std::memcpy(head + 4, &r64, 8);
+      ok = !rc && frec::write_record(f, head, 12);
+      std::vector<double> hv(3 * (size_t)sem_h.n);
+      for (double* dv : {sem_h.pos, sem_h.amp}) {
+        if (!ok || cudaMemcpy(hv.data(), dv, hv.size() * 8, cudaMemcpyDeviceToHost) != cudaSuccess) { ok = false; break; }
+        ok = frec::write_record(f, hv.data(), 8 * (int64_t)hv.size());
+      }
+    }
     ok = (std::fclose(f) == 0) && ok;
     if (rc) return rc;
     if (!ok) return DPM_ERR_ARG;
@@ -1740,9 +1931,23 @@ struct Solver {
         bad = bad || !next() || store(F.upf, nb, 3, rec);
         if (!bad) filt_ready = true;
       }
-      if (mask & 16) {  // synthetic-eddy inflow state: not on this path, the records are skipped
-        bad = bad || !next() || !next() || !next();
-        std::fprintf(stderr, "dopamine_b200: checkpoint synthetic-eddy state ignored\n");
+      if (mask & 16) {  // synthetic-eddy state, adopted when this run has the same eddy count
+        std::vector<char> head, rp, ra;
+        bad = bad || !frec::read_record(f, head) || !frec::read_record(f, rp) || !frec::read_record(f, ra);
+        if (!bad && head.size() == 12) {
+          int32_t n32;
+          int64_t r64;
+          std::memcpy(&n32, head.data(), 4);
+          std::memcpy(&r64, head.data() + 4, 8);
+          if (sem_on && n32 == sem_h.n && rp.size() == 24 * (size_t)n32 && ra.size() == rp.size()) {
+            CK(cudaMemcpy(sem_h.pos, rp.data(), rp.size(), cudaMemcpyHostToDevice));
+            CK(cudaMemcpy(sem_h.amp, ra.data(), ra.size(), cudaMemcpyHostToDevice));
+            sem_h.rng = (unsigned long long)r64;
+            CK(cudaMemcpy(sem_d, &sem_h, sizeof(SemState), cudaMemcpyHostToDevice));
+          } else {
+            std::fprintf(stderr, "dopamine_b200: checkpoint synthetic-eddy state does not match this run\n");
+          }
+        }
       }
       if (bad) break;
       rc = 0;
@@ -1751,6 +1956,7 @@ struct Solver {
     if (rc) return rc;
     time = t;
     step = hdr[3];
+    if (sem_on) update_sem(false, 0.0);  // inlet fluctuation of the restored eddies (:262-263)
     refresh_halos_and_bc();
     grad_all();
     pressure_gradient();
@@ -2023,6 +2229,7 @@ struct Solver {
         explicit_rhs(dt, RK3W_ALPHA[k], RK3W_BETA[k], 1);
         scalars_rhs(dt, RK3W_ALPHA[k], RK3W_BETA[k]);
       }
+      if (sem_on) update_sem(true, (RK3W_C[k] + RK3W_GAMMA[k]) * dt);  // the stage's end (mod_fv_solver.f90:1350-1358)
       velocity_bc_refresh();
       copy(F.p_old, F.p, nc);
       if (cp_on) launch_fill(F.gpc, 3 * (int64_t)nc, 0.0);  // nothing to add back (mod_fv_solver.f90:1373-1377)
@@ -2109,6 +2316,10 @@ struct Solver {
       std::swap(F.H, F.H0);
       std::swap(HT, HT0);
       std::swap(HC, HC0);
+    }
+    if (sem_on) {  // sem_advance (mod_fv_solver.f90:1606-1610)
+      k_sem_advance<<<1, 1, 0, st>>>(sem_d, dt);
+      launches++;
     }
     scalar_bcs(-1);
     time = time_n + dt;

@@ -201,7 +201,24 @@ typedef struct dpm_params {
   int use_nudging;
   double nudging_tau, nudging_z_start, nudging_z_full;
   int nudging_horizontal_only;
+  /* ABL inlet (BC_ABL_INLET patches; src/bc/mod_bc.f90:352-372, :557-562, src/abl/mod_abl_profiles.f90):
+   * the neutral log-law mean U(z) = (u_star / kappa) ln(z / z0_m) along the wind direction
+   * (meteorological degrees), u_star = kappa u_ref / ln(z_ref / z0_m), abl_z0_m the roughness; the
+   * temperature there follows the log law from abl_T_surface towards abl_T_ref at z_ref with
+   * abl_z0_h.  With use_sem the synthetic-eddy fluctuation is added (src/abl/mod_sem_inflow.f90):
+   * sem_type DPM_SEM_DFSEM (divergence-free eddies, the reference's default) or DPM_SEM_JARRIN,
+   * sem_n_eddies eddies of scale sem_sigma (<= 0: a tenth of the smaller inlet span), seed
+   * sem_seed (0: the built-in one); target stresses from Panofsky-Dutton (sem_Iu_ref <= 0) or an
+   * intensity law (sem_Iu_ref, sem_Iv_ratio, sem_Iw_ratio, sem_rho_uw); sem_mean_law
+   * DPM_SEM_MEAN_LOG or DPM_SEM_MEAN_POWER (exponent sem_alpha). */
+  double abl_u_ref, abl_z_ref, abl_T_ref, abl_wind_dir_deg;
+  int use_sem, sem_type, sem_n_eddies, sem_seed, sem_mean_law;
+  double sem_sigma, sem_alpha, sem_Iu_ref, sem_Iv_ratio, sem_Iw_ratio, sem_rho_uw;
 } dpm_params_t;
+#define DPM_SEM_DFSEM 0
+#define DPM_SEM_JARRIN 1
+#define DPM_SEM_MEAN_LOG 0
+#define DPM_SEM_MEAN_POWER 1
 
 /* Per-step integral statistics (src/stats/mod_stats.f90:compute_stats_sums and
  * src/solver/mod_fv_solver.f90:solver_divergence_metrics). */

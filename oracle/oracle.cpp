@@ -178,6 +178,19 @@ struct Solver {
   std::vector<double> u_par_filt;
   bool filt_ready = false;
 
+  // ABL inlet mean and temperature per boundary face, and the synthetic-eddy state
+  // (src/abl/mod_abl_types.f90:SEMState, src/abl/mod_sem_inflow.f90)
+  std::vector<double> abl_mean, abl_T, sem_fluc;
+  struct Sem {
+    bool initialized = false, dfsem = true, per1 = false, per2 = false;
+    double n_in[3] = {0, 0, 0}, x_inlet[3] = {0, 0, 0}, t1[3] = {0, 0, 0}, t2[3] = {0, 0, 0};
+    double t1_min = 0, t1_max = 0, t2_min = 0, t2_max = 0, period1 = 0, period2 = 0, per1_lo = 0, per2_lo = 0;
+    double sigma = 0, rsup = 0, box_volume = 0, u_convect = 0, lam_ref = 0, sig_min = 0;
+    int n = 0;
+    std::vector<double> pos, amp, frame, sig, ampl;
+    uint64_t rng = 88172645463325252ULL;
+  } sem;
+
   // body forces (mod_fv_solver.f90:959-983, :1662-1699), nudging profiles
   // (src/abl/mod_abl_weather.f90:NudgingData) and passive-scalar sources (src/mod_scalar.f90)
   double mass_flux_force[3] = {0.0, 0.0, 0.0};
@@ -245,6 +258,7 @@ struct Solver {
     built.assign(nf, 0);
     Tinv.assign(9 * nc, 0.0);
     for (int64_t c = 0; c < nc; ++c) Tinv[9 * c] = Tinv[9 * c + 4] = Tinv[9 * c + 8] = 1.0;
+    abl_inlet_profiles();
     // build_patch_classification
     for (int q = 0; q < m.n_patches; ++q)
       for (int64_t f = 0; f < m.patch_nfaces[q]; ++f)
@@ -274,7 +288,390 @@ struct Solver {
       if (m.is_refine[f]) { diag_interface = true; break; }
     build_filter_tensor();
     build_cell_projection();
+    if (P.use_sem && sem_init()) update_sem_inflow(time, false, 0.0);  // mod_fv_solver.f90:486-492
     return 0;
+  }
+
+  // ------------------------------------------------------------------ ABL inlet (mod_abl_profiles.f90)
+  static double ustar_from_ref(double u_ref, double z_ref, double z0) {
+    return (z_ref > z0 && z0 > SMALL && u_ref > SMALL) ? KAPPA * u_ref / std::log(z_ref / z0) : 0.05 * u_ref;
+  }
+  static double u_profile(double z, double u_star, double z0) {  // neutral (L = 0)
+    if (z <= z0 || u_star <= SMALL || z0 <= SMALL) return 0.0;
+    return (u_star / KAPPA) * std::log(z / z0);
+  }
+  double patch_z0m(int q) const { return pc[q].abl_z0_m > 0.0 ? pc[q].abl_z0_m : P.abl_z0_m; }
+  double patch_z0h(int q) const { return pc[q].abl_z0_h > 0.0 ? pc[q].abl_z0_h : P.abl_z0_h; }
+  // the log-law mean (mod_bc.f90:352-372) and temperature (:557-562, abl_T_profile) of each
+  // ABL-inlet face; the synthetic fluctuation starts at zero
+  void abl_inlet_profiles() {
+    abl_mean.assign(3 * nb, 0.0);
+    abl_T.assign(nb, P.T_ref);
+    sem_fluc.assign(3 * nb, 0.0);
+    const double wr = P.abl_wind_dir_deg * 3.14159265358979323846 / 180.0;
+    for (int64_t fb = 0; fb < nb; ++fb) {
+      int64_t fg = nfi + fb;
+      if (bc_of_face(fg) != BC_ABL_INLET) continue;
+      const int q = m.patch[fg];
+      const double z = m.centre[3 * fg + 2];
+      const double us = ustar_from_ref(P.abl_u_ref, P.abl_z_ref, patch_z0m(q));
+      const double um = u_profile(z, us, patch_z0m(q));
+      abl_mean[3 * fb] = -um * std::sin(wr);
+      abl_mean[3 * fb + 1] = -um * std::cos(wr);
+      const double z0h = patch_z0h(q);
+      const double ts = (P.abl_z_ref > z0h && z0h > SMALL) ? KAPPA * (P.abl_T_ref - P.abl_T_surface) / std::log(P.abl_z_ref / z0h) : 0.0;
+      double Tz = P.abl_T_surface;
+      if (!(z <= z0h || std::fabs(ts) <= SMALL || z0h <= SMALL)) Tz = P.abl_T_surface + (ts / KAPPA) * std::log(z / z0h);
+      abl_T[fb] = Tz;
+    }
+  }
+
+  // ------------------------------------------------------------------ synthetic eddies (mod_sem_inflow.f90)
+  static constexpr double SEM_SMALL = 1.0e-16, SEM_PI = 3.14159265358979323846;
+  double sem_rand() {  // :50-55, xorshift64
+    sem.rng ^= sem.rng << 13;
+    sem.rng ^= sem.rng >> 7;
+    sem.rng ^= sem.rng << 17;
+    return (double)(sem.rng & 4503599627370495ULL) / 4503599627370496.0;
+  }
+  static void cross(const double* a, const double* b, double* c) {
+    c[0] = a[1] * b[2] - a[2] * b[1];
+    c[1] = a[2] * b[0] - a[0] * b[2];
+    c[2] = a[0] * b[1] - a[1] * b[0];
+  }
+  // sem_inlet_frame + sem_detect_periodic (:59-165)
+  bool sem_frame() {
+    double ns[3] = {0, 0, 0}, xs[3] = {0, 0, 0}, asum = 0.0;
+    for (int64_t fb = 0; fb < nb; ++fb) {
+      int64_t fg = nfi + fb;
+      if (bc_of_face(fg) != BC_ABL_INLET) continue;
+      double a = m.area[fg];
+      for (int k = 0; k < 3; ++k) { ns[k] = ns[k] + a * m.normal[3 * fg + k]; xs[k] = xs[k] + a * m.centre[3 * fg + k]; }
+      asum = asum + a;
+    }
+    if (!(asum > SEM_SMALL)) return false;
+    double nl = std::sqrt(ns[0] * ns[0] + ns[1] * ns[1] + ns[2] * ns[2]);
+    if (nl <= SEM_SMALL) return false;
+    for (int k = 0; k < 3; ++k) { sem.n_in[k] = -ns[k] / nl; sem.x_inlet[k] = xs[k] / asum; }
+    const double ez[3] = {0, 0, 1}, ex[3] = {1, 0, 0};
+    cross(std::fabs(sem.n_in[2]) < 0.9 ? ez : ex, sem.n_in, sem.t1);
+    double tl = std::max(std::sqrt(sem.t1[0] * sem.t1[0] + sem.t1[1] * sem.t1[1] + sem.t1[2] * sem.t1[2]), SEM_SMALL);
+    for (int k = 0; k < 3; ++k) sem.t1[k] = sem.t1[k] / tl;
+    cross(sem.n_in, sem.t1, sem.t2);
+    double lo[2] = {1.7976931348623157e308, 1.7976931348623157e308}, hi[2] = {-1.7976931348623157e308, -1.7976931348623157e308};
+    for (int64_t fb = 0; fb < nb; ++fb) {
+      int64_t fg = nfi + fb;
+      if (bc_of_face(fg) != BC_ABL_INLET) continue;
+      double d[3];
+      for (int k = 0; k < 3; ++k) d[k] = m.centre[3 * fg + k] - sem.x_inlet[k];
+      double s1 = dot3(d, sem.t1), s2 = dot3(d, sem.t2);
+      lo[0] = std::min(lo[0], s1); hi[0] = std::max(hi[0], s1);
+      lo[1] = std::min(lo[1], s2); hi[1] = std::max(hi[1], s2);
+    }
+    sem.t1_min = lo[0]; sem.t1_max = hi[0]; sem.t2_min = lo[1]; sem.t2_max = hi[1];
+    double plo[2] = {1.7976931348623157e308, 1.7976931348623157e308}, phi2[2] = {-1.7976931348623157e308, -1.7976931348623157e308};
+    for (int k = 0; k < 2; ++k) {
+      const double* tk = k == 0 ? sem.t1 : sem.t2;
+      for (int64_t fb = 0; fb < nb; ++fb) {
+        int64_t fg = nfi + fb;
+        if (bc_of_face(fg) != BC_PERIODIC) continue;
+        if (std::fabs(dot3(&m.normal[3 * fg], tk)) < 0.99) continue;
+        double d[3];
+        for (int j = 0; j < 3; ++j) d[j] = m.centre[3 * fg + j] - sem.x_inlet[j];
+        double sv = dot3(d, tk);
+        plo[k] = std::min(plo[k], sv); phi2[k] = std::max(phi2[k], sv);
+      }
+    }
+    sem.per1 = sem.per2 = false;
+    sem.period1 = sem.period2 = 0.0;
+    if (phi2[0] - plo[0] > SEM_SMALL && plo[0] <= sem.t1_min + SEM_SMALL && phi2[0] >= sem.t1_max - SEM_SMALL) {
+      sem.per1 = true; sem.period1 = phi2[0] - plo[0]; sem.per1_lo = plo[0];
+    }
+    if (phi2[1] - plo[1] > SEM_SMALL && plo[1] <= sem.t2_min + SEM_SMALL && phi2[1] >= sem.t2_max - SEM_SMALL) {
+      sem.per2 = true; sem.period2 = phi2[1] - plo[1]; sem.per2_lo = plo[1];
+    }
+    return true;
+  }
+  // sem_target_at (:663-711) without a profile table: mean (global axes) and R = [uu,vv,ww,uv,uw,vw]
+  void sem_target(double z, double um[3], double R[6]) const {
+    const double z0 = P.abl_z0_m, zf = std::max(z0, 1.0e-6), zz = std::max(z, zf);
+    const double us = ustar_from_ref(P.abl_u_ref, P.abl_z_ref, z0);
+    double umag = P.sem_mean_law == DPM_SEM_MEAN_POWER ? P.abl_u_ref * std::pow(zz / std::max(P.abl_z_ref, SEM_SMALL), P.sem_alpha)
+                                                       : u_profile(z, us, z0);
+    const double wr = P.abl_wind_dir_deg * SEM_PI / 180.0;
+    um[0] = -umag * std::sin(wr); um[1] = -umag * std::cos(wr); um[2] = 0.0;
+    for (int k = 0; k < 6; ++k) R[k] = 0.0;
+    if (P.sem_Iu_ref > 0.0) {
+      const double zi = std::max(z, 10.0 * z0);
+      const double Iu = P.sem_Iu_ref * std::log(std::max(P.abl_z_ref, 1.0001 * z0) / z0) / std::log(zi / z0);
+      umag = P.sem_mean_law == DPM_SEM_MEAN_POWER ? P.abl_u_ref * std::pow(std::max(zi, zf) / std::max(P.abl_z_ref, SEM_SMALL), P.sem_alpha)
+                                                  : u_profile(zi, us, z0);
+      const double su = Iu * umag, sv = P.sem_Iv_ratio * su, sw = P.sem_Iw_ratio * su;
+      R[0] = su * su; R[1] = sv * sv; R[2] = sw * sw;
+      R[4] = P.sem_rho_uw * su * sw;
+    } else {
+      R[0] = (2.4 * us) * (2.4 * us);
+      R[1] = (1.9 * us) * (1.9 * us);
+      R[2] = (1.25 * us) * (1.25 * us);
+      R[4] = -(us * us);
+    }
+  }
+  // sem_stress_at (:725-748): Rm (row-major 3x3) in the mean-wind frame and the frame axes Wr
+  void sem_stress(double z, double Rm[9], double Wr[9]) const {
+    double um[3], R[6];
+    sem_target(z, um, R);
+    Rm[0] = R[0]; Rm[4] = R[1]; Rm[8] = R[2];
+    Rm[1] = R[3]; Rm[3] = R[3];
+    Rm[2] = R[4]; Rm[6] = R[4];
+    Rm[5] = R[5]; Rm[7] = R[5];
+    const double wr = P.abl_wind_dir_deg * SEM_PI / 180.0;
+    // columns e_s, e_n, e_z
+    Wr[0] = -std::sin(wr); Wr[3] = -std::cos(wr); Wr[6] = 0.0;
+    Wr[1] = std::cos(wr);  Wr[4] = -std::sin(wr); Wr[7] = 0.0;
+    Wr[2] = 0.0;           Wr[5] = 0.0;           Wr[8] = 1.0;
+  }
+  // sem_eigen3 (:752-792): cyclic Jacobi, A = V diag(lam) V^T (row-major V, columns the vectors)
+  static void eigen3(const double Ain[9], double lam[3], double V[9]) {
+    double A[3][3], W[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) A[i][j] = Ain[3 * i + j];
+    for (int sweep = 1; sweep <= 30; ++sweep) {
+      double off = std::fabs(A[0][1]) + std::fabs(A[0][2]) + std::fabs(A[1][2]);
+      if (off <= 1.0e-15 * (std::fabs(A[0][0]) + std::fabs(A[1][1]) + std::fabs(A[2][2]) + SEM_SMALL)) break;
+      for (int p = 0; p < 2; ++p)
+        for (int q = p + 1; q < 3; ++q) {
+          double apq = A[p][q];
+          if (std::fabs(apq) <= SEM_SMALL) continue;
+          double th = (A[q][q] - A[p][p]) / (2.0 * apq);
+          double t = std::copysign(1.0, th) / (std::fabs(th) + std::sqrt(th * th + 1.0));
+          double c = 1.0 / std::sqrt(t * t + 1.0), sn = t * c, tau = sn / (1.0 + c);
+          A[p][p] = A[p][p] - t * apq;
+          A[q][q] = A[q][q] + t * apq;
+          A[p][q] = 0.0; A[q][p] = 0.0;
+          for (int k = 0; k < 3; ++k) {
+            if (k != p && k != q) {
+              double akp = A[k][p], akq = A[k][q];
+              A[k][p] = akp - sn * (akq + tau * akp); A[p][k] = A[k][p];
+              A[k][q] = akq + sn * (akp - tau * akq); A[q][k] = A[k][q];
+            }
+            double vkp = W[k][p], vkq = W[k][q];
+            W[k][p] = vkp - sn * (vkq + tau * vkp);
+            W[k][q] = vkq + sn * (vkp - tau * vkq);
+          }
+        }
+    }
+    lam[0] = A[0][0]; lam[1] = A[1][1]; lam[2] = A[2][2];
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) V[3 * i + j] = W[i][j];
+  }
+  // sem_reference_scales (:795-841)
+  void sem_scales() {
+    const int nl = 65;
+    std::vector<double> zl(nl);
+    const double zlo = sem.x_inlet[2] + sem.t2_min, zhi = sem.x_inlet[2] + sem.t2_max;
+    for (int k = 1; k <= nl - 1; ++k) zl[k - 1] = zlo + (zhi - zlo) * (double)(k - 1) / (double)(nl - 2);
+    zl[nl - 1] = P.abl_z_ref;
+    double lmax = SEM_SMALL;
+    double Rm[9], Wr[9], lam[3], V[9];
+    for (int k = 0; k < nl; ++k) {
+      sem_stress(zl[k], Rm, Wr);
+      eigen3(Rm, lam, V);
+      lmax = std::max(lmax, std::max(lam[0], std::max(lam[1], lam[2])));
+    }
+    sem.lam_ref = lmax;
+    sem.rsup = sem.sigma;
+    double fmin = 1.0;
+    for (int k = 0; k < nl; ++k) {
+      sem_stress(zl[k], Rm, Wr);
+      eigen3(Rm, lam, V);
+      double mx = std::max(lam[0], std::max(lam[1], lam[2])), mn = std::min(lam[0], std::min(lam[1], lam[2]));
+      if (mx >= 0.25 * lmax) fmin = std::min(fmin, std::max(0.2, std::sqrt(std::max(mn, 0.0) / lmax)));
+    }
+    sem.sig_min = sem.sigma * fmin;
+  }
+  // sem_place_eddy (:320-338)
+  void sem_place(int i, double sv, bool new_amp) {
+    double a = sem.t1_min + (sem.t1_max - sem.t1_min) * sem_rand();
+    double b = sem.t2_min + (sem.t2_max - sem.t2_min) * sem_rand();
+    for (int k = 0; k < 3; ++k) sem.pos[3 * i + k] = sem.x_inlet[k] + sv * sem.n_in[k] + a * sem.t1[k] + b * sem.t2[k];
+    if (new_amp)
+      for (int k = 0; k < 3; ++k) sem.amp[3 * i + k] = std::copysign(1.0, sem_rand() - 0.5);
+  }
+  // sem_init + sem_setup + sem_balance_amplitudes (:176-316); false without an ABL inlet
+  bool sem_init() {
+    sem = Sem();
+    if (!sem_frame()) return false;
+    const int ne = std::max(1, P.sem_n_eddies);
+    sem.n = ne;
+    sem.pos.assign(3 * ne, 0.0);
+    sem.amp.assign(3 * ne, 0.0);
+    const double span1 = sem.t1_max - sem.t1_min, span2 = sem.t2_max - sem.t2_min;
+    sem.sigma = P.sem_sigma <= SEM_SMALL ? 0.1 * std::min(span1, span2) : P.sem_sigma;
+    if (sem.sigma <= SEM_SMALL) sem.sigma = 0.1 * P.abl_z_ref;
+    sem.dfsem = P.sem_type != DPM_SEM_JARRIN;
+    sem.rsup = sem.sigma;
+    if (sem.dfsem) {
+      sem.frame.assign(9 * ne, 0.0);
+      sem.sig.assign(3 * ne, 0.0);
+      sem.ampl.assign(3 * ne, 0.0);
+      sem_scales();
+    }
+    if (sem.per1) { sem.t1_min = sem.per1_lo; sem.t1_max = sem.per1_lo + sem.period1; }
+    else { sem.t1_min = sem.t1_min - sem.rsup; sem.t1_max = sem.t1_max + sem.rsup; }
+    if (sem.per2) { sem.t2_min = sem.per2_lo; sem.t2_max = sem.per2_lo + sem.period2; }
+    else { sem.t2_min = sem.t2_min - sem.rsup; sem.t2_max = sem.t2_max + sem.rsup; }
+    sem.box_volume = 2.0 * sem.rsup * (sem.t1_max - sem.t1_min) * (sem.t2_max - sem.t2_min);
+    sem.u_convect = std::max(P.abl_u_ref, SEM_SMALL);
+    sem.rng = 88172645463325252ULL;
+    if (P.sem_seed != 0) {
+      sem.rng = 88172645463325252ULL ^ ((uint64_t)(int64_t)P.sem_seed * 2654435761ULL);
+      if (sem.rng == 0) sem.rng = 88172645463325252ULL;
+      for (int i = 0; i < 8; ++i) sem_rand();
+    }
+    for (int i = 0; i < ne; ++i) sem_place(i, sem.rsup * (2.0 * sem_rand() - 1.0), true);
+    for (int k = 0; k < 3; ++k) {  // sem_balance_amplitudes
+      double ssum = 0.0;
+      for (int i = 0; i < ne; ++i) ssum = ssum + sem.amp[3 * i + k];
+      for (int i = 0; i < ne; ++i) {
+        if (std::fabs(ssum) < 1.0) break;
+        if (sem.amp[3 * i + k] * ssum > 0.0) {
+          sem.amp[3 * i + k] = -sem.amp[3 * i + k];
+          ssum = ssum + 2.0 * sem.amp[3 * i + k];
+        }
+      }
+    }
+    if (sem.dfsem) sem_prepare();
+    sem.initialized = true;
+    return true;
+  }
+  // sem_prepare (:867-892)
+  void sem_prepare() {
+    if (!sem.dfsem) return;
+    const double DF_I = 32.0 * SEM_PI / 945.0;
+    for (int i = 0; i < sem.n; ++i) {
+      double Rm[9], Wr[9], lam[3], V[9];
+      sem_stress(sem.pos[3 * i + 2], Rm, Wr);
+      eigen3(Rm, lam, V);
+      double s[3];
+      for (int j = 0; j < 3; ++j) {
+        for (int r = 0; r < 3; ++r) {  // Vg = Wr V, column j
+          double acc = 0.0;
+          for (int k = 0; k < 3; ++k) acc = acc + Wr[3 * r + k] * V[3 * k + j];
+          sem.frame[9 * i + 3 * j + r] = acc;
+        }
+        s[j] = sem.sigma * std::max(0.2, std::sqrt(std::max(lam[j], 0.0) / sem.lam_ref));
+      }
+      for (int j = 0; j < 3; ++j) sem.sig[3 * i + j] = s[j];
+      const double K = (double)sem.n * s[0] * s[1] * s[2] * DF_I / sem.box_volume;
+      double b[3], A[3];
+      for (int j = 0; j < 3; ++j) b[j] = std::max(lam[j], 0.0) / (K * (s[j] * s[j]));
+      A[0] = 0.5 * (b[1] + b[2] - b[0]);
+      A[1] = 0.5 * (b[0] + b[2] - b[1]);
+      A[2] = 0.5 * (b[0] + b[1] - b[2]);
+      for (int j = 0; j < 3; ++j) sem.ampl[3 * i + j] = std::sqrt(std::max(A[j], 0.0)) * sem.amp[3 * i + j];
+    }
+  }
+  // the eddy offset wrapped across periodic inlet directions (add_eddy, :968-976 / :1024-1032)
+  void sem_wrap(double d[3]) const {
+    if (sem.per1) {
+      double k = std::round(dot3(d, sem.t1) / sem.period1);
+      for (int j = 0; j < 3; ++j) d[j] = d[j] - sem.period1 * k * sem.t1[j];
+    }
+    if (sem.per2) {
+      double k = std::round(dot3(d, sem.t2) / sem.period2);
+      for (int j = 0; j < 3; ++j) d[j] = d[j] - sem.period2 * k * sem.t2[j];
+    }
+  }
+  // sem_velocity_at_face (:933-978) and sem_velocity_jarrin (:980-1039), every eddy in index order
+  void sem_face(const double* centre, bool look_ahead, double tau, double uf[3]) const {
+    double xs[3];
+    for (int k = 0; k < 3; ++k) xs[k] = look_ahead ? centre[k] - sem.u_convect * tau * sem.n_in[k] : centre[k];
+    uf[0] = uf[1] = uf[2] = 0.0;
+    if (sem.dfsem) {
+      const double rs2 = sem.rsup * sem.rsup;
+      for (int e = 0; e < sem.n; ++e) {
+        double d[3];
+        for (int k = 0; k < 3; ++k) d[k] = xs[k] - sem.pos[3 * e + k];
+        sem_wrap(d);
+        if (d[0] * d[0] + d[1] * d[1] + d[2] * d[2] >= rs2) continue;
+        const double* fr = &sem.frame[9 * e];
+        const double* sg = &sem.sig[3 * e];
+        const double* al = &sem.ampl[3 * e];
+        double r[3], d2 = 0.0;
+        for (int j = 0; j < 3; ++j) {
+          r[j] = dot3(d, fr + 3 * j) / sg[j];
+          d2 = d2 + r[j] * r[j];
+        }
+        if (d2 >= 1.0) continue;
+        const double g = 1.0 - d2;
+        const double up0 = sg[0] * g * (r[1] * al[2] - r[2] * al[1]);
+        const double up1 = sg[1] * g * (r[2] * al[0] - r[0] * al[2]);
+        const double up2 = sg[2] * g * (r[0] * al[1] - r[1] * al[0]);
+        for (int k = 0; k < 3; ++k) uf[k] = uf[k] + (up0 * fr[k] + up1 * fr[3 + k] + up2 * fr[6 + k]);
+      }
+      return;
+    }
+    double um[3], R[6];
+    sem_target(centre[2], um, R);
+    const double wr = P.abl_wind_dir_deg * SEM_PI / 180.0;
+    const double sg = std::max(sem.sigma, SEM_SMALL);
+    const double norm = 1.5450968080927583 * std::sqrt(sem.box_volume / (sg * sg * sg)) / std::sqrt((double)sem.n);
+    double iso[3] = {0, 0, 0};
+    for (int e = 0; e < sem.n; ++e) {
+      double d[3];
+      for (int k = 0; k < 3; ++k) d[k] = xs[k] - sem.pos[3 * e + k];
+      sem_wrap(d);
+      if (std::fabs(d[0]) >= sg || std::fabs(d[1]) >= sg || std::fabs(d[2]) >= sg) continue;
+      const double rr = std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]) / sg;
+      const double tent = std::max(0.0, 1.0 - rr);
+      if (tent <= 0.0) continue;
+      for (int k = 0; k < 3; ++k) iso[k] = iso[k] + norm * tent * sem.amp[3 * e + k];
+    }
+    // sem_cholesky (:651-661)
+    double L11 = std::sqrt(std::max(R[0], SEM_SMALL));
+    double L21 = R[3] / L11, L31 = R[4] / L11;
+    double L22 = std::sqrt(std::max(R[1] - L21 * L21, SEM_SMALL));
+    double L32 = (R[5] - L31 * L21) / L22;
+    double L33 = std::sqrt(std::max(R[2] - L31 * L31 - L32 * L32, SEM_SMALL));
+    const double a0 = L11 * iso[0], a1 = L21 * iso[0] + L22 * iso[1], a2 = L31 * iso[0] + L32 * iso[1] + L33 * iso[2];
+    uf[0] = -a0 * std::sin(wr) + a1 * std::cos(wr);
+    uf[1] = -a0 * std::cos(wr) - a1 * std::sin(wr);
+    uf[2] = a2;
+  }
+  // update_sem_inflow (mod_fv_solver.f90:2062-2119): the fluctuation of every ABL-inlet face, then
+  // the mean inflow it adds removed along each face normal
+  void update_sem_inflow(double /*t*/, bool look_ahead, double tau) {
+    std::fill(sem_fluc.begin(), sem_fluc.end(), 0.0);
+    if (!sem.initialized) return;
+    sem_prepare();
+    double b1 = 0.0, b2 = 0.0;
+    for (int64_t fb = 0; fb < nb; ++fb) {
+      int64_t fg = nfi + fb;
+      if (bc_of_face(fg) != BC_ABL_INLET) continue;
+      double uf[3];
+      sem_face(&m.centre[3 * fg], look_ahead, tau, uf);
+      for (int k = 0; k < 3; ++k) sem_fluc[3 * fb + k] = uf[k];
+      b1 = b1 + dot3(uf, &m.sf[3 * fg]);
+      b2 = b2 + m.area[fg];
+    }
+    if (b2 <= SMALL) return;
+    const double delta = b1 / b2;
+    for (int64_t fb = 0; fb < nb; ++fb) {
+      int64_t fg = nfi + fb;
+      if (bc_of_face(fg) != BC_ABL_INLET) continue;
+      for (int k = 0; k < 3; ++k) sem_fluc[3 * fb + k] = sem_fluc[3 * fb + k] - delta * m.normal[3 * fg + k];
+    }
+  }
+  // sem_advance (:341-358)
+  void sem_advance(double dt) {
+    if (!sem.initialized) return;
+    const double disp = sem.u_convect * dt;
+    for (int i = 0; i < sem.n; ++i) {
+      double d[3];
+      for (int k = 0; k < 3; ++k) sem.pos[3 * i + k] = sem.pos[3 * i + k] + disp * sem.n_in[k];
+      for (int k = 0; k < 3; ++k) d[k] = sem.pos[3 * i + k] - sem.x_inlet[k];
+      if (dot3(d, sem.n_in) > sem.rsup) sem_place(i, -sem.rsup, false);
+    }
   }
 
   // src/solver/mod_pressure_solver.f90:100-452
@@ -541,6 +938,9 @@ struct Solver {
         case BC_INLET:
           for (int k = 0; k < 3; ++k) u[k] = pc[m.patch[fg]].U_val[k];
           break;
+        case BC_ABL_INLET:  // mod_bc.f90:352-372: the log-law mean plus the synthetic fluctuation
+          for (int k = 0; k < 3; ++k) u[k] = abl_mean[3 * fb + k] + sem_fluc[3 * fb + k];
+          break;
         case BC_OUTLET:
         case BC_ZEROGRADIENT: {
           for (int k = 0; k < 3; ++k) u[k] = U[3 * o + k];
@@ -631,7 +1031,7 @@ struct Solver {
   }
 
   // src/bc/mod_bc.f90:489-588 (apply_temperature_bc; every caller passes grad_T, so the default
-  // branch always extrapolates with it).  The ABL-inlet profile is not part of this path.
+  // branch always extrapolates with it).
   void apply_temperature_bc(int filt) {
     for (int64_t fb = 0; fb < nb; ++fb) {
       int64_t fg = nfi + fb;
@@ -643,6 +1043,9 @@ struct Solver {
         case BC_INLET:
         case BC_FIXEDTEMP:
           T_bnd[fb] = pc[m.patch[fg]].T_val;
+          break;
+        case BC_ABL_INLET:  // mod_bc.f90:559-562
+          T_bnd[fb] = abl_T[fb];
           break;
         case BC_PERIODIC: {
           int pnb = m.periodic_partner_cell(fb);
@@ -2544,6 +2947,8 @@ struct Solver {
         for (int j = 0; j < 3; ++j) U[3 * c + j] = U[3 * c + j] + dt * (a_k * H_U[3 * c + j] + b_k * H_U0[3 * c + j]);
       for (int64_t c = 0; c < nc; ++c) T[c] = T[c] + dt * (a_k * H_T[c] + b_k * H_T0[c]);
       for (size_t i = 0; i < Cs.size(); ++i) Cs[i] = Cs[i] + dt * (a_k * H_C[i] + b_k * H_C0[i]);
+      if (sem.initialized)  // the stage's end time, sampled upstream of the step-start eddies (:1350-1358)
+        update_sem_inflow(time_n + (RK3W_C[k] + RK3W_GAMMA[k]) * dt, true, (RK3W_C[k] + RK3W_GAMMA[k]) * dt);
       velocity_bc_refresh();
       p_old = p;
       if (cp_on) std::fill(gp_cell.begin(), gp_cell.end(), 0.0);  // nothing to add back (mod_fv_solver.f90:1373-1377)
@@ -2616,6 +3021,7 @@ struct Solver {
       H_T0 = H_T;
       H_C0 = H_C;
     }
+    sem_advance(dt);  // mod_fv_solver.f90:1606-1610
     apply_scalar_bcs_all();
     time = time_n + dt;
     step++;

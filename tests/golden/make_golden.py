@@ -10,7 +10,8 @@ import os
 import sys
 
 CASES = ("tgv", "tgv_skew", "tgv_skew_chk", "pdrop", "hydro", "hydrowall", "rb", "channel", "amd", "graded",
-         "channel_most", "duct", "duct_exact", "hydro_exact", "tgv_skew_exact", "default_skew")
+         "channel_most", "duct", "duct_exact", "hydro_exact", "tgv_skew_exact", "default_skew", "inflow",
+         "inflow_jarrin")
 COLS = ("step", "time", "E", "eps", "Umax", "Ub", "tauw_mean", "nu_sgs_mean", "max_abs_divU", "max_abs_divU_cell",
         "volavg_abs_divU_cell", "dt")
 

@@ -10,7 +10,8 @@ Coverage: KEP / CDS / QUICK momentum advection, skewed and graded meshes, non-or
 correctors, outlets and walls (tgv*, pdrop, hydro*); Vreman and AMD with the log-law wall model
 and its filter (channel, amd, graded); temperature transport with van Leer TVD, fixed-temperature
 walls and Boussinesq buoyancy (rb); the MOST surface layer with its heat flux into a
-transported, buoyant temperature (channel_most).  The graded wall boxes are the reference's RB.geo meshes,
+transported, buoyant temperature (channel_most); inlet, outlet and the synthetic-eddy inflow at an
+ABL inlet, divergence-free (inflow) and Jarrin (inflow_jarrin) eddies.  The graded wall boxes are the reference's RB.geo meshes,
 rebuilt with the closed-form "Bump" node distribution (dopamine_b200.cases.bump_nodes).
 """
 import csv
@@ -47,7 +48,7 @@ def run_case(name, steps=None):
 
 
 @pytest.mark.parametrize("name", ["tgv_skew", "tgv_skew_chk", "pdrop", "hydro", "hydrowall", "tgv", "rb", "channel",
-                                  "amd", "graded", "channel_most", "duct"])
+                                  "amd", "graded", "channel_most", "duct", "inflow", "inflow_jarrin"])
 def test_oracle_matches_reference_csv(name):
     ref, got = run_case(name)
     for step, s in got.items():
