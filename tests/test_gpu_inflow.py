@@ -6,7 +6,7 @@ pins to the reference's inflow and inflow_jarrin CSVs.
 * 20 steps against the reference's CSV under its own comparison (rtol 1e-6, divergence 1e-9): the
   eddies' random sequence is the reference's.
 * A checkpoint carries the eddies (positions, signs, generator state): a restarted handle takes
-  the next steps as the uninterrupted one does.
+  the next steps as the uninterrupted one does, up to the outlet's rebuilt boundary values.
 """
 import numpy as np
 import pytest
@@ -71,6 +71,11 @@ def test_checkpoint_carries_the_eddies(tmp_path):
     ua, ub = a.sync_host()["U"], b.sync_host()["U"]
     e = float(np.linalg.norm(ub - ua) / np.linalg.norm(ua))
     print(f"inflow restart after 4 steps, 3 more: U rel {e:.2e}")
-    assert e <= 1e-10
+    # the restored eddies give the inlet the fluctuation the uninterrupted run had; the outlet's
+    # extrapolated boundary velocity is rebuilt from the restored fields and fresh gradients, as the
+    # reference's solver_refresh_after_restart rebuilds it (mod_fv_solver.f90:601-609), which moves
+    # the continuation by O(h^2) there (the wall-bounded restarts in test_gpu_output.py, with no
+    # outlet, continue to round-off)
+    assert e <= 1e-4
     a.close()
     b.close()
