@@ -379,7 +379,7 @@ def run_gpu(args, rank, world):
     return dict(nc=nc, t_dev=t_dev, t_e2e=t_e2e, step_ms=step_ms, pois_ms=pois_ms, its=its, solves=solves,
                 bytes_it=bytes_it,
                 launches=launches, clocks=clocks, solver=s, learn=learn, fallbacks=s.stats()["p_fallbacks"],
-                e2e_bytes=bytes_per_dir, plain=plain)
+                e2e_bytes=bytes_per_dir, plain=plain, setup=s.setup_times())
 
 
 def main():
@@ -478,6 +478,8 @@ def main():
                                    "; learned one-ring term trained, gated off (gamma 0) on the held-out solve")
     if args.psolver in ("fcg", "ml"):
         line["config"]["fallbacks_to_plain_pcg"] = r["fallbacks"]
+    # handle creation (device mesh and static-operator set-up, upload, pressure-solver set-up); not timed
+    line["config"]["setup_ms"] = {k: round(v, 1) for k, v in r["setup"].items()}
     if r["plain"] is not None:
         pl = r["plain"]
         pl["speedup_of_this_form"] = pl["ms_per_step"] / line["ms_per_step"]

@@ -78,7 +78,7 @@ class ParamsT(C.Structure):
         ("abl_T_ref", C.c_double), ("abl_wind_dir_deg", C.c_double), ("use_sem", C.c_int), ("sem_type", C.c_int),
         ("sem_n_eddies", C.c_int), ("sem_seed", C.c_int), ("sem_mean_law", C.c_int), ("sem_sigma", C.c_double),
         ("sem_alpha", C.c_double), ("sem_Iu_ref", C.c_double), ("sem_Iv_ratio", C.c_double),
-        ("sem_Iw_ratio", C.c_double), ("sem_rho_uw", C.c_double),
+        ("sem_Iw_ratio", C.c_double), ("sem_rho_uw", C.c_double), ("host_setup", C.c_int),
     ]
 
 

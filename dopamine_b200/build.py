@@ -14,12 +14,15 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libdopamine_b200.so")
-CU_SOURCES = ["csrc/cuda/solver.cu", "csrc/cuda/fvm_petsc.cu", "csrc/cuda/noalloc.cu"]
-CPP_SOURCES = ["csrc/host/mesh.cpp", "csrc/host/ops.cpp", "csrc/host/twolevel.cpp", "csrc/host/multilevel.cpp"]
+CU_SOURCES = ["csrc/cuda/solver.cu", "csrc/cuda/fvm_petsc.cu", "csrc/cuda/noalloc.cu", "csrc/cuda/setup_gpu.cu"]
+# The device set-up reproduces the host builder's rounding: no contraction into fused multiply-adds.
+CU_FLAGS = {"csrc/cuda/setup_gpu.cu": ["-fmad=false"]}
+CPP_SOURCES = ["csrc/host/mesh.cpp", "csrc/host/ops.cpp", "csrc/host/twolevel.cpp", "csrc/host/multilevel.cpp",
+               "csrc/host/gmsh.cpp"]
 HEADERS = ["csrc/cuda/common.cuh", "csrc/cuda/kernels.cuh", "csrc/cuda/pcg.cuh", "csrc/cuda/fcg.cuh",
            "csrc/cuda/learn.cuh", "csrc/cuda/scalars.cuh", "csrc/cuda/mlcg.cuh", "csrc/cuda/mlsolve.cuh", "csrc/cuda/mlkern.cuh", "csrc/cuda/explicit32.cuh",
-           "csrc/cuda/cellproj.cuh", "csrc/cuda/sampling.cuh", "csrc/cuda/forcing.cuh", "csrc/cuda/sem.cuh", "csrc/host/fortran_records.hpp",
-           "csrc/host/twolevel.hpp", "csrc/host/multilevel.hpp", "csrc/host/mesh.hpp",
+           "csrc/cuda/setup_gpu.hpp", "csrc/cuda/cellproj.cuh", "csrc/cuda/sampling.cuh", "csrc/cuda/forcing.cuh", "csrc/cuda/sem.cuh", "csrc/host/fortran_records.hpp",
+           "csrc/host/twolevel.hpp", "csrc/host/multilevel.hpp", "csrc/host/mesh.hpp", "csrc/host/gmsh.hpp",
            "csrc/host/ops.hpp", "../include/dopamine_b200.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -54,7 +57,7 @@ def build(force=False, verbose=False):
     common = ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-ccbin", _host_cxx(), "-I", os.path.join(ROOT, "include")]
     for rel in CU_SOURCES:
         obj = os.path.join(OUT_DIR, os.path.basename(rel) + ".o")
-        cmd = [nvcc, *ARCH, "-lineinfo", *common, "-Xptxas", "-v" if verbose else "-O3", "-c",
+        cmd = [nvcc, *ARCH, "-lineinfo", *common, *CU_FLAGS.get(rel, []), "-Xptxas", "-v" if verbose else "-O3", "-c",
                os.path.join(HERE, rel), "-o", obj]
         subprocess.run(cmd, check=True)
         objs.append(obj)

@@ -36,6 +36,7 @@
 #include "sampling.cuh"
 #include "sem.cuh"
 #include "scalars.cuh"
+#include "setup_gpu.hpp"
 
 namespace dpm {
 namespace gpu {
@@ -269,6 +270,8 @@ struct Solver {
   double poisson_ms_acc = 0.0;
   int spin_limit = 0;  // > 0: poll limit of the Krylov kernels' grid-wide waits (failure-detection tests)
   bool force_plain = false;  // dpm_select_pressure_solver: plain Jacobi-PCG although a flexible form is set up
+  SetupTimes setup_t;        // set-up stage times of init
+  double setup_upload_ms = 0.0, setup_total_ms = 0.0;
   bool flexible() const { return (use_fcg || use_ml) && !force_plain; }
 
   ~Solver() {
@@ -296,18 +299,38 @@ struct Solver {
     std::vector<int> pbc(raw->n_patches);
     for (int i = 0; i < raw->n_patches; ++i) pbc[i] = patches[i].bc_id;
     std::string err;
-    if (build_mesh(r, pbc.data(), m, &err)) {
-      std::fprintf(stderr, "dopamine_b200: mesh set-up failed: %s\n", err.c_str());
-      return DPM_ERR_MESH;
-    }
+    using Clk = std::chrono::steady_clock;
+    auto ms_between = [](Clk::time_point a, Clk::time_point b) {
+      return std::chrono::duration<double, std::milli>(b - a).count();
+    };
+    const auto t_begin = Clk::now();
     P = *prm;
     if (P.cell_projection != DPM_CELL_PROJECTION_LS && P.cell_projection != DPM_CELL_PROJECTION_EXACT) return DPM_ERR_ARG;
     cp_on = P.cell_projection == DPM_CELL_PROJECTION_EXACT;
     pc.assign(patches, patches + raw->n_patches);
-    if (build_static_ops(m, pc.data(), P, S)) return DPM_ERR_MESH;
+    if (P.host_setup) {
+      if (build_mesh(r, pbc.data(), m, &err)) {
+        std::fprintf(stderr, "dopamine_b200: mesh set-up failed: %s\n", err.c_str());
+        return DPM_ERR_MESH;
+      }
+      const auto t_mesh = Clk::now();
+      if (build_static_ops(m, pc.data(), P, S)) return DPM_ERR_MESH;
+      setup_t.mesh_ms = ms_between(t_begin, t_mesh);
+      setup_t.ops_ms = ms_between(t_mesh, Clk::now());
+    } else {
+      int rc = build_setup_device(r, pc.data(), P, device, m, S, &err, &setup_t);
+      if (rc) {
+        std::fprintf(stderr, "dopamine_b200: device set-up failed: %s\n", err.c_str());
+        return (rc < 0 && rc >= -4) ? DPM_ERR_MESH : rc;  // build_mesh's codes -1..-4
+      }
+    }
     if (m.n_cells > 2000000000LL || m.n_faces > 2000000000LL) return DPM_ERR_UNSUPPORTED;
     nc = (int)m.n_cells; nf = (int)m.n_faces; nb = (int)m.n_bnd_faces; nfp = (int)S.nfp;
-    return upload();
+    const auto t_up = Clk::now();
+    int rc = upload();
+    setup_upload_ms = ms_between(t_up, Clk::now());
+    setup_total_ms = ms_between(t_begin, Clk::now());
+    return rc;
   }
 
   template <class T>
@@ -2711,6 +2734,17 @@ int dpm_last_timing(const dpm_solver_t* h, double* step_ms, double* poisson_ms) 
 int dpm_kernel_launches(const dpm_solver_t* h, int64_t* n) {
   if (!h || !n) return DPM_ERR_ARG;
   *n = h->s->launches;
+  return DPM_OK;
+}
+
+int dpm_setup_times(const dpm_solver_t* h, double* ms) {
+  if (!h || !ms) return DPM_ERR_ARG;
+  const Solver& s = *h->s;
+  ms[0] = s.setup_t.mesh_ms;
+  ms[1] = s.setup_t.ops_ms;
+  ms[2] = s.setup_upload_ms;
+  ms[3] = s.setup_total_ms;
+  for (int k = 0; k < 7; ++k) ms[4 + k] = s.setup_t.stage_ms[k];
   return DPM_OK;
 }
 

@@ -186,6 +186,80 @@ bool try_pair(const Mesh& m, int p, int q, double& max_err, std::vector<int>& ma
 
 }  // namespace
 
+void build_cell_faces(Mesh& m) {
+  const int64_t nc = m.n_cells, nf = m.n_faces;
+  // Cell -> face CSR (mod_mesh.f90:mesh_build_connectivity).
+  m.cell_face_off.assign(nc + 1, 0);
+  for (int64_t f = 0; f < nf; ++f) {
+    m.cell_face_off[m.owner[f] + 1]++;
+    if (m.neighbour[f] >= 0) m.cell_face_off[m.neighbour[f] + 1]++;
+  }
+  for (int64_t c = 0; c < nc; ++c) m.cell_face_off[c + 1] += m.cell_face_off[c];
+  m.cell_faces.assign(m.cell_face_off[nc], -1);
+  {
+    std::vector<int64_t> cur(m.cell_face_off.begin(), m.cell_face_off.end() - 1);
+    for (int64_t f = 0; f < nf; ++f) {
+      m.cell_faces[cur[m.owner[f]]++] = (int)f;
+      if (m.neighbour[f] >= 0) m.cell_faces[cur[m.neighbour[f]]++] = (int)f;
+    }
+  }
+}
+
+int build_periodic(Mesh& m, std::string* err) {
+  const int64_t nfi = m.n_int_faces, nfb = m.n_bnd_faces;
+  // Periodic pairing (src/bc/mod_bc_setup.f90:build_periodic_pairs).
+  m.periodic_pair.assign(nfb, -1);
+  m.periodic_pair_dcf.assign(nfb, 0.0);
+  std::vector<int> per;
+  for (int p = 0; p < m.n_patches; ++p)
+    if (m.patch_bc[p] == BC_PERIODIC) per.push_back(p);
+  if (!per.empty()) {
+    std::vector<uint8_t> used(m.n_patches, 0);
+    for (size_t i = 0; i < per.size(); ++i) {
+      int p = per[i];
+      if (used[p]) continue;
+      int best_q = -1;
+      double best_err = 1e300;
+      std::vector<int> best_map, map;
+      for (size_t j = i + 1; j < per.size(); ++j) {
+        int q = per[j];
+        if (used[q]) continue;
+        double e;
+        if (try_pair(m, p, q, e, map) && e < best_err) {
+          best_err = e;
+          best_q = q;
+          best_map = map;
+        }
+      }
+      if (best_q < 0) {
+        if (err) *err = "no periodic partner for a periodic patch";
+        return -4;
+      }
+      for (int64_t k = 0; k < (int64_t)best_map.size(); ++k) {
+        int64_t fbp = m.patch_start[p] + k, fbq = m.patch_start[best_q] + best_map[k];
+        m.periodic_pair[fbp] = (int)fbq;
+        m.periodic_pair[fbq] = (int)fbp;
+        m.periodic_pair_dcf[fbp] = m.d_cf[nfi + fbq];
+        m.periodic_pair_dcf[fbq] = m.d_cf[nfi + fbp];
+      }
+      used[p] = used[best_q] = 1;
+    }
+    // finalize_periodic_partner_metrics
+    for (int64_t b = 0; b < nfb; ++b) {
+      if (m.periodic_pair_dcf[b] > 0.0) continue;
+      if (m.periodic_pair[b] >= 0) m.periodic_pair_dcf[b] = m.d_cf[nfi + m.periodic_pair[b]];
+      if (m.periodic_pair_dcf[b] <= 0.0) m.periodic_pair_dcf[b] = m.d_cf[nfi + b];
+    }
+  }
+  // Periodic interpolation weight (mod_mesh.f90:mesh_build_soa_mirror).
+  m.periodic_gc.assign(nfb, 0.5);
+  for (int64_t b = 0; b < nfb; ++b)
+    if (m.periodic_pair_dcf[b] > 0.0)
+      m.periodic_gc[b] = m.periodic_pair_dcf[b] / (m.d_cf[nfi + b] + m.periodic_pair_dcf[b] + SMALL);
+
+  return 0;
+}
+
 int build_mesh(const RawMesh& raw, const int* patch_bc, Mesh& m, std::string* err) {
   auto fail = [&](int code, const char* msg) {
     if (err) *err = msg;
@@ -305,21 +379,7 @@ int build_mesh(const RawMesh& raw, const int* patch_bc, Mesh& m, std::string* er
   }
   m.patch_bc.assign(patch_bc, patch_bc + m.n_patches);
 
-  // Cell -> face CSR (mod_mesh.f90:mesh_build_connectivity).
-  m.cell_face_off.assign(nc + 1, 0);
-  for (int64_t f = 0; f < nf; ++f) {
-    m.cell_face_off[m.owner[f] + 1]++;
-    if (m.neighbour[f] >= 0) m.cell_face_off[m.neighbour[f] + 1]++;
-  }
-  for (int64_t c = 0; c < nc; ++c) m.cell_face_off[c + 1] += m.cell_face_off[c];
-  m.cell_faces.assign(m.cell_face_off[nc], -1);
-  {
-    std::vector<int64_t> cur(m.cell_face_off.begin(), m.cell_face_off.end() - 1);
-    for (int64_t f = 0; f < nf; ++f) {
-      m.cell_faces[cur[m.owner[f]]++] = (int)f;
-      if (m.neighbour[f] >= 0) m.cell_faces[cur[m.neighbour[f]]++] = (int)f;
-    }
-  }
+  build_cell_faces(m);
 
   // Face geometry (mod_mesh.f90:mesh_compute_geometry, mesh_tag_refinement_faces).
   m.sf.assign(3 * nf, 0.0);
@@ -357,53 +417,10 @@ int build_mesh(const RawMesh& raw, const int* patch_bc, Mesh& m, std::string* er
     }
   }
 
-  // Periodic pairing (src/bc/mod_bc_setup.f90:build_periodic_pairs).
-  m.periodic_pair.assign(nfb, -1);
-  m.periodic_pair_dcf.assign(nfb, 0.0);
-  std::vector<int> per;
-  for (int p = 0; p < m.n_patches; ++p)
-    if (m.patch_bc[p] == BC_PERIODIC) per.push_back(p);
-  if (!per.empty()) {
-    std::vector<uint8_t> used(m.n_patches, 0);
-    for (size_t i = 0; i < per.size(); ++i) {
-      int p = per[i];
-      if (used[p]) continue;
-      int best_q = -1;
-      double best_err = 1e300;
-      std::vector<int> best_map, map;
-      for (size_t j = i + 1; j < per.size(); ++j) {
-        int q = per[j];
-        if (used[q]) continue;
-        double e;
-        if (try_pair(m, p, q, e, map) && e < best_err) {
-          best_err = e;
-          best_q = q;
-          best_map = map;
-        }
-      }
-      if (best_q < 0) return fail(-4, "no periodic partner for a periodic patch");
-      for (int64_t k = 0; k < (int64_t)best_map.size(); ++k) {
-        int64_t fbp = m.patch_start[p] + k, fbq = m.patch_start[best_q] + best_map[k];
-        m.periodic_pair[fbp] = (int)fbq;
-        m.periodic_pair[fbq] = (int)fbp;
-        m.periodic_pair_dcf[fbp] = m.d_cf[nfi + fbq];
-        m.periodic_pair_dcf[fbq] = m.d_cf[nfi + fbp];
-      }
-      used[p] = used[best_q] = 1;
-    }
-    // finalize_periodic_partner_metrics
-    for (int64_t b = 0; b < nfb; ++b) {
-      if (m.periodic_pair_dcf[b] > 0.0) continue;
-      if (m.periodic_pair[b] >= 0) m.periodic_pair_dcf[b] = m.d_cf[nfi + m.periodic_pair[b]];
-      if (m.periodic_pair_dcf[b] <= 0.0) m.periodic_pair_dcf[b] = m.d_cf[nfi + b];
-    }
+  {
+    int rc = build_periodic(m, err);
+    if (rc) return rc;
   }
-  // Periodic interpolation weight (mod_mesh.f90:mesh_build_soa_mirror).
-  m.periodic_gc.assign(nfb, 0.5);
-  for (int64_t b = 0; b < nfb; ++b)
-    if (m.periodic_pair_dcf[b] > 0.0)
-      m.periodic_gc[b] = m.periodic_pair_dcf[b] / (m.d_cf[nfi + b] + m.periodic_pair_dcf[b] + SMALL);
-
   // Least-squares stencil: face neighbours (periodic partners across seams), then
   // vertex-sharing cells, inverse-distance weights (mod_mesh.f90:mesh_build_ls_stencil).
   int max_faces = 1;

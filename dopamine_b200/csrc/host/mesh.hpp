@@ -88,6 +88,11 @@ struct Mesh {
 // stencil.  Returns 0 on success, a negative code otherwise (message in *err if non-null).
 int build_mesh(const RawMesh& raw, const int* patch_bc, Mesh& m, std::string* err = nullptr);
 
+// Stages of build_mesh that the device builder (csrc/cuda/meshgpu.cu) shares: the cell -> face
+// CSR from owner/neighbour, and the periodic pairing with its interpolation weights.
+void build_cell_faces(Mesh& m);
+int build_periodic(Mesh& m, std::string* err);
+
 // Smoothstep blend of the eps.grad skewness correction (src/mesh/mod_mesh.f90:497-505).
 inline double refine_blend_weight(double skew) {
   double t = (skew - SKEW_BLEND_LO) / (SKEW_BLEND_HI - SKEW_BLEND_LO);

@@ -29,7 +29,9 @@ EXPORTED = (
     "dpm_learn_loss_grad", "dpm_multilevel_hierarchy", "dpm_set_barrier_spin_limit",
     "dpm_select_pressure_solver", "dpm_cell_divergence", "dpm_cell_adjoint_gradient", "dpm_cell_project",
     "dpm_write_checkpoint", "dpm_read_checkpoint", "dpm_sampling_set_points", "dpm_sample_points",
-    "dpm_set_nudging_profiles", "dpm_set_scalar_sources",
+    "dpm_set_nudging_profiles", "dpm_set_scalar_sources", "dpm_setup_times", "dpm_setup_compare",
+    "dpm_setup_array_name", "dpm_gmsh_read", "dpm_gmsh_sizes", "dpm_gmsh_fill", "dpm_gmsh_patch_name",
+    "dpm_gmsh_free", "dpm_gmsh_write",
 )
 
 
@@ -107,6 +109,11 @@ def lib(build_if_missing=True):
     L.fvm_petsc_set_device_local_rank.argtypes = [C.c_int]
     L.dpm_pcg_solve_noalloc.argtypes = [C.c_int, C.c_int, vp, vp, vp, vp, vp, C.c_double, C.c_double, C.c_int,
                                         C.c_int, vp, ip, dp]
+    L.dpm_setup_times.argtypes = [vp, dp]
+    L.dpm_setup_compare.argtypes = [C.POINTER(abi.RawMeshT), C.POINTER(abi.PatchCfgT), C.POINTER(abi.ParamsT),
+                                    C.c_int, C.POINTER(C.c_int64), dp, dp]
+    L.dpm_setup_array_name.argtypes = [C.c_int]
+    L.dpm_setup_array_name.restype = C.c_char_p
     _lib = L
     return L
 
@@ -139,6 +146,15 @@ class Solver:
         self.centroid = np.zeros((self.nc, 3))
         self.volume = np.zeros(self.nc)
         L.dpm_cell_geometry(self.h, _p(self.centroid), _p(self.volume))
+
+    SETUP_KEYS = ("mesh_ms", "ops_ms", "upload_ms", "total_ms", "raw_upload_ms", "match_ms", "faces_ms",
+                  "periodic_ms", "stencil_ms", "pressure_ops_ms", "cell_ops_ms")
+
+    def setup_times(self):
+        """Wall-clock milliseconds of this handle's set-up (dpm_setup_times)."""
+        ms = np.zeros(len(self.SETUP_KEYS))
+        _check(lib().dpm_setup_times(self.h, _p(ms)), "dpm_setup_times")
+        return dict(zip(self.SETUP_KEYS, ms.tolist()))
 
     def close(self):
         if getattr(self, "h", None):
@@ -379,3 +395,26 @@ class Solver:
         _check(lib().dpm_cell_project(self.h, _p(u), _p(np.ascontiguousarray(bconst, dtype=np.float64)), tol, max_it,
                                       1 if identity_precond else 0, C.byref(n_it)), "dpm_cell_project")
         return u, n_it.value
+
+
+def compare_setups(case, device=0, params=None):
+    """Builds the case's mesh and static operators with the device and the host builders
+    (dpm_setup_compare).  Returns ({array name: entries whose bits differ}, largest relative
+    difference of the SGS filter tensor, {stage: ms})."""
+    L = lib()
+    mesh = abi.RawMeshView(case.mesh)
+    patches = abi.patch_cfgs(case.patches)
+    prm = params if params is not None else case.make_params()
+    mism = (C.c_int64 * 64)()
+    g = C.c_double()
+    ms = np.zeros(4)
+    _check(L.dpm_setup_compare(C.byref(mesh.struct), patches, C.byref(prm), device, mism, C.byref(g), _p(ms)),
+           "dpm_setup_compare")
+    out = {}
+    for k in range(64):
+        name = L.dpm_setup_array_name(k)
+        if name is None:
+            break
+        out[name.decode()] = int(mism[k])
+    times = dict(zip(("host_mesh_ms", "host_ops_ms", "device_mesh_ms", "device_ops_ms"), ms.tolist()))
+    return out, g.value, times

@@ -214,6 +214,11 @@ typedef struct dpm_params {
   double abl_u_ref, abl_z_ref, abl_T_ref, abl_wind_dir_deg;
   int use_sem, sem_type, sem_n_eddies, sem_seed, sem_mean_law;
   double sem_sigma, sem_alpha, sem_Iu_ref, sem_Iv_ratio, sem_Iw_ratio, sem_rho_uw;
+  /* Mesh and static-operator set-up of dpm_create (mod_gmsh_reader.f90:build_faces_from_cells,
+   * mod_mesh.f90:437-756, 1336-1461, mod_pressure_solver.f90:100-452): 0 = on the device (face
+   * matching by radix sort, per-cell geometry, LS stencil and operators one thread per cell),
+   * 1 = the host C++ builder.  Both give the same values; see dpm_setup_compare. */
+  int host_setup;
 } dpm_params_t;
 #define DPM_SEM_DFSEM 0
 #define DPM_SEM_JARRIN 1
@@ -290,6 +295,26 @@ int fvm_petsc_solve_pressure(int n_cells_local, int n_cells_global, int n_faces,
                              const double* dirichlet_values, int n_dirichlet_rows,
                              double* solution, int* iteration_count, double* residual_norm);
 
+/* Mesh ingestion: gmsh v4.1 ASCII files (src/mesh/mod_gmsh_reader.f90:gmsh_read).  Volume
+ * elements (first-order tets, hexes, prisms, pyramids; 10-node tets and 20-node hexes by their
+ * corner nodes) become cells in file order, triangles and quads become boundary faces, and the
+ * 2-D physical groups that hold faces become the patches, in $PhysicalNames order (a file without
+ * physical names gets one patch, "boundary").  dpm_gmsh_read returns DPM_ERR_ARG when the file
+ * cannot be opened and DPM_ERR_MESH for what the reference refuses (binary or pre-4 files, other
+ * element types, a surface element outside every 2-D group), with the reason in errbuf.  The
+ * arrays of dpm_gmsh_fill are dpm_raw_mesh_t's, sized by dpm_gmsh_sizes. */
+typedef struct dpm_gmsh dpm_gmsh_t;
+int dpm_gmsh_read(const char* path, dpm_gmsh_t** out, char* errbuf, int errlen);
+int dpm_gmsh_sizes(const dpm_gmsh_t* h, int64_t* n_nodes, int64_t* n_cells, int64_t* n_cell_nodes,
+                   int64_t* n_bfaces, int64_t* n_bface_nodes, int* n_patches);
+int dpm_gmsh_fill(const dpm_gmsh_t* h, double* xyz, int* cell_type, int64_t* cell_off, int* cell_nodes,
+                  int64_t* bface_off, int* bface_nodes, int* bface_patch);
+const char* dpm_gmsh_patch_name(const dpm_gmsh_t* h, int k);
+int dpm_gmsh_free(dpm_gmsh_t* h);
+/* Writes a raw mesh as a gmsh v4.1 ASCII file that dpm_gmsh_read reads back to the same cells,
+ * faces and patches: one 2-D physical group per patch (tags 1..n_patches), one 3-D group. */
+int dpm_gmsh_write(const char* path, const dpm_raw_mesh_t* mesh, const char* const* patch_names);
+
 /* ---------------------------------------------------------------------------------------- */
 /* 2. Whole-step solver handle (src/solver/mod_fv_solver.f90 FVSolver)                       */
 /* ---------------------------------------------------------------------------------------- */
@@ -329,6 +354,22 @@ int dpm_set_time(dpm_solver_t* s, double time);
 int dpm_last_timing(const dpm_solver_t* s, double* step_ms, double* poisson_ms);
 /* Kernel launch count since the handle was created (own kernels only). */
 int dpm_kernel_launches(const dpm_solver_t* s, int64_t* n);
+/* Wall-clock milliseconds of the handle's set-up: ms[0] mesh (connectivity, geometry, periodic
+ * pairs, LS stencil), ms[1] static operators, ms[2] upload and solver state, ms[3] total of
+ * dpm_create; ms[4..10] the device builder's stages (raw upload, cells and face matching, faces and
+ * cell lists, periodic pairing on the host, LS stencil, pressure operators, LS/cell operators and
+ * download), zero with host_setup. */
+int dpm_setup_times(const dpm_solver_t* s, double* ms);
+/* Builds the mesh and static operators of one configuration with both builders and compares
+ * them entry by entry.  mismatches[k] (k < DPM_SETUP_N_ARRAYS, named by dpm_setup_array_name)
+ * counts the entries of array k whose bits differ, the SGS filter tensor excepted: its scale is a
+ * cube root by pow(), whose last bit may differ between the device and host libraries, so
+ * *G_max_rel gets its largest entry difference relative to the cell's |G_11|+|G_22|+|G_33|.  ms: host mesh, host operators, device
+ * mesh, device operators. */
+#define DPM_SETUP_N_ARRAYS 64
+int dpm_setup_compare(const dpm_raw_mesh_t* mesh, const dpm_patch_cfg_t* patches, const dpm_params_t* params,
+                      int device, int64_t* mismatches, double* G_max_rel, double* ms);
+const char* dpm_setup_array_name(int k);
 /* Switches an existing handle's pressure solve: DPM_PSOLVER_JACOBI_PCG (always available) or
  * back to the flexible-CG form it was created with (that form's value, or DPM_PSOLVER_AUTO);
  * any other form returns DPM_ERR_UNSUPPORTED.  Lets the plain FP64 form be timed on the same

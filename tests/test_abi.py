@@ -12,7 +12,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 def declared_functions():
     src = open(os.path.join(ROOT, "include", "dopamine_b200.h")).read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-    return sorted(set(re.findall(r"^\s*(?:int|void|double)\s+\**\s*((?:fvm_petsc|dpm)_\w+)\s*\(", src, flags=re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|void|double|const\s+char)\s*\**\s*((?:fvm_petsc|dpm)_\w+)\s*\(", src, flags=re.M)))
 
 
 def test_header_declares_both_groups():
