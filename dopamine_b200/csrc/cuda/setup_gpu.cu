@@ -758,6 +758,43 @@ __global__ void k_wblend(int64_t nf, int64_t nfi, const double* skew, double* wb
   wbl[f] = 1.0 - t * t * (3.0 - 2.0 * t);
 }
 
+// Per-cell list widths: [0] faces, [1] boundary faces (atomicMax over cells).
+__global__ void k_cell_widths(int64_t nc, int64_t nfi, const long long* cfo, const int* cfl, int* w) {
+  int64_t c = gtid();
+  if (c >= nc) return;
+  int nbd = 0;
+  for (long long k = cfo[c]; k < cfo[c + 1]; ++k) nbd += cfl[k] >= nfi;
+  atomicMax(&w[0], (int)(cfo[c + 1] - cfo[c]));
+  atomicMax(&w[1], nbd);
+}
+
+__global__ void k_ls_width(int64_t nc, const long long* cnt, int* w) {
+  int64_t c = gtid();
+  if (c < nc) atomicMax(w, (int)cnt[c]);
+}
+
+__global__ void k_any(int64_t n, const unsigned char* v, int* flag) {
+  int64_t i = gtid();
+  if (i < n && v[i]) atomicOr(flag, 1);
+}
+
+// [n][K] -> [K][n]
+__global__ void k_to_soa(int64_t n, int K, const double* src, double* dst) {
+  int64_t i = gtid();
+  if (i >= n) return;
+  for (int k = 0; k < K; ++k) dst[(int64_t)k * n + i] = src[(int64_t)K * i + k];
+}
+
+__global__ void k_inv_floor(int64_t n, const double* v, double floor_, double* out) {
+  int64_t i = gtid();
+  if (i < n) out[i] = 1.0 / dmax(v[i], floor_);
+}
+
+__global__ void k_recip(int64_t n, const double* v, double* out) {
+  int64_t i = gtid();
+  if (i < n) out[i] = 1.0 / v[i];
+}
+
 // ---- host side -------------------------------------------------------------------------------
 
 struct Arena {
@@ -787,6 +824,16 @@ struct Arena {
       if (q == p) {
         cudaFree(q);
         q = nullptr;
+      }
+  }
+  // hands p over to `to` (no longer freed here)
+  void give(void* p, std::vector<void*>& to) {
+    if (!p) return;
+    for (auto& q : ptrs)
+      if (q == p) {
+        q = nullptr;
+        to.push_back(p);
+        return;
       }
   }
 };
@@ -824,8 +871,13 @@ struct Stream {
 
 }  // namespace
 
+SetupDeviceArrays::~SetupDeviceArrays() {
+  for (void* p : owned) cudaFree(p);
+}
+
 int build_setup_device(const RawMesh& raw, const dpm_patch_cfg_t* pc, const dpm_params_t& P, int device, Mesh& m,
-                       StaticOps& S, std::string* err, SetupTimes* times) {
+                       StaticOps& S, std::string* err, SetupTimes* times, SetupDeviceArrays* dev) {
+  const bool full = dev == nullptr;  // every array to the host, as the host builder fills them
   auto fail = [&](int code, const char* msg) {
     if (err) *err = msg;
     return code;
@@ -1013,25 +1065,36 @@ int build_setup_device(const RawMesh& raw, const dpm_patch_cfg_t* pc, const dpm_
   SLAUNCH(nc, k_sort_rows, nc, d_cfo, d_cfl);
   // the host needs the boundary faces for the periodic pairing and the outlet rows, and the
   // whole mesh for the rest of the solver set-up
-  std::vector<long long> cfo_h;
+  int widths[2] = {0, 0}, refine_any = 0;
+  int* d_widths = ar.get<int>(4);
+  SCK(cudaGetLastError());
+  SCK(cudaMemsetAsync(d_widths, 0, 4 * sizeof(int), st));
+  SLAUNCH(nc, k_cell_widths, nc, nfi, d_cfo, d_cfl, d_widths);
+  SLAUNCH(nfi, k_any, nfi, d_isref, d_widths + 2);
+  SCK(cudaMemcpyAsync(widths, d_widths, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+  SCK(cudaMemcpyAsync(&refine_any, d_widths + 2, sizeof(int), cudaMemcpyDeviceToHost, st));
   SCK(fetch(m.centroid, d_cen, 3 * nc, st) ? cudaSuccess : cudaErrorUnknown);
   SCK(fetch(m.volume, d_vol, nc, st) ? cudaSuccess : cudaErrorUnknown);
   SCK(fetch(m.owner, d_owner, nf, st) ? cudaSuccess : cudaErrorUnknown);
-  SCK(fetch(m.neighbour, d_nbr, nf, st) ? cudaSuccess : cudaErrorUnknown);
   SCK(fetch(m.patch, d_patch, nf, st) ? cudaSuccess : cudaErrorUnknown);
   SCK(fetch(m.area, d_area, nf, st) ? cudaSuccess : cudaErrorUnknown);
   SCK(fetch(m.centre, d_centre, 3 * nf, st) ? cudaSuccess : cudaErrorUnknown);
   SCK(fetch(m.normal, d_normal, 3 * nf, st) ? cudaSuccess : cudaErrorUnknown);
-  SCK(fetch(m.sf, d_sf, 3 * nf, st) ? cudaSuccess : cudaErrorUnknown);
   SCK(fetch(m.d_cf, d_dcf, nf, st) ? cudaSuccess : cudaErrorUnknown);
-  SCK(fetch(m.gc, d_gc, nf, st) ? cudaSuccess : cudaErrorUnknown);
-  SCK(fetch(m.eps, d_eps, 3 * nf, st) ? cudaSuccess : cudaErrorUnknown);
-  SCK(fetch(m.skew, d_skew, nf, st) ? cudaSuccess : cudaErrorUnknown);
-  SCK(fetch(m.is_refine, d_isref, nf, st) ? cudaSuccess : cudaErrorUnknown);
-  SCK(fetch(cfo_h, d_cfo, nc + 1, st) ? cudaSuccess : cudaErrorUnknown);
-  SCK(fetch(m.cell_faces, d_cfl, ncf, st) ? cudaSuccess : cudaErrorUnknown);
+  if (full) {
+    std::vector<long long> cfo_h;
+    SCK(fetch(m.neighbour, d_nbr, nf, st) ? cudaSuccess : cudaErrorUnknown);
+    SCK(fetch(m.sf, d_sf, 3 * nf, st) ? cudaSuccess : cudaErrorUnknown);
+    SCK(fetch(m.gc, d_gc, nf, st) ? cudaSuccess : cudaErrorUnknown);
+    SCK(fetch(m.eps, d_eps, 3 * nf, st) ? cudaSuccess : cudaErrorUnknown);
+    SCK(fetch(m.skew, d_skew, nf, st) ? cudaSuccess : cudaErrorUnknown);
+    SCK(fetch(m.is_refine, d_isref, nf, st) ? cudaSuccess : cudaErrorUnknown);
+    SCK(fetch(cfo_h, d_cfo, nc + 1, st) ? cudaSuccess : cudaErrorUnknown);
+    SCK(fetch(m.cell_faces, d_cfl, ncf, st) ? cudaSuccess : cudaErrorUnknown);
+    SCK(cudaStreamSynchronize(st));
+    m.cell_face_off.assign(cfo_h.begin(), cfo_h.end());
+  }
   SCK(cudaStreamSynchronize(st));
-  m.cell_face_off.assign(cfo_h.begin(), cfo_h.end());
   T.stage_ms[2] = ms_since(t0);
 
   // periodic pairing (host, boundary faces only)
@@ -1044,8 +1107,7 @@ int build_setup_device(const RawMesh& raw, const dpm_patch_cfg_t* pc, const dpm_
 
   // LS stencil: face neighbours (periodic partners across seams), then vertex-sharing cells
   t0 = Clock::now();
-  int max_faces = 1;
-  for (int64_t c = 0; c < nc; ++c) max_faces = std::max<int>(max_faces, (int)(cfo_h[c + 1] - cfo_h[c]));
+  const int max_faces = std::max(1, widths[0]);
   const int max_st = std::max(32, 4 * max_faces);
   int* d_pbc = ar.put(m.patch_bc.data(), (size_t)m.n_patches, st);
   int* d_ppair = ar.put(m.periodic_pair.data(), nfb, st);
@@ -1082,15 +1144,22 @@ int build_setup_device(const RawMesh& raw, const dpm_patch_cfg_t* pc, const dpm_
              d_lscell, d_lsface, d_lsw, d_cnt1};
     SLAUNCH(nc, k_ls_weights, a);
   }
-  std::vector<long long> lsoff_h;
   unsigned long long ndeg = 0;
-  SCK(fetch(lsoff_h, d_lsoff, nc + 1, st) ? cudaSuccess : cudaErrorUnknown);
-  SCK(fetch(m.ls_cell, d_lscell, ns, st) ? cudaSuccess : cudaErrorUnknown);
-  SCK(fetch(m.ls_face, d_lsface, ns, st) ? cudaSuccess : cudaErrorUnknown);
-  SCK(fetch(m.ls_w, d_lsw, 3 * ns, st) ? cudaSuccess : cudaErrorUnknown);
+  SCK(cudaMemsetAsync(d_widths + 3, 0, sizeof(int), st));
+  SLAUNCH(nc, k_ls_width, nc, d_lcnt, d_widths + 3);
+  int W = 0;
+  SCK(cudaMemcpyAsync(&W, d_widths + 3, sizeof(int), cudaMemcpyDeviceToHost, st));
+  if (full) {
+    std::vector<long long> lsoff_h;
+    SCK(fetch(lsoff_h, d_lsoff, nc + 1, st) ? cudaSuccess : cudaErrorUnknown);
+    SCK(fetch(m.ls_cell, d_lscell, ns, st) ? cudaSuccess : cudaErrorUnknown);
+    SCK(fetch(m.ls_face, d_lsface, ns, st) ? cudaSuccess : cudaErrorUnknown);
+    SCK(fetch(m.ls_w, d_lsw, 3 * ns, st) ? cudaSuccess : cudaErrorUnknown);
+    SCK(cudaStreamSynchronize(st));
+    m.ls_off.assign(lsoff_h.begin(), lsoff_h.end());
+  }
   SCK(cudaMemcpyAsync(&ndeg, d_cnt1, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
   SCK(cudaStreamSynchronize(st));
-  m.ls_off.assign(lsoff_h.begin(), lsoff_h.end());
   m.ls_degenerate = (int64_t)ndeg;
   for (void* p : {(void*)d_vcnt, (void*)d_voff, (void*)d_vcell, (void*)d_tnb, (void*)d_tface, (void*)d_tper,
                   (void*)d_lcnt})
@@ -1187,7 +1256,7 @@ int build_setup_device(const RawMesh& raw, const dpm_patch_cfg_t* pc, const dpm_
     if (S.bnd_bc[b] != BC_OUTLET) continue;
     int64_t f = nfi + b;
     int o = m.owner[f];
-    const double* s = &m.sf[3 * f];
+    const double s[3] = {m.area[f] * m.normal[3 * f], m.area[f] * m.normal[3 * f + 1], m.area[f] * m.normal[3 * f + 2]};
     double d[3], k[3];
     for (int j = 0; j < 3; ++j) d[j] = m.centre[3 * f + j] - m.centroid[3 * o + j];
     double len = std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
@@ -1230,19 +1299,12 @@ int build_setup_device(const RawMesh& raw, const dpm_patch_cfg_t* pc, const dpm_
   SLAUNCH(nfi, k_ps_interior, nfi, d_owner, d_nbr, d_cen, d_normal, d_area, d_dcf, cfl, d_pso, d_psn, d_psf, d_psc,
           d_bad);
   SLAUNCH(nfp, k_ps_jasak, nfp, d_pso, d_psn, d_psf, d_sf, d_cen, cfl, d_kk, d_cnt1);
-  int Sw = 0, SB = 0;
-  for (int64_t c = 0; c < nc; ++c) {
-    Sw = std::max<int>(Sw, (int)(cfo_h[c + 1] - cfo_h[c]));
-    int nbd = 0;
-    for (long long k = cfo_h[c]; k < cfo_h[c + 1]; ++k) nbd += m.cell_faces[k] >= nfi;
-    SB = std::max(SB, nbd);
-  }
+  const int Sw = widths[0], SB = widths[1];
   S.S = Sw;
   S.SB = SB;
   int* d_cfell = ar.get<int>((size_t)std::max(Sw, 1) * nc);
   int* d_cbell = ar.get<int>((size_t)std::max(SB, 1) * nc);
   int* d_cpsell = ar.get<int>((size_t)CPS_CAP * nc);
-  int* d_widths = ar.get<int>(2);
   double* d_diag = ar.get<double>(nc);
   SCK(cudaGetLastError());
   SCK(cudaMemsetAsync(d_widths, 0, 2 * sizeof(int), st));
@@ -1250,7 +1312,6 @@ int build_setup_device(const RawMesh& raw, const dpm_patch_cfg_t* pc, const dpm_
           d_cbell, std::max(SB, 1), d_widths, d_bad);
   SLAUNCH(nc, k_diag, nc, nfi, SB, d_cpsell, d_cbell, d_psc, d_bdiag, d_bdiag_on, d_diag);
   SLAUNCH(nc, k_arow, nc, d_cpsell, d_pso, d_psn, d_psc, d_diag, 0, (int*)nullptr, (double*)nullptr, d_widths + 1);
-  int widths[2] = {0, 0};
   unsigned long long n_active_i = 0;
   SCK(cudaMemcpyAsync(widths, d_widths, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
   SCK(cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -1268,8 +1329,6 @@ int build_setup_device(const RawMesh& raw, const dpm_patch_cfg_t* pc, const dpm_
   T.stage_ms[5] = ms_since(t0);
   // LS stencil as ELL, T^-1, filter tensor, blend weights
   t0 = Clock::now();
-  int W = 0;
-  for (int64_t c = 0; c < nc; ++c) W = std::max<int>(W, (int)(lsoff_h[c + 1] - lsoff_h[c]));
   S.W = W;
   const int Wc = std::max(W, 1);
   int* d_lsidx = ar.get<int>((size_t)Wc * nc);
@@ -1287,43 +1346,112 @@ int build_setup_device(const RawMesh& raw, const dpm_patch_cfg_t* pc, const dpm_
   } else {
     SLAUNCH(nc, k_ls_ell, nc, nfi, nfb, W, d_lsoff, d_lscell, d_lsface, d_lsw, d_lsidx, d_lswell);
   }
+  if (!full) {  // the ELL copy is what the step reads
+    SCK(cudaStreamSynchronize(st));
+    for (void* q : {(void*)d_lscell, (void*)d_lsface, (void*)d_lsw}) ar.drop(q);
+  }
   SLAUNCH(nc, k_tinv, nc, nfi, SB, d_cpsell, d_cbell, d_psf, d_bbc, d_area, d_normal, d_tinv);
   SLAUNCH(nc, k_filter, nc, d_cfo, d_cfl, d_centre, d_cen, d_area, d_vol, d_G0);
   SLAUNCH(nc, k_filter_smooth, nc, nfi, d_cfo, d_cfl, d_owner, d_nbr, d_area, d_G0, d_G1);
   SLAUNCH(nc, k_filter_smooth, nc, nfi, d_cfo, d_cfl, d_owner, d_nbr, d_area, d_G1, d_G0);
   SLAUNCH(nf, k_wblend, nf, nfi, d_skew, d_wbl);
-  // download
-  std::vector<int> cps_full;
-  std::vector<double> kk_h;
-  SCK(fetch(S.ps_o, d_pso, nfp, st) ? cudaSuccess : cudaErrorUnknown);
-  SCK(fetch(S.ps_n, d_psn, nfp, st) ? cudaSuccess : cudaErrorUnknown);
-  SCK(fetch(S.ps_f, d_psf, nfp, st) ? cudaSuccess : cudaErrorUnknown);
-  SCK(fetch(S.ps_coeff, d_psc, nfp, st) ? cudaSuccess : cudaErrorUnknown);
-  SCK(fetch(kk_h, d_kk, 3 * nfp, st) ? cudaSuccess : cudaErrorUnknown);
-  SCK(fetch(S.diag, d_diag, nc, st) ? cudaSuccess : cudaErrorUnknown);
-  SCK(fetch(S.A_col, d_acol, (size_t)S.WA * nc, st) ? cudaSuccess : cudaErrorUnknown);
-  SCK(fetch(S.A_val, d_aval, (size_t)S.WA * nc, st) ? cudaSuccess : cudaErrorUnknown);
-  SCK(fetch(S.cell_face, d_cfell, (size_t)std::max(Sw, 1) * nc, st) ? cudaSuccess : cudaErrorUnknown);
-  SCK(fetch(S.cell_bnd, d_cbell, (size_t)std::max(SB, 1) * nc, st) ? cudaSuccess : cudaErrorUnknown);
-  SCK(fetch(cps_full, d_cpsell, (size_t)std::max(S.SP, 1) * nc, st) ? cudaSuccess : cudaErrorUnknown);
-  SCK(fetch(S.ls_idx, d_lsidx, (size_t)Wc * nc, st) ? cudaSuccess : cudaErrorUnknown);
-  SCK(fetch(S.ls_w, d_lswell, (size_t)3 * Wc * nc, st) ? cudaSuccess : cudaErrorUnknown);
-  SCK(fetch(S.Tinv, d_tinv, 9 * (size_t)nc, st) ? cudaSuccess : cudaErrorUnknown);
-  SCK(fetch(S.G, d_G0, 9 * (size_t)nc, st) ? cudaSuccess : cudaErrorUnknown);
-  SCK(fetch(S.wblend, d_wbl, nf, st) ? cudaSuccess : cudaErrorUnknown);
-  SCK(cudaStreamSynchronize(st));
-  S.cell_ps.swap(cps_full);
-  T.stage_ms[6] = ms_since(t0);
-  // host remainder: weights of the periodic faces, non-orthogonal switches, volumes, wall distance
-  S.ps_gcf.resize(nfp);
-  S.ps_gcw.resize(nfp);
-  std::memcpy(S.ps_gcf.data(), m.gc.data(), nfi * sizeof(double));
-  std::memcpy(S.ps_gcw.data(), m.gc.data(), nfi * sizeof(double));
-  for (int64_t k = 0; k < npc; ++k) {
-    S.ps_gcf[nfi + k] = tp_gcf[k];
-    S.ps_gcw[nfi + k] = tp_gcw[k];
-  }
   const int64_t n_active = (int64_t)n_active_i + n_active_b;
+  S.skip_nonortho = (n_active == 0);
+  if (full) {
+    std::vector<int> cps_full;
+    std::vector<double> kk_h;
+    SCK(fetch(S.ps_o, d_pso, nfp, st) ? cudaSuccess : cudaErrorUnknown);
+    SCK(fetch(S.ps_n, d_psn, nfp, st) ? cudaSuccess : cudaErrorUnknown);
+    SCK(fetch(S.ps_f, d_psf, nfp, st) ? cudaSuccess : cudaErrorUnknown);
+    SCK(fetch(S.ps_coeff, d_psc, nfp, st) ? cudaSuccess : cudaErrorUnknown);
+    SCK(fetch(kk_h, d_kk, 3 * nfp, st) ? cudaSuccess : cudaErrorUnknown);
+    SCK(fetch(S.diag, d_diag, nc, st) ? cudaSuccess : cudaErrorUnknown);
+    SCK(fetch(S.A_col, d_acol, (size_t)S.WA * nc, st) ? cudaSuccess : cudaErrorUnknown);
+    SCK(fetch(S.A_val, d_aval, (size_t)S.WA * nc, st) ? cudaSuccess : cudaErrorUnknown);
+    SCK(fetch(S.cell_face, d_cfell, (size_t)std::max(Sw, 1) * nc, st) ? cudaSuccess : cudaErrorUnknown);
+    SCK(fetch(S.cell_bnd, d_cbell, (size_t)std::max(SB, 1) * nc, st) ? cudaSuccess : cudaErrorUnknown);
+    SCK(fetch(cps_full, d_cpsell, (size_t)std::max(S.SP, 1) * nc, st) ? cudaSuccess : cudaErrorUnknown);
+    SCK(fetch(S.ls_idx, d_lsidx, (size_t)Wc * nc, st) ? cudaSuccess : cudaErrorUnknown);
+    SCK(fetch(S.ls_w, d_lswell, (size_t)3 * Wc * nc, st) ? cudaSuccess : cudaErrorUnknown);
+    SCK(fetch(S.Tinv, d_tinv, 9 * (size_t)nc, st) ? cudaSuccess : cudaErrorUnknown);
+    SCK(fetch(S.G, d_G0, 9 * (size_t)nc, st) ? cudaSuccess : cudaErrorUnknown);
+    SCK(fetch(S.wblend, d_wbl, nf, st) ? cudaSuccess : cudaErrorUnknown);
+    SCK(cudaStreamSynchronize(st));
+    S.cell_ps.swap(cps_full);
+    S.ps_gcf.resize(nfp);
+    S.ps_gcw.resize(nfp);
+    std::memcpy(S.ps_gcf.data(), m.gc.data(), nfi * sizeof(double));
+    std::memcpy(S.ps_gcw.data(), m.gc.data(), nfi * sizeof(double));
+    for (int64_t k = 0; k < npc; ++k) {
+      S.ps_gcf[nfi + k] = tp_gcf[k];
+      S.ps_gcw[nfi + k] = tp_gcw[k];
+    }
+    S.ps_k.assign(3 * nfp, 0.0);
+    S.ps_krc.assign(3 * nfp, 0.0);
+    if (!S.skip_nonortho) {
+      S.ps_k = kk_h;
+      if (!P.rhie_chow_dual) S.ps_krc = kk_h;
+    }
+  } else {
+    // the time step's layouts, in HBM; the host keeps the matrix for the hierarchy set-ups
+    SCK(fetch(S.A_col, d_acol, (size_t)S.WA * nc, st) ? cudaSuccess : cudaErrorUnknown);
+    SCK(fetch(S.A_val, d_aval, (size_t)S.WA * nc, st) ? cudaSuccess : cudaErrorUnknown);
+    SetupDeviceArrays& o = *dev;
+    auto soa = [&](const double* src, int64_t n, int K) {
+      double* dst = ar.get<double>((size_t)K * n);
+      if (dst && n > 0) k_to_soa<<<nblocks(n), STPB, 0, st>>>(n, K, src, dst);
+      return dst;
+    };
+    o.cen = soa(d_cen, nc, 3);
+    o.Tinv = soa(d_tinv, nc, 9);
+    o.G = soa(d_G0, nc, 9);
+    o.sf = soa(d_sf, nf, 3);
+    o.nrm = soa(d_normal, nf, 3);
+    o.fcen = soa(d_centre, nf, 3);
+    o.eps = soa(d_eps, nf, 3);
+    o.ivol = ar.get<double>(nc);
+    o.Adinv = ar.get<double>(nc);
+    o.psgcf = ar.get<double>(nfp);
+    o.psgcw = ar.get<double>(nfp);
+    SCK(cudaGetLastError());
+    SLAUNCH(nc, k_inv_floor, nc, d_vol, SMALL, o.ivol);
+    SLAUNCH(nc, k_recip, nc, d_diag, o.Adinv);
+    SCK(cudaMemcpyAsync(o.psgcf, d_gc, nfi * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    SCK(cudaMemcpyAsync(o.psgcw, d_gc, nfi * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    if (npc) {
+      SCK(cudaMemcpyAsync(o.psgcf + nfi, tp_gcf.data(), npc * sizeof(double), cudaMemcpyHostToDevice, st));
+      SCK(cudaMemcpyAsync(o.psgcw + nfi, tp_gcw.data(), npc * sizeof(double), cudaMemcpyHostToDevice, st));
+    }
+    if (S.skip_nonortho) {  // both k-vectors zero
+      SCK(cudaMemsetAsync(d_kk, 0, 3 * nfp * sizeof(double), st));
+      o.psk = o.pskrc = d_kk;
+    } else {
+      o.psk = d_kk;
+      if (P.rhie_chow_dual) {
+        o.pskrc = ar.get<double>(3 * nfp);
+        SCK(cudaGetLastError());
+        SCK(cudaMemsetAsync(o.pskrc, 0, 3 * nfp * sizeof(double), st));
+      } else {
+        o.pskrc = d_kk;  // the same vector, read-only
+      }
+    }
+    o.vol = d_vol; o.area = d_area; o.gc = d_gc; o.wbl = d_wbl; o.dcf = d_dcf;
+    o.fo = d_owner; o.fn = d_nbr;
+    o.cf = d_cfell; o.cps = d_cpsell; o.cbn = d_cbell; o.ls_idx = d_lsidx; o.ls_w = d_lswell;
+    o.pso = d_pso; o.psn = d_psn; o.psf = d_psf; o.psc = d_psc; o.Acol = d_acol; o.Aval = d_aval;
+    o.bps = bps;
+    o.bcanon.assign(bcanon.begin(), bcanon.end());
+    SCK(cudaStreamSynchronize(st));
+    for (void* q : {(void*)o.cen, (void*)o.Tinv, (void*)o.G, (void*)o.sf, (void*)o.nrm, (void*)o.fcen, (void*)o.eps,
+                    (void*)o.ivol, (void*)o.Adinv, (void*)o.psgcf, (void*)o.psgcw, (void*)o.psk, (void*)o.vol,
+                    (void*)o.area, (void*)o.gc, (void*)o.wbl, (void*)o.dcf, (void*)o.fo, (void*)o.fn, (void*)o.cf,
+                    (void*)o.cps, (void*)o.cbn, (void*)o.ls_idx, (void*)o.ls_w, (void*)o.pso, (void*)o.psn,
+                    (void*)o.psf, (void*)o.psc, (void*)o.Acol, (void*)o.Aval})
+      ar.give(q, o.owned);
+    if (o.pskrc != o.psk) ar.give(o.pskrc, o.owned);
+  }
+  T.stage_ms[6] = ms_since(t0);
+  // host remainder: non-orthogonal switches, volumes, wall distance
   int n_gradbc = 0;
   for (int q = 0; q < m.n_patches; ++q) {
     int b = pc[q].bc_id;
@@ -1331,20 +1459,12 @@ int build_setup_device(const RawMesh& raw, const dpm_patch_cfg_t* pc, const dpm_
           b == BC_WALL_MODEL || b == BC_SLIP || b == BC_SYMMETRY))
       n_gradbc++;
   }
-  S.skip_nonortho = (n_active == 0);
   S.skip_grad_p = S.skip_nonortho && n_gradbc == 0;
   S.n_nonortho_corr = P.n_nonortho_corr > 0 ? P.n_nonortho_corr : (S.skip_nonortho ? 1 : 2);
-  S.ps_k.assign(3 * nfp, 0.0);
-  S.ps_krc.assign(3 * nfp, 0.0);
-  if (!S.skip_nonortho) {
-    S.ps_k = kk_h;
+  if (!S.skip_nonortho)
     for (int64_t b = 0; b < nfb; ++b)
       for (int j = 0; j < 3; ++j) S.bnd_kout[j * nfb + b] = kb[3 * b + j];
-    if (!P.rhie_chow_dual) S.ps_krc = kk_h;
-  }
-  S.diag_interface = false;
-  for (int64_t f = 0; f < nfi; ++f)
-    if (m.is_refine[f]) { S.diag_interface = true; break; }
+  S.diag_interface = refine_any != 0;
   S.V_min = 1e300;
   S.V_total = 0.0;
   for (int64_t c = 0; c < nc; ++c) { S.V_min = std::min(S.V_min, m.volume[c]); S.V_total += m.volume[c]; }

@@ -271,7 +271,7 @@ struct Solver {
   int spin_limit = 0;  // > 0: poll limit of the Krylov kernels' grid-wide waits (failure-detection tests)
   bool force_plain = false;  // dpm_select_pressure_solver: plain Jacobi-PCG although a flexible form is set up
   SetupTimes setup_t;        // set-up stage times of init
-  double setup_upload_ms = 0.0, setup_total_ms = 0.0;
+  double setup_upload_ms = 0.0, setup_total_ms = 0.0, setup_psolver_ms = 0.0;
   bool flexible() const { return (use_fcg || use_ml) && !force_plain; }
 
   ~Solver() {
@@ -317,8 +317,10 @@ struct Solver {
       if (build_static_ops(m, pc.data(), P, S)) return DPM_ERR_MESH;
       setup_t.mesh_ms = ms_between(t_begin, t_mesh);
       setup_t.ops_ms = ms_between(t_mesh, Clk::now());
-    } else {
-      int rc = build_setup_device(r, pc.data(), P, device, m, S, &err, &setup_t);
+    }
+    SetupDeviceArrays da;
+    if (!P.host_setup) {
+      int rc = build_setup_device(r, pc.data(), P, device, m, S, &err, &setup_t, &da);
       if (rc) {
         std::fprintf(stderr, "dopamine_b200: device set-up failed: %s\n", err.c_str());
         return (rc < 0 && rc >= -4) ? DPM_ERR_MESH : rc;  // build_mesh's codes -1..-4
@@ -327,7 +329,7 @@ struct Solver {
     if (m.n_cells > 2000000000LL || m.n_faces > 2000000000LL) return DPM_ERR_UNSUPPORTED;
     nc = (int)m.n_cells; nf = (int)m.n_faces; nb = (int)m.n_bnd_faces; nfp = (int)S.nfp;
     const auto t_up = Clk::now();
-    int rc = upload();
+    int rc = upload(P.host_setup ? nullptr : &da);
     setup_upload_ms = ms_between(t_up, Clk::now());
     setup_total_ms = ms_between(t_begin, Clk::now());
     return rc;
@@ -348,39 +350,67 @@ struct Solver {
     return s;
   }
 
-  int upload() {
+  // Static data to HBM: from the host builder's m and S, or (da) adopted from the device builder,
+  // whose arrays are already in these layouts.
+  int upload(SetupDeviceArrays* da) {
     const int64_t nfi = m.n_int_faces;
     d.nc = nc; d.nf = nf; d.nfi = (int)nfi; d.nb = nb; d.nfp = nfp;
     d.S = S.S; d.SP = S.SP; d.SB = S.SB; d.W = S.W; d.WA = S.WA;
-    std::vector<double> ivol(nc);
-    for (int c = 0; c < nc; ++c) ivol[c] = 1.0 / std::max(m.volume[c], SMALL);
-    d.vol = mem.upload(m.volume);
-    d.ivol = mem.upload(ivol);
-    d.cen = mem.upload(soa3(m.centroid, nc));
-    d.Tinv = mem.upload(soa9(S.Tinv, nc));
-    d.G = mem.upload(soa9(S.G, nc));
-    d.cf = mem.upload(S.cell_face);
-    d.cps = mem.upload(S.cell_ps);
-    d.cbn = mem.upload(S.cell_bnd);
-    d.ls_idx = mem.upload(S.ls_idx);
-    d.ls_w = mem.upload(S.ls_w);
-    d.fo = mem.upload(m.owner);
-    d.fn = mem.upload(m.neighbour);
-    d.sf = mem.upload(soa3(m.sf, nf));
-    d.nrm = mem.upload(soa3(m.normal, nf));
-    d.fcen = mem.upload(soa3(m.centre, nf));
-    d.eps = mem.upload(soa3(m.eps, nf));
-    d.area = mem.upload(m.area);
-    d.gc = mem.upload(m.gc);
-    d.wbl = mem.upload(S.wblend);
-    d.dcf = mem.upload(m.d_cf);
     std::vector<int> bps(nb, -1), bcanon(nb, 0);
-    for (int i = (int)nfi; i < nfp; ++i) {
-      int b = S.ps_f[i] - (int)nfi;
-      bps[b] = i;
-      bcanon[b] = 1;
-      int pb = m.periodic_pair[b];
-      if (pb >= 0) bps[pb] = i;
+    if (da) {
+      for (void* q : da->release()) mem.ptrs.push_back(q);
+      d.vol = da->vol; d.ivol = da->ivol; d.cen = da->cen; d.Tinv = da->Tinv; d.G = da->G;
+      d.cf = da->cf; d.cps = da->cps; d.cbn = da->cbn; d.ls_idx = da->ls_idx; d.ls_w = da->ls_w;
+      d.fo = da->fo; d.fn = da->fn; d.sf = da->sf; d.nrm = da->nrm; d.fcen = da->fcen; d.eps = da->eps;
+      d.area = da->area; d.gc = da->gc; d.wbl = da->wbl; d.dcf = da->dcf;
+      d.pso = da->pso; d.psn = da->psn; d.psf = da->psf; d.psc = da->psc; d.psgcf = da->psgcf;
+      d.psgcw = da->psgcw; d.psk = da->psk; d.pskrc = da->pskrc;
+      d.Acol = da->Acol; d.Aval = da->Aval; d.Adinv = da->Adinv;
+      bps = da->bps;
+      bcanon = da->bcanon;
+    } else {
+      std::vector<double> ivol(nc);
+      for (int c = 0; c < nc; ++c) ivol[c] = 1.0 / std::max(m.volume[c], SMALL);
+      d.vol = mem.upload(m.volume);
+      d.ivol = mem.upload(ivol);
+      d.cen = mem.upload(soa3(m.centroid, nc));
+      d.Tinv = mem.upload(soa9(S.Tinv, nc));
+      d.G = mem.upload(soa9(S.G, nc));
+      d.cf = mem.upload(S.cell_face);
+      d.cps = mem.upload(S.cell_ps);
+      d.cbn = mem.upload(S.cell_bnd);
+      d.ls_idx = mem.upload(S.ls_idx);
+      d.ls_w = mem.upload(S.ls_w);
+      d.fo = mem.upload(m.owner);
+      d.fn = mem.upload(m.neighbour);
+      d.sf = mem.upload(soa3(m.sf, nf));
+      d.nrm = mem.upload(soa3(m.normal, nf));
+      d.fcen = mem.upload(soa3(m.centre, nf));
+      d.eps = mem.upload(soa3(m.eps, nf));
+      d.area = mem.upload(m.area);
+      d.gc = mem.upload(m.gc);
+      d.wbl = mem.upload(S.wblend);
+      d.dcf = mem.upload(m.d_cf);
+      d.pso = mem.upload(S.ps_o);
+      d.psn = mem.upload(S.ps_n);
+      d.psf = mem.upload(S.ps_f);
+      d.psc = mem.upload(S.ps_coeff);
+      d.psgcf = mem.upload(S.ps_gcf);
+      d.psgcw = mem.upload(S.ps_gcw);
+      d.psk = mem.upload(S.ps_k);
+      d.pskrc = mem.upload(S.ps_krc);
+      d.Acol = mem.upload(S.A_col);
+      d.Aval = mem.upload(S.A_val);
+      std::vector<double> dinv(nc);
+      for (int c = 0; c < nc; ++c) dinv[c] = 1.0 / S.diag[c];
+      d.Adinv = mem.upload(dinv);
+      for (int i = (int)nfi; i < nfp; ++i) {
+        int b = S.ps_f[i] - (int)nfi;
+        bps[b] = i;
+        bcanon[b] = 1;
+        int pb = m.periodic_pair[b];
+        if (pb >= 0) bps[pb] = i;
+      }
     }
     std::vector<double> bU(3 * nb, 0.0), bp(nb, 0.0);
     const double wr = P.abl_wind_dir_deg * SEM_PI / 180.0;
@@ -409,19 +439,6 @@ struct Solver {
     d.yw = mem.upload(S.y_w);
     d.bUval = mem.upload(bU);
     d.bpval = mem.upload(bp);
-    d.pso = mem.upload(S.ps_o);
-    d.psn = mem.upload(S.ps_n);
-    d.psf = mem.upload(S.ps_f);
-    d.psc = mem.upload(S.ps_coeff);
-    d.psgcf = mem.upload(S.ps_gcf);
-    d.psgcw = mem.upload(S.ps_gcw);
-    d.psk = mem.upload(S.ps_k);
-    d.pskrc = mem.upload(S.ps_krc);
-    d.Acol = mem.upload(S.A_col);
-    d.Aval = mem.upload(S.A_val);
-    std::vector<double> dinv(nc);
-    for (int c = 0; c < nc; ++c) dinv[c] = 1.0 / S.diag[c];
-    d.Adinv = mem.upload(dinv);
     {  // TVD upwind context per face and flux sign, when a van Leer / Koren scheme is configured
       auto is_tvd = [](int sch) { return sch == DPM_SCHEME_VANLEER_TVD || sch == DPM_SCHEME_KOREN_TVD; };
       if (is_tvd(P.scheme) || (P.boussinesq && is_tvd(P.temperature_scheme)) ||
@@ -500,6 +517,7 @@ struct Solver {
       if (rc) return rc;
       if (x32 && P.use_nudging) return DPM_ERR_UNSUPPORTED;  // the FP32 explicit half fuses the predictor
     }
+    const auto t_ps = std::chrono::steady_clock::now();
     if (P.p_solver == DPM_PSOLVER_TWOLEVEL_FCG) {
       int rc = setup_fcg(dev_sms);
       if (rc) return rc;
@@ -516,6 +534,7 @@ struct Solver {
     } else if (P.form == DPM_FORM_MIXED) {
       return DPM_ERR_UNSUPPORTED;  // the precision form is built on the flexible CG
     }
+    setup_psolver_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_ps).count();
     // initial fields: T = T_ref, velocity from an inlet patch (initialize_velocity_from_bc)
     launch_fill(F.T, nc, P.T_ref);
     double u0[3] = {0, 0, 0};
@@ -2745,6 +2764,7 @@ int dpm_setup_times(const dpm_solver_t* h, double* ms) {
   ms[2] = s.setup_upload_ms;
   ms[3] = s.setup_total_ms;
   for (int k = 0; k < 7; ++k) ms[4 + k] = s.setup_t.stage_ms[k];
+  ms[11] = s.setup_psolver_ms;
   return DPM_OK;
 }
 

@@ -14,28 +14,53 @@ struct Csr {
   std::vector<double> val;
 };
 
+// Rows are independent: counted in parallel, then filled in parallel at their prefix offsets.
 Csr csr_from_ell(int n, int WA, const int* col, const double* val) {
   Csr A;
   A.n = n;
   A.off.assign(n + 1, 0);
-  std::vector<std::pair<int, double>> row;
-  for (int i = 0; i < n; ++i) {
-    row.clear();
+  auto row_entries = [&](int i, int* cj, double* vj) {  // sorted, equal columns summed
+    int m = 0;
     for (int s = 0; s < WA; ++s) {
       const int j = col[(size_t)s * n + i];
       const double v = val[(size_t)s * n + i];
-      if (j == i || v != 0.0) row.emplace_back(j, v);
+      if (!(j == i || v != 0.0)) continue;
+      int t = m++;
+      while (t > 0 && cj[t - 1] > j) { cj[t] = cj[t - 1]; vj[t] = vj[t - 1]; --t; }  // stable
+      cj[t] = j;
+      vj[t] = v;
     }
-    std::sort(row.begin(), row.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
-    for (size_t k = 0; k < row.size(); ++k) {
-      if (k > 0 && row[k].first == row[k - 1].first) {  // padding slots share the own column
-        A.val.back() += row[k].second;
+    int u = 0;
+    for (int k = 0; k < m; ++k) {
+      if (u > 0 && cj[u - 1] == cj[k]) {  // padding slots share the own column
+        vj[u - 1] += vj[k];
         continue;
       }
-      A.col.push_back(row[k].first);
-      A.val.push_back(row[k].second);
+      cj[u] = cj[k];
+      vj[u] = vj[k];
+      ++u;
     }
-    A.off[i + 1] = (int64_t)A.col.size();
+    return u;
+  };
+  std::vector<int> cnt(n);
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < n; ++i) {
+    int cj[64];
+    double vj[64];
+    cnt[i] = row_entries(i, cj, vj);
+  }
+  for (int i = 0; i < n; ++i) A.off[i + 1] = A.off[i] + cnt[i];
+  A.col.resize(A.off[n]);
+  A.val.resize(A.off[n]);
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < n; ++i) {
+    int cj[64];
+    double vj[64];
+    const int u = row_entries(i, cj, vj);
+    for (int k = 0; k < u; ++k) {
+      A.col[A.off[i] + k] = cj[k];
+      A.val[A.off[i] + k] = vj[k];
+    }
   }
   return A;
 }
@@ -114,10 +139,9 @@ Csr galerkin(const Csr& A, const std::vector<int>& agg, int na) {
   Csr C;
   C.n = na;
   C.off.assign(na + 1, 0);
-  std::vector<int64_t> pos(na, -1);
-  std::vector<int> cols;
-  std::vector<double> vals;
-  for (int a = 0; a < na; ++a) {
+  // one aggregate's row: columns in order of first appearance, summed, then sorted by column
+  auto agg_row = [&](int a, std::vector<int64_t>& pos, std::vector<int>& cols, std::vector<double>& vals,
+                     std::vector<int>& order) {
     cols.clear();
     vals.clear();
     for (int64_t m = moff[a]; m < moff[a + 1]; ++m) {
@@ -132,37 +156,75 @@ Csr galerkin(const Csr& A, const std::vector<int>& agg, int na) {
         vals[pos[c]] += A.val[k];
       }
     }
-    std::vector<int> order(cols.size());
+    order.resize(cols.size());
     for (size_t k = 0; k < order.size(); ++k) order[k] = (int)k;
     std::sort(order.begin(), order.end(), [&](int x, int y) { return cols[x] < cols[y]; });
-    for (int k : order) {
-      C.col.push_back(cols[k]);
-      C.val.push_back(vals[k]);
-      pos[cols[k]] = -1;
+    for (int c : cols) pos[c] = -1;
+  };
+  std::vector<int64_t> cnt(na);
+#pragma omp parallel
+  {
+    std::vector<int64_t> pos(na, -1);
+    std::vector<int> cols, order;
+    std::vector<double> vals;
+#pragma omp for schedule(static)
+    for (int a = 0; a < na; ++a) {
+      agg_row(a, pos, cols, vals, order);
+      cnt[a] = (int64_t)cols.size();
     }
-    C.off[a + 1] = (int64_t)C.col.size();
+  }
+  for (int a = 0; a < na; ++a) C.off[a + 1] = C.off[a] + cnt[a];
+  C.col.resize(C.off[na]);
+  C.val.resize(C.off[na]);
+#pragma omp parallel
+  {
+    std::vector<int64_t> pos(na, -1);
+    std::vector<int> cols, order;
+    std::vector<double> vals;
+#pragma omp for schedule(static)
+    for (int a = 0; a < na; ++a) {
+      agg_row(a, pos, cols, vals, order);
+      int64_t o = C.off[a];
+      for (int k : order) {
+        C.col[o] = cols[k];
+        C.val[o] = vals[k];
+        ++o;
+      }
+    }
   }
   return C;
 }
 
-// Largest eigenvalue of D^-1 A by 30 power steps from a fixed start vector.
+// Largest eigenvalue of D^-1 A by 30 power steps from a fixed start vector.  The norms are summed
+// over fixed chunks of rows, then the chunks in order: the same value on any number of threads.
 double lambda_max(const Csr& A, const std::vector<double>& dinv) {
-  std::vector<double> v(A.n), w(A.n);
-  for (int i = 0; i < A.n; ++i) v[i] = 1.0 + 0.5 * std::sin(0.7 * i + 0.3);
+  constexpr int CH = 16384;
+  const int n = A.n, nch = (n + CH - 1) / CH;
+  std::vector<double> v(n), w(n), pv(nch), pw(nch);
+  for (int i = 0; i < n; ++i) v[i] = 1.0 + 0.5 * std::sin(0.7 * i + 0.3);
   double lam = 0.0;
   for (int it = 0; it < 30; ++it) {
-    double nv = 0.0, nw = 0.0;
-    for (int i = 0; i < A.n; ++i) {
-      double s = 0.0;
-      for (int64_t k = A.off[i]; k < A.off[i + 1]; ++k) s += A.val[k] * v[A.col[k]];
-      w[i] = dinv[i] * s;
-      nv += v[i] * v[i];
-      nw += w[i] * w[i];
+#pragma omp parallel for schedule(static)
+    for (int c = 0; c < nch; ++c) {
+      double nv = 0.0, nw = 0.0;
+      const int i1 = std::min(n, (c + 1) * CH);
+      for (int i = c * CH; i < i1; ++i) {
+        double s = 0.0;
+        for (int64_t k = A.off[i]; k < A.off[i + 1]; ++k) s += A.val[k] * v[A.col[k]];
+        w[i] = dinv[i] * s;
+        nv += v[i] * v[i];
+        nw += w[i] * w[i];
+      }
+      pv[c] = nv;
+      pw[c] = nw;
     }
+    double nv = 0.0, nw = 0.0;
+    for (int c = 0; c < nch; ++c) { nv += pv[c]; nw += pw[c]; }
     if (!(nw > 0.0)) return 1.0;
     lam = std::sqrt(nw / nv);
     const double sc = 1.0 / std::sqrt(nw);
-    for (int i = 0; i < A.n; ++i) v[i] = w[i] * sc;
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n; ++i) v[i] = w[i] * sc;
   }
   return lam;
 }
@@ -248,14 +310,17 @@ MlLevel make_level(const Csr& A, const std::vector<int>& agg, int na, int& rc) {
   for (int i = 0; i < A.n; ++i) L.W = std::max<int>(L.W, (int)(A.off[i + 1] - A.off[i]));
   L.dinv.resize(A.n);
   std::vector<double> dinv(A.n, 0.0);
+  int bad = 0;
+#pragma omp parallel for schedule(static) reduction(| : bad)
   for (int i = 0; i < A.n; ++i) {
     double dg = 0.0;
     for (int64_t k = A.off[i]; k < A.off[i + 1]; ++k)
       if (A.col[k] == i) dg = A.val[k];
-    if (!(dg > 0.0)) rc = -5;
+    if (!(dg > 0.0)) bad = 1;
     dinv[i] = dg > 0.0 ? 1.0 / dg : 0.0;
     L.dinv[i] = (float)dinv[i];
   }
+  if (bad) rc = -5;
   L.lmax = lambda_max(A, dinv);
   // scaled off-diagonal form of the smoother
   for (int i = 0; i < A.n; ++i) L.Wo = std::max<int>(L.Wo, (int)(A.off[i + 1] - A.off[i]) - 1);
@@ -266,6 +331,7 @@ MlLevel make_level(const Csr& A, const std::vector<int>& agg, int na, int& rc) {
   L.g32.resize(A.n);
   L.g16.resize(A.n);
   L.diag.resize(A.n);
+#pragma omp parallel for schedule(static)
   for (int i = 0; i < A.n; ++i) {
     int s = 0;
     double d32 = 1.0, d16 = 1.0;
@@ -301,7 +367,7 @@ MlLevel make_level(const Csr& A, const std::vector<int>& agg, int na, int& rc) {
 
 int build_multilevel(int n, int WA, const int* A_col, const double* A_val, bool nullsp, int passes, double beta,
                      int ncoarse, int max_dense, Multilevel& M) {
-  if (n < 1 || WA < 1 || passes < 1 || ncoarse < 1) return -1;
+  if (n < 1 || WA < 1 || WA > 64 || passes < 1 || ncoarse < 1) return -1;
   M = Multilevel{};
   Csr A = csr_from_ell(n, WA, A_col, A_val);
   for (;;) {
@@ -312,14 +378,17 @@ int build_multilevel(int n, int WA, const int* A_col, const double* A_val, bool 
       if (A.n > max_dense) return -3;
       break;
     }
-    std::vector<int> agg_tot(A.n);
-    for (int i = 0; i < A.n; ++i) agg_tot[i] = i;
-    Csr Ac = A;
+    std::vector<int> agg_tot;
+    Csr Ac;
     for (int p = 0; p < passes; ++p) {
       std::vector<int> agg;
-      const int na = pairwise(Ac, beta, agg);
-      Ac = galerkin(Ac, agg, na);
-      for (int i = 0; i < A.n; ++i) agg_tot[i] = agg[agg_tot[i]];
+      const Csr& from = p == 0 ? A : Ac;
+      const int na = pairwise(from, beta, agg);
+      Csr next = galerkin(from, agg, na);
+      if (p == 0) agg_tot = agg;
+      else
+        for (int i = 0; i < A.n; ++i) agg_tot[i] = agg[agg_tot[i]];
+      Ac = std::move(next);
     }
     if (Ac.n > 0.85 * A.n) {  // coarsening stalled: solve this level directly if it is small enough
       if (A.n > max_dense) return -2;

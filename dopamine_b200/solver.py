@@ -148,7 +148,7 @@ class Solver:
         L.dpm_cell_geometry(self.h, _p(self.centroid), _p(self.volume))
 
     SETUP_KEYS = ("mesh_ms", "ops_ms", "upload_ms", "total_ms", "raw_upload_ms", "match_ms", "faces_ms",
-                  "periodic_ms", "stencil_ms", "pressure_ops_ms", "cell_ops_ms")
+                  "periodic_ms", "stencil_ms", "pressure_ops_ms", "cell_ops_ms", "psolver_ms")
 
     def setup_times(self):
         """Wall-clock milliseconds of this handle's set-up (dpm_setup_times)."""

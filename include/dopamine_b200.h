@@ -354,11 +354,11 @@ int dpm_set_time(dpm_solver_t* s, double time);
 int dpm_last_timing(const dpm_solver_t* s, double* step_ms, double* poisson_ms);
 /* Kernel launch count since the handle was created (own kernels only). */
 int dpm_kernel_launches(const dpm_solver_t* s, int64_t* n);
-/* Wall-clock milliseconds of the handle's set-up: ms[0] mesh (connectivity, geometry, periodic
- * pairs, LS stencil), ms[1] static operators, ms[2] upload and solver state, ms[3] total of
- * dpm_create; ms[4..10] the device builder's stages (raw upload, cells and face matching, faces and
- * cell lists, periodic pairing on the host, LS stencil, pressure operators, LS/cell operators and
- * download), zero with host_setup. */
+/* Wall-clock milliseconds of the handle's set-up (12 values): ms[0] mesh (connectivity, geometry,
+ * periodic pairs, LS stencil), ms[1] static operators, ms[2] upload and solver state, ms[3] total
+ * of dpm_create; ms[4..10] the device builder's stages (raw upload, cells and face matching, faces
+ * and cell lists, periodic pairing on the host, LS stencil, pressure operators, LS/cell operators),
+ * zero with host_setup; ms[11] the pressure-solver hierarchy (part of ms[2]). */
 int dpm_setup_times(const dpm_solver_t* s, double* ms);
 /* Builds the mesh and static operators of one configuration with both builders and compares
  * them entry by entry.  mismatches[k] (k < DPM_SETUP_N_ARRAYS, named by dpm_setup_array_name)
