@@ -376,10 +376,17 @@ def run_gpu(args, rank, world):
         plain = dict(ms_per_step=sum(pm) / len(pm), poisson_ms_per_step=sum(pp) / len(pp),
                      pcg_iterations_per_step=pit / len(pm), steps=len(pm))
         s.select_pressure_solver(3)
+    phases = None
+    if args.fcg_phases and args.psolver == "fcg":
+        # diagnostics after the timed region: where an iteration of the two-level kernel goes
+        s.fcg_phase_times(True)
+        for _ in range(2):
+            s.advance()
+        phases = s.fcg_phase_times(False)
     return dict(nc=nc, t_dev=t_dev, t_e2e=t_e2e, step_ms=step_ms, pois_ms=pois_ms, its=its, solves=solves,
                 bytes_it=bytes_it,
                 launches=launches, clocks=clocks, solver=s, learn=learn, fallbacks=s.stats()["p_fallbacks"],
-                e2e_bytes=bytes_per_dir, plain=plain, setup=s.setup_times())
+                e2e_bytes=bytes_per_dir, plain=plain, setup=s.setup_times(), phases=phases)
 
 
 def main():
@@ -400,6 +407,8 @@ def main():
     ap.add_argument("--mixed", action="store_true",
                     help="precision form: FP32 gradients, SGS and flux assembly; with the two-level form also "
                          "FP32-operator inner iterations inside FP64 defect correction")
+    ap.add_argument("--fcg-phases", action="store_true",
+                    help="after the timed region, record the two-level kernel's phase times for 2 steps")
     ap.add_argument("--psolver", default="auto", choices=["auto", "pcg", "fcg", "ml"],
                     help="auto: fcg when the mesh fits the two-level kernel, else ml; pcg: plain FP64 "
                          "Jacobi-PCG; fcg: flexible CG, two-level part-local preconditioner; "
@@ -480,6 +489,9 @@ def main():
         line["config"]["fallbacks_to_plain_pcg"] = r["fallbacks"]
     # handle creation (device mesh and static-operator set-up, upload, pressure-solver set-up); not timed
     line["config"]["setup_ms"] = {k: round(v, 1) for k, v in r["setup"].items()}
+    if r["phases"] is not None:
+        line["config"]["fcg_phase_us_per_iteration"] = {k: (round(v, 3) if isinstance(v, float) else v)
+                                                        for k, v in r["phases"].items()}
     if r["plain"] is not None:
         pl = r["plain"]
         pl["speedup_of_this_form"] = pl["ms_per_step"] / line["ms_per_step"]

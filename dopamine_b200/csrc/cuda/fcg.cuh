@@ -72,7 +72,17 @@ struct FcgArgs {
   const float* val32;
   float* zs32;
   double inner_rel;
+  // diagnostics: non-null = block 0 adds the globaltimer nanoseconds of each phase of an iteration
+  // to phase[0..5] (coarse values, smoother, z published + barrier, w = A z and the sums, reduce and
+  // gather, update) and counts the iterations in phase[7]
+  double* phase;
 };
+
+__device__ __forceinline__ unsigned long long fcg_clock() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 
 // Bounded grid barrier on the same monotonic counter as grid_allreduce (one arrival per block).
 __device__ __forceinline__ bool grid_barrier(unsigned* bar, unsigned& gen, int* status) {
@@ -293,8 +303,20 @@ __global__ void __launch_bounds__(FCG_TPB, 1) k_fcg(FcgArgs a, int WA) {
   double dp_mark = dp;
   const float th = a.theta, de = a.delta;
   const float sig = th / de;
+  const bool timed = a.phase != nullptr && blockIdx.x == 0 && threadIdx.x == 0;
+  unsigned long long tph = 0;
+#define FCG_PHASE(k)                                    \
+  if (timed) {                                          \
+    const unsigned long long t_ = fcg_clock();          \
+    a.phase[k] += (double)(t_ - tph);                   \
+    tph = t_;                                           \
+  }
   while (!reason) {
     if (its >= a.maxit) { reason = -3; break; }
+    if (timed) {
+      tph = fcg_clock();
+      a.phase[7] += 1.0;
+    }
     __syncthreads();  // s_c complete
     // ---- coarse values y = E^-1 c of this part and its neighbour parts (warp w: slot w)
     {
@@ -307,6 +329,7 @@ __global__ void __launch_bounds__(FCG_TPB, 1) k_fcg(FcgArgs a, int WA) {
       }
     }
     __syncthreads();
+    FCG_PHASE(0)
     const double yb = s_yn[0];
     // ---- part-local Chebyshev on D^-1 A_bb z = D^-1 r (FP32, shared memory).  With the
     // scaled residual s = D^-1 (r - A_bb z):  z += d;  s -= D^-1 A_bb d = d + sum a~_ij d_j;
@@ -368,6 +391,7 @@ __global__ void __launch_bounds__(FCG_TPB, 1) k_fcg(FcgArgs a, int WA) {
       float* t = dcur; dcur = dnext; dnext = t;
     }
     __syncthreads();
+    FCG_PHASE(1)
     // ---- z to global, barrier, w = A z and the sums
     double rz[CPT];
 #pragma unroll
@@ -385,6 +409,7 @@ __global__ void __launch_bounds__(FCG_TPB, 1) k_fcg(FcgArgs a, int WA) {
       }
     }
     if (!grid_barrier(a.bar, gen, a.status)) return;
+    FCG_PHASE(2)
     double v[FCG_NV + FCG_NG], t[FCG_NV];
 #pragma unroll
     for (int k = 0; k < FCG_NV + FCG_NG; ++k) v[k] = 0.0;
@@ -409,7 +434,9 @@ __global__ void __launch_bounds__(FCG_TPB, 1) k_fcg(FcgArgs a, int WA) {
         v[10] += qk;
       }
     }
+    FCG_PHASE(3)
     if (!grid_reduce_gather<FCG_NV, FCG_NG>(v, a.partials, a.bar, gen, a.status, t, s_gat)) return;
+    FCG_PHASE(4)
     dp = sqrt(t[4]);
     reason = classify(dp, ttol, a.atol, rnorm0);
     if (reason) break;
@@ -437,8 +464,10 @@ __global__ void __launch_bounds__(FCG_TPB, 1) k_fcg(FcgArgs a, int WA) {
     for (int j = threadIdx.x; j < P; j += blockDim.x)
       s_c[j] = s_gat[j] - al * (s_gat[P + j] + beta * s_gat[2 * P + j]);
     pq_old = pq;
+    FCG_PHASE(5)
     ++its;
   }
+#undef FCG_PHASE
   // ---- write back x (original numbering) and the true residual ||b - A x||
   double v1[1] = {0.0}, t1[1];
 #pragma unroll

@@ -271,6 +271,7 @@ struct Solver {
   int spin_limit = 0;  // > 0: poll limit of the Krylov kernels' grid-wide waits (failure-detection tests)
   bool force_plain = false;  // dpm_select_pressure_solver: plain Jacobi-PCG although a flexible form is set up
   SetupTimes setup_t;        // set-up stage times of init
+  double* fcg_phase = nullptr;  // dpm_fcg_phase_times: per-phase ns of the two-level kernel, [8]
   double setup_upload_ms = 0.0, setup_total_ms = 0.0, setup_psolver_ms = 0.0;
   bool flexible() const { return (use_fcg || use_ml) && !force_plain; }
 
@@ -1280,6 +1281,7 @@ struct Solver {
                  double* resid, int* reason, double inner_rel) {
     FcgArgs a = fa;
     a.inner_rel = inner_rel;
+    a.phase = fcg_phase;
     a.b = rhs; a.x = x; a.rtol = rtol; a.atol = atol; a.maxit = maxit; a.guess_zero = guess_zero;
     a.gamma = lp_ready ? lp_gamma : 0.0f;
     const bool rec = lp_recording && lp_count < lp_S && inner_rel_is_first_;
@@ -2753,6 +2755,33 @@ int dpm_last_timing(const dpm_solver_t* h, double* step_ms, double* poisson_ms) 
 int dpm_kernel_launches(const dpm_solver_t* h, int64_t* n) {
   if (!h || !n) return DPM_ERR_ARG;
   *n = h->s->launches;
+  return DPM_OK;
+}
+
+int dpm_fcg_phase_times(dpm_solver_t* h, int enable, double* us) {
+  if (!h) return DPM_ERR_ARG;
+  Solver& s = *h->s;
+  CK(cudaSetDevice(s.device));
+  if (us) {
+    double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    if (s.fcg_phase) {
+      CK(cudaStreamSynchronize(s.st));
+      CK(cudaMemcpy(v, s.fcg_phase, sizeof(v), cudaMemcpyDeviceToHost));
+    }
+    const double n = v[7] > 0.0 ? v[7] : 1.0;
+    for (int k = 0; k < 6; ++k) us[k] = v[k] / n * 1e-3;
+    us[6] = 0.0;
+    us[7] = v[7];
+  }
+  if (enable) {
+    if (!s.fcg_phase) {
+      s.fcg_phase = s.mem.alloc<double>(8);
+      if (!s.fcg_phase) return DPM_ERR_CUDA;
+    }
+    CK(cudaMemsetAsync(s.fcg_phase, 0, 8 * sizeof(double), s.st));
+  } else {
+    s.fcg_phase = nullptr;  // the buffer stays with the handle's allocations
+  }
   return DPM_OK;
 }
 

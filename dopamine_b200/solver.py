@@ -31,7 +31,7 @@ EXPORTED = (
     "dpm_write_checkpoint", "dpm_read_checkpoint", "dpm_sampling_set_points", "dpm_sample_points",
     "dpm_set_nudging_profiles", "dpm_set_scalar_sources", "dpm_setup_times", "dpm_setup_compare",
     "dpm_setup_array_name", "dpm_gmsh_read", "dpm_gmsh_sizes", "dpm_gmsh_fill", "dpm_gmsh_patch_name",
-    "dpm_gmsh_free", "dpm_gmsh_write",
+    "dpm_gmsh_free", "dpm_gmsh_write", "dpm_fcg_phase_times",
 )
 
 
@@ -110,6 +110,7 @@ def lib(build_if_missing=True):
     L.dpm_pcg_solve_noalloc.argtypes = [C.c_int, C.c_int, vp, vp, vp, vp, vp, C.c_double, C.c_double, C.c_int,
                                         C.c_int, vp, ip, dp]
     L.dpm_setup_times.argtypes = [vp, dp]
+    L.dpm_fcg_phase_times.argtypes = [vp, C.c_int, dp]
     L.dpm_setup_compare.argtypes = [C.POINTER(abi.RawMeshT), C.POINTER(abi.PatchCfgT), C.POINTER(abi.ParamsT),
                                     C.c_int, C.POINTER(C.c_int64), dp, dp]
     L.dpm_setup_array_name.argtypes = [C.c_int]
@@ -155,6 +156,17 @@ class Solver:
         ms = np.zeros(len(self.SETUP_KEYS))
         _check(lib().dpm_setup_times(self.h, _p(ms)), "dpm_setup_times")
         return dict(zip(self.SETUP_KEYS, ms.tolist()))
+
+    FCG_PHASES = ("coarse", "smoother", "publish_z_barrier", "w_Az_sums", "reduce_gather", "update")
+
+    def fcg_phase_times(self, enable=True):
+        """Two-level kernel phase times recorded since the last call (mean us per iteration by
+        phase, and the iteration count); enable=False stops the recording."""
+        us = np.zeros(8)
+        _check(lib().dpm_fcg_phase_times(self.h, 1 if enable else 0, _p(us)), "dpm_fcg_phase_times")
+        out = dict(zip(self.FCG_PHASES, us[:6].tolist()))
+        out["iterations"] = int(us[7])
+        return out
 
     def close(self):
         if getattr(self, "h", None):

@@ -360,6 +360,12 @@ int dpm_kernel_launches(const dpm_solver_t* s, int64_t* n);
  * and cell lists, periodic pairing on the host, LS stencil, pressure operators, LS/cell operators),
  * zero with host_setup; ms[11] the pressure-solver hierarchy (part of ms[2]). */
 int dpm_setup_times(const dpm_solver_t* s, double* ms);
+/* Phase times of the two-level flexible-CG kernel (diagnostics).  us (may be NULL) receives what
+ * was recorded since the last call: us[0..5] the mean microseconds per iteration that block 0
+ * spends in the coarse values, the part-local smoother, publishing z plus the grid barrier,
+ * w = A z with the sums, the reduce-and-gather, and the update; us[7] the iterations counted.
+ * enable = 1 (re)starts the recording (one globaltimer read per phase in one thread), 0 stops it. */
+int dpm_fcg_phase_times(dpm_solver_t* s, int enable, double* us);
 /* Builds the mesh and static operators of one configuration with both builders and compares
  * them entry by entry.  mismatches[k] (k < DPM_SETUP_N_ARRAYS, named by dpm_setup_array_name)
  * counts the entries of array k whose bits differ, the SGS filter tensor excepted: its scale is a
