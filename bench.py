@@ -287,6 +287,8 @@ def run_gpu(args, rank, world):
         case.params["p_ml_value_bits"] = args.ml_value_bits
     if args.ml_degree:
         case.params["p_ml_degree"] = args.ml_degree
+    if args.fcg_degree:
+        case.params["p_smooth_degree"] = args.fcg_degree
     s = Solver(case, device=dev)
     s.initialise()
     nc = s.nc
@@ -407,6 +409,8 @@ def main():
     ap.add_argument("--mixed", action="store_true",
                     help="precision form: FP32 gradients, SGS and flux assembly; with the two-level form also "
                          "FP32-operator inner iterations inside FP64 defect correction")
+    ap.add_argument("--fcg-degree", type=int, default=0,
+                    help="Chebyshev degree of the two-level form's part-local smoother (0: library default 7)")
     ap.add_argument("--fcg-phases", action="store_true",
                     help="after the timed region, record the two-level kernel's phase times for 2 steps")
     ap.add_argument("--psolver", default="auto", choices=["auto", "pcg", "fcg", "ml"],
