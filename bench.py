@@ -8,10 +8,12 @@ one passive scalar (van Leer), synthetic inputs (seeded uniform flow with +-10 %
 "step" is one RK3W time step (three stages, three Poisson solves) of the whole mesh.  The timed
 form is the chosen pressure solve (flexible CG with the two-level preconditioner when the mesh
 fits it, else with the FP32 aggregation-multigrid V-cycle; the learned term trained on 3
-recorded steps and gated on a held-out solve); on one GPU the plain FP64 Jacobi-PCG form is timed
-beside it on the same handle, mesh and state and reported in the config.
+recorded steps and gated on a held-out solve) in the precision form (FP32 explicit half: first
+gradient pass, SGS and flux assembly; FP64 state and projection; `--fp64` for the FP64 explicit
+half); on one GPU the plain FP64 Jacobi-PCG form is timed beside it on the same handle, mesh and
+state and reported in the config.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--fp64]
                     [--config urban|channel|channel3m|tgv|rb|mixed] [--psolver auto|fcg|pcg|ml] [--no-plain]
 
 value   : cell-steps/s with the state resident in HBM (CUDA events around K steps, max over ranks)
@@ -406,9 +408,11 @@ def main():
                     help="multilevel form: Chebyshev steps per smoothing (0: library default, 3)")
     ap.add_argument("--ml-value-bits", type=int, default=0, choices=[0, 16, 32],
                     help="multilevel form: storage of the smoother's scaled off-diagonals (0: library default, 16)")
-    ap.add_argument("--mixed", action="store_true",
-                    help="precision form: FP32 gradients, SGS and flux assembly; with the two-level form also "
-                         "FP32-operator inner iterations inside FP64 defect correction")
+    ap.add_argument("--mixed", action="store_true", default=True,
+                    help="precision form (the default: the metric is learned+mixed): FP32 gradients, SGS and flux "
+                         "assembly; with the two-level form also FP32-operator inner iterations inside FP64 defect "
+                         "correction")
+    ap.add_argument("--fp64", action="store_true", help="the FP64 explicit half instead of the precision form")
     ap.add_argument("--fcg-degree", type=int, default=0,
                     help="Chebyshev degree of the two-level form's part-local smoother (0: library default 7)")
     ap.add_argument("--fcg-phases", action="store_true",
@@ -418,6 +422,8 @@ def main():
                          "Jacobi-PCG; fcg: flexible CG, two-level part-local preconditioner; "
                          "ml: flexible CG, aggregation-multigrid V-cycle")
     args = ap.parse_args()
+    if args.fp64:
+        args.mixed = False
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -465,7 +471,7 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world, "steps": K,
         "warmup": args.warmup, "ms_per_step": 1e3 * r["t_dev"] / K, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "vs_baseline": None, "dtype": "f64+f32" if args.mixed else "f64", "data": "synthetic",
         "config": {"workload": cfg_name, "cells": nc, "form": FORMS[args.psolver],
                    "poisson_ms_per_step": 1e3 * pois_s / K, "pcg_iterations_per_step": r["its"] / K,
                    "poisson_solves_per_step": r["solves"] / K,
