@@ -47,6 +47,7 @@ struct LsScalarSet32 {
   const double* pb[LS_SET];
   float* g[LS_SET];
 };
+constexpr int LS32_CHUNK = 2;  // stencil slots gathered together by k_ls32_gradient_all
 template <int NS>
 __global__ void __launch_bounds__(TPB) k_ls32_gradient_all(Dev d, Geo32 g, const double* __restrict__ U,
                                                            const double* __restrict__ Ub, float* __restrict__ gU,
@@ -63,39 +64,54 @@ __global__ void __launch_bounds__(TPB) k_ls32_gradient_all(Dev d, Geo32 g, const
     pc[k] = q.phi[k][c];
     a0[k] = a1[k] = a2[k] = 0.0f;
   }
-  for (int s = 0; s < W; ++s) {
-    int v = __ldg(&d.ls_idx[s * nc + c]);
-    if (v == PADI) break;
-    const float w0 = __ldg(&g.ls_w[(0 * W + s) * nc + c]);
-    const float w1 = __ldg(&g.ls_w[(1 * W + s) * nc + c]);
-    const float w2 = __ldg(&g.ls_w[(2 * W + s) * nc + c]);
-    double un0, un1, un2, pv[NS > 0 ? NS : 1];
-    if (v >= 0) {
-      un0 = U[v]; un1 = U[nc + v]; un2 = U[2 * nc + v];
+  // LS32_CHUNK slots at a time: all their loads are issued before the sums (slot order kept)
+  constexpr int CH = LS32_CHUNK;
+  for (int s0 = 0; s0 < W; s0 += CH) {
+    int v[CH];
 #pragma unroll
-      for (int k = 0; k < NS; ++k) pv[k] = q.phi[k][v];
-    } else {
-      int b = -v - 1;
-      if (b < nb) {
-        un0 = Ub[b]; un1 = Ub[nb + b]; un2 = Ub[2 * nb + b];
+    for (int u = 0; u < CH; ++u) v[u] = s0 + u < W ? __ldg(&d.ls_idx[(s0 + u) * nc + c]) : PADI;
+    if (v[0] == PADI) break;
+    float w0[CH], w1[CH], w2[CH];
+    double un0[CH], un1[CH], un2[CH], pv[CH][NS > 0 ? NS : 1];
 #pragma unroll
-        for (int k = 0; k < NS; ++k) pv[k] = q.pb[k][b];
+    for (int u = 0; u < CH; ++u) {
+      const int s = s0 + u;
+      const bool on = v[u] != PADI;
+      w0[u] = on ? __ldg(&g.ls_w[(0 * W + s) * nc + c]) : 0.0f;
+      w1[u] = on ? __ldg(&g.ls_w[(1 * W + s) * nc + c]) : 0.0f;
+      w2[u] = on ? __ldg(&g.ls_w[(2 * W + s) * nc + c]) : 0.0f;
+      const int vv = v[u];
+      if (vv >= 0) {
+        un0[u] = U[vv]; un1[u] = U[nc + vv]; un2[u] = U[2 * nc + vv];
+#pragma unroll
+        for (int k = 0; k < NS; ++k) pv[u][k] = q.phi[k][vv];
       } else {
-        un0 = uc0; un1 = uc1; un2 = uc2;
+        const int b = on ? -vv - 1 : nb;  // a padding slot reads nothing
+        if (b < nb) {
+          un0[u] = Ub[b]; un1[u] = Ub[nb + b]; un2[u] = Ub[2 * nb + b];
 #pragma unroll
-        for (int k = 0; k < NS; ++k) pv[k] = pc[k];
+          for (int k = 0; k < NS; ++k) pv[u][k] = q.pb[k][b];
+        } else {
+          un0[u] = uc0; un1[u] = uc1; un2[u] = uc2;
+#pragma unroll
+          for (int k = 0; k < NS; ++k) pv[u][k] = pc[k];
+        }
       }
     }
-    const float du0 = (float)(un0 - uc0), du1 = (float)(un1 - uc1), du2 = (float)(un2 - uc2);
-    a[0] = fmaf(w0, du0, a[0]); a[1] = fmaf(w1, du0, a[1]); a[2] = fmaf(w2, du0, a[2]);
-    a[3] = fmaf(w0, du1, a[3]); a[4] = fmaf(w1, du1, a[4]); a[5] = fmaf(w2, du1, a[5]);
-    a[6] = fmaf(w0, du2, a[6]); a[7] = fmaf(w1, du2, a[7]); a[8] = fmaf(w2, du2, a[8]);
 #pragma unroll
-    for (int k = 0; k < NS; ++k) {
-      const float dd = (float)(pv[k] - pc[k]);
-      a0[k] = fmaf(w0, dd, a0[k]);
-      a1[k] = fmaf(w1, dd, a1[k]);
-      a2[k] = fmaf(w2, dd, a2[k]);
+    for (int u = 0; u < CH; ++u) {
+      if (v[u] == PADI) break;
+      const float du0 = (float)(un0[u] - uc0), du1 = (float)(un1[u] - uc1), du2 = (float)(un2[u] - uc2);
+      a[0] = fmaf(w0[u], du0, a[0]); a[1] = fmaf(w1[u], du0, a[1]); a[2] = fmaf(w2[u], du0, a[2]);
+      a[3] = fmaf(w0[u], du1, a[3]); a[4] = fmaf(w1[u], du1, a[4]); a[5] = fmaf(w2[u], du1, a[5]);
+      a[6] = fmaf(w0[u], du2, a[6]); a[7] = fmaf(w1[u], du2, a[7]); a[8] = fmaf(w2[u], du2, a[8]);
+#pragma unroll
+      for (int k = 0; k < NS; ++k) {
+        const float dd = (float)(pv[u][k] - pc[k]);
+        a0[k] = fmaf(w0[u], dd, a0[k]);
+        a1[k] = fmaf(w1[u], dd, a1[k]);
+        a2[k] = fmaf(w2[u], dd, a2[k]);
+      }
     }
   }
 #pragma unroll

@@ -229,6 +229,7 @@ __global__ void __launch_bounds__(TPB) k_ls_gradient_scalars(Dev d, LsScalarSet 
 // indices and weights (624 B per hex cell, the dominant traffic of both operators) are read once
 // instead of once per operator.  Each field's sums are formed exactly as in k_ls_gradient_vector
 // and k_ls_gradient_scalars (same stencil order, same products), so the results are the same.
+constexpr int LS_CHUNK = 2;  // stencil slots gathered together by the fused LS gradient kernels
 template <int NS>
 __global__ void __launch_bounds__(TPB) k_ls_gradient_all(Dev d, const double* __restrict__ U,
                                                          const double* __restrict__ Ub, double* __restrict__ gU,
@@ -244,39 +245,53 @@ __global__ void __launch_bounds__(TPB) k_ls_gradient_all(Dev d, const double* __
     pc[k] = q.phi[k][c];
     a0[k] = a1[k] = a2[k] = 0.0;
   }
-  for (int s = 0; s < W; ++s) {
-    int v = __ldg(&d.ls_idx[s * nc + c]);
-    if (v == PADI) break;
-    const double w0 = __ldg(&d.ls_w[(0 * W + s) * nc + c]);
-    const double w1 = __ldg(&d.ls_w[(1 * W + s) * nc + c]);
-    const double w2 = __ldg(&d.ls_w[(2 * W + s) * nc + c]);
-    double un0, un1, un2, pv[NS];
-    if (v >= 0) {
-      un0 = U[v]; un1 = U[nc + v]; un2 = U[2 * nc + v];
+  // LS_CHUNK slots at a time: their indices, weights and neighbour values are all requested
+  // before any is used (the gathers are the latency chain), then summed in slot order as before
+  for (int s0 = 0; s0 < W; s0 += LS_CHUNK) {
+    int v[LS_CHUNK];
 #pragma unroll
-      for (int k = 0; k < NS; ++k) pv[k] = q.phi[k][v];
-    } else {
-      int b = -v - 1;
-      if (b < nb) {
-        un0 = Ub[b]; un1 = Ub[nb + b]; un2 = Ub[2 * nb + b];
+    for (int u = 0; u < LS_CHUNK; ++u) v[u] = s0 + u < W ? __ldg(&d.ls_idx[(s0 + u) * nc + c]) : PADI;
+    if (v[0] == PADI) break;
+    double w0[LS_CHUNK], w1[LS_CHUNK], w2[LS_CHUNK], un0[LS_CHUNK], un1[LS_CHUNK], un2[LS_CHUNK], pv[LS_CHUNK][NS];
 #pragma unroll
-        for (int k = 0; k < NS; ++k) pv[k] = q.pb[k][b];
+    for (int u = 0; u < LS_CHUNK; ++u) {
+      const int s = s0 + u;
+      const bool on = v[u] != PADI;
+      w0[u] = on ? __ldg(&d.ls_w[(0 * W + s) * nc + c]) : 0.0;
+      w1[u] = on ? __ldg(&d.ls_w[(1 * W + s) * nc + c]) : 0.0;
+      w2[u] = on ? __ldg(&d.ls_w[(2 * W + s) * nc + c]) : 0.0;
+      const int vv = v[u];
+      if (vv >= 0) {
+        un0[u] = U[vv]; un1[u] = U[nc + vv]; un2[u] = U[2 * nc + vv];
+#pragma unroll
+        for (int k = 0; k < NS; ++k) pv[u][k] = q.phi[k][vv];
       } else {
-        un0 = uc0; un1 = uc1; un2 = uc2;
+        const int b = on ? -vv - 1 : nb;  // a padding slot reads nothing
+        if (b < nb) {
+          un0[u] = Ub[b]; un1[u] = Ub[nb + b]; un2[u] = Ub[2 * nb + b];
 #pragma unroll
-        for (int k = 0; k < NS; ++k) pv[k] = pc[k];
+          for (int k = 0; k < NS; ++k) pv[u][k] = q.pb[k][b];
+        } else {
+          un0[u] = uc0; un1[u] = uc1; un2[u] = uc2;
+#pragma unroll
+          for (int k = 0; k < NS; ++k) pv[u][k] = pc[k];
+        }
       }
     }
-    double du0 = un0 - uc0, du1 = un1 - uc1, du2 = un2 - uc2;
-    a[0] += w0 * du0; a[1] += w1 * du0; a[2] += w2 * du0;
-    a[3] += w0 * du1; a[4] += w1 * du1; a[5] += w2 * du1;
-    a[6] += w0 * du2; a[7] += w1 * du2; a[8] += w2 * du2;
 #pragma unroll
-    for (int k = 0; k < NS; ++k) {
-      double dd = pv[k] - pc[k];
-      a0[k] += w0 * dd;
-      a1[k] += w1 * dd;
-      a2[k] += w2 * dd;
+    for (int u = 0; u < LS_CHUNK; ++u) {
+      if (v[u] == PADI) break;
+      const double du0 = un0[u] - uc0, du1 = un1[u] - uc1, du2 = un2[u] - uc2;
+      a[0] += w0[u] * du0; a[1] += w1[u] * du0; a[2] += w2[u] * du0;
+      a[3] += w0[u] * du1; a[4] += w1[u] * du1; a[5] += w2[u] * du1;
+      a[6] += w0[u] * du2; a[7] += w1[u] * du2; a[8] += w2[u] * du2;
+#pragma unroll
+      for (int k = 0; k < NS; ++k) {
+        const double dd = pv[u][k] - pc[k];
+        a0[k] += w0[u] * dd;
+        a1[k] += w1[u] * dd;
+        a2[k] += w2[u] * dd;
+      }
     }
   }
 #pragma unroll
