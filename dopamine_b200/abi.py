@@ -43,6 +43,14 @@ class RawMeshT(C.Structure):
     ]
 
 
+class PolyMeshT(C.Structure):
+    _fields_ = [
+        ("n_points", C.c_int64), ("xyz", _dp), ("n_faces", C.c_int64), ("face_off", _lp), ("face_nodes", _ip),
+        ("owner", _ip), ("n_int_faces", C.c_int64), ("neighbour", _ip), ("n_patches", C.c_int),
+        ("patch_start", _lp), ("patch_nfaces", _lp),
+    ]
+
+
 class PatchCfgT(C.Structure):
     _fields_ = [
         ("bc_id", C.c_int), ("U_val", C.c_double * 3), ("p_val", C.c_double), ("T_val", C.c_double),
@@ -249,4 +257,26 @@ class RawMeshView:
             cell_off=_ptr(co, C.c_int64), cell_nodes=_ptr(cn, C.c_int), n_bfaces=bp.shape[0],
             bface_off=_ptr(bo, C.c_int64), bface_nodes=_ptr(bn, C.c_int), bface_patch=_ptr(bp, C.c_int),
             n_patches=len(mesh.patch_names),
+        )
+
+
+class PolyMeshView:
+    """Keeps the numpy buffers of a cases.PolyMesh alive while its C struct is in use."""
+
+    def __init__(self, mesh):
+        self._keep = [
+            np.ascontiguousarray(mesh.xyz, dtype=np.float64),
+            np.ascontiguousarray(mesh.face_off, dtype=np.int64),
+            np.ascontiguousarray(mesh.face_nodes, dtype=np.int32),
+            np.ascontiguousarray(mesh.owner, dtype=np.int32),
+            np.ascontiguousarray(mesh.neighbour, dtype=np.int32),
+            np.ascontiguousarray(mesh.patch_start, dtype=np.int64),
+            np.ascontiguousarray(mesh.patch_nfaces, dtype=np.int64),
+        ]
+        xyz, fo, fn, ow, nb, ps, pn = self._keep
+        self.struct = PolyMeshT(
+            n_points=xyz.shape[0], xyz=_ptr(xyz, C.c_double), n_faces=ow.shape[0], face_off=_ptr(fo, C.c_int64),
+            face_nodes=_ptr(fn, C.c_int), owner=_ptr(ow, C.c_int), n_int_faces=nb.shape[0],
+            neighbour=_ptr(nb, C.c_int), n_patches=len(mesh.patch_names), patch_start=_ptr(ps, C.c_int64),
+            patch_nfaces=_ptr(pn, C.c_int64),
         )

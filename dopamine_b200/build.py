@@ -18,7 +18,7 @@ CU_SOURCES = ["csrc/cuda/solver.cu", "csrc/cuda/fvm_petsc.cu", "csrc/cuda/noallo
 # The device set-up reproduces the host builder's rounding: no contraction into fused multiply-adds.
 CU_FLAGS = {"csrc/cuda/setup_gpu.cu": ["-fmad=false"]}
 CPP_SOURCES = ["csrc/host/mesh.cpp", "csrc/host/ops.cpp", "csrc/host/twolevel.cpp", "csrc/host/multilevel.cpp",
-               "csrc/host/gmsh.cpp"]
+               "csrc/host/gmsh.cpp", "csrc/host/foam.cpp"]
 HEADERS = ["csrc/cuda/common.cuh", "csrc/cuda/kernels.cuh", "csrc/cuda/pcg.cuh", "csrc/cuda/fcg.cuh",
            "csrc/cuda/learn.cuh", "csrc/cuda/scalars.cuh", "csrc/cuda/mlcg.cuh", "csrc/cuda/mlsolve.cuh", "csrc/cuda/mlkern.cuh", "csrc/cuda/explicit32.cuh",
            "csrc/cuda/setup_gpu.hpp", "csrc/cuda/cellproj.cuh", "csrc/cuda/sampling.cuh", "csrc/cuda/forcing.cuh", "csrc/cuda/sem.cuh", "csrc/host/fortran_records.hpp",

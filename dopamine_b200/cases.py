@@ -263,6 +263,28 @@ def _hex_nodes(n, i, j, k):
 _PATCHES6 = ("x0", "xL", "y0", "yL", "z0", "zL")
 
 
+@dataclass
+class PolyMesh:
+    """Face-based mesh as an OpenFOAM polyMesh holds it (dpm_create_poly): faces in the file's
+    order (internal faces first, owner < neighbour), then each patch's faces."""
+    xyz: np.ndarray            # (n_points, 3) float64
+    face_off: np.ndarray       # (n_faces+1,) int64
+    face_nodes: np.ndarray     # int32
+    owner: np.ndarray          # (n_faces,) int32
+    neighbour: np.ndarray      # (n_int_faces,) int32
+    patch_start: np.ndarray    # (n_patches,) int64, startFace
+    patch_nfaces: np.ndarray   # (n_patches,) int64
+    patch_names: list = field(default_factory=list)
+    patch_types: list = field(default_factory=list)
+
+    @property
+    def n_cells(self):
+        return int(max(self.owner.max(initial=-1), self.neighbour.max(initial=-1))) + 1
+
+    def vertex_bounds(self):
+        return self.xyz.min(axis=0), self.xyz.max(axis=0)
+
+
 def _assemble(xyz, cells, bfaces):
     """cells: [(type, [nodes])], bfaces: [(patch, [nodes])] -> RawMesh."""
     ct = np.array([c[0] for c in cells], dtype=np.int32)

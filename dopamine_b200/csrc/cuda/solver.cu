@@ -336,6 +336,46 @@ struct Solver {
     return rc;
   }
 
+  // Polyhedral mesh (dpm_create_poly): the host builds the mesh and the static operators.
+  int init_poly(const dpm_poly_mesh_t* pmsh, const dpm_patch_cfg_t* patches, const dpm_params_t* prm, int dev) {
+    device = dev;
+    CK(cudaSetDevice(device));
+    CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    CK(cudaEventCreate(&ev0)); CK(cudaEventCreate(&ev1)); CK(cudaEventCreate(&evp0)); CK(cudaEventCreate(&evp1));
+    PolyMesh pm;
+    pm.n_points = pmsh->n_points; pm.xyz = pmsh->xyz; pm.n_faces = pmsh->n_faces; pm.face_off = pmsh->face_off;
+    pm.face_nodes = pmsh->face_nodes; pm.owner = pmsh->owner; pm.n_int_faces = pmsh->n_int_faces;
+    pm.neighbour = pmsh->neighbour; pm.n_patches = pmsh->n_patches; pm.patch_start = pmsh->patch_start;
+    pm.patch_nfaces = pmsh->patch_nfaces;
+    std::vector<int> pbc(pmsh->n_patches);
+    for (int i = 0; i < pmsh->n_patches; ++i) pbc[i] = patches[i].bc_id;
+    using Clk = std::chrono::steady_clock;
+    auto ms_between = [](Clk::time_point a, Clk::time_point b) {
+      return std::chrono::duration<double, std::milli>(b - a).count();
+    };
+    const auto t_begin = Clk::now();
+    P = *prm;
+    if (P.cell_projection != DPM_CELL_PROJECTION_LS && P.cell_projection != DPM_CELL_PROJECTION_EXACT) return DPM_ERR_ARG;
+    cp_on = P.cell_projection == DPM_CELL_PROJECTION_EXACT;
+    pc.assign(patches, patches + pmsh->n_patches);
+    std::string err;
+    if (build_mesh_poly(pm, pbc.data(), m, &err)) {
+      std::fprintf(stderr, "dopamine_b200: polyhedral mesh set-up failed: %s\n", err.c_str());
+      return DPM_ERR_MESH;
+    }
+    const auto t_mesh = Clk::now();
+    if (build_static_ops(m, pc.data(), P, S)) return DPM_ERR_MESH;
+    setup_t.mesh_ms = ms_between(t_begin, t_mesh);
+    setup_t.ops_ms = ms_between(t_mesh, Clk::now());
+    if (m.n_cells > 2000000000LL || m.n_faces > 2000000000LL) return DPM_ERR_UNSUPPORTED;
+    nc = (int)m.n_cells; nf = (int)m.n_faces; nb = (int)m.n_bnd_faces; nfp = (int)S.nfp;
+    const auto t_up = Clk::now();
+    int rc = upload(nullptr);
+    setup_upload_ms = ms_between(t_up, Clk::now());
+    setup_total_ms = ms_between(t_begin, Clk::now());
+    return rc;
+  }
+
   template <class T>
   static std::vector<T> soa3(const std::vector<T>& aos, int64_t n) {
     std::vector<T> s(3 * n);
@@ -2474,6 +2514,21 @@ int dpm_create(const dpm_raw_mesh_t* mesh, const dpm_patch_cfg_t* patches, const
   auto* h = new dpm_solver();
   h->s = std::make_unique<Solver>();
   int rc = h->s->init(mesh, patches, params, device);
+  if (rc) {
+    delete h;
+    *out = nullptr;
+    return rc;
+  }
+  *out = h;
+  return DPM_OK;
+}
+
+int dpm_create_poly(const dpm_poly_mesh_t* mesh, const dpm_patch_cfg_t* patches, const dpm_params_t* params,
+                    int device, dpm_solver_t** out) {
+  if (!mesh || !patches || !params || !out) return DPM_ERR_ARG;
+  auto* h = new dpm_solver();
+  h->s = std::make_unique<Solver>();
+  int rc = h->s->init_poly(mesh, patches, params, device);
   if (rc) {
     delete h;
     *out = nullptr;

@@ -260,6 +260,178 @@ int build_periodic(Mesh& m, std::string* err) {
   return 0;
 }
 
+// The part of the set-up that both the element path (build_mesh) and the polyhedral path
+// (build_mesh_poly) share, once faces (owner, neighbour, patch, area, centre, normal), cells
+// (centroid, volume, vertex lists) and patches are in m: cell -> face lists, face metrics,
+// periodic pairing, LS stencil.
+int finish_mesh(Mesh& m, std::string* err) {
+  const int64_t nc = m.n_cells, nf = m.n_faces, nfi = m.n_int_faces, nfb = m.n_bnd_faces;
+  build_cell_faces(m);
+
+  // Face geometry (mod_mesh.f90:mesh_compute_geometry, mesh_tag_refinement_faces).
+  m.sf.assign(3 * nf, 0.0);
+  m.d_cf.assign(nf, 0.0);
+  m.gc.assign(nf, 0.0);
+  m.eps.assign(3 * nf, 0.0);
+  m.skew.assign(nf, 0.0);
+  m.is_refine.assign(nf, 0);
+#pragma omp parallel for schedule(static)
+  for (int64_t f = 0; f < nf; ++f) {
+    for (int k = 0; k < 3; ++k) m.sf[3 * f + k] = m.area[f] * m.normal[3 * f + k];
+    const double* co = &m.centroid[3 * (int64_t)m.owner[f]];
+    const double* ce = &m.centre[3 * f];
+    if (m.neighbour[f] >= 0) {
+      const double* cn = &m.centroid[3 * (int64_t)m.neighbour[f]];
+      double d_on[3], d_oc[3];
+      for (int k = 0; k < 3; ++k) { d_on[k] = cn[k] - co[k]; d_oc[k] = ce[k] - co[k]; }
+      double d_on2 = d_on[0] * d_on[0] + d_on[1] * d_on[1] + d_on[2] * d_on[2];
+      m.d_cf[f] = std::max(std::sqrt(d_on2), 1.0e-30);
+      double w = dot3(d_oc, d_on) / (d_on2 + SMALL);
+      m.gc[f] = std::max(0.0, std::min(1.0, 1.0 - w));
+      double em[3], s2 = 0.0;
+      for (int k = 0; k < 3; ++k) {
+        m.eps[3 * f + k] = ce[k] - (co[k] + (1.0 - m.gc[f]) * (cn[k] - co[k]));
+        em[k] = ce[k] - 0.5 * (co[k] + cn[k]);
+        s2 += em[k] * em[k];
+      }
+      m.skew[f] = std::sqrt(s2) / std::max(m.d_cf[f], 1.0e-30);
+      m.is_refine[f] = m.skew[f] > REFINE_SKEW_TOL;
+    } else {
+      double d[3];
+      for (int k = 0; k < 3; ++k) d[k] = ce[k] - co[k];
+      m.d_cf[f] = std::max(std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]), 1.0e-30);
+      m.gc[f] = 1.0;
+    }
+  }
+
+  {
+    int rc = build_periodic(m, err);
+    if (rc) return rc;
+  }
+  // Least-squares stencil: face neighbours (periodic partners across seams), then
+  // vertex-sharing cells, inverse-distance weights (mod_mesh.f90:mesh_build_ls_stencil).
+  int max_faces = 1;
+  for (int64_t c = 0; c < nc; ++c) max_faces = std::max<int>(max_faces, (int)(m.cell_face_off[c + 1] - m.cell_face_off[c]));
+  const int max_stencil = std::max(32, 4 * max_faces);
+  std::vector<int> cnt(nc, 0), tnb((size_t)nc * max_stencil, -1), tface((size_t)nc * max_stencil, -1);
+  std::vector<uint8_t> tper((size_t)nc * max_stencil, 0);
+  for (int64_t i = 0; i < nc; ++i) {
+    for (int64_t idx = m.cell_face_off[i]; idx < m.cell_face_off[i + 1]; ++idx) {
+      int f = m.cell_faces[idx];
+      int nb = m.owner[f];
+      if (nb == i) nb = m.neighbour[f];
+      bool is_per = false;
+      if (nb < 0) {
+        int64_t fb = f - nfi;
+        int p = m.patch[f];
+        if (p >= 0 && m.patch_bc[p] == BC_PERIODIC) {
+          int pb = m.periodic_pair[fb];
+          if (pb >= 0) nb = m.owner[nfi + pb];
+          if (nb >= 0) is_per = true;
+        }
+        if (nb < 0) nb = -1;
+      }
+      size_t s = (size_t)i * max_stencil + cnt[i]++;
+      tnb[s] = nb;
+      tper[s] = is_per;
+      if (nb == -1) tface[s] = f;
+    }
+  }
+  {
+    const int64_t nv = m.n_vertices;
+    const int64_t* coff = m.cell_vert_off.data();
+    const int* cnodes = m.cell_vertices.data();
+    std::vector<int64_t> voff(nv + 1, 0);
+    for (int64_t c = 0; c < nc; ++c)
+      for (int64_t k = coff[c]; k < coff[c + 1]; ++k) voff[cnodes[k] + 1]++;
+    for (int64_t v = 0; v < nv; ++v) voff[v + 1] += voff[v];
+    std::vector<int> vcell(voff[nv]);
+    std::vector<int64_t> vp(voff.begin(), voff.end() - 1);
+    for (int64_t c = 0; c < nc; ++c)
+      for (int64_t k = coff[c]; k < coff[c + 1]; ++k) vcell[vp[cnodes[k]]++] = (int)c;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < nc; ++i) {
+      int* nbs = &tnb[(size_t)i * max_stencil];
+      for (int64_t k = coff[i]; k < coff[i + 1]; ++k) {
+        int v = cnodes[k];
+        for (int64_t kk = voff[v]; kk < voff[v + 1]; ++kk) {
+          int cnb = vcell[kk];
+          if (cnb == i) continue;
+          bool found = false;
+          for (int j = 0; j < cnt[i]; ++j)
+            if (nbs[j] == cnb) { found = true; break; }
+          if (found) continue;
+          if (cnt[i] < max_stencil) {
+            size_t s = (size_t)i * max_stencil + cnt[i]++;
+            tnb[s] = cnb;
+            tper[s] = 0;
+            tface[s] = -1;
+          }
+        }
+      }
+    }
+  }
+  m.ls_off.assign(nc + 1, 0);
+  for (int64_t i = 0; i < nc; ++i) m.ls_off[i + 1] = m.ls_off[i] + cnt[i];
+  const int64_t ns = m.ls_off[nc];
+  m.ls_cell.assign(ns, -1);
+  m.ls_face.assign(ns, -1);
+  m.ls_w.assign(3 * ns, 0.0);
+  int64_t n_deg = 0;
+#pragma omp parallel for schedule(static) reduction(+ : n_deg)
+  for (int64_t i = 0; i < nc; ++i) {
+    const int64_t off = m.ls_off[i];
+    auto offset_of = [&](int idx, double d[3]) {
+      size_t s = (size_t)i * max_stencil + idx;
+      int nb = tnb[s];
+      const double* ci = &m.centroid[3 * i];
+      if (nb >= 0 && tper[s]) {
+        int f = m.cell_faces[m.cell_face_off[i] + idx];
+        double dpo = m.d_cf[f], dpn = dpo;
+        int64_t fb = f - nfi;
+        if (fb >= 0 && fb < nfb && m.periodic_pair_dcf[fb] > 0.0) dpn = m.periodic_pair_dcf[fb];
+        for (int k = 0; k < 3; ++k) d[k] = (dpo + dpn) * m.normal[3 * (int64_t)f + k];
+      } else if (nb >= 0) {
+        for (int k = 0; k < 3; ++k) d[k] = m.centroid[3 * (int64_t)nb + k] - ci[k];
+      } else {
+        int f = m.cell_faces[m.cell_face_off[i] + idx];
+        for (int k = 0; k < 3; ++k) d[k] = m.centre[3 * (int64_t)f + k] - ci[k];
+      }
+    };
+    double A[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    for (int idx = 0; idx < cnt[i]; ++idx) {
+      size_t s = (size_t)i * max_stencil + idx;
+      m.ls_cell[off + idx] = tnb[s];
+      m.ls_face[off + idx] = tface[s];
+      double d[3];
+      offset_of(idx, d);
+      double w = 1.0 / (std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]) + SMALL);
+      double ww = w * w;
+      A[0][0] += ww * d[0] * d[0]; A[0][1] += ww * d[0] * d[1];
+      A[0][2] += ww * d[0] * d[2]; A[1][1] += ww * d[1] * d[1];
+      A[1][2] += ww * d[1] * d[2]; A[2][2] += ww * d[2] * d[2];
+    }
+    A[1][0] = A[0][1]; A[2][0] = A[0][2]; A[2][1] = A[1][2];
+    double scale = (A[0][0] + A[1][1] + A[2][2]) / 3.0;
+    double Ai[3][3], det;
+    invert3x3(A, Ai, det);
+    if (scale <= 0.0 || std::fabs(det) < LS_DET_TOL * (scale * scale * scale)) {
+      for (int k = 0; k < 3; ++k) A[k][k] += LS_REG_FRAC * std::max(scale, SMALL);
+      invert3x3(A, Ai, det);
+      n_deg++;
+    }
+    for (int idx = 0; idx < cnt[i]; ++idx) {
+      double d[3];
+      offset_of(idx, d);
+      double w = 1.0 / (std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]) + SMALL);
+      double r[3] = {w * w * d[0], w * w * d[1], w * w * d[2]};
+      for (int k = 0; k < 3; ++k) m.ls_w[3 * (off + idx) + k] = Ai[k][0] * r[0] + Ai[k][1] * r[1] + Ai[k][2] * r[2];
+    }
+  }
+  m.ls_degenerate = n_deg;
+  return 0;
+}
+
 int build_mesh(const RawMesh& raw, const int* patch_bc, Mesh& m, std::string* err) {
   auto fail = [&](int code, const char* msg) {
     if (err) *err = msg;
@@ -378,169 +550,186 @@ int build_mesh(const RawMesh& raw, const int* patch_bc, Mesh& m, std::string* er
     }
   }
   m.patch_bc.assign(patch_bc, patch_bc + m.n_patches);
+  return finish_mesh(m, err);
+}
 
-  build_cell_faces(m);
+// Polygon face geometry (src/mesh/mod_mesh.f90:compute_polygon_face_geometry): area vector by a
+// fan from the first node, centre weighted by the fan triangles' signed areas.
+static void polygon_geometry(const int* fn, int nn, const double* xyz, double centre[3], double normal[3],
+                             double& area) {
+  centre[0] = centre[1] = centre[2] = 0.0;
+  if (nn < 3) {
+    area = SMALL;
+    normal[0] = normal[1] = normal[2] = 0.0;
+    return;
+  }
+  const double* pref = xyz + 3 * (int64_t)fn[0];
+  double nacc[3] = {0.0, 0.0, 0.0};
+  for (int i = 1; i < nn - 1; ++i) {
+    const double* pi = xyz + 3 * (int64_t)fn[i];
+    const double* pj = xyz + 3 * (int64_t)fn[i + 1];
+    double a[3], b[3], c[3];
+    for (int k = 0; k < 3; ++k) { a[k] = pi[k] - pref[k]; b[k] = pj[k] - pref[k]; }
+    cross3(a, b, c);
+    for (int k = 0; k < 3; ++k) nacc[k] = nacc[k] + 0.5 * c[k];
+  }
+  area = std::sqrt(nacc[0] * nacc[0] + nacc[1] * nacc[1] + nacc[2] * nacc[2]) + SMALL;
+  for (int k = 0; k < 3; ++k) normal[k] = nacc[k] / area;
+  double asum = 0.0;
+  for (int i = 1; i < nn - 1; ++i) {
+    const double* pi = xyz + 3 * (int64_t)fn[i];
+    const double* pj = xyz + 3 * (int64_t)fn[i + 1];
+    double a[3], b[3], c[3];
+    for (int k = 0; k < 3; ++k) { a[k] = pi[k] - pref[k]; b[k] = pj[k] - pref[k]; }
+    cross3(a, b, c);
+    double tv[3];
+    for (int k = 0; k < 3; ++k) tv[k] = 0.5 * c[k];
+    const double ta = dot3(tv, normal);
+    for (int k = 0; k < 3; ++k) centre[k] = centre[k] + ta * ((pref[k] + pi[k]) + pj[k]) / 3.0;
+    asum = asum + ta;
+  }
+  if (std::fabs(asum) > SMALL)
+    for (int k = 0; k < 3; ++k) centre[k] = centre[k] / asum;
+  else
+    for (int k = 0; k < 3; ++k) centre[k] = pref[k];
+}
 
-  // Face geometry (mod_mesh.f90:mesh_compute_geometry, mesh_tag_refinement_faces).
-  m.sf.assign(3 * nf, 0.0);
-  m.d_cf.assign(nf, 0.0);
-  m.gc.assign(nf, 0.0);
-  m.eps.assign(3 * nf, 0.0);
-  m.skew.assign(nf, 0.0);
-  m.is_refine.assign(nf, 0);
-#pragma omp parallel for schedule(static)
+int build_mesh_poly(const PolyMesh& pm, const int* patch_bc, Mesh& m, std::string* err) {
+  auto fail = [&](int code, const char* msg) {
+    if (err) *err = msg;
+    return code;
+  };
+  const int64_t nf = pm.n_faces, nfi = pm.n_int_faces, nfb = nf - nfi, nv = pm.n_points;
+  if (nf < 1 || nfi < 0 || nfi > nf) return fail(-5, "face counts out of range");
+  // foam_read: cell count from owner and neighbour, upper-triangular internal faces
+  int64_t mx = -1;
   for (int64_t f = 0; f < nf; ++f) {
-    for (int k = 0; k < 3; ++k) m.sf[3 * f + k] = m.area[f] * m.normal[3 * f + k];
-    const double* co = &m.centroid[3 * (int64_t)m.owner[f]];
-    const double* ce = &m.centre[3 * f];
-    if (m.neighbour[f] >= 0) {
-      const double* cn = &m.centroid[3 * (int64_t)m.neighbour[f]];
-      double d_on[3], d_oc[3];
-      for (int k = 0; k < 3; ++k) { d_on[k] = cn[k] - co[k]; d_oc[k] = ce[k] - co[k]; }
-      double d_on2 = d_on[0] * d_on[0] + d_on[1] * d_on[1] + d_on[2] * d_on[2];
-      m.d_cf[f] = std::max(std::sqrt(d_on2), 1.0e-30);
-      double w = dot3(d_oc, d_on) / (d_on2 + SMALL);
-      m.gc[f] = std::max(0.0, std::min(1.0, 1.0 - w));
-      double em[3], s2 = 0.0;
-      for (int k = 0; k < 3; ++k) {
-        m.eps[3 * f + k] = ce[k] - (co[k] + (1.0 - m.gc[f]) * (cn[k] - co[k]));
-        em[k] = ce[k] - 0.5 * (co[k] + cn[k]);
-        s2 += em[k] * em[k];
-      }
-      m.skew[f] = std::sqrt(s2) / std::max(m.d_cf[f], 1.0e-30);
-      m.is_refine[f] = m.skew[f] > REFINE_SKEW_TOL;
-    } else {
-      double d[3];
-      for (int k = 0; k < 3; ++k) d[k] = ce[k] - co[k];
-      m.d_cf[f] = std::max(std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]), 1.0e-30);
-      m.gc[f] = 1.0;
-    }
+    if (pm.owner[f] < 0) return fail(-5, "negative cell index in owner/neighbour (corrupt polyMesh files)");
+    mx = std::max<int64_t>(mx, pm.owner[f]);
   }
-
-  {
-    int rc = build_periodic(m, err);
-    if (rc) return rc;
+  for (int64_t f = 0; f < nfi; ++f) {
+    if (pm.neighbour[f] < 0) return fail(-5, "negative cell index in owner/neighbour (corrupt polyMesh files)");
+    mx = std::max<int64_t>(mx, pm.neighbour[f]);
   }
-  // Least-squares stencil: face neighbours (periodic partners across seams), then
-  // vertex-sharing cells, inverse-distance weights (mod_mesh.f90:mesh_build_ls_stencil).
-  int max_faces = 1;
-  for (int64_t c = 0; c < nc; ++c) max_faces = std::max<int>(max_faces, (int)(m.cell_face_off[c + 1] - m.cell_face_off[c]));
-  const int max_stencil = std::max(32, 4 * max_faces);
-  std::vector<int> cnt(nc, 0), tnb((size_t)nc * max_stencil, -1), tface((size_t)nc * max_stencil, -1);
-  std::vector<uint8_t> tper((size_t)nc * max_stencil, 0);
-  for (int64_t i = 0; i < nc; ++i) {
-    for (int64_t idx = m.cell_face_off[i]; idx < m.cell_face_off[i + 1]; ++idx) {
-      int f = m.cell_faces[idx];
-      int nb = m.owner[f];
-      if (nb == i) nb = m.neighbour[f];
-      bool is_per = false;
-      if (nb < 0) {
-        int64_t fb = f - nfi;
-        int p = m.patch[f];
-        if (p >= 0 && m.patch_bc[p] == BC_PERIODIC) {
-          int pb = m.periodic_pair[fb];
-          if (pb >= 0) nb = m.owner[nfi + pb];
-          if (nb >= 0) is_per = true;
-        }
-        if (nb < 0) nb = -1;
-      }
-      size_t s = (size_t)i * max_stencil + cnt[i]++;
-      tnb[s] = nb;
-      tper[s] = is_per;
-      if (nb == -1) tface[s] = f;
-    }
+  for (int64_t f = 0; f < nfi; ++f)
+    if (pm.owner[f] >= pm.neighbour[f]) return fail(-6, "OpenFOAM upper-triangular convention violated");
+  for (int64_t k = 0; k < pm.face_off[nf]; ++k)
+    if (pm.face_nodes[k] < 0 || pm.face_nodes[k] >= nv) return fail(-5, "face node index out of range");
+  const int64_t nc = mx + 1;
+  m = Mesh();
+  m.n_cells = nc;
+  m.n_faces = nf;
+  m.n_int_faces = nfi;
+  m.n_bnd_faces = nfb;
+  m.n_patches = pm.n_patches;
+  m.n_vertices = nv;
+  m.vertices.assign(pm.xyz, pm.xyz + 3 * nv);
+  // patches (foam_read_boundary, validate_foam_boundary_connectivity)
+  m.patch.assign(nf, -1);
+  m.patch_start.assign(m.n_patches, 0);
+  m.patch_nfaces.assign(m.n_patches, 0);
+  int n_periodic = 0;
+  for (int p = 0; p < m.n_patches; ++p) {
+    const int64_t s0 = pm.patch_start[p] - nfi, n = pm.patch_nfaces[p];
+    if (s0 < 0 || n < 0) return fail(-7, "boundary connectivity invalid (patch has invalid start_face/n_faces)");
+    if (s0 + n > nfb) return fail(-7, "patch face range exceeds boundary faces");
+    m.patch_start[p] = s0;
+    m.patch_nfaces[p] = n;
+    for (int64_t f = nfi + s0; f < nfi + s0 + n; ++f) m.patch[f] = p;
+    if (patch_bc[p] == BC_PERIODIC) n_periodic++;
   }
-  {
-    const int64_t nv = raw.n_nodes;
-    std::vector<int64_t> voff(nv + 1, 0);
-    for (int64_t c = 0; c < nc; ++c)
-      for (int64_t k = raw.cell_off[c]; k < raw.cell_off[c + 1]; ++k) voff[raw.cell_nodes[k] + 1]++;
-    for (int64_t v = 0; v < nv; ++v) voff[v + 1] += voff[v];
-    std::vector<int> vcell(voff[nv]);
-    std::vector<int64_t> vp(voff.begin(), voff.end() - 1);
-    for (int64_t c = 0; c < nc; ++c)
-      for (int64_t k = raw.cell_off[c]; k < raw.cell_off[c + 1]; ++k) vcell[vp[raw.cell_nodes[k]]++] = (int)c;
+  for (int64_t f = nfi; f < nf; ++f)
+    if (m.patch[f] < 0) return fail(-7, "boundary faces not mapped to a patch");
+  if (n_periodic % 2) return fail(-8, "odd number of periodic patches");
+  m.patch_bc.assign(patch_bc, patch_bc + m.n_patches);
+  // faces
+  m.owner.assign(pm.owner, pm.owner + nf);
+  m.neighbour.assign(nf, -1);
+  for (int64_t f = 0; f < nfi; ++f) m.neighbour[f] = pm.neighbour[f];
+  m.area.assign(nf, 0.0);
+  m.centre.assign(3 * nf, 0.0);
+  m.normal.assign(3 * nf, 0.0);
 #pragma omp parallel for schedule(static)
-    for (int64_t i = 0; i < nc; ++i) {
-      int* nbs = &tnb[(size_t)i * max_stencil];
-      for (int64_t k = raw.cell_off[i]; k < raw.cell_off[i + 1]; ++k) {
-        int v = raw.cell_nodes[k];
-        for (int64_t kk = voff[v]; kk < voff[v + 1]; ++kk) {
-          int cnb = vcell[kk];
-          if (cnb == i) continue;
-          bool found = false;
-          for (int j = 0; j < cnt[i]; ++j)
-            if (nbs[j] == cnb) { found = true; break; }
-          if (found) continue;
-          if (cnt[i] < max_stencil) {
-            size_t s = (size_t)i * max_stencil + cnt[i]++;
-            tnb[s] = cnb;
-            tper[s] = 0;
-            tface[s] = -1;
-          }
+  for (int64_t f = 0; f < nf; ++f)
+    polygon_geometry(pm.face_nodes + pm.face_off[f], (int)(pm.face_off[f + 1] - pm.face_off[f]), pm.xyz,
+                     &m.centre[3 * f], &m.normal[3 * f], m.area[f]);
+  // cell moments (mod_mesh.f90:compute_polyhedron_cell_moments), about the first vertex of the
+  // first face (in face order) that touches the cell
+  std::vector<double> ref(3 * nc, 0.0), mom(3 * nc, 0.0);
+  std::vector<uint8_t> ref_set(nc, 0);
+  m.volume.assign(nc, 0.0);
+  m.centroid.assign(3 * nc, 0.0);
+  for (int64_t f = 0; f < nf; ++f) {
+    if (pm.face_off[f + 1] - pm.face_off[f] < 3) continue;
+    for (int side = 0; side < 2; ++side) {
+      const int64_t c = side == 0 ? m.owner[f] : m.neighbour[f];
+      if (c < 0 || ref_set[c]) continue;
+      for (int k = 0; k < 3; ++k) ref[3 * c + k] = pm.xyz[3 * (int64_t)pm.face_nodes[pm.face_off[f]] + k];
+      ref_set[c] = 1;
+    }
+  }
+  for (int64_t f = 0; f < nf; ++f) {
+    const int64_t s0 = pm.face_off[f], s1 = pm.face_off[f + 1];
+    if (s1 - s0 < 3) continue;
+    for (int side = 0; side < 2; ++side) {
+      const int64_t c = side == 0 ? m.owner[f] : m.neighbour[f];
+      if (c < 0) break;
+      const double* r = &ref[3 * c];
+      double v0[3];
+      for (int k = 0; k < 3; ++k) v0[k] = pm.xyz[3 * (int64_t)pm.face_nodes[s0] + k] - r[k];
+      for (int64_t i = s0 + 1; i < s1 - 1; ++i) {
+        double v1[3], v2[3], cr[3];
+        for (int k = 0; k < 3; ++k) {
+          v1[k] = pm.xyz[3 * (int64_t)pm.face_nodes[i] + k] - r[k];
+          v2[k] = pm.xyz[3 * (int64_t)pm.face_nodes[i + 1] + k] - r[k];
+        }
+        cross3(v1, v2, cr);
+        const double sv = dot3(v0, cr) / 6.0;
+        double sm[3];
+        for (int k = 0; k < 3; ++k) sm[k] = sv * ((v0[k] + v1[k]) + v2[k]) / 4.0;
+        if (side == 0) {
+          m.volume[c] = m.volume[c] + sv;
+          for (int k = 0; k < 3; ++k) mom[3 * c + k] = mom[3 * c + k] + sm[k];
+        } else {
+          m.volume[c] = m.volume[c] - sv;
+          for (int k = 0; k < 3; ++k) mom[3 * c + k] = mom[3 * c + k] - sm[k];
         }
       }
     }
   }
-  m.ls_off.assign(nc + 1, 0);
-  for (int64_t i = 0; i < nc; ++i) m.ls_off[i + 1] = m.ls_off[i] + cnt[i];
-  const int64_t ns = m.ls_off[nc];
-  m.ls_cell.assign(ns, -1);
-  m.ls_face.assign(ns, -1);
-  m.ls_w.assign(3 * ns, 0.0);
-  int64_t n_deg = 0;
-#pragma omp parallel for schedule(static) reduction(+ : n_deg)
-  for (int64_t i = 0; i < nc; ++i) {
-    const int64_t off = m.ls_off[i];
-    auto offset_of = [&](int idx, double d[3]) {
-      size_t s = (size_t)i * max_stencil + idx;
-      int nb = tnb[s];
-      const double* ci = &m.centroid[3 * i];
-      if (nb >= 0 && tper[s]) {
-        int f = m.cell_faces[m.cell_face_off[i] + idx];
-        double dpo = m.d_cf[f], dpn = dpo;
-        int64_t fb = f - nfi;
-        if (fb >= 0 && fb < nfb && m.periodic_pair_dcf[fb] > 0.0) dpn = m.periodic_pair_dcf[fb];
-        for (int k = 0; k < 3; ++k) d[k] = (dpo + dpn) * m.normal[3 * (int64_t)f + k];
-      } else if (nb >= 0) {
-        for (int k = 0; k < 3; ++k) d[k] = m.centroid[3 * (int64_t)nb + k] - ci[k];
-      } else {
-        int f = m.cell_faces[m.cell_face_off[i] + idx];
-        for (int k = 0; k < 3; ++k) d[k] = m.centre[3 * (int64_t)f + k] - ci[k];
+  for (int64_t c = 0; c < nc; ++c) {
+    if (std::fabs(m.volume[c]) > SMALL)
+      for (int k = 0; k < 3; ++k) m.centroid[3 * c + k] = ref[3 * c + k] + mom[3 * c + k] / m.volume[c];
+    m.volume[c] = std::fabs(m.volume[c]);
+  }
+  // cell vertex lists (mod_foam_reader.f90:build_cell_topology_metadata): the cell's owner faces
+  // in face order, then its neighbour faces, each vertex at its first appearance
+  {
+    std::vector<int64_t> cnt(nc + 1, 0);
+    for (int64_t f = 0; f < nf; ++f) cnt[m.owner[f] + 1]++;
+    for (int64_t f = 0; f < nfi; ++f) cnt[m.neighbour[f] + 1]++;
+    for (int64_t c = 0; c < nc; ++c) cnt[c + 1] += cnt[c];
+    std::vector<int> cfaces(cnt[nc]);
+    std::vector<int64_t> pos(cnt.begin(), cnt.end() - 1);
+    for (int64_t f = 0; f < nf; ++f) cfaces[pos[m.owner[f]]++] = (int)f;
+    for (int64_t f = 0; f < nfi; ++f) cfaces[pos[m.neighbour[f]]++] = (int)f;
+    std::vector<int64_t> mark(nv, -1);
+    m.cell_vert_off.assign(nc + 1, 0);
+    m.cell_vertices.clear();
+    for (int64_t c = 0; c < nc; ++c) {
+      for (int64_t q = cnt[c]; q < cnt[c + 1]; ++q) {
+        const int f = cfaces[q];
+        for (int64_t k = pm.face_off[f]; k < pm.face_off[f + 1]; ++k) {
+          const int v = pm.face_nodes[k];
+          if (mark[v] == c) continue;
+          mark[v] = c;
+          m.cell_vertices.push_back(v);
+        }
       }
-    };
-    double A[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-    for (int idx = 0; idx < cnt[i]; ++idx) {
-      size_t s = (size_t)i * max_stencil + idx;
-      m.ls_cell[off + idx] = tnb[s];
-      m.ls_face[off + idx] = tface[s];
-      double d[3];
-      offset_of(idx, d);
-      double w = 1.0 / (std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]) + SMALL);
-      double ww = w * w;
-      A[0][0] += ww * d[0] * d[0]; A[0][1] += ww * d[0] * d[1];
-      A[0][2] += ww * d[0] * d[2]; A[1][1] += ww * d[1] * d[1];
-      A[1][2] += ww * d[1] * d[2]; A[2][2] += ww * d[2] * d[2];
-    }
-    A[1][0] = A[0][1]; A[2][0] = A[0][2]; A[2][1] = A[1][2];
-    double scale = (A[0][0] + A[1][1] + A[2][2]) / 3.0;
-    double Ai[3][3], det;
-    invert3x3(A, Ai, det);
-    if (scale <= 0.0 || std::fabs(det) < LS_DET_TOL * (scale * scale * scale)) {
-      for (int k = 0; k < 3; ++k) A[k][k] += LS_REG_FRAC * std::max(scale, SMALL);
-      invert3x3(A, Ai, det);
-      n_deg++;
-    }
-    for (int idx = 0; idx < cnt[i]; ++idx) {
-      double d[3];
-      offset_of(idx, d);
-      double w = 1.0 / (std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]) + SMALL);
-      double r[3] = {w * w * d[0], w * w * d[1], w * w * d[2]};
-      for (int k = 0; k < 3; ++k) m.ls_w[3 * (off + idx) + k] = Ai[k][0] * r[0] + Ai[k][1] * r[1] + Ai[k][2] * r[2];
+      m.cell_vert_off[c + 1] = (int64_t)m.cell_vertices.size();
     }
   }
-  m.ls_degenerate = n_deg;
-  return 0;
+  return finish_mesh(m, err);
 }
 
 }  // namespace dpm

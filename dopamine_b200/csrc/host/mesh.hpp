@@ -88,6 +88,32 @@ struct Mesh {
 // stencil.  Returns 0 on success, a negative code otherwise (message in *err if non-null).
 int build_mesh(const RawMesh& raw, const int* patch_bc, Mesh& m, std::string* err = nullptr);
 
+// Face-based mesh as an OpenFOAM polyMesh holds it (src/mesh/mod_foam_reader.f90:foam_read):
+// every face's node list in OpenFOAM order (internal faces first, owner < neighbour, then the
+// boundary faces of the patches), the owner of every face, the neighbour of every internal face,
+// and each patch's face range (startFace, nFaces; absolute face indices).
+struct PolyMesh {
+  int64_t n_points = 0;
+  const double* xyz = nullptr;           // [n_points][3]
+  int64_t n_faces = 0;
+  const int64_t* face_off = nullptr;     // [n_faces+1]
+  const int* face_nodes = nullptr;
+  const int* owner = nullptr;            // [n_faces]
+  int64_t n_int_faces = 0;
+  const int* neighbour = nullptr;        // [n_int_faces]
+  int n_patches = 0;
+  const int64_t* patch_start = nullptr;  // [n_patches] startFace
+  const int64_t* patch_nfaces = nullptr; // [n_patches]
+};
+
+// The polyhedral set-up of the reference's OpenFOAM path: faces kept in the file's order, polygon
+// face geometry (fan from the first node, area-weighted centre), cell centroids and volumes from
+// the faces (polyhedron moments about a vertex of the cell), cell vertex lists in face order;
+// then the same face metrics, periodic pairing and LS stencil as build_mesh.  Negative codes:
+// -5 corrupt connectivity, -6 owner >= neighbour on an internal face, -7 patch ranges that do not
+// cover the boundary faces, -8 an odd number of periodic patches.
+int build_mesh_poly(const PolyMesh& pm, const int* patch_bc, Mesh& m, std::string* err = nullptr);
+
 // Stages of build_mesh that the device builder (csrc/cuda/meshgpu.cu) shares: the cell -> face
 // CSR from owner/neighbour, and the periodic pairing with its interpolation weights.
 void build_cell_faces(Mesh& m);

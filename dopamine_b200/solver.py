@@ -31,7 +31,9 @@ EXPORTED = (
     "dpm_write_checkpoint", "dpm_read_checkpoint", "dpm_sampling_set_points", "dpm_sample_points",
     "dpm_set_nudging_profiles", "dpm_set_scalar_sources", "dpm_setup_times", "dpm_setup_compare",
     "dpm_setup_array_name", "dpm_gmsh_read", "dpm_gmsh_sizes", "dpm_gmsh_fill", "dpm_gmsh_patch_name",
-    "dpm_gmsh_free", "dpm_gmsh_write", "dpm_fcg_phase_times",
+    "dpm_gmsh_free", "dpm_gmsh_write", "dpm_fcg_phase_times", "dpm_create_poly", "dpm_foam_read",
+    "dpm_foam_sizes", "dpm_foam_fill", "dpm_foam_patch_name", "dpm_foam_patch_type", "dpm_foam_free",
+    "dpm_poly_cell_geometry",
 )
 
 
@@ -110,6 +112,8 @@ def lib(build_if_missing=True):
     L.dpm_pcg_solve_noalloc.argtypes = [C.c_int, C.c_int, vp, vp, vp, vp, vp, C.c_double, C.c_double, C.c_int,
                                         C.c_int, vp, ip, dp]
     L.dpm_setup_times.argtypes = [vp, dp]
+    L.dpm_create_poly.argtypes = [C.POINTER(abi.PolyMeshT), C.POINTER(abi.PatchCfgT), C.POINTER(abi.ParamsT), C.c_int,
+                                  C.POINTER(vp)]
     L.dpm_fcg_phase_times.argtypes = [vp, C.c_int, dp]
     L.dpm_setup_compare.argtypes = [C.POINTER(abi.RawMeshT), C.POINTER(abi.PatchCfgT), C.POINTER(abi.ParamsT),
                                     C.c_int, C.POINTER(C.c_int64), dp, dp]
@@ -134,12 +138,18 @@ class Solver:
     def __init__(self, case, device=0, params=None):
         L = lib()
         self.case = case
-        self._mesh = abi.RawMeshView(case.mesh)
         self._patches = abi.patch_cfgs(case.patches)
         self.params = params if params is not None else case.make_params()
         h = C.c_void_p()
-        _check(L.dpm_create(C.byref(self._mesh.struct), self._patches, C.byref(self.params), device, C.byref(h)),
-               "dpm_create")
+        from .cases import PolyMesh
+        if isinstance(case.mesh, PolyMesh):  # OpenFOAM-style face-based mesh
+            self._mesh = abi.PolyMeshView(case.mesh)
+            _check(L.dpm_create_poly(C.byref(self._mesh.struct), self._patches, C.byref(self.params), device,
+                                     C.byref(h)), "dpm_create_poly")
+        else:
+            self._mesh = abi.RawMeshView(case.mesh)
+            _check(L.dpm_create(C.byref(self._mesh.struct), self._patches, C.byref(self.params), device,
+                                C.byref(h)), "dpm_create")
         self.h = h
         nc, nf, nb = C.c_int64(), C.c_int64(), C.c_int64()
         L.dpm_n_cells(self.h, C.byref(nc), C.byref(nf), C.byref(nb))

@@ -315,6 +315,21 @@ int dpm_gmsh_free(dpm_gmsh_t* h);
  * faces and patches: one 2-D physical group per patch (tags 1..n_patches), one 3-D group. */
 int dpm_gmsh_write(const char* path, const dpm_raw_mesh_t* mesh, const char* const* patch_names);
 
+/* Mesh ingestion: OpenFOAM polyMesh directories (src/mesh/mod_foam_reader.f90:foam_read), ASCII
+ * files (points, faces as a faceList, owner, neighbour, boundary).  The arrays of dpm_foam_fill
+ * are dpm_poly_mesh_t's, sized by dpm_foam_sizes; each patch's name and OpenFOAM type are kept
+ * for the caller's choice of dpm_patch_cfg_t.  DPM_ERR_ARG when a file cannot be opened,
+ * DPM_ERR_MESH when one is malformed or binary, with the reason in errbuf. */
+typedef struct dpm_foam dpm_foam_t;
+int dpm_foam_read(const char* polymesh_dir, dpm_foam_t** out, char* errbuf, int errlen);
+int dpm_foam_sizes(const dpm_foam_t* h, int64_t* n_points, int64_t* n_faces, int64_t* n_face_nodes,
+                   int64_t* n_int_faces, int* n_patches);
+int dpm_foam_fill(const dpm_foam_t* h, double* xyz, int64_t* face_off, int* face_nodes, int* owner,
+                  int* neighbour, int64_t* patch_start, int64_t* patch_nfaces);
+const char* dpm_foam_patch_name(const dpm_foam_t* h, int k);
+const char* dpm_foam_patch_type(const dpm_foam_t* h, int k);
+int dpm_foam_free(dpm_foam_t* h);
+
 /* ---------------------------------------------------------------------------------------- */
 /* 2. Whole-step solver handle (src/solver/mod_fv_solver.f90 FVSolver)                       */
 /* ---------------------------------------------------------------------------------------- */
@@ -324,6 +339,33 @@ typedef struct dpm_solver dpm_solver_t;
  * LS stencils and the static projection operators on the host, uploads them to HBM. */
 int dpm_create(const dpm_raw_mesh_t* mesh, const dpm_patch_cfg_t* patches, const dpm_params_t* params,
                int device, dpm_solver_t** out);
+/* Face-based (polyhedral) mesh, as an OpenFOAM polyMesh holds it: faces in the file's order
+ * (internal faces first with owner < neighbour, then each patch's faces), 0-based indices. */
+typedef struct {
+  int64_t n_points;
+  const double* xyz;            /* [n_points][3] */
+  int64_t n_faces;
+  const int64_t* face_off;      /* [n_faces+1] into face_nodes */
+  const int* face_nodes;
+  const int* owner;             /* [n_faces] */
+  int64_t n_int_faces;
+  const int* neighbour;         /* [n_int_faces] */
+  int n_patches;
+  const int64_t* patch_start;   /* [n_patches] startFace (absolute face index) */
+  const int64_t* patch_nfaces;  /* [n_patches] nFaces */
+} dpm_poly_mesh_t;
+/* dpm_create for a polyhedral mesh: the reference's OpenFOAM-path geometry (faces kept in the
+ * file's order, polygon face geometry, cell moments from the faces; mod_mesh.f90:1336-1461) on
+ * the host, then the same static operators and time step as dpm_create.  Patches must cover the
+ * boundary faces, periodic patches come in pairs (DPM_ERR_MESH otherwise). */
+int dpm_create_poly(const dpm_poly_mesh_t* mesh, const dpm_patch_cfg_t* patches, const dpm_params_t* params,
+                    int device, dpm_solver_t** out);
+/* The polyhedral set-up alone, on the host (no device needed): cell centroids (3, n_cells) and
+ * volumes of a dpm_poly_mesh_t with the given per-patch bc ids, or DPM_ERR_MESH with the
+ * reason in errbuf (corrupt connectivity, owner >= neighbour, patches not covering the boundary,
+ * an odd number of periodic patches). */
+int dpm_poly_cell_geometry(const dpm_poly_mesh_t* mesh, const int* patch_bc, double* centroid, double* volume,
+                           char* errbuf, int errlen);
 int dpm_destroy(dpm_solver_t* s);
 int dpm_n_cells(const dpm_solver_t* s, int64_t* n_cells, int64_t* n_faces, int64_t* n_bnd_faces);
 /* solver_to_device (mod_fv_solver.f90:3286): U(3,nc), p(nc), T(nc) may be NULL. */
