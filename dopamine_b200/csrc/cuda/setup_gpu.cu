@@ -758,6 +758,135 @@ __global__ void k_wblend(int64_t nf, int64_t nfi, const double* skew, double* wb
   wbl[f] = 1.0 - t * t * (3.0 - 2.0 * t);
 }
 
+// ---- kernels: face-based (polyhedral) meshes ---------------------------------------------------
+
+// Polygon face geometry (src/mesh/mod_mesh.f90:compute_polygon_face_geometry), as build_mesh_poly.
+__global__ void k_poly_faces(int64_t nf, const int64_t* foff, const int* fnodes, const double* xyz, double* area,
+                             double* centre, double* normal) {
+  int64_t f = gtid();
+  if (f >= nf) return;
+  const int* fn = fnodes + foff[f];
+  const int nn = (int)(foff[f + 1] - foff[f]);
+  double ce[3] = {0.0, 0.0, 0.0}, nr[3] = {0.0, 0.0, 0.0}, a = SMALL;
+  if (nn >= 3) {
+    const double* pref = xyz + 3 * (int64_t)fn[0];
+    double nacc[3] = {0.0, 0.0, 0.0};
+    for (int i = 1; i < nn - 1; ++i) {
+      const double* pi = xyz + 3 * (int64_t)fn[i];
+      const double* pj = xyz + 3 * (int64_t)fn[i + 1];
+      double u[3], v[3];
+      for (int k = 0; k < 3; ++k) { u[k] = pi[k] - pref[k]; v[k] = pj[k] - pref[k]; }
+      const double c0 = u[1] * v[2] - u[2] * v[1], c1 = u[2] * v[0] - u[0] * v[2], c2 = u[0] * v[1] - u[1] * v[0];
+      nacc[0] = nacc[0] + 0.5 * c0;
+      nacc[1] = nacc[1] + 0.5 * c1;
+      nacc[2] = nacc[2] + 0.5 * c2;
+    }
+    a = sqrt(nacc[0] * nacc[0] + nacc[1] * nacc[1] + nacc[2] * nacc[2]) + SMALL;
+    for (int k = 0; k < 3; ++k) nr[k] = nacc[k] / a;
+    double asum = 0.0;
+    for (int i = 1; i < nn - 1; ++i) {
+      const double* pi = xyz + 3 * (int64_t)fn[i];
+      const double* pj = xyz + 3 * (int64_t)fn[i + 1];
+      double u[3], v[3];
+      for (int k = 0; k < 3; ++k) { u[k] = pi[k] - pref[k]; v[k] = pj[k] - pref[k]; }
+      const double tv[3] = {0.5 * (u[1] * v[2] - u[2] * v[1]), 0.5 * (u[2] * v[0] - u[0] * v[2]),
+                            0.5 * (u[0] * v[1] - u[1] * v[0])};
+      const double ta = ddot(tv, nr);
+      for (int k = 0; k < 3; ++k) ce[k] = ce[k] + ta * ((pref[k] + pi[k]) + pj[k]) / 3.0;
+      asum = asum + ta;
+    }
+    if (fabs(asum) > SMALL)
+      for (int k = 0; k < 3; ++k) ce[k] = ce[k] / asum;
+    else
+      for (int k = 0; k < 3; ++k) ce[k] = pref[k];
+  }
+  area[f] = a;
+  for (int k = 0; k < 3; ++k) {
+    centre[3 * f + k] = ce[k];
+    normal[3 * f + k] = nr[k];
+  }
+}
+
+// Cell volume and centroid from the faces (mod_mesh.f90:compute_polyhedron_cell_moments): fan
+// tetrahedra about the first vertex of the cell's first face, signed by the face's side, summed in
+// face order.
+__global__ void k_poly_cells(int64_t nc, const long long* cfo, const int* cfl, const int* owner, const int64_t* foff,
+                             const int* fnodes, const double* xyz, double* cen, double* vol) {
+  int64_t c = gtid();
+  if (c >= nc) return;
+  double r[3] = {0.0, 0.0, 0.0};
+  for (long long q = cfo[c]; q < cfo[c + 1]; ++q) {
+    const int f = cfl[q];
+    if (foff[f + 1] - foff[f] < 3) continue;
+    for (int k = 0; k < 3; ++k) r[k] = xyz[3 * (int64_t)fnodes[foff[f]] + k];
+    break;
+  }
+  double v = 0.0, mo[3] = {0.0, 0.0, 0.0};
+  for (long long q = cfo[c]; q < cfo[c + 1]; ++q) {
+    const int f = cfl[q];
+    const int64_t s0 = foff[f], s1 = foff[f + 1];
+    if (s1 - s0 < 3) continue;
+    const bool own = owner[f] == c;
+    double v0[3];
+    for (int k = 0; k < 3; ++k) v0[k] = xyz[3 * (int64_t)fnodes[s0] + k] - r[k];
+    for (int64_t i = s0 + 1; i < s1 - 1; ++i) {
+      double v1[3], v2[3];
+      for (int k = 0; k < 3; ++k) {
+        v1[k] = xyz[3 * (int64_t)fnodes[i] + k] - r[k];
+        v2[k] = xyz[3 * (int64_t)fnodes[i + 1] + k] - r[k];
+      }
+      const double cr[3] = {v1[1] * v2[2] - v1[2] * v2[1], v1[2] * v2[0] - v1[0] * v2[2], v1[0] * v2[1] - v1[1] * v2[0]};
+      const double sv = ddot(v0, cr) / 6.0;
+      double sm[3];
+      for (int k = 0; k < 3; ++k) sm[k] = sv * ((v0[k] + v1[k]) + v2[k]) / 4.0;
+      if (own) {
+        v = v + sv;
+        for (int k = 0; k < 3; ++k) mo[k] = mo[k] + sm[k];
+      } else {
+        v = v - sv;
+        for (int k = 0; k < 3; ++k) mo[k] = mo[k] - sm[k];
+      }
+    }
+  }
+  for (int k = 0; k < 3; ++k) cen[3 * c + k] = fabs(v) > SMALL ? r[k] + mo[k] / v : 0.0;
+  vol[c] = fabs(v);
+}
+
+// Cell vertex lists (mod_foam_reader.f90:build_cell_topology_metadata): the cell's owner faces in
+// face order, then its neighbour faces, each vertex once at its first appearance.  coff == null:
+// count into cnt; else write at coff[c].
+constexpr int CV_CAP = 64;
+__global__ void k_poly_cellverts(int64_t nc, const long long* cfo, const int* cfl, const int* owner,
+                                 const int64_t* foff, const int* fnodes, const int64_t* coff, long long* cnt, int* cn,
+                                 int* bad) {
+  int64_t c = gtid();
+  if (c >= nc) return;
+  int vs[CV_CAP];
+  int n = 0;
+  for (int pass = 0; pass < 2; ++pass)
+    for (long long q = cfo[c]; q < cfo[c + 1]; ++q) {
+      const int f = cfl[q];
+      if ((owner[f] == c) != (pass == 0)) continue;
+      for (int64_t k = foff[f]; k < foff[f + 1]; ++k) {
+        const int v = fnodes[k];
+        bool seen = false;
+        for (int j = 0; j < n; ++j)
+          if (vs[j] == v) { seen = true; break; }
+        if (seen) continue;
+        if (n == CV_CAP) {
+          atomicOr(bad, 8);
+          return;
+        }
+        vs[n++] = v;
+      }
+    }
+  if (!coff) {
+    cnt[c] = n;
+    return;
+  }
+  for (int j = 0; j < n; ++j) cn[coff[c] + j] = vs[j];
+}
+
 // Per-cell list widths: [0] faces, [1] boundary faces (atomicMax over cells).
 __global__ void k_cell_widths(int64_t nc, int64_t nfi, const long long* cfo, const int* cfl, int* w) {
   int64_t c = gtid();
@@ -875,8 +1004,9 @@ SetupDeviceArrays::~SetupDeviceArrays() {
   for (void* p : owned) cudaFree(p);
 }
 
-int build_setup_device(const RawMesh& raw, const dpm_patch_cfg_t* pc, const dpm_params_t& P, int device, Mesh& m,
-                       StaticOps& S, std::string* err, SetupTimes* times, SetupDeviceArrays* dev) {
+namespace {
+int setup_device_impl(const RawMesh* rawp, const PolyMesh* polyp, const dpm_patch_cfg_t* pc, const dpm_params_t& P,
+                      int device, Mesh& m, StaticOps& S, std::string* err, SetupTimes* times, SetupDeviceArrays* dev) {
   const bool full = dev == nullptr;  // every array to the host, as the host builder fills them
   auto fail = [&](int code, const char* msg) {
     if (err) *err = msg;
@@ -900,169 +1030,298 @@ int build_setup_device(const RawMesh& raw, const dpm_patch_cfg_t* pc, const dpm_
     SCK(cudaGetLastError());                                         \
   } while (0)
 
+  int64_t nc = 0, nv = 0, nfb = 0, ncn = 0, nfi = 0, nf = 0;
+  double *d_xyz = nullptr, *d_cen = nullptr, *d_vol = nullptr, *d_area = nullptr, *d_centre = nullptr,
+         *d_normal = nullptr;
+  int64_t* d_coff = nullptr;
+  int *d_cn = nullptr, *d_owner = nullptr, *d_nbr = nullptr, *d_patch = nullptr, *d_bad = nullptr, *d_cfl = nullptr;
+  unsigned long long *d_cnt1 = nullptr, *d_ccnt = nullptr;
+  long long* d_cfo = nullptr;
+  long long ncf = 0;
+  int bad = 0;
+  bool csr_done = false;  // the face-based path builds the cell -> face lists with its geometry
   auto t_all = Clock::now();
   auto t0 = Clock::now();
-  const int64_t nc = raw.n_cells, nv = raw.n_nodes, nfb = raw.n_bfaces;
-  if (nc <= 0 || nc > 2000000000LL || nv > 2000000000LL) return fail(DPM_ERR_UNSUPPORTED, "mesh size out of range");
-  m = Mesh();
-  m.n_cells = nc;
-  m.n_patches = raw.n_patches;
-  m.n_vertices = nv;
-  m.vertices.assign(raw.xyz, raw.xyz + 3 * nv);
-  m.cell_vert_off.assign(raw.cell_off, raw.cell_off + nc + 1);
-  m.cell_vertices.assign(raw.cell_nodes, raw.cell_nodes + raw.cell_off[nc]);
-  const int64_t ncn = raw.cell_off[nc];
-  double* d_xyz = ar.put(raw.xyz, 3 * nv, st);
-  int* d_type = ar.put(raw.cell_type, nc, st);
-  int64_t* d_coff = ar.put(raw.cell_off, nc + 1, st);
-  int* d_cn = ar.put(raw.cell_nodes, ncn, st);
-  int64_t* d_boff = ar.put(raw.bface_off, nfb + 1, st);
-  int* d_bnodes = ar.put(raw.bface_nodes, raw.bface_off[nfb], st);
-  int* d_bpatch = ar.put(raw.bface_patch, nfb, st);
-  SCK(cudaStreamSynchronize(st));
-  T.stage_ms[0] = ms_since(t0);
+  if (rawp) {
+    const RawMesh& raw = *rawp;
+    nc = raw.n_cells; nv = raw.n_nodes; nfb = raw.n_bfaces;
+    if (nc <= 0 || nc > 2000000000LL || nv > 2000000000LL) return fail(DPM_ERR_UNSUPPORTED, "mesh size out of range");
+    m = Mesh();
+    m.n_cells = nc;
+    m.n_patches = raw.n_patches;
+    m.n_vertices = nv;
+    m.vertices.assign(raw.xyz, raw.xyz + 3 * nv);
+    m.cell_vert_off.assign(raw.cell_off, raw.cell_off + nc + 1);
+    m.cell_vertices.assign(raw.cell_nodes, raw.cell_nodes + raw.cell_off[nc]);
+    ncn = raw.cell_off[nc];
+    d_xyz = ar.put(raw.xyz, 3 * nv, st);
+    int* d_type = ar.put(raw.cell_type, nc, st);
+    d_coff = ar.put(raw.cell_off, nc + 1, st);
+    d_cn = ar.put(raw.cell_nodes, ncn, st);
+    int64_t* d_boff = ar.put(raw.bface_off, nfb + 1, st);
+    int* d_bnodes = ar.put(raw.bface_nodes, raw.bface_off[nfb], st);
+    int* d_bpatch = ar.put(raw.bface_patch, nfb, st);
+    SCK(cudaStreamSynchronize(st));
+    T.stage_ms[0] = ms_since(t0);
 
-  // cells and face matching
-  t0 = Clock::now();
-  int* d_bad = ar.get<int>(4);
-  unsigned long long* d_cnt1 = ar.get<unsigned long long>(2);
-  double* d_cen = ar.get<double>(3 * nc);
-  double* d_vol = ar.get<double>(nc);
-  long long* d_nfc = ar.get<long long>(nc);
-  long long* d_roff = ar.get<long long>(nc + 1);
-  SCK(cudaMemsetAsync(d_bad, 0, 4 * sizeof(int), st));
-  SCK(cudaMemsetAsync(d_cnt1, 0, 2 * sizeof(unsigned long long), st));
-  SLAUNCH(nc, k_cells, nc, d_type, d_coff, d_cn, d_xyz, d_cen, d_vol, d_nfc, d_bad);
-  if (!scan_counts(ar, reinterpret_cast<unsigned long long*>(d_nfc), d_roff, nc, st)) return fail(DPM_ERR_CUDA, "scan");
-  long long nrec_ll = 0;
-  int bad = 0;
-  SCK(cudaMemcpyAsync(&nrec_ll, d_roff + nc, sizeof(long long), cudaMemcpyDeviceToHost, st));
-  SCK(cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, st));
-  SCK(cudaStreamSynchronize(st));
-  if (bad & 1) return fail(-1, "unsupported element type");
-  if (nrec_ll > 2147483647LL) return fail(DPM_ERR_UNSUPPORTED, "too many element faces for the device set-up");
-  const int64_t nrec = nrec_ll;
-  ar.drop(d_nfc);
-  int B = 1;
-  while (B < 32 && (1LL << B) <= nv) ++B;  // ids + 1 in [0, nv] fit in B bits
-  unsigned long long* d_hi = ar.get<unsigned long long>(nrec);
-  unsigned long long* d_lo = ar.get<unsigned long long>(nrec);
-  unsigned long long* d_k1 = ar.get<unsigned long long>(nrec);
-  unsigned long long* d_hs = ar.get<unsigned long long>(nrec);
-  int* d_rcell = ar.get<int>(nrec);
-  unsigned char* d_rfi = ar.get<unsigned char>(nrec);
-  int* d_rid = ar.get<int>(nrec);
-  int* d_p1 = ar.get<int>(nrec);
-  int* d_perm = ar.get<int>(nrec);
-  SCK(cudaGetLastError());
-  SLAUNCH(nc, k_records, nc, d_type, d_coff, d_cn, d_roff, B, d_hi, d_lo, d_rcell, d_rfi, d_rid);
-  {
-    size_t tb1 = 0, tb2 = 0;
-    SCK(cub::DeviceRadixSort::SortPairs(nullptr, tb1, d_lo, d_k1, d_rid, d_p1, (int)nrec, 0, 2 * B, st));
-    SCK(cub::DeviceRadixSort::SortPairs(nullptr, tb2, d_k1, d_hs, d_p1, d_perm, (int)nrec, 0, 2 * B, st));
-    void* tmp = ar.get<unsigned char>(std::max(tb1, tb2));
+    // cells and face matching
+    t0 = Clock::now();
+    d_bad = ar.get<int>(4);
+    d_cnt1 = ar.get<unsigned long long>(2);
+    d_cen = ar.get<double>(3 * nc);
+    d_vol = ar.get<double>(nc);
+    long long* d_nfc = ar.get<long long>(nc);
+    long long* d_roff = ar.get<long long>(nc + 1);
+    SCK(cudaMemsetAsync(d_bad, 0, 4 * sizeof(int), st));
+    SCK(cudaMemsetAsync(d_cnt1, 0, 2 * sizeof(unsigned long long), st));
+    SLAUNCH(nc, k_cells, nc, d_type, d_coff, d_cn, d_xyz, d_cen, d_vol, d_nfc, d_bad);
+    if (!scan_counts(ar, reinterpret_cast<unsigned long long*>(d_nfc), d_roff, nc, st)) return fail(DPM_ERR_CUDA, "scan");
+    long long nrec_ll = 0;
+    bad = 0;
+    SCK(cudaMemcpyAsync(&nrec_ll, d_roff + nc, sizeof(long long), cudaMemcpyDeviceToHost, st));
+    SCK(cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, st));
+    SCK(cudaStreamSynchronize(st));
+    if (bad & 1) return fail(-1, "unsupported element type");
+    if (nrec_ll > 2147483647LL) return fail(DPM_ERR_UNSUPPORTED, "too many element faces for the device set-up");
+    const int64_t nrec = nrec_ll;
+    ar.drop(d_nfc);
+    int B = 1;
+    while (B < 32 && (1LL << B) <= nv) ++B;  // ids + 1 in [0, nv] fit in B bits
+    unsigned long long* d_hi = ar.get<unsigned long long>(nrec);
+    unsigned long long* d_lo = ar.get<unsigned long long>(nrec);
+    unsigned long long* d_k1 = ar.get<unsigned long long>(nrec);
+    unsigned long long* d_hs = ar.get<unsigned long long>(nrec);
+    int* d_rcell = ar.get<int>(nrec);
+    unsigned char* d_rfi = ar.get<unsigned char>(nrec);
+    int* d_rid = ar.get<int>(nrec);
+    int* d_p1 = ar.get<int>(nrec);
+    int* d_perm = ar.get<int>(nrec);
     SCK(cudaGetLastError());
-    // stable LSD: low word first, then the high word (carrying the low-word order)
-    SCK(cub::DeviceRadixSort::SortPairs(tmp, tb1, d_lo, d_k1, d_rid, d_p1, (int)nrec, 0, 2 * B, st));
-    SLAUNCH(nrec, k_gather64, nrec, d_hi, d_p1, d_k1);
-    SCK(cub::DeviceRadixSort::SortPairs(tmp, tb2, d_k1, d_hs, d_p1, d_perm, (int)nrec, 0, 2 * B, st));
-    ar.drop(tmp);
-  }
-  unsigned long long* d_ls = d_k1;  // low words in sorted order
-  SLAUNCH(nrec, k_gather64, nrec, d_lo, d_perm, d_ls);
-  ar.drop(d_hi);
-  ar.drop(d_lo);
-  ar.drop(d_rid);
-  ar.drop(d_p1);
-  unsigned char* d_matched = ar.get<unsigned char>(nrec);
-  int* d_sflag = ar.get<int>(nrec);
-  int* d_sowner = ar.get<int>(nrec);
-  int* d_sidx = ar.get<int>(nrec);
-  SCK(cudaGetLastError());
-  SCK(cudaMemsetAsync(d_sflag, 0, nrec * sizeof(int), st));
-  SLAUNCH(nrec, k_match, nrec, d_hs, d_ls, d_perm, d_rcell, d_matched, d_sflag, d_sowner);
-  {
-    size_t tb = 0;
-    SCK(cub::DeviceScan::ExclusiveSum(nullptr, tb, d_sflag, d_sidx, (int)nrec, st));
-    void* tmp = ar.get<unsigned char>(tb);
+    SLAUNCH(nc, k_records, nc, d_type, d_coff, d_cn, d_roff, B, d_hi, d_lo, d_rcell, d_rfi, d_rid);
+    {
+      size_t tb1 = 0, tb2 = 0;
+      SCK(cub::DeviceRadixSort::SortPairs(nullptr, tb1, d_lo, d_k1, d_rid, d_p1, (int)nrec, 0, 2 * B, st));
+      SCK(cub::DeviceRadixSort::SortPairs(nullptr, tb2, d_k1, d_hs, d_p1, d_perm, (int)nrec, 0, 2 * B, st));
+      void* tmp = ar.get<unsigned char>(std::max(tb1, tb2));
+      SCK(cudaGetLastError());
+      // stable LSD: low word first, then the high word (carrying the low-word order)
+      SCK(cub::DeviceRadixSort::SortPairs(tmp, tb1, d_lo, d_k1, d_rid, d_p1, (int)nrec, 0, 2 * B, st));
+      SLAUNCH(nrec, k_gather64, nrec, d_hi, d_p1, d_k1);
+      SCK(cub::DeviceRadixSort::SortPairs(tmp, tb2, d_k1, d_hs, d_p1, d_perm, (int)nrec, 0, 2 * B, st));
+      ar.drop(tmp);
+    }
+    unsigned long long* d_ls = d_k1;  // low words in sorted order
+    SLAUNCH(nrec, k_gather64, nrec, d_lo, d_perm, d_ls);
+    ar.drop(d_hi);
+    ar.drop(d_lo);
+    ar.drop(d_rid);
+    ar.drop(d_p1);
+    unsigned char* d_matched = ar.get<unsigned char>(nrec);
+    int* d_sflag = ar.get<int>(nrec);
+    int* d_sowner = ar.get<int>(nrec);
+    int* d_sidx = ar.get<int>(nrec);
     SCK(cudaGetLastError());
-    SCK(cub::DeviceScan::ExclusiveSum(tmp, tb, d_sflag, d_sidx, (int)nrec, st));
-    ar.drop(tmp);
-  }
-  int last_idx = 0, last_flag = 0;
-  SCK(cudaMemcpyAsync(&last_idx, d_sidx + nrec - 1, sizeof(int), cudaMemcpyDeviceToHost, st));
-  SCK(cudaMemcpyAsync(&last_flag, d_sflag + nrec - 1, sizeof(int), cudaMemcpyDeviceToHost, st));
-  SCK(cudaStreamSynchronize(st));
-  T.stage_ms[1] = ms_since(t0);
+    SCK(cudaMemsetAsync(d_sflag, 0, nrec * sizeof(int), st));
+    SLAUNCH(nrec, k_match, nrec, d_hs, d_ls, d_perm, d_rcell, d_matched, d_sflag, d_sowner);
+    {
+      size_t tb = 0;
+      SCK(cub::DeviceScan::ExclusiveSum(nullptr, tb, d_sflag, d_sidx, (int)nrec, st));
+      void* tmp = ar.get<unsigned char>(tb);
+      SCK(cudaGetLastError());
+      SCK(cub::DeviceScan::ExclusiveSum(tmp, tb, d_sflag, d_sidx, (int)nrec, st));
+      ar.drop(tmp);
+    }
+    int last_idx = 0, last_flag = 0;
+    SCK(cudaMemcpyAsync(&last_idx, d_sidx + nrec - 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+    SCK(cudaMemcpyAsync(&last_flag, d_sflag + nrec - 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+    SCK(cudaStreamSynchronize(st));
+    T.stage_ms[1] = ms_since(t0);
 
-  // faces: interior in creation order, boundary regrouped by patch
-  t0 = Clock::now();
-  const int64_t nfi = (int64_t)last_idx + last_flag, nf = nfi + nfb;
-  if (nf > 2000000000LL) return fail(DPM_ERR_UNSUPPORTED, "too many faces");
-  m.n_int_faces = nfi;
-  m.n_bnd_faces = nfb;
-  m.n_faces = nf;
-  m.patch_start.assign(m.n_patches, 0);
-  m.patch_nfaces.assign(m.n_patches, 0);
-  std::vector<long long> bpos(nfb);
-  for (int64_t b = 0; b < nfb; ++b) {
-    int p = raw.bface_patch[b];
-    if (p < 0 || p >= m.n_patches) return fail(DPM_ERR_ARG, "boundary face with a patch index out of range");
-    m.patch_nfaces[p]++;
+    // faces: interior in creation order, boundary regrouped by patch
+    t0 = Clock::now();
+    nfi = (int64_t)last_idx + last_flag;
+    nf = nfi + nfb;
+    if (nf > 2000000000LL) return fail(DPM_ERR_UNSUPPORTED, "too many faces");
+    m.n_int_faces = nfi;
+    m.n_bnd_faces = nfb;
+    m.n_faces = nf;
+    m.patch_start.assign(m.n_patches, 0);
+    m.patch_nfaces.assign(m.n_patches, 0);
+    std::vector<long long> bpos(nfb);
+    for (int64_t b = 0; b < nfb; ++b) {
+      int p = raw.bface_patch[b];
+      if (p < 0 || p >= m.n_patches) return fail(DPM_ERR_ARG, "boundary face with a patch index out of range");
+      m.patch_nfaces[p]++;
+    }
+    for (int p = 1; p < m.n_patches; ++p) m.patch_start[p] = m.patch_start[p - 1] + m.patch_nfaces[p - 1];
+    {
+      std::vector<int64_t> cursor(m.patch_start);
+      for (int64_t b = 0; b < nfb; ++b) bpos[b] = cursor[raw.bface_patch[b]]++;
+    }
+    m.patch_bc.resize(m.n_patches);
+    for (int p = 0; p < m.n_patches; ++p) m.patch_bc[p] = pc[p].bc_id;
+    long long* d_bpos = ar.put(bpos.data(), nfb, st);
+    d_owner = ar.get<int>(nf);
+    d_nbr = ar.get<int>(nf);
+    d_patch = ar.get<int>(nf);
+    d_area = ar.get<double>(nf);
+    d_centre = ar.get<double>(3 * nf);
+    d_normal = ar.get<double>(3 * nf);
+    SCK(cudaGetLastError());
+    SLAUNCH(nrec, k_int_faces, nrec, d_sflag, d_sidx, d_sowner, d_rcell, d_rfi, d_type, d_coff, d_cn, d_xyz, d_cen,
+            d_owner, d_nbr, d_patch, d_area, d_centre, d_normal);
+    SLAUNCH(nfb, k_bnd_faces, nfb, d_boff, d_bnodes, d_bpatch, d_bpos, nfi, B, nrec, d_hs, d_ls, d_perm, d_rcell, d_xyz,
+            d_cen, d_matched, d_bad, d_owner, d_nbr, d_patch, d_area, d_centre, d_normal);
+    SLAUNCH(nrec, k_count_zero, nrec, d_matched, d_cnt1);
+    unsigned long long unmatched = 0;
+    SCK(cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, st));
+    SCK(cudaMemcpyAsync(&unmatched, d_cnt1, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    SCK(cudaStreamSynchronize(st));
+    if (bad & 4) return fail(DPM_ERR_UNSUPPORTED, "boundary face with other than 3 or 4 nodes");
+    if (bad & 2) return fail(-2, "boundary face has no owner cell");
+    if (unmatched) return fail(-3, "unlabelled boundary faces (open cells)");
+    for (void* p : {(void*)d_hs, (void*)d_ls, (void*)d_perm, (void*)d_rcell, (void*)d_rfi, (void*)d_matched,
+                    (void*)d_sflag, (void*)d_sowner, (void*)d_sidx, (void*)d_roff, (void*)d_bpos})
+      ar.drop(p);
+
+  } else {
+    // face-based mesh: faces, owners and patches as given (build_mesh_poly's checks), the
+    // reference's polygon face geometry and polyhedron moments, cell vertices in face order
+    const PolyMesh& pm = *polyp;
+    nf = pm.n_faces;
+    nfi = pm.n_int_faces;
+    nfb = nf - nfi;
+    nv = pm.n_points;
+    if (nf < 1 || nfi < 0 || nfi > nf || nf > 2000000000LL || nv > 2000000000LL)
+      return fail(-5, "face counts out of range");
+    int64_t mx = -1;
+    for (int64_t f = 0; f < nf; ++f) {
+      if (pm.owner[f] < 0) return fail(-5, "negative cell index in owner/neighbour (corrupt polyMesh files)");
+      mx = std::max<int64_t>(mx, pm.owner[f]);
+    }
+    for (int64_t f = 0; f < nfi; ++f) {
+      if (pm.neighbour[f] < 0) return fail(-5, "negative cell index in owner/neighbour (corrupt polyMesh files)");
+      mx = std::max<int64_t>(mx, pm.neighbour[f]);
+    }
+    for (int64_t f = 0; f < nfi; ++f)
+      if (pm.owner[f] >= pm.neighbour[f]) return fail(-6, "OpenFOAM upper-triangular convention violated");
+    for (int64_t k = 0; k < pm.face_off[nf]; ++k)
+      if (pm.face_nodes[k] < 0 || pm.face_nodes[k] >= nv) return fail(-5, "face node index out of range");
+    nc = mx + 1;
+    if (nc <= 0 || nc > 2000000000LL) return fail(DPM_ERR_UNSUPPORTED, "mesh size out of range");
+    m = Mesh();
+    m.n_cells = nc;
+    m.n_faces = nf;
+    m.n_int_faces = nfi;
+    m.n_bnd_faces = nfb;
+    m.n_patches = pm.n_patches;
+    m.n_vertices = nv;
+    m.vertices.assign(pm.xyz, pm.xyz + 3 * nv);
+    m.patch_start.assign(m.n_patches, 0);
+    m.patch_nfaces.assign(m.n_patches, 0);
+    m.patch_bc.resize(m.n_patches);
+    std::vector<int> fpatch(nf, -1), fnbr(nf, -1);
+    int n_periodic = 0;
+    for (int p = 0; p < m.n_patches; ++p) {
+      const int64_t s0 = pm.patch_start[p] - nfi, n = pm.patch_nfaces[p];
+      if (s0 < 0 || n < 0) return fail(-7, "boundary connectivity invalid (patch has invalid start_face/n_faces)");
+      if (s0 + n > nfb) return fail(-7, "patch face range exceeds boundary faces");
+      m.patch_start[p] = s0;
+      m.patch_nfaces[p] = n;
+      m.patch_bc[p] = pc[p].bc_id;
+      for (int64_t f = nfi + s0; f < nfi + s0 + n; ++f) fpatch[f] = p;
+      if (pc[p].bc_id == BC_PERIODIC) n_periodic++;
+    }
+    for (int64_t f = nfi; f < nf; ++f)
+      if (fpatch[f] < 0) return fail(-7, "boundary faces not mapped to a patch");
+    if (n_periodic % 2) return fail(-8, "odd number of periodic patches");
+    for (int64_t f = 0; f < nfi; ++f) fnbr[f] = pm.neighbour[f];
+    d_xyz = ar.put(pm.xyz, 3 * nv, st);
+    int64_t* d_foff = ar.put(pm.face_off, nf + 1, st);
+    int* d_fnodes = ar.put(pm.face_nodes, pm.face_off[nf], st);
+    d_owner = ar.put(pm.owner, nf, st);
+    d_nbr = ar.put(fnbr.data(), nf, st);
+    d_patch = ar.put(fpatch.data(), nf, st);
+    SCK(cudaStreamSynchronize(st));
+    T.stage_ms[0] = ms_since(t0);
+    t0 = Clock::now();
+    d_bad = ar.get<int>(4);
+    d_cnt1 = ar.get<unsigned long long>(2);
+    d_cen = ar.get<double>(3 * nc);
+    d_vol = ar.get<double>(nc);
+    d_area = ar.get<double>(nf);
+    d_centre = ar.get<double>(3 * nf);
+    d_normal = ar.get<double>(3 * nf);
+    d_ccnt = ar.get<unsigned long long>(nc);
+    d_cfo = ar.get<long long>(nc + 1);
+    long long* d_cvn = ar.get<long long>(nc);
+    SCK(cudaGetLastError());
+    SCK(cudaMemsetAsync(d_bad, 0, 4 * sizeof(int), st));
+    SCK(cudaMemsetAsync(d_cnt1, 0, 2 * sizeof(unsigned long long), st));
+    SLAUNCH(nf, k_poly_faces, nf, d_foff, d_fnodes, d_xyz, d_area, d_centre, d_normal);
+    SCK(cudaMemsetAsync(d_ccnt, 0, nc * sizeof(unsigned long long), st));
+    SLAUNCH(nf, k_cf_count, nf, d_owner, d_nbr, d_ccnt);
+    if (!scan_counts(ar, d_ccnt, d_cfo, nc, st)) return fail(DPM_ERR_CUDA, "scan");
+    SCK(cudaMemcpyAsync(&ncf, d_cfo + nc, sizeof(long long), cudaMemcpyDeviceToHost, st));
+    SCK(cudaStreamSynchronize(st));
+    d_cfl = ar.get<int>(ncf);
+    SCK(cudaGetLastError());
+    SCK(cudaMemcpyAsync(d_ccnt, d_cfo, nc * sizeof(long long), cudaMemcpyDeviceToDevice, st));
+    SLAUNCH(nf, k_cf_fill, nf, d_owner, d_nbr, d_ccnt, d_cfl);
+    SLAUNCH(nc, k_sort_rows, nc, d_cfo, d_cfl);
+    csr_done = true;
+    SLAUNCH(nc, k_poly_cells, nc, d_cfo, d_cfl, d_owner, d_foff, d_fnodes, d_xyz, d_cen, d_vol);
+    // cell vertex lists: count, offsets, fill
+    SLAUNCH(nc, k_poly_cellverts, nc, d_cfo, d_cfl, d_owner, d_foff, d_fnodes, (const int64_t*)nullptr, d_cvn,
+            (int*)nullptr, d_bad);
+    d_coff = ar.get<int64_t>(nc + 1);
+    SCK(cudaGetLastError());
+    if (!scan_counts(ar, reinterpret_cast<unsigned long long*>(d_cvn), reinterpret_cast<long long*>(d_coff), nc, st))
+      return fail(DPM_ERR_CUDA, "scan");
+    long long ncn_ll = 0;
+    SCK(cudaMemcpyAsync(&ncn_ll, d_coff + nc, sizeof(long long), cudaMemcpyDeviceToHost, st));
+    SCK(cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, st));
+    SCK(cudaStreamSynchronize(st));
+    if (bad & 8) return fail(DPM_ERR_UNSUPPORTED, "a cell with more vertices than the device set-up holds");
+    ncn = ncn_ll;
+    d_cn = ar.get<int>(ncn);
+    SCK(cudaGetLastError());
+    SLAUNCH(nc, k_poly_cellverts, nc, d_cfo, d_cfl, d_owner, d_foff, d_fnodes, d_coff, d_cvn, d_cn, d_bad);
+    if (full) {
+      SCK(fetch(m.cell_vert_off, d_coff, nc + 1, st) ? cudaSuccess : cudaErrorUnknown);
+      SCK(fetch(m.cell_vertices, d_cn, ncn, st) ? cudaSuccess : cudaErrorUnknown);
+    }
+    SCK(cudaStreamSynchronize(st));
+    ar.drop(d_cvn);
+    T.stage_ms[1] = ms_since(t0);
+    t0 = Clock::now();
   }
-  for (int p = 1; p < m.n_patches; ++p) m.patch_start[p] = m.patch_start[p - 1] + m.patch_nfaces[p - 1];
-  {
-    std::vector<int64_t> cursor(m.patch_start);
-    for (int64_t b = 0; b < nfb; ++b) bpos[b] = cursor[raw.bface_patch[b]]++;
-  }
-  m.patch_bc.resize(m.n_patches);
-  for (int p = 0; p < m.n_patches; ++p) m.patch_bc[p] = pc[p].bc_id;
-  long long* d_bpos = ar.put(bpos.data(), nfb, st);
-  int* d_owner = ar.get<int>(nf);
-  int* d_nbr = ar.get<int>(nf);
-  int* d_patch = ar.get<int>(nf);
-  double* d_area = ar.get<double>(nf);
-  double* d_centre = ar.get<double>(3 * nf);
-  double* d_normal = ar.get<double>(3 * nf);
-  SCK(cudaGetLastError());
-  SLAUNCH(nrec, k_int_faces, nrec, d_sflag, d_sidx, d_sowner, d_rcell, d_rfi, d_type, d_coff, d_cn, d_xyz, d_cen,
-          d_owner, d_nbr, d_patch, d_area, d_centre, d_normal);
-  SLAUNCH(nfb, k_bnd_faces, nfb, d_boff, d_bnodes, d_bpatch, d_bpos, nfi, B, nrec, d_hs, d_ls, d_perm, d_rcell, d_xyz,
-          d_cen, d_matched, d_bad, d_owner, d_nbr, d_patch, d_area, d_centre, d_normal);
-  SLAUNCH(nrec, k_count_zero, nrec, d_matched, d_cnt1);
-  unsigned long long unmatched = 0;
-  SCK(cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, st));
-  SCK(cudaMemcpyAsync(&unmatched, d_cnt1, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
-  SCK(cudaStreamSynchronize(st));
-  if (bad & 4) return fail(DPM_ERR_UNSUPPORTED, "boundary face with other than 3 or 4 nodes");
-  if (bad & 2) return fail(-2, "boundary face has no owner cell");
-  if (unmatched) return fail(-3, "unlabelled boundary faces (open cells)");
-  for (void* p : {(void*)d_hs, (void*)d_ls, (void*)d_perm, (void*)d_rcell, (void*)d_rfi, (void*)d_matched,
-                  (void*)d_sflag, (void*)d_sowner, (void*)d_sidx, (void*)d_roff, (void*)d_bpos})
-    ar.drop(p);
   double* d_sf = ar.get<double>(3 * nf);
   double* d_dcf = ar.get<double>(nf);
   double* d_gc = ar.get<double>(nf);
   double* d_eps = ar.get<double>(3 * nf);
   double* d_skew = ar.get<double>(nf);
   unsigned char* d_isref = ar.get<unsigned char>(nf);
-  unsigned long long* d_ccnt = ar.get<unsigned long long>(nc);
-  long long* d_cfo = ar.get<long long>(nc + 1);
+  if (!csr_done) {
+    d_ccnt = ar.get<unsigned long long>(nc);
+    d_cfo = ar.get<long long>(nc + 1);
+  }
   SCK(cudaGetLastError());
   SLAUNCH(nf, k_face_metrics, nf, d_owner, d_nbr, d_area, d_normal, d_centre, d_cen, d_sf, d_dcf, d_gc, d_eps, d_skew,
           d_isref);
   // cell -> face lists (mod_mesh.f90:mesh_build_connectivity), faces ascending
-  SCK(cudaMemsetAsync(d_ccnt, 0, nc * sizeof(unsigned long long), st));
-  SLAUNCH(nf, k_cf_count, nf, d_owner, d_nbr, d_ccnt);
-  if (!scan_counts(ar, d_ccnt, d_cfo, nc, st)) return fail(DPM_ERR_CUDA, "scan");
-  long long ncf = 0;
-  SCK(cudaMemcpyAsync(&ncf, d_cfo + nc, sizeof(long long), cudaMemcpyDeviceToHost, st));
-  SCK(cudaStreamSynchronize(st));
-  int* d_cfl = ar.get<int>(ncf);
-  SCK(cudaGetLastError());
-  SCK(cudaMemcpyAsync(d_ccnt, d_cfo, nc * sizeof(long long), cudaMemcpyDeviceToDevice, st));
-  SLAUNCH(nf, k_cf_fill, nf, d_owner, d_nbr, d_ccnt, d_cfl);
-  SLAUNCH(nc, k_sort_rows, nc, d_cfo, d_cfl);
+  if (!csr_done) {
+    SCK(cudaMemsetAsync(d_ccnt, 0, nc * sizeof(unsigned long long), st));
+    SLAUNCH(nf, k_cf_count, nf, d_owner, d_nbr, d_ccnt);
+    if (!scan_counts(ar, d_ccnt, d_cfo, nc, st)) return fail(DPM_ERR_CUDA, "scan");
+    SCK(cudaMemcpyAsync(&ncf, d_cfo + nc, sizeof(long long), cudaMemcpyDeviceToHost, st));
+    SCK(cudaStreamSynchronize(st));
+    d_cfl = ar.get<int>(ncf);
+    SCK(cudaGetLastError());
+    SCK(cudaMemcpyAsync(d_ccnt, d_cfo, nc * sizeof(long long), cudaMemcpyDeviceToDevice, st));
+    SLAUNCH(nf, k_cf_fill, nf, d_owner, d_nbr, d_ccnt, d_cfl);
+    SLAUNCH(nc, k_sort_rows, nc, d_cfo, d_cfl);
+  }
   // the host needs the boundary faces for the periodic pairing and the outlet rows, and the
   // whole mesh for the rest of the solver set-up
   int widths[2] = {0, 0}, refine_any = 0;
@@ -1482,6 +1741,17 @@ int build_setup_device(const RawMesh& raw, const dpm_patch_cfg_t* pc, const dpm_
 #undef SLAUNCH
   return 0;
 }
+}  // namespace
+
+int build_setup_device(const RawMesh& raw, const dpm_patch_cfg_t* pc, const dpm_params_t& P, int device, Mesh& m,
+                       StaticOps& S, std::string* err, SetupTimes* times, SetupDeviceArrays* dev) {
+  return setup_device_impl(&raw, nullptr, pc, P, device, m, S, err, times, dev);
+}
+
+int build_setup_device_poly(const PolyMesh& pm, const dpm_patch_cfg_t* pc, const dpm_params_t& P, int device,
+                            Mesh& m, StaticOps& S, std::string* err, SetupTimes* times, SetupDeviceArrays* dev) {
+  return setup_device_impl(nullptr, &pm, pc, P, device, m, S, err, times, dev);
+}
 
 }  // namespace dpm
 
@@ -1507,42 +1777,8 @@ int64_t n_diff(const std::vector<T>& a, const std::vector<T>& b) {
   return n;
 }
 
-}  // namespace
-
-}  // namespace dpm
-
-extern "C" int dpm_setup_compare(const dpm_raw_mesh_t* raw, const dpm_patch_cfg_t* patches, const dpm_params_t* params,
-                                 int device, int64_t* mismatches, double* G_max_rel, double* ms) {
-  using namespace dpm;
-  if (!raw || !patches || !params || !mismatches || !G_max_rel) return DPM_ERR_ARG;
-  static_assert(kNSetupArrays <= DPM_SETUP_N_ARRAYS, "array table");
-  RawMesh r;
-  r.n_nodes = raw->n_nodes; r.xyz = raw->xyz; r.n_cells = raw->n_cells; r.cell_type = raw->cell_type;
-  r.cell_off = raw->cell_off; r.cell_nodes = raw->cell_nodes; r.n_bfaces = raw->n_bfaces;
-  r.bface_off = raw->bface_off; r.bface_nodes = raw->bface_nodes; r.bface_patch = raw->bface_patch;
-  r.n_patches = raw->n_patches;
-  std::vector<int> pbc(raw->n_patches);
-  for (int i = 0; i < raw->n_patches; ++i) pbc[i] = patches[i].bc_id;
-  Mesh mh, md;
-  StaticOps Sh, Sd;
-  std::string err;
-  auto t0 = std::chrono::steady_clock::now();
-  if (build_mesh(r, pbc.data(), mh, &err)) return DPM_ERR_MESH;
-  auto t1 = std::chrono::steady_clock::now();
-  if (build_static_ops(mh, patches, *params, Sh)) return DPM_ERR_MESH;
-  auto t2 = std::chrono::steady_clock::now();
-  SetupTimes tt;
-  int rc = build_setup_device(r, patches, *params, device, md, Sd, &err, &tt);
-  if (rc) {
-    std::fprintf(stderr, "dopamine_b200: device set-up failed: %s\n", err.c_str());
-    return rc < 0 && rc >= -4 ? DPM_ERR_MESH : rc;
-  }
-  if (ms) {
-    ms[0] = std::chrono::duration<double, std::milli>(t1 - t0).count();
-    ms[1] = std::chrono::duration<double, std::milli>(t2 - t1).count();
-    ms[2] = tt.mesh_ms;
-    ms[3] = tt.ops_ms;
-  }
+void compare_meshes(const Mesh& mh, const StaticOps& Sh, const Mesh& md, const StaticOps& Sd, int64_t* mismatches,
+                    double* G_max_rel) {
   for (int k = 0; k < DPM_SETUP_N_ARRAYS; ++k) mismatches[k] = 0;
   int k = 0;
   auto put = [&](int64_t v) { mismatches[k++] = v; };
@@ -1589,9 +1825,84 @@ extern "C" int dpm_setup_compare(const dpm_raw_mesh_t* raw, const dpm_patch_cfg_
       }
     }
   *G_max_rel = gmax;
+}
+
+}  // namespace
+
+}  // namespace dpm
+
+extern "C" int dpm_setup_compare(const dpm_raw_mesh_t* raw, const dpm_patch_cfg_t* patches, const dpm_params_t* params,
+                                 int device, int64_t* mismatches, double* G_max_rel, double* ms) {
+  using namespace dpm;
+  if (!raw || !patches || !params || !mismatches || !G_max_rel) return DPM_ERR_ARG;
+  static_assert(kNSetupArrays <= DPM_SETUP_N_ARRAYS, "array table");
+  RawMesh r;
+  r.n_nodes = raw->n_nodes; r.xyz = raw->xyz; r.n_cells = raw->n_cells; r.cell_type = raw->cell_type;
+  r.cell_off = raw->cell_off; r.cell_nodes = raw->cell_nodes; r.n_bfaces = raw->n_bfaces;
+  r.bface_off = raw->bface_off; r.bface_nodes = raw->bface_nodes; r.bface_patch = raw->bface_patch;
+  r.n_patches = raw->n_patches;
+  std::vector<int> pbc(raw->n_patches);
+  for (int i = 0; i < raw->n_patches; ++i) pbc[i] = patches[i].bc_id;
+  Mesh mh, md;
+  StaticOps Sh, Sd;
+  std::string err;
+  auto t0 = std::chrono::steady_clock::now();
+  if (build_mesh(r, pbc.data(), mh, &err)) return DPM_ERR_MESH;
+  auto t1 = std::chrono::steady_clock::now();
+  if (build_static_ops(mh, patches, *params, Sh)) return DPM_ERR_MESH;
+  auto t2 = std::chrono::steady_clock::now();
+  SetupTimes tt;
+  int rc = build_setup_device(r, patches, *params, device, md, Sd, &err, &tt);
+  if (rc) {
+    std::fprintf(stderr, "dopamine_b200: device set-up failed: %s\n", err.c_str());
+    return rc < 0 && rc >= -4 ? DPM_ERR_MESH : rc;
+  }
+  if (ms) {
+    ms[0] = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    ms[1] = std::chrono::duration<double, std::milli>(t2 - t1).count();
+    ms[2] = tt.mesh_ms;
+    ms[3] = tt.ops_ms;
+  }
+  compare_meshes(mh, Sh, md, Sd, mismatches, G_max_rel);
   return 0;
 }
 
 extern "C" const char* dpm_setup_array_name(int k) {
   return (k >= 0 && k < dpm::kNSetupArrays) ? dpm::kSetupArrays[k] : nullptr;
+}
+
+extern "C" int dpm_setup_compare_poly(const dpm_poly_mesh_t* pmsh, const dpm_patch_cfg_t* patches,
+                                      const dpm_params_t* params, int device, int64_t* mismatches, double* G_max_rel,
+                                      double* ms) {
+  using namespace dpm;
+  if (!pmsh || !patches || !params || !mismatches || !G_max_rel) return DPM_ERR_ARG;
+  PolyMesh pm;
+  pm.n_points = pmsh->n_points; pm.xyz = pmsh->xyz; pm.n_faces = pmsh->n_faces; pm.face_off = pmsh->face_off;
+  pm.face_nodes = pmsh->face_nodes; pm.owner = pmsh->owner; pm.n_int_faces = pmsh->n_int_faces;
+  pm.neighbour = pmsh->neighbour; pm.n_patches = pmsh->n_patches; pm.patch_start = pmsh->patch_start;
+  pm.patch_nfaces = pmsh->patch_nfaces;
+  std::vector<int> pbc(pmsh->n_patches);
+  for (int i = 0; i < pmsh->n_patches; ++i) pbc[i] = patches[i].bc_id;
+  Mesh mh, md;
+  StaticOps Sh, Sd;
+  std::string err;
+  auto t0 = std::chrono::steady_clock::now();
+  if (build_mesh_poly(pm, pbc.data(), mh, &err)) return DPM_ERR_MESH;
+  auto t1 = std::chrono::steady_clock::now();
+  if (build_static_ops(mh, patches, *params, Sh)) return DPM_ERR_MESH;
+  auto t2 = std::chrono::steady_clock::now();
+  SetupTimes tt;
+  int rc = build_setup_device_poly(pm, patches, *params, device, md, Sd, &err, &tt);
+  if (rc) {
+    std::fprintf(stderr, "dopamine_b200: device set-up failed: %s\n", err.c_str());
+    return rc < 0 && rc >= -8 ? DPM_ERR_MESH : rc;
+  }
+  if (ms) {
+    ms[0] = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    ms[1] = std::chrono::duration<double, std::milli>(t2 - t1).count();
+    ms[2] = tt.mesh_ms;
+    ms[3] = tt.ops_ms;
+  }
+  compare_meshes(mh, Sh, md, Sd, mismatches, G_max_rel);
+  return 0;
 }

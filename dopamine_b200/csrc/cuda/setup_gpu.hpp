@@ -55,4 +55,10 @@ struct SetupDeviceArrays {
 int build_setup_device(const RawMesh& raw, const dpm_patch_cfg_t* pc, const dpm_params_t& P, int device, Mesh& m,
                        StaticOps& S, std::string* err, SetupTimes* t, SetupDeviceArrays* dev = nullptr);
 
+// The same for a face-based (OpenFOAM) mesh: the reference's polyhedral geometry
+// (build_mesh_poly's checks, polygon faces, polyhedron moments, face-ordered cell vertices) on
+// the device in the host builder's operation order, then the shared stages.
+int build_setup_device_poly(const PolyMesh& pm, const dpm_patch_cfg_t* pc, const dpm_params_t& P, int device,
+                            Mesh& m, StaticOps& S, std::string* err, SetupTimes* t, SetupDeviceArrays* dev = nullptr);
+
 }  // namespace dpm

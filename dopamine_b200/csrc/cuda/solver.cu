@@ -336,7 +336,7 @@ struct Solver {
     return rc;
   }
 
-  // Polyhedral mesh (dpm_create_poly): the host builds the mesh and the static operators.
+  // Polyhedral mesh (dpm_create_poly): the device builder (or the host one with host_setup).
   int init_poly(const dpm_poly_mesh_t* pmsh, const dpm_patch_cfg_t* patches, const dpm_params_t* prm, int dev) {
     device = dev;
     CK(cudaSetDevice(device));
@@ -359,18 +359,27 @@ struct Solver {
     cp_on = P.cell_projection == DPM_CELL_PROJECTION_EXACT;
     pc.assign(patches, patches + pmsh->n_patches);
     std::string err;
-    if (build_mesh_poly(pm, pbc.data(), m, &err)) {
-      std::fprintf(stderr, "dopamine_b200: polyhedral mesh set-up failed: %s\n", err.c_str());
-      return DPM_ERR_MESH;
+    SetupDeviceArrays da;
+    if (P.host_setup) {
+      if (build_mesh_poly(pm, pbc.data(), m, &err)) {
+        std::fprintf(stderr, "dopamine_b200: polyhedral mesh set-up failed: %s\n", err.c_str());
+        return DPM_ERR_MESH;
+      }
+      const auto t_mesh = Clk::now();
+      if (build_static_ops(m, pc.data(), P, S)) return DPM_ERR_MESH;
+      setup_t.mesh_ms = ms_between(t_begin, t_mesh);
+      setup_t.ops_ms = ms_between(t_mesh, Clk::now());
+    } else {
+      int rc = build_setup_device_poly(pm, pc.data(), P, device, m, S, &err, &setup_t, &da);
+      if (rc) {
+        std::fprintf(stderr, "dopamine_b200: polyhedral mesh set-up failed: %s\n", err.c_str());
+        return (rc < 0 && rc >= -8) ? DPM_ERR_MESH : rc;  // build_mesh_poly's codes -5..-8
+      }
     }
-    const auto t_mesh = Clk::now();
-    if (build_static_ops(m, pc.data(), P, S)) return DPM_ERR_MESH;
-    setup_t.mesh_ms = ms_between(t_begin, t_mesh);
-    setup_t.ops_ms = ms_between(t_mesh, Clk::now());
     if (m.n_cells > 2000000000LL || m.n_faces > 2000000000LL) return DPM_ERR_UNSUPPORTED;
     nc = (int)m.n_cells; nf = (int)m.n_faces; nb = (int)m.n_bnd_faces; nfp = (int)S.nfp;
     const auto t_up = Clk::now();
-    int rc = upload(nullptr);
+    int rc = upload(P.host_setup ? nullptr : &da);
     setup_upload_ms = ms_between(t_up, Clk::now());
     setup_total_ms = ms_between(t_begin, Clk::now());
     return rc;

@@ -33,7 +33,7 @@ EXPORTED = (
     "dpm_setup_array_name", "dpm_gmsh_read", "dpm_gmsh_sizes", "dpm_gmsh_fill", "dpm_gmsh_patch_name",
     "dpm_gmsh_free", "dpm_gmsh_write", "dpm_fcg_phase_times", "dpm_create_poly", "dpm_foam_read",
     "dpm_foam_sizes", "dpm_foam_fill", "dpm_foam_patch_name", "dpm_foam_patch_type", "dpm_foam_free",
-    "dpm_poly_cell_geometry",
+    "dpm_poly_cell_geometry", "dpm_setup_compare_poly",
 )
 
 
@@ -117,6 +117,8 @@ def lib(build_if_missing=True):
     L.dpm_fcg_phase_times.argtypes = [vp, C.c_int, dp]
     L.dpm_setup_compare.argtypes = [C.POINTER(abi.RawMeshT), C.POINTER(abi.PatchCfgT), C.POINTER(abi.ParamsT),
                                     C.c_int, C.POINTER(C.c_int64), dp, dp]
+    L.dpm_setup_compare_poly.argtypes = [C.POINTER(abi.PolyMeshT), C.POINTER(abi.PatchCfgT), C.POINTER(abi.ParamsT),
+                                         C.c_int, C.POINTER(C.c_int64), dp, dp]
     L.dpm_setup_array_name.argtypes = [C.c_int]
     L.dpm_setup_array_name.restype = C.c_char_p
     _lib = L
@@ -423,15 +425,21 @@ def compare_setups(case, device=0, params=None):
     """Builds the case's mesh and static operators with the device and the host builders
     (dpm_setup_compare).  Returns ({array name: entries whose bits differ}, largest relative
     difference of the SGS filter tensor, {stage: ms})."""
+    from .cases import PolyMesh
     L = lib()
-    mesh = abi.RawMeshView(case.mesh)
     patches = abi.patch_cfgs(case.patches)
     prm = params if params is not None else case.make_params()
     mism = (C.c_int64 * 64)()
     g = C.c_double()
     ms = np.zeros(4)
-    _check(L.dpm_setup_compare(C.byref(mesh.struct), patches, C.byref(prm), device, mism, C.byref(g), _p(ms)),
-           "dpm_setup_compare")
+    if isinstance(case.mesh, PolyMesh):
+        mesh = abi.PolyMeshView(case.mesh)
+        _check(L.dpm_setup_compare_poly(C.byref(mesh.struct), patches, C.byref(prm), device, mism, C.byref(g),
+                                        _p(ms)), "dpm_setup_compare_poly")
+    else:
+        mesh = abi.RawMeshView(case.mesh)
+        _check(L.dpm_setup_compare(C.byref(mesh.struct), patches, C.byref(prm), device, mism, C.byref(g), _p(ms)),
+               "dpm_setup_compare")
     out = {}
     for k in range(64):
         name = L.dpm_setup_array_name(k)

@@ -355,9 +355,10 @@ typedef struct {
   const int64_t* patch_nfaces;  /* [n_patches] nFaces */
 } dpm_poly_mesh_t;
 /* dpm_create for a polyhedral mesh: the reference's OpenFOAM-path geometry (faces kept in the
- * file's order, polygon face geometry, cell moments from the faces; mod_mesh.f90:1336-1461) on
- * the host, then the same static operators and time step as dpm_create.  Patches must cover the
- * boundary faces, periodic patches come in pairs (DPM_ERR_MESH otherwise). */
+ * file's order, polygon face geometry, cell moments from the faces; mod_mesh.f90:1336-1461), on
+ * the device by default (host_setup = 1: on the host; the same values), then the same static
+ * operators and time step as dpm_create.  Patches must cover the boundary faces, periodic
+ * patches come in pairs (DPM_ERR_MESH otherwise). */
 int dpm_create_poly(const dpm_poly_mesh_t* mesh, const dpm_patch_cfg_t* patches, const dpm_params_t* params,
                     int device, dpm_solver_t** out);
 /* The polyhedral set-up alone, on the host (no device needed): cell centroids (3, n_cells) and
@@ -418,6 +419,9 @@ int dpm_fcg_phase_times(dpm_solver_t* s, int enable, double* us);
 int dpm_setup_compare(const dpm_raw_mesh_t* mesh, const dpm_patch_cfg_t* patches, const dpm_params_t* params,
                       int device, int64_t* mismatches, double* G_max_rel, double* ms);
 const char* dpm_setup_array_name(int k);
+/* dpm_setup_compare for a face-based mesh (the builders behind dpm_create_poly). */
+int dpm_setup_compare_poly(const dpm_poly_mesh_t* mesh, const dpm_patch_cfg_t* patches, const dpm_params_t* params,
+                           int device, int64_t* mismatches, double* G_max_rel, double* ms);
 /* Switches an existing handle's pressure solve: DPM_PSOLVER_JACOBI_PCG (always available) or
  * back to the flexible-CG form it was created with (that form's value, or DPM_PSOLVER_AUTO);
  * any other form returns DPM_ERR_UNSUPPORTED.  Lets the plain FP64 form be timed on the same

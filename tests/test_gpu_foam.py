@@ -57,4 +57,22 @@ def test_face_based_mesh_steps_like_the_element_mesh(tmp_path, name):
     else:
         assert e <= 1e-10
     assert stp["max_abs_divU"] <= 1e-9 and ste["max_abs_divU"] <= 1e-9
-    assert tp["mesh_ms"] > 0.0 and tp["match_ms"] == 0.0  # the host polyhedral set-up ran
+    assert tp["mesh_ms"] > 0.0 and tp["match_ms"] > 0.0  # the device polyhedral set-up ran
+
+
+@pytest.mark.parametrize("name", ["channel", "tet8", "mixed8", "urban24"])
+def test_device_polyhedral_setup_matches_host(name):
+    """The device builder on a face-based mesh against the host builder (build_mesh_poly), entry
+    by entry, as tests/test_gpu_setup.py does for element meshes."""
+    from dopamine_b200.solver import compare_setups
+    case = {"channel": lambda: cases.regression_case("channel"),
+            "tet8": lambda: cases.hybrid_config(n=8, kind="tet"),
+            "mixed8": lambda: cases.hybrid_config(n=8, kind="mixed"),
+            "urban24": lambda: cases.urban_config(nx=24, ny=24, nz=12, n_blocks=4, lx=2.4, ly=2.4, lz=0.72,
+                                                  scale=0.01)}[name]()
+    case.mesh = meshio.to_poly(case.mesh)
+    mism, g, t = compare_setups(case)
+    bad = {k: v for k, v in mism.items() if v}
+    print(f"{name} (face-based): {len(mism)} arrays compared, G max rel {g:.1e}")
+    assert not bad, bad
+    assert g <= 1e-14
