@@ -1,7 +1,8 @@
-// OpenFOAM polyMesh reader (ASCII), src/mesh/mod_foam_reader.f90:foam_read and its file readers:
-// points, faces, owner, neighbour and boundary of a polyMesh directory, as the face-based arrays
-// of dpm_create_poly.  Mesh ingestion is host work; the set-up of the mesh itself is
-// build_mesh_poly (mesh.cpp).
+// OpenFOAM polyMesh reader, src/mesh/mod_foam_reader.f90:foam_read and its file readers: points,
+// faces, owner, neighbour and boundary of a polyMesh directory, ASCII or binary (byte order and
+// label / scalar sizes from the header's arch entry; faces as a faceList or a faceCompactList),
+// as the face-based arrays of dpm_create_poly.  Mesh ingestion is host work; the set-up of the
+// mesh itself is on the device (setup_gpu.cu) or in build_mesh_poly (mesh.cpp).
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -92,9 +93,17 @@ bool to_d(std::string_view t, double& v) {
   return *e == 0;
 }
 
-// Opens a polyMesh file and moves past its FoamFile header (foam_skip_header), refusing binary
-// files; class_out gets the header's class.
-int open_list(Toks& T, const std::string& path, std::string* err, std::string* class_out = nullptr) {
+// Header facts of a polyMesh file (foam_probe_file): format, byte order and label / scalar
+// sizes of binary data, class.
+struct Arch {
+  bool binary = false, little = true;
+  int label = 4, scalar = 8;
+  std::string cls;
+};
+
+// Opens a polyMesh file and moves past its FoamFile header (foam_skip_header), reading the format,
+// arch and class entries.
+int open_list(Toks& T, const std::string& path, std::string* err, Arch& A) {
   if (!T.read(path)) {
     if (err) *err = "cannot open " + path;
     return -1;
@@ -113,11 +122,13 @@ int open_list(Toks& T, const std::string& path, std::string* err, std::string* c
       else if (t == "}") --depth;
       else if (t == ";") key.clear();
       else if (key.empty()) key = std::string(t);
-      else if (key == "format" && t == "binary") {
-        if (err) *err = "binary polyMesh files are not read (" + path + "): write the mesh in ASCII";
-        return -2;
-      } else if (key == "class" && class_out) {
-        *class_out = std::string(t);
+      else if (key == "format") A.binary = t == "binary";
+      else if (key == "class") A.cls = std::string(t);
+      else if (key == "arch") {
+        const std::string a(t);
+        if (a.find("MSB") != std::string::npos) A.little = false;
+        if (a.find("label=64") != std::string::npos) A.label = 8;
+        if (a.find("scalar=32") != std::string::npos) A.scalar = 4;
       }
     }
   } else {
@@ -126,16 +137,57 @@ int open_list(Toks& T, const std::string& path, std::string* err, std::string* c
   return 0;
 }
 
-// "N (" of a list; N >= 0
+// "N (" of a list; N >= 0.  In a binary file the data starts right after '(' (no whitespace is
+// skipped there: a value's first byte may look like whitespace).
 bool list_head(Toks& T, long long& n) {
   std::string_view t;
   if (!T.next(t) || !to_ll(t, n) || n < 0) return false;
   return T.next(t) && t == "(";
 }
 
+// Raw binary label / scalar at the cursor, in the file's byte order.
+bool raw_bytes(Toks& T, const Arch& A, int size, unsigned char* out) {
+  if (T.p + size > T.text.size()) return false;
+  for (int i = 0; i < size; ++i) out[i] = (unsigned char)T.text[T.p + (A.little ? i : size - 1 - i)];
+  T.p += size;
+  return true;
+}
+bool raw_label(Toks& T, const Arch& A, long long& v) {
+  unsigned char b[8];
+  if (!raw_bytes(T, A, A.label, b)) return false;
+  if (A.label == 8) {
+    int64_t x;
+    std::memcpy(&x, b, 8);
+    v = x;
+  } else {
+    int32_t x;
+    std::memcpy(&x, b, 4);
+    v = x;
+  }
+  return true;
+}
+bool raw_scalar(Toks& T, const Arch& A, double& v) {
+  unsigned char b[8];
+  if (!raw_bytes(T, A, A.scalar, b)) return false;
+  if (A.scalar == 8) {
+    std::memcpy(&v, b, 8);
+  } else {
+    float x;
+    std::memcpy(&x, b, 4);
+    v = x;
+  }
+  return true;
+}
+bool label_at(Toks& T, const Arch& A, long long& v) {
+  if (A.binary) return raw_label(T, A, v);
+  std::string_view t;
+  return T.next(t) && to_ll(t, v);
+}
+
 int read_labels(const std::string& path, std::vector<int>& out, std::string* err) {
   Toks T;
-  int rc = open_list(T, path, err);
+  Arch A;
+  int rc = open_list(T, path, err, A);
   if (rc) return rc;
   long long n;
   std::string_view t;
@@ -146,7 +198,7 @@ int read_labels(const std::string& path, std::vector<int>& out, std::string* err
   out.resize(n);
   for (long long i = 0; i < n; ++i) {
     long long v;
-    if (!T.next(t) || !to_ll(t, v)) {
+    if (!label_at(T, A, v)) {
       if (err) *err = "malformed label in " + path;
       return -2;
     }
@@ -168,40 +220,86 @@ int read_foam(const std::string& dir, FoamMesh& M, std::string* err) {
     if (err) *err = msg;
     return -2;
   };
-  {  // points: N ( (x y z) ... )
+  {  // points: N ( (x y z) ... ), or N raw scalar triples in a binary file
     Toks T;
-    int rc = open_list(T, dir + "/points", err);
+    Arch A;
+    int rc = open_list(T, dir + "/points", err, A);
     if (rc) return rc;
     long long n;
     if (!list_head(T, n)) return fail("malformed point list in " + dir + "/points");
     M.xyz.resize(3 * n);
     for (long long i = 0; i < n; ++i) {
+      if (A.binary) {
+        for (int k = 0; k < 3; ++k)
+          if (!raw_scalar(T, A, M.xyz[3 * i + k])) return fail("truncated binary points in " + dir + "/points");
+        continue;
+      }
       if (!T.next(t) || t != "(") return fail("malformed point in " + dir + "/points");
       for (int k = 0; k < 3; ++k)
         if (!T.next(t) || !to_d(t, M.xyz[3 * i + k])) return fail("malformed coordinate in " + dir + "/points");
       if (!T.next(t) || t != ")") return fail("malformed point in " + dir + "/points");
     }
+    if (A.binary && (!T.next(t) || t != ")")) return fail("binary point list of " + dir + "/points does not end");
   }
-  {  // faces: N ( k(a b c ...) ... )
+  {  // faces: a faceList N ( k(a b ...) ... ), or a faceCompactList (offsets N+1, then the
+     // concatenated node labels); in binary files the compact form is recognised by its leading
+     // 0 label as well (foam_read_faces_binary)
     Toks T;
-    std::string cls;
-    int rc = open_list(T, dir + "/faces", err, &cls);
+    Arch A;
+    int rc = open_list(T, dir + "/faces", err, A);
     if (rc) return rc;
-    if (cls == "faceCompactList") return fail("faceCompactList faces files are not read: write the mesh as a faceList");
     long long n;
     if (!list_head(T, n)) return fail("malformed face list in " + dir + "/faces");
-    M.face_off.reserve(n + 1);
-    for (long long i = 0; i < n; ++i) {
-      long long k;
-      if (!T.next(t) || !to_ll(t, k) || k < 0) return fail("malformed face size in " + dir + "/faces");
-      if (!T.next(t) || t != "(") return fail("malformed face in " + dir + "/faces");
-      for (long long j = 0; j < k; ++j) {
+    bool compact = A.cls == "faceCompactList";
+    if (A.binary && !compact && n >= 2) {
+      const size_t save = T.p;
+      long long first;
+      if (!raw_label(T, A, first)) return fail("truncated binary faces in " + dir + "/faces");
+      T.p = save;
+      compact = first == 0;
+    }
+    if (compact) {
+      if (n < 1) return fail("compact-face offset table too small in " + dir + "/faces");
+      M.face_off.resize(n);
+      for (long long i = 0; i < n; ++i) {
         long long v;
-        if (!T.next(t) || !to_ll(t, v)) return fail("malformed face node in " + dir + "/faces");
-        M.face_nodes.push_back((int)v);
+        if (!label_at(T, A, v)) return fail("malformed compact-face offset in " + dir + "/faces");
+        M.face_off[i] = v;
+        if ((i == 0 && v != 0) || (i > 0 && v < M.face_off[i - 1]))
+          return fail("compact-face offsets must start at 0 and not decrease in " + dir + "/faces");
       }
-      if (!T.next(t) || t != ")") return fail("malformed face in " + dir + "/faces");
-      M.face_off.push_back((int64_t)M.face_nodes.size());
+      long long m2;
+      if (!T.next(t) || t != ")" || !list_head(T, m2)) return fail("malformed compact-face lists in " + dir + "/faces");
+      if (m2 != M.face_off[n - 1]) return fail("compact offsets mismatch in " + dir + "/faces");
+      M.face_nodes.resize(m2);
+      for (long long j = 0; j < m2; ++j) {
+        long long v;
+        if (!label_at(T, A, v)) return fail("malformed compact-face node in " + dir + "/faces");
+        M.face_nodes[j] = (int)v;
+      }
+    } else {
+      M.face_off.reserve(n + 1);
+      for (long long i = 0; i < n; ++i) {
+        long long k;
+        if (A.binary) {
+          if (!raw_label(T, A, k) || k < 0) return fail("malformed binary face in " + dir + "/faces");
+          for (long long j = 0; j < k; ++j) {
+            long long v;
+            if (!raw_label(T, A, v)) return fail("truncated binary faces in " + dir + "/faces");
+            M.face_nodes.push_back((int)v);
+          }
+        } else {
+          if (!T.next(t) || !to_ll(t, k) || k < 0) return fail("malformed face size in " + dir + "/faces");
+          if (!T.next(t) || t != "(") return fail("malformed face in " + dir + "/faces");
+          for (long long j = 0; j < k; ++j) {
+            long long v;
+            if (!T.next(t) || !to_ll(t, v)) return fail("malformed face node in " + dir + "/faces");
+            M.face_nodes.push_back((int)v);
+          }
+          if (!T.next(t) || t != ")") return fail("malformed face in " + dir + "/faces");
+        }
+        M.face_off.push_back((int64_t)M.face_nodes.size());
+      }
     }
   }
   int rc = read_labels(dir + "/owner", M.owner, err);
@@ -212,7 +310,8 @@ int read_foam(const std::string& dir, FoamMesh& M, std::string* err) {
   if (M.neighbour.size() > M.owner.size()) return fail("more neighbours than faces");
   {  // boundary: N ( name { type t; nFaces n; startFace s; ... } ... )
     Toks T;
-    rc = open_list(T, dir + "/boundary", err);
+    Arch A;
+    rc = open_list(T, dir + "/boundary", err, A);
     if (rc) return rc;
     long long n;
     if (!list_head(T, n)) return fail("malformed patch list in " + dir + "/boundary");

@@ -170,51 +170,82 @@ def to_poly(mesh):
                     patch_names=list(mesh.patch_names), patch_types=["patch"] * len(mesh.patch_names))
 
 
-def _foam_header(cls, obj, note=None):
-    s = ("FoamFile\n{\n    version     2.0;\n    format      ascii;\n"
-         f"    class       {cls};\n")
+def _foam_header(cls, obj, note=None, binary=False, arch=None):
+    s = ("FoamFile\n{\n    version     2.0;\n"
+         f"    format      {'binary' if binary else 'ascii'};\n")
+    if arch:
+        s += f'    arch        "{arch}";\n'
+    s += f"    class       {cls};\n"
     if note:
         s += f'    note        "{note}";\n'
     s += f'    location    "constant/polyMesh";\n    object      {obj};\n}}\n\n'
     return s
 
 
-def write_foam(polymesh_dir, mesh):
-    """Writes a mesh (cases.PolyMesh, or an element mesh converted by to_poly) as an ASCII
-    OpenFOAM polyMesh directory that read_foam reads back to the same arrays."""
+def write_foam(polymesh_dir, mesh, binary=False, compact=False, label_bytes=4, big_endian=False):
+    """Writes a mesh (cases.PolyMesh, or an element mesh converted by to_poly) as an OpenFOAM
+    polyMesh directory that read_foam reads back to the same arrays: ASCII by default, or binary
+    (labels of label_bytes bytes, 64-bit scalars, little- or big-endian), faces as a faceList or a
+    faceCompactList."""
     import os
     from .cases import PolyMesh
     pm = mesh if isinstance(mesh, PolyMesh) else to_poly(mesh)
     os.makedirs(polymesh_dir, exist_ok=True)
     nf = pm.owner.shape[0]
-    with open(os.path.join(polymesh_dir, "points"), "w") as fh:
-        fh.write(_foam_header("vectorField", "points"))
-        fh.write(f"{pm.xyz.shape[0]}\n(\n")
-        for p in pm.xyz:
-            fh.write(f"({p[0]:.17g} {p[1]:.17g} {p[2]:.17g})\n")
-        fh.write(")\n")
-    with open(os.path.join(polymesh_dir, "faces"), "w") as fh:
-        fh.write(_foam_header("faceList", "faces"))
-        fh.write(f"{nf}\n(\n")
-        for f in range(nf):
-            nodes = pm.face_nodes[pm.face_off[f]:pm.face_off[f + 1]]
-            fh.write(f"{len(nodes)}(" + " ".join(str(int(v)) for v in nodes) + ")\n")
-        fh.write(")\n")
+    order = ">" if big_endian else "<"
+    lab = np.dtype(f"{order}i{label_bytes}")
+    arch = f"{'MSB' if big_endian else 'LSB'};label={8 * label_bytes};scalar=64" if binary else None
     nc = pm.n_cells
     note = f"nPoints:{pm.xyz.shape[0]} nCells:{nc} nFaces:{nf} nInternalFaces:{pm.neighbour.shape[0]}"
+
+    def put(name, cls, body, note_=None):
+        with open(os.path.join(polymesh_dir, name), "wb") as fh:
+            fh.write(_foam_header(cls, name, note_, binary, arch).encode())
+            fh.write(body)
+
+    def blist(arr, dtype):
+        return f"{arr.size // (3 if dtype.kind == 'f' else 1)}\n(".encode() + np.ascontiguousarray(arr, dtype=dtype).tobytes() + b")\n"
+
+    def alist(items):
+        return (f"{len(items)}\n(\n" + "\n".join(items) + "\n)\n").encode()
+
+    if binary:
+        put("points", "vectorField", blist(pm.xyz.ravel(), np.dtype(f"{order}f8")))
+    else:
+        put("points", "vectorField", alist([f"({p[0]:.17g} {p[1]:.17g} {p[2]:.17g})" for p in pm.xyz]))
+    if compact:
+        off = np.asarray(pm.face_off, dtype=np.int64)
+        if binary:
+            body = (f"{off.size}\n(".encode() + off.astype(lab).tobytes() + b")\n" +
+                    f"{pm.face_nodes.size}\n(".encode() + pm.face_nodes.astype(lab).tobytes() + b")\n")
+        else:
+            body = alist([str(int(v)) for v in off]) + alist([str(int(v)) for v in pm.face_nodes])
+        put("faces", "faceCompactList", body)
+    elif binary:
+        parts = []
+        for f in range(nf):
+            nodes = pm.face_nodes[pm.face_off[f]:pm.face_off[f + 1]]
+            parts.append(np.concatenate([[len(nodes)], nodes]).astype(lab).tobytes())
+        put("faces", "faceList", f"{nf}\n(".encode() + b"".join(parts) + b")\n")
+    else:
+        put("faces", "faceList", alist([f"{pm.face_off[f + 1] - pm.face_off[f]}(" +
+                                        " ".join(str(int(v)) for v in pm.face_nodes[pm.face_off[f]:pm.face_off[f + 1]]) + ")"
+                                        for f in range(nf)]))
     for name, arr in (("owner", pm.owner), ("neighbour", pm.neighbour)):
-        with open(os.path.join(polymesh_dir, name), "w") as fh:
-            fh.write(_foam_header("labelList", name, note))
-            fh.write(f"{arr.shape[0]}\n(\n" + "\n".join(str(int(v)) for v in arr) + "\n)\n")
-    with open(os.path.join(polymesh_dir, "boundary"), "w") as fh:
-        fh.write(_foam_header("polyBoundaryMesh", "boundary"))
-        fh.write(f"{len(pm.patch_names)}\n(\n")
-        types = pm.patch_types or ["patch"] * len(pm.patch_names)
-        for k, name in enumerate(pm.patch_names):
-            fh.write(f"    {name}\n    {{\n        type            {types[k]};\n"
-                     f"        nFaces          {int(pm.patch_nfaces[k])};\n"
-                     f"        startFace       {int(pm.patch_start[k])};\n    }}\n")
-        fh.write(")\n")
+        if binary:
+            put(name, "labelList", f"{arr.size}\n(".encode() + arr.astype(lab).tobytes() + b")\n", note)
+        else:
+            put(name, "labelList", alist([str(int(v)) for v in arr]), note)
+    types = pm.patch_types or ["patch"] * len(pm.patch_names)
+    body = f"{len(pm.patch_names)}\n(\n"
+    for k, name in enumerate(pm.patch_names):
+        body += (f"    {name}\n    {{\n        type            {types[k]};\n"
+                 f"        nFaces          {int(pm.patch_nfaces[k])};\n"
+                 f"        startFace       {int(pm.patch_start[k])};\n    }}\n")
+    body += ")\n"
+    with open(os.path.join(polymesh_dir, "boundary"), "wb") as fh:  # always ASCII, as OpenFOAM writes it
+        fh.write(_foam_header("polyBoundaryMesh", "boundary").encode())
+        fh.write(body.encode())
 
 
 def poly_cell_geometry(pm, patch_bc):

@@ -315,11 +315,12 @@ int dpm_gmsh_free(dpm_gmsh_t* h);
  * faces and patches: one 2-D physical group per patch (tags 1..n_patches), one 3-D group. */
 int dpm_gmsh_write(const char* path, const dpm_raw_mesh_t* mesh, const char* const* patch_names);
 
-/* Mesh ingestion: OpenFOAM polyMesh directories (src/mesh/mod_foam_reader.f90:foam_read), ASCII
- * files (points, faces as a faceList, owner, neighbour, boundary).  The arrays of dpm_foam_fill
- * are dpm_poly_mesh_t's, sized by dpm_foam_sizes; each patch's name and OpenFOAM type are kept
- * for the caller's choice of dpm_patch_cfg_t.  DPM_ERR_ARG when a file cannot be opened,
- * DPM_ERR_MESH when one is malformed or binary, with the reason in errbuf. */
+/* Mesh ingestion: OpenFOAM polyMesh directories (src/mesh/mod_foam_reader.f90:foam_read): points,
+ * faces (faceList or faceCompactList), owner, neighbour and boundary, ASCII or binary (byte order,
+ * label and scalar sizes from the header's arch entry).  The arrays of dpm_foam_fill are
+ * dpm_poly_mesh_t's, sized by dpm_foam_sizes; each patch's name and OpenFOAM type are kept for
+ * the caller's choice of dpm_patch_cfg_t.  DPM_ERR_ARG when a file cannot be opened,
+ * DPM_ERR_MESH when one is malformed, with the reason in errbuf. */
 typedef struct dpm_foam dpm_foam_t;
 int dpm_foam_read(const char* polymesh_dir, dpm_foam_t** out, char* errbuf, int errlen);
 int dpm_foam_sizes(const dpm_foam_t* h, int64_t* n_points, int64_t* n_faces, int64_t* n_face_nodes,

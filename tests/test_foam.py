@@ -3,9 +3,11 @@ set-up (csrc/host/mesh.cpp:build_mesh_poly) on the host, against the reference's
 (src/mesh/mod_foam_reader.f90) and its polyhedral geometry (src/mesh/mod_mesh.f90:1336-1461).
 
 * A hand-written polyMesh (two hexes, comments, a FoamFile header, a patch with nested entries)
-  is read to the expected arrays; binary files, faceCompactList files and missing files are
-  refused.
-* Element meshes converted to their face-based form, written and read back, give the same arrays.
+  is read to the expected arrays; missing files, truncated binary data and compact offsets that
+  do not start at 0 are refused.
+* Element meshes converted to their face-based form, written and read back, give the same arrays
+  in every format foam_read takes: ASCII or binary (32- or 64-bit labels, either byte order),
+  faces as a faceList or a faceCompactList.
 * Cell centroids and volumes from the faces (polyhedron moments about a vertex of each cell)
   agree with the element path's independent numpy restatement where both are exact: tetrahedra
   and planar-faced hexahedra.
@@ -91,25 +93,40 @@ def test_refusals(tmp_path):
     with pytest.raises(DopamineError) as e:
         meshio.read_foam(tmp_path / "nowhere")
     assert e.value.status == abi.ERR_ARG
-    _write(tmp_path / "bin", fmt="binary")
+    # a binary points file cut short
+    _write(tmp_path / "bin")
+    pm = meshio.read_foam(tmp_path / "bin")
+    meshio.write_foam(tmp_path / "bin", pm, binary=True)
+    data = (tmp_path / "bin" / "points").read_bytes()
+    (tmp_path / "bin" / "points").write_bytes(data[:-40])
     with pytest.raises(DopamineError) as e:
         meshio.read_foam(tmp_path / "bin")
-    assert e.value.status == abi.ERR_MESH and "binary" in str(e.value)
-    _write(tmp_path / "compact", faces_cls="faceCompactList")
+    assert e.value.status == abi.ERR_MESH and "points" in str(e.value)
+    # compact offsets that do not start at 0
+    meshio.write_foam(tmp_path / "cmp", pm, compact=True)
+    text = (tmp_path / "cmp" / "faces").read_text()
+    head, rest = text.split("(\n0\n", 1)
+    (tmp_path / "cmp" / "faces").write_text(head + "(\n1\n" + rest)
     with pytest.raises(DopamineError) as e:
-        meshio.read_foam(tmp_path / "compact")
-    assert e.value.status == abi.ERR_MESH and "faceCompactList" in str(e.value)
+        meshio.read_foam(tmp_path / "cmp")
+    assert e.value.status == abi.ERR_MESH and "start at 0" in str(e.value)
 
 
 def _bcs(case):
     return [p.bc_id for p in abi.patch_cfgs(case.patches)]
 
 
+FORMATS = {"ascii": {}, "ascii-compact": dict(compact=True), "binary": dict(binary=True),
+           "binary-compact": dict(binary=True, compact=True), "binary-label64": dict(binary=True, label_bytes=8),
+           "binary-msb-compact": dict(binary=True, big_endian=True, compact=True)}
+
+
+@pytest.mark.parametrize("fmt", sorted(FORMATS))
 @pytest.mark.parametrize("make", [lambda: cases.hybrid_config(n=4, kind="tet"), lambda: cases.regression_case("channel"),
                                   lambda: cases.hybrid_config(n=4, kind="mixed")], ids=["tet", "channel", "mixed"])
-def test_round_trip(tmp_path, make):
+def test_round_trip(tmp_path, make, fmt):
     pm = meshio.to_poly(make().mesh)
-    meshio.write_foam(tmp_path / "polyMesh", pm)
+    meshio.write_foam(tmp_path / "polyMesh", pm, **FORMATS[fmt])
     r = meshio.read_foam(tmp_path / "polyMesh")
     for k in ("xyz", "face_off", "face_nodes", "owner", "neighbour", "patch_start", "patch_nfaces"):
         assert np.array_equal(getattr(pm, k), getattr(r, k)), k
