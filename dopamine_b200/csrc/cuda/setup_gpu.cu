@@ -1082,7 +1082,7 @@ int setup_device_impl(const RawMesh* rawp, const PolyMesh* polyp, const dpm_patc
     SCK(cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, st));
     SCK(cudaStreamSynchronize(st));
     if (bad & 1) return fail(-1, "unsupported element type");
-    if (nrec_ll > 2147483647LL) return fail(DPM_ERR_UNSUPPORTED, "too many element faces for the device set-up");
+    if (nrec_ll > 2147483647LL) return fail(SETUP_DEVICE_LIMIT, "too many element faces for the device set-up");
     const int64_t nrec = nrec_ll;
     ar.drop(d_nfc);
     int B = 1;
@@ -1177,7 +1177,7 @@ int setup_device_impl(const RawMesh* rawp, const PolyMesh* polyp, const dpm_patc
     SCK(cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, st));
     SCK(cudaMemcpyAsync(&unmatched, d_cnt1, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
     SCK(cudaStreamSynchronize(st));
-    if (bad & 4) return fail(DPM_ERR_UNSUPPORTED, "boundary face with other than 3 or 4 nodes");
+    if (bad & 4) return fail(-2, "boundary face with other than 3 or 4 nodes");
     if (bad & 2) return fail(-2, "boundary face has no owner cell");
     if (unmatched) return fail(-3, "unlabelled boundary faces (open cells)");
     for (void* p : {(void*)d_hs, (void*)d_ls, (void*)d_perm, (void*)d_rcell, (void*)d_rfi, (void*)d_matched,
@@ -1282,7 +1282,7 @@ int setup_device_impl(const RawMesh* rawp, const PolyMesh* polyp, const dpm_patc
     SCK(cudaMemcpyAsync(&ncn_ll, d_coff + nc, sizeof(long long), cudaMemcpyDeviceToHost, st));
     SCK(cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, st));
     SCK(cudaStreamSynchronize(st));
-    if (bad & 8) return fail(DPM_ERR_UNSUPPORTED, "a cell with more vertices than the device set-up holds");
+    if (bad & 8) return fail(SETUP_DEVICE_LIMIT, "a cell with more vertices than the device set-up holds");
     ncn = ncn_ll;
     d_cn = ar.get<int>(ncn);
     SCK(cudaGetLastError());
@@ -1577,7 +1577,7 @@ int setup_device_impl(const RawMesh* rawp, const PolyMesh* polyp, const dpm_patc
   SCK(cudaMemcpyAsync(&n_active_i, d_cnt1, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
   SCK(cudaStreamSynchronize(st));
   if (bad & 1) return fail(DPM_ERR_MESH, "non-finite or non-positive pressure coefficient");
-  if (bad & 2) return fail(DPM_ERR_UNSUPPORTED, "more pressure-solver faces per cell than the device set-up holds");
+  if (bad & 2) return fail(SETUP_DEVICE_LIMIT, "more pressure-solver faces per cell than the device set-up holds");
   S.SP = widths[0];
   S.WA = widths[1];
   if (S.WA > 16) return fail(DPM_ERR_UNSUPPORTED, "matrix row wider than 16");
@@ -1855,7 +1855,7 @@ extern "C" int dpm_setup_compare(const dpm_raw_mesh_t* raw, const dpm_patch_cfg_
   int rc = build_setup_device(r, patches, *params, device, md, Sd, &err, &tt);
   if (rc) {
     std::fprintf(stderr, "dopamine_b200: device set-up failed: %s\n", err.c_str());
-    return rc < 0 && rc >= -4 ? DPM_ERR_MESH : rc;
+    return rc == SETUP_DEVICE_LIMIT ? DPM_ERR_UNSUPPORTED : (rc < 0 && rc >= -4 ? DPM_ERR_MESH : rc);
   }
   if (ms) {
     ms[0] = std::chrono::duration<double, std::milli>(t1 - t0).count();
@@ -1895,7 +1895,7 @@ extern "C" int dpm_setup_compare_poly(const dpm_poly_mesh_t* pmsh, const dpm_pat
   int rc = build_setup_device_poly(pm, patches, *params, device, md, Sd, &err, &tt);
   if (rc) {
     std::fprintf(stderr, "dopamine_b200: device set-up failed: %s\n", err.c_str());
-    return rc < 0 && rc >= -8 ? DPM_ERR_MESH : rc;
+    return rc == SETUP_DEVICE_LIMIT ? DPM_ERR_UNSUPPORTED : (rc < 0 && rc >= -8 ? DPM_ERR_MESH : rc);
   }
   if (ms) {
     ms[0] = std::chrono::duration<double, std::milli>(t1 - t0).count();

@@ -44,6 +44,10 @@ struct SetupDeviceArrays {
   ~SetupDeviceArrays();
 };
 
+// Status of the device builder when a mesh is beyond its per-cell capacities (more than 64 vertices
+// or 16 faces in a cell, more than 2^31 element faces); the host builder has no such limits.
+constexpr int SETUP_DEVICE_LIMIT = -100;
+
 // Builds m and S on device `device`.  Returns 0, a negative mesh code of build_mesh (message in
 // *err), or a DPM_ERR_* code from the static-operator stage / the CUDA runtime.
 // dev == nullptr: every array of m and S is copied to the host (as the host builder fills them).

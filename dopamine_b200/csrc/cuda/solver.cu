@@ -322,7 +322,20 @@ struct Solver {
     SetupDeviceArrays da;
     if (!P.host_setup) {
       int rc = build_setup_device(r, pc.data(), P, device, m, S, &err, &setup_t, &da);
-      if (rc) {
+      if (rc == SETUP_DEVICE_LIMIT) {  // beyond the device builder's per-cell limits: the host builder
+        std::fprintf(stderr, "dopamine_b200: %s; building the mesh on the host\n", err.c_str());
+        P.host_setup = 1;
+        const auto t_h = Clk::now();
+        if (build_mesh(r, pbc.data(), m, &err)) {
+          std::fprintf(stderr, "dopamine_b200: mesh set-up failed: %s\n", err.c_str());
+          return DPM_ERR_MESH;
+        }
+        const auto t_mesh = Clk::now();
+        if (build_static_ops(m, pc.data(), P, S)) return DPM_ERR_MESH;
+        setup_t = SetupTimes();
+        setup_t.mesh_ms = ms_between(t_h, t_mesh);
+        setup_t.ops_ms = ms_between(t_mesh, Clk::now());
+      } else if (rc) {
         std::fprintf(stderr, "dopamine_b200: device set-up failed: %s\n", err.c_str());
         return (rc < 0 && rc >= -4) ? DPM_ERR_MESH : rc;  // build_mesh's codes -1..-4
       }
@@ -371,7 +384,20 @@ struct Solver {
       setup_t.ops_ms = ms_between(t_mesh, Clk::now());
     } else {
       int rc = build_setup_device_poly(pm, pc.data(), P, device, m, S, &err, &setup_t, &da);
-      if (rc) {
+      if (rc == SETUP_DEVICE_LIMIT) {  // cells beyond the device builder's limits: the host builder
+        std::fprintf(stderr, "dopamine_b200: %s; building the mesh on the host\n", err.c_str());
+        P.host_setup = 1;
+        const auto t_h = Clk::now();
+        if (build_mesh_poly(pm, pbc.data(), m, &err)) {
+          std::fprintf(stderr, "dopamine_b200: polyhedral mesh set-up failed: %s\n", err.c_str());
+          return DPM_ERR_MESH;
+        }
+        const auto t_mesh = Clk::now();
+        if (build_static_ops(m, pc.data(), P, S)) return DPM_ERR_MESH;
+        setup_t = SetupTimes();
+        setup_t.mesh_ms = ms_between(t_h, t_mesh);
+        setup_t.ops_ms = ms_between(t_mesh, Clk::now());
+      } else if (rc) {
         std::fprintf(stderr, "dopamine_b200: polyhedral mesh set-up failed: %s\n", err.c_str());
         return (rc < 0 && rc >= -8) ? DPM_ERR_MESH : rc;  // build_mesh_poly's codes -5..-8
       }

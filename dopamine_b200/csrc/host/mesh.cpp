@@ -516,6 +516,7 @@ int build_mesh(const RawMesh& raw, const int* patch_bc, Mesh& m, std::string* er
   for (int64_t b = 0; b < nfb; ++b) {
     const int* fn = raw.bface_nodes + raw.bface_off[b];
     int nn = (int)(raw.bface_off[b + 1] - raw.bface_off[b]);
+    if (nn < 3 || nn > 4) return fail(-2, "boundary face with other than 3 or 4 nodes");
     FaceKey key = canonical(fn, nn);
     Rec probe{key, -1, -1};
     auto it = std::lower_bound(recs.begin(), recs.end(), probe, [](const Rec& a, const Rec& p) { return a.key < p.key; });
