@@ -553,8 +553,8 @@ __global__ void k_cell_lists(int64_t nc, int64_t nfi, const long long* cfo, cons
       entry = bcanon[b] ? i : ~i;
     }
     if (has) {
-      if (ne == CPS_CAP) { atomicOr(bad, 2); return; }
-      e[ne++] = entry;
+      if (ne == CPS_CAP) atomicOr(bad, 2);  // the host stops before any kernel reads this cell's list
+      else e[ne++] = entry;
     }
   }
   for (; s < S; ++s) cf_ell[(int64_t)s * nc + c] = NONE_PAD;
@@ -873,8 +873,9 @@ __global__ void k_poly_cellverts(int64_t nc, const long long* cfo, const int* cf
         for (int j = 0; j < n; ++j)
           if (vs[j] == v) { seen = true; break; }
         if (seen) continue;
-        if (n == CV_CAP) {
+        if (n == CV_CAP) {  // the host stops after the counting pass
           atomicOr(bad, 8);
+          if (!coff) cnt[c] = n;
           return;
         }
         vs[n++] = v;
@@ -1569,6 +1570,11 @@ int setup_device_impl(const RawMesh* rawp, const PolyMesh* polyp, const dpm_patc
   SCK(cudaMemsetAsync(d_widths, 0, 2 * sizeof(int), st));
   SLAUNCH(nc, k_cell_lists, nc, nfi, d_cfo, d_cfl, d_owner, d_bps, d_bcanon, d_cfell, std::max(Sw, 1), d_cpsell,
           d_cbell, std::max(SB, 1), d_widths, d_bad);
+  // a cell whose pressure-solver list overflowed has an incomplete list: stop before reading it
+  SCK(cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, st));
+  SCK(cudaStreamSynchronize(st));
+  if (bad & 2)
+    return fail(SETUP_DEVICE_LIMIT, "more pressure-solver faces per cell than the device set-up holds");
   SLAUNCH(nc, k_diag, nc, nfi, SB, d_cpsell, d_cbell, d_psc, d_bdiag, d_bdiag_on, d_diag);
   SLAUNCH(nc, k_arow, nc, d_cpsell, d_pso, d_psn, d_psc, d_diag, 0, (int*)nullptr, (double*)nullptr, d_widths + 1);
   unsigned long long n_active_i = 0;

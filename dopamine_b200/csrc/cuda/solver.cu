@@ -315,7 +315,10 @@ struct Solver {
         return DPM_ERR_MESH;
       }
       const auto t_mesh = Clk::now();
-      if (build_static_ops(m, pc.data(), P, S)) return DPM_ERR_MESH;
+      {
+          const int rs = build_static_ops(m, pc.data(), P, S);  // rows wider than 16: unsupported
+          if (rs) return rs == DPM_ERR_UNSUPPORTED ? rs : DPM_ERR_MESH;
+        }
       setup_t.mesh_ms = ms_between(t_begin, t_mesh);
       setup_t.ops_ms = ms_between(t_mesh, Clk::now());
     }
@@ -331,7 +334,10 @@ struct Solver {
           return DPM_ERR_MESH;
         }
         const auto t_mesh = Clk::now();
-        if (build_static_ops(m, pc.data(), P, S)) return DPM_ERR_MESH;
+        {
+          const int rs = build_static_ops(m, pc.data(), P, S);  // rows wider than 16: unsupported
+          if (rs) return rs == DPM_ERR_UNSUPPORTED ? rs : DPM_ERR_MESH;
+        }
         setup_t = SetupTimes();
         setup_t.mesh_ms = ms_between(t_h, t_mesh);
         setup_t.ops_ms = ms_between(t_mesh, Clk::now());
@@ -379,7 +385,10 @@ struct Solver {
         return DPM_ERR_MESH;
       }
       const auto t_mesh = Clk::now();
-      if (build_static_ops(m, pc.data(), P, S)) return DPM_ERR_MESH;
+      {
+          const int rs = build_static_ops(m, pc.data(), P, S);  // rows wider than 16: unsupported
+          if (rs) return rs == DPM_ERR_UNSUPPORTED ? rs : DPM_ERR_MESH;
+        }
       setup_t.mesh_ms = ms_between(t_begin, t_mesh);
       setup_t.ops_ms = ms_between(t_mesh, Clk::now());
     } else {
@@ -393,7 +402,10 @@ struct Solver {
           return DPM_ERR_MESH;
         }
         const auto t_mesh = Clk::now();
-        if (build_static_ops(m, pc.data(), P, S)) return DPM_ERR_MESH;
+        {
+          const int rs = build_static_ops(m, pc.data(), P, S);  // rows wider than 16: unsupported
+          if (rs) return rs == DPM_ERR_UNSUPPORTED ? rs : DPM_ERR_MESH;
+        }
         setup_t = SetupTimes();
         setup_t.mesh_ms = ms_between(t_h, t_mesh);
         setup_t.ops_ms = ms_between(t_mesh, Clk::now());

@@ -78,19 +78,19 @@ def test_device_polyhedral_setup_matches_host(name):
     assert g <= 1e-14
 
 
-def _merged_center_mesh():
-    """A 4x4x4 box of unit hexes whose central 2x2x2 block is one polyhedral cell: 24 faces (each
-    side of the block split in four by the neighbours' faces), 26 vertices.  Faces in OpenFOAM
-    order (internal faces by owner, then neighbour), patches as in the box."""
+def _merged_mesh(block):
+    """A 4x4x4 box of unit hexes whose cells inside `block` (a box of cell-centre bounds) are merged
+    into one polyhedral cell, its faces the block's outer faces (each split where the neighbours'
+    faces meet).  Faces in OpenFOAM order (internal faces by owner, then neighbour)."""
     from dopamine_b200.cases import PolyMesh, uniform_box
     box = uniform_box(4, 4, 4, 4.0, 4.0, 4.0)
     pm = meshio.to_poly(box)
     cen = np.array([box.xyz[box.cell_nodes[box.cell_off[c]:box.cell_off[c + 1]]].mean(axis=0) for c in range(box.n_cells)])
-    inner = np.all((cen > 1.0) & (cen < 3.0), axis=1)
+    lo, hi = np.array(block[0]), np.array(block[1])
+    inner = np.all((cen > lo) & (cen < hi), axis=1)
     first = int(np.nonzero(inner)[0][0])
-    new_id = np.cumsum(~inner) - 1  # outer cells keep their order
-    new_id = np.where(inner, -1, new_id)
     merged = int((~inner[:first]).sum())  # the merged cell takes the first inner cell's place
+    new_id = np.cumsum(~inner) - 1
     new_id = np.where(new_id >= merged, new_id + 1, new_id)
     new_id[inner] = merged
     nfi = pm.neighbour.shape[0]
@@ -111,14 +111,14 @@ def _merged_center_mesh():
     return PolyMesh(xyz=pm.xyz, face_off=np.concatenate([[0], np.cumsum([len(f) for f in faces])]).astype(np.int64),
                     face_nodes=np.concatenate(faces).astype(np.int32), owner=np.array(owner, np.int32),
                     neighbour=np.array(nbr, np.int32), patch_start=pm.patch_start - nfi + n_int,
-                    patch_nfaces=pm.patch_nfaces, patch_names=pm.patch_names, patch_types=pm.patch_types)
+                    patch_nfaces=pm.patch_nfaces, patch_names=pm.patch_names, patch_types=pm.patch_types), int(inner.sum())
 
 
-def test_polyhedral_cell_beyond_the_device_limits_is_set_up_on_the_host():
-    """A 24-face cell exceeds the device builder's 16 pressure-solver entries per cell: dpm_create_
-    poly builds that mesh with the host builder instead, and the handle steps exactly as one
-    created with host_setup = 1; the merged cell's volume is the block's (8)."""
-    pm = _merged_center_mesh()
+def test_merged_polyhedral_cell():
+    """Two unit hexes merged into one 10-face polyhedral cell (volume 2) inside a periodic box: the
+    device builder takes it and the handle steps exactly as with the host builder."""
+    pm, k = _merged_mesh(((1.0, 1.0, 1.0), (3.0, 2.0, 2.0)))
+    assert k == 2
     out = []
     for host in (0, 1):
         case = cases.hybrid_config(n=4, kind="mixed", n_steps=3)  # the periodic box's parameters
@@ -126,13 +126,36 @@ def test_polyhedral_cell_beyond_the_device_limits_is_set_up_on_the_host():
         p = case.make_params()
         p.host_setup = host
         s = Solver(case, params=p)
-        assert s.nc == 64 - 7
-        assert abs(s.volume.max() - 8.0) < 1e-12 and abs(s.volume.sum() - 64.0) < 1e-10
+        assert s.nc == 63
+        assert abs(s.volume.max() - 2.0) < 1e-12 and abs(s.volume.sum() - 64.0) < 1e-10
         s.initialise()
         for _ in range(3):
             s.advance()
         out.append(s.sync_host()["U"])
         assert s.stats()["max_abs_divU"] <= 1e-9
-        assert s.setup_times()["match_ms"] == 0.0  # no device set-up stage ran
         s.close()
     assert np.array_equal(out[0], out[1])
+
+
+def test_cell_with_more_than_fifteen_neighbours_is_refused():
+    """A 2x2x2 block merged into one cell has 24 face neighbours: its pressure-operator row is wider
+    than the kernels' 16 entries. The device builder stops before reading the cell's lists and hands
+    the mesh to the host builder, which refuses the row: DPM_ERR_UNSUPPORTED either way, and the
+    handle's context stays usable."""
+    from dopamine_b200 import abi
+    from dopamine_b200.solver import DopamineError
+    pm, k = _merged_mesh(((1.0, 1.0, 1.0), (3.0, 3.0, 3.0)))
+    assert k == 8
+    for host in (0, 1):
+        case = cases.hybrid_config(n=4, kind="mixed", n_steps=3)
+        case.mesh = pm
+        p = case.make_params()
+        p.host_setup = host
+        with pytest.raises(DopamineError) as e:
+            Solver(case, params=p)
+        assert e.value.status == abi.ERR_UNSUPPORTED
+    s = Solver(cases.regression_case("channel"))  # the context still works
+    s.initialise()
+    s.advance()
+    assert s.stats()["max_abs_divU"] <= 1e-9
+    s.close()
