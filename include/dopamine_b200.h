@@ -337,7 +337,8 @@ int dpm_foam_free(dpm_foam_t* h);
 typedef struct dpm_solver dpm_solver_t;
 
 /* Mesh set-up and solver_init (mod_fv_solver.f90:302-508): builds geometry, periodic pairs,
- * LS stencils and the static projection operators on the host, uploads them to HBM. */
+ * LS stencils and the static projection operators on the device, where they stay (host_setup =
+ * 1: on the host, then uploaded; the same values), and the pressure solver's hierarchy. */
 int dpm_create(const dpm_raw_mesh_t* mesh, const dpm_patch_cfg_t* patches, const dpm_params_t* params,
                int device, dpm_solver_t** out);
 /* Face-based (polyhedral) mesh, as an OpenFOAM polyMesh holds it: faces in the file's order
