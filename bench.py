@@ -291,6 +291,8 @@ def run_gpu(args, rank, world):
         case.params["p_ml_degree"] = args.ml_degree
     if args.fcg_degree:
         case.params["p_smooth_degree"] = args.fcg_degree
+    if args.host_setup:
+        case.params["host_setup"] = 1
     s = Solver(case, device=dev)
     s.initialise()
     nc = s.nc
@@ -415,6 +417,8 @@ def main():
     ap.add_argument("--fp64", action="store_true", help="the FP64 explicit half instead of the precision form")
     ap.add_argument("--fcg-degree", type=int, default=0,
                     help="Chebyshev degree of the two-level form's part-local smoother (0: library default 7)")
+    ap.add_argument("--host-setup", action="store_true",
+                    help="build the mesh and static operators with the host builder (reported in config.setup_ms)")
     ap.add_argument("--fcg-phases", action="store_true",
                     help="after the timed region, record the two-level kernel's phase times for 2 steps")
     ap.add_argument("--psolver", default="auto", choices=["auto", "pcg", "fcg", "ml"],
