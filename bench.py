@@ -409,7 +409,7 @@ def main():
     ap.add_argument("--ml-degree", type=int, default=0,
                     help="multilevel form: Chebyshev steps per smoothing (0: library default, 3)")
     ap.add_argument("--ml-value-bits", type=int, default=0, choices=[0, 16, 32],
-                    help="multilevel form: storage of the smoother's scaled off-diagonals (0: library default, 16)")
+                    help="multilevel form: storage of the smoother's scaled off-diagonals (0: library default, FP32)")
     ap.add_argument("--mixed", action="store_true", default=True,
                     help="precision form (the default: the metric is learned+mixed): FP32 gradients, SGS and flux "
                          "assembly; with the two-level form also FP32-operator inner iterations inside FP64 defect "
