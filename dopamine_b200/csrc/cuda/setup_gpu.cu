@@ -17,8 +17,14 @@
 //     slots by atomics, then each list sorted, which makes the result independent of the order
 //     in which the atomics landed;
 //   * LS stencil and per-cell operators: one thread per cell over its sorted lists.
+//   * face-based (OpenFOAM) meshes skip the matching: their faces come in the file's order, and
+//     polygon face geometry, polyhedron moments and face-ordered cell vertices (the reference's
+//     OpenFOAM path) are one thread per face or cell before the shared stages.
 // Periodic pairing (per patch, a sort of the patch's face centres) and the outlet rows stay on
-// the host; they touch boundary faces only.
+// the host; they touch boundary faces only.  Per-cell work arrays have fixed capacities (16
+// pressure-solver entries, 64 vertices): a cell beyond them makes the builder stop with
+// SETUP_DEVICE_LIMIT before any kernel reads an incomplete list, and the caller uses the host
+// builder.
 #include "setup_gpu.hpp"
 
 #include <cuda_runtime.h>
