@@ -2,6 +2,7 @@
 #include "mesh.hpp"
 
 #include <algorithm>
+#include <parallel/algorithm>
 #include <array>
 #include <cmath>
 #include <cstring>
@@ -315,6 +316,7 @@ int finish_mesh(Mesh& m, std::string* err) {
   const int max_stencil = std::max(32, 4 * max_faces);
   std::vector<int> cnt(nc, 0), tnb((size_t)nc * max_stencil, -1), tface((size_t)nc * max_stencil, -1);
   std::vector<uint8_t> tper((size_t)nc * max_stencil, 0);
+#pragma omp parallel for schedule(static)
   for (int64_t i = 0; i < nc; ++i) {
     for (int64_t idx = m.cell_face_off[i]; idx < m.cell_face_off[i + 1]; ++idx) {
       int f = m.cell_faces[idx];
@@ -457,15 +459,27 @@ int build_mesh(const RawMesh& raw, const int* patch_bc, Mesh& m, std::string* er
   // created when its second cell reaches it, so ordering (second cell, local face) reproduces
   // its face numbering (mod_gmsh_reader.f90:build_faces_from_cells).
   struct Rec { FaceKey key; int cell; int fi; };
-  std::vector<Rec> recs;
-  recs.reserve(nc * 6);
+  // (key, cell, local face) is a strict total order over distinct records, so any sort gives the
+  // same sequence; the parallel one is used.
+  std::vector<int64_t> roff(nc + 1, 0);
+  int bad_type = 0;
+#pragma omp parallel for schedule(static) reduction(| : bad_type)
   for (int64_t c = 0; c < nc; ++c) {
     int fn[6][4], nn[6];
     int nfc = element_faces(raw.cell_type[c], raw.cell_nodes + raw.cell_off[c], fn, nn);
-    if (nfc == 0) return fail(-1, "unsupported element type");
-    for (int i = 0; i < nfc; ++i) recs.push_back({canonical(fn[i], nn[i]), (int)c, i});
+    if (nfc == 0) bad_type = 1;
+    roff[c + 1] = nfc;
   }
-  std::sort(recs.begin(), recs.end(), [](const Rec& a, const Rec& b) {
+  if (bad_type) return fail(-1, "unsupported element type");
+  for (int64_t c = 0; c < nc; ++c) roff[c + 1] += roff[c];
+  std::vector<Rec> recs(roff[nc]);
+#pragma omp parallel for schedule(static)
+  for (int64_t c = 0; c < nc; ++c) {
+    int fn[6][4], nn[6];
+    int nfc = element_faces(raw.cell_type[c], raw.cell_nodes + raw.cell_off[c], fn, nn);
+    for (int i = 0; i < nfc; ++i) recs[roff[c] + i] = {canonical(fn[i], nn[i]), (int)c, i};
+  }
+  __gnu_parallel::sort(recs.begin(), recs.end(), [](const Rec& a, const Rec& b) {
     if (a.key < b.key) return true;
     if (b.key < a.key) return false;
     return a.cell < b.cell || (a.cell == b.cell && a.fi < b.fi);
@@ -482,7 +496,7 @@ int build_mesh(const RawMesh& raw, const int* patch_bc, Mesh& m, std::string* er
     }
     i = j;
   }
-  std::sort(ifaces.begin(), ifaces.end(), [](const IntFace& a, const IntFace& b) {
+  __gnu_parallel::sort(ifaces.begin(), ifaces.end(), [](const IntFace& a, const IntFace& b) {
     return a.second_cell < b.second_cell || (a.second_cell == b.second_cell && a.second_fi < b.second_fi);
   });
   const int64_t nfi = (int64_t)ifaces.size();
@@ -512,16 +526,20 @@ int build_mesh(const RawMesh& raw, const int* patch_bc, Mesh& m, std::string* er
   }
   // Boundary faces in element order, then regrouped by patch.
   std::vector<int> b_owner(nfb), b_patch(nfb);
+  std::vector<int64_t> b_rec(nfb, -1);
   std::vector<double> b_centre(3 * nfb), b_normal(3 * nfb), b_area(nfb);
+  // The first failing boundary face decides the message, as in a sequential walk.
+  int64_t first_bad = nfb;
+#pragma omp parallel for schedule(static) reduction(min : first_bad)
   for (int64_t b = 0; b < nfb; ++b) {
     const int* fn = raw.bface_nodes + raw.bface_off[b];
     int nn = (int)(raw.bface_off[b + 1] - raw.bface_off[b]);
-    if (nn < 3 || nn > 4) return fail(-2, "boundary face with other than 3 or 4 nodes");
+    if (nn < 3 || nn > 4) { first_bad = std::min(first_bad, b); continue; }
     FaceKey key = canonical(fn, nn);
     Rec probe{key, -1, -1};
     auto it = std::lower_bound(recs.begin(), recs.end(), probe, [](const Rec& a, const Rec& p) { return a.key < p.key; });
-    if (it == recs.end() || !(it->key == key)) return fail(-2, "boundary face has no owner cell");
-    matched[it - recs.begin()] = 1;
+    if (it == recs.end() || !(it->key == key)) { first_bad = std::min(first_bad, b); continue; }
+    b_rec[b] = it - recs.begin();
     b_owner[b] = it->cell;
     b_patch[b] = raw.bface_patch[b];
     face_geometry(fn, nn, raw.xyz, &b_centre[3 * b], &b_normal[3 * b], b_area[b]);
@@ -530,6 +548,11 @@ int build_mesh(const RawMesh& raw, const int* patch_bc, Mesh& m, std::string* er
     if (dot3(&b_normal[3 * b], d) < 0.0)
       for (int k = 0; k < 3; ++k) b_normal[3 * b + k] = -b_normal[3 * b + k];
   }
+  if (first_bad < nfb) {
+    int nn = (int)(raw.bface_off[first_bad + 1] - raw.bface_off[first_bad]);
+    return fail(-2, (nn < 3 || nn > 4) ? "boundary face with other than 3 or 4 nodes" : "boundary face has no owner cell");
+  }
+  for (int64_t b = 0; b < nfb; ++b) matched[b_rec[b]] = 1;
   for (size_t i = 0; i < recs.size(); ++i)
     if (!matched[i]) return fail(-3, "unlabelled boundary faces (open cells)");
   m.patch_start.assign(m.n_patches, 0);
