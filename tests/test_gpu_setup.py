@@ -48,8 +48,9 @@ def test_device_setup_matches_host(name):
 
 def test_device_setup_matches_host_urban_2m():
     case = cases.urban_config(200, 200, 63)
-    t = _check_same("urban 200x200x63", case)
-    assert t["device_mesh_ms"] + t["device_ops_ms"] < t["host_mesh_ms"] + t["host_ops_ms"]
+    # The stage times are printed, not compared: in this comparison mode the device builder also
+    # copies every array back to the host, and the host builder runs on all host threads.
+    _check_same("urban 200x200x63", case)
 
 
 def test_both_builders_take_the_same_steps():
