@@ -18,8 +18,7 @@
 //    until the process exits.  That first call can fail with DPM_ERR_CUDA when the device has no
 //    free memory left.  A call with max_iterations == 0 does only this per-device set-up (module
 //    load, every solve kernel variant, the array's address) and returns 0 without touching any
-//    array argument: make it before the host's pool reserves the device's memory, and before
-//    any stream capture;
+//    array argument: make it before the host's pool reserves the device's memory;
 //  * all calls share that one array and it keeps the last call's contents; each call clears
 //    the parts that must start at zero (barrier counter, status words) itself;
 //  * calls that overlap on the GPU (two streams, or two host threads) race on the array and must

@@ -578,7 +578,7 @@ int dpm_multilevel_hierarchy(int n, int width, const int* col, const double* val
  * with DPM_ERR_CUDA if the device has no free memory) and are then held until the process
  * exits.  A call with max_iterations == 0 (sizes in range, array pointers may be NULL) does only
  * that set-up and returns 0: make it once per device before the host's pool reserves the
- * device's memory, and before any stream capture.
+ * device's memory.
  * Stopping rule: the PETSc KSPCG test of fvm_petsc_solve_pressure (unpreconditioned norm,
  * ||r|| <= max(rtol ||b||, atol)); null_space != 0 projects the constant mode out of the
  * right-hand side.  Unlike fvm_petsc_solve_pressure there is no retry from a zero guess, no
