@@ -1918,3 +1918,120 @@ extern "C" int dpm_setup_compare_poly(const dpm_poly_mesh_t* pmsh, const dpm_pat
   compare_meshes(mh, Sh, md, Sd, mismatches, G_max_rel);
   return 0;
 }
+
+// ---- host builder digests (C-ABI, no device) ---------------------------------------------------
+
+namespace dpm {
+namespace {
+
+// 64-bit FNV-1a over the bytes, seeded with the element count.
+struct Fnv {
+  uint64_t h = 1469598103934665603ull;
+  void bytes(const void* p, size_t n) {
+    const unsigned char* b = static_cast<const unsigned char*>(p);
+    for (size_t i = 0; i < n; ++i) { h ^= b[i]; h *= 1099511628211ull; }
+  }
+  void i64(int64_t v) { bytes(&v, sizeof(v)); }
+  template <class T> void vec(const std::vector<T>& v) {
+    i64((int64_t)v.size());
+    bytes(v.data(), v.size() * sizeof(T));
+  }
+};
+
+template <class T> uint64_t digest(const std::vector<T>& v) {
+  Fnv f;
+  f.vec(v);
+  return f.h;
+}
+
+// One digest per array, in kSetupArrays order; returns how many were written.
+int digest_setup(const Mesh& m, const StaticOps& S, uint64_t* out) {
+  int k = 0;
+  auto put = [&](uint64_t v) { out[k++] = v; };
+  put(digest(m.centroid)); put(digest(m.volume)); put(digest(m.cell_face_off)); put(digest(m.cell_faces));
+  put(digest(m.owner)); put(digest(m.neighbour)); put(digest(m.patch)); put(digest(m.area));
+  put(digest(m.centre)); put(digest(m.normal)); put(digest(m.sf)); put(digest(m.d_cf)); put(digest(m.gc));
+  put(digest(m.eps)); put(digest(m.skew)); put(digest(m.is_refine)); put(digest(m.patch_start));
+  put(digest(m.patch_nfaces)); put(digest(m.periodic_pair)); put(digest(m.periodic_pair_dcf));
+  put(digest(m.periodic_gc)); put(digest(m.ls_off)); put(digest(m.ls_cell)); put(digest(m.ls_face));
+  put(digest(m.ls_w));
+  {
+    Fnv f;
+    f.i64(m.n_cells); f.i64(m.n_faces); f.i64(m.n_int_faces); f.i64(m.n_bnd_faces); f.i64(m.ls_degenerate);
+    f.vec(m.vertices); f.vec(m.cell_vert_off); f.vec(m.cell_vertices); f.vec(m.patch_bc);
+    put(f.h);
+  }
+  put(digest(S.ps_o)); put(digest(S.ps_n)); put(digest(S.ps_f)); put(digest(S.ps_coeff)); put(digest(S.ps_gcf));
+  put(digest(S.ps_gcw)); put(digest(S.ps_k)); put(digest(S.ps_krc)); put(digest(S.diag)); put(digest(S.bnd_kout));
+  put(digest(S.bnd_cb)); put(digest(S.bnd_bc)); put(digest(S.bnd_pnb)); put(digest(S.dir_rows));
+  put(digest(S.dir_vals)); put(digest(S.A_col)); put(digest(S.A_val)); put(digest(S.cell_face));
+  put(digest(S.cell_ps)); put(digest(S.cell_bnd)); put(digest(S.ls_idx)); put(digest(S.ls_w)); put(digest(S.Tinv));
+  put(digest(S.y_w)); put(digest(S.wblend));
+  {
+    Fnv f;
+    for (int64_t v : {(int64_t)S.nc, (int64_t)S.nf, (int64_t)S.nfi, (int64_t)S.nb, (int64_t)S.nfp, (int64_t)S.S,
+                      (int64_t)S.SP, (int64_t)S.SB, (int64_t)S.W, (int64_t)S.WA, (int64_t)S.skip_nonortho,
+                      (int64_t)S.skip_grad_p, (int64_t)S.diag_interface, (int64_t)S.n_nonortho_corr,
+                      (int64_t)S.n_outlet})
+      f.i64(v);
+    f.bytes(&S.V_min, sizeof(double));
+    f.bytes(&S.V_total, sizeof(double));
+    put(f.h);
+  }
+  return k;
+}
+
+int host_digest(const RawMesh* raw, const PolyMesh* poly, int n_patches, const dpm_patch_cfg_t* patches,
+                const dpm_params_t& P, uint64_t* digests, int* n_arrays, uint64_t* G_digest, char* errbuf,
+                int errlen) {
+  std::vector<int> pbc(n_patches);
+  for (int i = 0; i < n_patches; ++i) pbc[i] = patches[i].bc_id;
+  Mesh m;
+  StaticOps S;
+  std::string err;
+  int rc = raw ? build_mesh(*raw, pbc.data(), m, &err) : build_mesh_poly(*poly, pbc.data(), m, &err);
+  if (rc) {
+    if (errbuf && errlen > 0) std::snprintf(errbuf, (size_t)errlen, "%s", err.c_str());
+    return DPM_ERR_MESH;
+  }
+  rc = build_static_ops(m, patches, P, S);
+  if (rc) {
+    if (errbuf && errlen > 0)
+      std::snprintf(errbuf, (size_t)errlen, "%s",
+                    rc == DPM_ERR_UNSUPPORTED ? "a matrix row wider than 16 entries" : "static operators refused the mesh");
+    return rc;
+  }
+  const int n = digest_setup(m, S, digests);
+  if (n_arrays) *n_arrays = n;
+  if (G_digest) *G_digest = digest(S.G);
+  return n == kNSetupArrays ? DPM_OK : DPM_ERR_ARG;
+}
+
+}  // namespace
+}  // namespace dpm
+
+extern "C" int dpm_setup_host_digest(const dpm_raw_mesh_t* raw, const dpm_patch_cfg_t* patches,
+                                     const dpm_params_t* params, uint64_t* digests, int* n_arrays, uint64_t* G_digest,
+                                     char* errbuf, int errlen) {
+  using namespace dpm;
+  if (!raw || (raw->n_patches > 0 && !patches) || !params || !digests) return DPM_ERR_ARG;
+  RawMesh r;
+  r.n_nodes = raw->n_nodes; r.xyz = raw->xyz; r.n_cells = raw->n_cells; r.cell_type = raw->cell_type;
+  r.cell_off = raw->cell_off; r.cell_nodes = raw->cell_nodes; r.n_bfaces = raw->n_bfaces;
+  r.bface_off = raw->bface_off; r.bface_nodes = raw->bface_nodes; r.bface_patch = raw->bface_patch;
+  r.n_patches = raw->n_patches;
+  return host_digest(&r, nullptr, raw->n_patches, patches, *params, digests, n_arrays, G_digest, errbuf, errlen);
+}
+
+extern "C" int dpm_setup_host_digest_poly(const dpm_poly_mesh_t* pmsh, const dpm_patch_cfg_t* patches,
+                                          const dpm_params_t* params, uint64_t* digests, int* n_arrays,
+                                          uint64_t* G_digest, char* errbuf, int errlen) {
+  using namespace dpm;
+  if (!pmsh || (pmsh->n_patches > 0 && !patches) || !params || !digests) return DPM_ERR_ARG;
+  PolyMesh pm;
+  pm.n_points = pmsh->n_points; pm.xyz = pmsh->xyz; pm.n_faces = pmsh->n_faces; pm.face_off = pmsh->face_off;
+  pm.face_nodes = pmsh->face_nodes; pm.owner = pmsh->owner; pm.n_int_faces = pmsh->n_int_faces;
+  pm.neighbour = pmsh->neighbour; pm.n_patches = pmsh->n_patches; pm.patch_start = pmsh->patch_start;
+  pm.patch_nfaces = pmsh->patch_nfaces;
+  return host_digest(nullptr, &pm, pmsh->n_patches, patches, *params, digests, n_arrays, G_digest, errbuf, errlen);
+}

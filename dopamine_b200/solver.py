@@ -33,7 +33,7 @@ EXPORTED = (
     "dpm_setup_array_name", "dpm_gmsh_read", "dpm_gmsh_sizes", "dpm_gmsh_fill", "dpm_gmsh_patch_name",
     "dpm_gmsh_free", "dpm_gmsh_write", "dpm_fcg_phase_times", "dpm_create_poly", "dpm_foam_read",
     "dpm_foam_sizes", "dpm_foam_fill", "dpm_foam_patch_name", "dpm_foam_patch_type", "dpm_foam_free",
-    "dpm_poly_cell_geometry", "dpm_setup_compare_poly",
+    "dpm_poly_cell_geometry", "dpm_setup_compare_poly", "dpm_setup_host_digest", "dpm_setup_host_digest_poly",
 )
 
 
@@ -121,6 +121,10 @@ def lib(build_if_missing=True):
                                          C.c_int, C.POINTER(C.c_int64), dp, dp]
     L.dpm_setup_array_name.argtypes = [C.c_int]
     L.dpm_setup_array_name.restype = C.c_char_p
+    for name, mt in (("dpm_setup_host_digest", abi.RawMeshT), ("dpm_setup_host_digest_poly", abi.PolyMeshT)):
+        getattr(L, name).argtypes = [C.POINTER(mt), C.POINTER(abi.PatchCfgT), C.POINTER(abi.ParamsT),
+                                     C.POINTER(C.c_uint64), C.POINTER(C.c_int), C.POINTER(C.c_uint64), C.c_char_p,
+                                     C.c_int]
     _lib = L
     return L
 
@@ -448,3 +452,28 @@ def compare_setups(case, device=0, params=None):
         out[name.decode()] = int(mism[k])
     times = dict(zip(("host_mesh_ms", "host_ops_ms", "device_mesh_ms", "device_ops_ms"), ms.tolist()))
     return out, g.value, times
+
+
+def host_setup_digests(case, params=None):
+    """Builds the case's mesh and static operators with the host builder alone (no device) and
+    returns ({array name: 64-bit FNV-1a digest}, digest of the SGS filter tensor)
+    (dpm_setup_host_digest)."""
+    from .cases import PolyMesh
+    L = lib()
+    patches = abi.patch_cfgs(case.patches)
+    prm = params if params is not None else case.make_params()
+    dig = (C.c_uint64 * 64)()
+    n = C.c_int()
+    g = C.c_uint64()
+    err = C.create_string_buffer(512)
+    if isinstance(case.mesh, PolyMesh):
+        mesh = abi.PolyMeshView(case.mesh)
+        rc = L.dpm_setup_host_digest_poly(C.byref(mesh.struct), patches, C.byref(prm), dig, C.byref(n), C.byref(g),
+                                          err, len(err))
+    else:
+        mesh = abi.RawMeshView(case.mesh)
+        rc = L.dpm_setup_host_digest(C.byref(mesh.struct), patches, C.byref(prm), dig, C.byref(n), C.byref(g), err,
+                                     len(err))
+    if rc != 0:
+        raise DopamineError(f"dpm_setup_host_digest: {err.value.decode()}", rc)
+    return {L.dpm_setup_array_name(k).decode(): int(dig[k]) for k in range(n.value)}, int(g.value)
