@@ -2674,6 +2674,36 @@ int dpm_multilevel_hierarchy(int n, int width, const int* col, const double* val
   return (int)M.sizes.size();
 }
 
+int dpm_multilevel_digest(int n, int width, const int* col, const double* val, int nullsp, int passes,
+                          unsigned long long* digest) {
+  if (n < 1 || width < 1 || !col || !val || !digest) return DPM_ERR_ARG;
+  dpm::Multilevel M;
+  int rc = dpm::build_multilevel(n, width, col, val, nullsp != 0, passes > 0 ? passes : 3, 0.25, 300, 1024, M);
+  if (rc) return rc;
+  // 64-bit FNV-1a over every array of every level, each preceded by its element count
+  uint64_t h = 1469598103934665603ull;
+  auto mix = [&](const void* p, size_t bytes) {
+    const unsigned char* b = static_cast<const unsigned char*>(p);
+    for (size_t i = 0; i < bytes; ++i) { h ^= b[i]; h *= 1099511628211ull; }
+  };
+  auto vec = [&](const auto& v) {
+    const int64_t k = (int64_t)v.size();
+    mix(&k, sizeof(k));
+    if (k) mix(v.data(), v.size() * sizeof(v[0]));
+  };
+  for (const dpm::MlLevel& L : M.lv) {
+    const int hdr[4] = {L.n, L.W, L.M, L.Wo};
+    mix(hdr, sizeof(hdr));
+    vec(L.dinv); vec(L.ocol); vec(L.sv32); vec(L.sv16); vec(L.g32); vec(L.g16); vec(L.diag); vec(L.agg);
+    vec(L.mem);
+    mix(&L.lmax, sizeof(L.lmax));
+  }
+  mix(&M.nC, sizeof(M.nC));
+  vec(M.cinv); vec(M.sizes); vec(M.nnz);
+  *digest = (unsigned long long)h;
+  return (int)M.sizes.size();
+}
+
 int dpm_learn_sizes(dpm_solver_t* h, int* sizes) {
   if (!h || !sizes) return DPM_ERR_ARG;
   Solver& s = *h->s;

@@ -34,6 +34,7 @@ EXPORTED = (
     "dpm_gmsh_free", "dpm_gmsh_write", "dpm_fcg_phase_times", "dpm_create_poly", "dpm_foam_read",
     "dpm_foam_sizes", "dpm_foam_fill", "dpm_foam_patch_name", "dpm_foam_patch_type", "dpm_foam_free",
     "dpm_poly_cell_geometry", "dpm_setup_compare_poly", "dpm_setup_host_digest", "dpm_setup_host_digest_poly",
+    "dpm_multilevel_digest",
 )
 
 
@@ -100,6 +101,7 @@ def lib(build_if_missing=True):
     L.dpm_learn_sizes.argtypes = [vp, ip]
     L.dpm_multilevel_hierarchy.argtypes = [C.c_int, C.c_int, ip, dp, C.c_int, C.c_int, ip, C.POINTER(C.c_longlong),
                                            C.c_int]
+    L.dpm_multilevel_digest.argtypes = [C.c_int, C.c_int, ip, dp, C.c_int, C.c_int, C.POINTER(C.c_ulonglong)]
     L.dpm_learn_export.argtypes = [vp, fp, C.c_void_p, ip, dp, dp, dp, dp, dp, fp]
     L.dpm_learn_loss_grad.argtypes = [vp, fp, dp, fp]
     L.dpm_download_scalars.argtypes = [vp, dp]

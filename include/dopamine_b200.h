@@ -574,6 +574,11 @@ int dpm_download_scalars(dpm_solver_t* s, double* C);
  * number of levels (<= max_levels) or a negative code. */
 int dpm_multilevel_hierarchy(int n, int width, const int* col, const double* val, int nullsp, int passes,
                              int* sizes, long long* nnz, int max_levels);
+/* The same hierarchy, reduced to one 64-bit FNV-1a digest of every level's arrays (operator, scaled
+ * rows in FP32 and binary16, diagonals, aggregates, members, eigenvalue estimate) and the coarsest
+ * level's inverse.  Returns the number of levels or a negative code. */
+int dpm_multilevel_digest(int n, int width, const int* col, const double* val, int nullsp, int passes,
+                          unsigned long long* digest);
 
 /* ---- allocation-free Jacobi-PCG solve --------------------------------------------------------
  * No counterpart in the reference.  For callers that cannot allocate device memory when they

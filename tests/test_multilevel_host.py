@@ -3,10 +3,13 @@
 
 On the channel's assembled pressure operator (stretched wall-normal spacing) and on a seeded
 7-point Neumann box, three pairwise passes per level must coarsen by at least 3x per level down to
-a directly solved level of at most 300 rows, keeping the coarse operators sparse."""
+a directly solved level of at most 300 rows, keeping the coarse operators sparse.  The host
+threads build rows and aggregates in a fixed order and reduce norms over fixed chunks, so the whole
+hierarchy (dpm_multilevel_digest) is the same bit for bit on 1, 3 or all host threads."""
 import ctypes as C
 
 import numpy as np
+import pytest
 
 from dopamine_b200 import cases
 from dopamine_b200.solver import lib
@@ -37,6 +40,15 @@ def hierarchy(n, W, ec, ev, nullsp, passes=3):
     return sizes[:nl], nnz[:nl]
 
 
+def digest(n, W, ec, ev, nullsp, passes=3):
+    d = C.c_ulonglong()
+    nl = lib().dpm_multilevel_digest(n, W, ec.ctypes.data_as(C.POINTER(C.c_int)),
+                                     ev.ctypes.data_as(C.POINTER(C.c_double)), 1 if nullsp else 0, passes,
+                                     C.byref(d))
+    assert nl > 0, nl
+    return d.value
+
+
 def check(sizes, nnz):
     assert sizes[-1] <= 300
     for a, b in zip(sizes[:-1], sizes[1:]):
@@ -54,7 +66,8 @@ def test_channel_operator_hierarchy():
     check(sizes, nnz)
 
 
-def test_neumann_box_hierarchy():
+def neumann_box_operator():
+    """A seeded anisotropic 7-point Neumann operator on a 40x30x20 box, in padded ELL."""
     rng = np.random.default_rng(7)
     nx, ny, nz = 40, 30, 20
     n = nx * ny * nz
@@ -81,8 +94,39 @@ def test_neumann_box_hierarchy():
         vals += [v for _, v in r]
         off[i + 1] = len(cols)
     W, ec, ev = ell_from_csr(off, np.array(cols, dtype=np.int32), np.array(vals))
+    return n, W, ec, ev
+
+
+def test_neumann_box_hierarchy():
+    n, W, ec, ev = neumann_box_operator()
     sizes, nnz = hierarchy(n, W, ec, ev, True)
     check(sizes, nnz)
     # the hierarchy is a pure function of the operator
     s2, z2 = hierarchy(n, W, ec, ev, True)
     assert np.array_equal(sizes, s2) and np.array_equal(nnz, z2)
+
+
+def _oracle_operator(case):
+    off, col, val = O.Oracle(case).poisson_csr()
+    return (off.size - 1, *ell_from_csr(off, col, val))
+
+
+@pytest.mark.parametrize("name", ["channel", "neumann box", "jittered tets"])
+def test_same_hierarchy_on_any_thread_count(name):
+    from tests.test_host_setup import _Threads
+    op = {"channel": lambda: _oracle_operator(cases.channel_config(nx=32, ny=24, nz=16, n_steps=1)),
+          "neumann box": neumann_box_operator,
+          "jittered tets": lambda: _oracle_operator(cases.hybrid_config(n=10, kind="tet"))}[name]()
+    threads = _Threads()
+    out = []
+    try:
+        for t in (1, 3, threads.default):
+            threads(t)
+            out.append(digest(*op, True))
+    finally:
+        threads(threads.default)
+    assert out[0] == out[1] == out[2], [hex(d) for d in out]
+    n, W, ec, ev = op
+    ev = ev.copy()
+    ev[n + 5] *= 1.01  # the second stored entry of row 5
+    assert digest(n, W, ec, ev, True) != out[0]
