@@ -426,8 +426,8 @@ int dpm_setup_compare_poly(const dpm_poly_mesh_t* mesh, const dpm_patch_cfg_t* p
                            int device, int64_t* mismatches, double* G_max_rel, double* ms);
 /* The host builder alone (no device needed): builds the mesh and static operators on the host
  * threads and writes a 64-bit FNV-1a digest of each array's element count and bytes to
- * digests[k], k < *n_arrays, in dpm_setup_array_name order, and the SGS filter tensor's to
- * *G_digest.  A refused mesh returns DPM_ERR_MESH (or DPM_ERR_UNSUPPORTED for an assembled row
+ * digests[k], k < *n_arrays, in dpm_setup_array_name order (digests holds DPM_SETUP_N_ARRAYS
+ * entries), and the SGS filter tensor's to *G_digest.  A refused mesh returns DPM_ERR_MESH (or DPM_ERR_UNSUPPORTED for an assembled row
  * wider than 16 entries) with the host builder's reason in errbuf. */
 int dpm_setup_host_digest(const dpm_raw_mesh_t* mesh, const dpm_patch_cfg_t* patches, const dpm_params_t* params,
                           uint64_t* digests, int* n_arrays, uint64_t* G_digest, char* errbuf, int errlen);
